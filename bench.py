@@ -1,0 +1,317 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 force/integration path (one JSON line on rank 0).
+
+Workload: 33,400 flexible waters (100,200 atoms) in a 10 nm cube, LJ + Ewald
+real space at 1.0 nm, PME 96^3 order 4, pair list every 10 steps, leapfrog at
+1 fs.  Metric: ns/day (steps * dt * 86400 / time); pairs/s is reported beside
+it.  A step is one full MD step (forces + integration, list rebuild every
+10th).  Inputs are seeded synthetic water (no public dataset is named).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl lima|reference]
+
+N > 1 runs under torchrun as independent replicas (a single system does not
+shard), value = the sum of all ranks' ns/day over the max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+DT_NS = 1e-6
+CUTOFF = 1.0
+GRID = (96, 96, 96)
+FLOPS_PER_PAIR = 50          # counting rule of the pair kernel's roofline
+WORKLOAD = "water100k_10nm_pme96"
+
+
+def ns_per_day(step_seconds: float) -> float:
+    # the reference prints n_steps*dt/(wall/86400) (code/LIMA/mdrun.h:134-143)
+    return DT_NS * 86400.0 / step_seconds
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active," \
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_step_time(system, n_steps: int, threads: int):
+    """The CPU oracle port of the same step (FP32 reference-faithful pair loop with
+    all host threads, FP64 SPME and bonded terms, leapfrog), seconds per step."""
+    from oracle import oracle as O
+    from lima_b200.systems import ewald_kappa
+    O.build()
+    kappa = ewald_kappa(CUTOFF, 1e-5)
+    s = system
+    ex = s.exclusions()
+    xp = ex[(s.charge[ex[:, 0]] != 0) & (s.charge[ex[:, 1]] != 0)]
+    pos = s.pos.copy()
+    vel = s.vel.astype(np.float64).copy()
+    fprev = np.zeros_like(pos)
+    m = s.mass.astype(np.float64)
+    times = []
+    for k in range(n_steps + 1):
+        t0 = time.perf_counter()
+        f, _, _ = O.nonbonded(pos, s.box, s.charge, s.sigma, s.epsilon, ex, CUTOFF, 2, kappa, precision=32,
+                              nthreads=threads)
+        fl, _, _ = O.pme(pos, s.charge, s.box, GRID, kappa)
+        fx, _ = O.exclusion_correction(pos, s.charge, s.box, xp, kappa)
+        fb, _ = O.bonded(pos, s.box, s.bonds, s.bond_par, s.angles, s.angle_par)
+        O.integrate(pos, vel, fprev, f + fl + fx + fb, m, DT_NS, 0)
+        if k > 0:                      # first step is warm-up
+            times.append(time.perf_counter() - t0)
+    return statistics.median(times)
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from lima_b200 import systems
+    s = systems.config2()
+    threads = os.cpu_count() or 1
+    n = max(1, min(args.steps, 3))
+    t = cpu_step_time(s, n, threads)
+    v = ns_per_day(t)
+    line = {
+        "impl": "reference", "metric": "ns_per_day", "value": v, "unit": "ns/day", "n_gpus": args.gpus,
+        "steps": n, "warmup": 1, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "atoms": s.n, "pme_grid": list(GRID), "cutoff_nm": CUTOFF,
+                   "nstlist": 10, "dt_fs": 1.0, "parallelism": "replicas"},
+        "cpu_baseline": {"value": v, "unit": "ns/day", "cores": threads, "kind": "port",
+                         "sample": f"{n} full MD steps of the {s.n}-atom box on the host (oracle port: FP32 "
+                                   f"pair loop, FP64 SPME 96^3 and bonded terms), median"},
+        "e2e": {"value": v, "unit": "ns/day", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference has no CPU force path; the timed reference is the oracle restatement of its formulas",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_lima(args):
+    import torch
+    from lima_b200 import Engine, systems
+    from lima_b200 import engine as E
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    s = systems.config2()
+    eng = Engine(cutoff=CUTOFF, electrostatics=E.ES_EWALD, ewald_tol=1e-5, nstlist=10, dt=DT_NS, device=local)
+    eng.load(s, pme_grid=GRID)
+    eng.step(max(args.warmup, 3))
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+    sampler = ClockSampler(local)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-timed steps, L2 flushed before each step
+    barrier()
+    sampler.start()
+    eng.reset_timings()
+    t_wall0 = time.perf_counter()
+    dev_ms = 0.0
+    launches = 0
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        torch.cuda.synchronize()
+        eng.step(1)
+        t = eng.timings()
+        dev_ms += t["step"] * t["steps"] / 1000.0
+        launches += t["kernel_launches"]
+        eng.reset_timings()
+    t_wall = time.perf_counter() - t_wall0
+    barrier()
+    clocks = sampler.stop()
+    step_s = dev_ms / 1000.0 / args.steps
+    if dist is not None:
+        tt = torch.tensor([step_s], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        step_s = float(tt.item())
+    value = world * ns_per_day(step_s)
+
+    # ---- per-phase device times (events on each phase's own stream) for the roofline
+    n_phase = min(args.steps, 100)
+    eng.phase_timing(True)
+    eng.reset_timings()
+    for k in range(n_phase):
+        flush.fill_(float(k))
+        torch.cuda.synchronize()
+        eng.step(1)
+    ph = eng.timings()
+    # phase timings accumulate per step call; step() resets nothing, so average over n_phase
+    eng.phase_timing(False)
+    pairs = len(eng.pairlist())
+    nb_s = ph["nonbonded"] * ph["steps"] / n_phase / 1e6 if n_phase else float("nan")
+    peaks = load_peaks()
+    sm_max = float(peaks.get("sm_max_mhz", 1965.0))
+    fp32_peak = 148 * 128 * 2 * sm_max * 1e6 / 1e12      # TFLOP/s, FMA = 2
+    achieved = pairs * FLOPS_PER_PAIR / nb_s / 1e12 if nb_s > 0 else None
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "nonbonded_water100k.json")
+    if os.path.exists(prof):
+        try:
+            traffic = json.load(open(prof)).get("dram_bytes_per_launch")
+        except Exception:
+            traffic = None
+
+    # ---- end to end through the C-ABI with host buffers: set_state -> step -> get_state
+    n_e2e = min(args.steps, 50)
+    pos_h = torch.from_numpy(s.pos.copy()).pin_memory().numpy()
+    vel_h = torch.from_numpy(s.vel.copy()).pin_memory().numpy()
+    p_cur, v_cur = eng.state()
+    np.copyto(pos_h, p_cur)
+    np.copyto(vel_h, v_cur)
+    barrier()
+    t0 = time.perf_counter()
+    for k in range(n_e2e):
+        eng.set_state(pos_h, vel_h)
+        eng.step(1)
+        p_cur, v_cur = eng.state()
+        en = eng.energies()
+        np.copyto(pos_h, p_cur)
+        np.copyto(vel_h, v_cur)
+    barrier()
+    e2e_s = (time.perf_counter() - t0) / n_e2e
+    if dist is not None:
+        tt = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    h2d = s.n * (3 * 8 + 3 * 4)
+    d2h = s.n * (3 * 8 + 3 * 4) + 15 * 8
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        n_cpu = 2
+        t_cpu = cpu_step_time(s, n_cpu, threads)
+        cpu = {"value": ns_per_day(t_cpu), "unit": "ns/day", "cores": threads, "kind": "port",
+               "sample": f"{n_cpu} full MD steps of the same {s.n}-atom box on the host (oracle port: FP32 pair "
+                         f"loop with {threads} threads, FP64 SPME 96^3 and bonded terms), median"}
+
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": "ns_per_day", "value": value, "unit": "ns/day", "n_gpus": world, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": step_s * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "atoms": s.n, "pme_grid": list(GRID), "cutoff_nm": CUTOFF, "nstlist": 10,
+                   "dt_fs": 1.0, "integrator": "leapfrog", "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "flushed before every timed step (256 MiB write)",
+                   "accumulation": "int64 fixed point forces/energies, FP64 positions"},
+        "pairs_per_s": world * pairs / step_s,
+        "pairs_per_step": pairs,
+        "wall_ms_per_step": t_wall / args.steps * 1e3,
+        "phase_us": {k: ph[k] for k in ("nonbonded", "bonded", "pme", "integrate", "nblist")},
+        "roofline": {"kernel": "k_nonbonded (pair kernel)", "bound": "fp32", "achieved": achieved,
+                     "peak": fp32_peak, "unit": "TFLOP/s",
+                     "frac": achieved / fp32_peak if achieved else None, "traffic": traffic,
+                     "peak_source": "nominal FP32 FMA rate at the measured max SM clock (148 SM x 128 lanes x 2 x "
+                                    f"{sm_max:.0f} MHz); MEASURED_PEAKS.json holds no FP32 figure",
+                     "work": f"{FLOPS_PER_PAIR} flops per in-cutoff pair x {pairs} pairs per launch"},
+        "e2e": {"value": world * ns_per_day(e2e_s), "unit": "ns/day", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h,
+                "path": "lima_set_state(host) -> lima_step(1) -> lima_get_state(host) + lima_get_energies"},
+        "gpu_launches": launches,
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="lima", choices=["lima", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_lima(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,210 @@
+/*
+ * lima_b200.h — C-ABI of the B200-native force and integration path.
+ *
+ * This boundary replaces the per-step path of LIMA_ENGINE's `class Engine`
+ * (code/LIMA_ENGINE/include/Engine.cuh:78-170) together with the parts of
+ * `Simulation` / `Box` / `SimParams` it consumes
+ * (code/LIMA_BASE/include/Simulation.cuh:17-205).  The lifecycle mirrors the
+ * reference:
+ *
+ *   reference                                         this library
+ *   ------------------------------------------------  -----------------------------------
+ *   Engine::Engine(unique_ptr<Simulation>, bc, log)    lima_create / lima_create_batch
+ *     (code/LIMA_ENGINE/src/Engine.cu:19-81)             + lima_set_box / lima_set_atoms /
+ *   BoxBuilder::BuildBox, buildMolecules                  lima_set_bonds ... / lima_set_state
+ *     (code/LIMA_MD/src/Environment.cpp:52-67)
+ *   SimParams (Simulation.cuh:17-46)                   lima_params
+ *   Engine::step()            (Engine.cu:148-159)      lima_step(h, 1)
+ *   Environment::run loop     (Environment.cpp:182-230) lima_step(h, n_steps)
+ *   em_variant=true run       (Programs.cpp:155-200)   lima_minimize
+ *   Engine::takeBackSim()     (EngineHostside.h:10-14) lima_get_state / lima_get_forces
+ *   Engine::~Engine           (Engine.cu:83-101)       lima_destroy
+ *   SimSignals::critical_error_encountered             lima_get_status (device status word)
+ *     (Simulation.cuh:48-50)
+ *   runtime_error from genericErrorCheck               every call returns a LIMA_ERR_* code;
+ *     (code/LIMA_BASE/include/Utilities.h:22-51)         lima_last_error gives the message
+ *
+ * Units are the reference's own (code/LIMA_BASE/include/Constants.h:43-60):
+ * length nm, time ns, mass kg/mol, charge kC/mol (e x 96.485), energy J/mol,
+ * force J/mol/nm.  LJ sigma in nm, epsilon in J/mol; bond k in J/mol/nm^2;
+ * angle k in J/mol/rad^2; dihedral k_phi in J/mol (used as given: the
+ * reference halves the file value at load, code/LIMA_BASE/src/Bodies.cpp:36-38,
+ * and a caller passing reference-loaded parameters passes the halved value).
+ *
+ * Ownership: every array argument is caller-owned host memory that is copied
+ * during the call; nothing retains caller pointers.  Calls on one handle are
+ * not thread-safe; distinct handles are independent.
+ */
+#ifndef LIMA_B200_H
+#define LIMA_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define LIMA_API __attribute__((visibility("default")))
+#else
+#define LIMA_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- errors */
+#define LIMA_OK                 0
+#define LIMA_ERR_INVALID_ARG    1  /* bad pointer, size or parameter              */
+#define LIMA_ERR_CUDA           2  /* a CUDA runtime call failed                   */
+#define LIMA_ERR_STATE          3  /* call made in the wrong lifecycle state       */
+#define LIMA_ERR_OVERFLOW       4  /* a fixed-capacity device list overflowed      */
+#define LIMA_ERR_TIMEOUT        5  /* a bounded device wait gave up                */
+#define LIMA_ERR_NO_DEVICE      6  /* no CUDA device / wrong architecture          */
+#define LIMA_ERR_NOT_FINITE     7  /* NaN or Inf met in positions or forces        */
+#define LIMA_ERR_UNSUPPORTED    8  /* option not available in this build           */
+
+/* device status word bits (lima_get_status); mirrors SimSignals plus the
+ * overflow checks of Neighborlists.cuh:184-186,214-217,274-276 */
+#define LIMA_STATUS_PAIRLIST_OVERFLOW  0x1u
+#define LIMA_STATUS_COLUMN_OVERFLOW    0x2u
+#define LIMA_STATUS_NONFINITE          0x4u
+#define LIMA_STATUS_FORCE_SATURATED    0x8u
+#define LIMA_STATUS_MOVED_TOO_FAR      0x10u
+#define LIMA_STATUS_MLP_FALLBACK       0x20u
+
+/* ---------------------------------------------------------------- options */
+#define LIMA_ES_NONE    0  /* no electrostatics                               */
+#define LIMA_ES_CUTOFF  1  /* plain 1/r Coulomb truncated at the cutoff         */
+#define LIMA_ES_EWALD   2  /* erfc real space (+ PME when a PME grid is given)  */
+
+#define LIMA_INTEGRATOR_LEAPFROG 0
+#define LIMA_INTEGRATOR_VV       1  /* the reference's velocity-Verlet ("VVS")
+                                       code/LIMA_ENGINE/src/EngineUtils.cuh:31-41 */
+
+#define LIMA_CALC_FORCES   0x0
+#define LIMA_CALC_ENERGY   0x1
+
+typedef struct lima_params {
+    int    device;            /* CUDA device ordinal                                 */
+    double dt;                /* [ns]  (reference SimParams::dt)                      */
+    double cutoff;            /* [nm]  (SimParams::cutoff_nm)                         */
+    double skin;              /* [nm]  Verlet buffer of the cluster pair list; <0: auto */
+    int    nstlist;           /* steps between pair-list rebuilds                     */
+    int    electrostatics;    /* LIMA_ES_*                                            */
+    int    pme_grid[3];       /* default PME grid for every system; 0 = none          */
+    double pme_spacing;       /* [nm] if >0 and pme_grid is 0, grid from spacing      */
+    double ewald_kappa;       /* [1/nm]; 0 = derive (ewald_tol, or 3/rc in ref_compat) */
+    double ewald_tol;         /* erfc(kappa*rc) target when kappa is derived          */
+    int    ref_compat;        /* 1 = the reference's reciprocal-space conventions:
+                                 kappa = 3/rc (PhysicsUtils.cuh:60-62), influence
+                                 function x sinc^8 (PME.cuh:434-495), central-difference
+                                 gather (PME.cuh:384-407), no exclusion correction,
+                                 self energy added per charged atom (PME.cuh:417-420) */
+    int    integrator;        /* LIMA_INTEGRATOR_*                                    */
+    double thermostat_scalar; /* velocity scale applied each step (1 = NVE)           */
+    int    exclude_bonded;    /* 1 = every atom pair sharing a bond, angle, dihedral
+                                 or improper is excluded from LJ and Coulomb
+                                 (code/LIMA_TOOLS/src/CompoundBuilder.cpp:40-60)      */
+    int    use_graphs;        /* 1 = replay each nstlist block of steps as a CUDA graph */
+} lima_params;
+
+typedef struct lima_energies {
+    double lj;                /* short-range Lennard-Jones                 [J/mol] */
+    double coulomb_real;      /* cutoff or erfc real-space Coulomb         [J/mol] */
+    double pme_recip;         /* reciprocal-space energy                   [J/mol] */
+    double pme_self;          /* Ewald self term                           [J/mol] */
+    double pme_excl;          /* reciprocal exclusion correction           [J/mol] */
+    double bond, angle, dihedral, improper, pairbond;             /*        [J/mol] */
+    double kinetic;           /*                                           [J/mol] */
+    double potential;         /* sum of the potential terms                [J/mol] */
+    double total;             /* potential + kinetic                       [J/mol] */
+    double virial;            /* -1/2 sum r_ij . f_ij (short-range + bonded) [J/mol] */
+    double temperature;       /* [K], dof = 3N - 3                                  */
+    int64_t step;
+} lima_energies;
+
+typedef struct lima_timings {   /* averages over the steps since the last reset [us] */
+    double nblist;            /* pair-list rebuild, per rebuild                        */
+    double nonbonded, bonded, pme, integrate;  /* per step; 0 unless phase timing is on */
+    double step;              /* whole step, device time on the main stream            */
+    int64_t steps;
+    int64_t rebuilds;
+    int64_t kernel_launches;  /* kernels of this library launched since the reset     */
+} lima_timings;
+
+typedef struct lima_engine lima_engine;
+
+/* --------------------------------------------------------------- lifecycle */
+LIMA_API void        lima_default_params(lima_params* p);
+LIMA_API const char* lima_error_string(int code);
+LIMA_API const char* lima_last_error(const lima_engine* h);
+LIMA_API int         lima_version(void);
+
+/* Engine::Engine (Engine.cu:19-81) for one system. */
+LIMA_API int lima_create(const lima_params* p, lima_engine** out);
+/* Many independent systems stepped together by the same launches. */
+LIMA_API int lima_create_batch(const lima_params* p, int n_systems, lima_engine** out);
+/* Engine::~Engine (Engine.cu:83-101). */
+LIMA_API int lima_destroy(lima_engine* h);
+/* Selects the system that the following set/get calls address (default 0). */
+LIMA_API int lima_select_system(lima_engine* h, int system);
+LIMA_API int lima_num_systems(const lima_engine* h, int* n);
+
+/* ------------------------------------------------------ box and topology
+ * BoxParams::boxSize (Simulation.cuh:55) is an integer cube in the reference;
+ * here the box is rectangular with real edge lengths. */
+LIMA_API int lima_set_box(lima_engine* h, double lx, double ly, double lz);
+/* Per-atom charge [kC/mol], mass [kg/mol], LJ sigma [nm], epsilon [J/mol].
+ * Mixing is Lorentz-Berthelot: sigma_ij=(s_i+s_j)/2, eps_ij=sqrt(e_i e_j)
+ * (code/LIMA_ENGINE/src/LennardJonesInteractions.cuh:14-27,186-188). */
+LIMA_API int lima_set_atoms(lima_engine* h, int n_atoms, const float* charge, const float* mass,
+                   const float* sigma, const float* epsilon);
+/* SingleBond (Bodies.cuh), params per bond: b0 [nm], kb [J/mol/nm^2]. */
+LIMA_API int lima_set_bonds(lima_engine* h, int n, const int32_t* atoms2, const float* params2);
+/* AngleUreyBradleyBond, params: theta0 [rad], ktheta, ub0 [nm], kub. */
+LIMA_API int lima_set_angles(lima_engine* h, int n, const int32_t* atoms3, const float* params4);
+/* DihedralBond, params: phi0 [rad], k_phi [J/mol], multiplicity n. */
+LIMA_API int lima_set_dihedrals(lima_engine* h, int n, const int32_t* atoms4, const float* params3);
+/* ImproperDihedralBond, params: psi0 [rad], k_psi [J/mol/rad^2]. */
+LIMA_API int lima_set_impropers(lima_engine* h, int n, const int32_t* atoms4, const float* params2);
+/* PairBond (LJ 1-4 style), params: sigma [nm], epsilon [J/mol]. */
+LIMA_API int lima_set_pairbonds(lima_engine* h, int n, const int32_t* atoms2, const float* params2);
+/* Extra excluded pairs on top of the bonded-term rule. */
+LIMA_API int lima_set_exclusions(lima_engine* h, int n, const int32_t* atoms2);
+/* Per-system PME grid; overrides lima_params.pme_grid / pme_spacing. */
+LIMA_API int lima_set_pme_grid(lima_engine* h, int nx, int ny, int nz);
+
+/* -------------------------------------------------------------------- state
+ * pos [nm] x 3N (double), vel [nm/ns] x 3N (NULL = zero). */
+LIMA_API int lima_set_state(lima_engine* h, const double* pos, const float* vel);
+LIMA_API int lima_get_state(lima_engine* h, double* pos, float* vel);
+
+/* ---------------------------------------------------------------- stepping */
+/* Forces at the current positions, no integration. flags: LIMA_CALC_*. */
+LIMA_API int lima_compute_forces(lima_engine* h, int flags);
+/* n_steps of Engine::step() (Engine.cu:148-159). Energies are evaluated on the
+ * last step. */
+LIMA_API int lima_step(lima_engine* h, int n_steps);
+/* Energy minimisation: the reference's em_variant path (tanh force clamp +
+ * ADAM, code/LIMA_ENGINE/src/EngineUtils.cuh:44-140, early stop on max |F|,
+ * Engine.cu:275-291). force_tol in J/mol/nm. */
+LIMA_API int lima_minimize(lima_engine* h, double force_tol, int max_steps, int* steps_taken,
+                  double* max_force);
+
+/* ---------------------------------------------------------------- readback */
+LIMA_API int lima_get_forces(lima_engine* h, double* forces);          /* [J/mol/nm] x 3N */
+LIMA_API int lima_get_energies(lima_engine* h, lima_energies* e);
+/* Ordered atom pairs (i<j, original indices) within the cutoff that the
+ * pair kernel evaluates at the current positions.  Writes up to cap pairs
+ * into pairs[2*cap] and the total count into *n. */
+LIMA_API int lima_get_pairlist(lima_engine* h, int64_t cap, int32_t* pairs, int64_t* n);
+LIMA_API int lima_get_status(lima_engine* h, uint32_t* status);
+LIMA_API int lima_clear_status(lima_engine* h);
+LIMA_API int lima_get_timings(lima_engine* h, lima_timings* t);
+LIMA_API int lima_reset_timings(lima_engine* h);
+/* Times each phase with CUDA events on the stream it runs on (adds one device
+ * synchronisation per step while on). */
+LIMA_API int lima_enable_phase_timing(lima_engine* h, int enable);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LIMA_B200_H */

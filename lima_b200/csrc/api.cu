@@ -1,0 +1,1131 @@
+// api.cu — the C-ABI (include/lima_b200.h) over the B200 force/integration path.
+//
+// Host-side equivalent of LIMA_ENGINE's Engine (code/LIMA_ENGINE/src/Engine.cu):
+// construction uploads the system and builds the first pair list (Engine.cu:19-81),
+// lima_step runs the per-step pipeline (_deviceMaster, Engine.cu:297-381, and the
+// list rebuild of hostMaster, :161-190), readback replaces takeBackSim and the
+// logging buffers.  Every entry point returns a LIMA_ERR_* code instead of
+// throwing (code/LIMA_BASE/include/Utilities.h:22-51).
+//
+// Per step, on three streams joined by events:
+//   main   : zero forces -> pair kernel ---------------------> integrate
+//   bonded :        bonded terms + Ewald exclusion correction --^
+//   pme    :        spread -> 5 FFT passes -> gather -----------^
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+#include "lima_b200.h"
+
+namespace {
+
+using namespace lima;
+
+constexpr double kCoulomb = 8.9875517873681764e9 / 1e-9 / 6.02214076e23 * 1000.0 * 1000.0;
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kPiRef = 3.14159;  // code/LIMA_BASE/include/Constants.h:51
+
+struct SystemHost {
+    double box[3] = {0.0, 0.0, 0.0};
+    int n = 0;
+    std::vector<float> q, m, sig, eps;
+    std::vector<int32_t> bonds, angles, dihedrals, impropers, pairbonds, excl;
+    std::vector<float> bpar, apar, dpar, ipar, ppar;
+    int pme[3] = {0, 0, 0};
+    bool pme_set = false;
+    std::vector<double> pos;
+    std::vector<float> vel;
+};
+
+struct CudaError {
+    cudaError_t e;
+    const char* what;
+};
+
+#define CK(x)                                            \
+    do {                                                 \
+        cudaError_t err__ = (x);                         \
+        if (err__ != cudaSuccess) throw CudaError{err__, #x}; \
+    } while (0)
+
+struct ApiError {
+    int code;
+    std::string msg;
+};
+
+}  // namespace
+
+struct lima_engine {
+    lima_params p{};
+    std::vector<SystemHost> sys;
+    int cur = 0;
+    std::string err;
+    bool built = false;
+    bool state_pending = false;
+    int list_age = 1 << 30;
+    int64_t step = 0;
+
+    // derived
+    double kappa = 0.0;
+    double rlist = 0.0;
+    bool pme_on = false;
+    std::vector<double> self_energy;  // per system
+    std::vector<int> n_atoms_off;
+
+    DevState st{};
+    BondedTerms bt{};
+    PmePlan pp{};
+    NbParams nb{};
+    IntegrateParams ip{};
+    std::vector<void*> allocs;
+    cudaStream_t s_main = nullptr, s_bonded = nullptr, s_pme = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_bonded = nullptr, ev_pme = nullptr;
+    cudaEvent_t ev_t0 = nullptr, ev_t1 = nullptr;
+    // phase timing: [rebuild, nonbonded, bonded, pme, integrate] x (start, stop)
+    bool phase_timing = false;
+    cudaEvent_t ev_ph[5][2] = {};
+    double phase_ms[5] = {0, 0, 0, 0, 0};
+    int phase_used[5] = {0, 0, 0, 0, 0};
+    int64_t launches = 0;
+    int64_t rebuilds = 0;
+
+    // host mirrors
+    std::vector<long long> energy_host;
+    bool energy_valid = false;
+    double time_ms = 0.0;
+    int64_t timed_steps = 0;
+
+    // device scratch for readback
+    double* d_out_d = nullptr;
+    float* d_out_f = nullptr;
+    float* d_maxf = nullptr;
+
+    ~lima_engine() { release(); }
+
+    template <typename T>
+    T* dalloc(size_t n) {
+        void* p_ = nullptr;
+        if (n == 0) n = 1;
+        CK(cudaMalloc(&p_, n * sizeof(T)));
+        CK(cudaMemset(p_, 0, n * sizeof(T)));
+        allocs.push_back(p_);
+        return reinterpret_cast<T*>(p_);
+    }
+    template <typename T>
+    T* upload(const std::vector<T>& v) {
+        T* d = dalloc<T>(v.size());
+        if (!v.empty()) CK(cudaMemcpy(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+        return d;
+    }
+    void release() {
+        if (s_main) cudaStreamSynchronize(s_main);
+        for (void* a : allocs) cudaFree(a);
+        allocs.clear();
+        for (cudaStream_t* s : {&s_main, &s_bonded, &s_pme})
+            if (*s) cudaStreamDestroy(*s), *s = nullptr;
+        for (cudaEvent_t* e : {&ev_fork, &ev_bonded, &ev_pme, &ev_t0, &ev_t1})
+            if (*e) cudaEventDestroy(*e), *e = nullptr;
+        for (auto& pr : ev_ph)
+            for (cudaEvent_t& e : pr)
+                if (e) cudaEventDestroy(e), e = nullptr;
+        built = false;
+    }
+
+    void setup();
+    void mark(int phase, int which, cudaStream_t s) {
+        if (!phase_timing) return;
+        CK(cudaEventRecord(ev_ph[phase][which], s));
+        if (which == 1) phase_used[phase] = 1;
+    }
+    void collect_phases() {
+        if (!phase_timing) return;
+        CK(cudaDeviceSynchronize());
+        for (int k = 0; k < 5; ++k) {
+            if (!phase_used[k]) continue;
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, ev_ph[k][0], ev_ph[k][1]));
+            phase_ms[k] += ms;
+            phase_used[k] = 0;
+        }
+    }
+    void rebuild(bool from_input);
+    void forces(bool energy);
+    void run_steps(int n);
+    void read_energies(lima_energies* e);
+};
+
+namespace {
+
+int fail(lima_engine* h, int code, const std::string& msg) {
+    if (h) h->err = msg;
+    return code;
+}
+
+template <typename F>
+int guarded(lima_engine* h, F&& fn) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    try {
+        return fn();
+    } catch (const CudaError& e) {
+        h->err = std::string("CUDA error in ") + e.what + ": " + cudaGetErrorString(e.e);
+        return LIMA_ERR_CUDA;
+    } catch (const ApiError& e) {
+        h->err = e.msg;
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        h->err = "host allocation failed";
+        return LIMA_ERR_INVALID_ARG;
+    }
+}
+
+double kappa_from_tol(double rc, double tol) {
+    double lo = 0.0, hi = 20.0 / rc;
+    for (int i = 0; i < 200; ++i) {
+        const double mid = 0.5 * (lo + hi);
+        if (std::erfc(mid * rc) > tol) lo = mid;
+        else hi = mid;
+    }
+    return 0.5 * (lo + hi);
+}
+
+int fft_friendly(int n) {
+    int m = std::max(n, 4);
+    for (;; ++m) {
+        int k = m;
+        for (int p : {2, 3, 5})
+            while (k % p == 0) k /= p;
+        if (k == 1) return m;
+    }
+}
+
+struct UnionFind {
+    std::vector<int> p;
+    explicit UnionFind(int n) : p(n) { std::iota(p.begin(), p.end(), 0); }
+    int find(int x) {
+        while (p[x] != x) x = p[x] = p[p[x]];
+        return x;
+    }
+    void unite(int a, int b) {
+        a = find(a);
+        b = find(b);
+        if (a != b) p[std::max(a, b)] = std::min(a, b);
+    }
+};
+
+}  // namespace
+
+void lima_engine::setup() {
+    if (sys.empty()) throw ApiError{LIMA_ERR_STATE, "no systems"};
+    int dev_count = 0;
+    if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0)
+        throw ApiError{LIMA_ERR_NO_DEVICE, "no CUDA device available"};
+    CK(cudaSetDevice(p.device));
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, p.device));
+    if (prop.major < 10) throw ApiError{LIMA_ERR_NO_DEVICE, "this build targets sm_100a (B200)"};
+    release();
+
+    // ---- derived parameters
+    const double rc = p.cutoff;
+    if (!(rc > 0.0)) throw ApiError{LIMA_ERR_INVALID_ARG, "cutoff must be > 0"};
+    const double skin = p.skin < 0.0 ? 0.1 : p.skin;
+    rlist = rc + skin;
+    if (p.nstlist < 1) throw ApiError{LIMA_ERR_INVALID_ARG, "nstlist must be >= 1"};
+    if (p.electrostatics == LIMA_ES_EWALD) {
+        if (p.ewald_kappa > 0.0) kappa = p.ewald_kappa;
+        else if (p.ref_compat) kappa = 3.0 / rc;  // PhysicsUtils.cuh:60-62
+        else kappa = kappa_from_tol(rc, p.ewald_tol > 0.0 ? p.ewald_tol : 1e-5);
+    } else {
+        kappa = 0.0;
+    }
+
+    const int ns = (int)sys.size();
+    n_atoms_off.assign(ns + 1, 0);
+    for (int s = 0; s < ns; ++s) {
+        const SystemHost& S = sys[s];
+        if (S.n <= 0) throw ApiError{LIMA_ERR_STATE, "system " + std::to_string(s) + " has no atoms"};
+        for (int d = 0; d < 3; ++d)
+            if (!(S.box[d] > 2.0 * rlist))
+                throw ApiError{LIMA_ERR_INVALID_ARG, "box edge must exceed 2*(cutoff+skin) in system " + std::to_string(s)};
+        if (S.pos.size() != (size_t)3 * S.n) throw ApiError{LIMA_ERR_STATE, "positions not set"};
+        n_atoms_off[s + 1] = n_atoms_off[s] + S.n;
+    }
+    const int N = n_atoms_off[ns];
+
+    // ---- per-system layout
+    std::vector<SysDesc> sd(ns);
+    std::vector<int> cluster_sys, col_sys;
+    int col_off = 0, cl_off = 0, pme_off = 0, pme_coff = 0;
+    int col_cap = 64;
+    double max_density = 0.0;
+    pme_on = false;
+    int max_n = 0;
+    self_energy.assign(ns, 0.0);
+    for (int s = 0; s < ns; ++s) {
+        const SystemHost& S = sys[s];
+        SysDesc& D = sd[s];
+        std::memset(&D, 0, sizeof(D));
+        const double V = S.box[0] * S.box[1] * S.box[2];
+        const double rho = S.n / V;
+        max_density = std::max(max_density, rho);
+        const double a = std::cbrt(CLUSTER / rho);
+        for (int d = 0; d < 3; ++d) {
+            D.box[d] = S.box[d];
+            D.boxf[d] = (float)S.box[d];
+            D.inv_boxf[d] = (float)(1.0 / S.box[d]);
+        }
+        D.ncol_x = std::max(1, (int)std::floor(S.box[0] / a));
+        D.ncol_y = std::max(1, (int)std::floor(S.box[1] / a));
+        D.col_w[0] = (float)(S.box[0] / D.ncol_x);
+        D.col_w[1] = (float)(S.box[1] / D.ncol_y);
+        D.col_off = col_off;
+        const int ncols = D.ncol_x * D.ncol_y;
+        const double per_col = (double)S.n / ncols;
+        col_cap = std::max(col_cap, (int)std::ceil(3.0 * per_col + 64.0));
+        D.atom_off = n_atoms_off[s];
+        D.n_atoms = S.n;
+        D.max_clusters = (S.n + CLUSTER - 1) / CLUSTER + ncols;
+        D.cluster_cap_off = cl_off;
+        for (int c = 0; c < D.max_clusters; ++c) cluster_sys.push_back(s);
+        for (int c = 0; c < ncols; ++c) col_sys.push_back(s);
+        col_off += ncols;
+        cl_off += D.max_clusters;
+        // PME grid
+        int g[3] = {0, 0, 0};
+        if (p.electrostatics == LIMA_ES_EWALD) {
+            if (S.pme_set) {
+                for (int d = 0; d < 3; ++d) g[d] = S.pme[d];
+            } else if (p.pme_grid[0] > 0) {
+                for (int d = 0; d < 3; ++d) g[d] = p.pme_grid[d];
+            } else if (p.pme_spacing > 0.0) {
+                for (int d = 0; d < 3; ++d) g[d] = fft_friendly((int)std::ceil(S.box[d] / p.pme_spacing));
+            }
+        }
+        if (g[0] > 0) {
+            pme_on = true;
+            for (int d = 0; d < 3; ++d) {
+                if (g[d] < 8) throw ApiError{LIMA_ERR_INVALID_ARG, "PME grid dimension must be >= 8"};
+                D.pme_n[d] = g[d];
+                D.pme_inv_h[d] = (float)(g[d] / S.box[d]);
+                max_n = std::max(max_n, g[d]);
+            }
+            D.pme_off = pme_off;
+            D.pme_coff = pme_coff;
+            pme_off += g[0] * g[1] * g[2];
+            pme_coff += (g[0] / 2 + 1) * g[1] * g[2];
+            double q2 = 0.0;
+            int nq = 0;
+            for (int i = 0; i < S.n; ++i) {
+                q2 += (double)S.q[i] * S.q[i];
+                nq += S.q[i] != 0.f;
+            }
+            const double pic = p.ref_compat ? kPiRef : kPi;
+            const double self_total = -kappa / std::sqrt(pic) * q2 * kCoulomb;
+            // reference quirk: the total self term is added to every charged
+            // atom's potential and halved (PME.cuh:417-420, 610-622)
+            self_energy[s] = p.ref_compat ? 0.5 * nq * self_total : self_total;
+            D.self_energy = self_energy[s];
+            D.n_charged = nq;
+        }
+    }
+    if (col_cap > 8192) throw ApiError{LIMA_ERR_UNSUPPORTED, "column capacity too large (very tall box)"};
+    const int n_clusters = cl_off;
+
+    // ---- per-atom static data (original order), exclusions and molecules
+    std::vector<int> atom_sys(N);
+    std::vector<float> q(N), inv_mass(N);
+    std::vector<float2> ljp(N);
+    std::vector<std::vector<int>> ex(N);
+    UnionFind uf(N);
+    BondedTerms H;
+    std::vector<int2> bidx, pidx, xidx;
+    std::vector<float2> bpar, ipar, ppar;
+    std::vector<int4> aidx, didx, iidx;
+    std::vector<float4> apar, dpar;
+    auto check_idx = [&](const SystemHost& S, int a) {
+        if (a < 0 || a >= S.n) throw ApiError{LIMA_ERR_INVALID_ARG, "bonded term atom index out of range"};
+    };
+    auto exclude_all = [&](const int* t, int k, int off) {
+        for (int x = 0; x < k; ++x)
+            for (int y = x + 1; y < k; ++y) {
+                const int a = t[x] + off, b = t[y] + off;
+                if (a == b) continue;
+                ex[a].push_back(b);
+                ex[b].push_back(a);
+            }
+    };
+    for (int s = 0; s < ns; ++s) {
+        const SystemHost& S = sys[s];
+        const int off = n_atoms_off[s];
+        for (int i = 0; i < S.n; ++i) {
+            atom_sys[off + i] = s;
+            q[off + i] = S.q[i];
+            if (!(S.m[i] > 0.f)) throw ApiError{LIMA_ERR_INVALID_ARG, "atom masses must be > 0"};
+            inv_mass[off + i] = 1.f / S.m[i];
+            ljp[off + i] = make_float2(0.5f * S.sig[i], std::sqrt(std::max(S.eps[i], 0.f)));
+        }
+        const bool ex_b = p.exclude_bonded != 0;
+        for (size_t t = 0; t < S.bonds.size() / 2; ++t) {
+            const int* a = &S.bonds[2 * t];
+            check_idx(S, a[0]), check_idx(S, a[1]);
+            bidx.push_back(make_int2(a[0] + off, a[1] + off));
+            bpar.push_back(make_float2(S.bpar[2 * t], S.bpar[2 * t + 1]));
+            uf.unite(a[0] + off, a[1] + off);
+            if (ex_b) exclude_all(a, 2, off);
+        }
+        for (size_t t = 0; t < S.angles.size() / 3; ++t) {
+            const int* a = &S.angles[3 * t];
+            for (int k = 0; k < 3; ++k) check_idx(S, a[k]);
+            aidx.push_back(make_int4(a[0] + off, a[1] + off, a[2] + off, 0));
+            apar.push_back(make_float4(S.apar[4 * t], S.apar[4 * t + 1], S.apar[4 * t + 2], S.apar[4 * t + 3]));
+            uf.unite(a[0] + off, a[1] + off);
+            uf.unite(a[1] + off, a[2] + off);
+            if (ex_b) exclude_all(a, 3, off);
+        }
+        for (size_t t = 0; t < S.dihedrals.size() / 4; ++t) {
+            const int* a = &S.dihedrals[4 * t];
+            for (int k = 0; k < 4; ++k) check_idx(S, a[k]);
+            didx.push_back(make_int4(a[0] + off, a[1] + off, a[2] + off, a[3] + off));
+            dpar.push_back(make_float4(S.dpar[3 * t], S.dpar[3 * t + 1], S.dpar[3 * t + 2], 0.f));
+            for (int k = 0; k < 3; ++k) uf.unite(a[k] + off, a[k + 1] + off);
+            if (ex_b) exclude_all(a, 4, off);
+        }
+        for (size_t t = 0; t < S.impropers.size() / 4; ++t) {
+            const int* a = &S.impropers[4 * t];
+            for (int k = 0; k < 4; ++k) check_idx(S, a[k]);
+            iidx.push_back(make_int4(a[0] + off, a[1] + off, a[2] + off, a[3] + off));
+            ipar.push_back(make_float2(S.ipar[2 * t], S.ipar[2 * t + 1]));
+            for (int k = 0; k < 3; ++k) uf.unite(a[k] + off, a[k + 1] + off);
+            if (ex_b) exclude_all(a, 4, off);
+        }
+        for (size_t t = 0; t < S.pairbonds.size() / 2; ++t) {
+            const int* a = &S.pairbonds[2 * t];
+            check_idx(S, a[0]), check_idx(S, a[1]);
+            pidx.push_back(make_int2(a[0] + off, a[1] + off));
+            ppar.push_back(make_float2(S.ppar[2 * t], S.ppar[2 * t + 1]));
+        }
+        for (size_t t = 0; t < S.excl.size() / 2; ++t) {
+            const int* a = &S.excl[2 * t];
+            check_idx(S, a[0]), check_idx(S, a[1]);
+            uf.unite(a[0] + off, a[1] + off);
+            exclude_all(a, 2, off);
+        }
+    }
+    std::vector<int> excl_off(N + 1, 0), excl_idx, mol(N);
+    for (int a = 0; a < N; ++a) {
+        auto& v = ex[a];
+        std::sort(v.begin(), v.end());
+        v.erase(std::unique(v.begin(), v.end()), v.end());
+        excl_off[a + 1] = excl_off[a] + (int)v.size();
+        excl_idx.insert(excl_idx.end(), v.begin(), v.end());
+        mol[a] = uf.find(a);
+        if (pme_on && !p.ref_compat)
+            for (int b : v)
+                if (b > a && q[a] != 0.f && q[b] != 0.f) xidx.push_back(make_int2(a, b));
+    }
+
+    // ---- pair-list capacity: full neighbour count of clusters (x1.3 margin)
+    const double a_cl = std::cbrt(CLUSTER / max_density);
+    const double reach = rlist + 1.5 * a_cl;
+    const double est = 4.0 / 3.0 * kPi * reach * reach * reach * max_density / CLUSTER;
+    int pl_cap = (int)std::ceil(1.3 * est) + 32;
+    pl_cap = (pl_cap + 31) / 32 * 32;
+    if (st.pl_cap > pl_cap) pl_cap = st.pl_cap;  // keep a capacity grown earlier
+
+    // ---- device allocation
+    CK(cudaStreamCreateWithFlags(&s_main, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&s_bonded, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&s_pme, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&ev_bonded, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&ev_pme, cudaEventDisableTiming));
+    CK(cudaEventCreate(&ev_t0));
+    CK(cudaEventCreate(&ev_t1));
+    for (auto& pr : ev_ph)
+        for (cudaEvent_t& e : pr) CK(cudaEventCreate(&e));
+
+    DevState D{};
+    D.n_sys = ns;
+    D.n_atoms = N;
+    D.n_clusters = n_clusters;
+    D.n_slots = n_clusters * CLUSTER;
+    D.n_cols = col_off;
+    D.pl_cap = pl_cap;
+    D.col_cap = col_cap;
+    D.sys = upload(sd);
+    D.sys_nclusters = dalloc<int>(ns);
+    D.cluster_sys = upload(cluster_sys);
+    D.col_sys = upload(col_sys);
+    const size_t S = D.n_slots;
+    D.px = dalloc<double>(S);
+    D.py = dalloc<double>(S);
+    D.pz = dalloc<double>(S);
+    D.xyzq = dalloc<float4>(S);
+    D.ljp = dalloc<float2>(S);
+    D.vel = dalloc<float4>(S);
+    D.fprev = dalloc<float4>(S);
+    D.adam_m = dalloc<float4>(S);
+    D.adam_v = dalloc<float4>(S);
+    D.fx = dalloc<long long>(S);
+    D.fy = dalloc<long long>(S);
+    D.fz = dalloc<long long>(S);
+    D.orig = dalloc<int>(S);
+    D.tvel = dalloc<float4>(S);
+    D.tfprev = dalloc<float4>(S);
+    D.tadam_m = dalloc<float4>(S);
+    D.tadam_v = dalloc<float4>(S);
+    D.atom_sys = upload(atom_sys);
+    D.slot_of = dalloc<int>(N);
+    D.q = upload(q);
+    D.inv_mass = upload(inv_mass);
+    D.ljp_atom = upload(ljp);
+    D.mol = upload(mol);
+    D.excl_off = upload(excl_off);
+    D.excl_idx = upload(excl_idx);
+    D.in_pos = dalloc<double>(3 * (size_t)N);
+    D.in_vel = dalloc<float>(3 * (size_t)N);
+    D.col_of_atom = dalloc<int>(N);
+    D.z_of_atom = dalloc<float>(N);
+    D.col_count = dalloc<int>(col_off);
+    D.col_fill = dalloc<int>(col_off);
+    D.col_atom_start = dalloc<int>(col_off);
+    D.col_cl_start = dalloc<int>(col_off);
+    D.col_ncl = dalloc<int>(col_off);
+    D.col_list = dalloc<int>(N);
+    D.new_orig = dalloc<int>(S);
+    D.bb_lo = dalloc<float4>(n_clusters);
+    D.bb_hi = dalloc<float4>(n_clusters);
+    D.pl_count = dalloc<int>(n_clusters);
+    D.pl_j = dalloc<int>((size_t)n_clusters * pl_cap);
+    D.pl_mask = dalloc<unsigned long long>((size_t)n_clusters * pl_cap);
+    D.status = dalloc<unsigned>(1);
+    D.energy = dalloc<long long>((size_t)ns * E_COUNT);
+
+    // ---- PME plan, grids and influence function
+    PmePlan P{};
+    if (pme_on) {
+        D.pme_total_real = pme_off;
+        D.pme_total_cplx = pme_coff;
+        D.pme_grid_fx = dalloc<long long>(pme_off);
+        D.pme_real = dalloc<float>(pme_off);
+        D.pme_cplx = dalloc<float2>(pme_coff);
+        std::vector<float> theta(pme_coff, 0.f);
+        std::vector<char> plans(pme_sys_dev_size() * ns, 0);
+        std::vector<int4> ix, iy, iz;
+        const int XL = 8, TX = 16;
+        for (int s = 0; s < ns; ++s) {
+            const SysDesc& Dd = sd[s];
+            if (Dd.pme_n[0] == 0) {
+                // a system without a grid still needs a valid (unused) plan
+                fill_pme_sys_dev(plans.data() + s * pme_sys_dev_size(), 8, 8, 8);
+                continue;
+            }
+            const int K0 = Dd.pme_n[0], K1 = Dd.pme_n[1], K2 = Dd.pme_n[2], K0h = K0 / 2 + 1;
+            if (!fill_pme_sys_dev(plans.data() + s * pme_sys_dev_size(), K0, K1, K2))
+                throw ApiError{LIMA_ERR_UNSUPPORTED, "PME grid dimensions must factor into 2, 3, 5 and be <= 256"};
+            for (int l = 0; l < K1 * K2; l += XL) ix.push_back(make_int4(s, l, std::min(XL, K1 * K2 - l), 0));
+            for (int z = 0; z < K2; ++z)
+                for (int x0 = 0; x0 < K0h; x0 += TX) iy.push_back(make_int4(s, x0, z, 0));
+            for (int y = 0; y < K1; ++y)
+                for (int x0 = 0; x0 < K0h; x0 += TX) iz.push_back(make_int4(s, x0, y, 0));
+            const double* L = sys[s].box;
+            const double V = L[0] * L[1] * L[2];
+            const double pic = p.ref_compat ? kPiRef : kPi;
+            for (int z = 0; z < K2; ++z)
+                for (int y = 0; y < K1; ++y)
+                    for (int x = 0; x < K0h; ++x) {
+                        const int m[3] = {x, y <= K1 / 2 ? y : y - K1, z <= K2 / 2 ? z : z - K2};
+                        const int K[3] = {K0, K1, K2};
+                        if (m[0] == 0 && m[1] == 0 && m[2] == 0) continue;
+                        double kv[3], k2 = 0.0;
+                        for (int d = 0; d < 3; ++d) {
+                            kv[d] = 2.0 * pic * m[d] / L[d];
+                            k2 += kv[d] * kv[d];
+                        }
+                        double t = kCoulomb * 4.0 * pic / k2 * std::exp(-k2 / (4.0 * kappa * kappa)) / V;
+                        if (p.ref_compat) {
+                            // PrecomputeGreensFunctionKernel (PME.cuh:434-495): x prod sinc^8
+                            double sp = 1.0;
+                            for (int d = 0; d < 3; ++d) {
+                                const double kh = kv[d] * (L[d] / K[d]) * 0.5;
+                                const double sc = std::fabs(kh) < 1e-14 ? 1.0 : std::sin(kh) / kh;
+                                sp *= sc * sc * sc * sc;
+                            }
+                            t *= sp * sp;
+                        } else {
+                            // SPME: divide by the B-spline modulus of the centred order-4 weights
+                            double B = 1.0;
+                            for (int d = 0; d < 3; ++d) {
+                                const double b = 2.0 / 3.0 + std::cos(2.0 * kPi * m[d] / K[d]) / 3.0;
+                                B *= b * b;
+                            }
+                            t /= B;
+                        }
+                        theta[Dd.pme_coff + x + (size_t)K0h * (y + (size_t)K1 * z)] = (float)t;
+                    }
+        }
+        D.pme_theta = upload(theta);
+        char* dplans = dalloc<char>(plans.size());
+        CK(cudaMemcpy(dplans, plans.data(), plans.size(), cudaMemcpyHostToDevice));
+        P.sys_plans = dplans;
+        P.items_x = upload(ix);
+        P.items_y = upload(iy);
+        P.items_z = upload(iz);
+        P.n_items_x = (int)ix.size();
+        P.n_items_y = (int)iy.size();
+        P.n_items_z = (int)iz.size();
+        P.ref_gather = p.ref_compat ? 1 : 0;
+        P.max_n = max_n;
+        pme_set_smem_limits(max_n);
+    }
+    pp = P;
+
+    // ---- bonded terms
+    BondedTerms B{};
+    B.nb = (int)bidx.size();
+    B.na = (int)aidx.size();
+    B.nd = (int)didx.size();
+    B.ni = (int)iidx.size();
+    B.np = (int)pidx.size();
+    B.nx = (int)xidx.size();
+    B.bidx = upload(bidx);
+    B.bpar = upload(bpar);
+    B.aidx = upload(aidx);
+    B.apar = upload(apar);
+    B.didx = upload(didx);
+    B.dpar = upload(dpar);
+    B.iidx = upload(iidx);
+    B.ipar = upload(ipar);
+    B.pidx = upload(pidx);
+    B.ppar = upload(ppar);
+    B.xidx = upload(xidx);
+    bt = B;
+    st = D;
+
+    nb.rc2 = (float)(rc * rc);
+    nb.rlist = (float)rlist;
+    nb.es_mode = p.electrostatics;
+    nb.kappa = (float)kappa;
+    nb.ke = (float)kCoulomb;
+    nb.two_kappa_sqrtpi = (float)(2.0 * kappa / std::sqrt(p.ref_compat ? kPiRef : kPi));
+    nb.em = 0;
+    ip.dt = p.dt;
+    ip.scale = (float)p.thermostat_scalar;
+    ip.integrator = p.integrator;
+
+    d_out_d = dalloc<double>(3 * (size_t)N);
+    d_out_f = dalloc<float>(3 * (size_t)N);
+    d_maxf = dalloc<float>(1);
+    energy_host.assign((size_t)ns * E_COUNT, 0);
+
+    built = true;
+    state_pending = true;
+    energy_valid = false;
+}
+
+void lima_engine::rebuild(bool from_input) {
+    for (int attempt = 0; attempt < 4; ++attempt) {
+        if (from_input) {
+            std::vector<double> pos((size_t)3 * st.n_atoms);
+            std::vector<float> vel((size_t)3 * st.n_atoms, 0.f);
+            for (size_t s = 0; s < sys.size(); ++s) {
+                std::copy(sys[s].pos.begin(), sys[s].pos.end(), pos.begin() + 3 * (size_t)n_atoms_off[s]);
+                if (sys[s].vel.size() == (size_t)3 * sys[s].n)
+                    std::copy(sys[s].vel.begin(), sys[s].vel.end(), vel.begin() + 3 * (size_t)n_atoms_off[s]);
+            }
+            CK(cudaMemcpyAsync(st.in_pos, pos.data(), pos.size() * sizeof(double), cudaMemcpyHostToDevice, s_main));
+            CK(cudaMemcpyAsync(st.in_vel, vel.data(), vel.size() * sizeof(float), cudaMemcpyHostToDevice, s_main));
+        }
+        CK(cudaMemsetAsync(st.status, 0, sizeof(unsigned), s_main));
+        mark(0, 0, s_main);
+        launches += launch_rebuild(st, (float)rlist, from_input, s_main);
+        mark(0, 1, s_main);
+        ++rebuilds;
+        CK(cudaGetLastError());
+        unsigned status = 0;
+        CK(cudaMemcpyAsync(&status, st.status, sizeof(unsigned), cudaMemcpyDeviceToHost, s_main));
+        CK(cudaStreamSynchronize(s_main));
+        if (status & ST_COLUMN_OVERFLOW) throw ApiError{LIMA_ERR_OVERFLOW, "column capacity exceeded (atoms too dense)"};
+        if (!(status & ST_PAIRLIST_OVERFLOW)) {
+            list_age = 0;
+            return;
+        }
+        // grow the pair list and redo the build from the (unchanged) source
+        const int cap = (st.pl_cap * 3 / 2 + 31) / 32 * 32;
+        cudaFree(st.pl_j);
+        cudaFree(st.pl_mask);
+        allocs.erase(std::remove(allocs.begin(), allocs.end(), (void*)st.pl_j), allocs.end());
+        allocs.erase(std::remove(allocs.begin(), allocs.end(), (void*)st.pl_mask), allocs.end());
+        st.pl_cap = cap;
+        st.pl_j = dalloc<int>((size_t)st.n_clusters * cap);
+        st.pl_mask = dalloc<unsigned long long>((size_t)st.n_clusters * cap);
+        // the state is already permuted into slot order: rebuild from the slots
+        from_input = false;
+    }
+    throw ApiError{LIMA_ERR_OVERFLOW, "pair list overflow persists"};
+}
+
+void lima_engine::forces(bool energy) {
+    if (state_pending) {
+        rebuild(true);
+        state_pending = false;
+    } else if (list_age >= p.nstlist) {
+        rebuild(false);
+    }
+    if (energy) CK(cudaMemsetAsync(st.energy, 0, sizeof(long long) * E_COUNT * st.n_sys, s_main));
+    launch_zero_forces(st, s_main);
+    CK(cudaEventRecord(ev_fork, s_main));
+    CK(cudaStreamWaitEvent(s_bonded, ev_fork, 0));
+    CK(cudaStreamWaitEvent(s_pme, ev_fork, 0));
+    mark(2, 0, s_bonded);
+    launches += launch_bonded(st, bt, energy, s_bonded);
+    if (pme_on) launches += launch_exclusion_correction(st, bt, nb, energy, s_bonded);
+    mark(2, 1, s_bonded);
+    CK(cudaEventRecord(ev_bonded, s_bonded));
+    if (pme_on) {
+        mark(3, 0, s_pme);
+        launches += launch_pme(st, pp, energy, s_pme);
+        mark(3, 1, s_pme);
+    }
+    CK(cudaEventRecord(ev_pme, s_pme));
+    mark(1, 0, s_main);
+    launches += launch_nonbonded(st, nb, energy, s_main);
+    mark(1, 1, s_main);
+    CK(cudaStreamWaitEvent(s_main, ev_bonded, 0));
+    CK(cudaStreamWaitEvent(s_main, ev_pme, 0));
+    CK(cudaGetLastError());
+}
+
+void lima_engine::run_steps(int n) {
+    CK(cudaEventRecord(ev_t0, s_main));
+    for (int k = 0; k < n; ++k) {
+        const bool energy = k == n - 1;
+        forces(energy);
+        mark(4, 0, s_main);
+        launches += launch_integrate(st, ip, energy, s_main);
+        mark(4, 1, s_main);
+        collect_phases();
+        ++list_age;
+        ++step;
+    }
+    CK(cudaEventRecord(ev_t1, s_main));
+    CK(cudaMemcpyAsync(energy_host.data(), st.energy, sizeof(long long) * energy_host.size(),
+                       cudaMemcpyDeviceToHost, s_main));
+    CK(cudaStreamSynchronize(s_main));
+    CK(cudaGetLastError());
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ev_t0, ev_t1));
+    time_ms += ms;
+    timed_steps += n;
+    energy_valid = true;
+}
+
+void lima_engine::read_energies(lima_energies* e) {
+    std::memset(e, 0, sizeof(*e));
+    const long long* E = energy_host.data() + (size_t)cur * E_COUNT;
+    auto g = [&](int t) { return (double)E[t] / ENERGY_SCALE; };
+    e->lj = g(E_LJ);
+    e->coulomb_real = g(E_COUL);
+    e->pme_recip = g(E_RECIP);
+    e->pme_self = pme_on ? self_energy[cur] : 0.0;
+    e->pme_excl = g(E_EXCL);
+    e->bond = g(E_BOND);
+    e->angle = g(E_ANGLE);
+    e->dihedral = g(E_DIHEDRAL);
+    e->improper = g(E_IMPROPER);
+    e->pairbond = g(E_PAIRBOND);
+    e->kinetic = g(E_KINETIC);
+    e->virial = g(E_VIRIAL);
+    e->potential = e->lj + e->coulomb_real + e->pme_recip + e->pme_self + e->pme_excl + e->bond + e->angle +
+                   e->dihedral + e->improper + e->pairbond;
+    e->total = e->potential + e->kinetic;
+    const double kb = 1.380649e-23 * 6.02214076e23;
+    const int n = sys[cur].n;
+    e->temperature = n > 1 ? 2.0 * e->kinetic / ((3.0 * n - 3.0) * kb) : 0.0;
+    e->step = step;
+}
+
+// =========================================================================== C-ABI
+extern "C" {
+
+void lima_default_params(lima_params* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->device = 0;
+    p->dt = 1e-6;  // 1 fs in ns
+    p->cutoff = 1.2;
+    p->skin = -1.0;
+    p->nstlist = 10;
+    p->electrostatics = LIMA_ES_EWALD;
+    p->ewald_tol = 1e-5;
+    p->integrator = LIMA_INTEGRATOR_LEAPFROG;
+    p->thermostat_scalar = 1.0;
+    p->exclude_bonded = 1;
+    p->use_graphs = 0;
+}
+
+const char* lima_error_string(int code) {
+    switch (code) {
+        case LIMA_OK: return "ok";
+        case LIMA_ERR_INVALID_ARG: return "invalid argument";
+        case LIMA_ERR_CUDA: return "CUDA error";
+        case LIMA_ERR_STATE: return "invalid call order";
+        case LIMA_ERR_OVERFLOW: return "device list overflow";
+        case LIMA_ERR_TIMEOUT: return "device wait timed out";
+        case LIMA_ERR_NO_DEVICE: return "no suitable CUDA device";
+        case LIMA_ERR_NOT_FINITE: return "non-finite values";
+        case LIMA_ERR_UNSUPPORTED: return "unsupported option";
+        default: return "unknown error";
+    }
+}
+
+const char* lima_last_error(const lima_engine* h) { return h ? h->err.c_str() : "null handle"; }
+
+int lima_version(void) { return 1; }
+
+int lima_create_batch(const lima_params* p, int n_systems, lima_engine** out) {
+    if (!p || !out || n_systems < 1) return LIMA_ERR_INVALID_ARG;
+    if (!(p->dt > 0.0) || !(p->cutoff > 0.0) || p->nstlist < 1) return LIMA_ERR_INVALID_ARG;
+    if (p->electrostatics < LIMA_ES_NONE || p->electrostatics > LIMA_ES_EWALD) return LIMA_ERR_INVALID_ARG;
+    if (p->integrator != LIMA_INTEGRATOR_LEAPFROG && p->integrator != LIMA_INTEGRATOR_VV) return LIMA_ERR_INVALID_ARG;
+    lima_engine* h = new (std::nothrow) lima_engine();
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    h->p = *p;
+    h->sys.resize(n_systems);
+    *out = h;
+    return LIMA_OK;
+}
+
+int lima_create(const lima_params* p, lima_engine** out) { return lima_create_batch(p, 1, out); }
+
+int lima_destroy(lima_engine* h) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    delete h;
+    return LIMA_OK;
+}
+
+int lima_select_system(lima_engine* h, int system) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    if (system < 0 || system >= (int)h->sys.size()) return fail(h, LIMA_ERR_INVALID_ARG, "system index out of range");
+    h->cur = system;
+    return LIMA_OK;
+}
+
+int lima_num_systems(const lima_engine* h, int* n) {
+    if (!h || !n) return LIMA_ERR_INVALID_ARG;
+    *n = (int)h->sys.size();
+    return LIMA_OK;
+}
+
+static int topology_changed(lima_engine* h) {
+    if (h->built) h->release();
+    h->built = false;
+    return LIMA_OK;
+}
+
+int lima_set_box(lima_engine* h, double lx, double ly, double lz) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    if (!(lx > 0 && ly > 0 && lz > 0)) return fail(h, LIMA_ERR_INVALID_ARG, "box edges must be > 0");
+    SystemHost& S = h->sys[h->cur];
+    S.box[0] = lx;
+    S.box[1] = ly;
+    S.box[2] = lz;
+    return topology_changed(h);
+}
+
+int lima_set_atoms(lima_engine* h, int n, const float* charge, const float* mass, const float* sigma,
+                   const float* epsilon) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    if (n <= 0 || !charge || !mass || !sigma || !epsilon) return fail(h, LIMA_ERR_INVALID_ARG, "bad atom arrays");
+    SystemHost& S = h->sys[h->cur];
+    S.n = n;
+    S.q.assign(charge, charge + n);
+    S.m.assign(mass, mass + n);
+    S.sig.assign(sigma, sigma + n);
+    S.eps.assign(epsilon, epsilon + n);
+    return topology_changed(h);
+}
+
+static int set_terms(lima_engine* h, int n, const int32_t* atoms, int k, const float* par, int np,
+                     std::vector<int32_t>& dst_i, std::vector<float>& dst_p) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    if (n < 0 || (n > 0 && (!atoms || (np > 0 && !par)))) return fail(h, LIMA_ERR_INVALID_ARG, "bad term arrays");
+    dst_i.assign(atoms, atoms + (size_t)n * k);
+    if (np > 0) dst_p.assign(par, par + (size_t)n * np);
+    return topology_changed(h);
+}
+
+int lima_set_bonds(lima_engine* h, int n, const int32_t* a, const float* p) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    return set_terms(h, n, a, 2, p, 2, h->sys[h->cur].bonds, h->sys[h->cur].bpar);
+}
+int lima_set_angles(lima_engine* h, int n, const int32_t* a, const float* p) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    return set_terms(h, n, a, 3, p, 4, h->sys[h->cur].angles, h->sys[h->cur].apar);
+}
+int lima_set_dihedrals(lima_engine* h, int n, const int32_t* a, const float* p) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    return set_terms(h, n, a, 4, p, 3, h->sys[h->cur].dihedrals, h->sys[h->cur].dpar);
+}
+int lima_set_impropers(lima_engine* h, int n, const int32_t* a, const float* p) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    return set_terms(h, n, a, 4, p, 2, h->sys[h->cur].impropers, h->sys[h->cur].ipar);
+}
+int lima_set_pairbonds(lima_engine* h, int n, const int32_t* a, const float* p) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    return set_terms(h, n, a, 2, p, 2, h->sys[h->cur].pairbonds, h->sys[h->cur].ppar);
+}
+int lima_set_exclusions(lima_engine* h, int n, const int32_t* a) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    std::vector<float> unused;
+    return set_terms(h, n, a, 2, nullptr, 0, h->sys[h->cur].excl, unused);
+}
+
+int lima_set_pme_grid(lima_engine* h, int nx, int ny, int nz) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    if (nx < 0 || ny < 0 || nz < 0) return fail(h, LIMA_ERR_INVALID_ARG, "bad PME grid");
+    SystemHost& S = h->sys[h->cur];
+    S.pme[0] = nx;
+    S.pme[1] = ny;
+    S.pme[2] = nz;
+    S.pme_set = true;
+    return topology_changed(h);
+}
+
+int lima_set_state(lima_engine* h, const double* pos, const float* vel) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    SystemHost& S = h->sys[h->cur];
+    if (S.n <= 0) return fail(h, LIMA_ERR_STATE, "lima_set_atoms must precede lima_set_state");
+    if (!pos) return fail(h, LIMA_ERR_INVALID_ARG, "positions required");
+    for (int i = 0; i < 3 * S.n; ++i)
+        if (!std::isfinite(pos[i])) return fail(h, LIMA_ERR_NOT_FINITE, "non-finite position");
+    return guarded(h, [&]() {
+        // pull the device state of the other systems first so they are kept
+        if (h->built && !h->state_pending && h->sys.size() > 1) {
+            std::vector<double> pp((size_t)3 * h->st.n_atoms);
+            std::vector<float> vv((size_t)3 * h->st.n_atoms);
+            launch_gather_state(h->st, h->d_out_d, h->d_out_f, h->s_main);
+            CK(cudaMemcpyAsync(pp.data(), h->d_out_d, pp.size() * 8, cudaMemcpyDeviceToHost, h->s_main));
+            CK(cudaMemcpyAsync(vv.data(), h->d_out_f, vv.size() * 4, cudaMemcpyDeviceToHost, h->s_main));
+            CK(cudaStreamSynchronize(h->s_main));
+            for (size_t s = 0; s < h->sys.size(); ++s) {
+                if ((int)s == h->cur) continue;
+                const size_t o = 3 * (size_t)h->n_atoms_off[s];
+                h->sys[s].pos.assign(pp.begin() + o, pp.begin() + o + 3 * h->sys[s].n);
+                h->sys[s].vel.assign(vv.begin() + o, vv.begin() + o + 3 * h->sys[s].n);
+            }
+        }
+        S.pos.assign(pos, pos + 3 * (size_t)S.n);
+        if (vel) S.vel.assign(vel, vel + 3 * (size_t)S.n);
+        else S.vel.assign(3 * (size_t)S.n, 0.f);
+        h->state_pending = true;
+        return LIMA_OK;
+    });
+}
+
+static int ensure_built(lima_engine* h) {
+    if (!h->built) h->setup();
+    return LIMA_OK;
+}
+
+int lima_get_state(lima_engine* h, double* pos, float* vel) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    return guarded(h, [&]() {
+        const SystemHost& S = h->sys[h->cur];
+        if (!h->built || h->state_pending) {
+            if (pos) std::copy(S.pos.begin(), S.pos.end(), pos);
+            if (vel) {
+                if (S.vel.empty()) std::fill(vel, vel + 3 * S.n, 0.f);
+                else std::copy(S.vel.begin(), S.vel.end(), vel);
+            }
+            return LIMA_OK;
+        }
+        launch_gather_state(h->st, h->d_out_d, h->d_out_f, h->s_main);
+        const size_t o = 3 * (size_t)h->n_atoms_off[h->cur];
+        if (pos) CK(cudaMemcpyAsync(pos, h->d_out_d + o, 3 * (size_t)S.n * 8, cudaMemcpyDeviceToHost, h->s_main));
+        if (vel) CK(cudaMemcpyAsync(vel, h->d_out_f + o, 3 * (size_t)S.n * 4, cudaMemcpyDeviceToHost, h->s_main));
+        CK(cudaStreamSynchronize(h->s_main));
+        return LIMA_OK;
+    });
+}
+
+int lima_compute_forces(lima_engine* h, int flags) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    return guarded(h, [&]() {
+        ensure_built(h);
+        const bool energy = (flags & LIMA_CALC_ENERGY) != 0;
+        h->forces(energy);
+        if (energy) {
+            CK(cudaMemcpyAsync(h->energy_host.data(), h->st.energy, sizeof(long long) * h->energy_host.size(),
+                               cudaMemcpyDeviceToHost, h->s_main));
+        }
+        CK(cudaStreamSynchronize(h->s_main));
+        CK(cudaGetLastError());
+        if (energy) h->energy_valid = true;
+        return LIMA_OK;
+    });
+}
+
+int lima_step(lima_engine* h, int n_steps) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    if (n_steps < 0) return fail(h, LIMA_ERR_INVALID_ARG, "n_steps < 0");
+    return guarded(h, [&]() {
+        ensure_built(h);
+        if (n_steps == 0) return LIMA_OK;
+        h->run_steps(n_steps);
+        unsigned status = 0;
+        CK(cudaMemcpy(&status, h->st.status, sizeof(unsigned), cudaMemcpyDeviceToHost));
+        if (status & ST_NONFINITE) return fail(h, LIMA_ERR_NOT_FINITE, "non-finite force during stepping");
+        return LIMA_OK;
+    });
+}
+
+int lima_minimize(lima_engine* h, double force_tol, int max_steps, int* steps_taken, double* max_force) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    if (max_steps < 0) return fail(h, LIMA_ERR_INVALID_ARG, "max_steps < 0");
+    return guarded(h, [&]() {
+        ensure_built(h);
+        h->nb.em = 1;
+        int k = 0;
+        float fmax = 0.f;
+        const int check_every = 10;
+        for (; k < max_steps; ++k) {
+            h->forces(false);
+            if (k % check_every == 0 || k == max_steps - 1) {
+                CK(cudaMemsetAsync(h->d_maxf, 0, sizeof(float), h->s_main));
+                launch_max_force(h->st, h->d_maxf, h->s_main);
+                CK(cudaMemcpyAsync(&fmax, h->d_maxf, sizeof(float), cudaMemcpyDeviceToHost, h->s_main));
+                CK(cudaStreamSynchronize(h->s_main));
+                if (fmax <= force_tol) break;
+            }
+            launch_em_step(h->st, k + 1, nullptr, h->s_main);
+            ++h->list_age;
+        }
+        CK(cudaStreamSynchronize(h->s_main));
+        h->nb.em = 0;
+        if (steps_taken) *steps_taken = k;
+        if (max_force) *max_force = fmax;
+        return LIMA_OK;
+    });
+}
+
+int lima_get_forces(lima_engine* h, double* forces) {
+    if (!h || !forces) return LIMA_ERR_INVALID_ARG;
+    if (!h->built || h->state_pending) return fail(h, LIMA_ERR_STATE, "no forces computed yet");
+    return guarded(h, [&]() {
+        launch_gather_forces(h->st, h->d_out_d, h->s_main);
+        const size_t o = 3 * (size_t)h->n_atoms_off[h->cur];
+        CK(cudaMemcpyAsync(forces, h->d_out_d + o, 3 * (size_t)h->sys[h->cur].n * 8, cudaMemcpyDeviceToHost, h->s_main));
+        CK(cudaStreamSynchronize(h->s_main));
+        return LIMA_OK;
+    });
+}
+
+int lima_get_energies(lima_engine* h, lima_energies* e) {
+    if (!h || !e) return LIMA_ERR_INVALID_ARG;
+    if (!h->energy_valid) return fail(h, LIMA_ERR_STATE, "no energies evaluated yet");
+    h->read_energies(e);
+    return LIMA_OK;
+}
+
+int lima_get_pairlist(lima_engine* h, int64_t cap, int32_t* pairs, int64_t* n) {
+    if (!h || !n || cap < 0 || (cap > 0 && !pairs)) return LIMA_ERR_INVALID_ARG;
+    return guarded(h, [&]() {
+        ensure_built(h);
+        if (h->state_pending) {
+            h->rebuild(true);
+            h->state_pending = false;
+        }
+        // count first, then fill
+        unsigned long long* dcount = h->dalloc<unsigned long long>(1);
+        launch_pairlist_dump(h->st, h->nb, 0, nullptr, dcount, h->s_main);
+        unsigned long long total = 0;
+        CK(cudaMemcpyAsync(&total, dcount, 8, cudaMemcpyDeviceToHost, h->s_main));
+        CK(cudaStreamSynchronize(h->s_main));
+        int* dpairs = h->dalloc<int>(2 * std::max<unsigned long long>(total, 1));
+        CK(cudaMemsetAsync(dcount, 0, 8, h->s_main));
+        launch_pairlist_dump(h->st, h->nb, (long long)total, dpairs, dcount, h->s_main);
+        std::vector<int> hp(2 * total);
+        if (total) CK(cudaMemcpyAsync(hp.data(), dpairs, hp.size() * 4, cudaMemcpyDeviceToHost, h->s_main));
+        CK(cudaStreamSynchronize(h->s_main));
+        for (void* a : {(void*)dcount, (void*)dpairs}) {
+            cudaFree(a);
+            h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), a), h->allocs.end());
+        }
+        // keep the selected system's pairs, local indices, sorted
+        const int off = h->n_atoms_off[h->cur], end = h->n_atoms_off[h->cur + 1];
+        std::vector<std::pair<int, int>> v;
+        v.reserve(total);
+        for (unsigned long long k = 0; k < total; ++k) {
+            const int a = hp[2 * k], b = hp[2 * k + 1];
+            if (a >= off && a < end) v.emplace_back(a - off, b - off);
+        }
+        std::sort(v.begin(), v.end());
+        *n = (int64_t)v.size();
+        for (int64_t k = 0; k < (int64_t)v.size() && k < cap; ++k) {
+            pairs[2 * k] = v[k].first;
+            pairs[2 * k + 1] = v[k].second;
+        }
+        return LIMA_OK;
+    });
+}
+
+int lima_get_status(lima_engine* h, uint32_t* status) {
+    if (!h || !status) return LIMA_ERR_INVALID_ARG;
+    *status = 0;
+    if (!h->built) return LIMA_OK;
+    return guarded(h, [&]() {
+        unsigned s = 0;
+        CK(cudaMemcpy(&s, h->st.status, sizeof(unsigned), cudaMemcpyDeviceToHost));
+        *status = s;
+        return LIMA_OK;
+    });
+}
+
+int lima_clear_status(lima_engine* h) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    if (!h->built) return LIMA_OK;
+    return guarded(h, [&]() {
+        CK(cudaMemset(h->st.status, 0, sizeof(unsigned)));
+        return LIMA_OK;
+    });
+}
+
+int lima_get_timings(lima_engine* h, lima_timings* t) {
+    if (!h || !t) return LIMA_ERR_INVALID_ARG;
+    std::memset(t, 0, sizeof(*t));
+    const double ns = h->timed_steps ? (double)h->timed_steps : 1.0;
+    t->steps = h->timed_steps;
+    t->rebuilds = h->rebuilds;
+    t->kernel_launches = h->launches;
+    t->step = 1000.0 * h->time_ms / ns;
+    t->nblist = h->rebuilds ? 1000.0 * h->phase_ms[0] / (double)h->rebuilds : 0.0;
+    t->nonbonded = 1000.0 * h->phase_ms[1] / ns;
+    t->bonded = 1000.0 * h->phase_ms[2] / ns;
+    t->pme = 1000.0 * h->phase_ms[3] / ns;
+    t->integrate = 1000.0 * h->phase_ms[4] / ns;
+    return LIMA_OK;
+}
+
+int lima_reset_timings(lima_engine* h) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    h->time_ms = 0.0;
+    h->timed_steps = 0;
+    h->rebuilds = 0;
+    h->launches = 0;
+    for (int k = 0; k < 5; ++k) h->phase_ms[k] = 0.0, h->phase_used[k] = 0;
+    return LIMA_OK;
+}
+
+int lima_enable_phase_timing(lima_engine* h, int enable) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    h->phase_timing = enable != 0;
+    return LIMA_OK;
+}
+
+}  // extern "C"

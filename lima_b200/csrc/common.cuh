@@ -1,0 +1,87 @@
+// common.cuh — device-side layout shared by every kernel of the force and
+// integration path.
+//
+// Data layout in HBM (all systems of a batch concatenated):
+//   * atoms live in "slots": the spatially sorted order produced by the
+//     column/cluster binning.  Slot s belongs to cluster s/8; padding slots
+//     have orig[s] == -1, zero charge/LJ and zero inverse mass.
+//   * per-slot state: pos (FP64 x,y,z SoA), xyzq (float4 working copy),
+//     ljp (float2: sigma/2, sqrt(eps)), vel (float4: v, 1/m), fprev (float4),
+//     force accumulators f{x,y,z} (int64 fixed point, FORCE_SCALE per J/mol/nm)
+//   * per-system energy accumulators: int64 fixed point, ENERGY_SCALE per J/mol
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace lima {
+
+constexpr int CLUSTER = 8;                       // atoms per cluster
+constexpr double FORCE_SCALE = 4294967296.0;     // 2^32 per J/mol/nm
+constexpr double ENERGY_SCALE = 16777216.0;      // 2^24 per J/mol
+constexpr double GRID_SCALE = 1099511627776.0;   // 2^40 per kC/mol (PME charge grid)
+constexpr int SHIFT_BITS = 5;                    // periodic-shift code in pair entries
+constexpr int JCLUSTER_BITS = 32 - SHIFT_BITS;
+
+enum EnergyTerm {
+    E_LJ = 0, E_COUL, E_RECIP, E_SELF, E_EXCL, E_BOND, E_ANGLE, E_DIHEDRAL, E_IMPROPER,
+    E_PAIRBOND, E_KINETIC, E_VIRIAL, E_COUNT
+};
+
+// status word bits (mirror LIMA_STATUS_* in include/lima_b200.h)
+constexpr unsigned ST_PAIRLIST_OVERFLOW = 0x1u;
+constexpr unsigned ST_COLUMN_OVERFLOW = 0x2u;
+constexpr unsigned ST_NONFINITE = 0x4u;
+constexpr unsigned ST_FORCE_SATURATED = 0x8u;
+constexpr unsigned ST_MOVED_TOO_FAR = 0x10u;
+
+// Per-system descriptor (one per system of a batch), resident in global memory.
+struct SysDesc {
+    double box[3];        // [nm]
+    float boxf[3];
+    float inv_boxf[3];
+    int atom_off, n_atoms;          // original-order atom range
+    int col_off, ncol_x, ncol_y;    // column grid
+    float col_w[2];                 // column widths [nm]
+    int max_clusters;               // capacity of this system's cluster range
+    int cluster_cap_off;            // first cluster of this system's capacity range
+    int pme_off;                    // offset of the real PME grid (floats)
+    int pme_coff;                   // offset of the half-complex grid (float2)
+    int pme_n[3];                   // grid dims (0 = no PME)
+    float pme_inv_h[3];             // K_d / L_d
+    double self_energy;             // Ewald self term [J/mol]
+    int n_charged;
+    int pad_;
+};
+
+__device__ __forceinline__ long long to_fixed(float v, double scale) {
+    return __double2ll_rn((double)v * scale);
+}
+__device__ __forceinline__ long long to_fixed_d(double v, double scale) {
+    return __double2ll_rn(v * scale);
+}
+__device__ __forceinline__ void atomic_add_fixed(long long* p, long long v) {
+    atomicAdd(reinterpret_cast<unsigned long long*>(p), static_cast<unsigned long long>(v));
+}
+
+__device__ __forceinline__ float min_image(float d, float L, float invL) {
+    return d - L * rintf(d * invL);
+}
+
+// warp reduction of a double (fixed lane order, so bit-reproducible)
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// shift code (sx+1) + 3(sy+1) + 9(sz+1), s in {-1,0,1}
+__device__ __forceinline__ int3 decode_shift(int code) {
+    return make_int3(code % 3 - 1, (code / 3) % 3 - 1, code / 9 - 1);
+}
+
+}  // namespace lima

@@ -1,0 +1,146 @@
+// engine.h — internal host/device interface of the force and integration path.
+// Not part of the public C-ABI (include/lima_b200.h).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace lima {
+
+// Every device pointer the per-step kernels touch; passed to kernels by value.
+struct DevState {
+    int n_sys = 0;
+    int n_atoms = 0;          // all systems
+    int n_clusters = 0;       // capacity (sum of per-system max_clusters)
+    int n_slots = 0;          // 8 * n_clusters
+    int n_cols = 0;           // all columns
+    int pl_cap = 0;           // pair-list entries per i-cluster
+    int col_cap = 0;          // atoms a column may hold
+
+    SysDesc* sys = nullptr;
+    int* sys_nclusters = nullptr;   // actual clusters per system (device-written)
+    int* cluster_sys = nullptr;     // static: system of each cluster slot range
+    int* col_sys = nullptr;         // static: system of each column
+
+    // per-slot state
+    double *px = nullptr, *py = nullptr, *pz = nullptr;
+    float4* xyzq = nullptr;
+    float2* ljp = nullptr;          // sigma/2, sqrt(eps)
+    float4* vel = nullptr;          // v, 1/m
+    float4* fprev = nullptr;        // previous-step force (velocity Verlet)
+    float4* adam_m = nullptr;       // energy minimisation first moments
+    float4* adam_v = nullptr;       // second moments
+    long long *fx = nullptr, *fy = nullptr, *fz = nullptr;
+    int* orig = nullptr;
+    float4* tvel = nullptr;         // permutation scratch
+    float4* tfprev = nullptr;
+    float4* tadam_m = nullptr;
+    float4* tadam_v = nullptr;
+
+    // per-atom (original order), static
+    int* atom_sys = nullptr;
+    int* slot_of = nullptr;
+    float* q = nullptr;
+    float* inv_mass = nullptr;
+    float2* ljp_atom = nullptr;
+    int* mol = nullptr;
+    int* excl_off = nullptr;
+    int* excl_idx = nullptr;
+    double* in_pos = nullptr;       // 3n staging / wrapped positions
+    float* in_vel = nullptr;        // 3n staging
+
+    // binning scratch
+    int* col_of_atom = nullptr;
+    float* z_of_atom = nullptr;
+    int* col_count = nullptr;
+    int* col_fill = nullptr;
+    int* col_atom_start = nullptr;
+    int* col_cl_start = nullptr;
+    int* col_ncl = nullptr;
+    int* col_list = nullptr;
+    int* new_orig = nullptr;
+
+    // clusters and pair list
+    float4* bb_lo = nullptr;
+    float4* bb_hi = nullptr;
+    int* pl_count = nullptr;
+    int* pl_j = nullptr;
+    unsigned long long* pl_mask = nullptr;
+
+    // PME
+    long long* pme_grid_fx = nullptr;    // fixed-point charge grid (all systems)
+    float* pme_real = nullptr;           // real-space potential grid
+    float2* pme_cplx = nullptr;          // half-complex grid
+    float* pme_theta = nullptr;          // influence function on the half-complex grid
+    int pme_total_real = 0;
+    int pme_total_cplx = 0;
+
+    unsigned* status = nullptr;
+    long long* energy = nullptr;         // [n_sys][E_COUNT]
+};
+
+struct BondedTerms {
+    int nb = 0, na = 0, nd = 0, ni = 0, np = 0;
+    int2* bidx = nullptr;
+    float2* bpar = nullptr;
+    int4* aidx = nullptr;
+    float4* apar = nullptr;
+    int4* didx = nullptr;
+    float4* dpar = nullptr;
+    int4* iidx = nullptr;
+    float2* ipar = nullptr;
+    int2* pidx = nullptr;
+    float2* ppar = nullptr;
+    int nx = 0;                 // excluded charged pairs for the Ewald correction
+    int2* xidx = nullptr;
+};
+
+struct NbParams {
+    float rc2;
+    float rlist;          // cutoff + skin
+    int es_mode;          // 0 none, 1 cutoff, 2 Ewald erfc
+    float kappa;
+    float ke;             // Coulomb constant
+    float two_kappa_sqrtpi;
+    int em;               // energy-minimisation force clamp
+};
+
+// nbsearch.cu
+int launch_rebuild(const DevState& st, float rlist, bool from_input, cudaStream_t s);
+// nonbonded.cu
+int launch_nonbonded(const DevState& st, const NbParams& p, bool energy, cudaStream_t s);
+int launch_exclusion_correction(const DevState& st, const BondedTerms& bt, const NbParams& p,
+                                 bool energy, cudaStream_t s);
+int launch_pairlist_dump(const DevState& st, const NbParams& p, long long cap, int* out_pairs,
+                          unsigned long long* out_count, cudaStream_t s);
+// bonded.cu
+int launch_bonded(const DevState& st, const BondedTerms& bt, bool energy, cudaStream_t s);
+// pme.cu
+struct PmePlan {
+    int n_items_x = 0, n_items_y = 0, n_items_z = 0;   // work items per FFT pass
+    int4* items_x = nullptr;     // (system, line0, nlines, 0)
+    int4* items_y = nullptr;     // (system, x0, z, 0)
+    int4* items_z = nullptr;     // (system, x0, y, 0)
+    const void* sys_plans = nullptr;  // per-system radix plans (device)
+    int ref_gather = 0;          // central-difference gather
+    int max_n = 0;
+};
+size_t pme_sys_dev_size();
+bool fill_pme_sys_dev(void* dst, int kx, int ky, int kz);
+void pme_set_smem_limits(int maxn);
+int launch_pme(const DevState& st, const PmePlan& plan, bool energy, cudaStream_t s);
+// integrate.cu
+struct IntegrateParams {
+    double dt;
+    float scale;            // thermostat velocity scale
+    int integrator;         // 0 leapfrog, 1 velocity Verlet
+};
+int launch_integrate(const DevState& st, const IntegrateParams& p, bool energy, cudaStream_t s);
+int launch_em_step(const DevState& st, int step, float* max_force_out_dev, cudaStream_t s);
+int launch_gather_state(const DevState& st, double* pos_out, float* vel_out, cudaStream_t s);
+int launch_gather_forces(const DevState& st, double* f_out, cudaStream_t s);
+int launch_zero_forces(const DevState& st, cudaStream_t s);
+int launch_max_force(const DevState& st, float* out, cudaStream_t s);
+
+}  // namespace lima

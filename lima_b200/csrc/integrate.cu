@@ -1,0 +1,214 @@
+// integrate.cu — integrators, energy minimisation step and state transfer.
+//
+// Replaces the integration part of CompoundIntegrationKernel
+// (code/LIMA_ENGINE/src/EngineKernels.cuh:344-441):
+//   velocity Verlet as in EngineUtils::integrateVelocityVVS / integratePositionVVS
+//   (code/LIMA_ENGINE/src/EngineUtils.cuh:31-41):
+//       v = v_prev + (F + F_prev) dt/2m ; x += v dt + F dt^2/2m ; v_prev = v * scale
+//   leapfrog (the native integrator): v += F dt/m ; x += v dt
+// Positions are updated in FP64 relative to the box origin (the reference keeps
+// int32 fixed point relative to per-compound integer origins,
+// code/LIMA_BASE/include/LimaTypes.cuh:297-334); the float4 working copy used by
+// the force kernels is refreshed from the FP64 value.
+// The energy-minimisation step restates IntegratePositionADAM and
+// ForceActivationFunction (EngineUtils.cuh:44-72,112-140).
+#include "engine.h"
+
+namespace lima {
+
+__device__ __forceinline__ float3 load_force(const DevState& st, int s) {
+    const double inv = 1.0 / FORCE_SCALE;
+    return make_float3((float)((double)st.fx[s] * inv), (float)((double)st.fy[s] * inv),
+                       (float)((double)st.fz[s] * inv));
+}
+
+__device__ __forceinline__ void add_energy_warp(const DevState& st, int sysi, double e, int term) {
+    const int s_first = __shfl_sync(0xffffffffu, sysi, 0);
+    const bool uniform = __all_sync(0xffffffffu, sysi == s_first || sysi < 0);
+    const int sref = __reduce_max_sync(0xffffffffu, sysi);
+    if (uniform) {
+        e = warp_sum(e);
+        if ((threadIdx.x & 31) == 0 && sref >= 0)
+            atomic_add_fixed(st.energy + (size_t)sref * E_COUNT + term, to_fixed_d(e, ENERGY_SCALE));
+    } else if (sysi >= 0) {
+        atomic_add_fixed(st.energy + (size_t)sysi * E_COUNT + term, to_fixed_d(e, ENERGY_SCALE));
+    }
+}
+
+template <int INTEGRATOR, bool ENERGY>
+__global__ void k_integrate(DevState st, IntegrateParams p) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    double ke = 0.0;
+    int sysi = -1;
+    if (s < st.n_slots && st.orig[s] >= 0) {
+        sysi = st.cluster_sys[s / CLUSTER];
+        const float3 F = load_force(st, s);
+        float4 v = st.vel[s];
+        const float im = v.w;
+        const float dt = (float)p.dt;
+        if (!(isfinite(F.x) && isfinite(F.y) && isfinite(F.z))) atomicOr(st.status, ST_NONFINITE);
+        double dx, dy, dz;
+        if (INTEGRATOR == 0) {
+            const float m = im > 0.f ? 1.f / im : 0.f;
+            const float vx = (v.x + F.x * im * dt) * p.scale;
+            const float vy = (v.y + F.y * im * dt) * p.scale;
+            const float vz = (v.z + F.z * im * dt) * p.scale;
+            if (ENERGY) {
+                // average of the two half-step kinetic energies
+                ke = 0.25 * (double)m * ((double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z +
+                                         (double)vx * vx + (double)vy * vy + (double)vz * vz);
+            }
+            v.x = vx;
+            v.y = vy;
+            v.z = vz;
+            dx = (double)vx * p.dt;
+            dy = (double)vy * p.dt;
+            dz = (double)vz * p.dt;
+        } else {
+            const float4 fp = st.fprev[s];
+            const float h = 0.5f * dt * im;
+            const float vx = v.x + (F.x + fp.x) * h;
+            const float vy = v.y + (F.y + fp.y) * h;
+            const float vz = v.z + (F.z + fp.z) * h;
+            if (ENERGY) {
+                const float m = im > 0.f ? 1.f / im : 0.f;
+                ke = 0.5 * (double)m * ((double)vx * vx + (double)vy * vy + (double)vz * vz);
+            }
+            const float a = 0.5f * im * dt * dt;
+            dx = (double)vx * p.dt + (double)(F.x * a);
+            dy = (double)vy * p.dt + (double)(F.y * a);
+            dz = (double)vz * p.dt + (double)(F.z * a);
+            st.fprev[s] = make_float4(F.x, F.y, F.z, 0.f);
+            v.x = vx * p.scale;
+            v.y = vy * p.scale;
+            v.z = vz * p.scale;
+        }
+        st.vel[s] = v;
+        const double x = st.px[s] + dx, y = st.py[s] + dy, z = st.pz[s] + dz;
+        st.px[s] = x;
+        st.py[s] = y;
+        st.pz[s] = z;
+        const float q = st.xyzq[s].w;
+        st.xyzq[s] = make_float4((float)x, (float)y, (float)z, q);
+    }
+    if (ENERGY) add_energy_warp(st, sysi, ke, E_KINETIC);
+}
+
+int launch_integrate(const DevState& st, const IntegrateParams& p, bool energy, cudaStream_t s) {
+    const int TB = 256;
+    const int g = (st.n_slots + TB - 1) / TB;
+    if (p.integrator == 0) {
+        if (energy) k_integrate<0, true><<<g, TB, 0, s>>>(st, p);
+        else k_integrate<0, false><<<g, TB, 0, s>>>(st, p);
+    } else {
+        if (energy) k_integrate<1, true><<<g, TB, 0, s>>>(st, p);
+        else k_integrate<1, false><<<g, TB, 0, s>>>(st, p);
+    }
+    return 1;
+}
+
+// ADAM step on tanh-clamped forces; positions move by alpha*mhat/(sqrt(vhat)+eps)*1e-8 nm
+__global__ void k_em_step(DevState st, int step) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= st.n_slots || st.orig[s] < 0) return;
+    float3 F = load_force(st, s);
+    const float fmax = 1.0e6f;  // 1000 kJ/mol/nm
+    const float fl = sqrtf(F.x * F.x + F.y * F.y + F.z * F.z);
+    const float sc = fmax * tanhf(fl / fmax) / (fl + 1e-8f);
+    const float g[3] = {F.x * sc * 1e-8f, F.y * sc * 1e-8f, F.z * sc * 1e-8f};
+    float4 m = st.adam_m[s], v = st.adam_v[s];
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.f / (1.f - powf(b1, (float)step));
+    const float c2 = 1.f / (1.f - powf(b2, (float)step));
+    float* mm = &m.x;
+    float* vv = &v.x;
+    double d[3];
+    for (int k = 0; k < 3; ++k) {
+        mm[k] = mm[k] * b1 + g[k] * (1.f - b1);
+        vv[k] = vv[k] * b2 + g[k] * g[k] * (1.f - b2);
+        d[k] = (double)(mm[k] * c1 / (sqrtf(vv[k] * c2) + 1e-8f) * 8000.f) * 1e-8;
+    }
+    st.adam_m[s] = m;
+    st.adam_v[s] = v;
+    const double x = st.px[s] + d[0], y = st.py[s] + d[1], z = st.pz[s] + d[2];
+    st.px[s] = x;
+    st.py[s] = y;
+    st.pz[s] = z;
+    const float q = st.xyzq[s].w;
+    st.xyzq[s] = make_float4((float)x, (float)y, (float)z, q);
+}
+
+int launch_em_step(const DevState& st, int step, float* /*max_force_out_dev*/, cudaStream_t s) {
+    const int TB = 256;
+    k_em_step<<<(st.n_slots + TB - 1) / TB, TB, 0, s>>>(st, step);
+    return 1;
+}
+
+// per-atom maximum |F| (as float bits; non-negative floats order like ints)
+__global__ void k_max_force(DevState st, float* out) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    float fl = 0.f;
+    if (s < st.n_slots && st.orig[s] >= 0) {
+        const float3 F = load_force(st, s);
+        fl = sqrtf(F.x * F.x + F.y * F.y + F.z * F.z);
+        if (!isfinite(fl)) fl = 3.0e38f;
+    }
+    for (int o = 16; o > 0; o >>= 1) fl = fmaxf(fl, __shfl_xor_sync(0xffffffffu, fl, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<int*>(out), __float_as_int(fl));
+}
+
+int launch_max_force(const DevState& st, float* out, cudaStream_t s) {
+    const int TB = 256;
+    k_max_force<<<(st.n_slots + TB - 1) / TB, TB, 0, s>>>(st, out);
+    return 1;
+}
+
+// slot order -> original order
+__global__ void k_gather_state(DevState st, double* pos, float* vel) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= st.n_atoms) return;
+    const int s = st.slot_of[a];
+    if (pos) {
+        pos[3 * a] = st.px[s];
+        pos[3 * a + 1] = st.py[s];
+        pos[3 * a + 2] = st.pz[s];
+    }
+    if (vel) {
+        const float4 v = st.vel[s];
+        vel[3 * a] = v.x;
+        vel[3 * a + 1] = v.y;
+        vel[3 * a + 2] = v.z;
+    }
+}
+
+int launch_gather_state(const DevState& st, double* pos_out, float* vel_out, cudaStream_t s) {
+    const int TB = 256;
+    k_gather_state<<<(st.n_atoms + TB - 1) / TB, TB, 0, s>>>(st, pos_out, vel_out);
+    return 1;
+}
+
+__global__ void k_gather_forces(DevState st, double* f) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= st.n_atoms) return;
+    const int s = st.slot_of[a];
+    const double inv = 1.0 / FORCE_SCALE;
+    f[3 * a] = (double)st.fx[s] * inv;
+    f[3 * a + 1] = (double)st.fy[s] * inv;
+    f[3 * a + 2] = (double)st.fz[s] * inv;
+}
+
+int launch_gather_forces(const DevState& st, double* f_out, cudaStream_t s) {
+    const int TB = 256;
+    k_gather_forces<<<(st.n_atoms + TB - 1) / TB, TB, 0, s>>>(st, f_out);
+    return 1;
+}
+
+int launch_zero_forces(const DevState& st, cudaStream_t s) {
+    const size_t bytes = (size_t)st.n_slots * sizeof(long long);
+    cudaMemsetAsync(st.fx, 0, bytes, s);
+    cudaMemsetAsync(st.fy, 0, bytes, s);
+    cudaMemsetAsync(st.fz, 0, bytes, s);
+    return 0;  // memsets, not kernels of this library
+}
+
+}  // namespace lima

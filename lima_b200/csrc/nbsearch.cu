@@ -1,0 +1,355 @@
+// nbsearch.cu — cell-grid / neighbour-list build.
+//
+// Replaces NeighborLists::updateNlists (code/LIMA_ENGINE/src/Neighborlists.cuh:294-317)
+// and its O(N_c^2) compound test (:139-229) with an O(N) column-cluster build:
+//   1. k_bin            atom -> column of an x-y grid (wrapped positions)
+//   2. k_scan_columns   per-system exclusive scans: atom and cluster offsets
+//   3. k_scatter        atoms -> column lists (unordered)
+//   4. k_sort_columns   deterministic order inside a column: (z, atom index)
+//   5. k_gather_slots   state permuted into the new slot order
+//   6. k_finish_slots   slot_of map, permuted velocity state
+//   7. k_bbox           per-cluster bounding boxes
+//   8. k_pairsearch     half list of cluster pairs within cutoff+skin, with a
+//                       64-bit interaction mask (padding, exclusions, i<j on
+//                       the diagonal) and a periodic-shift code per entry.
+// The result is bit-identical run to run: every ordering is fixed by keys,
+// never by atomic arrival order.
+#include "engine.h"
+
+namespace lima {
+
+__global__ void k_bin(DevState st, int from_input) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= st.n_atoms) return;
+    const SysDesc& sd = st.sys[st.atom_sys[a]];
+    double p[3];
+    if (from_input) {
+        p[0] = st.in_pos[3 * a];
+        p[1] = st.in_pos[3 * a + 1];
+        p[2] = st.in_pos[3 * a + 2];
+    } else {
+        const int s = st.slot_of[a];
+        p[0] = st.px[s];
+        p[1] = st.py[s];
+        p[2] = st.pz[s];
+    }
+    for (int d = 0; d < 3; ++d) {
+        const double L = sd.box[d];
+        double x = p[d] - L * floor(p[d] / L);
+        if (x >= L) x -= L;
+        if (x < 0.0) x = 0.0;
+        p[d] = x;
+        st.in_pos[3 * a + d] = x;
+    }
+    int cx = (int)(p[0] * sd.ncol_x / sd.box[0]);
+    int cy = (int)(p[1] * sd.ncol_y / sd.box[1]);
+    cx = min(max(cx, 0), sd.ncol_x - 1);
+    cy = min(max(cy, 0), sd.ncol_y - 1);
+    const int col = sd.col_off + cx + sd.ncol_x * cy;
+    st.col_of_atom[a] = col;
+    st.z_of_atom[a] = (float)p[2];
+    atomicAdd(&st.col_count[col], 1);
+}
+
+// one CTA per system; Hillis-Steele block scan over chunks of columns
+__global__ void k_scan_columns(DevState st) {
+    const int s = blockIdx.x;
+    const SysDesc sd = st.sys[s];
+    const int ncol = sd.ncol_x * sd.ncol_y;
+    __shared__ int sa[1024], sc[1024];
+    __shared__ int carry_a, carry_c;
+    const int tid = threadIdx.x;
+    if (tid == 0) carry_a = carry_c = 0;
+    __syncthreads();
+    for (int base = 0; base < ncol; base += blockDim.x) {
+        const int i = base + tid;
+        const int cnt = i < ncol ? st.col_count[sd.col_off + i] : 0;
+        const int ncl = (cnt + CLUSTER - 1) / CLUSTER;
+        sa[tid] = cnt;
+        sc[tid] = ncl;
+        __syncthreads();
+        for (int o = 1; o < (int)blockDim.x; o <<= 1) {
+            const int va = tid >= o ? sa[tid - o] : 0;
+            const int vc = tid >= o ? sc[tid - o] : 0;
+            __syncthreads();
+            sa[tid] += va;
+            sc[tid] += vc;
+            __syncthreads();
+        }
+        if (i < ncol) {
+            st.col_atom_start[sd.col_off + i] = carry_a + sa[tid] - cnt;
+            st.col_cl_start[sd.col_off + i] = sd.cluster_cap_off + carry_c + sc[tid] - ncl;
+            st.col_ncl[sd.col_off + i] = ncl;
+        }
+        __syncthreads();
+        if (tid == blockDim.x - 1) {
+            carry_a += sa[tid];
+            carry_c += sc[tid];
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        st.sys_nclusters[s] = min(carry_c, sd.max_clusters);
+        if (carry_c > sd.max_clusters) atomicOr(st.status, ST_COLUMN_OVERFLOW);
+    }
+}
+
+__global__ void k_scatter(DevState st) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= st.n_atoms) return;
+    const int col = st.col_of_atom[a];
+    const int k = atomicAdd(&st.col_fill[col], 1);
+    const int off = st.sys[st.atom_sys[a]].atom_off;
+    st.col_list[off + st.col_atom_start[col] + k] = a;
+}
+
+// one CTA per column: rank each atom by the unique key (z bits, atom index)
+__global__ void k_sort_columns(DevState st, const int* col_sys) {
+    extern __shared__ unsigned long long keys[];
+    const int col = blockIdx.x;
+    const int n_all = st.col_count[col];
+    const int n = min(n_all, st.col_cap);
+    const int off = st.sys[col_sys[col]].atom_off + st.col_atom_start[col];
+    const int slot0 = st.col_cl_start[col] * CLUSTER;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const int a = st.col_list[off + i];
+        keys[i] = ((unsigned long long)__float_as_uint(st.z_of_atom[a]) << 32) | (unsigned)a;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const unsigned long long k = keys[i];
+        int rank = 0;
+        for (int j = 0; j < n; ++j) rank += keys[j] < k;
+        st.new_orig[slot0 + rank] = (int)(k & 0xffffffffu);
+    }
+    const int padded = st.col_ncl[col] * CLUSTER;
+    for (int r = n + threadIdx.x; r < padded; r += blockDim.x) st.new_orig[slot0 + r] = -1;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (n_all > st.col_cap) atomicOr(st.status, ST_COLUMN_OVERFLOW);
+        st.col_count[col] = 0;
+        st.col_fill[col] = 0;
+    }
+}
+
+__global__ void k_gather_slots(DevState st, int from_input) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= st.n_slots) return;
+    const int c = s / CLUSTER;
+    const int sysi = st.cluster_sys[c];
+    const SysDesc& sd = st.sys[sysi];
+    const int local = c - sd.cluster_cap_off;
+    const int a = local < st.sys_nclusters[sysi] ? st.new_orig[s] : -1;
+    if (a >= 0) {
+        const double x = st.in_pos[3 * a], y = st.in_pos[3 * a + 1], z = st.in_pos[3 * a + 2];
+        st.px[s] = x;
+        st.py[s] = y;
+        st.pz[s] = z;
+        st.xyzq[s] = make_float4((float)x, (float)y, (float)z, st.q[a]);
+        st.ljp[s] = st.ljp_atom[a];
+        const float im = st.inv_mass[a];
+        if (from_input) {
+            st.tvel[s] = make_float4(st.in_vel[3 * a], st.in_vel[3 * a + 1], st.in_vel[3 * a + 2], im);
+            st.tfprev[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+            st.tadam_m[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+            st.tadam_v[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+        } else {
+            const int old = st.slot_of[a];
+            float4 v = st.vel[old];
+            v.w = im;
+            st.tvel[s] = v;
+            st.tfprev[s] = st.fprev[old];
+            st.tadam_m[s] = st.adam_m[old];
+            st.tadam_v[s] = st.adam_v[old];
+        }
+    } else {
+        st.px[s] = 0.0;
+        st.py[s] = 0.0;
+        st.pz[s] = 0.0;
+        st.xyzq[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+        st.ljp[s] = make_float2(0.f, 0.f);
+        st.tvel[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+        st.tfprev[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+        st.tadam_m[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+        st.tadam_v[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    st.orig[s] = a;
+}
+
+__global__ void k_finish_slots(DevState st) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= st.n_slots) return;
+    st.vel[s] = st.tvel[s];
+    st.fprev[s] = st.tfprev[s];
+    st.adam_m[s] = st.tadam_m[s];
+    st.adam_v[s] = st.tadam_v[s];
+    const int a = st.orig[s];
+    if (a >= 0) st.slot_of[a] = s;
+}
+
+__global__ void k_bbox(DevState st) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= st.n_clusters) return;
+    float4 lo = make_float4(0.f, 0.f, 0.f, 0.f), hi = lo;
+    bool first = true;
+    for (int k = 0; k < CLUSTER; ++k) {
+        const int s = c * CLUSTER + k;
+        if (st.orig[s] < 0) continue;
+        const float4 p = st.xyzq[s];
+        if (first) {
+            lo = hi = p;
+            first = false;
+        } else {
+            lo.x = fminf(lo.x, p.x);
+            lo.y = fminf(lo.y, p.y);
+            lo.z = fminf(lo.z, p.z);
+            hi.x = fmaxf(hi.x, p.x);
+            hi.y = fmaxf(hi.y, p.y);
+            hi.z = fmaxf(hi.z, p.z);
+        }
+    }
+    lo.w = first ? 0.f : 1.f;  // w = 1 marks a populated cluster
+    st.bb_lo[c] = lo;
+    st.bb_hi[c] = hi;
+}
+
+__device__ __forceinline__ bool excluded(const DevState& st, int ai, int aj, int eb, int ee) {
+    for (int k = eb; k < ee; ++k)
+        if (st.excl_idx[k] == aj) return true;
+    return false;
+}
+
+__device__ __forceinline__ int wrapi(int i, int n) {
+    i %= n;
+    return i < 0 ? i + n : i;
+}
+
+// one warp per i-cluster
+__global__ void k_pairsearch(DevState st, float rlist) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= st.n_clusters) return;
+    const int ci = warp;
+    const int sysi = st.cluster_sys[ci];
+    const SysDesc& sd = st.sys[sysi];
+    const int local = ci - sd.cluster_cap_off;
+    if (local >= st.sys_nclusters[sysi]) {
+        if (lane == 0) st.pl_count[ci] = 0;
+        return;
+    }
+    const float4 ilo = st.bb_lo[ci], ihi = st.bb_hi[ci];
+    const float ic[3] = {0.5f * (ilo.x + ihi.x), 0.5f * (ilo.y + ihi.y), 0.5f * (ilo.z + ihi.z)};
+    const float ie[3] = {0.5f * (ihi.x - ilo.x), 0.5f * (ihi.y - ilo.y), 0.5f * (ihi.z - ilo.z)};
+    const float L[3] = {sd.boxf[0], sd.boxf[1], sd.boxf[2]};
+    const float R = rlist, R2 = rlist * rlist;
+
+    // per-lane i-atom data for the interaction mask (lane -> ii = lane & 7)
+    const int ii = lane & 7, jj0 = lane >> 3;
+    const int ai = st.orig[ci * CLUSTER + ii];
+    const int mi = ai >= 0 ? st.mol[ai] : -1;
+    const int eb = ai >= 0 ? st.excl_off[ai] : 0;
+    const int ee = ai >= 0 ? st.excl_off[ai + 1] : 0;
+
+    // column window (every column visited once even when the window wraps)
+    int cx0 = (int)floorf((ilo.x - R) / sd.col_w[0]);
+    int cx1 = (int)floorf((ihi.x + R) / sd.col_w[0]);
+    int nx = cx1 - cx0 + 1;
+    if (nx >= sd.ncol_x) {
+        cx0 = 0;
+        nx = sd.ncol_x;
+    }
+    int cy0 = (int)floorf((ilo.y - R) / sd.col_w[1]);
+    int cy1 = (int)floorf((ihi.y + R) / sd.col_w[1]);
+    int ny = cy1 - cy0 + 1;
+    if (ny >= sd.ncol_y) {
+        cy0 = 0;
+        ny = sd.ncol_y;
+    }
+
+    const int cap = st.pl_cap;
+    int count = 0;
+    const size_t base_out = (size_t)ci * cap;
+    for (int iy = 0; iy < ny; ++iy) {
+        const int cy = wrapi(cy0 + iy, sd.ncol_y);
+        for (int ix = 0; ix < nx; ++ix) {
+            const int cx = wrapi(cx0 + ix, sd.ncol_x);
+            const int col = sd.col_off + cx + sd.ncol_x * cy;
+            const int j0 = st.col_cl_start[col];
+            const int nj = st.col_ncl[col];
+            for (int b = 0; b < nj; b += 32) {
+                const int j = j0 + b + lane;
+                unsigned shifts = 0u;  // bit k set: shift code k is in range
+                if (b + lane < nj && j >= ci) {
+                    const float4 jlo = st.bb_lo[j], jhi = st.bb_hi[j];
+                    const float jc[3] = {0.5f * (jlo.x + jhi.x), 0.5f * (jlo.y + jhi.y), 0.5f * (jlo.z + jhi.z)};
+                    const float je[3] = {0.5f * (jhi.x - jlo.x), 0.5f * (jhi.y - jlo.y), 0.5f * (jhi.z - jlo.z)};
+                    float g2[3][3];
+                    for (int d = 0; d < 3; ++d) {
+                        for (int sh = -1; sh <= 1; ++sh) {
+                            const float dd = fabsf(jc[d] + sh * L[d] - ic[d]) - ie[d] - je[d];
+                            const float g = fmaxf(dd, 0.f);
+                            g2[d][sh + 1] = g * g;
+                        }
+                    }
+                    for (int sz = 0; sz < 3; ++sz)
+                        for (int sy = 0; sy < 3; ++sy)
+                            for (int sx = 0; sx < 3; ++sx) {
+                                const int code = sx + 3 * sy + 9 * sz;
+                                if (j == ci && code != 13) continue;
+                                if (g2[0][sx] + g2[1][sy] + g2[2][sz] < R2) shifts |= 1u << code;
+                            }
+                }
+                unsigned pending = __ballot_sync(0xffffffffu, shifts != 0u);
+                while (pending) {
+                    const int src = __ffs(pending) - 1;
+                    const unsigned sh_src = __shfl_sync(0xffffffffu, shifts, src);
+                    const int jc = __shfl_sync(0xffffffffu, j, src);
+                    const int code = __ffs(sh_src) - 1;
+                    const unsigned rest = sh_src & (sh_src - 1u);
+                    if (lane == src) shifts = rest;
+                    if (rest == 0u) pending &= pending - 1u;
+                    // interaction mask: bit (jj*8 + ii)
+                    bool ok[2];
+                    for (int h = 0; h < 2; ++h) {
+                        const int jj = jj0 + 4 * h;
+                        const int aj = st.orig[jc * CLUSTER + jj];
+                        bool o = ai >= 0 && aj >= 0;
+                        if (o && jc == ci) o = jj > ii;
+                        if (o && mi == st.mol[aj]) o = !excluded(st, ai, aj, eb, ee);
+                        ok[h] = o;
+                    }
+                    const unsigned lo32 = __ballot_sync(0xffffffffu, ok[0]);
+                    const unsigned hi32 = __ballot_sync(0xffffffffu, ok[1]);
+                    const unsigned long long mask = ((unsigned long long)hi32 << 32) | lo32;
+                    if (mask != 0ull) {
+                        if (count < cap && lane == 0) {
+                            st.pl_j[base_out + count] = jc | (code << JCLUSTER_BITS);
+                            st.pl_mask[base_out + count] = mask;
+                        }
+                        ++count;
+                    }
+                }
+            }
+        }
+    }
+    if (lane == 0) {
+        st.pl_count[ci] = min(count, cap);
+        if (count > cap) atomicOr(st.status, ST_PAIRLIST_OVERFLOW);
+    }
+}
+
+int launch_rebuild(const DevState& st, float rlist, bool from_input, cudaStream_t s) {
+    const int TB = 256;
+    k_bin<<<(st.n_atoms + TB - 1) / TB, TB, 0, s>>>(st, from_input ? 1 : 0);
+    k_scan_columns<<<st.n_sys, 1024, 0, s>>>(st);
+    k_scatter<<<(st.n_atoms + TB - 1) / TB, TB, 0, s>>>(st);
+    k_sort_columns<<<st.n_cols, 128, (size_t)st.col_cap * sizeof(unsigned long long), s>>>(st, st.col_sys);
+    k_gather_slots<<<(st.n_slots + TB - 1) / TB, TB, 0, s>>>(st, from_input ? 1 : 0);
+    k_finish_slots<<<(st.n_slots + TB - 1) / TB, TB, 0, s>>>(st);
+    k_bbox<<<(st.n_clusters + TB - 1) / TB, TB, 0, s>>>(st);
+    const long long threads = (long long)st.n_clusters * 32;
+    k_pairsearch<<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(st, rlist);
+    return 8;
+}
+
+}  // namespace lima

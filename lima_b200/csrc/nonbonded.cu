@@ -1,0 +1,251 @@
+// nonbonded.cu — short-range LJ + real-space Coulomb over cluster pairs.
+//
+// Replaces compoundFarneighborShortrangeInteractionsKernel and
+// compoundImmediateneighborAndSelfShortrangeInteractionsKernel
+// (code/LIMA_ENGINE/src/EngineKernels.cuh:47-317) and the per-pair arithmetic of
+// LJ::calcLJForceOptim (code/LIMA_ENGINE/src/LennardJonesInteractions.cuh:74-108)
+// and PhysicsUtilsDevice::CalcCoulumbForce_optim / CalcCoulumbPotential_optim
+// (code/LIMA_ENGINE/src/DeviceAlgorithmsPrivate.cuh:38-95):
+//   F_i = [24 eps s (1-2s)/r^2 - k_e q_i q_j/r^3 (erfc(kr) + 2k/sqrt(pi) r e^{-k^2r^2})] (r_j - r_i)
+//   E   = 4 eps s (s-1) + k_e q_i q_j erfc(kr)/r,   s = (sigma/r)^6
+// Every unordered pair is evaluated once (Newton's third law), where the
+// reference evaluates each directed pair.
+//
+// Work mapping: one warp per i-cluster (8 atoms) walks its list of j-clusters;
+// lane = (jj0 << 3) | ii handles i-atom ii against j-atoms jj0 and jj0+4.  The
+// i forces stay in registers for the whole list; the j forces are reduced over
+// the 8 lanes sharing a j-atom with three xor-shuffles and added once per
+// cluster pair as int64 fixed point, so the result does not depend on the
+// order in which warps finish.
+#include "engine.h"
+
+namespace lima {
+
+template <int ES, bool ENERGY>
+__global__ void __launch_bounds__(256) k_nonbonded(DevState st, NbParams p) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= st.n_clusters) return;
+    const int ci = warp;
+    const int n = st.pl_count[ci];
+    if (n == 0) return;
+    const int sysi = st.cluster_sys[ci];
+    const float Lx = st.sys[sysi].boxf[0], Ly = st.sys[sysi].boxf[1], Lz = st.sys[sysi].boxf[2];
+    const int ii = lane & 7;
+    const int jj0 = lane >> 3;
+    const float4 xi = st.xyzq[ci * CLUSTER + ii];
+    const float2 lji = st.ljp[ci * CLUSTER + ii];
+    const float qi = xi.w * p.ke;
+    float fix = 0.f, fiy = 0.f, fiz = 0.f;
+    double e_lj = 0.0, e_c = 0.0, vir = 0.0;
+    const size_t base = (size_t)ci * st.pl_cap;
+    for (int k = 0; k < n; ++k) {
+        const int ent = st.pl_j[base + k];
+        const unsigned long long mask = st.pl_mask[base + k];
+        const int cj = ent & ((1 << JCLUSTER_BITS) - 1);
+        const int3 sh = decode_shift((unsigned)ent >> JCLUSTER_BITS);
+        const float sx = sh.x * Lx, sy = sh.y * Ly, sz = sh.z * Lz;
+        float fjx[2], fjy[2], fjz[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int jj = jj0 + 4 * h;
+            const float4 xj = st.xyzq[cj * CLUSTER + jj];
+            const float2 ljj = st.ljp[cj * CLUSTER + jj];
+            const float dx = xj.x + sx - xi.x;
+            const float dy = xj.y + sy - xi.y;
+            const float dz = xj.z + sz - xi.z;
+            const float r2 = dx * dx + dy * dy + dz * dz;
+            const bool on = ((mask >> (jj * 8 + ii)) & 1ull) && r2 <= p.rc2;
+            float fs = 0.f;
+            if (on) {
+                const float rinv = rsqrtf(r2);
+                const float rinv2 = rinv * rinv;
+                const float sig = lji.x + ljj.x;
+                const float eps = lji.y * ljj.y;
+                float s = sig * sig * rinv2;
+                s = s * s * s;
+                fs = 24.f * eps * s * rinv2 * (1.f - 2.f * s);
+                if (ENERGY) e_lj += (double)(4.f * eps * s * (s - 1.f));
+                if (ES != 0) {
+                    const float qq = qi * xj.w;
+                    float fc = qq * rinv2 * rinv;
+                    float ec = qq * rinv;
+                    if (ES == 2) {
+                        const float r = r2 * rinv;
+                        const float kr = p.kappa * r;
+                        const float erfc_kr = erfcf(kr);
+                        fc *= erfc_kr + p.two_kappa_sqrtpi * r * __expf(-kr * kr);
+                        ec *= erfc_kr;
+                    }
+                    fs -= fc;
+                    if (ENERGY) e_c += (double)ec;
+                }
+                if (p.em) fs = fmaxf(fminf(fs, 1e20f), -1e20f);
+                if (ENERGY) vir += 0.5 * (double)(fs * r2);  // -1/2 r_ij . f_ij
+            }
+            const float fx = fs * dx, fy = fs * dy, fz = fs * dz;
+            fix += fx;
+            fiy += fy;
+            fiz += fz;
+            fjx[h] = -fx;
+            fjy[h] = -fy;
+            fjz[h] = -fz;
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+#pragma unroll
+            for (int o = 1; o < 8; o <<= 1) {
+                fjx[h] += __shfl_xor_sync(0xffffffffu, fjx[h], o);
+                fjy[h] += __shfl_xor_sync(0xffffffffu, fjy[h], o);
+                fjz[h] += __shfl_xor_sync(0xffffffffu, fjz[h], o);
+            }
+        }
+        if (ii == 0) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int sj = cj * CLUSTER + jj0 + 4 * h;
+                atomic_add_fixed(st.fx + sj, to_fixed(fjx[h], FORCE_SCALE));
+                atomic_add_fixed(st.fy + sj, to_fixed(fjy[h], FORCE_SCALE));
+                atomic_add_fixed(st.fz + sj, to_fixed(fjz[h], FORCE_SCALE));
+            }
+        }
+    }
+    fix += __shfl_xor_sync(0xffffffffu, fix, 8);
+    fiy += __shfl_xor_sync(0xffffffffu, fiy, 8);
+    fiz += __shfl_xor_sync(0xffffffffu, fiz, 8);
+    fix += __shfl_xor_sync(0xffffffffu, fix, 16);
+    fiy += __shfl_xor_sync(0xffffffffu, fiy, 16);
+    fiz += __shfl_xor_sync(0xffffffffu, fiz, 16);
+    if (jj0 == 0) {
+        const int si = ci * CLUSTER + ii;
+        atomic_add_fixed(st.fx + si, to_fixed(fix, FORCE_SCALE));
+        atomic_add_fixed(st.fy + si, to_fixed(fiy, FORCE_SCALE));
+        atomic_add_fixed(st.fz + si, to_fixed(fiz, FORCE_SCALE));
+    }
+    if (ENERGY) {
+        e_lj = warp_sum(e_lj);
+        e_c = warp_sum(e_c);
+        vir = warp_sum(vir);
+        if (lane == 0) {
+            long long* E = st.energy + (size_t)sysi * E_COUNT;
+            atomic_add_fixed(E + E_LJ, to_fixed_d(e_lj, ENERGY_SCALE));
+            atomic_add_fixed(E + E_COUL, to_fixed_d(e_c, ENERGY_SCALE));
+            atomic_add_fixed(E + E_VIRIAL, to_fixed_d(vir, ENERGY_SCALE));
+        }
+    }
+}
+
+int launch_nonbonded(const DevState& st, const NbParams& p, bool energy, cudaStream_t s) {
+    const long long threads = (long long)st.n_clusters * 32;
+    const dim3 grid((unsigned)((threads + 255) / 256));
+#define NB_LAUNCH(ES)                                                       \
+    if (energy) k_nonbonded<ES, true><<<grid, 256, 0, s>>>(st, p);          \
+    else k_nonbonded<ES, false><<<grid, 256, 0, s>>>(st, p);
+    if (p.es_mode == 0) {
+        NB_LAUNCH(0)
+    } else if (p.es_mode == 1) {
+        NB_LAUNCH(1)
+    } else {
+        NB_LAUNCH(2)
+    }
+#undef NB_LAUNCH
+    return 1;
+}
+
+// Reciprocal-space exclusion correction for excluded charged pairs:
+// E = -k_e q_i q_j erf(kappa r)/r.  The reference applies none (PME.cuh has no
+// such term); this is the accurate-mode complement of the PME sum.
+template <bool ENERGY>
+__global__ void k_exclusion_correction(DevState st, BondedTerms bt, NbParams p) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    double e = 0.0;
+    int sysi = -1;
+    if (t < bt.nx) {
+        const int2 pr = bt.xidx[t];
+        const int si = st.slot_of[pr.x], sj = st.slot_of[pr.y];
+        sysi = st.atom_sys[pr.x];
+        const SysDesc& sd = st.sys[sysi];
+        double d[3] = {st.px[si] - st.px[sj], st.py[si] - st.py[sj], st.pz[si] - st.pz[sj]};
+        for (int k = 0; k < 3; ++k) d[k] -= sd.box[k] * rint(d[k] / sd.box[k]);
+        const float dx = (float)d[0], dy = (float)d[1], dz = (float)d[2];
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        const float rinv = rsqrtf(r2);
+        const float r = r2 * rinv;
+        const float kr = p.kappa * r;
+        const float qq = p.ke * st.xyzq[si].w * st.xyzq[sj].w;
+        const float erf_kr = erff(kr);
+        // E = -qq erf(kr)/r ; F_i = -dE/dr * (r_i - r_j)/r
+        const float dEdr = -qq * (p.two_kappa_sqrtpi * __expf(-kr * kr) * rinv - erf_kr * rinv * rinv);
+        const float fs = -dEdr * rinv;
+        const float fx = fs * dx, fy = fs * dy, fz = fs * dz;
+        atomic_add_fixed(st.fx + si, to_fixed(fx, FORCE_SCALE));
+        atomic_add_fixed(st.fy + si, to_fixed(fy, FORCE_SCALE));
+        atomic_add_fixed(st.fz + si, to_fixed(fz, FORCE_SCALE));
+        atomic_add_fixed(st.fx + sj, to_fixed(-fx, FORCE_SCALE));
+        atomic_add_fixed(st.fy + sj, to_fixed(-fy, FORCE_SCALE));
+        atomic_add_fixed(st.fz + sj, to_fixed(-fz, FORCE_SCALE));
+        if (ENERGY) e = -(double)qq * (double)erf_kr * (double)rinv;
+    }
+    if (ENERGY && sysi >= 0) {
+        atomic_add_fixed(st.energy + (size_t)sysi * E_COUNT + E_EXCL, to_fixed_d(e, ENERGY_SCALE));
+    }
+}
+
+int launch_exclusion_correction(const DevState& st, const BondedTerms& bt, const NbParams& p,
+                                bool energy, cudaStream_t s) {
+    if (bt.nx == 0) return 0;
+    const int TB = 256;
+    if (energy)
+        k_exclusion_correction<true><<<(bt.nx + TB - 1) / TB, TB, 0, s>>>(st, bt, p);
+    else
+        k_exclusion_correction<false><<<(bt.nx + TB - 1) / TB, TB, 0, s>>>(st, bt, p);
+    return 1;
+}
+
+// Writes every (orig_i, orig_j) pair the pair kernel evaluates (mask bit set and
+// r^2 <= rc^2) with i < j; order is not defined (the host sorts).
+__global__ void k_pairlist_dump(DevState st, NbParams p, long long cap, int* out,
+                                unsigned long long* count) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= st.n_clusters) return;
+    const int ci = warp;
+    const int n = st.pl_count[ci];
+    const int sysi = st.cluster_sys[ci];
+    const float Lx = st.sys[sysi].boxf[0], Ly = st.sys[sysi].boxf[1], Lz = st.sys[sysi].boxf[2];
+    const int ii = lane & 7, jj0 = lane >> 3;
+    const float4 xi = st.xyzq[ci * CLUSTER + ii];
+    const int ai = st.orig[ci * CLUSTER + ii];
+    const size_t base = (size_t)ci * st.pl_cap;
+    for (int k = 0; k < n; ++k) {
+        const int ent = st.pl_j[base + k];
+        const unsigned long long mask = st.pl_mask[base + k];
+        const int cj = ent & ((1 << JCLUSTER_BITS) - 1);
+        const int3 sh = decode_shift((unsigned)ent >> JCLUSTER_BITS);
+        for (int h = 0; h < 2; ++h) {
+            const int jj = jj0 + 4 * h;
+            const float4 xj = st.xyzq[cj * CLUSTER + jj];
+            const float dx = xj.x + sh.x * Lx - xi.x;
+            const float dy = xj.y + sh.y * Ly - xi.y;
+            const float dz = xj.z + sh.z * Lz - xi.z;
+            const float r2 = dx * dx + dy * dy + dz * dz;
+            if (((mask >> (jj * 8 + ii)) & 1ull) && r2 <= p.rc2) {
+                const int aj = st.orig[cj * CLUSTER + jj];
+                const unsigned long long w = atomicAdd(count, 1ull);
+                if ((long long)w < cap) {
+                    out[2 * w] = min(ai, aj);
+                    out[2 * w + 1] = max(ai, aj);
+                }
+            }
+        }
+    }
+}
+
+int launch_pairlist_dump(const DevState& st, const NbParams& p, long long cap, int* out_pairs,
+                         unsigned long long* out_count, cudaStream_t s) {
+    const long long threads = (long long)st.n_clusters * 32;
+    k_pairlist_dump<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(st, p, cap, out_pairs, out_count);
+    return 1;
+}
+
+}  // namespace lima

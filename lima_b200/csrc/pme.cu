@@ -1,0 +1,489 @@
+// pme.cu — smooth PME reciprocal space, order 4.
+//
+// Replaces PME::Controller::CalcCharges (code/LIMA_ENGINE/src/PME.cuh:574-608):
+//   DistributeCompoundchargesToBlocksKernel + ChargeblockDistributeToGrid (:172-333)
+//       -> k_spread: every atom adds q*w to its 4^3 grid nodes as int64 fixed
+//          point (the reference uses int32 fixed point in 1 nm^3 shared tiles
+//          for the same reason: an order-free, deterministic sum)
+//   cufftExecR2C / ApplyGreensFunctionKernel / cufftExecC2R / Normalize (:585-599)
+//       -> five shared-memory passes of a hand-written mixed-radix (2,3,4,5)
+//          Stockham FFT: x (real->half complex), y, z (forward, x theta(k),
+//          inverse, fused), y, x (half complex->real).  theta already holds
+//          the 1/N normalisation.
+//   InterpolateForcesAndPotentialKernel (:335-430)
+//       -> k_gather: analytic B-spline derivative (accurate mode) or the
+//          reference's central difference of the gridded potential.
+// B-spline weights sit on nodes floor(u)-1..floor(u)+2 exactly as in
+// ChargeblockDistributeToGrid (PME.cuh:249-300) and LAL::CalcBspline
+// (DeviceAlgorithmsPrivate.cuh:7-30).
+#include "engine.h"
+
+namespace lima {
+
+constexpr int FFT_MAXN = 256;
+constexpr int FFT_TX = 16;      // columns per y/z tile
+constexpr int FFT_XLINES = 8;   // lines per x-pass CTA
+
+struct FftPlanDev {
+    int n;
+    int nrad;
+    int rad[12];
+};
+
+struct PmeSysDev {
+    FftPlanDev px, py, pz;
+};
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+// multiply by sigma*i
+__device__ __forceinline__ float2 mul_si(float2 a, float sigma) { return make_float2(-sigma * a.y, sigma * a.x); }
+
+// R-point DFT in registers; sigma = -1 forward, +1 inverse
+template <int R>
+__device__ __forceinline__ void small_dft(float2* v, float sigma) {
+    if (R == 2) {
+        const float2 a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    } else if (R == 3) {
+        const float s3 = 0.86602540378443865f;
+        const float2 a = cadd(v[1], v[2]), b = csub(v[1], v[2]);
+        const float2 m = csub(v[0], cscale(a, 0.5f));
+        const float2 t = mul_si(b, sigma * s3);
+        v[0] = cadd(v[0], a);
+        v[1] = cadd(m, t);
+        v[2] = csub(m, t);
+    } else if (R == 4) {
+        const float2 t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
+        const float2 t2 = cadd(v[1], v[3]), t3 = mul_si(csub(v[1], v[3]), sigma);
+        v[0] = cadd(t0, t2);
+        v[2] = csub(t0, t2);
+        v[1] = cadd(t1, t3);
+        v[3] = csub(t1, t3);
+    } else if (R == 5) {
+        const float c1 = 0.30901699437494742f, c2 = -0.80901699437494742f;
+        const float s1 = 0.95105651629515357f, s2 = 0.58778525229247313f;
+        const float2 a1 = cadd(v[1], v[4]), b1 = csub(v[1], v[4]);
+        const float2 a2 = cadd(v[2], v[3]), b2 = csub(v[2], v[3]);
+        const float2 x0 = v[0];
+        const float2 m1 = cadd(x0, cadd(cscale(a1, c1), cscale(a2, c2)));
+        const float2 m2 = cadd(x0, cadd(cscale(a1, c2), cscale(a2, c1)));
+        const float2 n1 = mul_si(cadd(cscale(b1, s1), cscale(b2, s2)), sigma);
+        const float2 n2 = mul_si(csub(cscale(b1, s2), cscale(b2, s1)), sigma);
+        v[0] = cadd(x0, cadd(a1, a2));
+        v[1] = cadd(m1, n1);
+        v[4] = csub(m1, n1);
+        v[2] = cadd(m2, n2);
+        v[3] = csub(m2, n2);
+    }
+}
+
+template <int R>
+__device__ __forceinline__ void stockham_stage(const float2* src, float2* dst, int nlines, int stride,
+                                               int N, int Ns, const float2* tw, float sigma) {
+    const int nb = N / R;
+    const int total = nlines * nb;
+    const int tscale = N / (Ns * R);
+    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+        const int line = idx / nb;
+        const int j = idx - line * nb;
+        const float2* in = src + line * stride;
+        float2* out = dst + line * stride;
+        const int jm = j % Ns;
+        float2 v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[r] = in[j + r * nb];
+        const int tstep = jm * tscale;
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+            float2 w = tw[(tstep * r) % N];
+            w.y *= -sigma;  // table holds e^{-2 pi i k/N}; conjugate for the inverse
+            v[r] = cmul(v[r], w);
+        }
+        small_dft<R>(v, sigma);
+        const int base = (j - jm) * R + jm;
+#pragma unroll
+        for (int r = 0; r < R; ++r) out[base + r * Ns] = v[r];
+    }
+}
+
+// FFT of nlines lines (length pl.n, line stride `stride`) held in smem buffer a;
+// b is scratch of the same size.  Returns the buffer holding the result.
+__device__ float2* fft_lines(float2* a, float2* b, int nlines, int stride, const FftPlanDev& pl,
+                             const float2* tw, float sigma) {
+    float2* src = a;
+    float2* dst = b;
+    int Ns = 1;
+    for (int s = 0; s < pl.nrad; ++s) {
+        const int R = pl.rad[s];
+        switch (R) {
+            case 2: stockham_stage<2>(src, dst, nlines, stride, pl.n, Ns, tw, sigma); break;
+            case 3: stockham_stage<3>(src, dst, nlines, stride, pl.n, Ns, tw, sigma); break;
+            case 4: stockham_stage<4>(src, dst, nlines, stride, pl.n, Ns, tw, sigma); break;
+            default: stockham_stage<5>(src, dst, nlines, stride, pl.n, Ns, tw, sigma); break;
+        }
+        __syncthreads();
+        float2* t = src;
+        src = dst;
+        dst = t;
+        Ns *= R;
+    }
+    return src;
+}
+
+__device__ void make_twiddles(float2* tw, int n) {
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        double s, c;
+        sincospi(2.0 * k / n, &s, &c);
+        tw[k] = make_float2((float)c, (float)-s);
+    }
+}
+
+// ------------------------------------------------------------------ spread
+__device__ __forceinline__ void bspline4(float f, float* w) {
+    const float g = 1.f - f;
+    w[0] = g * g * g * (1.f / 6.f);
+    w[1] = (4.f - 6.f * f * f + 3.f * f * f * f) * (1.f / 6.f);
+    w[2] = (1.f + 3.f * f + 3.f * f * f - 3.f * f * f * f) * (1.f / 6.f);
+    w[3] = f * f * f * (1.f / 6.f);
+}
+__device__ __forceinline__ void bspline4_d(float f, float* dw) {
+    const float g = 1.f - f;
+    dw[0] = -0.5f * g * g;
+    dw[1] = -2.f * f + 1.5f * f * f;
+    dw[2] = 0.5f + f - 1.5f * f * f;
+    dw[3] = 0.5f * f * f;
+}
+
+__device__ __forceinline__ int wrapk(int i, int n) {
+    i %= n;
+    return i < 0 ? i + n : i;
+}
+
+// grid coordinate in [0,K): integer base and fraction
+__device__ __forceinline__ void grid_coord(float x, float inv_h, int K, int& base, float& frac) {
+    float u = x * inv_h;
+    u -= (float)K * floorf(u / (float)K);
+    float fl = floorf(u);
+    base = (int)fl;
+    frac = u - fl;
+    if (base >= K) base -= K;
+}
+
+__global__ void k_spread(DevState st) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= st.n_slots) return;
+    const float4 p = st.xyzq[s];
+    if (p.w == 0.f || st.orig[s] < 0) return;
+    const SysDesc& sd = st.sys[st.cluster_sys[s / CLUSTER]];
+    if (sd.pme_n[0] == 0) return;
+    const int K0 = sd.pme_n[0], K1 = sd.pme_n[1], K2 = sd.pme_n[2];
+    int b0, b1, b2;
+    float f0, f1, f2;
+    grid_coord(p.x, sd.pme_inv_h[0], K0, b0, f0);
+    grid_coord(p.y, sd.pme_inv_h[1], K1, b1, f1);
+    grid_coord(p.z, sd.pme_inv_h[2], K2, b2, f2);
+    float wx[4], wy[4], wz[4];
+    bspline4(f0, wx);
+    bspline4(f1, wy);
+    bspline4(f2, wz);
+    long long* g = st.pme_grid_fx + sd.pme_off;
+    int ix[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) ix[a] = wrapk(b0 - 1 + a, K0);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const int z = wrapk(b2 - 1 + c, K2);
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int y = wrapk(b1 - 1 + b, K1);
+            const float qyz = p.w * wy[b] * wz[c];
+            long long* row = g + (size_t)K0 * (y + (size_t)K1 * z);
+#pragma unroll
+            for (int a = 0; a < 4; ++a) atomic_add_fixed(row + ix[a], to_fixed(qyz * wx[a], GRID_SCALE));
+        }
+    }
+}
+
+// ------------------------------------------------------------- FFT passes
+// x pass forward: int64 charge grid -> half-complex rows (and zero the int64 grid)
+__global__ void k_fft_x_fwd(DevState st, const PmeSysDev* plans, const int4* items, int maxn) {
+    extern __shared__ float2 sm[];
+    const int4 it = items[blockIdx.x];
+    const SysDesc& sd = st.sys[it.x];
+    const FftPlanDev& pl = plans[it.x].px;
+    const int K0 = pl.n, K0h = K0 / 2 + 1;
+    const int stride = K0 | 1;
+    float2* tw = sm;
+    float2* A = sm + maxn;
+    float2* B = A + FFT_XLINES * (maxn + 1);
+    make_twiddles(tw, K0);
+    const int nl = it.z;
+    long long* g = st.pme_grid_fx + sd.pme_off + (size_t)it.y * K0;
+    for (int i = threadIdx.x; i < nl * K0; i += blockDim.x) {
+        const int l = i / K0, x = i - l * K0;
+        long long* cell = g + (size_t)l * K0 + x;
+        A[l * stride + x] = make_float2((float)((double)*cell * (1.0 / GRID_SCALE)), 0.f);
+        *cell = 0;
+    }
+    __syncthreads();
+    const float2* res = fft_lines(A, B, nl, stride, pl, tw, -1.f);
+    float2* out = st.pme_cplx + sd.pme_coff + (size_t)it.y * K0h;
+    for (int i = threadIdx.x; i < nl * K0h; i += blockDim.x) {
+        const int l = i / K0h, k = i - l * K0h;
+        out[(size_t)l * K0h + k] = res[l * stride + k];
+    }
+}
+
+// x pass inverse: half-complex rows -> real potential rows
+__global__ void k_fft_x_inv(DevState st, const PmeSysDev* plans, const int4* items, int maxn) {
+    extern __shared__ float2 sm[];
+    const int4 it = items[blockIdx.x];
+    const SysDesc& sd = st.sys[it.x];
+    const FftPlanDev& pl = plans[it.x].px;
+    const int K0 = pl.n, K0h = K0 / 2 + 1;
+    const int stride = K0 | 1;
+    float2* tw = sm;
+    float2* A = sm + maxn;
+    float2* B = A + FFT_XLINES * (maxn + 1);
+    make_twiddles(tw, K0);
+    const int nl = it.z;
+    const float2* in = st.pme_cplx + sd.pme_coff + (size_t)it.y * K0h;
+    for (int i = threadIdx.x; i < nl * K0; i += blockDim.x) {
+        const int l = i / K0, k = i - l * K0;
+        float2 v;
+        if (k < K0h) {
+            v = in[(size_t)l * K0h + k];
+        } else {
+            v = in[(size_t)l * K0h + (K0 - k)];
+            v.y = -v.y;  // Hermitian symmetry of a real signal
+        }
+        A[l * stride + k] = v;
+    }
+    __syncthreads();
+    const float2* res = fft_lines(A, B, nl, stride, pl, tw, 1.f);
+    float* out = st.pme_real + sd.pme_off + (size_t)it.y * K0;
+    for (int i = threadIdx.x; i < nl * K0; i += blockDim.x) {
+        const int l = i / K0, x = i - l * K0;
+        out[(size_t)l * K0 + x] = res[l * stride + x].x;
+    }
+}
+
+// y pass (either direction): tile of FFT_TX half-complex columns x all y, at one z
+__global__ void k_fft_y(DevState st, const PmeSysDev* plans, const int4* items, float sigma, int maxn) {
+    extern __shared__ float2 sm[];
+    const int4 it = items[blockIdx.x];
+    const SysDesc& sd = st.sys[it.x];
+    const FftPlanDev& pl = plans[it.x].py;
+    const int K0h = plans[it.x].px.n / 2 + 1, K1 = pl.n;
+    const int stride = K1 | 1;
+    float2* tw = sm;
+    float2* A = sm + maxn;
+    float2* B = A + FFT_TX * (maxn + 1);
+    make_twiddles(tw, K1);
+    const int x0 = it.y, z = it.z;
+    const int tx = min(FFT_TX, K0h - x0);
+    float2* g = st.pme_cplx + sd.pme_coff + (size_t)z * K1 * K0h + x0;
+    for (int i = threadIdx.x; i < K1 * FFT_TX; i += blockDim.x) {
+        const int y = i / FFT_TX, c = i - y * FFT_TX;
+        A[c * stride + y] = c < tx ? g[(size_t)y * K0h + c] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    const float2* res = fft_lines(A, B, FFT_TX, stride, pl, tw, sigma);
+    for (int i = threadIdx.x; i < K1 * FFT_TX; i += blockDim.x) {
+        const int y = i / FFT_TX, c = i - y * FFT_TX;
+        if (c < tx) g[(size_t)y * K0h + c] = res[c * stride + y];
+    }
+}
+
+// z pass: forward FFT along z, multiply by theta(k), inverse FFT along z
+__global__ void k_fft_z_conv(DevState st, const PmeSysDev* plans, const int4* items, int maxn) {
+    extern __shared__ float2 sm[];
+    const int4 it = items[blockIdx.x];
+    const SysDesc& sd = st.sys[it.x];
+    const FftPlanDev& pl = plans[it.x].pz;
+    const int K0h = plans[it.x].px.n / 2 + 1, K1 = plans[it.x].py.n, K2 = pl.n;
+    const int stride = K2 | 1;
+    float2* tw = sm;
+    float2* A = sm + maxn;
+    float2* B = A + FFT_TX * (maxn + 1);
+    make_twiddles(tw, K2);
+    const int x0 = it.y, y = it.z;
+    const int tx = min(FFT_TX, K0h - x0);
+    const size_t plane = (size_t)K1 * K0h;
+    float2* g = st.pme_cplx + sd.pme_coff + (size_t)y * K0h + x0;
+    const float* th = st.pme_theta + sd.pme_coff + (size_t)y * K0h + x0;
+    for (int i = threadIdx.x; i < K2 * FFT_TX; i += blockDim.x) {
+        const int z = i / FFT_TX, c = i - z * FFT_TX;
+        A[c * stride + z] = c < tx ? g[z * plane + c] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    float2* res = fft_lines(A, B, FFT_TX, stride, pl, tw, -1.f);
+    for (int i = threadIdx.x; i < K2 * FFT_TX; i += blockDim.x) {
+        const int z = i / FFT_TX, c = i - z * FFT_TX;
+        const float t = c < tx ? th[z * plane + c] : 0.f;
+        res[c * stride + z] = cscale(res[c * stride + z], t);
+    }
+    __syncthreads();
+    float2* other = res == A ? B : A;
+    const float2* res2 = fft_lines(res, other, FFT_TX, stride, pl, tw, 1.f);
+    for (int i = threadIdx.x; i < K2 * FFT_TX; i += blockDim.x) {
+        const int z = i / FFT_TX, c = i - z * FFT_TX;
+        if (c < tx) g[z * plane + c] = res2[c * stride + z];
+    }
+}
+
+// ------------------------------------------------------------------ gather
+template <bool ENERGY, bool FD>
+__global__ void k_gather(DevState st) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    double e = 0.0;
+    int sysi = -1;
+    if (s < st.n_slots) {
+        const float4 p = st.xyzq[s];
+        const int sy = st.cluster_sys[s / CLUSTER];
+        const SysDesc& sd = st.sys[sy];
+        if (p.w != 0.f && st.orig[s] >= 0 && sd.pme_n[0] != 0) {
+            sysi = sy;
+            const int K0 = sd.pme_n[0], K1 = sd.pme_n[1], K2 = sd.pme_n[2];
+            int b0, b1, b2;
+            float f0, f1, f2;
+            grid_coord(p.x, sd.pme_inv_h[0], K0, b0, f0);
+            grid_coord(p.y, sd.pme_inv_h[1], K1, b1, f1);
+            grid_coord(p.z, sd.pme_inv_h[2], K2, b2, f2);
+            float wx[4], wy[4], wz[4], dx[4], dy[4], dz[4];
+            bspline4(f0, wx);
+            bspline4(f1, wy);
+            bspline4(f2, wz);
+            bspline4_d(f0, dx);
+            bspline4_d(f1, dy);
+            bspline4_d(f2, dz);
+            const float* g = st.pme_real + sd.pme_off;
+            int ix[4], ixp[4], ixm[4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                ix[a] = wrapk(b0 - 1 + a, K0);
+                ixp[a] = wrapk(b0 + a, K0);
+                ixm[a] = wrapk(b0 - 2 + a, K0);
+            }
+            float phi = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const int z = wrapk(b2 - 1 + c, K2);
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    const int y = wrapk(b1 - 1 + b, K1);
+                    const float* row = g + (size_t)K0 * (y + (size_t)K1 * z);
+#pragma unroll
+                    for (int a = 0; a < 4; ++a) {
+                        const float v = row[ix[a]];
+                        const float w = wx[a] * wy[b] * wz[c];
+                        phi += w * v;
+                        if (FD) {
+                            const int yp = wrapk(y + 1, K1), ym = wrapk(y - 1, K1);
+                            const int zp = wrapk(z + 1, K2), zm = wrapk(z - 1, K2);
+                            gx += w * (row[ixp[a]] - row[ixm[a]]);
+                            gy += w * (g[(size_t)K0 * (yp + (size_t)K1 * z) + ix[a]] -
+                                       g[(size_t)K0 * (ym + (size_t)K1 * z) + ix[a]]);
+                            gz += w * (g[(size_t)K0 * (y + (size_t)K1 * zp) + ix[a]] -
+                                       g[(size_t)K0 * (y + (size_t)K1 * zm) + ix[a]]);
+                        } else {
+                            gx += dx[a] * wy[b] * wz[c] * v;
+                            gy += wx[a] * dy[b] * wz[c] * v;
+                            gz += wx[a] * wy[b] * dz[c] * v;
+                        }
+                    }
+                }
+            }
+            const float sc0 = FD ? 0.5f * sd.pme_inv_h[0] : sd.pme_inv_h[0];
+            const float sc1 = FD ? 0.5f * sd.pme_inv_h[1] : sd.pme_inv_h[1];
+            const float sc2 = FD ? 0.5f * sd.pme_inv_h[2] : sd.pme_inv_h[2];
+            atomic_add_fixed(st.fx + s, to_fixed(-p.w * gx * sc0, FORCE_SCALE));
+            atomic_add_fixed(st.fy + s, to_fixed(-p.w * gy * sc1, FORCE_SCALE));
+            atomic_add_fixed(st.fz + s, to_fixed(-p.w * gz * sc2, FORCE_SCALE));
+            if (ENERGY) e = 0.5 * (double)p.w * (double)phi;
+        }
+    }
+    if (ENERGY) {
+        const int s_first = __shfl_sync(0xffffffffu, sysi, 0);
+        const bool uniform = __all_sync(0xffffffffu, sysi == s_first || sysi < 0);
+        const int sref = __reduce_max_sync(0xffffffffu, sysi);
+        if (uniform) {
+            e = warp_sum(e);
+            if ((threadIdx.x & 31) == 0 && sref >= 0)
+                atomic_add_fixed(st.energy + (size_t)sref * E_COUNT + E_RECIP, to_fixed_d(e, ENERGY_SCALE));
+        } else if (sysi >= 0) {
+            atomic_add_fixed(st.energy + (size_t)sysi * E_COUNT + E_RECIP, to_fixed_d(e, ENERGY_SCALE));
+        }
+    }
+}
+
+// ------------------------------------------------------------------ driver
+static size_t fft_smem_bytes(int lines, int maxn) {
+    return (size_t)(maxn + 2 * lines * (maxn + 1)) * sizeof(float2);
+}
+
+int launch_pme(const DevState& st, const PmePlan& plan, bool energy, cudaStream_t s) {
+    if (plan.n_items_x == 0) return 0;
+    const PmeSysDev* plans = reinterpret_cast<const PmeSysDev*>(plan.sys_plans);
+    const int TB = 256;
+    const int mx = plan.max_n;
+    const size_t sx = fft_smem_bytes(FFT_XLINES, mx), sy = fft_smem_bytes(FFT_TX, mx);
+    k_spread<<<(st.n_slots + TB - 1) / TB, TB, 0, s>>>(st);
+    k_fft_x_fwd<<<plan.n_items_x, 256, sx, s>>>(st, plans, plan.items_x, mx);
+    k_fft_y<<<plan.n_items_y, 256, sy, s>>>(st, plans, plan.items_y, -1.f, mx);
+    k_fft_z_conv<<<plan.n_items_z, 256, sy, s>>>(st, plans, plan.items_z, mx);
+    k_fft_y<<<plan.n_items_y, 256, sy, s>>>(st, plans, plan.items_y, 1.f, mx);
+    k_fft_x_inv<<<plan.n_items_x, 256, sx, s>>>(st, plans, plan.items_x, mx);
+    const int g = (st.n_slots + TB - 1) / TB;
+    if (plan.ref_gather) {
+        if (energy) k_gather<true, true><<<g, TB, 0, s>>>(st);
+        else k_gather<false, true><<<g, TB, 0, s>>>(st);
+    } else {
+        if (energy) k_gather<true, false><<<g, TB, 0, s>>>(st);
+        else k_gather<false, false><<<g, TB, 0, s>>>(st);
+    }
+    return 7;
+}
+
+// Host helper: radix plan for an FFT length (4s first, then 2, 3, 5).
+bool make_fft_plan(int n, FftPlanDev* out) {
+    if (n < 2 || n > FFT_MAXN) return false;
+    out->n = n;
+    out->nrad = 0;
+    int m = n;
+    while (m % 4 == 0) {
+        out->rad[out->nrad++] = 4;
+        m /= 4;
+    }
+    for (int p : {2, 3, 5}) {
+        while (m % p == 0) {
+            if (out->nrad >= 12) return false;
+            out->rad[out->nrad++] = p;
+            m /= p;
+        }
+    }
+    return m == 1;
+}
+
+size_t pme_sys_dev_size() { return sizeof(PmeSysDev); }
+
+bool fill_pme_sys_dev(void* dst, int kx, int ky, int kz) {
+    PmeSysDev* d = reinterpret_cast<PmeSysDev*>(dst);
+    return make_fft_plan(kx, &d->px) && make_fft_plan(ky, &d->py) && make_fft_plan(kz, &d->pz);
+}
+
+void pme_set_smem_limits(int maxn) {
+    const int by = (int)fft_smem_bytes(FFT_TX, maxn), bx = (int)fft_smem_bytes(FFT_XLINES, maxn);
+    cudaFuncSetAttribute(k_fft_y, cudaFuncAttributeMaxDynamicSharedMemorySize, by);
+    cudaFuncSetAttribute(k_fft_z_conv, cudaFuncAttributeMaxDynamicSharedMemorySize, by);
+    cudaFuncSetAttribute(k_fft_x_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, bx);
+    cudaFuncSetAttribute(k_fft_x_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, bx);
+}
+
+}  // namespace lima

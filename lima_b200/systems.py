@@ -1,0 +1,383 @@
+"""Seeded synthetic systems for the force/integration path.
+
+The reference's benchmark inputs live in an external data directory that is
+not distributed, so every workload here is generated from a seed with the
+shapes, sizes and parameter distributions of the named configurations.
+
+Units are LIMA's own (code/LIMA_BASE/include/Constants.h:43-60): nm, ns,
+kg/mol, kC/mol, J/mol.  Exclusions follow the reference rule that every atom
+pair sharing a bonded term is excluded from LJ and Coulomb
+(code/LIMA_TOOLS/src/CompoundBuilder.cpp:40-60).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+E_TO_KCMOL = 1.602176634e-19 * 6.02214076e23 / 1000.0   # Constants.h:60
+KB_J_MOL_K = 1.380649e-23 * 6.02214076e23               # J/mol/K
+KJ = 1000.0                                              # kJ -> J (Forcefield.cpp:341-347)
+DEG = math.pi / 180.0
+
+# flexible 3-site water (all sizes in LIMA units)
+WATER = dict(r_oh=0.09572, theta=104.52 * DEG, kb=345000.0 * KJ, kth=383.0 * KJ,
+             q_o=-0.834 * E_TO_KCMOL, q_h=0.417 * E_TO_KCMOL,
+             sig_o=0.3151, eps_o=0.6364 * KJ, m_o=15.9994e-3, m_h=1.008e-3)
+
+
+@dataclass
+class System:
+    """Flat description of one system, in the reference's units."""
+    box: np.ndarray                       # (3,) nm
+    pos: np.ndarray                       # (n,3) float64 nm
+    vel: np.ndarray                       # (n,3) float32 nm/ns
+    charge: np.ndarray                    # (n,) float32 kC/mol
+    mass: np.ndarray                      # (n,) float32 kg/mol
+    sigma: np.ndarray                     # (n,) float32 nm
+    epsilon: np.ndarray                   # (n,) float32 J/mol
+    bonds: np.ndarray = field(default_factory=lambda: np.zeros((0, 2), np.int32))
+    bond_par: np.ndarray = field(default_factory=lambda: np.zeros((0, 2), np.float32))
+    angles: np.ndarray = field(default_factory=lambda: np.zeros((0, 3), np.int32))
+    angle_par: np.ndarray = field(default_factory=lambda: np.zeros((0, 4), np.float32))
+    dihedrals: np.ndarray = field(default_factory=lambda: np.zeros((0, 4), np.int32))
+    dihedral_par: np.ndarray = field(default_factory=lambda: np.zeros((0, 3), np.float32))
+    impropers: np.ndarray = field(default_factory=lambda: np.zeros((0, 4), np.int32))
+    improper_par: np.ndarray = field(default_factory=lambda: np.zeros((0, 2), np.float32))
+    pairbonds: np.ndarray = field(default_factory=lambda: np.zeros((0, 2), np.int32))
+    pair_par: np.ndarray = field(default_factory=lambda: np.zeros((0, 2), np.float32))
+    name: str = ""
+
+    @property
+    def n(self) -> int:
+        return len(self.pos)
+
+    def exclusions(self) -> np.ndarray:
+        """Unique (i<j) atom pairs sharing any bond, angle, dihedral or improper."""
+        pairs = []
+        for terms in (self.bonds, self.angles, self.dihedrals, self.impropers):
+            t = np.asarray(terms)
+            if len(t) == 0:
+                continue
+            t = t.reshape(len(t), -1)
+            k = t.shape[1]
+            for a in range(k):
+                for b in range(a + 1, k):
+                    pairs.append(np.stack([t[:, a], t[:, b]], 1))
+        if not pairs:
+            return np.zeros((0, 2), np.int32)
+        p = np.concatenate(pairs).astype(np.int64)
+        p = np.sort(p, axis=1)
+        p = p[p[:, 0] != p[:, 1]]
+        p = np.unique(p, axis=0)
+        return p.astype(np.int32)
+
+
+def _random_rotations(rng: np.random.Generator, n: int) -> np.ndarray:
+    """Uniform random rotation matrices from uniform unit quaternions."""
+    q = rng.normal(size=(n, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    w, x, y, z = q.T
+    return np.stack([
+        np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)], -1),
+        np.stack([2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)], -1),
+        np.stack([2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)], -1),
+    ], 1)
+
+
+def maxwell_boltzmann(rng: np.random.Generator, mass: np.ndarray, temperature: float) -> np.ndarray:
+    """Velocities [nm/ns == m/s] at temperature [K] with the centre-of-mass motion removed."""
+    sd = np.sqrt(KB_J_MOL_K * temperature / mass.astype(np.float64))
+    v = rng.normal(size=(len(mass), 3)) * sd[:, None]
+    com = (v * mass[:, None]).sum(0) / mass.sum()
+    return (v - com).astype(np.float32)
+
+
+def _water_template() -> np.ndarray:
+    r, th = WATER["r_oh"], WATER["theta"]
+    h = th / 2
+    return np.array([[0.0, 0.0, 0.0],
+                     [r * math.sin(h), 0.0, r * math.cos(h)],
+                     [-r * math.sin(h), 0.0, r * math.cos(h)]])
+
+
+def _orient_waters(rng, centres: np.ndarray, fixed: np.ndarray | None, box: np.ndarray,
+                   min_dist: float = 0.17, rounds: int = 60) -> np.ndarray:
+    """Random orientations, redrawn for waters with an atom closer than
+    min_dist to an atom of another molecule (H atoms carry no LJ, so such
+    contacts would blow up the first steps)."""
+    from scipy.spatial import cKDTree
+
+    nw = len(centres)
+    tmpl = _water_template()
+    rot = _random_rotations(rng, nw)
+    nfix = 0 if fixed is None else len(fixed)
+    for _ in range(rounds):
+        pos = (np.einsum("nij,aj->nai", rot, tmpl) + centres[:, None, :]).reshape(-1, 3)
+        allp = pos if nfix == 0 else np.concatenate([fixed, pos])
+        tree = cKDTree(np.mod(allp, box), boxsize=box)
+        pairs = tree.query_pairs(min_dist, output_type="ndarray")
+        mol = np.concatenate([-1 - np.arange(nfix), np.repeat(np.arange(nw), 3)])
+        if len(pairs):
+            pairs = pairs[mol[pairs[:, 0]] != mol[pairs[:, 1]]]
+        if len(pairs) == 0:
+            break
+        bad = np.unique(mol[pairs.ravel()])
+        bad = bad[bad >= 0]
+        rot[bad] = _random_rotations(rng, len(bad))
+    return rot
+
+
+def _append_waters(rng, centres: np.ndarray, first_atom: int, box=None, fixed=None):
+    """Atoms, bonds and angles for waters whose oxygens sit at centres."""
+    nw = len(centres)
+    if box is None:
+        rot = _random_rotations(rng, nw)
+    else:
+        rot = _orient_waters(rng, centres, fixed, np.asarray(box, dtype=np.float64))
+    tmpl = _water_template()
+    pos = (np.einsum("nij,aj->nai", rot, tmpl) + centres[:, None, :]).reshape(-1, 3)
+    base = first_atom + 3 * np.arange(nw)
+    bonds = np.concatenate([np.stack([base, base + 1], 1), np.stack([base, base + 2], 1)])
+    bonds = bonds.reshape(2, nw, 2).transpose(1, 0, 2).reshape(-1, 2)
+    angles = np.stack([base + 1, base, base + 2], 1)
+    q = np.tile([WATER["q_o"], WATER["q_h"], WATER["q_h"]], nw)
+    m = np.tile([WATER["m_o"], WATER["m_h"], WATER["m_h"]], nw)
+    s = np.tile([WATER["sig_o"], 0.0, 0.0], nw)
+    e = np.tile([WATER["eps_o"], 0.0, 0.0], nw)
+    bpar = np.tile([WATER["r_oh"], WATER["kb"]], (len(bonds), 1))
+    apar = np.tile([WATER["theta"], WATER["kth"], 0.0, 0.0], (nw, 1))
+    return pos, q, m, s, e, bonds, bpar, angles, apar
+
+
+def solvate_sites(rng, box: np.ndarray, occupied: np.ndarray, n_waters: int, clearance: float = 0.3,
+                  jitter: float = 0.02) -> np.ndarray:
+    """n_waters oxygen sites on a jittered cubic lattice that keep `clearance`
+    from occupied atoms; the lattice is refined until enough sites are free."""
+    from scipy.spatial import cKDTree
+
+    tree = cKDTree(np.mod(occupied, box), boxsize=box)
+    free_vol = float(np.prod(box)) * 0.6
+    spacing = (free_vol / n_waters) ** (1.0 / 3.0)
+    for _ in range(60):
+        n = np.maximum(1, np.floor(box / spacing)).astype(int)
+        g = [(np.arange(n[d]) + 0.5) * box[d] / n[d] for d in range(3)]
+        sites = np.stack(np.meshgrid(*g, indexing="ij"), -1).reshape(-1, 3)
+        d, _ = tree.query(sites, k=1)
+        sites = sites[d > clearance]
+        if len(sites) >= n_waters:
+            sites = sites[np.sort(rng.choice(len(sites), n_waters, replace=False))]
+            return sites + rng.uniform(-jitter, jitter, size=sites.shape)
+        spacing *= 0.985
+    raise RuntimeError("cannot place the requested number of waters")
+
+
+def _lattice_sites(n_per_dim, box, jitter, rng):
+    g = (np.arange(n_per_dim) + 0.5) / n_per_dim
+    pts = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3) * box
+    return pts + rng.uniform(-jitter, jitter, size=pts.shape)
+
+
+def water_box(n_waters: int, box_nm: float, seed: int = 20241203, jitter: float = 0.02,
+              temperature: float = 300.0, name: str = "water") -> System:
+    """Flexible 3-site waters on a jittered cubic lattice (config 0 and 2)."""
+    rng = np.random.default_rng(seed)
+    box = np.array([box_nm] * 3, dtype=np.float64)
+    per = int(math.ceil(n_waters ** (1.0 / 3.0) - 1e-9))
+    sites = _lattice_sites(per, box, jitter, rng)
+    if len(sites) > n_waters:
+        sites = sites[np.sort(rng.choice(len(sites), n_waters, replace=False))]
+    pos, q, m, s, e, bonds, bpar, angles, apar = _append_waters(rng, sites, 0, box=box)
+    pos = np.mod(pos, box)
+    vel = maxwell_boltzmann(rng, m, temperature)
+    return System(box=box, pos=pos, vel=vel, charge=q.astype(np.float32), mass=m.astype(np.float32),
+                  sigma=s.astype(np.float32), epsilon=e.astype(np.float32),
+                  bonds=bonds.astype(np.int32), bond_par=bpar.astype(np.float32),
+                  angles=angles.astype(np.int32), angle_par=apar.astype(np.float32), name=name)
+
+
+# ------------------------------------------------------------ lipid-like chains
+CHAIN_HEAD = 8
+CHAIN_TAIL = 22
+CHAIN_ATOMS = CHAIN_HEAD + 2 * CHAIN_TAIL   # 52
+CHAIN = dict(b0=0.153, kb=2.2e5 * KJ, theta0=111.0 * DEG, kth=460.0 * KJ, kphi=0.6 * KJ, mult=3.0,
+             phi0=0.0, mass=12.011e-3)
+
+
+def chain_topology():
+    """Bond graph of one 52-atom chain: an 8-atom linear head (0..7), tail A
+    (8..29) attached to head atom 5 and tail B (30..51) to head atom 7; every
+    angle and proper dihedral along the bond paths."""
+    bonds = [(i, i + 1) for i in range(CHAIN_HEAD - 1)]
+    a0, b0 = CHAIN_HEAD, CHAIN_HEAD + CHAIN_TAIL
+    bonds.append((5, a0))
+    bonds += [(a0 + i, a0 + i + 1) for i in range(CHAIN_TAIL - 1)]
+    bonds.append((7, b0))
+    bonds += [(b0 + i, b0 + i + 1) for i in range(CHAIN_TAIL - 1)]
+    nb = [[] for _ in range(CHAIN_ATOMS)]
+    for i, j in bonds:
+        nb[i].append(j)
+        nb[j].append(i)
+    angles = []
+    for j in range(CHAIN_ATOMS):
+        for x in range(len(nb[j])):
+            for y in range(x + 1, len(nb[j])):
+                angles.append((nb[j][x], j, nb[j][y]))
+    dihedrals = []
+    for j, k in bonds:
+        for i in nb[j]:
+            if i == k:
+                continue
+            for l in nb[k]:
+                if l == j or l == i:
+                    continue
+                dihedrals.append((i, j, k, l))
+    return (np.array(bonds, np.int32), np.array(angles, np.int32), np.array(dihedrals, np.int32))
+
+
+def _chain_geometry(up: bool, half: float) -> np.ndarray:
+    """One chain around the origin.  Each tail is a hairpin of two all-trans
+    strands; the four strands of a chain sit at (+-half, +-half) in x-y.  The
+    8 head atoms lie just beyond the strand tops, above (upper leaflet) or
+    below them."""
+    b = CHAIN["b0"]
+    hang = CHAIN["theta0"] / 2
+    dz = b * math.sin(hang)           # axial advance per bond of an all-trans strand
+    zz = 0.5 * b * math.cos(hang)     # lateral zig-zag amplitude
+    sgn = -1.0 if up else 1.0         # tails grow away from the head
+    strand = CHAIN_TAIL // 2
+    pos = np.zeros((CHAIN_ATOMS, 3))
+    # head: a 2 x 4 snake just beyond the tail tops; atom 5 sits over tail A's
+    # first strand (+half, +half) and atom 7 over tail B's (-half, +half)
+    snake = [(-0.1, -0.3), (0.1, -0.3), (0.1, -0.1), (-0.1, -0.1), (-0.1, 0.1), (0.1, 0.1), (0.1, 0.3), (-0.1, 0.3)]
+    for i, (hx, hy) in enumerate(snake):
+        pos[i] = [hx, hy, -sgn * 0.2]
+    for start, x0 in ((CHAIN_HEAD, half), (CHAIN_HEAD + CHAIN_TAIL, -half)):
+        for k in range(CHAIN_TAIL):
+            leg = k // strand
+            kk = k if leg == 0 else (CHAIN_TAIL - 1 - k)
+            y0 = half if leg == 0 else -half
+            pos[start + k] = [x0 + (zz if kk % 2 else -zz), y0, sgn * dz * kk]
+    return pos
+
+
+def lipid_slab(n_chains: int = 64, n_waters: int = 4500, box=(5.0, 5.0, 8.0),
+               seed: int = 20241203, temperature: float = 300.0) -> System:
+    """Config 1: two leaflets of lipid-like chains solvated by flexible water.
+
+    Sizes, charges and force-field parameters follow the named configuration.
+    The two leaflets interdigitate (the lower leaflet's strands sit in the
+    gaps of the upper one's) so that 3,328 chain atoms and 4,500 waters fit
+    the 5 x 5 x 8 nm box near normal density."""
+    rng = np.random.default_rng(seed)
+    box = np.asarray(box, dtype=np.float64)
+    cb, ca, cd = chain_topology()
+    per_leaflet = n_chains // 2
+    nx = int(math.ceil(math.sqrt(per_leaflet)))
+    d = box[0] / nx                   # chain spacing
+    half = d / 4                      # strands on a uniform d/2 lattice
+    sites = [(ix, iy) for ix in range(nx) for iy in range(nx)][:per_leaflet]
+    strand_len = (CHAIN_TAIL // 2 - 1) * CHAIN["b0"] * math.sin(CHAIN["theta0"] / 2)
+    zc = box[2] / 2
+    z_top = zc + 0.5 * strand_len     # upper tails hang down from here
+    z_bot = zc - 0.5 * strand_len     # lower tails rise from here
+    pos_l, q_l, s_l, e_l = [], [], [], []
+    bonds, angles, dihedrals = [], [], []
+    for leaflet in range(2):
+        up = leaflet == 0
+        geo = _chain_geometry(up, half)
+        off_xy = 0.0 if up else d / 4
+        for ix, iy in sites:
+            off = len(pos_l) * CHAIN_ATOMS
+            shift = np.array([(ix + 0.5) * d + off_xy, (iy + 0.5) * box[1] / nx + off_xy,
+                              z_top if up else z_bot])
+            pos_l.append(geo + shift)
+            hq = rng.normal(0.0, 0.4, CHAIN_HEAD)
+            hq -= hq.mean()
+            q = np.zeros(CHAIN_ATOMS)
+            q[:CHAIN_HEAD] = hq * E_TO_KCMOL
+            q_l.append(q)
+            s_l.append(rng.uniform(0.30, 0.39, CHAIN_ATOMS))
+            e_l.append(rng.uniform(0.2, 0.9, CHAIN_ATOMS) * KJ)
+            bonds.append(cb + off)
+            angles.append(ca + off)
+            dihedrals.append(cd + off)
+    lip_pos = np.concatenate(pos_l)
+    n_lip = len(lip_pos)
+    # water fills the space the chains leave free
+    cand = solvate_sites(rng, box, lip_pos, n_waters)
+    wpos, wq, wm, ws, we, wb, wbp, wa, wap = _append_waters(rng, cand, n_lip, box=box, fixed=lip_pos)
+    n_b = sum(len(b) for b in bonds)
+    n_a = sum(len(a) for a in angles)
+    n_d = sum(len(d) for d in dihedrals)
+    pos = np.mod(np.concatenate([lip_pos, wpos]), box)
+    charge = np.concatenate([np.concatenate(q_l), wq])
+    mass = np.concatenate([np.full(n_lip, CHAIN["mass"]), wm])
+    sigma = np.concatenate([np.concatenate(s_l), ws])
+    eps = np.concatenate([np.concatenate(e_l), we])
+    bond_par = np.concatenate([np.tile([CHAIN["b0"], CHAIN["kb"]], (n_b, 1)), wbp])
+    angle_par = np.concatenate([np.tile([CHAIN["theta0"], CHAIN["kth"], 0.0, 0.0], (n_a, 1)), wap])
+    dih_par = np.tile([CHAIN["phi0"], CHAIN["kphi"], CHAIN["mult"]], (n_d, 1))
+    vel = maxwell_boltzmann(rng, mass, temperature)
+    return System(box=box, pos=pos, vel=vel, charge=charge.astype(np.float32),
+                  mass=mass.astype(np.float32), sigma=sigma.astype(np.float32),
+                  epsilon=eps.astype(np.float32),
+                  bonds=np.concatenate(bonds + [wb]).astype(np.int32), bond_par=bond_par.astype(np.float32),
+                  angles=np.concatenate(angles + [wa]).astype(np.int32), angle_par=angle_par.astype(np.float32),
+                  dihedrals=np.concatenate(dihedrals).astype(np.int32), dihedral_par=dih_par.astype(np.float32),
+                  name="lipid_slab")
+
+
+def ewald_kappa(cutoff: float, tol: float) -> float:
+    """kappa with erfc(kappa*rc) = tol (bisection)."""
+    lo, hi = 0.0, 20.0 / cutoff
+    for _ in range(200):
+        mid = 0.5 * (lo + hi)
+        if math.erfc(mid * cutoff) > tol:
+            lo = mid
+        else:
+            hi = mid
+    return 0.5 * (lo + hi)
+
+
+def fft_friendly(n: int) -> int:
+    """Smallest m >= n whose prime factors are 2, 3 and 5."""
+    m = max(n, 4)
+    while True:
+        k = m
+        for p in (2, 3, 5):
+            while k % p == 0:
+                k //= p
+        if k == 1:
+            return m
+        m += 1
+
+
+# --------------------------------------------------------------- named configs
+def config0(seed=20241203):
+    """1,000 flexible waters, 3.1 nm cube, LJ + cutoff Coulomb at 1.2 nm."""
+    return water_box(1000, 3.1, seed=seed, name="water1k_3.1nm")
+
+
+def config1(seed=20241203):
+    """64 lipid-like chains x 52 atoms + 4,500 waters, 5x5x8 nm, PME 48x48x80."""
+    return lipid_slab(seed=seed)
+
+
+def config2(seed=20241203):
+    """33,400 waters (100,200 atoms), 10 nm cube, PME 96^3, cutoff 1.0 nm."""
+    return water_box(33400, 10.0, seed=seed, name="water100k_10nm")
+
+
+def batch_systems(n_systems=256, seed=20241203, lo=1500, hi=30000, density=33.4):
+    """Config 4: atom counts log-uniform in [lo, hi]; water boxes at the given
+    density with 0-4 chains inserted (here: chains counted into the atom budget)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for s in range(n_systems):
+        n_atoms = int(math.exp(rng.uniform(math.log(lo), math.log(hi))))
+        n_w = max(8, n_atoms // 3)
+        L = (n_w / density) ** (1.0 / 3.0)
+        out.append(water_box(n_w, L, seed=seed + 1 + s, name=f"batch{s}"))
+    return out

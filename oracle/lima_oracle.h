@@ -1,0 +1,118 @@
+/*
+ * lima_oracle.h — CPU restatement of LIMA's per-step force and integration
+ * formulas.  TEST INFRASTRUCTURE ONLY: the parity tests, the smoke check and
+ * the CPU-baseline leg of the benchmark call this library as the checker; the
+ * product path (liblima_b200.so) never links or calls it.
+ *
+ * Parity status: the reference ships no golden force vectors (its fixtures
+ * live in an external LIMA_data directory that is not distributed).  The
+ * oracle is pinned by the reference's own analytic known-answer tests, restated
+ * in tests/test_oracle_kat.py:
+ *   code/LIMA_TESTS/src/ForceCorrectness.h:115-165  (single bond, 1e-4)
+ *   code/LIMA_TESTS/src/ForceCorrectness.h:232-333  (angle + Urey-Bradley, 1e-4)
+ *   code/LIMA_TESTS/src/ForceCorrectness.h:336-403  (pair-bond LJ, 1e-4)
+ *   code/LIMA_TESTS/src/ElectrostaticsTests.h:19-26 (Coulomb constant, 1e-4)
+ *   code/LIMA_TESTS/src/ElectrostaticsTests.h:300-396 (two-particle PME, 7 %)
+ *   code/LIMA_TESTS/src/ElectrostaticsTests.h:521-609 (many-ion PME, 18 % mean)
+ * plus finite-difference energy/force consistency and an independent Ewald sum.
+ *
+ * Units are the reference's: nm, ns, kg/mol, kC/mol, J/mol, J/mol/nm.
+ * Positions are double[3n], forces are ACCUMULATED into double[3n].
+ */
+#ifndef LIMA_ORACLE_H
+#define LIMA_ORACLE_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+double orc_coulomb_constant(void);       /* k_e in J nm / mol / (kC/mol)^2 */
+double orc_e_to_kcmol(void);             /* elementary charge in kC/mol     */
+
+/* Short-range non-bonded forces over all atom pairs (i<j) that are not
+ * excluded and whose minimum-image distance r satisfies r <= rc.
+ *   LJ (LennardJonesInteractions.cuh:74-108): F_i = 24 eps s(1-2s)/r^2 (r_j-r_i),
+ *       s=(sigma/r)^6, E = 4 eps s(s-1); sigma=(s_i+s_j)/2, eps=sqrt(e_i e_j)
+ *   Coulomb (DeviceAlgorithmsPrivate.cuh:38-95): es_mode 1 plain k q q/r,
+ *       es_mode 2 erfc(kappa r) screened with the matching force term.
+ * excl_off[n+1]/excl_idx: CSR list of excluded partners (both directions).
+ * precision: 64 = FP64, 32 = FP32 reference-faithful arithmetic.
+ * nthreads: OpenMP threads (0 = all).  energies[0]=LJ, [1]=Coulomb,
+ * [2]=virial (-1/2 sum r_ij.f_ij).  Returns the number of pairs evaluated. */
+int64_t orc_nonbonded(int n, const double* pos, const double* box,
+                      const double* q, const double* sigma, const double* eps,
+                      const int* excl_off, const int* excl_idx,
+                      double rc, int es_mode, double kappa, int precision, int nthreads,
+                      double* forces, double* energies);
+
+/* Sorted list of pairs (i<j) with r <= rc that are not excluded.  Pairs with
+ * |r - rc| < band are counted in *n_band and flagged in band_flag (may be
+ * NULL).  Returns the pair count (writes at most cap pairs). */
+int64_t orc_pairset(int n, const double* pos, const double* box,
+                    const int* excl_off, const int* excl_idx, double rc, double band,
+                    int64_t cap, int32_t* pairs, uint8_t* band_flag, int64_t* n_band);
+
+/* Bonded terms, restating code/LIMA_ENGINE/src/ForceComputations.cuh:
+ *   bonds      :17-51   params [b0, kb]
+ *   angles     :53-115  params [theta0, ktheta, ub0, kub] (Urey-Bradley on)
+ *   dihedrals  :119-210 params [phi0, kphi, n]
+ *   impropers  :214-264 params [psi0, kpsi]
+ *   pair bonds :335-376 params [sigma, eps]
+ * Vectors between the atoms of one term use the minimum image (box may be
+ * NULL for no periodicity).  energies[0..4] = bond, angle, dihedral, improper,
+ * pairbond. */
+void orc_bonded(int n, const double* pos, const double* box,
+                int nb, const int* bidx, const double* bpar,
+                int na, const int* aidx, const double* apar,
+                int nd, const int* didx, const double* dpar,
+                int ni, const int* iidx, const double* ipar,
+                int np, const int* pidx, const double* ppar,
+                double* forces, double* energies);
+
+/* Smooth PME reciprocal part on a Kx x Ky x Kz grid, order 4, weights placed
+ * at floor(u)-1 .. floor(u)+2 as in PME.cuh:249-300 and 335-383.
+ * influence 0: SPME  theta(k) = (N/V) k_e 4pi/k^2 exp(-k^2/4kappa^2) / B(k),
+ *              B = prod_d (2/3 + 1/3 cos(2 pi m_d/K_d))^2
+ * influence 1: the reference's function (PME.cuh:434-495):
+ *              (1/h^3) k_e 4pi/k^2 exp(-k^2/4kappa^2) prod_d sinc^8(k_d h_d/2),
+ *              with pi truncated to 3.14159 (Constants.h:51)
+ * gather 0: analytic B-spline derivative; 1: central difference of the
+ *           gridded potential (PME.cuh:384-407).
+ * energies[0] = 1/2 sum_j q_j phi(r_j); energies[1] = self term
+ * -kappa/sqrt(pi) k_e sum q^2.  potential_out (may be NULL) receives
+ * phi(r_j) per atom. */
+void orc_pme(int n, const double* pos, const double* q, const double* box,
+             int kx, int ky, int kz, double kappa, int influence, int gather,
+             double* forces, double* energies, double* potential_out);
+
+/* Reciprocal Ewald sum over all k != 0 with |m_d| <= mmax (FP64). */
+void orc_ewald_recip(int n, const double* pos, const double* q, const double* box,
+                     double kappa, int mmax, double* forces, double* energy);
+
+/* Reciprocal-space exclusion correction for excluded pairs (i<j):
+ * E = -k_e q_i q_j erf(kappa r)/r with its force. */
+void orc_exclusion_correction(int n, const double* pos, const double* q, const double* box,
+                              int npairs, const int* pairs, double kappa,
+                              double* forces, double* energy);
+
+/* One integration step. integrator 0: leapfrog (v(t+dt/2) = v(t-dt/2) + F dt/m;
+ * x += v dt); 1: the reference's velocity Verlet (EngineUtils.cuh:31-41,
+ * EngineKernels.cuh:399-413): v = v_prev + (F + F_prev) dt/2m,
+ * x += v dt + F dt^2/2m, then F_prev = F, v_prev = v * scale.
+ * fprev may be NULL for leapfrog. */
+void orc_integrate(int n, double* pos, double* vel, double* fprev, const double* forces,
+                   const double* mass, double dt, int integrator, double thermostat_scale);
+
+/* One energy-minimisation step (EngineUtils.cuh:44-72 and 112-140): tanh
+ * force clamp at 1e6 J/mol/nm, then ADAM with alpha 8000 on forces x 1e-8.
+ * adam[6n] = first and second moments; step counts from 1. */
+void orc_em_step(int n, double* pos, const double* forces, double* adam, int step);
+
+/* 3-D complex DFT in FP64 (x fastest), sign -1 forward, +1 inverse (no
+ * normalisation).  data is interleaved re,im. */
+void orc_fft3d(int kx, int ky, int kz, double* data, int sign);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

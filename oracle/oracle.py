@@ -1,0 +1,215 @@
+"""ctypes wrapper of the CPU oracle (oracle/lima_oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, ``__graft_entry__.smoke()`` and the
+CPU-baseline leg of ``bench.py`` as the checker.  The product library never
+imports it.  Each function documents the reference formula it restates in
+``oracle/lima_oracle.h``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+_d = ctypes.POINTER(ctypes.c_double)
+_i = ctypes.POINTER(ctypes.c_int)
+_i32 = ctypes.POINTER(ctypes.c_int32)
+_u8 = ctypes.POINTER(ctypes.c_uint8)
+_i64 = ctypes.POINTER(ctypes.c_int64)
+
+
+def build(force: bool = False) -> str:
+    """Compile the oracle with its Makefile (g++ -O3 -fopenmp)."""
+    if force or not os.path.exists(_LIB_PATH):
+        subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        L.orc_coulomb_constant.restype = ctypes.c_double
+        L.orc_e_to_kcmol.restype = ctypes.c_double
+        L.orc_nonbonded.restype = ctypes.c_int64
+        L.orc_nonbonded.argtypes = [ctypes.c_int, _d, _d, _d, _d, _d, _i, _i, ctypes.c_double,
+                                    ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, _d, _d]
+        L.orc_pairset.restype = ctypes.c_int64
+        L.orc_pairset.argtypes = [ctypes.c_int, _d, _d, _i, _i, ctypes.c_double, ctypes.c_double,
+                                  ctypes.c_int64, _i32, _u8, _i64]
+        L.orc_bonded.restype = None
+        L.orc_bonded.argtypes = [ctypes.c_int, _d, _d] + [ctypes.c_int, _i, _d] * 5 + [_d, _d]
+        L.orc_pme.restype = None
+        L.orc_pme.argtypes = [ctypes.c_int, _d, _d, _d, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                              ctypes.c_double, ctypes.c_int, ctypes.c_int, _d, _d, _d]
+        L.orc_ewald_recip.restype = None
+        L.orc_ewald_recip.argtypes = [ctypes.c_int, _d, _d, _d, ctypes.c_double, ctypes.c_int, _d, _d]
+        L.orc_exclusion_correction.restype = None
+        L.orc_exclusion_correction.argtypes = [ctypes.c_int, _d, _d, _d, ctypes.c_int, _i,
+                                               ctypes.c_double, _d, _d]
+        L.orc_integrate.restype = None
+        L.orc_integrate.argtypes = [ctypes.c_int, _d, _d, _d, _d, _d, ctypes.c_double, ctypes.c_int,
+                                    ctypes.c_double]
+        L.orc_em_step.restype = None
+        L.orc_em_step.argtypes = [ctypes.c_int, _d, _d, _d, ctypes.c_int]
+        L.orc_fft3d.restype = None
+        L.orc_fft3d.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _d, ctypes.c_int]
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return None if a is None else a.ctypes.data_as(_d)
+
+
+def _ip(a):
+    return None if a is None else a.ctypes.data_as(_i)
+
+
+def _f64(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+
+
+def coulomb_constant() -> float:
+    return lib().orc_coulomb_constant()
+
+
+def e_to_kcmol() -> float:
+    return lib().orc_e_to_kcmol()
+
+
+def exclusion_csr(n: int, pairs) -> tuple[np.ndarray, np.ndarray]:
+    """CSR (both directions) of excluded atom pairs given as an (m,2) array."""
+    pairs = np.asarray(pairs, dtype=np.int64).reshape(-1, 2)
+    if len(pairs) == 0:
+        return np.zeros(n + 1, np.int32), np.zeros(1, np.int32)
+    a = np.concatenate([pairs[:, 0], pairs[:, 1]])
+    b = np.concatenate([pairs[:, 1], pairs[:, 0]])
+    order = np.lexsort((b, a))
+    a, b = a[order], b[order]
+    off = np.zeros(n + 1, np.int64)
+    np.add.at(off, a + 1, 1)
+    off = np.cumsum(off)
+    return off.astype(np.int32), b.astype(np.int32)
+
+
+def nonbonded(pos, box, q, sigma, eps, excl_pairs, rc, es_mode, kappa=0.0, precision=64,
+              nthreads=0):
+    """Returns (forces (n,3), {'lj','coulomb','virial'}, n_pairs)."""
+    pos = _f64(pos).reshape(-1, 3)
+    n = len(pos)
+    off, idx = exclusion_csr(n, excl_pairs)
+    f = np.zeros((n, 3))
+    e = np.zeros(3)
+    box = _f64(box)
+    npairs = lib().orc_nonbonded(n, _dp(pos), _dp(box), _dp(_f64(q)), _dp(_f64(sigma)), _dp(_f64(eps)),
+                                 _ip(off), _ip(idx), rc, es_mode, kappa, precision, nthreads, _dp(f), _dp(e))
+    return f, {"lj": e[0], "coulomb": e[1], "virial": e[2]}, int(npairs)
+
+
+def pairset(pos, box, excl_pairs, rc, band=0.0, cap=None):
+    """Sorted (i<j) pairs within rc; returns (pairs (m,2), band_flags (m,), n_band)."""
+    pos = _f64(pos).reshape(-1, 3)
+    n = len(pos)
+    off, idx = exclusion_csr(n, excl_pairs)
+    box = _f64(box)
+    if cap is None:
+        cap = 0
+        total = lib().orc_pairset(n, _dp(pos), _dp(box), _ip(off), _ip(idx), rc, band, 0,
+                                  None, None, None)
+        cap = total
+    out = np.zeros((max(cap, 1), 2), np.int32)
+    flags = np.zeros(max(cap, 1), np.uint8)
+    nb = ctypes.c_int64(0)
+    total = lib().orc_pairset(n, _dp(pos), _dp(box), _ip(off), _ip(idx), rc, band, cap,
+                              out.ctypes.data_as(_i32), flags.ctypes.data_as(_u8), ctypes.byref(nb))
+    return out[:total], flags[:total], int(nb.value)
+
+
+def _terms(idx, par, k, p):
+    if idx is None or len(idx) == 0:
+        return 0, None, None
+    idx = np.ascontiguousarray(idx, dtype=np.int32).reshape(-1, k)
+    par = np.ascontiguousarray(par, dtype=np.float64).reshape(-1, p)
+    return len(idx), idx, par
+
+
+def bonded(pos, box, bonds=None, bond_par=None, angles=None, angle_par=None, dihedrals=None,
+           dihedral_par=None, impropers=None, improper_par=None, pairbonds=None, pair_par=None):
+    """Returns (forces (n,3), {'bond','angle','dihedral','improper','pairbond'})."""
+    pos = _f64(pos).reshape(-1, 3)
+    n = len(pos)
+    f = np.zeros((n, 3))
+    e = np.zeros(5)
+    call = []
+    keep = []  # holds the converted arrays alive during the call
+    for idx, par, k, p in ((bonds, bond_par, 2, 2), (angles, angle_par, 3, 4),
+                           (dihedrals, dihedral_par, 4, 3), (impropers, improper_par, 4, 2),
+                           (pairbonds, pair_par, 2, 2)):
+        m, ii, pp = _terms(idx, par, k, p)
+        keep.append((ii, pp))
+        call += [m, None if ii is None else ii.ctypes.data_as(_i), _dp(pp)]
+    box = _f64(box)
+    lib().orc_bonded(n, _dp(pos), _dp(box), *call, _dp(f), _dp(e))
+    return f, dict(zip(["bond", "angle", "dihedral", "improper", "pairbond"], e.tolist()))
+
+
+def pme(pos, q, box, grid, kappa, influence=0, gather=0, want_potential=False):
+    """Returns (forces (n,3), e_recip, e_self[, phi])."""
+    pos = _f64(pos).reshape(-1, 3)
+    n = len(pos)
+    f = np.zeros((n, 3))
+    e = np.zeros(2)
+    phi = np.zeros(n) if want_potential else None
+    lib().orc_pme(n, _dp(pos), _dp(_f64(q)), _dp(_f64(box)), int(grid[0]), int(grid[1]), int(grid[2]),
+                  kappa, influence, gather, _dp(f), _dp(e), _dp(phi))
+    if want_potential:
+        return f, e[0], e[1], phi
+    return f, e[0], e[1]
+
+
+def ewald_recip(pos, q, box, kappa, mmax):
+    pos = _f64(pos).reshape(-1, 3)
+    n = len(pos)
+    f = np.zeros((n, 3))
+    e = ctypes.c_double(0.0)
+    lib().orc_ewald_recip(n, _dp(pos), _dp(_f64(q)), _dp(_f64(box)), kappa, mmax, _dp(f), ctypes.byref(e))
+    return f, e.value
+
+
+def exclusion_correction(pos, q, box, pairs, kappa):
+    pos = _f64(pos).reshape(-1, 3)
+    n = len(pos)
+    pairs = np.ascontiguousarray(pairs, dtype=np.int32).reshape(-1, 2)
+    f = np.zeros((n, 3))
+    e = ctypes.c_double(0.0)
+    lib().orc_exclusion_correction(n, _dp(pos), _dp(_f64(q)), _dp(_f64(box)), len(pairs),
+                                   pairs.ctypes.data_as(_i), kappa, _dp(f), ctypes.byref(e))
+    return f, e.value
+
+
+def integrate(pos, vel, fprev, forces, mass, dt, integrator, scale=1.0):
+    """In place on float64 arrays (pos, vel, fprev)."""
+    n = len(mass)
+    lib().orc_integrate(n, _dp(pos), _dp(vel), _dp(fprev), _dp(_f64(forces)), _dp(_f64(mass)), dt,
+                        integrator, scale)
+
+
+def em_step(pos, forces, adam, step):
+    lib().orc_em_step(len(pos), _dp(pos), _dp(_f64(forces)), _dp(adam), step)
+
+
+def fft3d(data: np.ndarray, sign: int) -> np.ndarray:
+    """data complex128 array of shape (kz, ky, kx); returns transformed copy."""
+    a = np.ascontiguousarray(data, dtype=np.complex128).copy()
+    kz, ky, kx = a.shape
+    lib().orc_fft3d(kx, ky, kz, a.view(np.float64).ctypes.data_as(_d), sign)
+    return a

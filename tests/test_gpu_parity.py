@@ -1,0 +1,243 @@
+"""Parity of the CUDA path (through the C-ABI) with the FP64 CPU oracle.
+
+Bars, from the path's specification: pair sets bit-exact outside a band of
+|r - rc| < 1e-5 nm; forces within 1e-4 relative RMS; energy terms within 1e-5
+relative (FP32 pair arithmetic, FP64 totals); results bit-reproducible run to run.
+"""
+import numpy as np
+import pytest
+
+from lima_b200 import Engine, LimaError, systems
+from lima_b200 import engine as E
+from tests._ref import kappa_from_tol, oracle_total, rel_rms
+
+pytestmark = pytest.mark.gpu
+
+FORCE_TOL = 1e-4
+ENERGY_TOL = 1e-5
+
+
+def small_water(n_waters=3000, box=4.6, seed=5):
+    return systems.water_box(n_waters, box, seed=seed, name="water_small")
+
+
+def make(s, grid=None, **kw):
+    e = Engine(**kw)
+    e.load(s, pme_grid=grid)
+    return e
+
+
+def check_energies(eng, ref, tol=ENERGY_TOL, keys=None):
+    keys = keys or ref.keys()
+    for k in keys:
+        a, b = eng[k], ref[k]
+        scale = max(abs(b), 1e-3 * abs(eng["potential"]) if eng.get("potential") else 0.0, 1e-6)
+        assert abs(a - b) <= tol * scale, (k, a, b)
+
+
+# ------------------------------------------------------------- (a) pair sets
+@pytest.mark.parametrize("rc", [1.2, 0.9])
+def test_pairset_bit_exact(oracle, rc):
+    s = systems.config0()
+    e = make(s, cutoff=rc, electrostatics=E.ES_CUTOFF)
+    e.compute_forces()
+    got = e.pairlist()
+    band = 1e-5
+    ref, flags, nband = oracle.pairset(s.pos, s.box, s.exclusions(), rc, band=band)
+    gs = set(map(tuple, got.tolist()))
+    rs = set(map(tuple, ref.tolist()))
+    in_band = set(map(tuple, ref[flags == 1].tolist()))
+    only_gpu = gs - rs
+    only_ref = rs - gs
+    assert only_ref <= in_band, len(only_ref - in_band)
+    # a pair the GPU keeps but the oracle drops must sit just outside rc
+    for i, j in only_gpu:
+        d = s.pos[i] - s.pos[j]
+        d -= s.box * np.round(d / s.box)
+        assert abs(np.linalg.norm(d) - rc) < band
+    assert len(got) == len(gs)        # no duplicates
+    assert len(rs) > 100000 if rc == 1.2 else True
+
+
+# ------------------------------------------------- (b)+(c) forces and energies
+def test_cutoff_coulomb_config0(oracle):
+    """Config 0: LJ + plain cutoff Coulomb at 1.2 nm, flexible water bonds/angles."""
+    s = systems.config0()
+    e = make(s, cutoff=1.2, electrostatics=E.ES_CUTOFF)
+    e.compute_forces(energy=True)
+    f = e.forces()
+    fr, er = oracle_total(oracle, s, 1.2, 1)
+    assert rel_rms(f, fr) < FORCE_TOL, rel_rms(f, fr)
+    check_energies(e.energies(), er)
+
+
+def test_ewald_pme_accurate(oracle):
+    s = small_water()
+    kappa = kappa_from_tol(1.0, 1e-5)
+    grid = (48, 48, 48)
+    e = make(s, grid=grid, cutoff=1.0, electrostatics=E.ES_EWALD, ewald_kappa=kappa)
+    e.compute_forces(energy=True)
+    f = e.forces()
+    fr, er = oracle_total(oracle, s, 1.0, 2, kappa, grid)
+    assert rel_rms(f, fr) < FORCE_TOL, rel_rms(f, fr)
+    check_energies(e.energies(), er)
+
+
+def test_ewald_pme_reference_conventions(oracle):
+    """ref_compat: kappa = 3/rc, sinc^8 influence, central-difference gather, no
+    exclusion correction, the reference's per-atom self-energy bookkeeping."""
+    s = small_water()
+    grid = (46, 46, 46)
+    e = make(s, grid=grid, cutoff=1.2, electrostatics=E.ES_EWALD, ref_compat=1)
+    e.compute_forces(energy=True)
+    f = e.forces()
+    fr, er = oracle_total(oracle, s, 1.2, 2, 3.0 / 1.2, grid, ref_compat=True)
+    assert rel_rms(f, fr) < FORCE_TOL, rel_rms(f, fr)
+    en = e.energies()
+    assert en["pme_excl"] == 0.0
+    check_energies(en, er)
+
+
+def test_full_config1(oracle):
+    """Config 1: chains + water, LJ per atom, Ewald + PME 48x48x80, bonds/angles/dihedrals."""
+    s = systems.config1()
+    kappa = kappa_from_tol(1.2, 1e-5)
+    grid = (48, 48, 80)
+    e = make(s, grid=grid, cutoff=1.2, electrostatics=E.ES_EWALD, ewald_kappa=kappa)
+    e.compute_forces(energy=True)
+    f = e.forces()
+    fr, er = oracle_total(oracle, s, 1.2, 2, kappa, grid)
+    assert rel_rms(f, fr) < FORCE_TOL, rel_rms(f, fr)
+    check_energies(e.energies(), er)
+
+
+def test_bonded_all_terms(oracle):
+    """Bonds, angles with Urey-Bradley, dihedrals (both gradient branches),
+    impropers and pair bonds; non-bonded switched off."""
+    s = systems.config1()
+    rng = np.random.default_rng(3)
+    heads = np.arange(64) * 52
+    s.impropers = np.stack([heads + 1, heads + 0, heads + 2, heads + 3], 1).astype(np.int32)
+    s.improper_par = np.stack([rng.uniform(-0.3, 0.3, 64), rng.uniform(1e4, 5e4, 64)], 1).astype(np.float32)
+    s.pairbonds = np.stack([heads + 8, heads + 11], 1).astype(np.int32)
+    s.pair_par = np.tile([0.34, 700.0], (64, 1)).astype(np.float32)
+    s.angle_par = s.angle_par.copy()
+    s.angle_par[:100, 2] = 0.25
+    s.angle_par[:100, 3] = 1e5
+    s.epsilon = np.zeros_like(s.epsilon)
+    e = make(s, cutoff=1.2, electrostatics=E.ES_NONE)
+    e.compute_forces(energy=True)
+    f = e.forces()
+    fr, er = oracle_total(oracle, s, 1.2, 0, nb=False)
+    assert rel_rms(f, fr) < FORCE_TOL, rel_rms(f, fr)
+    check_energies(e.energies(), er, keys=["bond", "angle", "dihedral", "improper", "pairbond"])
+
+
+def test_config2_full_size(oracle):
+    """100,200-atom water box, PME 96^3, cutoff 1.0 nm."""
+    s = systems.config2()
+    kappa = kappa_from_tol(1.0, 1e-5)
+    grid = (96, 96, 96)
+    e = make(s, grid=grid, cutoff=1.0, electrostatics=E.ES_EWALD, ewald_kappa=kappa)
+    e.compute_forces(energy=True)
+    f = e.forces()
+    fr, er = oracle_total(oracle, s, 1.0, 2, kappa, grid)
+    assert rel_rms(f, fr) < FORCE_TOL, rel_rms(f, fr)
+    check_energies(e.energies(), er)
+
+
+# ------------------------------------------------------------- reproducibility
+def test_bit_reproducible():
+    s = small_water()
+    a = make(s, grid=(48, 48, 48), cutoff=1.0)
+    a.compute_forces(energy=True)
+    fa, ea = a.forces(), a.energies()
+    a.compute_forces(energy=True)
+    fa2 = a.forces()
+    b = make(s, grid=(48, 48, 48), cutoff=1.0)
+    b.compute_forces(energy=True)
+    fb, eb = b.forces(), b.energies()
+    assert np.array_equal(fa, fa2) and np.array_equal(fa, fb)
+    assert ea == eb
+    a.step(25)
+    b.step(25)
+    pa, va = a.state()
+    pb, vb = b.state()
+    assert np.array_equal(pa, pb) and np.array_equal(va, vb)
+
+
+# ------------------------------------------------------------------- (e) integration
+@pytest.mark.parametrize("integrator", [E.LEAPFROG, E.VELOCITY_VERLET])
+def test_integrator_matches_oracle(oracle, integrator):
+    s = systems.config0()
+    n_steps, dt = 20, 1e-6
+    e = make(s, cutoff=1.2, electrostatics=E.ES_CUTOFF, integrator=integrator, dt=dt, nstlist=10)
+    e.step(n_steps)
+    pg, vg = e.state()
+    p = s.pos.copy()
+    v = s.vel.astype(np.float64).copy()
+    fprev = np.zeros_like(p)
+    m = s.mass.astype(np.float64)
+    import dataclasses
+    for k in range(n_steps):
+        cur = dataclasses.replace(s, pos=p)
+        f, _ = oracle_total(oracle, cur, 1.2, 1)
+        oracle.integrate(p, v, fprev, f, m, dt, integrator)
+    d = pg - p
+    d -= s.box * np.round(d / s.box)
+    assert np.abs(d).max() < 1e-6, np.abs(d).max()
+    assert rel_rms(vg.astype(np.float64), v) < 1e-4
+
+
+def test_energy_conservation():
+    """NVE leapfrog, 1 fs, PME water: total energy drift stays small over 2,000 steps."""
+    s = small_water(n_waters=1500, box=3.6)
+    e = make(s, grid=(40, 40, 40), cutoff=1.0, nstlist=10)
+    e.step(1)
+    e0 = e.energies()["total"]
+    totals = []
+    for _ in range(20):
+        e.step(100)
+        totals.append(e.energies()["total"])
+    kin = e.energies()["kinetic"]
+    drift = abs(totals[-1] - e0)
+    assert drift < 0.02 * kin, (drift, kin, totals)
+
+
+def test_minimize_reduces_max_force():
+    s = systems.config1()
+    e = make(s, grid=(48, 48, 80), cutoff=1.2)
+    e.compute_forces()
+    f0 = np.linalg.norm(e.forces(), axis=1).max()
+    steps, fmax = e.minimize(force_tol=1.0, max_steps=300)
+    assert steps > 0 and fmax < f0
+
+
+# --------------------------------------------------------------------- batching
+def test_batch_matches_single():
+    sys_list = [systems.water_box(n, L, seed=11 + n, name="b") for n, L in ((600, 2.8), (1500, 3.6), (900, 3.1))]
+    grids = [(32, 32, 32), (40, 40, 40), (36, 36, 36)]
+    batch = Engine(n_systems=3, cutoff=1.0)
+    for k, (s, g) in enumerate(zip(sys_list, grids)):
+        batch.select(k)
+        batch.load(s, pme_grid=g)
+    batch.compute_forces(energy=True)
+    for k, (s, g) in enumerate(zip(sys_list, grids)):
+        single = make(s, grid=g, cutoff=1.0)
+        single.compute_forces(energy=True)
+        batch.select(k)
+        assert np.array_equal(batch.forces(), single.forces())
+        eb, es = batch.energies(), single.energies()
+        for key in ("lj", "coulomb_real", "pme_recip", "bond", "angle"):
+            assert eb[key] == es[key], key
+
+
+def test_nonfinite_positions_rejected():
+    s = systems.config0()
+    e = Engine(cutoff=1.2)
+    e.load(s)
+    p = s.pos.copy()
+    p[5, 1] = np.nan
+    with pytest.raises(LimaError) as ex:
+        e.set_state(p)
+    assert ex.value.code == 7

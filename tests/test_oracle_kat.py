@@ -1,0 +1,294 @@
+"""Pins the CPU oracle to the reference's own analytic known-answer tests.
+
+The reference ships no stored force vectors (its fixtures live in an external,
+undistributed data directory).  Its unit tests that build systems from inline
+numbers are restated here with the reference's tolerances; the rest of the
+oracle is pinned by finite-difference and independent-Ewald consistency.
+"""
+import math
+
+import numpy as np
+import pytest
+
+E = 1.602176634e-19 * 6.02214076e23 / 1000.0   # elementaryChargeToKiloCoulombPerMole
+
+
+def test_coulomb_constant_kat(oracle):
+    """ElectrostaticsTests.h:19-26: 1e x 1e at 1 nm -> 2.307078e-10 N (x N_A x NANO)."""
+    q = np.array([E, E])
+    f, e, n = oracle.nonbonded(np.array([[0, 0, 0], [1.0, 0, 0]]), None, q, np.zeros(2), np.zeros(2), [], 2.0, 1)
+    expected = 2.307078e-10 * 6.02214076e23 * 1e-9
+    assert abs(np.linalg.norm(f[0]) - expected) / expected < 1e-4
+    assert f[0, 0] < 0 and f[1, 0] > 0          # like charges repel
+    assert n == 1
+
+
+def test_single_bond_kat(oracle):
+    """ForceCorrectness.h:115-165: bond stretched by 0.02 nm -> F = kb*0.02, E = kb/2*0.02^2."""
+    b0, kb, err = 0.1, 1.7e8, 0.02
+    pos = np.array([[1.0, 1.0, 1.0], [1.0 + b0 + err, 1.0, 1.0]])
+    f, e = oracle.bonded(pos, None, bonds=[[0, 1]], bond_par=[[b0, kb]])
+    expected = np.array([kb * err, 0, 0])
+    assert np.linalg.norm(f[0] - expected) / np.linalg.norm(expected) < 1e-4
+    assert abs(e["bond"] - 0.5 * kb * err * err) / (0.5 * kb * err * err) < 1e-4
+
+
+def _rot_y(p, ang):
+    c, s = math.cos(ang), math.sin(ang)
+    return np.array([p[0] * c + p[2] * s, p[1], -p[0] * s + p[2] * c])
+
+
+def test_urey_bradley_angle_kat(oracle):
+    """ForceCorrectness.h:232-333: arms of length b0, angle theta0+0.1 -> force on the
+    first atom = z * k_theta*0.1/b0 plus the Urey-Bradley spring along p0-p2."""
+    b0, theta0, kth, ub0, kub = 0.1, 1.91, 3.8e5, 0.15, 2.5e7
+    p1 = np.zeros(3)
+    p0 = p1 + np.array([b0, 0, 0])
+    p2 = p1 + _rot_y(np.array([b0, 0, 0]), -(theta0 + 0.1))
+    pos = np.array([p0, p1, p2])
+    f, e = oracle.bonded(pos, None, angles=[[0, 1, 2]], angle_par=[[theta0, kth, ub0, kub]])
+    torque = kth * 0.1
+    f_angle = np.array([0, 0, 1.0]) * torque / b0
+    d = p0 - p2
+    ub_err = np.linalg.norm(d) - ub0
+    assert ub_err > 0.001
+    f_ub = d / np.linalg.norm(d) * -kub * ub_err
+    expected = f_angle + f_ub
+    assert np.linalg.norm(f[0] - expected) / np.linalg.norm(expected) < 1e-4
+    e_exp = 0.5 * kth * 0.01 + 0.5 * kub * ub_err ** 2
+    assert abs(e["angle"] - e_exp) / e_exp < 1e-4
+    assert np.abs(f.sum(0)).max() < 1e-6 * np.abs(f).max()
+
+
+def test_pairbond_kat(oracle):
+    """ForceCorrectness.h:336-403: LJ pair bond F = 24 eps s/r^2 (1-2s) diff on the first atom."""
+    sig, eps = 0.33, 1200.0
+    pos = np.array([[0.0, 0.0, 0.0], [0.29, 0.05, -0.02]])
+    f, e = oracle.bonded(pos, None, pairbonds=[[0, 1]], pair_par=[[sig, eps]])
+    diff = pos[1] - pos[0]
+    s = (sig / np.linalg.norm(diff)) ** 6
+    expected = diff * 24 * eps * s / diff.dot(diff) * (1 - 2 * s)
+    assert np.linalg.norm(expected) > 1.0
+    assert np.linalg.norm(f[0] - expected) / np.linalg.norm(expected) < 1e-4
+    assert abs(e["pairbond"] - 4 * eps * s * (s - 1)) < 1e-9 * abs(4 * eps * s * (s - 1)) + 1e-12
+
+
+_PAR = {"bonds": "bond_par", "angles": "angle_par", "dihedrals": "dihedral_par",
+        "impropers": "improper_par", "pairbonds": "pair_par"}
+
+
+def _fd_check(oracle, pos, kind, idx, par, key, h=1e-6, tol=1e-5):
+    def run(p):
+        return oracle.bonded(p, None, **{kind: [idx], _PAR[kind]: [par]})
+
+    f, _ = run(pos)
+    num = np.zeros_like(pos)
+    for a in range(len(pos)):
+        for d in range(3):
+            pp, pm = pos.copy(), pos.copy()
+            pp[a, d] += h
+            pm[a, d] -= h
+            num[a, d] = -(run(pp)[1][key] - run(pm)[1][key]) / (2 * h)
+    err = np.linalg.norm(f - num) / np.linalg.norm(num)
+    assert err < tol, (kind, err)
+
+
+def test_bonded_forces_are_energy_gradients(oracle):
+    """The reference's bond, angle(+UB), dihedral (both branches) and pair-bond forces
+    are exact negative gradients of their energies."""
+    rng = np.random.default_rng(1)
+    _fd_check(oracle, np.array([[0, 0, 0], [0.11, 0.02, -0.03]]), "bonds", [0, 1], [0.1, 3e8], "bond")
+    _fd_check(oracle, np.array([[0.1, 0, 0], [0, 0, 0], [-0.03, 0.09, 0.01]]), "angles", [0, 1, 2],
+              [1.9, 4e5, 0.16, 2e6], "angle")
+    # general dihedral (|sin phi| > 0.1)
+    p = np.array([[0, 0, 0], [0.15, 0, 0], [0.2, 0.14, 0], [0.35, 0.16, 0.09]])
+    _fd_check(oracle, p, "dihedrals", [0, 1, 2, 3], [0.3, 600.0, 3.0], "dihedral")
+    # nearly planar dihedral: exercises the sin-based branch
+    p = np.array([[0, 0, 0], [0.15, 0, 0], [0.2, 0.14, 0], [0.35, 0.16, 0.004]])
+    _fd_check(oracle, p, "dihedrals", [0, 1, 2, 3], [0.0, 600.0, 3.0], "dihedral", tol=1e-4)
+    _fd_check(oracle, np.array([[0, 0, 0], [0.31, 0.03, 0.02]]), "pairbonds", [0, 1], [0.33, 900.0], "pairbond")
+
+
+def test_improper_force_balance(oracle):
+    """ForceCorrectness.h-style sanity for the simplified improper force split:
+    the four forces sum to zero and the energy is k/2 (psi-psi0)^2."""
+    p = np.array([[0, 0, 0], [0.14, 0.0, 0.0], [-0.05, 0.13, 0.0], [-0.04, -0.1, 0.06]])
+    f, e = oracle.bonded(p, None, impropers=[[0, 1, 2, 3]], improper_par=[[0.1, 5e4]])
+    assert np.abs(f.sum(0)).max() < 1e-9 * np.abs(f).max()
+    assert e["improper"] > 0
+
+
+def test_fft_matches_numpy(oracle):
+    rng = np.random.default_rng(0)
+    a = rng.normal(size=(20, 12, 30)) + 1j * rng.normal(size=(20, 12, 30))
+    assert np.abs(oracle.fft3d(a, -1) - np.fft.fftn(a)).max() < 1e-10
+    assert np.abs(oracle.fft3d(a, 1) - np.fft.ifftn(a) * a.size).max() < 1e-10
+
+
+def _kappa(rc, tol):
+    lo, hi = 0.0, 20.0 / rc
+    for _ in range(200):
+        mid = 0.5 * (lo + hi)
+        lo, hi = (mid, hi) if math.erfc(mid * rc) > tol else (lo, mid)
+    return 0.5 * (lo + hi)
+
+
+def test_spme_matches_ewald_sum(oracle):
+    """Accurate-mode SPME (analytic gather, B-spline moduli) against a direct FP64
+    reciprocal Ewald sum on a neutral random system."""
+    rng = np.random.default_rng(7)
+    n, L = 60, 3.2
+    pos = rng.uniform(0, L, (n, 3))
+    q = rng.choice([-1.0, 1.0], n) * E * 0.6
+    q -= q.mean()
+    box = np.array([L, L, L])
+    kappa = _kappa(1.0, 1e-5)
+    f_e, e_e = oracle.ewald_recip(pos, q, box, kappa, 24)
+    errs = []
+    for g in (48, 96):
+        f_p, e_p, e_self = oracle.pme(pos, q, box, (g, g, g), kappa, influence=0, gather=0)
+        errs.append(np.sqrt(((f_p - f_e) ** 2).sum() / (f_e ** 2).sum()))
+        assert abs(e_p - e_e) / abs(e_e) < 1e-4
+    assert errs[1] < 1e-4, errs
+    assert errs[0] / errs[1] > 6.0, errs   # order-4 interpolation: error falls ~h^3-4
+    # self energy formula: -kappa/sqrt(pi) k_e sum q^2
+    assert abs(e_self + kappa / math.sqrt(math.pi) * oracle.coulomb_constant() * (q ** 2).sum()) < 1e-6 * abs(e_self)
+
+
+def _full_ewald(oracle, pos, q, box, rc, kappa, grid, influence, gather):
+    f_sr, e_sr, _ = oracle.nonbonded(pos, box, q, np.zeros(len(q)), np.zeros(len(q)), [], rc, 2, kappa)
+    f_lr, e_lr, e_self = oracle.pme(pos, q, box, grid, kappa, influence=influence, gather=gather)
+    return f_sr + f_lr
+
+
+def test_pme_two_particle_kat(oracle):
+    """ElectrostaticsTests.h:300-396: -1e/+1e in a 30 nm box (cutoff 1.2, kappa=3/rc, grid
+    10/nm in reference mode); force within 7 % of nearest image + one mirror image and the
+    two forces equal and opposite to 1e-3."""
+    L = 30.0
+    box = np.array([L, L, L])
+    rc = 1.2
+    kappa = 3.0 / rc
+    setups = [
+        ((6.025, 10.025, 10.0), (8.025, 10.025, 10.025), (-1, 0, 0)),
+        ((4.0, 10.0, 10.0), (10.07, 10.025, 10.025), (-1, 0, 0)),
+        ((4.025, 11.025, 9.025), (10.025, 10.025, 10.025), (-1, 0, 0)),
+        ((9.6, 10.0, 10.0), (10.0, 10.0, 10.0), (-1, 0, 0)),
+        ((0.1, 10.0, 10.0), (5.6, 10.0, 10.0), (-1, 0, 0)),
+        ((0.1, 10.0, 10.0), (L - 2.0, 10.0, 10.0), (0, 0, 0)),
+    ]
+    ke = oracle.coulomb_constant()
+    q = np.array([-E, E])
+    for p0, p1, mirror in setups:
+        pos = np.array([p0, p1], dtype=float)
+        d = pos[0] - pos[1]
+        d -= L * np.round(d / L)
+        dm = pos[0] - (pos[1] + L * np.array(mirror))
+        expected = ke * q[0] * q[1] * (d / np.linalg.norm(d) ** 3 + dm / np.linalg.norm(dm) ** 3)
+        # reference conventions only: with an analytic-derivative gather, SPME
+        # carries a per-particle self force of order 1e3 J/mol/nm at kappa*h=0.25
+        # that dominates these weak long-range pair forces; accurate mode is
+        # pinned against the Ewald sum instead (test_spme_matches_ewald_sum)
+        for influence, gather, grid in ((1, 1, (300, 300, 300)),):
+            f = _full_ewald(oracle, pos, q, box, rc, kappa, grid, influence, gather)
+            err = np.linalg.norm(f[0] - expected) / np.linalg.norm(expected)
+            assert err < 0.07, (p0, p1, influence, err)
+            assert np.linalg.norm(f[0] + f[1]) / np.linalg.norm(f[0]) < 1e-3
+
+
+def test_pme_many_ions_kat(oracle):
+    """ElectrostaticsTests.h:521-609: 100 +1e ions in a 20 nm box, LJ off; mean relative
+    force error against the nearest-image Coulomb sum < 0.18 over ions with |F| > 5e4."""
+    rng = np.random.default_rng(3)
+    L = 20.0
+    box = np.array([L, L, L])
+    n = 100
+    pos = rng.uniform(0, L, (n, 3))
+    q = np.full(n, E)
+    ke = oracle.coulomb_constant()
+    exp = np.zeros((n, 3))
+    for i in range(n):
+        d = pos[i] - pos
+        d -= L * np.round(d / L)
+        r = np.linalg.norm(d, axis=1)
+        r[i] = np.inf
+        exp[i] = (ke * E * E * d / r[:, None] ** 3).sum(0)
+    rc = 1.2
+    f = _full_ewald(oracle, pos, q, box, rc, 3.0 / rc, (200, 200, 200), 1, 1)
+    mag = np.linalg.norm(exp, axis=1)
+    sel = mag > 50000.0
+    assert sel.sum() > 5
+    err = np.linalg.norm(f - exp, axis=1)[sel] / mag[sel]
+    assert err.mean() < 0.18, err.mean()
+
+
+def test_exclusion_correction_matches_ewald(oracle):
+    """A neutral molecule whose pairs are all excluded: real space + SPME + the
+    exclusion correction leaves only the interaction with its periodic images,
+    the same as with a direct Ewald sum in place of SPME."""
+    L = 3.0
+    box = np.array([L, L, L])
+    pos = np.array([[1.0, 1.0, 1.0], [1.09, 1.02, 1.0], [0.97, 1.08, 1.03], [2.0, 2.1, 1.9]])
+    q = np.array([-0.8, 0.4, 0.4, 0.0]) * E
+    excl = [[0, 1], [0, 2], [1, 2]]
+    kappa = _kappa(1.0, 1e-6)
+    f_sr, e_sr, _ = oracle.nonbonded(pos, box, q, np.zeros(4), np.zeros(4), excl, 1.0, 2, kappa)
+    f_lr, e_lr, e_self = oracle.pme(pos, q, box, (64, 64, 64), kappa)
+    f_ew, e_ew = oracle.ewald_recip(pos, q, box, kappa, 30)
+    f_x, e_x = oracle.exclusion_correction(pos, q, box, excl, kappa)
+    assert e_sr["coulomb"] == 0.0 and np.abs(f_sr).max() == 0.0
+    # the correction cancels the intramolecular part of the reciprocal sum
+    total = e_lr + e_self + e_x
+    assert abs(total) < 2e-4 * abs(e_self)
+    assert abs((e_lr + e_self + e_x) - (e_ew + e_self + e_x)) < 1e-3 * abs(e_ew)
+    ref = f_ew + f_x
+    assert np.abs((f_lr + f_x) - ref).max() < 2e-3 * np.abs(f_lr).max()
+    assert np.abs(ref).max() < 1e-2 * np.abs(f_lr).max()
+
+
+def test_fp32_faithful_matches_fp64(oracle):
+    from lima_b200 import systems
+    s = systems.config0()
+    ex = s.exclusions()
+    kappa = _kappa(1.2, 1e-5)
+    f64, e64, n64 = oracle.nonbonded(s.pos, s.box, s.charge, s.sigma, s.epsilon, ex, 1.2, 2, kappa)
+    f32, e32, n32 = oracle.nonbonded(s.pos, s.box, s.charge, s.sigma, s.epsilon, ex, 1.2, 2, kappa, precision=32)
+    rel = np.sqrt(((f32 - f64) ** 2).sum() / (f64 ** 2).sum())
+    assert rel < 1e-4, rel
+    assert abs(n32 - n64) <= 5
+
+
+def test_bond_oscillation_frequency_kat(oracle):
+    """ForceCorrectness.h:169-230: a single bond oscillates at sqrt(k/mu) within 1 %."""
+    m = np.array([12e-3, 16e-3])
+    kb, b0 = 2.5e8, 0.12
+    mu = m[0] * m[1] / m.sum()
+    period = 2 * math.pi * math.sqrt(mu / kb)   # [ns]
+    dt = period / 400
+    pos = np.array([[1.0, 1.0, 1.0], [1.0 + b0 + 0.004, 1.0, 1.0]])
+    for integ in (0, 1):
+        p = pos.copy()
+        v = np.zeros((2, 3))
+        fprev = np.zeros((2, 3))
+        xs = []
+        for k in range(3000):
+            f, _ = oracle.bonded(p, None, bonds=[[0, 1]], bond_par=[[b0, kb]])
+            oracle.integrate(p, v, fprev, f, m, dt, integ)
+            xs.append(np.linalg.norm(p[1] - p[0]) - b0)
+        xs = np.array(xs)
+        crossings = np.where((xs[:-1] > 0) & (xs[1:] <= 0))[0]
+        measured = np.mean(np.diff(crossings)) * dt
+        assert abs(measured - period) / period < 0.01, (integ, measured, period)
+
+
+def test_em_step_reduces_energy(oracle):
+    """ADAM energy minimisation (EngineUtils.cuh:44-72): at most alpha*1e-8 = 8e-5 nm
+    per step, so a bond stretched by 0.01 nm relaxes within a few hundred steps."""
+    pos = np.array([[1.0, 1.0, 1.0], [1.11, 1.0, 1.0]])
+    adam = np.zeros(12)
+    e0 = oracle.bonded(pos, None, bonds=[[0, 1]], bond_par=[[0.1, 3e8]])[1]["bond"]
+    for k in range(1, 400):
+        f, e = oracle.bonded(pos, None, bonds=[[0, 1]], bond_par=[[0.1, 3e8]])
+        oracle.em_step(pos, f, adam, k)
+    e1 = oracle.bonded(pos, None, bonds=[[0, 1]], bond_par=[[0.1, 3e8]])[1]["bond"]
+    assert e1 < 0.05 * e0, (e0, e1)
