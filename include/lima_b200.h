@@ -200,8 +200,9 @@ LIMA_API int lima_get_status(lima_engine* h, uint32_t* status);
 LIMA_API int lima_clear_status(lima_engine* h);
 LIMA_API int lima_get_timings(lima_engine* h, lima_timings* t);
 LIMA_API int lima_reset_timings(lima_engine* h);
-/* Times each phase with CUDA events on the stream it runs on (adds one device
- * synchronisation per step while on). */
+/* Times each phase with CUDA events.  While on, the phases run one after the
+ * other on one stream (so each measurement covers that phase alone) and every
+ * step ends with a device synchronisation. */
 LIMA_API int lima_enable_phase_timing(lima_engine* h, int enable);
 
 #ifdef __cplusplus

@@ -679,20 +679,24 @@ void lima_engine::forces(bool energy) {
     }
     if (energy) CK(cudaMemsetAsync(st.energy, 0, sizeof(long long) * E_COUNT * st.n_sys, s_main));
     launch_zero_forces(st, s_main);
+    // with phase timing on, every phase runs on the main stream so that each
+    // phase's events bracket that phase alone
+    cudaStream_t sb = phase_timing ? s_main : s_bonded;
+    cudaStream_t sp = phase_timing ? s_main : s_pme;
     CK(cudaEventRecord(ev_fork, s_main));
-    CK(cudaStreamWaitEvent(s_bonded, ev_fork, 0));
-    CK(cudaStreamWaitEvent(s_pme, ev_fork, 0));
-    mark(2, 0, s_bonded);
-    launches += launch_bonded(st, bt, energy, s_bonded);
-    if (pme_on) launches += launch_exclusion_correction(st, bt, nb, energy, s_bonded);
-    mark(2, 1, s_bonded);
-    CK(cudaEventRecord(ev_bonded, s_bonded));
+    CK(cudaStreamWaitEvent(sb, ev_fork, 0));
+    CK(cudaStreamWaitEvent(sp, ev_fork, 0));
+    mark(2, 0, sb);
+    launches += launch_bonded(st, bt, energy, sb);
+    if (pme_on) launches += launch_exclusion_correction(st, bt, nb, energy, sb);
+    mark(2, 1, sb);
+    CK(cudaEventRecord(ev_bonded, sb));
     if (pme_on) {
-        mark(3, 0, s_pme);
-        launches += launch_pme(st, pp, energy, s_pme);
-        mark(3, 1, s_pme);
+        mark(3, 0, sp);
+        launches += launch_pme(st, pp, energy, sp);
+        mark(3, 1, sp);
     }
-    CK(cudaEventRecord(ev_pme, s_pme));
+    CK(cudaEventRecord(ev_pme, sp));
     mark(1, 0, s_main);
     launches += launch_nonbonded(st, nb, energy, s_main);
     mark(1, 1, s_main);

@@ -234,21 +234,9 @@ __global__ void k_bonded(DevState st, BondedTerms bt) {
         if (ENERGY) e[kind] = en;
     }
     if (ENERGY) {
-        // warps may straddle systems only at batch boundaries: reduce when uniform
-        const int s_first = __shfl_sync(0xffffffffu, sysi, 0);
-        const bool uniform = __all_sync(0xffffffffu, sysi == s_first || sysi < 0);
-        double ev[6] = {e[0], e[1], e[2], e[3], e[4], vir};
-        const int terms[6] = {E_BOND, E_ANGLE, E_DIHEDRAL, E_IMPROPER, E_PAIRBOND, E_VIRIAL};
-        if (uniform) {
-            for (int k = 0; k < 6; ++k) ev[k] = warp_sum(ev[k]);
-            if ((threadIdx.x & 31) == 0 && s_first >= 0) {
-                long long* E = st.energy + (size_t)s_first * E_COUNT;
-                for (int k = 0; k < 6; ++k) atomic_add_fixed(E + terms[k], to_fixed_d(ev[k], ENERGY_SCALE));
-            }
-        } else if (sysi >= 0) {
-            long long* E = st.energy + (size_t)sysi * E_COUNT;
-            for (int k = 0; k < 6; ++k) atomic_add_fixed(E + terms[k], to_fixed_d(ev[k], ENERGY_SCALE));
-        }
+        const int terms[5] = {E_BOND, E_ANGLE, E_DIHEDRAL, E_IMPROPER, E_PAIRBOND};
+        for (int k = 0; k < 5; ++k) add_energy_fixed(st.energy, sysi, (double)e[k], terms[k]);
+        add_energy_fixed(st.energy, sysi, (double)vir, E_VIRIAL);
     }
 }
 

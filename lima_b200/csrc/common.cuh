@@ -79,6 +79,32 @@ __device__ __forceinline__ float warp_sum(float v) {
     return v;
 }
 
+__device__ __forceinline__ long long warp_sum_ll(long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Adds one lane's energy contribution to system `sysi`'s accumulator.  Each
+// lane's value is rounded to fixed point first and the warp sums integers, so
+// the total does not depend on how lanes are grouped into warps (a system run
+// alone and the same system inside a batch give identical bits).
+__device__ __forceinline__ void add_energy_fixed(long long* energy, int sysi, double e, int term) {
+    const long long v = sysi >= 0 ? __double2ll_rn(e * ENERGY_SCALE) : 0ll;
+    const int s0 = __shfl_sync(0xffffffffu, sysi, 0);
+    const bool uniform = __all_sync(0xffffffffu, sysi == s0 || sysi < 0);
+    const int sref = __reduce_max_sync(0xffffffffu, sysi);
+    if (uniform) {
+        const long long t = warp_sum_ll(v);
+        if ((threadIdx.x & 31) == 0 && sref >= 0)
+            atomicAdd(reinterpret_cast<unsigned long long*>(energy + (size_t)sref * E_COUNT + term),
+                      static_cast<unsigned long long>(t));
+    } else if (sysi >= 0) {
+        atomicAdd(reinterpret_cast<unsigned long long*>(energy + (size_t)sysi * E_COUNT + term),
+                  static_cast<unsigned long long>(v));
+    }
+}
+
 // shift code (sx+1) + 3(sy+1) + 9(sz+1), s in {-1,0,1}
 __device__ __forceinline__ int3 decode_shift(int code) {
     return make_int3(code % 3 - 1, (code / 3) % 3 - 1, code / 9 - 1);

@@ -22,19 +22,6 @@ __device__ __forceinline__ float3 load_force(const DevState& st, int s) {
                        (float)((double)st.fz[s] * inv));
 }
 
-__device__ __forceinline__ void add_energy_warp(const DevState& st, int sysi, double e, int term) {
-    const int s_first = __shfl_sync(0xffffffffu, sysi, 0);
-    const bool uniform = __all_sync(0xffffffffu, sysi == s_first || sysi < 0);
-    const int sref = __reduce_max_sync(0xffffffffu, sysi);
-    if (uniform) {
-        e = warp_sum(e);
-        if ((threadIdx.x & 31) == 0 && sref >= 0)
-            atomic_add_fixed(st.energy + (size_t)sref * E_COUNT + term, to_fixed_d(e, ENERGY_SCALE));
-    } else if (sysi >= 0) {
-        atomic_add_fixed(st.energy + (size_t)sysi * E_COUNT + term, to_fixed_d(e, ENERGY_SCALE));
-    }
-}
-
 template <int INTEGRATOR, bool ENERGY>
 __global__ void k_integrate(DevState st, IntegrateParams p) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -91,7 +78,7 @@ __global__ void k_integrate(DevState st, IntegrateParams p) {
         const float q = st.xyzq[s].w;
         st.xyzq[s] = make_float4((float)x, (float)y, (float)z, q);
     }
-    if (ENERGY) add_energy_warp(st, sysi, ke, E_KINETIC);
+    if (ENERGY) add_energy_fixed(st.energy, sysi, ke, E_KINETIC);
 }
 
 int launch_integrate(const DevState& st, const IntegrateParams& p, bool energy, cudaStream_t s) {

@@ -123,15 +123,9 @@ __global__ void __launch_bounds__(256) k_nonbonded(DevState st, NbParams p) {
         atomic_add_fixed(st.fz + si, to_fixed(fiz, FORCE_SCALE));
     }
     if (ENERGY) {
-        e_lj = warp_sum(e_lj);
-        e_c = warp_sum(e_c);
-        vir = warp_sum(vir);
-        if (lane == 0) {
-            long long* E = st.energy + (size_t)sysi * E_COUNT;
-            atomic_add_fixed(E + E_LJ, to_fixed_d(e_lj, ENERGY_SCALE));
-            atomic_add_fixed(E + E_COUL, to_fixed_d(e_c, ENERGY_SCALE));
-            atomic_add_fixed(E + E_VIRIAL, to_fixed_d(vir, ENERGY_SCALE));
-        }
+        add_energy_fixed(st.energy, sysi, e_lj, E_LJ);
+        add_energy_fixed(st.energy, sysi, e_c, E_COUL);
+        add_energy_fixed(st.energy, sysi, vir, E_VIRIAL);
     }
 }
 
@@ -186,9 +180,7 @@ __global__ void k_exclusion_correction(DevState st, BondedTerms bt, NbParams p) 
         atomic_add_fixed(st.fz + sj, to_fixed(-fz, FORCE_SCALE));
         if (ENERGY) e = -(double)qq * (double)erf_kr * (double)rinv;
     }
-    if (ENERGY && sysi >= 0) {
-        atomic_add_fixed(st.energy + (size_t)sysi * E_COUNT + E_EXCL, to_fixed_d(e, ENERGY_SCALE));
-    }
+    if (ENERGY) add_energy_fixed(st.energy, sysi, e, E_EXCL);
 }
 
 int launch_exclusion_correction(const DevState& st, const BondedTerms& bt, const NbParams& p,

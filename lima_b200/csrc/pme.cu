@@ -173,6 +173,10 @@ __device__ __forceinline__ void grid_coord(float x, float inv_h, int K, int& bas
     base = (int)fl;
     frac = u - fl;
     if (base >= K) base -= K;
+    if (!(base >= 0 && base < K)) {  // non-finite position: keep the index in range
+        base = 0;
+        frac = 0.f;
+    }
 }
 
 __global__ void k_spread(DevState st) {
@@ -409,18 +413,7 @@ __global__ void k_gather(DevState st) {
             if (ENERGY) e = 0.5 * (double)p.w * (double)phi;
         }
     }
-    if (ENERGY) {
-        const int s_first = __shfl_sync(0xffffffffu, sysi, 0);
-        const bool uniform = __all_sync(0xffffffffu, sysi == s_first || sysi < 0);
-        const int sref = __reduce_max_sync(0xffffffffu, sysi);
-        if (uniform) {
-            e = warp_sum(e);
-            if ((threadIdx.x & 31) == 0 && sref >= 0)
-                atomic_add_fixed(st.energy + (size_t)sref * E_COUNT + E_RECIP, to_fixed_d(e, ENERGY_SCALE));
-        } else if (sysi >= 0) {
-            atomic_add_fixed(st.energy + (size_t)sysi * E_COUNT + E_RECIP, to_fixed_d(e, ENERGY_SCALE));
-        }
-    }
+    if (ENERGY) add_energy_fixed(st.energy, sysi, e, E_RECIP);
 }
 
 // ------------------------------------------------------------------ driver
