@@ -205,6 +205,32 @@ LIMA_API int lima_reset_timings(lima_engine* h);
  * step ends with a device synchronisation. */
 LIMA_API int lima_enable_phase_timing(lima_engine* h, int enable);
 
+/* ------------------------------------------------ allocation-free PME stage
+ * No counterpart in the reference: this entry point exists for callers that
+ * may not allocate device memory (work recorded while a stream is captured
+ * into a CUDA graph, a plug-in inside an application that owns every device
+ * allocation through its own pool, a real-time loop that must not allocate
+ * after start-up).  It computes the smooth-PME reciprocal forces and energy of
+ * one set of charges with the engine's own PME kernels (accurate conventions:
+ * B-spline moduli, analytic gather), using a static scratch array instead of
+ * allocated grids; it calls no allocator.
+ *   d_xyzq   device array of n_atoms x {x, y, z [nm], q [kC/mol]} (float)
+ *   d_forces device array of n_atoms x 3 doubles, overwritten [J/mol/nm]
+ *   d_energy device pointer to one double: 1/2 sum q phi [J/mol] (no self term)
+ *   stream   a cudaStream_t, or NULL for the default stream; the call is
+ *            asynchronous on it and uses the current device
+ * Limits: at most 64^3 real grid points and 128 points per dimension; larger
+ * grids return LIMA_ERR_OVERFLOW; dimensions must factor into 2, 3 and 5
+ * (LIMA_ERR_UNSUPPORTED otherwise).  Every GPU that loads the library holds
+ * about 5 MB of static device memory for it until the process exits.  The first
+ * call on a device looks up the scratch array's device address; make that
+ * first call before any stream capture.  All calls share the array and it
+ * keeps the last call's contents (each call clears what must start at zero):
+ * calls that overlap on the GPU race. */
+LIMA_API int lima_pme_recip_noalloc(const float* d_xyzq, int n_atoms, double lx, double ly, double lz,
+                                    int kx, int ky, int kz, double kappa, double* d_forces,
+                                    double* d_energy, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

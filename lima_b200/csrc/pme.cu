@@ -16,7 +16,10 @@
 // B-spline weights sit on nodes floor(u)-1..floor(u)+2 exactly as in
 // ChargeblockDistributeToGrid (PME.cuh:249-300) and LAL::CalcBspline
 // (DeviceAlgorithmsPrivate.cuh:7-30).
+#include <mutex>
+
 #include "engine.h"
+#include "lima_b200.h"
 
 namespace lima {
 
@@ -480,3 +483,352 @@ void pme_set_smem_limits(int maxn) {
 }
 
 }  // namespace lima
+
+namespace lima {
+
+// ===================================================================== no-alloc
+// Reciprocal-space PME for callers that cannot allocate device memory.
+//
+// Some callers of this library may not call cudaMalloc: code running while a
+// stream is being captured into a CUDA graph, a plug-in inside an application
+// that owns every device allocation through its own pool, or a real-time loop
+// that must not allocate after start-up.  For them lima_pme_recip_noalloc
+// computes the same reciprocal-space forces and energy as the engine's PME
+// stage, using the static scratch array below instead of allocated grids.
+//
+// Limits: at most NOALLOC_MAX_POINTS real grid points (64^3) and at most
+// NOALLOC_MAX_DIM points per dimension.  Every GPU that loads this library
+// holds NOALLOC_SCRATCH_BYTES (~5 MB) of static device memory until the
+// process exits.  All calls share the array and it keeps the last call's
+// contents; each call clears what must start at zero.  Calls whose work
+// overlaps on the GPU (other streams, other host threads) race on the array.
+namespace {
+constexpr int NOALLOC_MAX_POINTS = 64 * 64 * 64;
+constexpr int NOALLOC_MAX_DIM = 128;
+constexpr size_t NOALLOC_HALF_POINTS = (size_t)NOALLOC_MAX_POINTS * 5 / 8;  // >= (K0/2+1)K1K2 for K0 >= 8
+constexpr size_t NOALLOC_OFF_REAL = (size_t)NOALLOC_MAX_POINTS * sizeof(long long);
+constexpr size_t NOALLOC_OFF_CPLX = NOALLOC_OFF_REAL + (size_t)NOALLOC_MAX_POINTS * sizeof(float);
+constexpr size_t NOALLOC_OFF_THETA = NOALLOC_OFF_CPLX + NOALLOC_HALF_POINTS * sizeof(float2);
+constexpr size_t NOALLOC_OFF_ENERGY = NOALLOC_OFF_THETA + NOALLOC_HALF_POINTS * sizeof(float);
+constexpr size_t NOALLOC_SCRATCH_BYTES = NOALLOC_OFF_ENERGY + 256;
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_pme_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+
+struct NaGrid {
+    int n[3];
+    float inv_h[3];
+    double box[3];
+    double kappa;
+    FftPlanDev px, py, pz;
+};
+
+__device__ __forceinline__ long long* na_grid(unsigned char* s) { return reinterpret_cast<long long*>(s); }
+__device__ __forceinline__ float* na_real(unsigned char* s) { return reinterpret_cast<float*>(s + NOALLOC_OFF_REAL); }
+__device__ __forceinline__ float2* na_cplx(unsigned char* s) { return reinterpret_cast<float2*>(s + NOALLOC_OFF_CPLX); }
+__device__ __forceinline__ float* na_theta(unsigned char* s) { return reinterpret_cast<float*>(s + NOALLOC_OFF_THETA); }
+__device__ __forceinline__ long long* na_energy(unsigned char* s) {
+    return reinterpret_cast<long long*>(s + NOALLOC_OFF_ENERGY);
+}
+
+// zero the charge grid and the energy accumulator; influence function (SPME,
+// B-spline moduli of the centred order-4 weights, 1/N folded in) in FP64
+__global__ void k_na_prepare(unsigned char* scratch, NaGrid g) {
+    const int K0 = g.n[0], K1 = g.n[1], K2 = g.n[2], K0h = K0 / 2 + 1;
+    const int N = K0 * K1 * K2, Nh = K0h * K1 * K2;
+    long long* grid = na_grid(scratch);
+    float* theta = na_theta(scratch);
+    const double ke = 8.9875517873681764e9 / 1e-9 / 6.02214076e23 * 1000.0 * 1000.0;
+    const double pi = 3.14159265358979323846;
+    const double V = g.box[0] * g.box[1] * g.box[2];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < max(N, Nh); i += gridDim.x * blockDim.x) {
+        if (i < N) grid[i] = 0;
+        if (i < Nh) {
+            const int x = i % K0h, y = (i / K0h) % K1, z = i / (K0h * K1);
+            const int m[3] = {x, y <= K1 / 2 ? y : y - K1, z <= K2 / 2 ? z : z - K2};
+            double t = 0.0;
+            if (m[0] != 0 || m[1] != 0 || m[2] != 0) {
+                double k2 = 0.0, B = 1.0;
+                for (int d = 0; d < 3; ++d) {
+                    const double kv = 2.0 * pi * m[d] / g.box[d];
+                    k2 += kv * kv;
+                    const double b = 2.0 / 3.0 + cos(2.0 * pi * m[d] / g.n[d]) / 3.0;
+                    B *= b * b;
+                }
+                t = ke * 4.0 * pi / k2 * exp(-k2 / (4.0 * g.kappa * g.kappa)) / V / B;
+            }
+            theta[i] = (float)t;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *na_energy(scratch) = 0;
+}
+
+__global__ void k_na_spread(const float4* __restrict__ xyzq, int n, unsigned char* scratch, NaGrid g) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n) return;
+    const float4 p = xyzq[a];
+    if (p.w == 0.f) return;
+    const int K0 = g.n[0], K1 = g.n[1], K2 = g.n[2];
+    int b0, b1, b2;
+    float f0, f1, f2;
+    grid_coord(p.x, g.inv_h[0], K0, b0, f0);
+    grid_coord(p.y, g.inv_h[1], K1, b1, f1);
+    grid_coord(p.z, g.inv_h[2], K2, b2, f2);
+    float wx[4], wy[4], wz[4];
+    bspline4(f0, wx);
+    bspline4(f1, wy);
+    bspline4(f2, wz);
+    long long* grid = na_grid(scratch);
+    int ix[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) ix[k] = wrapk(b0 - 1 + k, K0);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const int z = wrapk(b2 - 1 + c, K2);
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int y = wrapk(b1 - 1 + b, K1);
+            const float qyz = p.w * wy[b] * wz[c];
+            long long* row = grid + (size_t)K0 * (y + (size_t)K1 * z);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) atomic_add_fixed(row + ix[k], to_fixed(qyz * wx[k], GRID_SCALE));
+        }
+    }
+}
+
+// x pass forward: block b handles lines [8b, 8b+8) of the K1*K2 lines
+__global__ void k_na_fft_x_fwd(unsigned char* scratch, NaGrid g) {
+    extern __shared__ float2 sm[];
+    const FftPlanDev& pl = g.px;
+    const int K0 = pl.n, K0h = K0 / 2 + 1, stride = K0 | 1, maxn = NOALLOC_MAX_DIM;
+    float2* tw = sm;
+    float2* A = sm + maxn;
+    float2* B = A + FFT_XLINES * (maxn + 1);
+    make_twiddles(tw, K0);
+    const int line0 = blockIdx.x * FFT_XLINES;
+    const int nl = min(FFT_XLINES, g.n[1] * g.n[2] - line0);
+    long long* grid = na_grid(scratch) + (size_t)line0 * K0;
+    for (int i = threadIdx.x; i < nl * K0; i += blockDim.x) {
+        const int l = i / K0, x = i - l * K0;
+        A[l * stride + x] = make_float2((float)((double)grid[(size_t)l * K0 + x] * (1.0 / GRID_SCALE)), 0.f);
+    }
+    __syncthreads();
+    const float2* res = fft_lines(A, B, nl, stride, pl, tw, -1.f);
+    float2* out = na_cplx(scratch) + (size_t)line0 * K0h;
+    for (int i = threadIdx.x; i < nl * K0h; i += blockDim.x) {
+        const int l = i / K0h, k = i - l * K0h;
+        out[(size_t)l * K0h + k] = res[l * stride + k];
+    }
+}
+
+__global__ void k_na_fft_x_inv(unsigned char* scratch, NaGrid g) {
+    extern __shared__ float2 sm[];
+    const FftPlanDev& pl = g.px;
+    const int K0 = pl.n, K0h = K0 / 2 + 1, stride = K0 | 1, maxn = NOALLOC_MAX_DIM;
+    float2* tw = sm;
+    float2* A = sm + maxn;
+    float2* B = A + FFT_XLINES * (maxn + 1);
+    make_twiddles(tw, K0);
+    const int line0 = blockIdx.x * FFT_XLINES;
+    const int nl = min(FFT_XLINES, g.n[1] * g.n[2] - line0);
+    const float2* in = na_cplx(scratch) + (size_t)line0 * K0h;
+    for (int i = threadIdx.x; i < nl * K0; i += blockDim.x) {
+        const int l = i / K0, k = i - l * K0;
+        float2 v;
+        if (k < K0h) {
+            v = in[(size_t)l * K0h + k];
+        } else {
+            v = in[(size_t)l * K0h + (K0 - k)];
+            v.y = -v.y;
+        }
+        A[l * stride + k] = v;
+    }
+    __syncthreads();
+    const float2* res = fft_lines(A, B, nl, stride, pl, tw, 1.f);
+    float* out = na_real(scratch) + (size_t)line0 * K0;
+    for (int i = threadIdx.x; i < nl * K0; i += blockDim.x) {
+        const int l = i / K0, x = i - l * K0;
+        out[(size_t)l * K0 + x] = res[l * stride + x].x;
+    }
+}
+
+// y pass: block (x-tile, z)
+__global__ void k_na_fft_y(unsigned char* scratch, NaGrid g, float sigma) {
+    extern __shared__ float2 sm[];
+    const FftPlanDev& pl = g.py;
+    const int K0h = g.n[0] / 2 + 1, K1 = pl.n, stride = K1 | 1, maxn = NOALLOC_MAX_DIM;
+    float2* tw = sm;
+    float2* A = sm + maxn;
+    float2* B = A + FFT_TX * (maxn + 1);
+    make_twiddles(tw, K1);
+    const int ntx = (K0h + FFT_TX - 1) / FFT_TX;
+    const int x0 = (blockIdx.x % ntx) * FFT_TX, z = blockIdx.x / ntx;
+    const int tx = min(FFT_TX, K0h - x0);
+    float2* gp = na_cplx(scratch) + (size_t)z * K1 * K0h + x0;
+    for (int i = threadIdx.x; i < K1 * FFT_TX; i += blockDim.x) {
+        const int y = i / FFT_TX, c = i - y * FFT_TX;
+        A[c * stride + y] = c < tx ? gp[(size_t)y * K0h + c] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    const float2* res = fft_lines(A, B, FFT_TX, stride, pl, tw, sigma);
+    for (int i = threadIdx.x; i < K1 * FFT_TX; i += blockDim.x) {
+        const int y = i / FFT_TX, c = i - y * FFT_TX;
+        if (c < tx) gp[(size_t)y * K0h + c] = res[c * stride + y];
+    }
+}
+
+// z pass: block (x-tile, y); forward FFT, x theta, inverse FFT
+__global__ void k_na_fft_z_conv(unsigned char* scratch, NaGrid g) {
+    extern __shared__ float2 sm[];
+    const FftPlanDev& pl = g.pz;
+    const int K0h = g.n[0] / 2 + 1, K1 = g.n[1], K2 = pl.n, stride = K2 | 1, maxn = NOALLOC_MAX_DIM;
+    float2* tw = sm;
+    float2* A = sm + maxn;
+    float2* B = A + FFT_TX * (maxn + 1);
+    make_twiddles(tw, K2);
+    const int ntx = (K0h + FFT_TX - 1) / FFT_TX;
+    const int x0 = (blockIdx.x % ntx) * FFT_TX, y = blockIdx.x / ntx;
+    const int tx = min(FFT_TX, K0h - x0);
+    const size_t plane = (size_t)K1 * K0h;
+    float2* gp = na_cplx(scratch) + (size_t)y * K0h + x0;
+    const float* th = na_theta(scratch) + (size_t)y * K0h + x0;
+    for (int i = threadIdx.x; i < K2 * FFT_TX; i += blockDim.x) {
+        const int z = i / FFT_TX, c = i - z * FFT_TX;
+        A[c * stride + z] = c < tx ? gp[z * plane + c] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    float2* res = fft_lines(A, B, FFT_TX, stride, pl, tw, -1.f);
+    for (int i = threadIdx.x; i < K2 * FFT_TX; i += blockDim.x) {
+        const int z = i / FFT_TX, c = i - z * FFT_TX;
+        const float t = c < tx ? th[z * plane + c] : 0.f;
+        res[c * stride + z] = cscale(res[c * stride + z], t);
+    }
+    __syncthreads();
+    float2* other = res == A ? B : A;
+    const float2* res2 = fft_lines(res, other, FFT_TX, stride, pl, tw, 1.f);
+    for (int i = threadIdx.x; i < K2 * FFT_TX; i += blockDim.x) {
+        const int z = i / FFT_TX, c = i - z * FFT_TX;
+        if (c < tx) gp[z * plane + c] = res2[c * stride + z];
+    }
+}
+
+// analytic-derivative gather; forces are rounded through the same int64 fixed
+// point the engine accumulates in, so both paths return identical values
+__global__ void k_na_gather(const float4* __restrict__ xyzq, int n, unsigned char* scratch, NaGrid g,
+                            double* __restrict__ forces) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    double e = 0.0;
+    if (a < n) {
+        const float4 p = xyzq[a];
+        float fx = 0.f, fy = 0.f, fz = 0.f;
+        if (p.w != 0.f) {
+            const int K0 = g.n[0], K1 = g.n[1], K2 = g.n[2];
+            int b0, b1, b2;
+            float f0, f1, f2;
+            grid_coord(p.x, g.inv_h[0], K0, b0, f0);
+            grid_coord(p.y, g.inv_h[1], K1, b1, f1);
+            grid_coord(p.z, g.inv_h[2], K2, b2, f2);
+            float wx[4], wy[4], wz[4], dx[4], dy[4], dz[4];
+            bspline4(f0, wx);
+            bspline4(f1, wy);
+            bspline4(f2, wz);
+            bspline4_d(f0, dx);
+            bspline4_d(f1, dy);
+            bspline4_d(f2, dz);
+            const float* gr = na_real(scratch);
+            int ix[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) ix[k] = wrapk(b0 - 1 + k, K0);
+            float phi = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const int z = wrapk(b2 - 1 + c, K2);
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    const int y = wrapk(b1 - 1 + b, K1);
+                    const float* row = gr + (size_t)K0 * (y + (size_t)K1 * z);
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const float v = row[ix[k]];
+                        phi += wx[k] * wy[b] * wz[c] * v;
+                        gx += dx[k] * wy[b] * wz[c] * v;
+                        gy += wx[k] * dy[b] * wz[c] * v;
+                        gz += wx[k] * wy[b] * dz[c] * v;
+                    }
+                }
+            }
+            fx = -p.w * gx * g.inv_h[0];
+            fy = -p.w * gy * g.inv_h[1];
+            fz = -p.w * gz * g.inv_h[2];
+            e = 0.5 * (double)p.w * (double)phi;
+        }
+        const double inv = 1.0 / FORCE_SCALE;
+        forces[3 * a] = (double)to_fixed(fx, FORCE_SCALE) * inv;
+        forces[3 * a + 1] = (double)to_fixed(fy, FORCE_SCALE) * inv;
+        forces[3 * a + 2] = (double)to_fixed(fz, FORCE_SCALE) * inv;
+    }
+    add_energy_fixed(na_energy(scratch), a < n ? 0 : -1, e, 0);
+}
+
+__global__ void k_na_finish(unsigned char* scratch, double* energy) {
+    *energy = (double)*na_energy(scratch) / ENERGY_SCALE;
+}
+
+namespace {
+std::mutex g_noalloc_mutex;
+void* g_noalloc_ptr[64] = {};
+}  // namespace
+
+}  // namespace lima
+
+extern "C" int lima_pme_recip_noalloc(const float* d_xyzq, int n_atoms, double lx, double ly, double lz,
+                                      int kx, int ky, int kz, double kappa, double* d_forces,
+                                      double* d_energy, void* stream) {
+    using namespace lima;
+    if (n_atoms < 0 || (n_atoms > 0 && (!d_xyzq || !d_forces)) || !d_energy) return LIMA_ERR_INVALID_ARG;
+    if (!(lx > 0.0 && ly > 0.0 && lz > 0.0) || !(kappa > 0.0)) return LIMA_ERR_INVALID_ARG;
+    const int K[3] = {kx, ky, kz};
+    for (int d = 0; d < 3; ++d)
+        if (K[d] < 8) return LIMA_ERR_INVALID_ARG;
+    if (kx > NOALLOC_MAX_DIM || ky > NOALLOC_MAX_DIM || kz > NOALLOC_MAX_DIM ||
+        (long long)kx * ky * kz > NOALLOC_MAX_POINTS)
+        return LIMA_ERR_OVERFLOW;  // beyond the static scratch array
+    NaGrid g{};
+    if (!make_fft_plan(kx, &g.px) || !make_fft_plan(ky, &g.py) || !make_fft_plan(kz, &g.pz))
+        return LIMA_ERR_UNSUPPORTED;  // grid dimensions must factor into 2, 3 and 5
+    const double L[3] = {lx, ly, lz};
+    for (int d = 0; d < 3; ++d) {
+        g.n[d] = K[d];
+        g.box[d] = L[d];
+        g.inv_h[d] = (float)(K[d] / L[d]);
+    }
+    g.kappa = kappa;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return LIMA_ERR_NO_DEVICE;
+    void* scratch = nullptr;
+    {
+        // set-up once per device: the device address of the static array
+        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+        if (!g_noalloc_ptr[dev]) {
+            void* ptr = nullptr;
+            if (cudaGetSymbolAddress(&ptr, g_pme_noalloc_scratch) != cudaSuccess || !ptr) return LIMA_ERR_CUDA;
+            g_noalloc_ptr[dev] = ptr;
+        }
+        scratch = g_noalloc_ptr[dev];
+    }
+    unsigned char* sp = static_cast<unsigned char*>(scratch);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int K0h = kx / 2 + 1;
+    const int ntx = (K0h + FFT_TX - 1) / FFT_TX;
+    const size_t sx = fft_smem_bytes(FFT_XLINES, NOALLOC_MAX_DIM), sy = fft_smem_bytes(FFT_TX, NOALLOC_MAX_DIM);
+    k_na_prepare<<<256, 256, 0, s>>>(sp, g);
+    if (n_atoms > 0) k_na_spread<<<(n_atoms + 255) / 256, 256, 0, s>>>(reinterpret_cast<const float4*>(d_xyzq), n_atoms, sp, g);
+    k_na_fft_x_fwd<<<(ky * kz + FFT_XLINES - 1) / FFT_XLINES, 256, sx, s>>>(sp, g);
+    k_na_fft_y<<<ntx * kz, 256, sy, s>>>(sp, g, -1.f);
+    k_na_fft_z_conv<<<ntx * ky, 256, sy, s>>>(sp, g);
+    k_na_fft_y<<<ntx * kz, 256, sy, s>>>(sp, g, 1.f);
+    k_na_fft_x_inv<<<(ky * kz + FFT_XLINES - 1) / FFT_XLINES, 256, sx, s>>>(sp, g);
+    if (n_atoms > 0) k_na_gather<<<(n_atoms + 255) / 256, 256, 0, s>>>(reinterpret_cast<const float4*>(d_xyzq), n_atoms, sp, g, d_forces);
+    k_na_finish<<<1, 1, 0, s>>>(sp, d_energy);
+    return cudaGetLastError() == cudaSuccess ? LIMA_OK : LIMA_ERR_CUDA;
+}

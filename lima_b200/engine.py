@@ -35,7 +35,7 @@ EXPORTED = [
     "lima_set_pairbonds", "lima_set_exclusions", "lima_set_pme_grid", "lima_set_state",
     "lima_get_state", "lima_compute_forces", "lima_step", "lima_minimize", "lima_get_forces",
     "lima_get_energies", "lima_get_pairlist", "lima_get_status", "lima_clear_status",
-    "lima_get_timings", "lima_reset_timings", "lima_enable_phase_timing",
+    "lima_get_timings", "lima_reset_timings", "lima_enable_phase_timing", "lima_pme_recip_noalloc",
 ]
 
 
@@ -116,6 +116,10 @@ def load_library(path: str = LIB_PATH):
         "lima_get_timings": (ctypes.c_int, [h, P(Timings)]),
         "lima_reset_timings": (ctypes.c_int, [h]),
         "lima_enable_phase_timing": (ctypes.c_int, [h, ctypes.c_int]),
+        "lima_pme_recip_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                                  ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                  ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p,
+                                                  ctypes.c_void_p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
