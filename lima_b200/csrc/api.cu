@@ -475,6 +475,7 @@ void lima_engine::setup() {
     D.fy = dalloc<long long>(S);
     D.fz = dalloc<long long>(S);
     D.orig = dalloc<int>(S);
+    D.slot_mol = dalloc<int>(S);
     D.tvel = dalloc<float4>(S);
     D.tfprev = dalloc<float4>(S);
     D.tadam_m = dalloc<float4>(S);

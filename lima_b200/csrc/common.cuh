@@ -53,8 +53,10 @@ struct SysDesc {
     int pad_;
 };
 
+// scale is a power of two, so v * (float)scale is exact and one float->int64
+// conversion gives the same integer as rounding (double)v * scale
 __device__ __forceinline__ long long to_fixed(float v, double scale) {
-    return __double2ll_rn((double)v * scale);
+    return __float2ll_rn(v * (float)scale);
 }
 __device__ __forceinline__ long long to_fixed_d(double v, double scale) {
     return __double2ll_rn(v * scale);

@@ -33,6 +33,7 @@ struct DevState {
     float4* adam_v = nullptr;       // second moments
     long long *fx = nullptr, *fy = nullptr, *fz = nullptr;
     int* orig = nullptr;
+    int* slot_mol = nullptr;        // molecule id per slot (-1 for padding)
     float4* tvel = nullptr;         // permutation scratch
     float4* tfprev = nullptr;
     float4* tadam_m = nullptr;

@@ -174,6 +174,7 @@ __global__ void k_gather_slots(DevState st, int from_input) {
         st.tadam_v[s] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
     st.orig[s] = a;
+    st.slot_mol[s] = a >= 0 ? st.mol[a] : -1;
 }
 
 __global__ void k_finish_slots(DevState st) {
@@ -246,9 +247,10 @@ __global__ void k_pairsearch(DevState st, float rlist) {
     // per-lane i-atom data for the interaction mask (lane -> ii = lane & 7)
     const int ii = lane & 7, jj0 = lane >> 3;
     const int ai = st.orig[ci * CLUSTER + ii];
-    const int mi = ai >= 0 ? st.mol[ai] : -1;
+    const int mi = st.slot_mol[ci * CLUSTER + ii];
     const int eb = ai >= 0 ? st.excl_off[ai] : 0;
     const int ee = ai >= 0 ? st.excl_off[ai + 1] : 0;
+    const float4 xi = st.xyzq[ci * CLUSTER + ii];
 
     // column window (every column visited once even when the window wraps)
     int cx0 = (int)floorf((ilo.x - R) / sd.col_w[0]);
@@ -308,14 +310,24 @@ __global__ void k_pairsearch(DevState st, float rlist) {
                     const unsigned rest = sh_src & (sh_src - 1u);
                     if (lane == src) shifts = rest;
                     if (rest == 0u) pending &= pending - 1u;
-                    // interaction mask: bit (jj*8 + ii)
+                    // interaction mask: bit (jj*8 + ii); a pair is kept when both atoms
+                    // are real, it is not excluded, it is counted once on the diagonal
+                    // and its image distance is inside the list radius (Verlet buffer)
+                    const int3 sh = decode_shift(code);
+                    const float shx = sh.x * L[0], shy = sh.y * L[1], shz = sh.z * L[2];
                     bool ok[2];
                     for (int h = 0; h < 2; ++h) {
                         const int jj = jj0 + 4 * h;
-                        const int aj = st.orig[jc * CLUSTER + jj];
-                        bool o = ai >= 0 && aj >= 0;
+                        const int sj = jc * CLUSTER + jj;
+                        const int mj = st.slot_mol[sj];
+                        bool o = ai >= 0 && mj >= 0;
                         if (o && jc == ci) o = jj > ii;
-                        if (o && mi == st.mol[aj]) o = !excluded(st, ai, aj, eb, ee);
+                        if (o) {
+                            const float4 xj = st.xyzq[sj];
+                            const float dx = xj.x + shx - xi.x, dy = xj.y + shy - xi.y, dz = xj.z + shz - xi.z;
+                            o = dx * dx + dy * dy + dz * dz < R2;
+                        }
+                        if (o && mi == mj) o = !excluded(st, ai, st.orig[sj], eb, ee);
                         ok[h] = o;
                     }
                     const unsigned lo32 = __ballot_sync(0xffffffffu, ok[0]);

@@ -21,6 +21,85 @@
 
 namespace lima {
 
+// erfc(x) ~ t (a1 + t (a2 + t (a3 + t (a4 + t a5)))) exp(-x^2), t = 1/(1 + p x):
+// Abramowitz & Stegun, Handbook of Mathematical Functions, 7.1.26 (|error| <=
+// 1.5e-7).  Its exp(-x^2) factor is the one the Ewald force's Gaussian term
+// needs, so the pair costs one exponential and one reciprocal.
+constexpr float AS_P = 0.3275911f;
+constexpr float AS_A1 = 0.254829592f, AS_A2 = -0.284496736f, AS_A3 = 1.421413741f;
+constexpr float AS_A4 = -1.453152027f, AS_A5 = 1.061405429f;
+
+struct PairAcc {
+    float fix, fiy, fiz;
+    double e_lj, e_c, vir;
+};
+
+// One half tile: i-atom `ii` of the lane against j-atom jj = jj0 + 4h.  Returns
+// the force on the j-atom (to be reduced over the 8 lanes sharing it).
+template <int ES, bool ENERGY>
+__device__ __forceinline__ float3 half_tile(const DevState& st, const NbParams& p, const float4& xi,
+                                           const float2& lji, float qi, int sj, float sx, float sy, float sz,
+                                           bool bit, PairAcc& acc) {
+    const float4 xj = st.xyzq[sj];
+    const float2 ljj = st.ljp[sj];
+    const float dx = xj.x + sx - xi.x;
+    const float dy = xj.y + sy - xi.y;
+    const float dz = xj.z + sz - xi.z;
+    const float r2 = dx * dx + dy * dy + dz * dz;
+    float fs = 0.f;
+    if (bit && r2 <= p.rc2) {
+        const float rinv = rsqrtf(r2);
+        const float rinv2 = rinv * rinv;
+        const float sig = lji.x + ljj.x;
+        const float eps = lji.y * ljj.y;
+        float s6 = sig * sig * rinv2;
+        s6 = s6 * s6 * s6;
+        fs = 24.f * eps * s6 * rinv2 * (1.f - 2.f * s6);
+        if (ENERGY) acc.e_lj += (double)(4.f * eps * s6 * (s6 - 1.f));
+        if (ES != 0) {
+            const float qq = qi * xj.w;
+            float fc, ec;
+            if (ES == 2) {
+                const float r = r2 * rinv;
+                const float x = p.kappa * r;
+                const float t = __fdividef(1.f, fmaf(AS_P, x, 1.f));
+                const float poly = t * fmaf(t, fmaf(t, fmaf(t, fmaf(t, AS_A5, AS_A4), AS_A3), AS_A2), AS_A1);
+                const float ex = __expf(-x * x);
+                const float erfc_x = poly * ex;
+                fc = qq * rinv2 * rinv * fmaf(p.two_kappa_sqrtpi * r, ex, erfc_x);
+                ec = qq * rinv * erfc_x;
+            } else {
+                fc = qq * rinv2 * rinv;
+                ec = qq * rinv;
+            }
+            fs -= fc;
+            if (ENERGY) acc.e_c += (double)ec;
+        }
+        if (p.em) fs = fmaxf(fminf(fs, 1e20f), -1e20f);
+        if (ENERGY) acc.vir += 0.5 * (double)(fs * r2);  // -1/2 r_ij . f_ij
+    }
+    const float fx = fs * dx, fy = fs * dy, fz = fs * dz;
+    acc.fix += fx;
+    acc.fiy += fy;
+    acc.fiz += fz;
+    return make_float3(-fx, -fy, -fz);
+}
+
+// sums a j-force over the 8 lanes with the same jj0 and adds it once (lane ii == 0)
+__device__ __forceinline__ void flush_j(const DevState& st, float3 f, int sj, int ii) {
+#pragma unroll
+    for (int o = 1; o < 8; o <<= 1) {
+        f.x += __shfl_xor_sync(0xffffffffu, f.x, o);
+        f.y += __shfl_xor_sync(0xffffffffu, f.y, o);
+        f.z += __shfl_xor_sync(0xffffffffu, f.z, o);
+    }
+    if (ii == 0) {
+        atomic_add_fixed(st.fx + sj, to_fixed(f.x, FORCE_SCALE));
+        atomic_add_fixed(st.fy + sj, to_fixed(f.y, FORCE_SCALE));
+        atomic_add_fixed(st.fz + sj, to_fixed(f.z, FORCE_SCALE));
+    }
+}
+
 template <int ES, bool ENERGY>
 __global__ void __launch_bounds__(256) k_nonbonded(DevState st, NbParams p) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -36,8 +115,7 @@ __global__ void __launch_bounds__(256) k_nonbonded(DevState st, NbParams p) {
     const float4 xi = st.xyzq[ci * CLUSTER + ii];
     const float2 lji = st.ljp[ci * CLUSTER + ii];
     const float qi = xi.w * p.ke;
-    float fix = 0.f, fiy = 0.f, fiz = 0.f;
-    double e_lj = 0.0, e_c = 0.0, vir = 0.0;
+    PairAcc acc{0.f, 0.f, 0.f, 0.0, 0.0, 0.0};
     const size_t base = (size_t)ci * st.pl_cap;
     for (int k = 0; k < n; ++k) {
         const int ent = st.pl_j[base + k];
@@ -45,71 +123,21 @@ __global__ void __launch_bounds__(256) k_nonbonded(DevState st, NbParams p) {
         const int cj = ent & ((1 << JCLUSTER_BITS) - 1);
         const int3 sh = decode_shift((unsigned)ent >> JCLUSTER_BITS);
         const float sx = sh.x * Lx, sy = sh.y * Ly, sz = sh.z * Lz;
-        float fjx[2], fjy[2], fjz[2];
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int jj = jj0 + 4 * h;
-            const float4 xj = st.xyzq[cj * CLUSTER + jj];
-            const float2 ljj = st.ljp[cj * CLUSTER + jj];
-            const float dx = xj.x + sx - xi.x;
-            const float dy = xj.y + sy - xi.y;
-            const float dz = xj.z + sz - xi.z;
-            const float r2 = dx * dx + dy * dy + dz * dz;
-            const bool on = ((mask >> (jj * 8 + ii)) & 1ull) && r2 <= p.rc2;
-            float fs = 0.f;
-            if (on) {
-                const float rinv = rsqrtf(r2);
-                const float rinv2 = rinv * rinv;
-                const float sig = lji.x + ljj.x;
-                const float eps = lji.y * ljj.y;
-                float s = sig * sig * rinv2;
-                s = s * s * s;
-                fs = 24.f * eps * s * rinv2 * (1.f - 2.f * s);
-                if (ENERGY) e_lj += (double)(4.f * eps * s * (s - 1.f));
-                if (ES != 0) {
-                    const float qq = qi * xj.w;
-                    float fc = qq * rinv2 * rinv;
-                    float ec = qq * rinv;
-                    if (ES == 2) {
-                        const float r = r2 * rinv;
-                        const float kr = p.kappa * r;
-                        const float erfc_kr = erfcf(kr);
-                        fc *= erfc_kr + p.two_kappa_sqrtpi * r * __expf(-kr * kr);
-                        ec *= erfc_kr;
-                    }
-                    fs -= fc;
-                    if (ENERGY) e_c += (double)ec;
-                }
-                if (p.em) fs = fmaxf(fminf(fs, 1e20f), -1e20f);
-                if (ENERGY) vir += 0.5 * (double)(fs * r2);  // -1/2 r_ij . f_ij
-            }
-            const float fx = fs * dx, fy = fs * dy, fz = fs * dz;
-            fix += fx;
-            fiy += fy;
-            fiz += fz;
-            fjx[h] = -fx;
-            fjy[h] = -fy;
-            fjz[h] = -fz;
+        // mask bit (jj*8 + ii): the lane's bit of half h is bit `lane` of word h.
+        // A half with no bit set is skipped by the whole warp.
+        const unsigned lo = (unsigned)mask, hi = (unsigned)(mask >> 32);
+        if (lo) {
+            const int sj = cj * CLUSTER + jj0;
+            const float3 fj = half_tile<ES, ENERGY>(st, p, xi, lji, qi, sj, sx, sy, sz, (lo >> lane) & 1u, acc);
+            flush_j(st, fj, sj, ii);
         }
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-#pragma unroll
-            for (int o = 1; o < 8; o <<= 1) {
-                fjx[h] += __shfl_xor_sync(0xffffffffu, fjx[h], o);
-                fjy[h] += __shfl_xor_sync(0xffffffffu, fjy[h], o);
-                fjz[h] += __shfl_xor_sync(0xffffffffu, fjz[h], o);
-            }
-        }
-        if (ii == 0) {
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int sj = cj * CLUSTER + jj0 + 4 * h;
-                atomic_add_fixed(st.fx + sj, to_fixed(fjx[h], FORCE_SCALE));
-                atomic_add_fixed(st.fy + sj, to_fixed(fjy[h], FORCE_SCALE));
-                atomic_add_fixed(st.fz + sj, to_fixed(fjz[h], FORCE_SCALE));
-            }
+        if (hi) {
+            const int sj = cj * CLUSTER + jj0 + 4;
+            const float3 fj = half_tile<ES, ENERGY>(st, p, xi, lji, qi, sj, sx, sy, sz, (hi >> lane) & 1u, acc);
+            flush_j(st, fj, sj, ii);
         }
     }
+    float fix = acc.fix, fiy = acc.fiy, fiz = acc.fiz;
     fix += __shfl_xor_sync(0xffffffffu, fix, 8);
     fiy += __shfl_xor_sync(0xffffffffu, fiy, 8);
     fiz += __shfl_xor_sync(0xffffffffu, fiz, 8);
@@ -123,9 +151,9 @@ __global__ void __launch_bounds__(256) k_nonbonded(DevState st, NbParams p) {
         atomic_add_fixed(st.fz + si, to_fixed(fiz, FORCE_SCALE));
     }
     if (ENERGY) {
-        add_energy_fixed(st.energy, sysi, e_lj, E_LJ);
-        add_energy_fixed(st.energy, sysi, e_c, E_COUL);
-        add_energy_fixed(st.energy, sysi, vir, E_VIRIAL);
+        add_energy_fixed(st.energy, sysi, acc.e_lj, E_LJ);
+        add_energy_fixed(st.energy, sysi, acc.e_c, E_COUL);
+        add_energy_fixed(st.energy, sysi, acc.vir, E_VIRIAL);
     }
 }
 
