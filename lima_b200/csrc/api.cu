@@ -571,6 +571,26 @@ void lima_engine::setup() {
                     }
         }
         D.pme_theta = upload(theta);
+        // twiddle tables, one per distinct grid length, in FP64 rounded to float
+        std::vector<float2> tw;
+        std::vector<std::pair<int, int>> tw_offsets;  // (length, offset)
+        auto tw_of = [&](int len) {
+            for (auto& pr : tw_offsets)
+                if (pr.first == len) return pr.second;
+            const int off = (int)tw.size();
+            for (int k = 0; k < len; ++k) {
+                const double a = 2.0 * kPi * k / len;
+                tw.push_back(make_float2((float)std::cos(a), (float)-std::sin(a)));
+            }
+            tw_offsets.push_back({len, off});
+            return off;
+        };
+        for (int s = 0; s < ns; ++s) {
+            const int* g = sd[s].pme_n;
+            if (g[0] == 0) continue;
+            set_pme_sys_twiddles(plans.data() + s * pme_sys_dev_size(), tw_of(g[0]), tw_of(g[1]), tw_of(g[2]));
+        }
+        D.pme_tw = upload(tw);
         char* dplans = dalloc<char>(plans.size());
         CK(cudaMemcpy(dplans, plans.data(), plans.size(), cudaMemcpyHostToDevice));
         P.sys_plans = dplans;

@@ -74,6 +74,7 @@ struct DevState {
     float* pme_real = nullptr;           // real-space potential grid
     float2* pme_cplx = nullptr;          // half-complex grid
     float* pme_theta = nullptr;          // influence function on the half-complex grid
+    float2* pme_tw = nullptr;            // twiddle tables e^{-2 pi i k/n} for every grid length
     int pme_total_real = 0;
     int pme_total_cplx = 0;
 
@@ -129,6 +130,7 @@ struct PmePlan {
 };
 size_t pme_sys_dev_size();
 bool fill_pme_sys_dev(void* dst, int kx, int ky, int kz);
+void set_pme_sys_twiddles(void* dst, int offx, int offy, int offz);
 void pme_set_smem_limits(int maxn);
 int launch_pme(const DevState& st, const PmePlan& plan, bool energy, cudaStream_t s);
 // integrate.cu

@@ -11,12 +11,10 @@
 // Every unordered pair is evaluated once (Newton's third law), where the
 // reference evaluates each directed pair.
 //
-// Work mapping: one warp per i-cluster (8 atoms) walks its list of j-clusters;
-// lane = (jj0 << 3) | ii handles i-atom ii against j-atoms jj0 and jj0+4.  The
-// i forces stay in registers for the whole list; the j forces are reduced over
-// the 8 lanes sharing a j-atom with three xor-shuffles and added once per
-// cluster pair as int64 fixed point, so the result does not depend on the
-// order in which warps finish.
+// Work mapping (see k_nonbonded): one warp per i-cluster; each lane owns one
+// j-atom of four list entries at a time and walks the 8 i-atoms.  Forces are
+// added as int64 fixed point, so the result does not depend on the order in
+// which warps finish.
 #include "engine.h"
 
 namespace lima {
@@ -30,78 +28,55 @@ constexpr float AS_A1 = 0.254829592f, AS_A2 = -0.284496736f, AS_A3 = 1.421413741
 constexpr float AS_A4 = -1.453152027f, AS_A5 = 1.061405429f;
 
 struct PairAcc {
-    float fix, fiy, fiz;
     double e_lj, e_c, vir;
 };
 
-// One half tile: i-atom `ii` of the lane against j-atom jj = jj0 + 4h.  Returns
-// the force on the j-atom (to be reduced over the 8 lanes sharing it).
+// One atom pair: i-atom (xi, lji, qi) and the lane's j-atom (xj, ljj).  Returns the
+// scalar fs with F_i = fs * (r_j - r_i); 0 outside the cutoff.
 template <int ES, bool ENERGY>
-__device__ __forceinline__ float3 half_tile(const DevState& st, const NbParams& p, const float4& xi,
-                                           const float2& lji, float qi, int sj, float sx, float sy, float sz,
-                                           bool bit, PairAcc& acc) {
-    const float4 xj = st.xyzq[sj];
-    const float2 ljj = st.ljp[sj];
-    const float dx = xj.x + sx - xi.x;
-    const float dy = xj.y + sy - xi.y;
-    const float dz = xj.z + sz - xi.z;
-    const float r2 = dx * dx + dy * dy + dz * dz;
-    float fs = 0.f;
-    if (bit && r2 <= p.rc2) {
-        const float rinv = rsqrtf(r2);
-        const float rinv2 = rinv * rinv;
-        const float sig = lji.x + ljj.x;
-        const float eps = lji.y * ljj.y;
-        float s6 = sig * sig * rinv2;
-        s6 = s6 * s6 * s6;
-        fs = 24.f * eps * s6 * rinv2 * (1.f - 2.f * s6);
-        if (ENERGY) acc.e_lj += (double)(4.f * eps * s6 * (s6 - 1.f));
-        if (ES != 0) {
-            const float qq = qi * xj.w;
-            float fc, ec;
-            if (ES == 2) {
-                const float r = r2 * rinv;
-                const float x = p.kappa * r;
-                const float t = __fdividef(1.f, fmaf(AS_P, x, 1.f));
-                const float poly = t * fmaf(t, fmaf(t, fmaf(t, fmaf(t, AS_A5, AS_A4), AS_A3), AS_A2), AS_A1);
-                const float ex = __expf(-x * x);
-                const float erfc_x = poly * ex;
-                fc = qq * rinv2 * rinv * fmaf(p.two_kappa_sqrtpi * r, ex, erfc_x);
-                ec = qq * rinv * erfc_x;
-            } else {
-                fc = qq * rinv2 * rinv;
-                ec = qq * rinv;
-            }
-            fs -= fc;
-            if (ENERGY) acc.e_c += (double)ec;
+__device__ __forceinline__ float pair_scalar(const NbParams& p, float r2, float2 lji, float2 ljj, float qq,
+                                             PairAcc& acc) {
+    const float rinv = rsqrtf(r2);
+    const float rinv2 = rinv * rinv;
+    const float sig = lji.x + ljj.x;
+    const float eps = lji.y * ljj.y;
+    float s6 = sig * sig * rinv2;
+    s6 = s6 * s6 * s6;
+    float fs = 24.f * eps * s6 * rinv2 * (1.f - 2.f * s6);
+    if (ENERGY) acc.e_lj += (double)(4.f * eps * s6 * (s6 - 1.f));
+    if (ES != 0) {
+        float fc, ec;
+        if (ES == 2) {
+            const float r = r2 * rinv;
+            const float x = p.kappa * r;
+            const float t = __fdividef(1.f, fmaf(AS_P, x, 1.f));
+            const float poly = t * fmaf(t, fmaf(t, fmaf(t, fmaf(t, AS_A5, AS_A4), AS_A3), AS_A2), AS_A1);
+            const float ex = __expf(-x * x);
+            const float erfc_x = poly * ex;
+            fc = qq * rinv2 * rinv * fmaf(p.two_kappa_sqrtpi * r, ex, erfc_x);
+            ec = qq * rinv * erfc_x;
+        } else {
+            fc = qq * rinv2 * rinv;
+            ec = qq * rinv;
         }
-        if (p.em) fs = fmaxf(fminf(fs, 1e20f), -1e20f);
-        if (ENERGY) acc.vir += 0.5 * (double)(fs * r2);  // -1/2 r_ij . f_ij
+        fs -= fc;
+        if (ENERGY) acc.e_c += (double)ec;
     }
-    const float fx = fs * dx, fy = fs * dy, fz = fs * dz;
-    acc.fix += fx;
-    acc.fiy += fy;
-    acc.fiz += fz;
-    return make_float3(-fx, -fy, -fz);
+    if (p.em) fs = fmaxf(fminf(fs, 1e20f), -1e20f);
+    if (ENERGY) acc.vir += 0.5 * (double)(fs * r2);  // -1/2 r_ij . f_ij
+    return fs;
 }
 
-// sums a j-force over the 8 lanes with the same jj0 and adds it once (lane ii == 0)
-__device__ __forceinline__ void flush_j(const DevState& st, float3 f, int sj, int ii) {
-#pragma unroll
-    for (int o = 1; o < 8; o <<= 1) {
-        f.x += __shfl_xor_sync(0xffffffffu, f.x, o);
-        f.y += __shfl_xor_sync(0xffffffffu, f.y, o);
-        f.z += __shfl_xor_sync(0xffffffffu, f.z, o);
-    }
-    if (ii == 0) {
-        atomic_add_fixed(st.fx + sj, to_fixed(f.x, FORCE_SCALE));
-        atomic_add_fixed(st.fy + sj, to_fixed(f.y, FORCE_SCALE));
-        atomic_add_fixed(st.fz + sj, to_fixed(f.z, FORCE_SCALE));
-    }
-}
-
+// Work mapping: one warp per i-cluster; the warp takes its list four entries at
+// a time and each lane owns one j-atom (entry k0 + lane/8, j-atom lane%8).  A
+// lane walks the 8 i-atoms (read from shared memory as broadcasts), keeps its
+// j-atom's force in registers and adds it once per entry; the i-forces live in
+// 24 registers per lane and are reduced across the warp once, after the list.
 template <int ES, bool ENERGY>
 __global__ void __launch_bounds__(256) k_nonbonded(DevState st, NbParams p) {
+    __shared__ float4 s_xi[8][CLUSTER];
+    __shared__ float2 s_lj[8][CLUSTER];
+    const int wib = threadIdx.x >> 5;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= st.n_clusters) return;
@@ -110,45 +85,83 @@ __global__ void __launch_bounds__(256) k_nonbonded(DevState st, NbParams p) {
     if (n == 0) return;
     const int sysi = st.cluster_sys[ci];
     const float Lx = st.sys[sysi].boxf[0], Ly = st.sys[sysi].boxf[1], Lz = st.sys[sysi].boxf[2];
-    const int ii = lane & 7;
-    const int jj0 = lane >> 3;
-    const float4 xi = st.xyzq[ci * CLUSTER + ii];
-    const float2 lji = st.ljp[ci * CLUSTER + ii];
-    const float qi = xi.w * p.ke;
-    PairAcc acc{0.f, 0.f, 0.f, 0.0, 0.0, 0.0};
+    if (lane < CLUSTER) {
+        float4 x = st.xyzq[ci * CLUSTER + lane];
+        x.w *= p.ke;  // i-charges carry the Coulomb constant
+        s_xi[wib][lane] = x;
+        s_lj[wib][lane] = st.ljp[ci * CLUSTER + lane];
+    }
+    __syncwarp();
+    float fi[CLUSTER][3];
+#pragma unroll
+    for (int a = 0; a < CLUSTER; ++a) fi[a][0] = fi[a][1] = fi[a][2] = 0.f;
+    PairAcc acc{0.0, 0.0, 0.0};
+    const int jj = lane & 7;
     const size_t base = (size_t)ci * st.pl_cap;
-    for (int k = 0; k < n; ++k) {
-        const int ent = st.pl_j[base + k];
-        const unsigned long long mask = st.pl_mask[base + k];
-        const int cj = ent & ((1 << JCLUSTER_BITS) - 1);
-        const int3 sh = decode_shift((unsigned)ent >> JCLUSTER_BITS);
-        const float sx = sh.x * Lx, sy = sh.y * Ly, sz = sh.z * Lz;
-        // mask bit (jj*8 + ii): the lane's bit of half h is bit `lane` of word h.
-        // A half with no bit set is skipped by the whole warp.
-        const unsigned lo = (unsigned)mask, hi = (unsigned)(mask >> 32);
-        if (lo) {
-            const int sj = cj * CLUSTER + jj0;
-            const float3 fj = half_tile<ES, ENERGY>(st, p, xi, lji, qi, sj, sx, sy, sz, (lo >> lane) & 1u, acc);
-            flush_j(st, fj, sj, ii);
+    for (int k0 = 0; k0 < n; k0 += 4) {
+        const int k = k0 + (lane >> 3);
+        unsigned bits = 0u;
+        int sj = 0;
+        float4 xj = make_float4(0.f, 0.f, 0.f, 0.f);
+        float2 ljj = make_float2(0.f, 0.f);
+        if (k < n) {
+            const int ent = st.pl_j[base + k];
+            const unsigned long long mask = st.pl_mask[base + k];
+            bits = (unsigned)(mask >> (8 * jj)) & 0xffu;   // bit ii: pair (ii, jj)
+            const int cj = ent & ((1 << JCLUSTER_BITS) - 1);
+            const int3 sh = decode_shift((unsigned)ent >> JCLUSTER_BITS);
+            sj = cj * CLUSTER + jj;
+            xj = st.xyzq[sj];
+            ljj = st.ljp[sj];
+            xj.x += sh.x * Lx;
+            xj.y += sh.y * Ly;
+            xj.z += sh.z * Lz;
         }
-        if (hi) {
-            const int sj = cj * CLUSTER + jj0 + 4;
-            const float3 fj = half_tile<ES, ENERGY>(st, p, xi, lji, qi, sj, sx, sy, sz, (hi >> lane) & 1u, acc);
-            flush_j(st, fj, sj, ii);
+        float fjx = 0.f, fjy = 0.f, fjz = 0.f;
+#pragma unroll
+        for (int ii = 0; ii < CLUSTER; ++ii) {
+            if ((bits >> ii) & 1u) {
+                const float4 xi = s_xi[wib][ii];
+                const float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+                const float r2 = dx * dx + dy * dy + dz * dz;
+                if (r2 <= p.rc2) {
+                    const float fs = pair_scalar<ES, ENERGY>(p, r2, s_lj[wib][ii], ljj, xi.w * xj.w, acc);
+                    const float fx = fs * dx, fy = fs * dy, fz = fs * dz;
+                    fi[ii][0] += fx;
+                    fi[ii][1] += fy;
+                    fi[ii][2] += fz;
+                    fjx -= fx;
+                    fjy -= fy;
+                    fjz -= fz;
+                }
+            }
+        }
+        if (bits) {
+            atomic_add_fixed(st.fx + sj, to_fixed(fjx, FORCE_SCALE));
+            atomic_add_fixed(st.fy + sj, to_fixed(fjy, FORCE_SCALE));
+            atomic_add_fixed(st.fz + sj, to_fixed(fjz, FORCE_SCALE));
         }
     }
-    float fix = acc.fix, fiy = acc.fiy, fiz = acc.fiz;
-    fix += __shfl_xor_sync(0xffffffffu, fix, 8);
-    fiy += __shfl_xor_sync(0xffffffffu, fiy, 8);
-    fiz += __shfl_xor_sync(0xffffffffu, fiz, 8);
-    fix += __shfl_xor_sync(0xffffffffu, fix, 16);
-    fiy += __shfl_xor_sync(0xffffffffu, fiy, 16);
-    fiz += __shfl_xor_sync(0xffffffffu, fiz, 16);
-    if (jj0 == 0) {
-        const int si = ci * CLUSTER + ii;
-        atomic_add_fixed(st.fx + si, to_fixed(fix, FORCE_SCALE));
-        atomic_add_fixed(st.fy + si, to_fixed(fiy, FORCE_SCALE));
-        atomic_add_fixed(st.fz + si, to_fixed(fiz, FORCE_SCALE));
+    // i-forces: sum each of the 24 values over the warp; lane a (< 8) adds atom a's
+#pragma unroll
+    for (int a = 0; a < CLUSTER; ++a) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            float v = fi[a][c];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            fi[a][c] = v;
+        }
+    }
+    if (lane < CLUSTER) {
+        float vx = 0.f, vy = 0.f, vz = 0.f;
+#pragma unroll
+        for (int a = 0; a < CLUSTER; ++a)
+            if (a == lane) vx = fi[a][0], vy = fi[a][1], vz = fi[a][2];
+        const int si = ci * CLUSTER + lane;
+        atomic_add_fixed(st.fx + si, to_fixed(vx, FORCE_SCALE));
+        atomic_add_fixed(st.fy + si, to_fixed(vy, FORCE_SCALE));
+        atomic_add_fixed(st.fz + si, to_fixed(vz, FORCE_SCALE));
     }
     if (ENERGY) {
         add_energy_fixed(st.energy, sysi, acc.e_lj, E_LJ);

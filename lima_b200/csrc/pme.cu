@@ -31,6 +31,7 @@ struct FftPlanDev {
     int n;
     int nrad;
     int rad[12];
+    int tw_off;  // offset of this length's twiddle table in DevState::pme_tw (-1: compute)
 };
 
 struct PmeSysDev {
@@ -147,6 +148,15 @@ __device__ void make_twiddles(float2* tw, int n) {
     }
 }
 
+// e^{-2 pi i k/n} from the table built at set-up (FP64 -> float), else computed
+__device__ __forceinline__ void load_twiddles(float2* tw, const FftPlanDev& pl, const float2* table) {
+    if (pl.tw_off >= 0 && table) {
+        for (int k = threadIdx.x; k < pl.n; k += blockDim.x) tw[k] = table[pl.tw_off + k];
+    } else {
+        make_twiddles(tw, pl.n);
+    }
+}
+
 // ------------------------------------------------------------------ spread
 __device__ __forceinline__ void bspline4(float f, float* w) {
     const float g = 1.f - f;
@@ -182,8 +192,10 @@ __device__ __forceinline__ void grid_coord(float x, float inv_h, int K, int& bas
     }
 }
 
+// four threads per atom, one per z-plane of the 4x4x4 stencil
 __global__ void k_spread(DevState st) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = t >> 2, c = t & 3;
     if (s >= st.n_slots) return;
     const float4 p = st.xyzq[s];
     if (p.w == 0.f || st.orig[s] < 0) return;
@@ -203,17 +215,15 @@ __global__ void k_spread(DevState st) {
     int ix[4];
 #pragma unroll
     for (int a = 0; a < 4; ++a) ix[a] = wrapk(b0 - 1 + a, K0);
+    const int z = wrapk(b2 - 1 + c, K2);
+    const float qz = p.w * wz[c];
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-        const int z = wrapk(b2 - 1 + c, K2);
+    for (int b = 0; b < 4; ++b) {
+        const int y = wrapk(b1 - 1 + b, K1);
+        const float qyz = qz * wy[b];
+        long long* row = g + (size_t)K0 * (y + (size_t)K1 * z);
 #pragma unroll
-        for (int b = 0; b < 4; ++b) {
-            const int y = wrapk(b1 - 1 + b, K1);
-            const float qyz = p.w * wy[b] * wz[c];
-            long long* row = g + (size_t)K0 * (y + (size_t)K1 * z);
-#pragma unroll
-            for (int a = 0; a < 4; ++a) atomic_add_fixed(row + ix[a], to_fixed(qyz * wx[a], GRID_SCALE));
-        }
+        for (int a = 0; a < 4; ++a) atomic_add_fixed(row + ix[a], to_fixed(qyz * wx[a], GRID_SCALE));
     }
 }
 
@@ -229,14 +239,12 @@ __global__ void k_fft_x_fwd(DevState st, const PmeSysDev* plans, const int4* ite
     float2* tw = sm;
     float2* A = sm + maxn;
     float2* B = A + FFT_XLINES * (maxn + 1);
-    make_twiddles(tw, K0);
+    load_twiddles(tw, pl, st.pme_tw);
     const int nl = it.z;
-    long long* g = st.pme_grid_fx + sd.pme_off + (size_t)it.y * K0;
+    const long long* g = st.pme_grid_fx + sd.pme_off + (size_t)it.y * K0;
     for (int i = threadIdx.x; i < nl * K0; i += blockDim.x) {
         const int l = i / K0, x = i - l * K0;
-        long long* cell = g + (size_t)l * K0 + x;
-        A[l * stride + x] = make_float2((float)((double)*cell * (1.0 / GRID_SCALE)), 0.f);
-        *cell = 0;
+        A[l * stride + x] = make_float2((float)((double)g[(size_t)l * K0 + x] * (1.0 / GRID_SCALE)), 0.f);
     }
     __syncthreads();
     const float2* res = fft_lines(A, B, nl, stride, pl, tw, -1.f);
@@ -258,7 +266,7 @@ __global__ void k_fft_x_inv(DevState st, const PmeSysDev* plans, const int4* ite
     float2* tw = sm;
     float2* A = sm + maxn;
     float2* B = A + FFT_XLINES * (maxn + 1);
-    make_twiddles(tw, K0);
+    load_twiddles(tw, pl, st.pme_tw);
     const int nl = it.z;
     const float2* in = st.pme_cplx + sd.pme_coff + (size_t)it.y * K0h;
     for (int i = threadIdx.x; i < nl * K0; i += blockDim.x) {
@@ -292,7 +300,7 @@ __global__ void k_fft_y(DevState st, const PmeSysDev* plans, const int4* items, 
     float2* tw = sm;
     float2* A = sm + maxn;
     float2* B = A + FFT_TX * (maxn + 1);
-    make_twiddles(tw, K1);
+    load_twiddles(tw, pl, st.pme_tw);
     const int x0 = it.y, z = it.z;
     const int tx = min(FFT_TX, K0h - x0);
     float2* g = st.pme_cplx + sd.pme_coff + (size_t)z * K1 * K0h + x0;
@@ -319,7 +327,7 @@ __global__ void k_fft_z_conv(DevState st, const PmeSysDev* plans, const int4* it
     float2* tw = sm;
     float2* A = sm + maxn;
     float2* B = A + FFT_TX * (maxn + 1);
-    make_twiddles(tw, K2);
+    load_twiddles(tw, pl, st.pme_tw);
     const int x0 = it.y, y = it.z;
     const int tx = min(FFT_TX, K0h - x0);
     const size_t plane = (size_t)K1 * K0h;
@@ -346,17 +354,23 @@ __global__ void k_fft_z_conv(DevState st, const PmeSysDev* plans, const int4* it
 }
 
 // ------------------------------------------------------------------ gather
+// four threads per atom, one z-plane each; partial sums combined with shuffles
 template <bool ENERGY, bool FD>
 __global__ void k_gather(DevState st) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = t >> 2, c = t & 3;
     double e = 0.0;
     int sysi = -1;
+    float phi = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
+    float q = 0.f;
+    float sc0 = 0.f, sc1 = 0.f, sc2 = 0.f;
     if (s < st.n_slots) {
         const float4 p = st.xyzq[s];
         const int sy = st.cluster_sys[s / CLUSTER];
         const SysDesc& sd = st.sys[sy];
         if (p.w != 0.f && st.orig[s] >= 0 && sd.pme_n[0] != 0) {
             sysi = sy;
+            q = p.w;
             const int K0 = sd.pme_n[0], K1 = sd.pme_n[1], K2 = sd.pme_n[2];
             int b0, b1, b2;
             float f0, f1, f2;
@@ -378,45 +392,52 @@ __global__ void k_gather(DevState st) {
                 ixp[a] = wrapk(b0 + a, K0);
                 ixm[a] = wrapk(b0 - 2 + a, K0);
             }
-            float phi = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
+            const int z = wrapk(b2 - 1 + c, K2);
+            const float wzc = wz[c], dzc = dz[c];
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                const int z = wrapk(b2 - 1 + c, K2);
+            for (int b = 0; b < 4; ++b) {
+                const int y = wrapk(b1 - 1 + b, K1);
+                const float* row = g + (size_t)K0 * (y + (size_t)K1 * z);
 #pragma unroll
-                for (int b = 0; b < 4; ++b) {
-                    const int y = wrapk(b1 - 1 + b, K1);
-                    const float* row = g + (size_t)K0 * (y + (size_t)K1 * z);
-#pragma unroll
-                    for (int a = 0; a < 4; ++a) {
-                        const float v = row[ix[a]];
-                        const float w = wx[a] * wy[b] * wz[c];
-                        phi += w * v;
-                        if (FD) {
-                            const int yp = wrapk(y + 1, K1), ym = wrapk(y - 1, K1);
-                            const int zp = wrapk(z + 1, K2), zm = wrapk(z - 1, K2);
-                            gx += w * (row[ixp[a]] - row[ixm[a]]);
-                            gy += w * (g[(size_t)K0 * (yp + (size_t)K1 * z) + ix[a]] -
-                                       g[(size_t)K0 * (ym + (size_t)K1 * z) + ix[a]]);
-                            gz += w * (g[(size_t)K0 * (y + (size_t)K1 * zp) + ix[a]] -
-                                       g[(size_t)K0 * (y + (size_t)K1 * zm) + ix[a]]);
-                        } else {
-                            gx += dx[a] * wy[b] * wz[c] * v;
-                            gy += wx[a] * dy[b] * wz[c] * v;
-                            gz += wx[a] * wy[b] * dz[c] * v;
-                        }
+                for (int a = 0; a < 4; ++a) {
+                    const float v = row[ix[a]];
+                    const float w = wx[a] * wy[b] * wzc;
+                    phi += w * v;
+                    if (FD) {
+                        const int yp = wrapk(y + 1, K1), ym = wrapk(y - 1, K1);
+                        const int zp = wrapk(z + 1, K2), zm = wrapk(z - 1, K2);
+                        gx += w * (row[ixp[a]] - row[ixm[a]]);
+                        gy += w * (g[(size_t)K0 * (yp + (size_t)K1 * z) + ix[a]] -
+                                   g[(size_t)K0 * (ym + (size_t)K1 * z) + ix[a]]);
+                        gz += w * (g[(size_t)K0 * (y + (size_t)K1 * zp) + ix[a]] -
+                                   g[(size_t)K0 * (y + (size_t)K1 * zm) + ix[a]]);
+                    } else {
+                        gx += dx[a] * wy[b] * wzc * v;
+                        gy += wx[a] * dy[b] * wzc * v;
+                        gz += wx[a] * wy[b] * dzc * v;
                     }
                 }
             }
-            const float sc0 = FD ? 0.5f * sd.pme_inv_h[0] : sd.pme_inv_h[0];
-            const float sc1 = FD ? 0.5f * sd.pme_inv_h[1] : sd.pme_inv_h[1];
-            const float sc2 = FD ? 0.5f * sd.pme_inv_h[2] : sd.pme_inv_h[2];
-            atomic_add_fixed(st.fx + s, to_fixed(-p.w * gx * sc0, FORCE_SCALE));
-            atomic_add_fixed(st.fy + s, to_fixed(-p.w * gy * sc1, FORCE_SCALE));
-            atomic_add_fixed(st.fz + s, to_fixed(-p.w * gz * sc2, FORCE_SCALE));
-            if (ENERGY) e = 0.5 * (double)p.w * (double)phi;
+            sc0 = FD ? 0.5f * sd.pme_inv_h[0] : sd.pme_inv_h[0];
+            sc1 = FD ? 0.5f * sd.pme_inv_h[1] : sd.pme_inv_h[1];
+            sc2 = FD ? 0.5f * sd.pme_inv_h[2] : sd.pme_inv_h[2];
         }
     }
-    if (ENERGY) add_energy_fixed(st.energy, sysi, e, E_RECIP);
+    // the four planes of one atom sit in adjacent lanes: fixed-order reduction
+#pragma unroll
+    for (int o = 1; o < 4; o <<= 1) {
+        phi += __shfl_xor_sync(0xffffffffu, phi, o);
+        gx += __shfl_xor_sync(0xffffffffu, gx, o);
+        gy += __shfl_xor_sync(0xffffffffu, gy, o);
+        gz += __shfl_xor_sync(0xffffffffu, gz, o);
+    }
+    if (sysi >= 0 && c == 0) {
+        atomic_add_fixed(st.fx + s, to_fixed(-q * gx * sc0, FORCE_SCALE));
+        atomic_add_fixed(st.fy + s, to_fixed(-q * gy * sc1, FORCE_SCALE));
+        atomic_add_fixed(st.fz + s, to_fixed(-q * gz * sc2, FORCE_SCALE));
+        if (ENERGY) e = 0.5 * (double)q * (double)phi;
+    }
+    if (ENERGY) add_energy_fixed(st.energy, c == 0 ? sysi : -1, e, E_RECIP);
 }
 
 // ------------------------------------------------------------------ driver
@@ -430,19 +451,20 @@ int launch_pme(const DevState& st, const PmePlan& plan, bool energy, cudaStream_
     const int TB = 256;
     const int mx = plan.max_n;
     const size_t sx = fft_smem_bytes(FFT_XLINES, mx), sy = fft_smem_bytes(FFT_TX, mx);
-    k_spread<<<(st.n_slots + TB - 1) / TB, TB, 0, s>>>(st);
+    cudaMemsetAsync(st.pme_grid_fx, 0, sizeof(long long) * (size_t)st.pme_total_real, s);
+    const int g4 = (int)(((long long)st.n_slots * 4 + TB - 1) / TB);
+    k_spread<<<g4, TB, 0, s>>>(st);
     k_fft_x_fwd<<<plan.n_items_x, 256, sx, s>>>(st, plans, plan.items_x, mx);
     k_fft_y<<<plan.n_items_y, 256, sy, s>>>(st, plans, plan.items_y, -1.f, mx);
     k_fft_z_conv<<<plan.n_items_z, 256, sy, s>>>(st, plans, plan.items_z, mx);
     k_fft_y<<<plan.n_items_y, 256, sy, s>>>(st, plans, plan.items_y, 1.f, mx);
     k_fft_x_inv<<<plan.n_items_x, 256, sx, s>>>(st, plans, plan.items_x, mx);
-    const int g = (st.n_slots + TB - 1) / TB;
     if (plan.ref_gather) {
-        if (energy) k_gather<true, true><<<g, TB, 0, s>>>(st);
-        else k_gather<false, true><<<g, TB, 0, s>>>(st);
+        if (energy) k_gather<true, true><<<g4, TB, 0, s>>>(st);
+        else k_gather<false, true><<<g4, TB, 0, s>>>(st);
     } else {
-        if (energy) k_gather<true, false><<<g, TB, 0, s>>>(st);
-        else k_gather<false, false><<<g, TB, 0, s>>>(st);
+        if (energy) k_gather<true, false><<<g4, TB, 0, s>>>(st);
+        else k_gather<false, false><<<g4, TB, 0, s>>>(st);
     }
     return 7;
 }
@@ -452,6 +474,7 @@ bool make_fft_plan(int n, FftPlanDev* out) {
     if (n < 2 || n > FFT_MAXN) return false;
     out->n = n;
     out->nrad = 0;
+    out->tw_off = -1;
     int m = n;
     while (m % 4 == 0) {
         out->rad[out->nrad++] = 4;
@@ -472,6 +495,13 @@ size_t pme_sys_dev_size() { return sizeof(PmeSysDev); }
 bool fill_pme_sys_dev(void* dst, int kx, int ky, int kz) {
     PmeSysDev* d = reinterpret_cast<PmeSysDev*>(dst);
     return make_fft_plan(kx, &d->px) && make_fft_plan(ky, &d->py) && make_fft_plan(kz, &d->pz);
+}
+
+void set_pme_sys_twiddles(void* dst, int offx, int offy, int offz) {
+    PmeSysDev* d = reinterpret_cast<PmeSysDev*>(dst);
+    d->px.tw_off = offx;
+    d->py.tw_off = offy;
+    d->pz.tw_off = offz;
 }
 
 void pme_set_smem_limits(int maxn) {
