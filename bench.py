@@ -155,6 +155,77 @@ def run_reference(args):
     return 0
 
 
+def _timed_steps(eng, n, per_step=False):
+    """Device time per step (engine's CUDA events on its main stream)."""
+    if per_step:
+        out = []
+        for _ in range(n):
+            eng.reset_timings()
+            eng.step(1)
+            out.append(eng.timings()["step"] * 1e-6)
+        return out
+    eng.reset_timings()
+    eng.step(n)
+    t = eng.timings()
+    return [t["step"] * 1e-6] * 1, t
+
+
+def other_configs(args, local):
+    """Secondary workloads of the specification, reported beside the headline:
+    C0 (1,000 waters, cutoff Coulomb), C1 (chains + water, PME 48x48x80) and C4
+    (256 uneven systems stepped together).  Pair-list periods replay as CUDA
+    graphs; these working sets are not flushed from L2 between steps (C4's is
+    larger than L2)."""
+    from lima_b200 import Engine, systems
+    from lima_b200 import engine as E
+    out = {}
+    k = max(args.other_steps, 21)
+    # C0
+    s0 = systems.config0()
+    e0 = Engine(cutoff=1.2, electrostatics=E.ES_CUTOFF, nstlist=10, dt=DT_NS, device=local, use_graphs=1)
+    e0.load(s0)
+    e0.step(20)
+    t = _timed_steps(e0, k)[0][0]
+    out["c0_water1k_cutoff"] = {"atoms": s0.n, "ns_per_day": ns_per_day(t), "ms_per_step": t * 1e3, "steps": k}
+    e0.close()
+    # C1
+    s1 = systems.config1()
+    e1 = Engine(cutoff=1.2, electrostatics=E.ES_EWALD, ewald_tol=1e-5, nstlist=10, dt=DT_NS, device=local,
+                use_graphs=1)
+    e1.load(s1, pme_grid=(48, 48, 80))
+    e1.minimize(force_tol=1e5, max_steps=300)
+    e1.step(20)
+    t = _timed_steps(e1, k)[0][0]
+    out["c1_chains_water_pme48x48x80"] = {"atoms": s1.n, "ns_per_day": ns_per_day(t), "ms_per_step": t * 1e3,
+                                          "steps": k, "prep": "300 energy-minimisation steps"}
+    e1.close()
+    # C4
+    if not args.skip_batch:
+        import time as _t
+        t0 = _t.perf_counter()
+        batch = systems.batch_systems(256)
+        gen_s = _t.perf_counter() - t0
+        e4 = Engine(n_systems=len(batch), cutoff=1.0, electrostatics=E.ES_EWALD, ewald_tol=1e-5, pme_spacing=0.12,
+                    nstlist=10, dt=DT_NS, device=local, use_graphs=1)
+        for i, sy in enumerate(batch):
+            e4.select(i)
+            e4.load(sy)
+        e4.minimize(force_tol=1e5, max_steps=100)
+        e4.step(20)
+        t = _timed_steps(e4, k)[0][0]
+        lat = sorted(_timed_steps(e4, min(k, 60), per_step=True))
+        n_at = sum(sy.n for sy in batch)
+        out["c4_batch256"] = {"systems": len(batch), "atoms": n_at, "aggregate_ns_per_day": len(batch) * ns_per_day(t),
+                              "ms_per_step": t * 1e3, "steps": k,
+                              "step_latency_ms_p50": 1e3 * lat[len(lat) // 2],
+                              "step_latency_ms_p99": 1e3 * lat[min(len(lat) - 1, int(0.99 * len(lat)))],
+                              "note": "every system advances each batched step, so a system's step latency is the "
+                                      "batched step time; p50/p99 over eagerly timed steps",
+                              "generation_s": gen_s}
+        e4.close()
+    return out
+
+
 def run_lima(args):
     import torch
     from lima_b200 import Engine, systems
@@ -264,6 +335,16 @@ def run_lima(args):
     h2d = s.n * (3 * 8 + 3 * 4)
     d2h = s.n * (3 * 8 + 3 * 4) + 15 * 8
 
+    # ---- the same headline workload with each pair-list period replayed as a CUDA graph
+    eng_g = Engine(cutoff=CUTOFF, electrostatics=E.ES_EWALD, ewald_tol=1e-5, nstlist=10, dt=DT_NS, device=local,
+                   use_graphs=1)
+    eng_g.load(s, pme_grid=GRID)
+    eng_g.step(21)
+    graph_step_s = _timed_steps(eng_g, max(args.steps, 21))[0][0]
+    eng_g.close()
+
+    others = other_configs(args, local) if (rank == 0 and not args.no_other_configs) else None
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -301,6 +382,9 @@ def run_lima(args):
         "gpu_launches": launches,
         "clocks": clocks,
         "cpu_baseline": cpu,
+        "graph_mode": {"ns_per_day": world * ns_per_day(graph_step_s), "ms_per_step": graph_step_s * 1e3,
+                       "l2": "not flushed: each pair-list period (rebuild + 10 steps) replays as one CUDA graph"},
+        "other_configs": others,
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -314,6 +398,9 @@ def main():
     ap.add_argument("--impl", default="lima", choices=["lima", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", type=int, default=0, help="only set up and run this many steps (ncu)")
+    ap.add_argument("--no-other-configs", action="store_true")
+    ap.add_argument("--skip-batch", action="store_true")
+    ap.add_argument("--other-steps", type=int, default=100)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

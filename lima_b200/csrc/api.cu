@@ -93,6 +93,10 @@ struct lima_engine {
     int phase_used[5] = {0, 0, 0, 0, 0};
     int64_t launches = 0;
     int64_t rebuilds = 0;
+    // CUDA graph of one pair-list period: rebuild + nstlist (forces, integrate) steps
+    cudaGraphExec_t graph_exec = nullptr;
+    int64_t graph_launches_per_replay = 0;
+    int64_t graph_replays = 0;
 
     // host mirrors
     std::vector<long long> energy_host;
@@ -122,8 +126,13 @@ struct lima_engine {
         if (!v.empty()) CK(cudaMemcpy(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
         return d;
     }
+    void drop_graph() {
+        if (graph_exec) cudaGraphExecDestroy(graph_exec);
+        graph_exec = nullptr;
+    }
     void release() {
         if (s_main) cudaStreamSynchronize(s_main);
+        drop_graph();
         for (void* a : allocs) cudaFree(a);
         allocs.clear();
         for (cudaStream_t* s : {&s_main, &s_bonded, &s_pme})
@@ -154,8 +163,10 @@ struct lima_engine {
         }
     }
     void rebuild(bool from_input);
+    void rebuild_async();
     void forces(bool energy);
     void run_steps(int n);
+    void capture_period();
     void read_energies(lima_energies* e);
 };
 
@@ -433,7 +444,8 @@ void lima_engine::setup() {
     const double a_cl = std::cbrt(CLUSTER / max_density);
     const double reach = rlist + 1.5 * a_cl;
     const double est = 4.0 / 3.0 * kPi * reach * reach * reach * max_density / CLUSTER;
-    int pl_cap = (int)std::ceil(1.3 * est) + 32;
+    // replayed graphs cannot grow the list between rebuilds: give them more room
+    int pl_cap = (int)std::ceil((p.use_graphs ? 1.8 : 1.3) * est) + 32;
     pl_cap = (pl_cap + 31) / 32 * 32;
     if (st.pl_cap > pl_cap) pl_cap = st.pl_cap;  // keep a capacity grown earlier
 
@@ -685,10 +697,54 @@ void lima_engine::rebuild(bool from_input) {
         st.pl_cap = cap;
         st.pl_j = dalloc<int>((size_t)st.n_clusters * cap);
         st.pl_mask = dalloc<unsigned long long>((size_t)st.n_clusters * cap);
+        drop_graph();
         // the state is already permuted into slot order: rebuild from the slots
         from_input = false;
     }
     throw ApiError{LIMA_ERR_OVERFLOW, "pair list overflow persists"};
+}
+
+// Pair-list rebuild without the host-side overflow check (inside a CUDA graph);
+// the status word is read after the replay.
+void lima_engine::rebuild_async() {
+    launches += launch_rebuild(st, (float)rlist, false, s_main);
+    ++rebuilds;
+}
+
+// Records one pair-list period — rebuild, then nstlist steps of forces and
+// integration without energies — as a CUDA graph on the main stream (the bonded
+// and PME streams join through the fork/join events).
+void lima_engine::capture_period() {
+    drop_graph();
+    const int64_t l0 = launches, r0 = rebuilds;
+    const bool pt = phase_timing;
+    phase_timing = false;
+    cudaGraph_t graph = nullptr;
+    CK(cudaStreamBeginCapture(s_main, cudaStreamCaptureModeThreadLocal));
+    rebuild_async();
+    for (int k = 0; k < p.nstlist; ++k) {
+        launch_zero_forces(st, s_main);
+        CK(cudaEventRecord(ev_fork, s_main));
+        CK(cudaStreamWaitEvent(s_bonded, ev_fork, 0));
+        CK(cudaStreamWaitEvent(s_pme, ev_fork, 0));
+        launches += launch_bonded(st, bt, false, s_bonded);
+        if (pme_on) launches += launch_exclusion_correction(st, bt, nb, false, s_bonded);
+        CK(cudaEventRecord(ev_bonded, s_bonded));
+        if (pme_on) launches += launch_pme(st, pp, false, s_pme);
+        CK(cudaEventRecord(ev_pme, s_pme));
+        launches += launch_nonbonded(st, nb, false, s_main);
+        CK(cudaStreamWaitEvent(s_main, ev_bonded, 0));
+        CK(cudaStreamWaitEvent(s_main, ev_pme, 0));
+        launches += launch_integrate(st, ip, false, s_main);
+    }
+    CK(cudaStreamEndCapture(s_main, &graph));
+    const cudaError_t e = cudaGraphInstantiate(&graph_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    CK(e);
+    graph_launches_per_replay = launches - l0;
+    launches = l0;
+    rebuilds = r0;
+    phase_timing = pt;
 }
 
 void lima_engine::forces(bool energy) {
@@ -728,7 +784,23 @@ void lima_engine::forces(bool energy) {
 
 void lima_engine::run_steps(int n) {
     CK(cudaEventRecord(ev_t0, s_main));
-    for (int k = 0; k < n; ++k) {
+    int k = 0;
+    if (p.use_graphs && !phase_timing && !state_pending) {
+        // whole pair-list periods replay as one graph; the last step stays eager
+        // so that it can evaluate energies
+        while (n - k > p.nstlist && list_age >= p.nstlist) {
+            if (!graph_exec) capture_period();
+            CK(cudaMemsetAsync(st.status, 0, sizeof(unsigned), s_main));
+            CK(cudaGraphLaunch(graph_exec, s_main));
+            launches += graph_launches_per_replay;
+            ++rebuilds;
+            ++graph_replays;
+            list_age = p.nstlist;
+            k += p.nstlist;
+            step += p.nstlist;
+        }
+    }
+    for (; k < n; ++k) {
         const bool energy = k == n - 1;
         forces(energy);
         mark(4, 0, s_main);
@@ -1006,6 +1078,8 @@ int lima_step(lima_engine* h, int n_steps) {
         unsigned status = 0;
         CK(cudaMemcpy(&status, h->st.status, sizeof(unsigned), cudaMemcpyDeviceToHost));
         if (status & ST_NONFINITE) return fail(h, LIMA_ERR_NOT_FINITE, "non-finite force during stepping");
+        if (status & (ST_PAIRLIST_OVERFLOW | ST_COLUMN_OVERFLOW))
+            return fail(h, LIMA_ERR_OVERFLOW, "pair list or column capacity exceeded inside a graph replay");
         return LIMA_OK;
     });
 }

@@ -103,29 +103,53 @@ def _water_template() -> np.ndarray:
 
 
 def _orient_waters(rng, centres: np.ndarray, fixed: np.ndarray | None, box: np.ndarray,
-                   min_dist: float = 0.17, rounds: int = 60) -> np.ndarray:
-    """Random orientations, redrawn for waters with an atom closer than
-    min_dist to an atom of another molecule (H atoms carry no LJ, so such
-    contacts would blow up the first steps)."""
+                   min_dist: float = 0.17, rounds: int = 40, tries: int = 16) -> np.ndarray:
+    """Random orientations; a water with an atom closer than min_dist to an atom
+    of another molecule (H atoms carry no LJ, so such contacts would blow up the
+    first steps) draws `tries` candidate orientations per round and keeps the
+    first one that is clear of the current positions of everything else."""
     from scipy.spatial import cKDTree
 
     nw = len(centres)
     tmpl = _water_template()
     rot = _random_rotations(rng, nw)
     nfix = 0 if fixed is None else len(fixed)
+    mol = np.concatenate([-1 - np.arange(nfix), np.repeat(np.arange(nw), 3)])
+    wpos = np.einsum("nij,aj->nai", rot, tmpl) + centres[:, None, :]          # (nw, 3, 3)
+
+    def all_pos():
+        p = wpos.reshape(-1, 3)
+        return np.mod(p if nfix == 0 else np.concatenate([fixed, p]), box)
+
+    tree = cKDTree(all_pos(), boxsize=box)
+    pairs = tree.query_pairs(min_dist, output_type="ndarray")
+    if len(pairs):
+        pairs = pairs[mol[pairs[:, 0]] != mol[pairs[:, 1]]]
+    bad = np.unique(mol[pairs.ravel()]) if len(pairs) else np.zeros(0, np.int64)
+    bad = bad[bad >= 0]
     for _ in range(rounds):
-        pos = (np.einsum("nij,aj->nai", rot, tmpl) + centres[:, None, :]).reshape(-1, 3)
-        allp = pos if nfix == 0 else np.concatenate([fixed, pos])
-        tree = cKDTree(np.mod(allp, box), boxsize=box)
-        pairs = tree.query_pairs(min_dist, output_type="ndarray")
-        mol = np.concatenate([-1 - np.arange(nfix), np.repeat(np.arange(nw), 3)])
-        if len(pairs):
-            pairs = pairs[mol[pairs[:, 0]] != mol[pairs[:, 1]]]
-        if len(pairs) == 0:
+        if len(bad) == 0:
             break
-        bad = np.unique(mol[pairs.ravel()])
-        bad = bad[bad >= 0]
-        rot[bad] = _random_rotations(rng, len(bad))
+        cand = _random_rotations(rng, len(bad) * tries).reshape(len(bad), tries, 3, 3)
+        pts = np.einsum("btij,aj->btai", cand, tmpl) + centres[bad][:, None, None, :]
+        d, idx = tree.query(np.mod(pts.reshape(-1, 3), box), k=4)
+        own = mol[idx] == np.repeat(bad, tries * 3)[:, None]
+        d = np.where(own, np.inf, d).min(1).reshape(len(bad), tries, 3).min(2)
+        ok = d >= min_dist
+        pick = np.where(ok.any(1), ok.argmax(1), 0)
+        rot[bad] = cand[np.arange(len(bad)), pick]
+        wpos[bad] = pts[np.arange(len(bad)), pick]
+        # re-check only the waters that moved, against everything at its new place
+        tree = cKDTree(all_pos(), boxsize=box)
+        moved = np.mod(wpos[bad].reshape(-1, 3), box)
+        hits = tree.query_ball_point(moved, min_dist)
+        still = np.zeros(len(bad), bool)
+        for k, h in enumerate(hits):
+            w = bad[k // 3]
+            if any(mol[j] != w for j in h):
+                still[k // 3] = True
+        # neighbours hit by a moved water are re-drawn too
+        bad = bad[still]
     return rot
 
 
@@ -370,14 +394,93 @@ def config2(seed=20241203):
     return water_box(33400, 10.0, seed=seed, name="water100k_10nm")
 
 
+def _merge(a: System, b: System) -> System:
+    """Concatenates two systems sharing a box (b's indices shifted)."""
+    off = a.n
+    cat = lambda x, y: np.concatenate([x, y]) if len(x) or len(y) else x
+    sh = lambda t: (t + off).astype(np.int32) if len(t) else t
+    return System(box=a.box, pos=np.concatenate([a.pos, b.pos]), vel=np.concatenate([a.vel, b.vel]),
+                  charge=cat(a.charge, b.charge), mass=cat(a.mass, b.mass), sigma=cat(a.sigma, b.sigma),
+                  epsilon=cat(a.epsilon, b.epsilon),
+                  bonds=cat(a.bonds, sh(b.bonds)), bond_par=cat(a.bond_par, b.bond_par),
+                  angles=cat(a.angles, sh(b.angles)), angle_par=cat(a.angle_par, b.angle_par),
+                  dihedrals=cat(a.dihedrals, sh(b.dihedrals)), dihedral_par=cat(a.dihedral_par, b.dihedral_par),
+                  impropers=cat(a.impropers, sh(b.impropers)), improper_par=cat(a.improper_par, b.improper_par),
+                  pairbonds=cat(a.pairbonds, sh(b.pairbonds)), pair_par=cat(a.pair_par, b.pair_par), name=a.name)
+
+
+def _chains(rng, n_chains: int, box: np.ndarray, temperature: float) -> System:
+    """n_chains lipid-like chains (config-1 topology and parameters) at random
+    positions and orientations."""
+    cb, ca, cd = chain_topology()
+    geo = _chain_geometry(True, 0.21)
+    geo -= geo.mean(0)
+    rot = _random_rotations(rng, n_chains)
+    pos, q, s, e, bonds, angles, dihedrals = [], [], [], [], [], [], []
+    for c in range(n_chains):
+        pos.append(geo @ rot[c].T + rng.uniform(0, 1, 3) * box)
+        hq = rng.normal(0.0, 0.4, CHAIN_HEAD)
+        hq -= hq.mean()
+        qq = np.zeros(CHAIN_ATOMS)
+        qq[:CHAIN_HEAD] = hq * E_TO_KCMOL
+        q.append(qq)
+        s.append(rng.uniform(0.30, 0.39, CHAIN_ATOMS))
+        e.append(rng.uniform(0.2, 0.9, CHAIN_ATOMS) * KJ)
+        off = c * CHAIN_ATOMS
+        bonds.append(cb + off)
+        angles.append(ca + off)
+        dihedrals.append(cd + off)
+    n = n_chains * CHAIN_ATOMS
+    mass = np.full(n, CHAIN["mass"], np.float32)
+    return System(box=box, pos=np.mod(np.concatenate(pos), box), vel=maxwell_boltzmann(rng, mass, temperature),
+                  charge=np.concatenate(q).astype(np.float32), mass=mass,
+                  sigma=np.concatenate(s).astype(np.float32), epsilon=np.concatenate(e).astype(np.float32),
+                  bonds=np.concatenate(bonds).astype(np.int32),
+                  bond_par=np.tile([CHAIN["b0"], CHAIN["kb"]], (len(cb) * n_chains, 1)).astype(np.float32),
+                  angles=np.concatenate(angles).astype(np.int32),
+                  angle_par=np.tile([CHAIN["theta0"], CHAIN["kth"], 0, 0], (len(ca) * n_chains, 1)).astype(np.float32),
+                  dihedrals=np.concatenate(dihedrals).astype(np.int32),
+                  dihedral_par=np.tile([CHAIN["phi0"], CHAIN["kphi"], CHAIN["mult"]],
+                                       (len(cd) * n_chains, 1)).astype(np.float32), name="chains")
+
+
+def water_with_chains(n_atoms: int, n_chains: int, density: float = 33.4, seed: int = 1,
+                      temperature: float = 300.0, name: str = "sys") -> System:
+    """A config-0-style water box of about n_atoms atoms (density waters/nm^3)
+    with n_chains config-1 chains inserted at random positions; waters with an
+    atom within 0.3 nm of a chain atom are removed."""
+    from scipy.spatial import cKDTree
+
+    rng = np.random.default_rng(seed)
+    n_w = max(8, n_atoms // 3)
+    L = (n_w / density) ** (1.0 / 3.0)
+    box = np.array([L, L, L])
+    w = water_box(n_w, L, seed=seed, temperature=temperature, name=name)
+    if n_chains == 0:
+        return w
+    ch = _chains(rng, n_chains, box, temperature)
+    d, _ = cKDTree(ch.pos, boxsize=box).query(np.mod(w.pos, box), k=1)
+    bad = np.unique(np.nonzero(d < 0.3)[0] // 3)
+    keep = np.setdiff1d(np.arange(w.n // 3), bad)
+    atoms = (3 * keep[:, None] + np.arange(3)).ravel()
+    remap = -np.ones(w.n, np.int64)
+    remap[atoms] = np.arange(len(atoms))
+    kb = np.all(np.isin(w.bonds, atoms), axis=1)
+    ka = np.all(np.isin(w.angles, atoms), axis=1)
+    w2 = System(box=box, pos=w.pos[atoms], vel=w.vel[atoms], charge=w.charge[atoms], mass=w.mass[atoms],
+                sigma=w.sigma[atoms], epsilon=w.epsilon[atoms],
+                bonds=remap[w.bonds[kb]].astype(np.int32), bond_par=w.bond_par[kb],
+                angles=remap[w.angles[ka]].astype(np.int32), angle_par=w.angle_par[ka], name=name)
+    return _merge(ch, w2)
+
+
 def batch_systems(n_systems=256, seed=20241203, lo=1500, hi=30000, density=33.4):
-    """Config 4: atom counts log-uniform in [lo, hi]; water boxes at the given
-    density with 0-4 chains inserted (here: chains counted into the atom budget)."""
+    """Config 4: atom counts log-uniform in [lo, hi] from a seed; each a water box
+    at the given density with 0-4 chains inserted at random positions."""
     rng = np.random.default_rng(seed)
     out = []
     for s in range(n_systems):
         n_atoms = int(math.exp(rng.uniform(math.log(lo), math.log(hi))))
-        n_w = max(8, n_atoms // 3)
-        L = (n_w / density) ** (1.0 / 3.0)
-        out.append(water_box(n_w, L, seed=seed + 1 + s, name=f"batch{s}"))
+        n_chains = int(rng.integers(0, 5))
+        out.append(water_with_chains(n_atoms, n_chains, density, seed=seed + 1 + s, name=f"batch{s}"))
     return out
