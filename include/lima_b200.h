@@ -231,6 +231,55 @@ LIMA_API int lima_pme_recip_noalloc(const float* d_xyzq, int n_atoms, double lx,
                                     int kx, int ky, int kz, double kappa, double* d_forces,
                                     double* d_energy, void* stream);
 
+/* ------------------------------------------------ learned coarse-grid PME
+ * No counterpart in the reference (LIMA has no learned component).  A small
+ * network (68 -> 128 -> 128 -> 128 -> 3, SiLU, BF16 tensor-core kernels with
+ * FP32 accumulation) predicts, per atom, the difference between the full-grid
+ * and a coarse-grid PME reciprocal force from the coarse force, the charge and
+ * a 64-value descriptor of the charges within 0.8 nm (16 Gaussians x 4
+ * channels: q_j, q_j x/r, q_j y/r, q_j z/r, cosine cutoff).  While enabled, the
+ * step's reciprocal part is coarse PME + network; the full grid runs every
+ * check_interval steps and on every step that evaluates energies, its forces
+ * are used on those steps, and once the relative RMSE of the predicted
+ * reciprocal force exceeds the tolerance the engine falls back to plain PME
+ * for good (until re-enabled).  Requires PME electrostatics and box edges
+ * above 1.8 nm.  Calls apply to every system of a batch. */
+
+/* Allocates the coarse grid (each dimension >= 8, factors 2, 3, 5), the
+ * network (fixed-seed Glorot-uniform initialisation) and a ring of max_frames
+ * training frames. */
+LIMA_API int lima_learned_pme_setup(lima_engine* h, int coarse_x, int coarse_y, int coarse_z, int max_frames);
+/* Labels the current state: features from the coarse grid, target = full-grid
+ * minus coarse-grid reciprocal force.  The first frame fixes the input
+ * normalisation and the output scale. */
+LIMA_API int lima_learned_pme_collect(lima_engine* h);
+/* Adam (beta 0.9/0.999) on the collected frames, rows shuffled per epoch by
+ * seed; batch <= 65536 rows.  final_loss (may be NULL): mean squared error of
+ * the normalised residual over the last epoch. */
+LIMA_API int lima_learned_pme_train(lima_engine* h, int epochs, int batch, float lr, uint64_t seed,
+                                    double* final_loss);
+/* Turns the correction on or off in stepping; check_interval <= 0 means 50,
+ * tolerance <= 0 means 1e-3.  Clears an earlier fallback. */
+LIMA_API int lima_learned_pme_enable(lima_engine* h, int on, int check_interval, double tolerance);
+/* Relative RMSE of the coarse and of the corrected reciprocal force against
+ * the full grid on the current state. */
+LIMA_API int lima_learned_pme_eval(lima_engine* h, double* coarse_rel, double* learned_rel);
+/* active: the correction is in use; fell_back: a check failed; last_rel: the
+ * last check's relative RMSE (-1 before the first check). */
+LIMA_API int lima_learned_pme_status(lima_engine* h, int* active, int* fell_back, double* last_rel);
+/* Reads (get != 0) or writes the model state: parameters W1[80][128] b1[128]
+ * W2[128][128] b2[128] W3[128][128] b3[128] W4[128][8] b4[8] (W[k][n]: input k
+ * to output n; rows 68..79 of W1 and columns 3..7 of W4 unused), then the 68
+ * input means, the 68 input scales and the output scale.  *needed receives the
+ * count (44,561 floats); buf may be NULL to query it. */
+LIMA_API int lima_learned_pme_weights(lima_engine* h, int get, float* buf, int64_t n, int64_t* needed);
+/* One forward/backward pass without an update on caller rows (x: rows x 68
+ * normalised inputs, t: rows x 3 targets, rows <= 65536): grads receives
+ * d loss / d parameters in the layout above (44,424 floats), loss the mean
+ * squared error.  For checking the training kernels. */
+LIMA_API int lima_learned_pme_gradients(lima_engine* h, int rows, const float* x, const float* t,
+                                        float* grads, double* loss);
+
 #ifdef __cplusplus
 }
 #endif

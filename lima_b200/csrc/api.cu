@@ -16,11 +16,13 @@
 #include <cstdio>
 #include <cstring>
 #include <numeric>
+#include <random>
 #include <string>
 #include <vector>
 
 #include "engine.h"
 #include "lima_b200.h"
+#include "mlp.h"
 
 namespace {
 
@@ -109,6 +111,43 @@ struct lima_engine {
     float* d_out_f = nullptr;
     float* d_maxf = nullptr;
 
+    // learned coarse-grid PME correction (mlp.cu, learned.cu)
+    std::vector<SysDesc> sd_host;     // per-system descriptors of the engine's own grid
+    bool lp_ready = false;            // buffers and model allocated
+    bool lp_on = false;               // replaces the full-grid reciprocal part in stepping
+    bool lp_fallback = false;         // a full-grid check failed: plain PME from then on
+    bool lp_norm = false;             // input normalisation and output scale fixed
+    bool lp_check_pending = false;
+    int lp_check = 50;                // steps between full-grid checks
+    double lp_tol = 1e-3;             // bound on the relative reciprocal-force RMSE
+    double lp_last_rel = -1.0;
+    int64_t lp_steps = 0;
+    DevState st_c{};                  // view with the coarse grid, forces into lp_fc
+    DevState st_f{};                  // view with the full grid, forces into lp_ff
+    PmePlan pp_c{};
+    long long* lp_fc = nullptr;       // coarse reciprocal force [3][n_slots]
+    long long* lp_ff = nullptr;       // full-grid reciprocal force [3][n_slots]
+    long long* lp_energy = nullptr;
+    float* lp_feat = nullptr;         // [n_slots][68]
+    __nv_bfloat16* lp_X = nullptr;    // [n_slots][80]
+    float* lp_Y = nullptr;            // [n_slots][8]
+    float* lp_mean = nullptr;
+    float* lp_invstd = nullptr;
+    MlpModel mlp{};
+    MlpActs acts{};
+    int batch_cap = 65536;
+    __nv_bfloat16* batch_X = nullptr;
+    float* batch_T = nullptr;
+    float* batch_raw = nullptr;       // [batch_cap][68] staging of caller rows
+    float* ds_feat = nullptr;         // collected frames, original atom order
+    float* ds_target = nullptr;
+    int ds_frames = 0;                // frames collected so far (ring of ds_cap)
+    int ds_cap = 0;
+    double* d_sums = nullptr;
+    double* d_loss = nullptr;
+    int* d_idx = nullptr;
+    size_t d_idx_cap = 0;
+
     ~lima_engine() { release(); }
 
     template <typename T>
@@ -143,6 +182,13 @@ struct lima_engine {
             for (cudaEvent_t& e : pr)
                 if (e) cudaEventDestroy(e), e = nullptr;
         built = false;
+        // the learned correction's buffers were among the allocations
+        lp_ready = lp_on = lp_fallback = lp_norm = lp_check_pending = false;
+        ds_frames = ds_cap = 0;
+        d_idx = nullptr;
+        d_idx_cap = 0;
+        mlp = MlpModel{};
+        acts = MlpActs{};
     }
 
     void setup();
@@ -162,12 +208,19 @@ struct lima_engine {
             phase_used[k] = 0;
         }
     }
+    PmePlan make_pme(std::vector<SysDesc>& sd, DevState& D);
     void rebuild(bool from_input);
     void rebuild_async();
     void forces(bool energy);
     void run_steps(int n);
     void capture_period();
     void read_energies(lima_energies* e);
+    bool learned_active() const { return lp_ready && lp_on && !lp_fallback; }
+    void learned_setup(int cx, int cy, int cz, int max_frames);
+    void learned_features(bool forward, cudaStream_t s);
+    void learned_full(cudaStream_t s, bool energy);
+    void learned_pme_stage(bool energy, cudaStream_t s);
+    void ensure_list();
 };
 
 namespace {
@@ -275,7 +328,6 @@ void lima_engine::setup() {
     int col_cap = 64;
     double max_density = 0.0;
     pme_on = false;
-    int max_n = 0;
     self_energy.assign(ns, 0.0);
     for (int s = 0; s < ns; ++s) {
         const SystemHost& S = sys[s];
@@ -323,7 +375,6 @@ void lima_engine::setup() {
                 if (g[d] < 8) throw ApiError{LIMA_ERR_INVALID_ARG, "PME grid dimension must be >= 8"};
                 D.pme_n[d] = g[d];
                 D.pme_inv_h[d] = (float)(g[d] / S.box[d]);
-                max_n = std::max(max_n, g[d]);
             }
             D.pme_off = pme_off;
             D.pme_coff = pme_coff;
@@ -520,103 +571,9 @@ void lima_engine::setup() {
     D.energy = dalloc<long long>((size_t)ns * E_COUNT);
 
     // ---- PME plan, grids and influence function
-    PmePlan P{};
-    if (pme_on) {
-        D.pme_total_real = pme_off;
-        D.pme_total_cplx = pme_coff;
-        D.pme_grid_fx = dalloc<long long>(pme_off);
-        D.pme_real = dalloc<float>(pme_off);
-        D.pme_cplx = dalloc<float2>(pme_coff);
-        std::vector<float> theta(pme_coff, 0.f);
-        std::vector<char> plans(pme_sys_dev_size() * ns, 0);
-        std::vector<int4> ix, iy, iz;
-        const int XL = 8, TX = 16;
-        for (int s = 0; s < ns; ++s) {
-            const SysDesc& Dd = sd[s];
-            if (Dd.pme_n[0] == 0) {
-                // a system without a grid still needs a valid (unused) plan
-                fill_pme_sys_dev(plans.data() + s * pme_sys_dev_size(), 8, 8, 8);
-                continue;
-            }
-            const int K0 = Dd.pme_n[0], K1 = Dd.pme_n[1], K2 = Dd.pme_n[2], K0h = K0 / 2 + 1;
-            if (!fill_pme_sys_dev(plans.data() + s * pme_sys_dev_size(), K0, K1, K2))
-                throw ApiError{LIMA_ERR_UNSUPPORTED, "PME grid dimensions must factor into 2, 3, 5 and be <= 256"};
-            for (int l = 0; l < K1 * K2; l += XL) ix.push_back(make_int4(s, l, std::min(XL, K1 * K2 - l), 0));
-            for (int z = 0; z < K2; ++z)
-                for (int x0 = 0; x0 < K0h; x0 += TX) iy.push_back(make_int4(s, x0, z, 0));
-            for (int y = 0; y < K1; ++y)
-                for (int x0 = 0; x0 < K0h; x0 += TX) iz.push_back(make_int4(s, x0, y, 0));
-            const double* L = sys[s].box;
-            const double V = L[0] * L[1] * L[2];
-            const double pic = p.ref_compat ? kPiRef : kPi;
-            for (int z = 0; z < K2; ++z)
-                for (int y = 0; y < K1; ++y)
-                    for (int x = 0; x < K0h; ++x) {
-                        const int m[3] = {x, y <= K1 / 2 ? y : y - K1, z <= K2 / 2 ? z : z - K2};
-                        const int K[3] = {K0, K1, K2};
-                        if (m[0] == 0 && m[1] == 0 && m[2] == 0) continue;
-                        double kv[3], k2 = 0.0;
-                        for (int d = 0; d < 3; ++d) {
-                            kv[d] = 2.0 * pic * m[d] / L[d];
-                            k2 += kv[d] * kv[d];
-                        }
-                        double t = kCoulomb * 4.0 * pic / k2 * std::exp(-k2 / (4.0 * kappa * kappa)) / V;
-                        if (p.ref_compat) {
-                            // PrecomputeGreensFunctionKernel (PME.cuh:434-495): x prod sinc^8
-                            double sp = 1.0;
-                            for (int d = 0; d < 3; ++d) {
-                                const double kh = kv[d] * (L[d] / K[d]) * 0.5;
-                                const double sc = std::fabs(kh) < 1e-14 ? 1.0 : std::sin(kh) / kh;
-                                sp *= sc * sc * sc * sc;
-                            }
-                            t *= sp * sp;
-                        } else {
-                            // SPME: divide by the B-spline modulus of the centred order-4 weights
-                            double B = 1.0;
-                            for (int d = 0; d < 3; ++d) {
-                                const double b = 2.0 / 3.0 + std::cos(2.0 * kPi * m[d] / K[d]) / 3.0;
-                                B *= b * b;
-                            }
-                            t /= B;
-                        }
-                        theta[Dd.pme_coff + x + (size_t)K0h * (y + (size_t)K1 * z)] = (float)t;
-                    }
-        }
-        D.pme_theta = upload(theta);
-        // twiddle tables, one per distinct grid length, in FP64 rounded to float
-        std::vector<float2> tw;
-        std::vector<std::pair<int, int>> tw_offsets;  // (length, offset)
-        auto tw_of = [&](int len) {
-            for (auto& pr : tw_offsets)
-                if (pr.first == len) return pr.second;
-            const int off = (int)tw.size();
-            for (int k = 0; k < len; ++k) {
-                const double a = 2.0 * kPi * k / len;
-                tw.push_back(make_float2((float)std::cos(a), (float)-std::sin(a)));
-            }
-            tw_offsets.push_back({len, off});
-            return off;
-        };
-        for (int s = 0; s < ns; ++s) {
-            const int* g = sd[s].pme_n;
-            if (g[0] == 0) continue;
-            set_pme_sys_twiddles(plans.data() + s * pme_sys_dev_size(), tw_of(g[0]), tw_of(g[1]), tw_of(g[2]));
-        }
-        D.pme_tw = upload(tw);
-        char* dplans = dalloc<char>(plans.size());
-        CK(cudaMemcpy(dplans, plans.data(), plans.size(), cudaMemcpyHostToDevice));
-        P.sys_plans = dplans;
-        P.items_x = upload(ix);
-        P.items_y = upload(iy);
-        P.items_z = upload(iz);
-        P.n_items_x = (int)ix.size();
-        P.n_items_y = (int)iy.size();
-        P.n_items_z = (int)iz.size();
-        P.ref_gather = p.ref_compat ? 1 : 0;
-        P.max_n = max_n;
-        pme_set_smem_limits(max_n);
-    }
-    pp = P;
+    pp = PmePlan{};
+    if (pme_on) pp = make_pme(sd, D);
+    sd_host = sd;
 
     // ---- bonded terms
     BondedTerms B{};
@@ -659,6 +616,265 @@ void lima_engine::setup() {
     built = true;
     state_pending = true;
     energy_valid = false;
+}
+
+// Grids, influence function, FFT plans and twiddles of the PME reciprocal part
+// for the systems in `sd` (their pme_n set; pme_off/pme_coff are assigned
+// here).  Used for the engine's own grid and for the coarse grid of the
+// learned correction.
+PmePlan lima_engine::make_pme(std::vector<SysDesc>& sd, DevState& D) {
+    const int ns = (int)sd.size();
+    PmePlan P{};
+    int pme_off = 0, pme_coff = 0, max_n = 0;
+    for (SysDesc& Dd : sd) {
+        if (Dd.pme_n[0] == 0) continue;
+        Dd.pme_off = pme_off;
+        Dd.pme_coff = pme_coff;
+        pme_off += Dd.pme_n[0] * Dd.pme_n[1] * Dd.pme_n[2];
+        pme_coff += (Dd.pme_n[0] / 2 + 1) * Dd.pme_n[1] * Dd.pme_n[2];
+        for (int d = 0; d < 3; ++d) max_n = std::max(max_n, Dd.pme_n[d]);
+    }
+    D.pme_total_real = pme_off;
+    D.pme_total_cplx = pme_coff;
+    D.pme_grid_fx = dalloc<long long>(pme_off);
+    D.pme_real = dalloc<float>(pme_off);
+    D.pme_cplx = dalloc<float2>(pme_coff);
+    std::vector<float> theta(pme_coff, 0.f);
+    std::vector<char> plans(pme_sys_dev_size() * ns, 0);
+    std::vector<int4> ix, iy, iz;
+    const int XL = 8, TX = 16;
+    for (int s = 0; s < ns; ++s) {
+        const SysDesc& Dd = sd[s];
+        if (Dd.pme_n[0] == 0) {
+            // a system without a grid still needs a valid (unused) plan
+            fill_pme_sys_dev(plans.data() + s * pme_sys_dev_size(), 8, 8, 8);
+            continue;
+        }
+        const int K0 = Dd.pme_n[0], K1 = Dd.pme_n[1], K2 = Dd.pme_n[2], K0h = K0 / 2 + 1;
+        if (!fill_pme_sys_dev(plans.data() + s * pme_sys_dev_size(), K0, K1, K2))
+            throw ApiError{LIMA_ERR_UNSUPPORTED, "PME grid dimensions must factor into 2, 3, 5 and be <= 256"};
+        for (int l = 0; l < K1 * K2; l += XL) ix.push_back(make_int4(s, l, std::min(XL, K1 * K2 - l), 0));
+        for (int z = 0; z < K2; ++z)
+            for (int x0 = 0; x0 < K0h; x0 += TX) iy.push_back(make_int4(s, x0, z, 0));
+        for (int y = 0; y < K1; ++y)
+            for (int x0 = 0; x0 < K0h; x0 += TX) iz.push_back(make_int4(s, x0, y, 0));
+        const double* L = Dd.box;
+        const double V = L[0] * L[1] * L[2];
+        const double pic = p.ref_compat ? kPiRef : kPi;
+        for (int z = 0; z < K2; ++z)
+            for (int y = 0; y < K1; ++y)
+                for (int x = 0; x < K0h; ++x) {
+                    const int m[3] = {x, y <= K1 / 2 ? y : y - K1, z <= K2 / 2 ? z : z - K2};
+                    const int K[3] = {K0, K1, K2};
+                    if (m[0] == 0 && m[1] == 0 && m[2] == 0) continue;
+                    double kv[3], k2 = 0.0;
+                    for (int d = 0; d < 3; ++d) {
+                        kv[d] = 2.0 * pic * m[d] / L[d];
+                        k2 += kv[d] * kv[d];
+                    }
+                    double t = kCoulomb * 4.0 * pic / k2 * std::exp(-k2 / (4.0 * kappa * kappa)) / V;
+                    if (p.ref_compat) {
+                        // PrecomputeGreensFunctionKernel (PME.cuh:434-495): x prod sinc^8
+                        double sp = 1.0;
+                        for (int d = 0; d < 3; ++d) {
+                            const double kh = kv[d] * (L[d] / K[d]) * 0.5;
+                            const double sc = std::fabs(kh) < 1e-14 ? 1.0 : std::sin(kh) / kh;
+                            sp *= sc * sc * sc * sc;
+                        }
+                        t *= sp * sp;
+                    } else {
+                        // SPME: divide by the B-spline modulus of the centred order-4 weights
+                        double B = 1.0;
+                        for (int d = 0; d < 3; ++d) {
+                            const double b = 2.0 / 3.0 + std::cos(2.0 * kPi * m[d] / K[d]) / 3.0;
+                            B *= b * b;
+                        }
+                        t /= B;
+                    }
+                    theta[Dd.pme_coff + x + (size_t)K0h * (y + (size_t)K1 * z)] = (float)t;
+                }
+    }
+    D.pme_theta = upload(theta);
+    // twiddle tables, one per distinct grid length, in FP64 rounded to float
+    std::vector<float2> tw;
+    std::vector<std::pair<int, int>> tw_offsets;  // (length, offset)
+    auto tw_of = [&](int len) {
+        for (auto& pr : tw_offsets)
+            if (pr.first == len) return pr.second;
+        const int off = (int)tw.size();
+        for (int k = 0; k < len; ++k) {
+            const double a = 2.0 * kPi * k / len;
+            tw.push_back(make_float2((float)std::cos(a), (float)-std::sin(a)));
+        }
+        tw_offsets.push_back({len, off});
+        return off;
+    };
+    for (int s = 0; s < ns; ++s) {
+        const int* g = sd[s].pme_n;
+        if (g[0] == 0) continue;
+        set_pme_sys_twiddles(plans.data() + s * pme_sys_dev_size(), tw_of(g[0]), tw_of(g[1]), tw_of(g[2]));
+    }
+    D.pme_tw = upload(tw);
+    char* dplans = dalloc<char>(plans.size());
+    CK(cudaMemcpy(dplans, plans.data(), plans.size(), cudaMemcpyHostToDevice));
+    P.sys_plans = dplans;
+    P.items_x = upload(ix);
+    P.items_y = upload(iy);
+    P.items_z = upload(iz);
+    P.n_items_x = (int)ix.size();
+    P.n_items_y = (int)iy.size();
+    P.n_items_z = (int)iz.size();
+    P.ref_gather = p.ref_compat ? 1 : 0;
+    P.max_n = max_n;
+    pme_set_smem_limits(max_n);
+    return P;
+}
+
+// ------------------------------------------------------------ learned PME
+// Allocates the coarse-grid view, the feature/target buffers, a dataset ring
+// of max_frames frames and the network (Glorot-uniform weights, fixed seed).
+void lima_engine::learned_setup(int cx, int cy, int cz, int max_frames) {
+    const int ns = (int)sd_host.size();
+    for (int s = 0; s < ns; ++s)
+        for (int d = 0; d < 3; ++d)
+            if (!(sd_host[s].box[d] > 2.0 * (DESC_CUT + 0.1)))
+                throw ApiError{LIMA_ERR_INVALID_ARG, "box edge must exceed 1.8 nm for the learned descriptor"};
+    const size_t S = st.n_slots;
+    // coarse view: same atoms and clusters, own grids, forces into lp_fc
+    std::vector<SysDesc> sdc = sd_host;
+    for (SysDesc& D : sdc) {
+        const int g[3] = {cx, cy, cz};
+        for (int d = 0; d < 3; ++d) {
+            D.pme_n[d] = g[d];
+            D.pme_inv_h[d] = (float)(g[d] / D.box[d]);
+        }
+    }
+    DevState Dc = st;
+    pp_c = make_pme(sdc, Dc);
+    Dc.sys = upload(sdc);
+    lp_fc = dalloc<long long>(3 * S);
+    lp_ff = dalloc<long long>(3 * S);
+    lp_energy = dalloc<long long>((size_t)st.n_sys * E_COUNT);
+    Dc.fx = lp_fc;
+    Dc.fy = lp_fc + S;
+    Dc.fz = lp_fc + 2 * S;
+    Dc.energy = lp_energy;
+    st_c = Dc;
+    DevState Df = st;
+    Df.fx = lp_ff;
+    Df.fy = lp_ff + S;
+    Df.fz = lp_ff + 2 * S;
+    st_f = Df;
+    lp_feat = dalloc<float>(S * MLP_IN);
+    lp_X = dalloc<__nv_bfloat16>(S * MLP_KIN);
+    lp_Y = dalloc<float>(S * 8);
+    lp_mean = dalloc<float>(MLP_IN);
+    lp_invstd = dalloc<float>(MLP_IN);
+    // dataset ring
+    ds_cap = max_frames;
+    ds_frames = 0;
+    ds_feat = dalloc<float>((size_t)max_frames * st.n_atoms * MLP_IN);
+    ds_target = dalloc<float>((size_t)max_frames * st.n_atoms * 3);
+    // network and training buffers
+    MlpModel m{};
+    std::mt19937_64 rng(20241203ull);
+    for (int l = 0; l < 4; ++l) {
+        const int K = MLP_K[l], N = MLP_N[l];
+        const int fan_in = l == 0 ? MLP_IN : K, fan_out = l == 3 ? MLP_OUT : N;
+        const double a = std::sqrt(6.0 / (fan_in + fan_out)) * (l == 3 ? 0.1 : 1.0);
+        std::uniform_real_distribution<double> U(-a, a);
+        std::vector<float> w((size_t)K * N, 0.f);
+        for (int k = 0; k < fan_in; ++k)
+            for (int n = 0; n < fan_out; ++n) w[(size_t)k * N + n] = (float)U(rng);
+        m.w[l] = upload(w);
+        m.b[l] = dalloc<float>(N);
+        m.mw[l] = dalloc<float>((size_t)K * N);
+        m.vw[l] = dalloc<float>((size_t)K * N);
+        m.mb[l] = dalloc<float>(N);
+        m.vb[l] = dalloc<float>(N);
+        m.gw[l] = dalloc<float>((size_t)K * N);
+        m.gb[l] = dalloc<float>(N);
+        m.wb[l] = dalloc<__nv_bfloat16>((size_t)K * (l == 3 ? 16 : N));
+        m.wtb[l] = dalloc<__nv_bfloat16>((size_t)N * K);
+    }
+    const size_t rows_max = std::max<size_t>(S, (size_t)batch_cap);
+    m.tmp[0] = dalloc<__nv_bfloat16>(rows_max * MLP_HID);
+    m.tmp[1] = dalloc<__nv_bfloat16>(rows_max * MLP_HID);
+    const size_t chunks = ((size_t)batch_cap + MLP_CHUNK - 1) / MLP_CHUNK;
+    m.part = dalloc<float>(chunks * 128 * 128);
+    m.bpart = dalloc<float>(chunks * 128);
+    m.max_rows = batch_cap;
+    for (int c = 0; c < MLP_IN; ++c) m.in_mean[c] = 0.f, m.in_std[c] = 1.f;
+    mlp = m;
+    mlp_sync_bf16(mlp, s_main);
+    MlpActs A{};
+    for (int l = 0; l < 3; ++l) {
+        A.z[l] = dalloc<__nv_bfloat16>((size_t)batch_cap * MLP_HID);
+        A.h[l] = dalloc<__nv_bfloat16>((size_t)batch_cap * MLP_HID);
+        A.dz[l] = dalloc<__nv_bfloat16>((size_t)batch_cap * MLP_HID);
+    }
+    A.dz4 = dalloc<__nv_bfloat16>((size_t)batch_cap * 16);
+    A.y = dalloc<float>((size_t)batch_cap * 8);
+    acts = A;
+    batch_X = dalloc<__nv_bfloat16>((size_t)batch_cap * MLP_KIN);
+    batch_T = dalloc<float>((size_t)batch_cap * 3);
+    batch_raw = dalloc<float>((size_t)batch_cap * MLP_IN);
+    d_sums = dalloc<double>(4);
+    d_loss = dalloc<double>(1);
+    CK(cudaStreamSynchronize(s_main));
+    lp_ready = true;
+    lp_on = lp_fallback = lp_norm = lp_check_pending = false;
+    lp_steps = 0;
+    lp_last_rel = -1.0;
+}
+
+// coarse-grid reciprocal force into lp_fc, features into lp_feat and, when
+// `forward`, the network's prediction into lp_Y
+void lima_engine::learned_features(bool forward, cudaStream_t s) {
+    CK(cudaMemsetAsync(lp_fc, 0, sizeof(long long) * 3 * (size_t)st.n_slots, s));
+    launches += launch_pme(st_c, pp_c, false, s);
+    launches += launch_descriptor(st, lp_fc, lp_feat, s);
+    if (forward && lp_norm) {
+        launches += launch_mlp_input(st, lp_feat, lp_mean, lp_invstd, lp_X, s);
+        launches += mlp_forward(mlp, st.n_slots, lp_X, nullptr, lp_Y, s);
+    }
+}
+
+// full-grid reciprocal force into lp_ff (energy, when asked, into the engine's
+// own accumulators)
+void lima_engine::learned_full(cudaStream_t s, bool energy) {
+    CK(cudaMemsetAsync(lp_ff, 0, sizeof(long long) * 3 * (size_t)st.n_slots, s));
+    st_f.pme_grid_fx = st.pme_grid_fx;
+    st_f.energy = st.energy;
+    launches += launch_pme(st_f, pp, energy, s);
+}
+
+// The reciprocal stage of one step with the correction on.  Every lp_check
+// steps (and whenever energies are wanted) the full grid runs as well: its
+// forces are the ones applied and the prediction's error against them is
+// summed for the host-side check after the step.
+void lima_engine::learned_pme_stage(bool energy, cudaStream_t s) {
+    const bool check = energy || lp_steps % lp_check == 0;
+    learned_features(true, s);
+    if (check) {
+        learned_full(s, energy);
+        CK(cudaMemsetAsync(d_sums, 0, 4 * sizeof(double), s));
+        launches += launch_pred_error(st, lp_fc, lp_Y, mlp.out_scale, lp_ff, d_sums, s);
+        launches += launch_add_forces(st, lp_ff, s);
+        lp_check_pending = true;
+    } else {
+        launches += launch_mlp_apply(st, lp_fc, lp_Y, mlp.out_scale, s);
+    }
+    ++lp_steps;
+}
+
+void lima_engine::ensure_list() {
+    if (state_pending) {
+        rebuild(true);
+        state_pending = false;
+    } else if (list_age >= p.nstlist) {
+        rebuild(false);
+    }
 }
 
 void lima_engine::rebuild(bool from_input) {
@@ -748,12 +964,7 @@ void lima_engine::capture_period() {
 }
 
 void lima_engine::forces(bool energy) {
-    if (state_pending) {
-        rebuild(true);
-        state_pending = false;
-    } else if (list_age >= p.nstlist) {
-        rebuild(false);
-    }
+    ensure_list();
     if (energy) CK(cudaMemsetAsync(st.energy, 0, sizeof(long long) * E_COUNT * st.n_sys, s_main));
     launch_zero_forces(st, s_main);
     // with phase timing on, every phase runs on the main stream so that each
@@ -770,7 +981,8 @@ void lima_engine::forces(bool energy) {
     CK(cudaEventRecord(ev_bonded, sb));
     if (pme_on) {
         mark(3, 0, sp);
-        launches += launch_pme(st, pp, energy, sp);
+        if (learned_active()) learned_pme_stage(energy, sp);
+        else launches += launch_pme(st, pp, energy, sp);
         mark(3, 1, sp);
     }
     CK(cudaEventRecord(ev_pme, sp));
@@ -785,7 +997,7 @@ void lima_engine::forces(bool energy) {
 void lima_engine::run_steps(int n) {
     CK(cudaEventRecord(ev_t0, s_main));
     int k = 0;
-    if (p.use_graphs && !phase_timing && !state_pending) {
+    if (p.use_graphs && !phase_timing && !state_pending && !learned_active()) {
         // whole pair-list periods replay as one graph; the last step stays eager
         // so that it can evaluate energies
         while (n - k > p.nstlist && list_age >= p.nstlist) {
@@ -809,6 +1021,16 @@ void lima_engine::run_steps(int n) {
         collect_phases();
         ++list_age;
         ++step;
+        if (lp_check_pending) {
+            // full-grid check of the learned correction: fall back to plain
+            // PME once the relative reciprocal-force RMSE exceeds the bound
+            double sums[4];
+            CK(cudaMemcpyAsync(sums, d_sums, sizeof(sums), cudaMemcpyDeviceToHost, s_main));
+            CK(cudaStreamSynchronize(s_main));
+            lp_check_pending = false;
+            lp_last_rel = sums[1] > 0.0 ? std::sqrt(sums[0] / sums[1]) : 0.0;
+            if (!(lp_last_rel <= lp_tol)) lp_fallback = true;
+        }
     }
     CK(cudaEventRecord(ev_t1, s_main));
     CK(cudaMemcpyAsync(energy_host.data(), st.energy, sizeof(long long) * energy_host.size(),
@@ -1181,7 +1403,7 @@ int lima_get_status(lima_engine* h, uint32_t* status) {
     return guarded(h, [&]() {
         unsigned s = 0;
         CK(cudaMemcpy(&s, h->st.status, sizeof(unsigned), cudaMemcpyDeviceToHost));
-        *status = s;
+        *status = s | (h->lp_fallback ? (unsigned)LIMA_STATUS_MLP_FALLBACK : 0u);
         return LIMA_OK;
     });
 }
@@ -1225,6 +1447,236 @@ int lima_enable_phase_timing(lima_engine* h, int enable) {
     if (!h) return LIMA_ERR_INVALID_ARG;
     h->phase_timing = enable != 0;
     return LIMA_OK;
+}
+
+// ------------------------------------------------------------ learned PME
+static int learned_ready(lima_engine* h) {
+    if (!h->built || !h->lp_ready) return fail(h, LIMA_ERR_STATE, "lima_learned_pme_setup must come first");
+    return LIMA_OK;
+}
+
+int lima_learned_pme_setup(lima_engine* h, int cx, int cy, int cz, int max_frames) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    if (cx < 8 || cy < 8 || cz < 8 || max_frames < 1)
+        return fail(h, LIMA_ERR_INVALID_ARG, "coarse grid dimensions must be >= 8 and max_frames >= 1");
+    return guarded(h, [&]() {
+        ensure_built(h);
+        if (!h->pme_on) return fail(h, LIMA_ERR_STATE, "the learned correction needs PME electrostatics");
+        h->learned_setup(cx, cy, cz, max_frames);
+        return LIMA_OK;
+    });
+}
+
+int lima_learned_pme_collect(lima_engine* h) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    return guarded(h, [&]() {
+        if (int e = learned_ready(h)) return e;
+        h->ensure_list();
+        cudaStream_t s = h->s_main;
+        h->learned_features(false, s);
+        h->learned_full(s, false);
+        const int N = h->st.n_atoms;
+        const int slot = h->ds_frames % h->ds_cap;
+        float* rf = h->ds_feat + (size_t)slot * N * MLP_IN;
+        float* rt = h->ds_target + (size_t)slot * N * 3;
+        h->launches += launch_collect(h->st, h->lp_feat, h->lp_fc, h->lp_ff, rf, rt, s);
+        if (!h->lp_norm) {
+            // the first frame fixes the input normalisation and the output scale
+            std::vector<float> f((size_t)N * MLP_IN), t((size_t)N * 3);
+            CK(cudaMemcpyAsync(f.data(), rf, f.size() * 4, cudaMemcpyDeviceToHost, s));
+            CK(cudaMemcpyAsync(t.data(), rt, t.size() * 4, cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            std::vector<float> mean(MLP_IN), inv(MLP_IN);
+            for (int c = 0; c < MLP_IN; ++c) {
+                double m1 = 0.0, m2 = 0.0;
+                for (int a = 0; a < N; ++a) {
+                    const double v = f[(size_t)a * MLP_IN + c];
+                    m1 += v;
+                    m2 += v * v;
+                }
+                m1 /= N;
+                const double sd = std::sqrt(std::max(m2 / N - m1 * m1, 0.0));
+                mean[c] = (float)m1;
+                h->mlp.in_mean[c] = (float)m1;
+                h->mlp.in_std[c] = (float)(sd > 1e-6 ? sd : 1.0);
+                inv[c] = 1.f / h->mlp.in_std[c];
+            }
+            double r2 = 0.0;
+            for (float v : t) r2 += (double)v * v;
+            const double rms = std::sqrt(r2 / std::max<size_t>(t.size(), 1));
+            h->mlp.out_scale = (float)(rms > 0.0 ? rms : 1.0);
+            CK(cudaMemcpyAsync(h->lp_mean, mean.data(), MLP_IN * 4, cudaMemcpyHostToDevice, s));
+            CK(cudaMemcpyAsync(h->lp_invstd, inv.data(), MLP_IN * 4, cudaMemcpyHostToDevice, s));
+            h->lp_norm = true;
+        }
+        CK(cudaStreamSynchronize(s));
+        ++h->ds_frames;
+        return LIMA_OK;
+    });
+}
+
+int lima_learned_pme_train(lima_engine* h, int epochs, int batch, float lr, uint64_t seed, double* final_loss) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    if (epochs < 0 || batch < 16 || !(lr >= 0.f)) return fail(h, LIMA_ERR_INVALID_ARG, "bad training arguments");
+    return guarded(h, [&]() {
+        if (int e = learned_ready(h)) return e;
+        if (h->ds_frames == 0) return fail(h, LIMA_ERR_STATE, "no frames collected");
+        if (batch > h->batch_cap) return fail(h, LIMA_ERR_INVALID_ARG, "batch larger than 65536 rows");
+        cudaStream_t s = h->s_main;
+        const size_t rows = (size_t)std::min(h->ds_frames, h->ds_cap) * h->st.n_atoms;
+        if (rows > (size_t)INT32_MAX) return fail(h, LIMA_ERR_UNSUPPORTED, "dataset above 2^31 rows");
+        if (h->d_idx_cap < rows) {
+            if (h->d_idx) {
+                cudaFree(h->d_idx);
+                h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), (void*)h->d_idx), h->allocs.end());
+            }
+            h->d_idx = h->dalloc<int>(rows);
+            h->d_idx_cap = rows;
+        }
+        std::vector<int> idx(rows);
+        std::iota(idx.begin(), idx.end(), 0);
+        const float inv_scale = 1.f / h->mlp.out_scale;
+        double last = 0.0;
+        for (int ep = 0; ep < epochs; ++ep) {
+            std::mt19937_64 rng(seed * 1000003ull + (uint64_t)ep);
+            for (size_t i = rows - 1; i > 0; --i) {
+                std::uniform_int_distribution<size_t> U(0, i);
+                std::swap(idx[i], idx[U(rng)]);
+            }
+            CK(cudaMemcpyAsync(h->d_idx, idx.data(), rows * sizeof(int), cudaMemcpyHostToDevice, s));
+            CK(cudaMemsetAsync(h->d_loss, 0, sizeof(double), s));
+            for (size_t off = 0; off < rows; off += batch) {
+                const int n = (int)std::min<size_t>(batch, rows - off);
+                h->launches += launch_gather_batch(h->ds_feat, h->ds_target, h->d_idx + off, n, h->lp_mean,
+                                                   h->lp_invstd, inv_scale, h->batch_X, h->batch_T, s);
+                h->launches += mlp_train_step(h->mlp, n, h->batch_X, h->batch_T, h->acts, lr, h->d_loss, s);
+            }
+            double sum = 0.0;
+            CK(cudaMemcpyAsync(&sum, h->d_loss, sizeof(double), cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            last = sum / (3.0 * rows);
+        }
+        CK(cudaStreamSynchronize(s));
+        if (final_loss) *final_loss = last;
+        return LIMA_OK;
+    });
+}
+
+int lima_learned_pme_enable(lima_engine* h, int on, int check_interval, double tolerance) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    if (int e = learned_ready(h)) return e;
+    if (on && !h->lp_norm) return fail(h, LIMA_ERR_STATE, "collect at least one frame before enabling");
+    h->lp_on = on != 0;
+    h->lp_check = check_interval > 0 ? check_interval : 50;
+    h->lp_tol = tolerance > 0.0 ? tolerance : 1e-3;
+    h->lp_fallback = false;
+    h->lp_check_pending = false;
+    h->lp_steps = 0;
+    h->lp_last_rel = -1.0;
+    return LIMA_OK;
+}
+
+int lima_learned_pme_eval(lima_engine* h, double* coarse_rel, double* learned_rel) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    return guarded(h, [&]() {
+        if (int e = learned_ready(h)) return e;
+        if (!h->lp_norm) return fail(h, LIMA_ERR_STATE, "collect at least one frame first");
+        h->ensure_list();
+        cudaStream_t s = h->s_main;
+        h->learned_features(true, s);
+        h->learned_full(s, false);
+        CK(cudaMemsetAsync(h->d_sums, 0, 4 * sizeof(double), s));
+        h->launches += launch_pred_error(h->st, h->lp_fc, h->lp_Y, h->mlp.out_scale, h->lp_ff, h->d_sums, s);
+        double sums[4];
+        CK(cudaMemcpyAsync(sums, h->d_sums, sizeof(sums), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        const double den = sums[1] > 0.0 ? sums[1] : 1.0;
+        if (coarse_rel) *coarse_rel = std::sqrt(sums[2] / den);
+        if (learned_rel) *learned_rel = std::sqrt(sums[0] / den);
+        return LIMA_OK;
+    });
+}
+
+int lima_learned_pme_status(lima_engine* h, int* active, int* fell_back, double* last_rel) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    if (active) *active = h->learned_active() ? 1 : 0;
+    if (fell_back) *fell_back = h->lp_fallback ? 1 : 0;
+    if (last_rel) *last_rel = h->lp_last_rel;
+    return LIMA_OK;
+}
+
+int lima_learned_pme_weights(lima_engine* h, int get, float* buf, int64_t n, int64_t* needed) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    if (needed) *needed = MLP_NSTATE;
+    if (!buf) return LIMA_OK;
+    if (n < MLP_NSTATE) return fail(h, LIMA_ERR_INVALID_ARG, "weight buffer too small");
+    return guarded(h, [&]() {
+        if (int e = learned_ready(h)) return e;
+        MlpModel& m = h->mlp;
+        size_t off = 0;
+        for (int l = 0; l < 4; ++l) {
+            const size_t nw = (size_t)MLP_K[l] * MLP_N[l], nb = MLP_N[l];
+            if (get) {
+                CK(cudaMemcpy(buf + off, m.w[l], nw * 4, cudaMemcpyDeviceToHost));
+                CK(cudaMemcpy(buf + off + nw, m.b[l], nb * 4, cudaMemcpyDeviceToHost));
+            } else {
+                CK(cudaMemcpy(m.w[l], buf + off, nw * 4, cudaMemcpyHostToDevice));
+                CK(cudaMemcpy(m.b[l], buf + off + nw, nb * 4, cudaMemcpyHostToDevice));
+            }
+            off += nw + nb;
+        }
+        if (get) {
+            std::copy(m.in_mean, m.in_mean + MLP_IN, buf + off);
+            std::copy(m.in_std, m.in_std + MLP_IN, buf + off + MLP_IN);
+            buf[off + 2 * MLP_IN] = m.out_scale;
+        } else {
+            std::vector<float> inv(MLP_IN);
+            for (int c = 0; c < MLP_IN; ++c) {
+                const float sd = buf[off + MLP_IN + c];
+                if (!(sd > 0.f)) return fail(h, LIMA_ERR_INVALID_ARG, "input scales must be > 0");
+                m.in_mean[c] = buf[off + c];
+                m.in_std[c] = sd;
+                inv[c] = 1.f / sd;
+            }
+            const float sc = buf[off + 2 * MLP_IN];
+            if (!(sc > 0.f)) return fail(h, LIMA_ERR_INVALID_ARG, "output scale must be > 0");
+            m.out_scale = sc;
+            CK(cudaMemcpy(h->lp_mean, m.in_mean, MLP_IN * 4, cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(h->lp_invstd, inv.data(), MLP_IN * 4, cudaMemcpyHostToDevice));
+            mlp_sync_bf16(m, h->s_main);
+            CK(cudaStreamSynchronize(h->s_main));
+            h->lp_norm = true;
+        }
+        return LIMA_OK;
+    });
+}
+
+int lima_learned_pme_gradients(lima_engine* h, int rows, const float* x, const float* t, float* grads,
+                               double* loss) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    if (rows < 1 || !x || !t || !grads) return fail(h, LIMA_ERR_INVALID_ARG, "bad gradient-check arguments");
+    return guarded(h, [&]() {
+        if (int e = learned_ready(h)) return e;
+        if (rows > h->batch_cap) return fail(h, LIMA_ERR_INVALID_ARG, "more than 65536 rows");
+        cudaStream_t s = h->s_main;
+        CK(cudaMemcpyAsync(h->batch_raw, x, (size_t)rows * MLP_IN * 4, cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(h->batch_T, t, (size_t)rows * 3 * 4, cudaMemcpyHostToDevice, s));
+        h->launches += launch_rows_to_bf16(rows, h->batch_raw, h->batch_X, s);
+        CK(cudaMemsetAsync(h->d_loss, 0, sizeof(double), s));
+        h->launches += mlp_train_step(h->mlp, rows, h->batch_X, h->batch_T, h->acts, 0.f, h->d_loss, s);
+        size_t off = 0;
+        for (int l = 0; l < 4; ++l) {
+            const size_t nw = (size_t)MLP_K[l] * MLP_N[l], nb = MLP_N[l];
+            CK(cudaMemcpyAsync(grads + off, h->mlp.gw[l], nw * 4, cudaMemcpyDeviceToHost, s));
+            CK(cudaMemcpyAsync(grads + off + nw, h->mlp.gb[l], nb * 4, cudaMemcpyDeviceToHost, s));
+            off += nw + nb;
+        }
+        double sum = 0.0;
+        CK(cudaMemcpyAsync(&sum, h->d_loss, sizeof(double), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        if (loss) *loss = sum / (3.0 * rows);
+        return LIMA_OK;
+    });
 }
 
 }  // extern "C"

@@ -1,0 +1,298 @@
+// mlp.cu — the network of the learned coarse-grid PME correction.
+//
+// A small MLP (68 -> 128 -> 128 -> 128 -> 3, SiLU) maps each atom's coarse-grid
+// reciprocal force (3), its charge (1) and a 64-value local descriptor to the
+// residual between the full-grid and the coarse-grid reciprocal force.  The
+// reference has no learned component.
+//
+// Layout: activations are row-major [rows][ld] BF16, one row per atom; weights
+// are kept as FP32 masters W[K][N] (Adam state beside them) and as two BF16
+// copies, W[K][N] and WT[N][K].  Every GEMM runs on the tensor cores through
+// mma.sync m16n8k16 (BF16 inputs, FP32 accumulation); a CTA of 8 warps owns 128
+// rows, a warp 16 rows and all N columns.  Weight and bias gradients are summed
+// per chunk of MLP_CHUNK rows into partial buffers and reduced in chunk order,
+// so training is deterministic.
+#include <cuda_bf16.h>
+
+#include "engine.h"
+#include "mlp.h"
+
+namespace lima {
+
+__device__ __forceinline__ void mma16816(float* c, const uint32_t* a, const uint32_t* b) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__device__ __forceinline__ uint32_t ld_pair(const __nv_bfloat16* p) {
+    return *reinterpret_cast<const uint32_t*>(p);
+}
+__device__ __forceinline__ uint32_t pack2(__nv_bfloat16 lo, __nv_bfloat16 hi) {
+    return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
+}
+__device__ __forceinline__ float silu(float z) { return z / (1.f + __expf(-z)); }
+__device__ __forceinline__ float dsilu(float z) {
+    const float s = 1.f / (1.f + __expf(-z));
+    return s * (1.f + z * (1.f - s));
+}
+
+// ------------------------------------------------------------------ row GEMM
+// C[rows][N] = A[rows][K] * B, with B given as BT[N][ldb] (row n holds B(:, n)).
+// MODE 0: hidden layer forward   z = C + bias; Z <- z (if Zout), H <- silu(z)
+// MODE 1: output layer forward   Y[row][0..7] <- C + bias (FP32)
+// MODE 2: backward through SiLU  dZ <- C * silu'(Zprev[row][n])
+template <int K, int N, int MODE>
+__global__ void __launch_bounds__(256) k_gemm_rows(int rows, const __nv_bfloat16* __restrict__ A, int lda,
+                                                   const __nv_bfloat16* __restrict__ BT, int ldb,
+                                                   const float* __restrict__ bias, __nv_bfloat16* __restrict__ Zout,
+                                                   __nv_bfloat16* __restrict__ Hout, int ldo,
+                                                   float* __restrict__ Y, const __nv_bfloat16* __restrict__ Zprev) {
+    constexpr int NT = N / 8;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, t = lane & 3;
+    const int r0 = blockIdx.x * 128 + warp * 16;
+    if (r0 >= rows) return;
+    float acc[NT][4];
+#pragma unroll
+    for (int n = 0; n < NT; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.f;
+    const int ra = min(r0 + g, rows - 1), rb = min(r0 + g + 8, rows - 1);
+#pragma unroll
+    for (int k0 = 0; k0 < K; k0 += 16) {
+        uint32_t a[4];
+        a[0] = ld_pair(A + (size_t)ra * lda + k0 + 2 * t);
+        a[1] = ld_pair(A + (size_t)rb * lda + k0 + 2 * t);
+        a[2] = ld_pair(A + (size_t)ra * lda + k0 + 8 + 2 * t);
+        a[3] = ld_pair(A + (size_t)rb * lda + k0 + 8 + 2 * t);
+#pragma unroll
+        for (int n = 0; n < NT; ++n) {
+            uint32_t b[2];
+            const __nv_bfloat16* bp = BT + (size_t)(8 * n + g) * ldb + k0 + 2 * t;
+            b[0] = ld_pair(bp);
+            b[1] = ld_pair(bp + 8);
+            mma16816(acc[n], a, b);
+        }
+    }
+#pragma unroll
+    for (int n = 0; n < NT; ++n) {
+        const int c = 8 * n + 2 * t;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int r = r0 + g + 8 * h;
+            if (r >= rows) continue;
+            float v0 = acc[n][2 * h], v1 = acc[n][2 * h + 1];
+            if (MODE == 0) {
+                v0 += bias[c];
+                v1 += bias[c + 1];
+                if (Zout)
+                    *reinterpret_cast<uint32_t*>(Zout + (size_t)r * ldo + c) =
+                        pack2(__float2bfloat16(v0), __float2bfloat16(v1));
+                *reinterpret_cast<uint32_t*>(Hout + (size_t)r * ldo + c) =
+                    pack2(__float2bfloat16(silu(v0)), __float2bfloat16(silu(v1)));
+            } else if (MODE == 1) {
+                Y[(size_t)r * 8 + c] = v0 + bias[c];
+                Y[(size_t)r * 8 + c + 1] = v1 + bias[c + 1];
+            } else {
+                const float z0 = __bfloat162float(Zprev[(size_t)r * ldo + c]);
+                const float z1 = __bfloat162float(Zprev[(size_t)r * ldo + c + 1]);
+                *reinterpret_cast<uint32_t*>(Hout + (size_t)r * ldo + c) =
+                    pack2(__float2bfloat16(v0 * dsilu(z0)), __float2bfloat16(v1 * dsilu(z1)));
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------- weight gradient
+// part[chunk][K][N] = sum over the chunk's rows m of X[m][k] * dZ[m][n]
+// (tensor cores: A = X^T, B = dZ; the row pairs (m, m+1) are gathered per lane)
+template <int K, int N>
+__global__ void __launch_bounds__(256) k_gemm_wgrad(int rows, const __nv_bfloat16* __restrict__ X, int ldx,
+                                                    const __nv_bfloat16* __restrict__ dZ, int ldz,
+                                                    float* __restrict__ part, int chunk) {
+    constexpr int NT = N / 8;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, t = lane & 3;
+    const int k0 = warp * 16;           // this warp's 16 rows of the K x N result
+    if (k0 >= K) return;
+    const int m_begin = blockIdx.x * chunk, m_end = min(rows, m_begin + chunk);
+    float acc[NT][4];
+#pragma unroll
+    for (int n = 0; n < NT; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.f;
+    const __nv_bfloat16 zero = __float2bfloat16(0.f);
+    for (int m0 = m_begin; m0 < m_end; m0 += 16) {
+        // A(r, c) = X[m0 + c][k0 + r]
+        auto xa = [&](int r, int c) {
+            const int m = m0 + c;
+            return m < m_end ? X[(size_t)m * ldx + k0 + r] : zero;
+        };
+        uint32_t a[4];
+        a[0] = pack2(xa(g, 2 * t), xa(g, 2 * t + 1));
+        a[1] = pack2(xa(g + 8, 2 * t), xa(g + 8, 2 * t + 1));
+        a[2] = pack2(xa(g, 2 * t + 8), xa(g, 2 * t + 9));
+        a[3] = pack2(xa(g + 8, 2 * t + 8), xa(g + 8, 2 * t + 9));
+#pragma unroll
+        for (int n = 0; n < NT; ++n) {
+            // B(k, n) = dZ[m0 + k][n]
+            auto zb = [&](int k, int col) {
+                const int m = m0 + k;
+                return m < m_end ? dZ[(size_t)m * ldz + col] : zero;
+            };
+            uint32_t b[2];
+            b[0] = pack2(zb(2 * t, 8 * n + g), zb(2 * t + 1, 8 * n + g));
+            b[1] = pack2(zb(2 * t + 8, 8 * n + g), zb(2 * t + 9, 8 * n + g));
+            mma16816(acc[n], a, b);
+        }
+    }
+    float* out = part + (size_t)blockIdx.x * K * N;
+#pragma unroll
+    for (int n = 0; n < NT; ++n) {
+        const int c = 8 * n + 2 * t;
+        out[(size_t)(k0 + g) * N + c] = acc[n][0];
+        out[(size_t)(k0 + g) * N + c + 1] = acc[n][1];
+        out[(size_t)(k0 + g + 8) * N + c] = acc[n][2];
+        out[(size_t)(k0 + g + 8) * N + c + 1] = acc[n][3];
+    }
+}
+
+// grad[i] = sum over chunks (fixed order) of part[chunk][i]
+__global__ void k_reduce_parts(const float* __restrict__ part, int n_chunks, int n, float* __restrict__ grad) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float s = 0.f;
+    for (int c = 0; c < n_chunks; ++c) s += part[(size_t)c * n + i];
+    grad[i] = s;
+}
+
+// bias-gradient partials: column sums of dZ over one chunk of rows per block
+__global__ void k_colsum_part(int rows, const __nv_bfloat16* __restrict__ dZ, int ldz, int n, int chunk,
+                              float* __restrict__ part) {
+    const int c = threadIdx.x;
+    if (c >= n) return;
+    const int r0 = blockIdx.x * chunk, r1 = min(rows, r0 + chunk);
+    float s = 0.f;
+    for (int r = r0; r < r1; ++r) s += __bfloat162float(dZ[(size_t)r * ldz + c]);
+    part[(size_t)blockIdx.x * n + c] = s;
+}
+
+// ------------------------------------------------------------ loss, optimiser
+// MSE over the 3 outputs; dZ4 = 2 (y - t) / (3 rows), padded to 16 columns
+__global__ void k_mse(int rows, const float* __restrict__ Y, const float* __restrict__ T,
+                      __nv_bfloat16* __restrict__ dZ4, double* __restrict__ loss) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    double l = 0.0;
+    if (r < rows) {
+        const float inv = 2.f / (3.f * (float)rows);
+        for (int c = 0; c < 16; ++c) {
+            float d = 0.f;
+            if (c < 3) {
+                const float e = Y[(size_t)r * 8 + c] - T[(size_t)r * 3 + c];
+                l += (double)e * e;
+                d = e * inv;
+            }
+            dZ4[(size_t)r * 16 + c] = __float2bfloat16(d);
+        }
+    }
+    l = warp_sum(l);
+    if ((threadIdx.x & 31) == 0 && l != 0.0) atomicAdd(loss, l);
+}
+
+__global__ void k_adam(int n, float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
+                       float* __restrict__ v, float lr, float b1, float b2, float c1, float c2, float eps) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    w[i] -= lr * (mi * c1) / (sqrtf(vi * c2) + eps);
+}
+
+// BF16 copies of a master weight W[K][N]: W[K][ldw] and WT[N][ldt]
+__global__ void k_to_bf16(const float* __restrict__ w, int K, int N, __nv_bfloat16* __restrict__ Wb, int ldw,
+                          __nv_bfloat16* __restrict__ WTb, int ldt) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= K * N) return;
+    const int k = i / N, n = i - k * N;
+    const __nv_bfloat16 b = __float2bfloat16(w[i]);
+    if (Wb) Wb[(size_t)k * ldw + n] = b;
+    if (WTb) WTb[(size_t)n * ldt + k] = b;
+}
+
+// ---------------------------------------------------------- model host side
+namespace {
+inline unsigned blocks(long long n, int tb) { return (unsigned)((n + tb - 1) / tb); }
+}  // namespace
+
+void mlp_sync_bf16(MlpModel& m, cudaStream_t s) {
+    for (int l = 0; l < 4; ++l) {
+        const int K = MLP_K[l], N = MLP_N[l];
+        // the last layer's W keeps 16 columns (8..15 zero) for the backward GEMM
+        const int ldw = l == 3 ? 16 : N;
+        k_to_bf16<<<blocks((long long)K * N, 256), 256, 0, s>>>(m.w[l], K, N, m.wb[l], ldw, m.wtb[l], K);
+    }
+}
+
+int mlp_forward(const MlpModel& m, int rows, const __nv_bfloat16* X, MlpActs* acts, float* Y, cudaStream_t s) {
+    const unsigned g = blocks(rows, 128);
+    __nv_bfloat16* z[3] = {acts ? acts->z[0] : nullptr, acts ? acts->z[1] : nullptr, acts ? acts->z[2] : nullptr};
+    __nv_bfloat16* h[3] = {acts ? acts->h[0] : m.tmp[0], acts ? acts->h[1] : m.tmp[1], acts ? acts->h[2] : m.tmp[0]};
+    k_gemm_rows<MLP_KIN, 128, 0><<<g, 256, 0, s>>>(rows, X, MLP_KIN, m.wtb[0], MLP_KIN, m.b[0], z[0], h[0], 128,
+                                                   nullptr, nullptr);
+    k_gemm_rows<128, 128, 0><<<g, 256, 0, s>>>(rows, h[0], 128, m.wtb[1], 128, m.b[1], z[1], h[1], 128, nullptr,
+                                               nullptr);
+    k_gemm_rows<128, 128, 0><<<g, 256, 0, s>>>(rows, h[1], 128, m.wtb[2], 128, m.b[2], z[2], h[2], 128, nullptr,
+                                               nullptr);
+    k_gemm_rows<128, 8, 1><<<g, 256, 0, s>>>(rows, h[2], 128, m.wtb[3], 128, m.b[3], nullptr, nullptr, 8, Y,
+                                             nullptr);
+    return 4;
+}
+
+int mlp_train_step(MlpModel& m, int rows, const __nv_bfloat16* X, const float* T, MlpActs& a, float lr,
+                   double* d_loss, cudaStream_t s) {
+    int launches = mlp_forward(m, rows, X, &a, a.y, s);
+    const unsigned g = blocks(rows, 128);
+    k_mse<<<blocks(rows, 256), 256, 0, s>>>(rows, a.y, T, a.dz4, d_loss);
+    const int chunk = MLP_CHUNK;
+    const unsigned nch = blocks(rows, chunk);
+    // layer 4: dW4 = H3^T dZ4 (first 8 of the 16 dZ4 columns), db4, dZ3
+    k_gemm_wgrad<128, 8><<<nch, 256, 0, s>>>(rows, a.h[2], 128, a.dz4, 16, m.part, chunk);
+    k_reduce_parts<<<blocks(128 * 8, 256), 256, 0, s>>>(m.part, nch, 128 * 8, m.gw[3]);
+    k_colsum_part<<<nch, 128, 0, s>>>(rows, a.dz4, 16, 8, chunk, m.bpart);
+    k_reduce_parts<<<1, 128, 0, s>>>(m.bpart, nch, 8, m.gb[3]);
+    k_gemm_rows<16, 128, 2><<<g, 256, 0, s>>>(rows, a.dz4, 16, m.wb[3], 16, nullptr, nullptr, a.dz[2], 128, nullptr,
+                                              a.z[2]);
+    // layers 3 and 2
+    for (int l = 2; l >= 1; --l) {
+        k_gemm_wgrad<128, 128><<<nch, 256, 0, s>>>(rows, a.h[l - 1], 128, a.dz[l], 128, m.part, chunk);
+        k_reduce_parts<<<blocks(128 * 128, 256), 256, 0, s>>>(m.part, nch, 128 * 128, m.gw[l]);
+        k_colsum_part<<<nch, 128, 0, s>>>(rows, a.dz[l], 128, 128, chunk, m.bpart);
+        k_reduce_parts<<<1, 128, 0, s>>>(m.bpart, nch, 128, m.gb[l]);
+        k_gemm_rows<128, 128, 2><<<g, 256, 0, s>>>(rows, a.dz[l], 128, m.wb[l], 128, nullptr, nullptr, a.dz[l - 1],
+                                                   128, nullptr, a.z[l - 1]);
+    }
+    // layer 1: dW1 = X^T dZ1
+    k_gemm_wgrad<MLP_KIN, 128><<<nch, 256, 0, s>>>(rows, X, MLP_KIN, a.dz[0], 128, m.part, chunk);
+    k_reduce_parts<<<blocks(MLP_KIN * 128, 256), 256, 0, s>>>(m.part, nch, MLP_KIN * 128, m.gw[0]);
+    k_colsum_part<<<nch, 128, 0, s>>>(rows, a.dz[0], 128, 128, chunk, m.bpart);
+    k_reduce_parts<<<1, 128, 0, s>>>(m.bpart, nch, 128, m.gb[0]);
+    launches += 21;
+    if (lr > 0.f) {
+        ++m.adam_step;
+        const float b1 = 0.9f, b2 = 0.999f;
+        const float c1 = 1.f / (1.f - powf(b1, (float)m.adam_step));
+        const float c2 = 1.f / (1.f - powf(b2, (float)m.adam_step));
+        for (int l = 0; l < 4; ++l) {
+            const int nw = MLP_K[l] * MLP_N[l];
+            k_adam<<<blocks(nw, 256), 256, 0, s>>>(nw, m.w[l], m.gw[l], m.mw[l], m.vw[l], lr, b1, b2, c1, c2, 1e-8f);
+            k_adam<<<1, 128, 0, s>>>(MLP_N[l], m.b[l], m.gb[l], m.mb[l], m.vb[l], lr, b1, b2, c1, c2, 1e-8f);
+        }
+        mlp_sync_bf16(m, s);
+        launches += 12;
+    }
+    return launches;
+}
+
+}  // namespace lima

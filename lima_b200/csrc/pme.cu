@@ -504,7 +504,12 @@ void set_pme_sys_twiddles(void* dst, int offx, int offy, int offz) {
     d->pz.tw_off = offz;
 }
 
+// The attribute is per kernel and process-wide: it only ever grows, so an
+// engine with small grids cannot shrink the room another engine relies on.
 void pme_set_smem_limits(int maxn) {
+    static int largest = 0;
+    if (maxn <= largest) return;
+    largest = maxn;
     const int by = (int)fft_smem_bytes(FFT_TX, maxn), bx = (int)fft_smem_bytes(FFT_XLINES, maxn);
     cudaFuncSetAttribute(k_fft_y, cudaFuncAttributeMaxDynamicSharedMemorySize, by);
     cudaFuncSetAttribute(k_fft_z_conv, cudaFuncAttributeMaxDynamicSharedMemorySize, by);

@@ -36,7 +36,12 @@ EXPORTED = [
     "lima_get_state", "lima_compute_forces", "lima_step", "lima_minimize", "lima_get_forces",
     "lima_get_energies", "lima_get_pairlist", "lima_get_status", "lima_clear_status",
     "lima_get_timings", "lima_reset_timings", "lima_enable_phase_timing", "lima_pme_recip_noalloc",
+    "lima_learned_pme_setup", "lima_learned_pme_collect", "lima_learned_pme_train", "lima_learned_pme_enable",
+    "lima_learned_pme_eval", "lima_learned_pme_status", "lima_learned_pme_weights",
+    "lima_learned_pme_gradients",
 ]
+MLP_NPARAM = 80 * 128 + 128 + 2 * (128 * 128 + 128) + 128 * 8 + 8   # network parameters
+MLP_NSTATE = MLP_NPARAM + 2 * 68 + 1                               # + normalisation and output scale
 
 
 class LimaError(RuntimeError):
@@ -120,6 +125,15 @@ def load_library(path: str = LIB_PATH):
                                                   ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                   ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p,
                                                   ctypes.c_void_p]),
+        "lima_learned_pme_setup": (ctypes.c_int, [h, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+        "lima_learned_pme_collect": (ctypes.c_int, [h]),
+        "lima_learned_pme_train": (ctypes.c_int, [h, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_uint64,
+                                                  f64p]),
+        "lima_learned_pme_enable": (ctypes.c_int, [h, ctypes.c_int, ctypes.c_int, ctypes.c_double]),
+        "lima_learned_pme_eval": (ctypes.c_int, [h, f64p, f64p]),
+        "lima_learned_pme_status": (ctypes.c_int, [h, P(ctypes.c_int), P(ctypes.c_int), f64p]),
+        "lima_learned_pme_weights": (ctypes.c_int, [h, ctypes.c_int, f32p, ctypes.c_int64, P(ctypes.c_int64)]),
+        "lima_learned_pme_gradients": (ctypes.c_int, [h, ctypes.c_int, f32p, f32p, f32p, f64p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -321,3 +335,63 @@ class Engine:
 
     def phase_timing(self, enable: bool):
         self._check(self.lib.lima_enable_phase_timing(self.h, 1 if enable else 0))
+
+
+class LearnedPME:
+    """The learned coarse-grid PME correction of one engine (no reference
+    counterpart): collect frames from the engine's own states, train the
+    network on the GPU, then let stepping use coarse PME + network with a
+    full-grid check every ``check_interval`` steps."""
+
+    def __init__(self, engine: Engine, coarse_grid=(32, 32, 32), max_frames: int = 16):
+        self.engine = engine
+        self.lib = engine.lib
+        g = [int(v) for v in coarse_grid]
+        engine._check(self.lib.lima_learned_pme_setup(engine.h, g[0], g[1], g[2], int(max_frames)))
+
+    def collect(self):
+        """Labels the engine's current state (one training frame)."""
+        self.engine._check(self.lib.lima_learned_pme_collect(self.engine.h))
+
+    def train(self, epochs: int, batch: int = 65536, lr: float = 1e-3, seed: int = 1) -> float:
+        loss = ctypes.c_double(0.0)
+        self.engine._check(self.lib.lima_learned_pme_train(self.engine.h, int(epochs), int(batch), float(lr),
+                                                           int(seed), ctypes.byref(loss)))
+        return loss.value
+
+    def enable(self, on: bool = True, check_interval: int = 50, tolerance: float = 1e-3):
+        self.engine._check(self.lib.lima_learned_pme_enable(self.engine.h, 1 if on else 0, int(check_interval),
+                                                            float(tolerance)))
+
+    def eval(self) -> tuple[float, float]:
+        """(coarse, corrected) relative RMSE of the reciprocal force vs the full grid."""
+        c, l = ctypes.c_double(0.0), ctypes.c_double(0.0)
+        self.engine._check(self.lib.lima_learned_pme_eval(self.engine.h, ctypes.byref(c), ctypes.byref(l)))
+        return c.value, l.value
+
+    def status(self) -> dict:
+        a, f, r = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_double(0.0)
+        self.engine._check(self.lib.lima_learned_pme_status(self.engine.h, ctypes.byref(a), ctypes.byref(f),
+                                                            ctypes.byref(r)))
+        return {"active": bool(a.value), "fell_back": bool(f.value), "last_rel": r.value}
+
+    def weights(self) -> np.ndarray:
+        buf = np.zeros(MLP_NSTATE, np.float32)
+        need = ctypes.c_int64(0)
+        self.engine._check(self.lib.lima_learned_pme_weights(self.engine.h, 1, _f32(buf)[1], buf.size,
+                                                             ctypes.byref(need)))
+        return buf
+
+    def set_weights(self, state):
+        buf, ptr = _f32(np.asarray(state, np.float32).reshape(-1))
+        self.engine._check(self.lib.lima_learned_pme_weights(self.engine.h, 0, ptr, buf.size, None))
+
+    def gradients(self, x, t) -> tuple[float, np.ndarray]:
+        """Loss and parameter gradients of one pass over caller rows (no update)."""
+        x, xp = _f32(x, 68)
+        t, tp = _f32(t, 3)
+        g = np.zeros(MLP_NPARAM, np.float32)
+        loss = ctypes.c_double(0.0)
+        self.engine._check(self.lib.lima_learned_pme_gradients(self.engine.h, len(x), xp, tp, _f32(g)[1],
+                                                               ctypes.byref(loss)))
+        return loss.value, g

@@ -743,4 +743,78 @@ void orc_fft3d(int kx, int ky, int kz, double* data, int sign) {
     fft3d(kx, ky, kz, reinterpret_cast<cd*>(data), sign);
 }
 
+double orc_mlp_grads(int rows, const double* x, const double* t, const double* params, double* grads) {
+    const int K[4] = {80, 128, 128, 128}, N[4] = {128, 128, 128, 8}, nin = 68, nout = 3;
+    const double* W[4];
+    const double* b[4];
+    double* gW[4];
+    double* gb[4];
+    size_t off = 0;
+    for (int l = 0; l < 4; ++l) {
+        W[l] = params + off;
+        gW[l] = grads + off;
+        off += (size_t)K[l] * N[l];
+        b[l] = params + off;
+        gb[l] = grads + off;
+        off += N[l];
+    }
+    std::fill(grads, grads + off, 0.0);
+    double loss = 0.0;
+    std::vector<double> a[4], z[3], dz(128), dprev(128);
+    for (int l = 0; l < 4; ++l) a[l].assign(128, 0.0);
+    for (int l = 0; l < 3; ++l) z[l].assign(128, 0.0);
+    std::vector<double> y(8);
+    const double inv = 2.0 / (3.0 * rows);
+    for (int r = 0; r < rows; ++r) {
+        std::fill(a[0].begin(), a[0].end(), 0.0);
+        for (int k = 0; k < nin; ++k) a[0][k] = x[(size_t)r * nin + k];
+        for (int l = 0; l < 3; ++l) {
+            for (int n = 0; n < N[l]; ++n) {
+                double s = b[l][n];
+                for (int k = 0; k < K[l]; ++k) s += a[l][k] * W[l][(size_t)k * N[l] + n];
+                z[l][n] = s;
+                a[l + 1][n] = s / (1.0 + std::exp(-s));
+            }
+        }
+        for (int n = 0; n < nout; ++n) {
+            double s = b[3][n];
+            for (int k = 0; k < 128; ++k) s += a[3][k] * W[3][(size_t)k * 8 + n];
+            y[n] = s;
+        }
+        // backward
+        std::fill(dz.begin(), dz.end(), 0.0);
+        for (int n = 0; n < nout; ++n) {
+            const double e = y[n] - t[(size_t)r * nout + n];
+            loss += e * e;
+            dz[n] = e * inv;
+        }
+        for (int n = 0; n < nout; ++n) {
+            gb[3][n] += dz[n];
+            for (int k = 0; k < 128; ++k) gW[3][(size_t)k * 8 + n] += a[3][k] * dz[n];
+        }
+        for (int k = 0; k < 128; ++k) {
+            double s = 0.0;
+            for (int n = 0; n < nout; ++n) s += W[3][(size_t)k * 8 + n] * dz[n];
+            dprev[k] = s;
+        }
+        for (int l = 2; l >= 0; --l) {
+            for (int n = 0; n < N[l]; ++n) {
+                const double sg = 1.0 / (1.0 + std::exp(-z[l][n]));
+                dz[n] = dprev[n] * sg * (1.0 + z[l][n] * (1.0 - sg));
+            }
+            for (int n = 0; n < N[l]; ++n) {
+                gb[l][n] += dz[n];
+                for (int k = 0; k < K[l]; ++k) gW[l][(size_t)k * N[l] + n] += a[l][k] * dz[n];
+            }
+            if (l > 0)
+                for (int k = 0; k < K[l]; ++k) {
+                    double s = 0.0;
+                    for (int n = 0; n < N[l]; ++n) s += W[l][(size_t)k * N[l] + n] * dz[n];
+                    dprev[k] = s;
+                }
+        }
+    }
+    return loss / (3.0 * rows);
+}
+
 }  // extern "C"

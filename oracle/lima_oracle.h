@@ -112,6 +112,16 @@ void orc_em_step(int n, double* pos, const double* forces, double* adam, int ste
  * normalisation).  data is interleaved re,im. */
 void orc_fft3d(int kx, int ky, int kz, double* data, int sign);
 
+/* FP64 forward and backward pass of the learned-PME network (no reference
+ * counterpart; the checker of the BF16 tensor-core training kernels).
+ * Network 68 -> 128 -> 128 -> 128 -> 3, SiLU after each hidden layer.
+ * params/grads layout: W1[80][128] b1[128] W2[128][128] b2[128] W3[128][128]
+ * b3[128] W4[128][8] b4[8] (W[k][n] maps input k to output n; rows 68..79 of
+ * W1 and columns 3..7 of W4 are unused).  x[rows][68], t[rows][3].
+ * Loss = mean over rows x 3 of (y - t)^2; returns the loss and overwrites
+ * grads with d loss / d params. */
+double orc_mlp_grads(int rows, const double* x, const double* t, const double* params, double* grads);
+
 #ifdef __cplusplus
 }
 #endif

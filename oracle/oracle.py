@@ -62,6 +62,8 @@ def lib():
         L.orc_em_step.argtypes = [ctypes.c_int, _d, _d, _d, ctypes.c_int]
         L.orc_fft3d.restype = None
         L.orc_fft3d.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _d, ctypes.c_int]
+        L.orc_mlp_grads.restype = ctypes.c_double
+        L.orc_mlp_grads.argtypes = [ctypes.c_int, _d, _d, _d, _d]
         _lib = L
     return _lib
 
@@ -213,3 +215,19 @@ def fft3d(data: np.ndarray, sign: int) -> np.ndarray:
     kz, ky, kx = a.shape
     lib().orc_fft3d(kx, ky, kz, a.view(np.float64).ctypes.data_as(_d), sign)
     return a
+
+
+MLP_NPARAM = 80 * 128 + 128 + 2 * (128 * 128 + 128) + 128 * 8 + 8
+
+
+def mlp_grads(x, t, params):
+    """FP64 loss and parameter gradients of the learned-PME network.
+
+    x (rows, 68), t (rows, 3), params (MLP_NPARAM,) in the engine's layout."""
+    x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1, 68)
+    t = np.ascontiguousarray(t, dtype=np.float64).reshape(-1, 3)
+    params = np.ascontiguousarray(params, dtype=np.float64).reshape(-1)
+    assert params.size == MLP_NPARAM and len(t) == len(x)
+    g = np.zeros(MLP_NPARAM)
+    loss = lib().orc_mlp_grads(len(x), _dp(x), _dp(t), _dp(params), _dp(g))
+    return loss, g
