@@ -308,6 +308,18 @@ def run_lima(args):
     s = systems.config2()
     eng = Engine(cutoff=CUTOFF, electrostatics=E.ES_EWALD, ewald_tol=1e-5, nstlist=10, dt=DT_NS, device=local)
     eng.load(s, pme_grid=GRID)
+    if args.profile_learned:
+        # profiling mode for the learned correction: one labelled frame, one
+        # epoch, then `profile_learned` steps with coarse PME + network
+        lp = E.LearnedPME(eng, coarse_grid=(32, 32, 32), max_frames=1)
+        eng.step(5)
+        lp.collect()
+        lp.train(epochs=1, batch=65536)
+        lp.enable(True, check_interval=1000, tolerance=1.0)
+        eng.step(args.profile_learned)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_learned_steps": args.profile_learned, "timings": eng.timings()}), flush=True)
+        return 0
     if args.profile:
         # profiling mode: set-up plus `profile` plain steps, nothing else (for ncu)
         eng.step(args.profile)
@@ -464,6 +476,8 @@ def main():
     ap.add_argument("--impl", default="lima", choices=["lima", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", type=int, default=0, help="only set up and run this many steps (ncu)")
+    ap.add_argument("--profile-learned", type=int, default=0,
+                    help="only set up the learned correction and run this many steps with it (ncu)")
     ap.add_argument("--no-other-configs", action="store_true")
     ap.add_argument("--skip-batch", action="store_true")
     ap.add_argument("--other-steps", type=int, default=100)

@@ -834,10 +834,7 @@ void lima_engine::learned_features(bool forward, cudaStream_t s) {
     CK(cudaMemsetAsync(lp_fc, 0, sizeof(long long) * 3 * (size_t)st.n_slots, s));
     launches += launch_pme(st_c, pp_c, false, s);
     launches += launch_descriptor(st, lp_fc, lp_feat, s);
-    if (forward && lp_norm) {
-        launches += launch_mlp_input(st, lp_feat, lp_mean, lp_invstd, lp_X, s);
-        launches += mlp_forward(mlp, st.n_slots, lp_X, nullptr, lp_Y, s);
-    }
+    if (forward && lp_norm) launches += mlp_infer(mlp, st.n_slots, lp_feat, lp_mean, lp_invstd, lp_Y, s);
 }
 
 // full-grid reciprocal force into lp_ff (energy, when asked, into the engine's

@@ -42,17 +42,19 @@ __device__ __forceinline__ void radial16(float r, float* g) {
     const int kc = min(DESC_RADIAL - 1, max(0, __float2int_rn(r / d)));
     const float dc = r - kc * d;
     const float A = (2.f * d * r - d * d) * i2w2;   // log(g_{k+1}/g_k) = A - k B
-    float gk = __expf(-dc * dc * i2w2);
-    g[kc] = gk;
+    const float gk = __expf(-dc * dc * i2w2);
+    // every index below is static (the loops unroll), so g stays in registers
     float up = __expf(A - kc * B);
     float v = gk;
 #pragma unroll
-    for (int k = 0; k < DESC_RADIAL; ++k)
+    for (int k = 0; k < DESC_RADIAL; ++k) {
+        if (k == kc) g[k] = gk;
         if (k > kc) {
             v *= up;
             up *= F;
             g[k] = v;
         }
+    }
     float dn = __expf(-(A - (kc - 1) * B));          // g_{k-1} / g_k at k = kc
     v = gk;
 #pragma unroll
@@ -64,55 +66,115 @@ __device__ __forceinline__ void radial16(float r, float* g) {
         }
 }
 
-// one thread per slot; neighbours come from the column/cluster grid of the
-// last pair-list build (the z extent of every cluster prunes a column)
-__global__ void __launch_bounds__(128) k_descriptor(DevState st, const long long* __restrict__ fc,
-                                                    float* __restrict__ feat) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= st.n_slots || st.orig[s] < 0) return;
-    const int sysi = st.cluster_sys[s / CLUSTER];
+// One warp per i-cluster.  Lane (ii = lane & 7, jq = lane >> 3) owns i-atom ii
+// and the j-atoms jq and jq + 4 of every candidate j-cluster; candidates come
+// from the column grid of the last pair-list build in units of up to 32
+// clusters of one column (one per lane), tested against the i-cluster's
+// extent, staged in shared memory with one round of loads and then visited in
+// order by the whole warp (so the warp never diverges on the walk).  The next
+// unit's extents are requested before the current unit is evaluated.
+constexpr int DS_WARPS = 4;
+
+__global__ void __launch_bounds__(DS_WARPS * 32, 3) k_descriptor(DevState st, const long long* __restrict__ fc,
+                                                                 float* __restrict__ feat) {
+    __shared__ float4 stage_x[DS_WARPS][32][CLUSTER];
+    const int ci = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    if (ci >= st.n_clusters) return;
+    const int sysi = st.cluster_sys[ci];
     const SysDesc& sd = st.sys[sysi];
-    const float4 xi = st.xyzq[s];
+    if (ci - sd.cluster_cap_off >= st.sys_nclusters[sysi]) return;
+    const float4 ilo = st.bb_lo[ci], ihi = st.bb_hi[ci];
+    if (ilo.w == 0.f) return;   // empty cluster
+    const int ii = lane & 7, jq = lane >> 3;
+    const int si = ci * CLUSTER + ii;
+    const bool ivalid = st.orig[si] >= 0;
+    const float4 xi = st.xyzq[si];
     const float L[3] = {sd.boxf[0], sd.boxf[1], sd.boxf[2]};
     const float iL[3] = {sd.inv_boxf[0], sd.inv_boxf[1], sd.inv_boxf[2]};
+    const float ic[3] = {0.5f * (ilo.x + ihi.x), 0.5f * (ilo.y + ihi.y), 0.5f * (ilo.z + ihi.z)};
+    const float ie[3] = {0.5f * (ihi.x - ilo.x), 0.5f * (ihi.y - ilo.y), 0.5f * (ihi.z - ilo.z)};
     float acc[4][DESC_RADIAL];
 #pragma unroll
     for (int c = 0; c < 4; ++c)
 #pragma unroll
         for (int k = 0; k < DESC_RADIAL; ++k) acc[c][k] = 0.f;
 
-    const float R = kDescReach;
-    int cx0 = (int)floorf((xi.x - R) / sd.col_w[0]);
-    int nx = (int)floorf((xi.x + R) / sd.col_w[0]) - cx0 + 1;
+    const float R = kDescReach, R2 = R * R;
+    int cx0 = (int)floorf((ilo.x - R) / sd.col_w[0]);
+    int nx = (int)floorf((ihi.x + R) / sd.col_w[0]) - cx0 + 1;
     if (nx >= sd.ncol_x) cx0 = 0, nx = sd.ncol_x;
-    int cy0 = (int)floorf((xi.y - R) / sd.col_w[1]);
-    int ny = (int)floorf((xi.y + R) / sd.col_w[1]) - cy0 + 1;
+    int cy0 = (int)floorf((ilo.y - R) / sd.col_w[1]);
+    int ny = (int)floorf((ihi.y + R) / sd.col_w[1]) - cy0 + 1;
     if (ny >= sd.ncol_y) cy0 = 0, ny = sd.ncol_y;
+    const int ncw = nx * ny;
+    auto header = [&](int k, int& j0, int& nj) {
+        const int iy = k / nx, ix = k - iy * nx;
+        const int col = sd.col_off + wrap_col(cx0 + ix, sd.ncol_x) + sd.ncol_x * wrap_col(cy0 + iy, sd.ncol_y);
+        j0 = st.col_cl_start[col];
+        nj = st.col_ncl[col];
+    };
     const float cut2 = DESC_CUT * DESC_CUT;
     constexpr float kPiF = 3.14159265358979f;
-    for (int iy = 0; iy < ny; ++iy) {
-        const int cy = wrap_col(cy0 + iy, sd.ncol_y);
-        for (int ix = 0; ix < nx; ++ix) {
-            const int cx = wrap_col(cx0 + ix, sd.ncol_x);
-            const int col = sd.col_off + cx + sd.ncol_x * cy;
-            const int j0 = st.col_cl_start[col], nj = st.col_ncl[col];
-            for (int jc = j0; jc < j0 + nj; ++jc) {
-                const float4 lo = st.bb_lo[jc], hi = st.bb_hi[jc];
-                // z gap to the cluster's extent under the nearest periodic image
-                const float zc = 0.5f * (lo.z + hi.z), ze = 0.5f * (hi.z - lo.z);
-                float dzc = zc - xi.z;
-                dzc -= L[2] * rintf(dzc * iL[2]);
-                if (fabsf(dzc) - ze > R) continue;
-                for (int k = 0; k < CLUSTER; ++k) {
-                    const int sj = jc * CLUSTER + k;
-                    if (sj == s || st.orig[sj] < 0) continue;
-                    const float4 xj = st.xyzq[sj];
-                    float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
-                    dx -= L[0] * rintf(dx * iL[0]);
-                    dy -= L[1] * rintf(dy * iL[1]);
-                    dz -= L[2] * rintf(dz * iL[2]);
-                    const float r2 = dx * dx + dy * dy + dz * dz;
-                    if (r2 >= cut2 || r2 <= 0.f || xj.w == 0.f) continue;
+    int k = 0, b = 0, j0 = 0, nj = 0;
+    while (k < ncw) {
+        header(k, j0, nj);
+        if (nj > 0) break;
+        ++k;
+    }
+    float4 jlo = make_float4(0.f, 0.f, 0.f, 0.f), jhi = jlo;
+    if (k < ncw && lane < nj) {
+        jlo = st.bb_lo[j0 + lane];
+        jhi = st.bb_hi[j0 + lane];
+    }
+    while (k < ncw) {
+        const int jc_lane = j0 + b + lane;
+        bool pass = false;
+        if (b + lane < nj && jlo.w != 0.f) {
+            // gap between the two extents under the nearest periodic image
+            const float jcx = 0.5f * (jlo.x + jhi.x) - ic[0], jcy = 0.5f * (jlo.y + jhi.y) - ic[1],
+                        jcz = 0.5f * (jlo.z + jhi.z) - ic[2];
+            const float d0 = fabsf(jcx - L[0] * rintf(jcx * iL[0])) - ie[0] - 0.5f * (jhi.x - jlo.x);
+            const float d1 = fabsf(jcy - L[1] * rintf(jcy * iL[1])) - ie[1] - 0.5f * (jhi.y - jlo.y);
+            const float d2 = fabsf(jcz - L[2] * rintf(jcz * iL[2])) - ie[2] - 0.5f * (jhi.z - jlo.z);
+            const float a0 = fmaxf(d0, 0.f), a1 = fmaxf(d1, 0.f), a2 = fmaxf(d2, 0.f);
+            pass = a0 * a0 + a1 * a1 + a2 * a2 < R2;
+        }
+        unsigned cand = __ballot_sync(0xffffffffu, pass);
+        if (pass) {
+#pragma unroll
+            for (int a = 0; a < CLUSTER; ++a) stage_x[wib][lane][a] = st.xyzq[jc_lane * CLUSTER + a];
+        }
+        b += 32;
+        if (b >= nj) {
+            b = 0;
+            ++k;
+            while (k < ncw) {
+                header(k, j0, nj);
+                if (nj > 0) break;
+                ++k;
+            }
+        }
+        if (k < ncw && b + lane < nj) {
+            jlo = st.bb_lo[j0 + b + lane];
+            jhi = st.bb_hi[j0 + b + lane];
+        }
+        __syncwarp();
+        while (cand) {
+            const int src = __ffs(cand) - 1;
+            cand &= cand - 1u;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const float4 xj = stage_x[wib][src][jq + 4 * h];
+                float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+                dx -= L[0] * rintf(dx * iL[0]);
+                dy -= L[1] * rintf(dy * iL[1]);
+                dz -= L[2] * rintf(dz * iL[2]);
+                const float r2 = dx * dx + dy * dy + dz * dz;
+                // padding slots carry q = 0, so the charge test drops them too
+                const bool hit = ivalid && r2 < cut2 && r2 > 0.f && xj.w != 0.f;
+                if (!__any_sync(0xffffffffu, hit)) continue;
+                if (hit) {
                     const float r = sqrtf(r2);
                     const float w0 = xj.w * (1.f / kE) * 0.5f * (__cosf(kPiF * r / DESC_CUT) + 1.f);
                     const float ir = 1.f / r;
@@ -126,17 +188,32 @@ __global__ void __launch_bounds__(128) k_descriptor(DevState st, const long long
                 }
             }
         }
+        __syncwarp();
     }
-    float* out = feat + (size_t)s * MLP_IN;
-    const float inv = (float)(1.0 / FORCE_SCALE);
-    out[0] = (float)fc[s] * inv;
-    out[1] = (float)fc[st.n_slots + s] * inv;
-    out[2] = (float)fc[2 * (size_t)st.n_slots + s] * inv;
-    out[3] = xi.w;
+    // sum the four lanes of each i-atom (fixed order), then lane jq writes channel jq
 #pragma unroll
     for (int c = 0; c < 4; ++c)
 #pragma unroll
-        for (int k = 0; k < DESC_RADIAL; ++k) out[4 + DESC_RADIAL * c + k] = acc[c][k];
+        for (int k = 0; k < DESC_RADIAL; ++k) {
+            float v = acc[c][k];
+            v += __shfl_xor_sync(0xffffffffu, v, 8);
+            v += __shfl_xor_sync(0xffffffffu, v, 16);
+            acc[c][k] = v;
+        }
+    if (!ivalid) return;
+    float* out = feat + (size_t)si * MLP_IN;
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+        if (c == jq)
+#pragma unroll
+            for (int k = 0; k < DESC_RADIAL; ++k) out[4 + DESC_RADIAL * c + k] = acc[c][k];
+    if (jq == 0) {
+        const float inv = (float)(1.0 / FORCE_SCALE);
+        out[0] = (float)fc[si] * inv;
+        out[1] = (float)fc[st.n_slots + si] * inv;
+        out[2] = (float)fc[2 * (size_t)st.n_slots + si] * inv;
+        out[3] = xi.w;
+    }
 }
 
 // normalised BF16 network input, rows padded from 68 to 80 columns with zeros
@@ -236,7 +313,7 @@ __global__ void k_rows_to_bf16(int n, const float* __restrict__ x, __nv_bfloat16
 }
 
 int launch_descriptor(const DevState& st, const long long* fc, float* feat, cudaStream_t s) {
-    k_descriptor<<<nblk(st.n_slots, 128), 128, 0, s>>>(st, fc, feat);
+    k_descriptor<<<nblk((long long)st.n_clusters * 32, DS_WARPS * 32), DS_WARPS * 32, 0, s>>>(st, fc, feat);
     return 1;
 }
 int launch_mlp_input(const DevState& st, const float* feat, const float* mean, const float* inv_std,

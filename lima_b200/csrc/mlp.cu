@@ -14,6 +14,8 @@
 // so training is deterministic.
 #include <cuda_bf16.h>
 
+#include <algorithm>
+
 #include "engine.h"
 #include "mlp.h"
 
@@ -221,6 +223,143 @@ __global__ void k_to_bf16(const float* __restrict__ w, int K, int N, __nv_bfloat
     if (WTb) WTb[(size_t)n * ldt + k] = b;
 }
 
+// ------------------------------------------------------- fused inference
+// One persistent kernel for the whole network: the BF16 weights (transposed,
+// rows padded by 8 elements so that ldmatrix rows fall on distinct banks) are
+// loaded into shared memory once per CTA; each warp then streams 16-row tiles:
+// normalise its 16 feature rows into shared memory, run the four layers with
+// ldmatrix + mma.sync (activations stay in the warp's own 16 rows of shared
+// memory), and write the 16 x 8 FP32 outputs.
+constexpr int INF_WARPS = 16;
+constexpr int LD1 = MLP_KIN + 8;     // 88
+constexpr int LDH = MLP_HID + 8;     // 136
+constexpr size_t INF_SMEM = sizeof(__nv_bfloat16) * ((size_t)128 * LD1 + 2 * (size_t)128 * LDH + 8 * (size_t)LDH +
+                                                     (size_t)INF_WARPS * 16 * LDH) +
+                            sizeof(float) * (3 * 128 + 8 + 2 * MLP_IN);
+
+__device__ __forceinline__ void ldsm_x4(uint32_t* r, const __nv_bfloat16* p) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(a));
+}
+
+// acc[16 x N] = A[16 x K] (rows of As, stride lda) * B, B given as BT[N][K] (stride ldb)
+template <int K, int N>
+__device__ __forceinline__ void warp_mma_tile(const __nv_bfloat16* As, int lda, const __nv_bfloat16* BT, int ldb,
+                                              float (*acc)[4]) {
+    const int lane = threadIdx.x & 31;
+    const int mi = lane >> 3, rr = lane & 7;
+#pragma unroll
+    for (int n = 0; n < N / 8; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.f;
+#pragma unroll
+    for (int k0 = 0; k0 < K; k0 += 16) {
+        uint32_t a[4];
+        ldsm_x4(a, As + (size_t)(rr + 8 * (mi & 1)) * lda + k0 + 8 * (mi >> 1));
+        if (N >= 16) {
+#pragma unroll
+            for (int n = 0; n < N / 8; n += 2) {
+                uint32_t b[4];
+                ldsm_x4(b, BT + (size_t)(8 * (n + (mi >> 1)) + rr) * ldb + k0 + 8 * (mi & 1));
+                mma16816(acc[n], a, b);
+                mma16816(acc[n + 1], a, b + 2);
+            }
+        } else {
+            // one n-tile: matrices (k0), (k0 + 8) of rows 0..7, loaded twice
+            uint32_t b[4];
+            ldsm_x4(b, BT + (size_t)rr * ldb + k0 + 8 * (mi & 1));
+            mma16816(acc[0], a, b);
+        }
+    }
+}
+
+// bias + SiLU of a 16 x 128 accumulator tile into the warp's rows (BF16)
+__device__ __forceinline__ void store_hidden(float (*acc)[4], const float* bias, __nv_bfloat16* H) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int n = 0; n < 16; ++n) {
+        const int c = 8 * n + 2 * t;
+        const float b0 = bias[c], b1 = bias[c + 1];
+        *reinterpret_cast<uint32_t*>(H + (size_t)g * LDH + c) =
+            pack2(__float2bfloat16(silu(acc[n][0] + b0)), __float2bfloat16(silu(acc[n][1] + b1)));
+        *reinterpret_cast<uint32_t*>(H + (size_t)(g + 8) * LDH + c) =
+            pack2(__float2bfloat16(silu(acc[n][2] + b0)), __float2bfloat16(silu(acc[n][3] + b1)));
+    }
+}
+
+__global__ void __launch_bounds__(INF_WARPS * 32, 1)
+    k_mlp_infer(int rows, const float* __restrict__ feat, const float* __restrict__ mean,
+                const float* __restrict__ inv_std, const __nv_bfloat16* __restrict__ wt0,
+                const __nv_bfloat16* __restrict__ wt1, const __nv_bfloat16* __restrict__ wt2,
+                const __nv_bfloat16* __restrict__ wt3, const float* __restrict__ b0, const float* __restrict__ b1,
+                const float* __restrict__ b2, const float* __restrict__ b3, float* __restrict__ Y) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __nv_bfloat16* W0 = reinterpret_cast<__nv_bfloat16*>(smem_raw);      // [128][LD1]
+    __nv_bfloat16* W1 = W0 + 128 * LD1;                                   // [128][LDH]
+    __nv_bfloat16* W2 = W1 + 128 * LDH;                                   // [128][LDH]
+    __nv_bfloat16* W3 = W2 + 128 * LDH;                                   // [8][LDH]
+    __nv_bfloat16* Hs = W3 + 8 * LDH;                                     // [warps][16][LDH]
+    float* bs = reinterpret_cast<float*>(Hs + INF_WARPS * 16 * LDH);      // 3 x 128 + 8
+    float* ms = bs + 3 * 128 + 8;                                         // mean, 1/std
+    const int tid = threadIdx.x;
+    for (int i = tid; i < 128 * MLP_KIN; i += blockDim.x) W0[(i / MLP_KIN) * LD1 + i % MLP_KIN] = wt0[i];
+    for (int i = tid; i < 128 * 128; i += blockDim.x) {
+        W1[(i >> 7) * LDH + (i & 127)] = wt1[i];
+        W2[(i >> 7) * LDH + (i & 127)] = wt2[i];
+    }
+    for (int i = tid; i < 8 * 128; i += blockDim.x) W3[(i >> 7) * LDH + (i & 127)] = wt3[i];
+    for (int i = tid; i < 128; i += blockDim.x) {
+        bs[i] = b0[i];
+        bs[128 + i] = b1[i];
+        bs[256 + i] = b2[i];
+    }
+    if (tid < 8) bs[384 + tid] = b3[tid];
+    for (int i = tid; i < MLP_IN; i += blockDim.x) {
+        ms[i] = mean[i];
+        ms[MLP_IN + i] = inv_std[i];
+    }
+    __syncthreads();
+    const int warp = tid >> 5, lane = tid & 31;
+    __nv_bfloat16* H = Hs + (size_t)warp * 16 * LDH;
+    const int n_tiles = (rows + 15) / 16;
+    float acc[16][4];
+    for (int tile = blockIdx.x * INF_WARPS + warp; tile < n_tiles; tile += gridDim.x * INF_WARPS) {
+        const int r0 = tile * 16;
+        // 16 contiguous feature rows, normalised, into columns 0..79 (68..79 zero)
+        for (int i = lane; i < 16 * MLP_KIN; i += 32) {
+            const int r = i / MLP_KIN, c = i - r * MLP_KIN;
+            float v = 0.f;
+            if (c < MLP_IN && r0 + r < rows) v = (feat[(size_t)(r0 + r) * MLP_IN + c] - ms[c]) * ms[MLP_IN + c];
+            H[r * LDH + c] = __float2bfloat16(v);
+        }
+        __syncwarp();
+        warp_mma_tile<MLP_KIN, 128>(H, LDH, W0, LD1, acc);
+        __syncwarp();
+        store_hidden(acc, bs, H);
+        __syncwarp();
+        warp_mma_tile<128, 128>(H, LDH, W1, LDH, acc);
+        __syncwarp();
+        store_hidden(acc, bs + 128, H);
+        __syncwarp();
+        warp_mma_tile<128, 128>(H, LDH, W2, LDH, acc);
+        __syncwarp();
+        store_hidden(acc, bs + 256, H);
+        __syncwarp();
+        warp_mma_tile<128, 8>(H, LDH, W3, LDH, acc);
+        const int g = lane >> 2, t = lane & 3;
+        const int c = 2 * t;
+        if (r0 + g < rows) {
+            Y[(size_t)(r0 + g) * 8 + c] = acc[0][0] + bs[384 + c];
+            Y[(size_t)(r0 + g) * 8 + c + 1] = acc[0][1] + bs[384 + c + 1];
+        }
+        if (r0 + g + 8 < rows) {
+            Y[(size_t)(r0 + g + 8) * 8 + c] = acc[0][2] + bs[384 + c];
+            Y[(size_t)(r0 + g + 8) * 8 + c + 1] = acc[0][3] + bs[384 + c + 1];
+        }
+        __syncwarp();
+    }
+}
+
 // ---------------------------------------------------------- model host side
 namespace {
 inline unsigned blocks(long long n, int tb) { return (unsigned)((n + tb - 1) / tb); }
@@ -233,6 +372,23 @@ void mlp_sync_bf16(MlpModel& m, cudaStream_t s) {
         const int ldw = l == 3 ? 16 : N;
         k_to_bf16<<<blocks((long long)K * N, 256), 256, 0, s>>>(m.w[l], K, N, m.wb[l], ldw, m.wtb[l], K);
     }
+}
+
+int mlp_infer(const MlpModel& m, int rows, const float* feat, const float* mean, const float* inv_std, float* Y,
+              cudaStream_t s) {
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)INF_SMEM);
+        attr_set = true;
+    }
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int tiles = (rows + 15) / 16;
+    const int grid = std::max(1, std::min(sms, (tiles + INF_WARPS - 1) / INF_WARPS));
+    k_mlp_infer<<<grid, INF_WARPS * 32, INF_SMEM, s>>>(rows, feat, mean, inv_std, m.wtb[0], m.wtb[1], m.wtb[2],
+                                                       m.wtb[3], m.b[0], m.b[1], m.b[2], m.b[3], Y);
+    return 1;
 }
 
 int mlp_forward(const MlpModel& m, int rows, const __nv_bfloat16* X, MlpActs* acts, float* Y, cudaStream_t s) {

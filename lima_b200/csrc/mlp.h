@@ -50,6 +50,9 @@ struct MlpActs {                  // training activations for one batch
 };
 
 void mlp_sync_bf16(MlpModel& m, cudaStream_t s);
+// inference of all four layers in one persistent kernel, inputs normalised on the fly
+int mlp_infer(const MlpModel& m, int rows, const float* feat, const float* mean, const float* inv_std, float* Y,
+              cudaStream_t s);
 int mlp_forward(const MlpModel& m, int rows, const __nv_bfloat16* X, MlpActs* acts, float* Y, cudaStream_t s);
 int mlp_train_step(MlpModel& m, int rows, const __nv_bfloat16* X, const float* T, MlpActs& a, float lr,
                    double* d_loss, cudaStream_t s);

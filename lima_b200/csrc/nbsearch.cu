@@ -256,9 +256,15 @@ __global__ void k_pairsearch(DevState st, float rlist) {
     int cx0 = (int)floorf((ilo.x - R) / sd.col_w[0]);
     int cx1 = (int)floorf((ihi.x + R) / sd.col_w[0]);
     int nx = cx1 - cx0 + 1;
+    // When the window does not cover a whole row of columns, each column in
+    // it is met once at a known unwrapped position, which fixes the x and y
+    // periodic shift of its clusters: only the three z shifts remain to test.
+    // Otherwise every one of the 27 shifts is tested.
+    bool fixed_xy = true;
     if (nx >= sd.ncol_x) {
         cx0 = 0;
         nx = sd.ncol_x;
+        fixed_xy = false;
     }
     int cy0 = (int)floorf((ilo.y - R) / sd.col_w[1]);
     int cy1 = (int)floorf((ihi.y + R) / sd.col_w[1]);
@@ -266,6 +272,7 @@ __global__ void k_pairsearch(DevState st, float rlist) {
     if (ny >= sd.ncol_y) {
         cy0 = 0;
         ny = sd.ncol_y;
+        fixed_xy = false;
     }
 
     const int cap = st.pl_cap;
@@ -273,8 +280,10 @@ __global__ void k_pairsearch(DevState st, float rlist) {
     const size_t base_out = (size_t)ci * cap;
     for (int iy = 0; iy < ny; ++iy) {
         const int cy = wrapi(cy0 + iy, sd.ncol_y);
+        const int sy_col = cy0 + iy < 0 ? -1 : (cy0 + iy >= sd.ncol_y ? 1 : 0);
         for (int ix = 0; ix < nx; ++ix) {
             const int cx = wrapi(cx0 + ix, sd.ncol_x);
+            const int sx_col = cx0 + ix < 0 ? -1 : (cx0 + ix >= sd.ncol_x ? 1 : 0);
             const int col = sd.col_off + cx + sd.ncol_x * cy;
             const int j0 = st.col_cl_start[col];
             const int nj = st.col_ncl[col];
@@ -285,21 +294,36 @@ __global__ void k_pairsearch(DevState st, float rlist) {
                     const float4 jlo = st.bb_lo[j], jhi = st.bb_hi[j];
                     const float jc[3] = {0.5f * (jlo.x + jhi.x), 0.5f * (jlo.y + jhi.y), 0.5f * (jlo.z + jhi.z)};
                     const float je[3] = {0.5f * (jhi.x - jlo.x), 0.5f * (jhi.y - jlo.y), 0.5f * (jhi.z - jlo.z)};
-                    float g2[3][3];
-                    for (int d = 0; d < 3; ++d) {
-                        for (int sh = -1; sh <= 1; ++sh) {
-                            const float dd = fabsf(jc[d] + sh * L[d] - ic[d]) - ie[d] - je[d];
-                            const float g = fmaxf(dd, 0.f);
-                            g2[d][sh + 1] = g * g;
-                        }
-                    }
-                    for (int sz = 0; sz < 3; ++sz)
-                        for (int sy = 0; sy < 3; ++sy)
-                            for (int sx = 0; sx < 3; ++sx) {
-                                const int code = sx + 3 * sy + 9 * sz;
+                    if (fixed_xy) {
+                        const float gx = fmaxf(fabsf(jc[0] + sx_col * L[0] - ic[0]) - ie[0] - je[0], 0.f);
+                        const float gy = fmaxf(fabsf(jc[1] + sy_col * L[1] - ic[1]) - ie[1] - je[1], 0.f);
+                        const float gxy = gx * gx + gy * gy;
+                        if (gxy < R2) {
+                            const int base = (sx_col + 1) + 3 * (sy_col + 1);
+                            for (int sz = -1; sz <= 1; ++sz) {
+                                const int code = base + 9 * (sz + 1);
                                 if (j == ci && code != 13) continue;
-                                if (g2[0][sx] + g2[1][sy] + g2[2][sz] < R2) shifts |= 1u << code;
+                                const float gz = fmaxf(fabsf(jc[2] + sz * L[2] - ic[2]) - ie[2] - je[2], 0.f);
+                                if (gxy + gz * gz < R2) shifts |= 1u << code;
                             }
+                        }
+                    } else {
+                        float g2[3][3];
+                        for (int d = 0; d < 3; ++d) {
+                            for (int sh = -1; sh <= 1; ++sh) {
+                                const float dd = fabsf(jc[d] + sh * L[d] - ic[d]) - ie[d] - je[d];
+                                const float g = fmaxf(dd, 0.f);
+                                g2[d][sh + 1] = g * g;
+                            }
+                        }
+                        for (int sz = 0; sz < 3; ++sz)
+                            for (int sy = 0; sy < 3; ++sy)
+                                for (int sx = 0; sx < 3; ++sx) {
+                                    const int code = sx + 3 * sy + 9 * sz;
+                                    if (j == ci && code != 13) continue;
+                                    if (g2[0][sx] + g2[1][sy] + g2[2][sz] < R2) shifts |= 1u << code;
+                                }
+                    }
                 }
                 unsigned pending = __ballot_sync(0xffffffffu, shifts != 0u);
                 while (pending) {
