@@ -104,6 +104,19 @@ typedef struct lima_params {
                                  or improper is excluded from LJ and Coulomb
                                  (code/LIMA_TOOLS/src/CompoundBuilder.cpp:40-60)      */
     int    use_graphs;        /* 1 = replay each nstlist block of steps as a CUDA graph */
+    /* thermostat (code/LIMA_ENGINE/src/Thermostat.cuh:55-103, Engine.cu:167-174): every
+       thermostat_interval steps the temperature of each system is measured from its
+       kinetic energy (3N - 3 degrees of freedom); with apply_thermostat the integrator's
+       velocity scale becomes clamp(target/T, 1 -+ 0.001/thermostat_interval) */
+    int    apply_thermostat;  /* 0 = measure only                                      */
+    int    thermostat_interval; /* steps between measurements; 0 = never (default 200) */
+    double target_temperature; /* [K] (the reference's fixed 310 K)                    */
+    /* per-particle logging (EngineUtils.cuh:143-158, Engine.cu:203-240): every
+       log_interval steps (0 = off) the position, potential energy, force and speed of
+       every atom go to a device ring of log_ring frames, offloaded to host memory
+       whenever it fills; read with lima_get_log */
+    int    log_interval;
+    int    log_ring;          /* frames held on the device (default 5, as the reference) */
 } lima_params;
 
 typedef struct lima_energies {
@@ -279,6 +292,21 @@ LIMA_API int lima_learned_pme_weights(lima_engine* h, int get, float* buf, int64
  * squared error.  For checking the training kernels. */
 LIMA_API int lima_learned_pme_gradients(lima_engine* h, int rows, const float* x, const float* t,
                                         float* grads, double* loss);
+
+/* ---------------------------------------------------------- thermostat, log */
+/* Last temperature measurement of the selected system: temperature [K], the
+ * velocity scale in use, and the step it was taken at (-1 before the first). */
+LIMA_API int lima_get_thermostat(lima_engine* h, double* temperature, double* scale, int64_t* step);
+/* Logged frames of the selected system, oldest first, starting at frame
+ * `first`; at most max_frames are written.  Per frame: steps[f]; pos_epot[f][n][4]
+ * = x, y, z [nm], potential energy [J/mol] (half of each pair energy, an equal
+ * share of each bonded term, 1/2 q phi plus the self term); force_speed[f][n][4]
+ * = force [J/mol/nm], |v| [nm/ns].  Output arrays may be NULL.  *n_frames
+ * receives the number of frames logged so far. */
+LIMA_API int lima_get_log(lima_engine* h, int64_t first, int64_t max_frames, int64_t* steps, float* pos_epot,
+                          float* force_speed, int64_t* n_frames);
+/* Drops every logged frame held on the host. */
+LIMA_API int lima_clear_log(lima_engine* h);
 
 #ifdef __cplusplus
 }

@@ -111,6 +111,17 @@ struct lima_engine {
     float* d_out_f = nullptr;
     float* d_maxf = nullptr;
 
+    // thermostat (per system) and per-particle log
+    long long* d_therm_ke = nullptr;   // [n_sys][E_COUNT]
+    std::vector<double> therm_T, therm_scale;
+    int64_t therm_step = -1;
+    float4* log_pe = nullptr;          // device ring [log_ring][n_atoms]
+    float4* log_fs = nullptr;
+    int log_fill = 0;
+    std::vector<int64_t> log_ring_steps;
+    std::vector<float4> log_host_pe, log_host_fs;   // offloaded frames [frame][n_atoms]
+    std::vector<int64_t> log_host_steps;
+
     // learned coarse-grid PME correction (mlp.cu, learned.cu)
     std::vector<SysDesc> sd_host;     // per-system descriptors of the engine's own grid
     bool lp_ready = false;            // buffers and model allocated
@@ -189,6 +200,8 @@ struct lima_engine {
         d_idx_cap = 0;
         mlp = MlpModel{};
         acts = MlpActs{};
+        log_fill = 0;
+        log_ring_steps.clear();
     }
 
     void setup();
@@ -221,6 +234,9 @@ struct lima_engine {
     void learned_full(cudaStream_t s, bool energy);
     void learned_pme_stage(bool energy, cudaStream_t s);
     void ensure_list();
+    void measure_temperature();
+    void log_frame();
+    void flush_log();
 };
 
 namespace {
@@ -293,6 +309,10 @@ void lima_engine::setup() {
     CK(cudaGetDeviceProperties(&prop, p.device));
     if (prop.major < 10) throw ApiError{LIMA_ERR_NO_DEVICE, "this build targets sm_100a (B200)"};
     release();
+    // frames logged under an earlier topology no longer match the atoms
+    log_host_pe.clear();
+    log_host_fs.clear();
+    log_host_steps.clear();
 
     // ---- derived parameters
     const double rc = p.cutoff;
@@ -393,6 +413,9 @@ void lima_engine::setup() {
             self_energy[s] = p.ref_compat ? 0.5 * nq * self_total : self_total;
             D.self_energy = self_energy[s];
             D.n_charged = nq;
+            // per-atom shares of the self term (per-particle log)
+            D.self_per_charge = p.ref_compat ? 1 : 0;
+            D.self_coef = p.ref_compat ? (float)(0.5 * self_total) : (float)(-kappa / std::sqrt(pic) * kCoulomb);
         }
     }
     if (col_cap > 8192) throw ApiError{LIMA_ERR_UNSUPPORTED, "column capacity too large (very tall box)"};
@@ -569,6 +592,19 @@ void lima_engine::setup() {
     D.pl_mask = dalloc<unsigned long long>((size_t)n_clusters * pl_cap);
     D.status = dalloc<unsigned>(1);
     D.energy = dalloc<long long>((size_t)ns * E_COUNT);
+    D.epot = dalloc<long long>(S);
+    D.vscale = upload(std::vector<float>(ns, (float)p.thermostat_scalar));
+    d_therm_ke = dalloc<long long>((size_t)ns * E_COUNT);
+    therm_T.assign(ns, 0.0);
+    therm_scale.assign(ns, p.thermostat_scalar);
+    therm_step = -1;
+    if (p.log_interval > 0) {
+        const int ring = p.log_ring > 0 ? p.log_ring : 5;
+        log_pe = dalloc<float4>((size_t)ring * N);
+        log_fs = dalloc<float4>((size_t)ring * N);
+        log_fill = 0;
+        log_ring_steps.clear();
+    }
 
     // ---- PME plan, grids and influence function
     pp = PmePlan{};
@@ -605,7 +641,6 @@ void lima_engine::setup() {
     nb.two_kappa_sqrtpi = (float)(2.0 * kappa / std::sqrt(p.ref_compat ? kPiRef : kPi));
     nb.em = 0;
     ip.dt = p.dt;
-    ip.scale = (float)p.thermostat_scalar;
     ip.integrator = p.integrator;
 
     d_out_d = dalloc<double>(3 * (size_t)N);
@@ -962,7 +997,10 @@ void lima_engine::capture_period() {
 
 void lima_engine::forces(bool energy) {
     ensure_list();
-    if (energy) CK(cudaMemsetAsync(st.energy, 0, sizeof(long long) * E_COUNT * st.n_sys, s_main));
+    if (energy) {
+        CK(cudaMemsetAsync(st.energy, 0, sizeof(long long) * E_COUNT * st.n_sys, s_main));
+        CK(cudaMemsetAsync(st.epot, 0, sizeof(long long) * st.n_slots, s_main));
+    }
     launch_zero_forces(st, s_main);
     // with phase timing on, every phase runs on the main stream so that each
     // phase's events bracket that phase alone
@@ -994,7 +1032,7 @@ void lima_engine::forces(bool energy) {
 void lima_engine::run_steps(int n) {
     CK(cudaEventRecord(ev_t0, s_main));
     int k = 0;
-    if (p.use_graphs && !phase_timing && !state_pending && !learned_active()) {
+    if (p.use_graphs && !phase_timing && !state_pending && !learned_active() && p.log_interval <= 0) {
         // whole pair-list periods replay as one graph; the last step stays eager
         // so that it can evaluate energies
         while (n - k > p.nstlist && list_age >= p.nstlist) {
@@ -1006,18 +1044,25 @@ void lima_engine::run_steps(int n) {
             ++graph_replays;
             list_age = p.nstlist;
             k += p.nstlist;
+            const int64_t before = step;
             step += p.nstlist;
+            // a thermostat measurement due inside the replayed period is taken after it
+            if (p.thermostat_interval > 0 && step / p.thermostat_interval != before / p.thermostat_interval)
+                measure_temperature();
         }
     }
     for (; k < n; ++k) {
-        const bool energy = k == n - 1;
+        const bool log_now = p.log_interval > 0 && step % p.log_interval == 0;
+        const bool energy = k == n - 1 || log_now;
         forces(energy);
+        if (log_now) log_frame();
         mark(4, 0, s_main);
         launches += launch_integrate(st, ip, energy, s_main);
         mark(4, 1, s_main);
         collect_phases();
         ++list_age;
         ++step;
+        if (p.thermostat_interval > 0 && step % p.thermostat_interval == 0) measure_temperature();
         if (lp_check_pending) {
             // full-grid check of the learned correction: fall back to plain
             // PME once the relative reciprocal-force RMSE exceeds the bound
@@ -1039,6 +1084,61 @@ void lima_engine::run_steps(int n) {
     time_ms += ms;
     timed_steps += n;
     energy_valid = true;
+}
+
+// Temperature of every system from its kinetic energy (3N - 3 degrees of
+// freedom, code/LIMA_BASE/include/PhysicsUtils.cuh:32-34) and, with
+// apply_thermostat, the new velocity scale clamp(target/T, 1 -+ 0.001/interval)
+// (_Thermostat::ComputeThermostatScalar, Thermostat.cuh:55-67; a zero
+// temperature counts as 1 K there).
+void lima_engine::measure_temperature() {
+    const int ns = st.n_sys;
+    CK(cudaMemsetAsync(d_therm_ke, 0, sizeof(long long) * E_COUNT * ns, s_main));
+    launches += launch_kinetic(st, d_therm_ke, s_main);
+    std::vector<long long> ke((size_t)ns * E_COUNT);
+    CK(cudaMemcpyAsync(ke.data(), d_therm_ke, ke.size() * sizeof(long long), cudaMemcpyDeviceToHost, s_main));
+    CK(cudaStreamSynchronize(s_main));
+    const double kb_na = 1.380649e-23 * 6.02214076e23;
+    const double max_step = 0.001 / (double)p.thermostat_interval;
+    std::vector<float> scale(ns);
+    for (int s = 0; s < ns; ++s) {
+        const double K = (double)ke[(size_t)s * E_COUNT + E_KINETIC] / ENERGY_SCALE;
+        const double dof = 3.0 * sys[s].n - 3.0;
+        const double T = dof > 0.0 ? K * 2.0 / dof / kb_na : 0.0;
+        therm_T[s] = T;
+        const double Tsafe = T == 0.0 ? 1.0 : T;
+        const double target = p.target_temperature > 0.0 ? p.target_temperature : 310.0;
+        const double sc = std::min(std::max(target / Tsafe, 1.0 - max_step), 1.0 + max_step);
+        if (p.apply_thermostat) therm_scale[s] = sc;
+        scale[s] = (float)therm_scale[s];
+    }
+    therm_step = step;
+    if (p.apply_thermostat)
+        CK(cudaMemcpyAsync(st.vscale, scale.data(), ns * sizeof(float), cudaMemcpyHostToDevice, s_main));
+    CK(cudaStreamSynchronize(s_main));
+}
+
+// one frame into the device ring; a full ring goes to host memory
+void lima_engine::log_frame() {
+    const int ring = p.log_ring > 0 ? p.log_ring : 5;
+    const size_t N = st.n_atoms;
+    launches += launch_log_frame(st, log_pe + (size_t)log_fill * N, log_fs + (size_t)log_fill * N, s_main);
+    log_ring_steps.push_back(step);
+    if (++log_fill == ring) flush_log();
+}
+
+void lima_engine::flush_log() {
+    if (log_fill == 0) return;
+    const size_t N = st.n_atoms, n = (size_t)log_fill * N;
+    const size_t old = log_host_pe.size();
+    log_host_pe.resize(old + n);
+    log_host_fs.resize(old + n);
+    CK(cudaMemcpyAsync(log_host_pe.data() + old, log_pe, n * sizeof(float4), cudaMemcpyDeviceToHost, s_main));
+    CK(cudaMemcpyAsync(log_host_fs.data() + old, log_fs, n * sizeof(float4), cudaMemcpyDeviceToHost, s_main));
+    CK(cudaStreamSynchronize(s_main));
+    log_host_steps.insert(log_host_steps.end(), log_ring_steps.begin(), log_ring_steps.end());
+    log_ring_steps.clear();
+    log_fill = 0;
 }
 
 void lima_engine::read_energies(lima_energies* e) {
@@ -1083,6 +1183,11 @@ void lima_default_params(lima_params* p) {
     p->thermostat_scalar = 1.0;
     p->exclude_bonded = 1;
     p->use_graphs = 0;
+    p->apply_thermostat = 0;
+    p->thermostat_interval = 200;   // SimParams::steps_per_temperature_measurement
+    p->target_temperature = 310.0;  // Thermostat.cuh:56
+    p->log_interval = 0;
+    p->log_ring = 5;                // DatabuffersDeviceController::nStepsInBuffer
 }
 
 const char* lima_error_string(int code) {
@@ -1674,6 +1779,52 @@ int lima_learned_pme_gradients(lima_engine* h, int rows, const float* x, const f
         if (loss) *loss = sum / (3.0 * rows);
         return LIMA_OK;
     });
+}
+
+// ------------------------------------------------------------ thermostat, log
+int lima_get_thermostat(lima_engine* h, double* temperature, double* scale, int64_t* step) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    const bool have = h->built && h->cur < (int)h->therm_T.size();
+    if (temperature) *temperature = have ? h->therm_T[h->cur] : 0.0;
+    if (scale) *scale = have ? h->therm_scale[h->cur] : h->p.thermostat_scalar;
+    if (step) *step = have ? h->therm_step : -1;
+    return LIMA_OK;
+}
+
+int lima_get_log(lima_engine* h, int64_t first, int64_t max_frames, int64_t* steps, float* pos_epot,
+                 float* force_speed, int64_t* n_frames) {
+    if (!h || first < 0 || max_frames < 0) return LIMA_ERR_INVALID_ARG;
+    return guarded(h, [&]() {
+        if (h->built) h->flush_log();
+        const int64_t total = (int64_t)h->log_host_steps.size();
+        if (n_frames) *n_frames = total;
+        const size_t N = h->built ? (size_t)h->st.n_atoms : 0;
+        const int off = h->n_atoms_off.empty() ? 0 : h->n_atoms_off[h->cur];
+        const int n = h->sys[h->cur].n;
+        for (int64_t f = 0; f < max_frames && first + f < total; ++f) {
+            const size_t fr = (size_t)(first + f);
+            if (steps) steps[f] = h->log_host_steps[fr];
+            for (int a = 0; a < n; ++a) {
+                const float4 pe = h->log_host_pe[fr * N + off + a];
+                const float4 fs = h->log_host_fs[fr * N + off + a];
+                const size_t o = ((size_t)f * n + a) * 4;
+                if (pos_epot) pos_epot[o] = pe.x, pos_epot[o + 1] = pe.y, pos_epot[o + 2] = pe.z, pos_epot[o + 3] = pe.w;
+                if (force_speed)
+                    force_speed[o] = fs.x, force_speed[o + 1] = fs.y, force_speed[o + 2] = fs.z, force_speed[o + 3] = fs.w;
+            }
+        }
+        return LIMA_OK;
+    });
+}
+
+int lima_clear_log(lima_engine* h) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    h->log_host_pe.clear();
+    h->log_host_fs.clear();
+    h->log_host_steps.clear();
+    h->log_host_pe.shrink_to_fit();
+    h->log_host_fs.shrink_to_fit();
+    return LIMA_OK;
 }
 
 }  // extern "C"

@@ -50,6 +50,8 @@ struct SysDesc {
     float pme_inv_h[3];             // K_d / L_d
     double self_energy;             // Ewald self term [J/mol]
     int n_charged;
+    float self_coef;                // per-atom self energy: self_coef * q^2, or self_coef per
+    int self_per_charge;            //   charged atom when self_per_charge (reference convention)
     int pad_;
 };
 
@@ -105,6 +107,14 @@ __device__ __forceinline__ void add_energy_fixed(long long* energy, int sysi, do
         atomicAdd(reinterpret_cast<unsigned long long*>(energy + (size_t)sysi * E_COUNT + term),
                   static_cast<unsigned long long>(v));
     }
+}
+
+// adds an atom's share of a potential energy [J/mol] to its per-slot accumulator
+// (fixed point, ENERGY_SCALE per J/mol; each share is rounded before the add,
+// so the per-atom sums do not depend on the order of the adds)
+__device__ __forceinline__ void add_atom_energy(long long* epot, int slot, double e) {
+    atomicAdd(reinterpret_cast<unsigned long long*>(epot + slot),
+              static_cast<unsigned long long>(__double2ll_rn(e * ENERGY_SCALE)));
 }
 
 // shift code (sx+1) + 3(sy+1) + 9(sz+1), s in {-1,0,1}

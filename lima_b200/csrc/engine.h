@@ -80,6 +80,8 @@ struct DevState {
 
     unsigned* status = nullptr;
     long long* energy = nullptr;         // [n_sys][E_COUNT]
+    long long* epot = nullptr;           // per-slot potential energy (energy steps), fixed point
+    float* vscale = nullptr;             // per-system velocity scale of the integrator (thermostat)
 };
 
 struct BondedTerms {
@@ -136,8 +138,7 @@ int launch_pme(const DevState& st, const PmePlan& plan, bool energy, cudaStream_
 // integrate.cu
 struct IntegrateParams {
     double dt;
-    float scale;            // thermostat velocity scale
-    int integrator;         // 0 leapfrog, 1 velocity Verlet
+    int integrator;         // 0 leapfrog, 1 velocity Verlet (velocity scale: DevState::vscale)
 };
 int launch_integrate(const DevState& st, const IntegrateParams& p, bool energy, cudaStream_t s);
 int launch_em_step(const DevState& st, int step, float* max_force_out_dev, cudaStream_t s);
@@ -145,5 +146,9 @@ int launch_gather_state(const DevState& st, double* pos_out, float* vel_out, cud
 int launch_gather_forces(const DevState& st, double* f_out, cudaStream_t s);
 int launch_zero_forces(const DevState& st, cudaStream_t s);
 int launch_max_force(const DevState& st, float* out, cudaStream_t s);
+// per-system kinetic energy (E_KINETIC of ke[n_sys][E_COUNT], fixed point)
+int launch_kinetic(const DevState& st, long long* ke, cudaStream_t s);
+// one log frame in original atom order: (x, y, z, potential energy), (F, |v|)
+int launch_log_frame(const DevState& st, float4* pos_epot, float4* force_speed, cudaStream_t s);
 
 }  // namespace lima

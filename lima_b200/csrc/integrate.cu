@@ -29,6 +29,7 @@ __global__ void k_integrate(DevState st, IntegrateParams p) {
     int sysi = -1;
     if (s < st.n_slots && st.orig[s] >= 0) {
         sysi = st.cluster_sys[s / CLUSTER];
+        const float scale = st.vscale[sysi];
         const float3 F = load_force(st, s);
         float4 v = st.vel[s];
         const float im = v.w;
@@ -37,9 +38,9 @@ __global__ void k_integrate(DevState st, IntegrateParams p) {
         double dx, dy, dz;
         if (INTEGRATOR == 0) {
             const float m = im > 0.f ? 1.f / im : 0.f;
-            const float vx = (v.x + F.x * im * dt) * p.scale;
-            const float vy = (v.y + F.y * im * dt) * p.scale;
-            const float vz = (v.z + F.z * im * dt) * p.scale;
+            const float vx = (v.x + F.x * im * dt) * scale;
+            const float vy = (v.y + F.y * im * dt) * scale;
+            const float vz = (v.z + F.z * im * dt) * scale;
             if (ENERGY) {
                 // average of the two half-step kinetic energies
                 ke = 0.25 * (double)m * ((double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z +
@@ -66,9 +67,9 @@ __global__ void k_integrate(DevState st, IntegrateParams p) {
             dy = (double)vy * p.dt + (double)(F.y * a);
             dz = (double)vz * p.dt + (double)(F.z * a);
             st.fprev[s] = make_float4(F.x, F.y, F.z, 0.f);
-            v.x = vx * p.scale;
-            v.y = vy * p.scale;
-            v.z = vz * p.scale;
+            v.x = vx * scale;
+            v.y = vy * scale;
+            v.z = vz * scale;
         }
         st.vel[s] = v;
         const double x = st.px[s] + dx, y = st.py[s] + dy, z = st.pz[s] + dz;
@@ -166,6 +167,47 @@ __global__ void k_gather_state(DevState st, double* pos, float* vel) {
         vel[3 * a + 1] = v.y;
         vel[3 * a + 2] = v.z;
     }
+}
+
+// kinetic energy per system from the stored velocities (thermostat measurement)
+__global__ void k_kinetic(DevState st, long long* ke) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    double e = 0.0;
+    int sysi = -1;
+    if (s < st.n_slots && st.orig[s] >= 0) {
+        sysi = st.cluster_sys[s / CLUSTER];
+        const float4 v = st.vel[s];
+        const double m = v.w > 0.f ? 1.0 / (double)v.w : 0.0;
+        e = 0.5 * m * ((double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z);
+    }
+    add_energy_fixed(ke, sysi, e, E_KINETIC);
+}
+
+int launch_kinetic(const DevState& st, long long* ke, cudaStream_t s) {
+    const int TB = 256;
+    k_kinetic<<<(st.n_slots + TB - 1) / TB, TB, 0, s>>>(st, ke);
+    return 1;
+}
+
+// Per-particle log entry (the reference's potE / traj / vel / force buffers,
+// EngineUtils.cuh:143-158): position, potential energy of this step's force
+// evaluation, force and speed of the stored velocity, in original atom order.
+__global__ void k_log_frame(DevState st, float4* pos_epot, float4* force_speed) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= st.n_slots) return;
+    const int a = st.orig[s];
+    if (a < 0) return;
+    const float4 v = st.vel[s];
+    const float3 F = load_force(st, s);
+    pos_epot[a] = make_float4((float)st.px[s], (float)st.py[s], (float)st.pz[s],
+                              (float)((double)st.epot[s] * (1.0 / ENERGY_SCALE)));
+    force_speed[a] = make_float4(F.x, F.y, F.z, sqrtf(v.x * v.x + v.y * v.y + v.z * v.z));
+}
+
+int launch_log_frame(const DevState& st, float4* pos_epot, float4* force_speed, cudaStream_t s) {
+    const int TB = 256;
+    k_log_frame<<<(st.n_slots + TB - 1) / TB, TB, 0, s>>>(st, pos_epot, force_speed);
+    return 1;
 }
 
 int launch_gather_state(const DevState& st, double* pos_out, float* vel_out, cudaStream_t s) {

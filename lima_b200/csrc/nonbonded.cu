@@ -35,7 +35,7 @@ struct PairAcc {
 // scalar fs with F_i = fs * (r_j - r_i); 0 outside the cutoff.
 template <int ES, bool ENERGY>
 __device__ __forceinline__ float pair_scalar(const NbParams& p, float r2, float2 lji, float2 ljj, float qq,
-                                             PairAcc& acc) {
+                                             PairAcc& acc, float& epair) {
     const float rinv = rsqrtf(r2);
     const float rinv2 = rinv * rinv;
     const float sig = lji.x + ljj.x;
@@ -43,7 +43,10 @@ __device__ __forceinline__ float pair_scalar(const NbParams& p, float r2, float2
     float s6 = sig * sig * rinv2;
     s6 = s6 * s6 * s6;
     float fs = 24.f * eps * s6 * rinv2 * (1.f - 2.f * s6);
-    if (ENERGY) acc.e_lj += (double)(4.f * eps * s6 * (s6 - 1.f));
+    if (ENERGY) {
+        epair = 4.f * eps * s6 * (s6 - 1.f);
+        acc.e_lj += (double)epair;
+    }
     if (ES != 0) {
         float fc, ec;
         if (ES == 2) {
@@ -60,7 +63,10 @@ __device__ __forceinline__ float pair_scalar(const NbParams& p, float r2, float2
             ec = qq * rinv;
         }
         fs -= fc;
-        if (ENERGY) acc.e_c += (double)ec;
+        if (ENERGY) {
+            acc.e_c += (double)ec;
+            epair += ec;
+        }
     }
     if (p.em) fs = fmaxf(fminf(fs, 1e20f), -1e20f);
     if (ENERGY) acc.vir += 0.5 * (double)(fs * r2);  // -1/2 r_ij . f_ij
@@ -93,8 +99,9 @@ __global__ void __launch_bounds__(256) k_nonbonded(DevState st, NbParams p) {
     }
     __syncwarp();
     float fi[CLUSTER][3];
+    float ei[CLUSTER];     // energy steps: half of each pair energy per i-atom
 #pragma unroll
-    for (int a = 0; a < CLUSTER; ++a) fi[a][0] = fi[a][1] = fi[a][2] = 0.f;
+    for (int a = 0; a < CLUSTER; ++a) fi[a][0] = fi[a][1] = fi[a][2] = ei[a] = 0.f;
     PairAcc acc{0.0, 0.0, 0.0};
     const int jj = lane & 7;
     const size_t base = (size_t)ci * st.pl_cap;
@@ -117,7 +124,7 @@ __global__ void __launch_bounds__(256) k_nonbonded(DevState st, NbParams p) {
             xj.y += sh.y * Ly;
             xj.z += sh.z * Lz;
         }
-        float fjx = 0.f, fjy = 0.f, fjz = 0.f;
+        float fjx = 0.f, fjy = 0.f, fjz = 0.f, ej = 0.f;
 #pragma unroll
         for (int ii = 0; ii < CLUSTER; ++ii) {
             if ((bits >> ii) & 1u) {
@@ -125,7 +132,12 @@ __global__ void __launch_bounds__(256) k_nonbonded(DevState st, NbParams p) {
                 const float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
                 const float r2 = dx * dx + dy * dy + dz * dz;
                 if (r2 <= p.rc2) {
-                    const float fs = pair_scalar<ES, ENERGY>(p, r2, s_lj[wib][ii], ljj, xi.w * xj.w, acc);
+                    float epair = 0.f;
+                    const float fs = pair_scalar<ES, ENERGY>(p, r2, s_lj[wib][ii], ljj, xi.w * xj.w, acc, epair);
+                    if (ENERGY) {
+                        ei[ii] += 0.5f * epair;
+                        ej += 0.5f * epair;
+                    }
                     const float fx = fs * dx, fy = fs * dy, fz = fs * dz;
                     fi[ii][0] += fx;
                     fi[ii][1] += fy;
@@ -140,6 +152,7 @@ __global__ void __launch_bounds__(256) k_nonbonded(DevState st, NbParams p) {
             atomic_add_fixed(st.fx + sj, to_fixed(fjx, FORCE_SCALE));
             atomic_add_fixed(st.fy + sj, to_fixed(fjy, FORCE_SCALE));
             atomic_add_fixed(st.fz + sj, to_fixed(fjz, FORCE_SCALE));
+            if (ENERGY) add_atom_energy(st.epot, sj, (double)ej);
         }
     }
     // i-forces: sum each of the 24 values over the warp; lane a (< 8) adds atom a's
@@ -153,15 +166,25 @@ __global__ void __launch_bounds__(256) k_nonbonded(DevState st, NbParams p) {
             fi[a][c] = v;
         }
     }
+    if (ENERGY) {
+#pragma unroll
+        for (int a = 0; a < CLUSTER; ++a) {
+            float v = ei[a];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            ei[a] = v;
+        }
+    }
     if (lane < CLUSTER) {
-        float vx = 0.f, vy = 0.f, vz = 0.f;
+        float vx = 0.f, vy = 0.f, vz = 0.f, ve = 0.f;
 #pragma unroll
         for (int a = 0; a < CLUSTER; ++a)
-            if (a == lane) vx = fi[a][0], vy = fi[a][1], vz = fi[a][2];
+            if (a == lane) vx = fi[a][0], vy = fi[a][1], vz = fi[a][2], ve = ei[a];
         const int si = ci * CLUSTER + lane;
         atomic_add_fixed(st.fx + si, to_fixed(vx, FORCE_SCALE));
         atomic_add_fixed(st.fy + si, to_fixed(vy, FORCE_SCALE));
         atomic_add_fixed(st.fz + si, to_fixed(vz, FORCE_SCALE));
+        if (ENERGY) add_atom_energy(st.epot, si, (double)ve);
     }
     if (ENERGY) {
         add_energy_fixed(st.energy, sysi, acc.e_lj, E_LJ);
@@ -219,7 +242,11 @@ __global__ void k_exclusion_correction(DevState st, BondedTerms bt, NbParams p) 
         atomic_add_fixed(st.fx + sj, to_fixed(-fx, FORCE_SCALE));
         atomic_add_fixed(st.fy + sj, to_fixed(-fy, FORCE_SCALE));
         atomic_add_fixed(st.fz + sj, to_fixed(-fz, FORCE_SCALE));
-        if (ENERGY) e = -(double)qq * (double)erf_kr * (double)rinv;
+        if (ENERGY) {
+            e = -(double)qq * (double)erf_kr * (double)rinv;
+            add_atom_energy(st.epot, si, 0.5 * e);
+            add_atom_energy(st.epot, sj, 0.5 * e);
+        }
     }
     if (ENERGY) add_energy_fixed(st.energy, sysi, e, E_EXCL);
 }

@@ -435,7 +435,13 @@ __global__ void k_gather(DevState st) {
         atomic_add_fixed(st.fx + s, to_fixed(-q * gx * sc0, FORCE_SCALE));
         atomic_add_fixed(st.fy + s, to_fixed(-q * gy * sc1, FORCE_SCALE));
         atomic_add_fixed(st.fz + s, to_fixed(-q * gz * sc2, FORCE_SCALE));
-        if (ENERGY) e = 0.5 * (double)q * (double)phi;
+        if (ENERGY) {
+            e = 0.5 * (double)q * (double)phi;
+            // the atom's reciprocal energy and its share of the Ewald self term
+            const SysDesc& sd = st.sys[sysi];
+            const double self = sd.self_per_charge ? (double)sd.self_coef : (double)sd.self_coef * q * q;
+            add_atom_energy(st.epot, s, e + self);
+        }
     }
     if (ENERGY) add_energy_fixed(st.energy, c == 0 ? sysi : -1, e, E_RECIP);
 }

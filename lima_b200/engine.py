@@ -38,7 +38,7 @@ EXPORTED = [
     "lima_get_timings", "lima_reset_timings", "lima_enable_phase_timing", "lima_pme_recip_noalloc",
     "lima_learned_pme_setup", "lima_learned_pme_collect", "lima_learned_pme_train", "lima_learned_pme_enable",
     "lima_learned_pme_eval", "lima_learned_pme_status", "lima_learned_pme_weights",
-    "lima_learned_pme_gradients",
+    "lima_learned_pme_gradients", "lima_get_thermostat", "lima_get_log", "lima_clear_log",
 ]
 MLP_NPARAM = 80 * 128 + 128 + 2 * (128 * 128 + 128) + 128 * 8 + 8   # network parameters
 MLP_NSTATE = MLP_NPARAM + 2 * 68 + 1                               # + normalisation and output scale
@@ -57,7 +57,9 @@ class Params(ctypes.Structure):
                 ("ewald_kappa", ctypes.c_double), ("ewald_tol", ctypes.c_double),
                 ("ref_compat", ctypes.c_int), ("integrator", ctypes.c_int),
                 ("thermostat_scalar", ctypes.c_double), ("exclude_bonded", ctypes.c_int),
-                ("use_graphs", ctypes.c_int)]
+                ("use_graphs", ctypes.c_int), ("apply_thermostat", ctypes.c_int),
+                ("thermostat_interval", ctypes.c_int), ("target_temperature", ctypes.c_double),
+                ("log_interval", ctypes.c_int), ("log_ring", ctypes.c_int)]
 
 
 class Energies(ctypes.Structure):
@@ -125,6 +127,10 @@ def load_library(path: str = LIB_PATH):
                                                   ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                   ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p,
                                                   ctypes.c_void_p]),
+        "lima_get_thermostat": (ctypes.c_int, [h, f64p, f64p, P(ctypes.c_int64)]),
+        "lima_get_log": (ctypes.c_int, [h, ctypes.c_int64, ctypes.c_int64, P(ctypes.c_int64), f32p, f32p,
+                                        P(ctypes.c_int64)]),
+        "lima_clear_log": (ctypes.c_int, [h]),
         "lima_learned_pme_setup": (ctypes.c_int, [h, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
         "lima_learned_pme_collect": (ctypes.c_int, [h]),
         "lima_learned_pme_train": (ctypes.c_int, [h, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_uint64,
@@ -335,6 +341,30 @@ class Engine:
 
     def phase_timing(self, enable: bool):
         self._check(self.lib.lima_enable_phase_timing(self.h, 1 if enable else 0))
+
+    def thermostat(self) -> dict:
+        """Last temperature measurement of the selected system."""
+        t, sc, st = ctypes.c_double(0.0), ctypes.c_double(0.0), ctypes.c_int64(0)
+        self._check(self.lib.lima_get_thermostat(self.h, ctypes.byref(t), ctypes.byref(sc), ctypes.byref(st)))
+        return {"temperature": t.value, "scale": sc.value, "step": st.value}
+
+    def log(self, first: int = 0, max_frames: int | None = None):
+        """Logged frames of the selected system: (steps, pos_epot (f,n,4), force_speed (f,n,4))."""
+        total = ctypes.c_int64(0)
+        self._check(self.lib.lima_get_log(self.h, 0, 0, None, None, None, ctypes.byref(total)))
+        nf = max(0, total.value - first)
+        if max_frames is not None:
+            nf = min(nf, max_frames)
+        n = self.natoms[self._sel]
+        steps = np.zeros(max(nf, 1), np.int64)
+        pe = np.zeros((max(nf, 1), n, 4), np.float32)
+        fs = np.zeros((max(nf, 1), n, 4), np.float32)
+        self._check(self.lib.lima_get_log(self.h, first, nf, steps.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                          _f32(pe)[1], _f32(fs)[1], ctypes.byref(total)))
+        return steps[:nf], pe[:nf], fs[:nf]
+
+    def clear_log(self):
+        self._check(self.lib.lima_clear_log(self.h))
 
 
 class LearnedPME:

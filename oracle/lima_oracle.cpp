@@ -169,7 +169,7 @@ template <typename T>
 int64_t nonbonded_impl(int n, const double* pos, const double* box, const double* q,
                        const double* sigma, const double* eps, const int* eo, const int* ei,
                        double rc, int es_mode, double kappa, int nthreads, double* forces,
-                       double* energies) {
+                       double* energies, double* atom_energy = nullptr) {
     CellGrid grid;
     grid.build(n, pos, box, rc);
     const T rcT = (T)rc;
@@ -220,6 +220,7 @@ int64_t nonbonded_impl(int n, const double* pos, const double* box, const double
         forces[3 * i] += (double)fi.x;
         forces[3 * i + 1] += (double)fi.y;
         forces[3 * i + 2] += (double)fi.z;
+        if (atom_energy) atom_energy[i] += el + ec;  // half of every pair energy of atom i
         e_lj += el;
         e_coul += ec;
         vir += vr;
@@ -467,6 +468,14 @@ int64_t orc_nonbonded(int n, const double* pos, const double* box, const double*
                                   kappa, nthreads, forces, energies);
 }
 
+int64_t orc_nonbonded_atoms(int n, const double* pos, const double* box, const double* q,
+                            const double* sigma, const double* eps, const int* excl_off,
+                            const int* excl_idx, double rc, int es_mode, double kappa, int nthreads,
+                            double* forces, double* energies, double* atom_energy) {
+    return nonbonded_impl<double>(n, pos, box, q, sigma, eps, excl_off, excl_idx, rc, es_mode,
+                                  kappa, nthreads, forces, energies, atom_energy);
+}
+
 int64_t orc_pairset(int n, const double* pos, const double* box, const int* excl_off,
                     const int* excl_idx, double rc, double band, int64_t cap, int32_t* pairs,
                     uint8_t* band_flag, int64_t* n_band) {
@@ -506,11 +515,16 @@ int64_t orc_pairset(int n, const double* pos, const double* box, const int* excl
     return total;
 }
 
-void orc_bonded(int n, const double* pos, const double* box, int nb, const int* bidx,
-                const double* bpar, int na, const int* aidx, const double* apar, int nd,
-                const int* didx, const double* dpar, int ni, const int* iidx, const double* ipar,
-                int np, const int* pidx, const double* ppar, double* forces, double* energies) {
-    (void)n;
+static void bonded_impl(const double* pos, const double* box, int nb, const int* bidx,
+                        const double* bpar, int na, const int* aidx, const double* apar, int nd,
+                        const int* didx, const double* dpar, int ni, const int* iidx, const double* ipar,
+                        int np, const int* pidx, const double* ppar, double* forces, double* energies,
+                        double* atom_energy) {
+    // a term's energy is shared equally by its atoms in atom_energy
+    auto share = [&](const int* idx, int k, double e) {
+        if (atom_energy)
+            for (int a = 0; a < k; ++a) atom_energy[idx[a]] += e / k;
+    };
     // positions of a term's atoms unwrapped by the minimum image relative to its first atom
     auto gather = [&](const int* idx, int k, D3* p) {
         p[0] = load(pos, idx[0]);
@@ -523,31 +537,55 @@ void orc_bonded(int n, const double* pos, const double* box, int nb, const int* 
         bond_term(p[0], p[1], bpar[2 * t], bpar[2 * t + 1], f, &e);
         for (int a = 0; a < 2; ++a) addf(forces, bidx[2 * t + a], f[a]);
         energies[0] += e;
+        share(bidx + 2 * t, 2, e);
     }
     for (int t = 0; t < na; ++t) {
         gather(aidx + 3 * t, 3, p);
         angle_term(p[0], p[1], p[2], apar + 4 * t, f, &e);
         for (int a = 0; a < 3; ++a) addf(forces, aidx[3 * t + a], f[a]);
         energies[1] += e;
+        share(aidx + 3 * t, 3, e);
     }
     for (int t = 0; t < nd; ++t) {
         gather(didx + 4 * t, 4, p);
         dihedral_term(p[0], p[1], p[2], p[3], dpar + 3 * t, f, &e);
         for (int a = 0; a < 4; ++a) addf(forces, didx[4 * t + a], f[a]);
         energies[2] += e;
+        share(didx + 4 * t, 4, e);
     }
     for (int t = 0; t < ni; ++t) {
         gather(iidx + 4 * t, 4, p);
         improper_term(p[0], p[1], p[2], p[3], ipar + 2 * t, f, &e);
         for (int a = 0; a < 4; ++a) addf(forces, iidx[4 * t + a], f[a]);
         energies[3] += e;
+        share(iidx + 4 * t, 4, e);
     }
     for (int t = 0; t < np; ++t) {
         gather(pidx + 2 * t, 2, p);
         pairbond_term(p[0], p[1], ppar[2 * t], ppar[2 * t + 1], f, &e);
         for (int a = 0; a < 2; ++a) addf(forces, pidx[2 * t + a], f[a]);
         energies[4] += e;
+        share(pidx + 2 * t, 2, e);
     }
+}
+
+void orc_bonded(int n, const double* pos, const double* box, int nb, const int* bidx,
+                const double* bpar, int na, const int* aidx, const double* apar, int nd,
+                const int* didx, const double* dpar, int ni, const int* iidx, const double* ipar,
+                int np, const int* pidx, const double* ppar, double* forces, double* energies) {
+    (void)n;
+    bonded_impl(pos, box, nb, bidx, bpar, na, aidx, apar, nd, didx, dpar, ni, iidx, ipar, np, pidx, ppar,
+                forces, energies, nullptr);
+}
+
+void orc_bonded_atoms(int n, const double* pos, const double* box, int nb, const int* bidx,
+                      const double* bpar, int na, const int* aidx, const double* apar, int nd,
+                      const int* didx, const double* dpar, int ni, const int* iidx, const double* ipar,
+                      int np, const int* pidx, const double* ppar, double* forces, double* energies,
+                      double* atom_energy) {
+    (void)n;
+    bonded_impl(pos, box, nb, bidx, bpar, na, aidx, apar, nd, didx, dpar, ni, iidx, ipar, np, pidx, ppar,
+                forces, energies, atom_energy);
 }
 
 void orc_pme(int n, const double* pos, const double* q, const double* box, int kx, int ky, int kz,
@@ -681,6 +719,12 @@ void orc_ewald_recip(int n, const double* pos, const double* q, const double* bo
 void orc_exclusion_correction(int n, const double* pos, const double* q, const double* box,
                               int npairs, const int* pairs, double kappa, double* forces,
                               double* energy) {
+    orc_exclusion_correction_atoms(n, pos, q, box, npairs, pairs, kappa, forces, energy, nullptr);
+}
+
+void orc_exclusion_correction_atoms(int n, const double* pos, const double* q, const double* box,
+                                    int npairs, const int* pairs, double kappa, double* forces,
+                                    double* energy, double* atom_energy) {
     (void)n;
     double e = 0.0;
     for (int t = 0; t < npairs; ++t) {
@@ -690,6 +734,10 @@ void orc_exclusion_correction(int n, const double* pos, const double* q, const d
         const double qq = q[i] * q[j] * kCoulomb;
         const double er = std::erf(kappa * r);
         e += -qq * er / r;
+        if (atom_energy) {
+            atom_energy[i] += -0.5 * qq * er / r;
+            atom_energy[j] += -0.5 * qq * er / r;
+        }
         // F_i = -dE/dr_i = qq * d/dr(erf(kr)/r) * d/r ... with E = -qq erf(kr)/r
         const double dedr = -qq * (2.0 * kappa / std::sqrt(kPi) * std::exp(-kappa * kappa * r * r) / r - er / (r * r));
         const D3 fi = d * (-dedr / r);

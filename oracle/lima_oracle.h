@@ -45,6 +45,15 @@ int64_t orc_nonbonded(int n, const double* pos, const double* box,
                       double rc, int es_mode, double kappa, int precision, int nthreads,
                       double* forces, double* energies);
 
+/* orc_nonbonded in FP64 that also adds, per atom, half of the energy of each of
+ * its pairs (LJ + Coulomb) to atom_energy[n]: the per-particle potential
+ * energy the reference logs (LennardJonesInteractions.cuh:101, factor 0.5). */
+int64_t orc_nonbonded_atoms(int n, const double* pos, const double* box,
+                            const double* q, const double* sigma, const double* eps,
+                            const int* excl_off, const int* excl_idx,
+                            double rc, int es_mode, double kappa, int nthreads,
+                            double* forces, double* energies, double* atom_energy);
+
 /* Sorted list of pairs (i<j) with r <= rc that are not excluded.  Pairs with
  * |r - rc| < band are counted in *n_band and flagged in band_flag (may be
  * NULL).  Returns the pair count (writes at most cap pairs). */
@@ -68,6 +77,16 @@ void orc_bonded(int n, const double* pos, const double* box,
                 int ni, const int* iidx, const double* ipar,
                 int np, const int* pidx, const double* ppar,
                 double* forces, double* energies);
+
+/* orc_bonded that also shares each term's energy equally among its atoms in
+ * atom_energy[n]. */
+void orc_bonded_atoms(int n, const double* pos, const double* box,
+                      int nb, const int* bidx, const double* bpar,
+                      int na, const int* aidx, const double* apar,
+                      int nd, const int* didx, const double* dpar,
+                      int ni, const int* iidx, const double* ipar,
+                      int np, const int* pidx, const double* ppar,
+                      double* forces, double* energies, double* atom_energy);
 
 /* Smooth PME reciprocal part on a Kx x Ky x Kz grid, order 4, weights placed
  * at floor(u)-1 .. floor(u)+2 as in PME.cuh:249-300 and 335-383.
@@ -94,6 +113,12 @@ void orc_ewald_recip(int n, const double* pos, const double* q, const double* bo
 void orc_exclusion_correction(int n, const double* pos, const double* q, const double* box,
                               int npairs, const int* pairs, double kappa,
                               double* forces, double* energy);
+
+/* orc_exclusion_correction that also gives half of each pair's energy to
+ * each of its atoms in atom_energy[n] (may be NULL). */
+void orc_exclusion_correction_atoms(int n, const double* pos, const double* q, const double* box,
+                                    int npairs, const int* pairs, double kappa,
+                                    double* forces, double* energy, double* atom_energy);
 
 /* One integration step. integrator 0: leapfrog (v(t+dt/2) = v(t-dt/2) + F dt/m;
  * x += v dt); 1: the reference's velocity Verlet (EngineUtils.cuh:31-41,

@@ -62,6 +62,14 @@ def lib():
         L.orc_em_step.argtypes = [ctypes.c_int, _d, _d, _d, ctypes.c_int]
         L.orc_fft3d.restype = None
         L.orc_fft3d.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _d, ctypes.c_int]
+        L.orc_nonbonded_atoms.restype = ctypes.c_int64
+        L.orc_nonbonded_atoms.argtypes = [ctypes.c_int, _d, _d, _d, _d, _d, _i, _i, ctypes.c_double,
+                                          ctypes.c_int, ctypes.c_double, ctypes.c_int, _d, _d, _d]
+        L.orc_bonded_atoms.restype = None
+        L.orc_bonded_atoms.argtypes = [ctypes.c_int, _d, _d] + [ctypes.c_int, _i, _d] * 5 + [_d, _d, _d]
+        L.orc_exclusion_correction_atoms.restype = None
+        L.orc_exclusion_correction_atoms.argtypes = [ctypes.c_int, _d, _d, _d, ctypes.c_int, _i,
+                                                     ctypes.c_double, _d, _d, _d]
         L.orc_mlp_grads.restype = ctypes.c_double
         L.orc_mlp_grads.argtypes = [ctypes.c_int, _d, _d, _d, _d]
         _lib = L
@@ -231,3 +239,37 @@ def mlp_grads(x, t, params):
     g = np.zeros(MLP_NPARAM)
     loss = lib().orc_mlp_grads(len(x), _dp(x), _dp(t), _dp(params), _dp(g))
     return loss, g
+
+
+def atom_energies(s, rc, kappa, grid):
+    """Per-atom potential energies in FP64 for the accurate Ewald/PME setup: half
+    of each pair energy, equal shares of bonded terms, 1/2 q phi + the self term
+    -kappa/sqrt(pi) k_e q^2, and half of each exclusion-correction pair."""
+    pos = _f64(s.pos).reshape(-1, 3)
+    n = len(pos)
+    box = _f64(s.box)
+    ex = s.exclusions()
+    off, idx = exclusion_csr(n, ex)
+    ae = np.zeros(n)
+    f = np.zeros((n, 3))
+    e = np.zeros(3)
+    lib().orc_nonbonded_atoms(n, _dp(pos), _dp(box), _dp(_f64(s.charge)), _dp(_f64(s.sigma)),
+                              _dp(_f64(s.epsilon)), _ip(off), _ip(idx), rc, 2, kappa, 0, _dp(f), _dp(e), _dp(ae))
+    call, keep = [], []
+    for ii, pp, k, pn in ((s.bonds, s.bond_par, 2, 2), (s.angles, s.angle_par, 3, 4),
+                          (s.dihedrals, s.dihedral_par, 4, 3), (s.impropers, s.improper_par, 4, 2),
+                          (s.pairbonds, s.pair_par, 2, 2)):
+        m, a, b = _terms(ii, pp, k, pn)
+        keep.append((a, b))
+        call += [m, None if a is None else a.ctypes.data_as(_i), _dp(b)]
+    eb = np.zeros(5)
+    lib().orc_bonded_atoms(n, _dp(pos), _dp(box), *call, _dp(f), _dp(eb), _dp(ae))
+    q = _f64(s.charge)
+    _, _, _, phi = pme(pos, q, box, grid, kappa, influence=0, gather=0, want_potential=True)
+    ae += 0.5 * q * phi - kappa / np.sqrt(np.pi) * coulomb_constant() * q * q
+    xp = ex[(q[ex[:, 0]] != 0) & (q[ex[:, 1]] != 0)] if len(ex) else ex
+    xp = np.ascontiguousarray(xp, dtype=np.int32).reshape(-1, 2)
+    ee = ctypes.c_double(0.0)
+    lib().orc_exclusion_correction_atoms(n, _dp(pos), _dp(q), _dp(box), len(xp), xp.ctypes.data_as(_i), kappa,
+                                         _dp(f), ctypes.byref(ee), _dp(ae))
+    return ae
