@@ -27,61 +27,64 @@ constexpr float AS_P = 0.3275911f;
 constexpr float AS_A1 = 0.254829592f, AS_A2 = -0.284496736f, AS_A3 = 1.421413741f;
 constexpr float AS_A4 = -1.453152027f, AS_A5 = 1.061405429f;
 
-struct PairAcc {
-    double e_lj, e_c, vir;
+// ---------------------------------------------------------------- packed FP32
+// Blackwell's packed FP32 instructions ({add,sub,mul,fma}.rn.f32x2, sm_100):
+// one instruction computes two lanes of a float pair held in a 64-bit register,
+// each rounded exactly like its scalar counterpart.
+struct f2p {
+    unsigned long long v;
 };
-
-// One atom pair: i-atom (xi, lji, qi) and the lane's j-atom (xj, ljj).  Returns the
-// scalar fs with F_i = fs * (r_j - r_i); 0 outside the cutoff.
-template <int ES, bool ENERGY>
-__device__ __forceinline__ float pair_scalar(const NbParams& p, float r2, float2 lji, float2 ljj, float qq,
-                                             PairAcc& acc, float& epair) {
-    const float rinv = rsqrtf(r2);
-    const float rinv2 = rinv * rinv;
-    const float sig = lji.x + ljj.x;
-    const float eps = lji.y * ljj.y;
-    float s6 = sig * sig * rinv2;
-    s6 = s6 * s6 * s6;
-    float fs = 24.f * eps * s6 * rinv2 * (1.f - 2.f * s6);
-    if (ENERGY) {
-        epair = 4.f * eps * s6 * (s6 - 1.f);
-        acc.e_lj += (double)epair;
-    }
-    if (ES != 0) {
-        float fc, ec;
-        if (ES == 2) {
-            const float r = r2 * rinv;
-            const float x = p.kappa * r;
-            const float t = __fdividef(1.f, fmaf(AS_P, x, 1.f));
-            const float poly = t * fmaf(t, fmaf(t, fmaf(t, fmaf(t, AS_A5, AS_A4), AS_A3), AS_A2), AS_A1);
-            const float ex = __expf(-x * x);
-            const float erfc_x = poly * ex;
-            fc = qq * rinv2 * rinv * fmaf(p.two_kappa_sqrtpi * r, ex, erfc_x);
-            ec = qq * rinv * erfc_x;
-        } else {
-            fc = qq * rinv2 * rinv;
-            ec = qq * rinv;
-        }
-        fs -= fc;
-        if (ENERGY) {
-            acc.e_c += (double)ec;
-            epair += ec;
-        }
-    }
-    if (p.em) fs = fmaxf(fminf(fs, 1e20f), -1e20f);
-    if (ENERGY) acc.vir += 0.5 * (double)(fs * r2);  // -1/2 r_ij . f_ij
-    return fs;
+__device__ __forceinline__ f2p pk2(float a, float b) {
+    f2p r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ float2 up2(f2p a) {
+    float2 r;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(a.v));
+    return r;
+}
+__device__ __forceinline__ f2p splat2(float a) { return pk2(a, a); }
+__device__ __forceinline__ f2p add2(f2p a, f2p b) {
+    f2p d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d.v) : "l"(a.v), "l"(b.v));
+    return d;
+}
+__device__ __forceinline__ f2p sub2(f2p a, f2p b) {
+    f2p d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d.v) : "l"(a.v), "l"(b.v));
+    return d;
+}
+__device__ __forceinline__ f2p mul2(f2p a, f2p b) {
+    f2p d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d.v) : "l"(a.v), "l"(b.v));
+    return d;
+}
+__device__ __forceinline__ f2p fma2(f2p a, f2p b, f2p c) {
+    f2p d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d.v) : "l"(a.v), "l"(b.v), "l"(c.v));
+    return d;
+}
+// 2^x, the hardware approximation (PTX ex2.approx.ftz.f32)
+__device__ __forceinline__ float ex2_approx(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
 }
 
 // Work mapping: one warp per i-cluster; the warp takes its list four entries at
 // a time and each lane owns one j-atom (entry k0 + lane/8, j-atom lane%8).  A
-// lane walks the 8 i-atoms (read from shared memory as broadcasts), keeps its
-// j-atom's force in registers and adds it once per entry; the i-forces live in
-// 24 registers per lane and are reduced across the warp once, after the list.
+// lane walks the 8 i-atoms two at a time, (ip, ip + 4) for ip = 0..3, in packed
+// FP32 (read as float4 pairs from shared memory), keeps its j-atom's force in a
+// packed register and adds it once per entry; the i-forces live in 12 packed
+// registers per lane and are reduced across the warp once, after the list.
+// Pair arithmetic per lane and the order of every sum are fixed, so results
+// are bit-reproducible.
 template <int ES, bool ENERGY>
-__global__ void __launch_bounds__(256) k_nonbonded(DevState st, NbParams p) {
-    __shared__ float4 s_xi[8][CLUSTER];
-    __shared__ float2 s_lj[8][CLUSTER];
+__global__ void __launch_bounds__(256, ENERGY ? 2 : 3) k_nonbonded(DevState st, NbParams p) {
+    // per warp, i-atom pairs (ip, ip + 4): (x0, x1, y0, y1), (z0, z1, q0 ke, q1 ke),
+    // (sigma0/2, sigma1/2, 24 sqrt(eps0), 24 sqrt(eps1))
+    __shared__ float4 s_xy[8][4], s_zq[8][4], s_lj[8][4];
     const int wib = threadIdx.x >> 5;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -92,17 +95,28 @@ __global__ void __launch_bounds__(256) k_nonbonded(DevState st, NbParams p) {
     const int sysi = st.cluster_sys[ci];
     const float Lx = st.sys[sysi].boxf[0], Ly = st.sys[sysi].boxf[1], Lz = st.sys[sysi].boxf[2];
     if (lane < CLUSTER) {
-        float4 x = st.xyzq[ci * CLUSTER + lane];
-        x.w *= p.ke;  // i-charges carry the Coulomb constant
-        s_xi[wib][lane] = x;
-        s_lj[wib][lane] = st.ljp[ci * CLUSTER + lane];
+        const float4 x = st.xyzq[ci * CLUSTER + lane];
+        const float2 lj = st.ljp[ci * CLUSTER + lane];
+        const int ip = lane & 3, h = lane >> 2;
+        float* xy = reinterpret_cast<float*>(&s_xy[wib][ip]);
+        float* zq = reinterpret_cast<float*>(&s_zq[wib][ip]);
+        float* lv = reinterpret_cast<float*>(&s_lj[wib][ip]);
+        xy[h] = x.x;
+        xy[2 + h] = x.y;
+        zq[h] = x.z;
+        zq[2 + h] = x.w * p.ke;   // i-charges carry the Coulomb constant
+        lv[h] = lj.x;
+        lv[2 + h] = 24.f * lj.y;  // the LJ force prefactor folded into the i side
     }
     __syncwarp();
-    float fi[CLUSTER][3];
-    float ei[CLUSTER];     // energy steps: half of each pair energy per i-atom
+    f2p fix[4], fiy[4], fiz[4], ei[4];
+    const f2p zero2 = splat2(0.f);
 #pragma unroll
-    for (int a = 0; a < CLUSTER; ++a) fi[a][0] = fi[a][1] = fi[a][2] = ei[a] = 0.f;
-    PairAcc acc{0.0, 0.0, 0.0};
+    for (int ip = 0; ip < 4; ++ip) fix[ip] = fiy[ip] = fiz[ip] = ei[ip] = zero2;
+    const f2p one2 = splat2(1.f), mtwo2 = splat2(-2.f);
+    // energy steps: per-lane packed FP32 sums of LJ, Coulomb and virial
+    // (a few tens of pairs each), converted to FP64 once per cluster
+    f2p s_elj = zero2, s_ec = zero2, s_vir = zero2;
     const int jj = lane & 7;
     const size_t base = (size_t)ci * st.pl_cap;
     for (int k0 = 0; k0 < n; k0 += 4) {
@@ -124,38 +138,97 @@ __global__ void __launch_bounds__(256) k_nonbonded(DevState st, NbParams p) {
             xj.y += sh.y * Ly;
             xj.z += sh.z * Lz;
         }
-        float fjx = 0.f, fjy = 0.f, fjz = 0.f, ej = 0.f;
+        f2p fjx = zero2, fjy = zero2, fjz = zero2, ej = zero2;
 #pragma unroll
-        for (int ii = 0; ii < CLUSTER; ++ii) {
-            if ((bits >> ii) & 1u) {
-                const float4 xi = s_xi[wib][ii];
-                const float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
-                const float r2 = dx * dx + dy * dy + dz * dz;
-                if (r2 <= p.rc2) {
-                    float epair = 0.f;
-                    const float fs = pair_scalar<ES, ENERGY>(p, r2, s_lj[wib][ii], ljj, xi.w * xj.w, acc, epair);
-                    if (ENERGY) {
-                        ei[ii] += 0.5f * epair;
-                        ej += 0.5f * epair;
-                    }
-                    const float fx = fs * dx, fy = fs * dy, fz = fs * dz;
-                    fi[ii][0] += fx;
-                    fi[ii][1] += fy;
-                    fi[ii][2] += fz;
-                    fjx -= fx;
-                    fjy -= fy;
-                    fjz -= fz;
+        for (int ip = 0; ip < 4; ++ip) {
+            const bool b0 = (bits >> ip) & 1u, b1 = (bits >> (ip + 4)) & 1u;
+            if (!(b0 || b1)) continue;
+            const float4 vxy = s_xy[wib][ip], vzq = s_zq[wib][ip];
+            const f2p dx = sub2(splat2(xj.x), pk2(vxy.x, vxy.y));
+            const f2p dy = sub2(splat2(xj.y), pk2(vxy.z, vxy.w));
+            const f2p dz = sub2(splat2(xj.z), pk2(vzq.x, vzq.y));
+            const float2 r2v = up2(fma2(dx, dx, fma2(dy, dy, mul2(dz, dz))));
+            const bool oka = b0 && r2v.x <= p.rc2, okb = b1 && r2v.y <= p.rc2;
+            if (!(oka || okb)) continue;
+            // an element outside the cutoff is evaluated at r = 1 and masked out below
+            const float r2a = oka ? r2v.x : 1.f, r2b = okb ? r2v.y : 1.f;
+            const f2p r2 = pk2(r2a, r2b);
+            const f2p rinv = pk2(rsqrtf(r2a), rsqrtf(r2b));
+            const f2p rinv2 = mul2(rinv, rinv);
+            const float4 vlj = s_lj[wib][ip];
+            const f2p sig = add2(pk2(vlj.x, vlj.y), splat2(ljj.x));
+            const f2p eps24 = mul2(pk2(vlj.z, vlj.w), splat2(ljj.y));
+            const f2p s2 = mul2(mul2(sig, sig), rinv2);
+            const f2p s6 = mul2(mul2(s2, s2), s2);
+            // LJ: 24 eps s6 (1 - 2 s6) / r^2
+            f2p fs = mul2(mul2(eps24, s6), mul2(rinv2, fma2(s6, mtwo2, one2)));
+            f2p ec = zero2;
+            if (ES != 0) {
+                const f2p qq = mul2(pk2(vzq.z, vzq.w), splat2(xj.w));
+                if (ES == 2) {
+                    const f2p r = mul2(r2, rinv);
+                    const f2p x = mul2(splat2(p.kappa), r);
+                    const float2 den = up2(fma2(splat2(AS_P), x, one2));
+                    const f2p t = pk2(__fdividef(1.f, den.x), __fdividef(1.f, den.y));
+                    const f2p poly = mul2(t, fma2(t, fma2(t, fma2(t, fma2(t, splat2(AS_A5), splat2(AS_A4)),
+                                                                splat2(AS_A3)), splat2(AS_A2)), splat2(AS_A1)));
+                    // exp(-x^2) = 2^(-x^2 log2 e)
+                    const float2 xs = up2(mul2(mul2(x, x), splat2(-1.4426950408889634f)));
+                    const f2p ex = pk2(ex2_approx(xs.x), ex2_approx(xs.y));
+                    const f2p erfc_x = mul2(poly, ex);
+                    const f2p qr3 = mul2(qq, mul2(rinv2, rinv));
+                    fs = sub2(fs, mul2(qr3, fma2(mul2(splat2(p.two_kappa_sqrtpi), r), ex, erfc_x)));
+                    if (ENERGY) ec = mul2(qq, mul2(rinv, erfc_x));
+                } else {
+                    fs = sub2(fs, mul2(qq, mul2(rinv2, rinv)));
+                    if (ENERGY) ec = mul2(qq, rinv);
                 }
+            }
+            float2 fsv = up2(fs);
+            if (p.em) {
+                fsv.x = fmaxf(fminf(fsv.x, 1e20f), -1e20f);
+                fsv.y = fmaxf(fminf(fsv.y, 1e20f), -1e20f);
+            }
+            fs = pk2(oka ? fsv.x : 0.f, okb ? fsv.y : 0.f);
+            const f2p fx = mul2(fs, dx), fy = mul2(fs, dy), fz = mul2(fs, dz);
+            fix[ip] = add2(fix[ip], fx);
+            fiy[ip] = add2(fiy[ip], fy);
+            fiz[ip] = add2(fiz[ip], fz);
+            fjx = sub2(fjx, fx);
+            fjy = sub2(fjy, fy);
+            fjz = sub2(fjz, fz);
+            if (ENERGY) {
+                // 4 eps s6 (s6 - 1) = (24 eps / 6) s6 (s6 - 1); masked like the force
+                const f2p m = pk2(oka ? 1.f : 0.f, okb ? 1.f : 0.f);
+                const f2p elj = mul2(m, mul2(mul2(eps24, splat2(1.f / 6.f)), mul2(s6, sub2(s6, one2))));
+                const f2p ecm = mul2(m, ec);
+                s_elj = add2(s_elj, elj);
+                s_ec = add2(s_ec, ecm);
+                s_vir = fma2(fs, r2, s_vir);   // fs is already masked; -1/2 r_ij . f_ij = fs r^2 / 2
+                const f2p eh = mul2(splat2(0.5f), add2(elj, ecm));
+                ei[ip] = add2(ei[ip], eh);
+                ej = add2(ej, eh);
             }
         }
         if (bits) {
-            atomic_add_fixed(st.fx + sj, to_fixed(fjx, FORCE_SCALE));
-            atomic_add_fixed(st.fy + sj, to_fixed(fjy, FORCE_SCALE));
-            atomic_add_fixed(st.fz + sj, to_fixed(fjz, FORCE_SCALE));
-            if (ENERGY) add_atom_energy(st.epot, sj, (double)ej);
+            const float2 x = up2(fjx), y = up2(fjy), z = up2(fjz);
+            atomic_add_fixed(st.fx + sj, to_fixed(x.x + x.y, FORCE_SCALE));
+            atomic_add_fixed(st.fy + sj, to_fixed(y.x + y.y, FORCE_SCALE));
+            atomic_add_fixed(st.fz + sj, to_fixed(z.x + z.y, FORCE_SCALE));
+            if (ENERGY) {
+                const float2 e = up2(ej);
+                add_atom_energy(st.epot, sj, (double)(e.x + e.y));
+            }
         }
     }
     // i-forces: sum each of the 24 values over the warp; lane a (< 8) adds atom a's
+    float fi[CLUSTER][3], eiv[CLUSTER];
+#pragma unroll
+    for (int ip = 0; ip < 4; ++ip) {
+        const float2 x = up2(fix[ip]), y = up2(fiy[ip]), z = up2(fiz[ip]), e = up2(ei[ip]);
+        fi[ip][0] = x.x, fi[ip][1] = y.x, fi[ip][2] = z.x, eiv[ip] = e.x;
+        fi[ip + 4][0] = x.y, fi[ip + 4][1] = y.y, fi[ip + 4][2] = z.y, eiv[ip + 4] = e.y;
+    }
 #pragma unroll
     for (int a = 0; a < CLUSTER; ++a) {
 #pragma unroll
@@ -165,21 +238,18 @@ __global__ void __launch_bounds__(256) k_nonbonded(DevState st, NbParams p) {
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
             fi[a][c] = v;
         }
-    }
-    if (ENERGY) {
-#pragma unroll
-        for (int a = 0; a < CLUSTER; ++a) {
-            float v = ei[a];
+        if (ENERGY) {
+            float v = eiv[a];
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            ei[a] = v;
+            eiv[a] = v;
         }
     }
     if (lane < CLUSTER) {
         float vx = 0.f, vy = 0.f, vz = 0.f, ve = 0.f;
 #pragma unroll
         for (int a = 0; a < CLUSTER; ++a)
-            if (a == lane) vx = fi[a][0], vy = fi[a][1], vz = fi[a][2], ve = ei[a];
+            if (a == lane) vx = fi[a][0], vy = fi[a][1], vz = fi[a][2], ve = eiv[a];
         const int si = ci * CLUSTER + lane;
         atomic_add_fixed(st.fx + si, to_fixed(vx, FORCE_SCALE));
         atomic_add_fixed(st.fy + si, to_fixed(vy, FORCE_SCALE));
@@ -187,9 +257,10 @@ __global__ void __launch_bounds__(256) k_nonbonded(DevState st, NbParams p) {
         if (ENERGY) add_atom_energy(st.epot, si, (double)ve);
     }
     if (ENERGY) {
-        add_energy_fixed(st.energy, sysi, acc.e_lj, E_LJ);
-        add_energy_fixed(st.energy, sysi, acc.e_c, E_COUL);
-        add_energy_fixed(st.energy, sysi, acc.vir, E_VIRIAL);
+        const float2 el = up2(s_elj), ecs = up2(s_ec), vr = up2(s_vir);
+        add_energy_fixed(st.energy, sysi, (double)el.x + (double)el.y, E_LJ);
+        add_energy_fixed(st.energy, sysi, (double)ecs.x + (double)ecs.y, E_COUL);
+        add_energy_fixed(st.energy, sysi, 0.5 * ((double)vr.x + (double)vr.y), E_VIRIAL);
     }
 }
 

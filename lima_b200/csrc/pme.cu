@@ -87,25 +87,32 @@ __device__ __forceinline__ void small_dft(float2* v, float sigma) {
     }
 }
 
+// floor(a / b) for 0 <= a < 2^20, b >= 1, with inv_b = 1.0f / b: (a + 1/2) / b sits at
+// least 1/(2b) from an integer and the two roundings of the product err by less
+// than 2^-23 (a + 1/2) / b < 1/(8b), so the truncation is exact
+__device__ __forceinline__ int div_small(int a, float inv_b) { return (int)(((float)a + 0.5f) * inv_b); }
+
 template <int R>
 __device__ __forceinline__ void stockham_stage(const float2* src, float2* dst, int nlines, int stride,
                                                int N, int Ns, const float2* tw, float sigma) {
     const int nb = N / R;
     const int total = nlines * nb;
     const int tscale = N / (Ns * R);
+    const float inv_nb = 1.f / (float)nb, inv_ns = 1.f / (float)Ns;
     for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-        const int line = idx / nb;
+        const int line = div_small(idx, inv_nb);
         const int j = idx - line * nb;
         const float2* in = src + line * stride;
         float2* out = dst + line * stride;
-        const int jm = j % Ns;
+        const int jm = j - Ns * div_small(j, inv_ns);
         float2 v[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) v[r] = in[j + r * nb];
+        // jm < Ns, so tstep * r <= (N/R)(R-1) < N: the twiddle index needs no wrap
         const int tstep = jm * tscale;
 #pragma unroll
         for (int r = 1; r < R; ++r) {
-            float2 w = tw[(tstep * r) % N];
+            float2 w = tw[tstep * r];
             w.y *= -sigma;  // table holds e^{-2 pi i k/N}; conjugate for the inverse
             v[r] = cmul(v[r], w);
         }
