@@ -139,32 +139,34 @@ __global__ void __launch_bounds__(256, ENERGY ? 2 : 3) k_nonbonded(DevState st, 
             xj.z += sh.z * Lz;
         }
         f2p fjx = zero2, fjy = zero2, fjz = zero2, ej = zero2;
+        const f2p jx = splat2(xj.x), jy = splat2(xj.y), jz = splat2(xj.z);
+        const f2p jsig = splat2(ljj.x), jeps = splat2(ljj.y), jq = splat2(xj.w);
 #pragma unroll
         for (int ip = 0; ip < 4; ++ip) {
-            const bool b0 = (bits >> ip) & 1u, b1 = (bits >> (ip + 4)) & 1u;
-            if (!(b0 || b1)) continue;
-            const float4 vxy = s_xy[wib][ip], vzq = s_zq[wib][ip];
-            const f2p dx = sub2(splat2(xj.x), pk2(vxy.x, vxy.y));
-            const f2p dy = sub2(splat2(xj.y), pk2(vxy.z, vxy.w));
-            const f2p dz = sub2(splat2(xj.z), pk2(vzq.x, vzq.y));
-            const float2 r2v = up2(fma2(dx, dx, fma2(dy, dy, mul2(dz, dz))));
-            const bool oka = b0 && r2v.x <= p.rc2, okb = b1 && r2v.y <= p.rc2;
-            if (!(oka || okb)) continue;
-            // an element outside the cutoff is evaluated at r = 1 and masked out below
-            const float r2a = oka ? r2v.x : 1.f, r2b = okb ? r2v.y : 1.f;
-            const f2p r2 = pk2(r2a, r2b);
-            const f2p rinv = pk2(rsqrtf(r2a), rsqrtf(r2b));
+            // the mask bit of each element folded into its cutoff: rc^2, or -1 (never met).
+            // Every lane evaluates both elements (a whole-warp skip almost never
+            // happens), and elements outside the mask or the cutoff — possibly
+            // non-finite, e.g. a padding slot at distance 0 — are dropped by the select.
+            const float tha = (bits >> ip) & 1u ? p.rc2 : -1.f;
+            const float thb = (bits >> (ip + 4)) & 1u ? p.rc2 : -1.f;
+            const float4 vxy = s_xy[wib][ip], vzq = s_zq[wib][ip], vlj = s_lj[wib][ip];
+            const f2p dx = sub2(jx, pk2(vxy.x, vxy.y));
+            const f2p dy = sub2(jy, pk2(vxy.z, vxy.w));
+            const f2p dz = sub2(jz, pk2(vzq.x, vzq.y));
+            const f2p r2 = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
+            const float2 r2v = up2(r2);
+            const bool oka = r2v.x <= tha, okb = r2v.y <= thb;
+            const f2p rinv = pk2(rsqrtf(r2v.x), rsqrtf(r2v.y));
             const f2p rinv2 = mul2(rinv, rinv);
-            const float4 vlj = s_lj[wib][ip];
-            const f2p sig = add2(pk2(vlj.x, vlj.y), splat2(ljj.x));
-            const f2p eps24 = mul2(pk2(vlj.z, vlj.w), splat2(ljj.y));
+            const f2p sig = add2(pk2(vlj.x, vlj.y), jsig);
+            const f2p eps24 = mul2(pk2(vlj.z, vlj.w), jeps);
             const f2p s2 = mul2(mul2(sig, sig), rinv2);
             const f2p s6 = mul2(mul2(s2, s2), s2);
             // LJ: 24 eps s6 (1 - 2 s6) / r^2
             f2p fs = mul2(mul2(eps24, s6), mul2(rinv2, fma2(s6, mtwo2, one2)));
             f2p ec = zero2;
             if (ES != 0) {
-                const f2p qq = mul2(pk2(vzq.z, vzq.w), splat2(xj.w));
+                const f2p qq = mul2(pk2(vzq.z, vzq.w), jq);
                 if (ES == 2) {
                     const f2p r = mul2(r2, rinv);
                     const f2p x = mul2(splat2(p.kappa), r);
@@ -198,13 +200,14 @@ __global__ void __launch_bounds__(256, ENERGY ? 2 : 3) k_nonbonded(DevState st, 
             fjy = sub2(fjy, fy);
             fjz = sub2(fjz, fz);
             if (ENERGY) {
-                // 4 eps s6 (s6 - 1) = (24 eps / 6) s6 (s6 - 1); masked like the force
-                const f2p m = pk2(oka ? 1.f : 0.f, okb ? 1.f : 0.f);
-                const f2p elj = mul2(m, mul2(mul2(eps24, splat2(1.f / 6.f)), mul2(s6, sub2(s6, one2))));
-                const f2p ecm = mul2(m, ec);
+                // 4 eps s6 (s6 - 1) = (24 eps / 6) s6 (s6 - 1); dropped like the force
+                const float2 eljv = up2(mul2(mul2(eps24, splat2(1.f / 6.f)), mul2(s6, sub2(s6, one2))));
+                const float2 ecv = up2(ec);
+                const f2p elj = pk2(oka ? eljv.x : 0.f, okb ? eljv.y : 0.f);
+                const f2p ecm = pk2(oka ? ecv.x : 0.f, okb ? ecv.y : 0.f);
                 s_elj = add2(s_elj, elj);
                 s_ec = add2(s_ec, ecm);
-                s_vir = fma2(fs, r2, s_vir);   // fs is already masked; -1/2 r_ij . f_ij = fs r^2 / 2
+                s_vir = fma2(fs, r2, s_vir);   // fs is already dropped; -1/2 r_ij . f_ij = fs r^2 / 2
                 const f2p eh = mul2(splat2(0.5f), add2(elj, ecm));
                 ei[ip] = add2(ei[ip], eh);
                 ej = add2(ej, eh);
