@@ -587,6 +587,7 @@ void lima_engine::setup() {
     D.new_orig = dalloc<int>(S);
     D.bb_lo = dalloc<float4>(n_clusters);
     D.bb_hi = dalloc<float4>(n_clusters);
+    D.bb_molsig = dalloc<unsigned long long>(n_clusters);
     D.pl_count = dalloc<int>(n_clusters);
     D.pl_j = dalloc<int>((size_t)n_clusters * pl_cap);
     D.pl_mask = dalloc<unsigned long long>((size_t)n_clusters * pl_cap);

@@ -65,6 +65,7 @@ struct DevState {
     // clusters and pair list
     float4* bb_lo = nullptr;
     float4* bb_hi = nullptr;
+    unsigned long long* bb_molsig = nullptr;  // bit (molecule id mod 64) of every atom in the cluster
     int* pl_count = nullptr;
     int* pl_j = nullptr;
     unsigned long long* pl_mask = nullptr;

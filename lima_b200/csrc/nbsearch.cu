@@ -193,9 +193,11 @@ __global__ void k_bbox(DevState st) {
     if (c >= st.n_clusters) return;
     float4 lo = make_float4(0.f, 0.f, 0.f, 0.f), hi = lo;
     bool first = true;
+    unsigned long long sig = 0ull;
     for (int k = 0; k < CLUSTER; ++k) {
         const int s = c * CLUSTER + k;
         if (st.orig[s] < 0) continue;
+        sig |= 1ull << (st.slot_mol[s] & 63);
         const float4 p = st.xyzq[s];
         if (first) {
             lo = hi = p;
@@ -212,6 +214,7 @@ __global__ void k_bbox(DevState st) {
     lo.w = first ? 0.f : 1.f;  // w = 1 marks a populated cluster
     st.bb_lo[c] = lo;
     st.bb_hi[c] = hi;
+    st.bb_molsig[c] = sig;
 }
 
 __device__ __forceinline__ bool excluded(const DevState& st, int ai, int aj, int eb, int ee) {
@@ -225,10 +228,26 @@ __device__ __forceinline__ int wrapi(int i, int n) {
     return i < 0 ? i + n : i;
 }
 
-// one warp per i-cluster
-__global__ void k_pairsearch(DevState st, float rlist) {
+// One warp per i-cluster, in two phases that alternate through the column
+// window:
+//   1. candidate search: the clusters of a column are tested 32 at a time
+//      (one per lane) against the i-cluster's extent, for each periodic shift
+//      in range; every (cluster, shift) in range is appended, in lane order, to
+//      a per-warp queue in shared memory;
+//   2. masks: whenever 32 candidates are queued, each lane builds the full
+//      64-bit interaction mask of one of them on its own (the eight i-atoms sit
+//      in registers), and the non-empty ones are appended to the pair list in
+//      lane order.
+// Instruction count, not memory, bounds this kernel; giving every lane a whole
+// candidate keeps all 32 lanes on distinct work.  The list order is fixed by
+// the column, lane and shift order, so the list is identical run to run.
+constexpr int PS_WARPS = 4;
+constexpr int PS_QCAP = 32 + 32 * 27;   // a full batch left over + one column batch with every shift
+
+__global__ void __launch_bounds__(PS_WARPS * 32, 1) k_pairsearch(DevState st, float rlist) {
+    __shared__ int q[PS_WARPS][PS_QCAP];
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     if (warp >= st.n_clusters) return;
     const int ci = warp;
     const int sysi = st.cluster_sys[ci];
@@ -244,22 +263,29 @@ __global__ void k_pairsearch(DevState st, float rlist) {
     const float L[3] = {sd.boxf[0], sd.boxf[1], sd.boxf[2]};
     const float R = rlist, R2 = rlist * rlist;
 
-    // per-lane i-atom data for the interaction mask (lane -> ii = lane & 7)
-    const int ii = lane & 7, jj0 = lane >> 3;
-    const int ai = st.orig[ci * CLUSTER + ii];
-    const int mi = st.slot_mol[ci * CLUSTER + ii];
-    const int eb = ai >= 0 ? st.excl_off[ai] : 0;
-    const int ee = ai >= 0 ? st.excl_off[ai + 1] : 0;
-    const float4 xi = st.xyzq[ci * CLUSTER + ii];
+    const unsigned long long isig = st.bb_molsig[ci];
+    // the eight i-atoms in every lane's registers; a padding i-atom is moved far
+    // away so that no distance test passes for it
+    float xi[CLUSTER], yi[CLUSTER], zi[CLUSTER];
+    int mi[CLUSTER];
+#pragma unroll
+    for (int a = 0; a < CLUSTER; ++a) {
+        const int s = ci * CLUSTER + a;
+        const float4 x = st.xyzq[s];
+        mi[a] = st.slot_mol[s];
+        const bool real = st.orig[s] >= 0;
+        xi[a] = real ? x.x : 1e30f;
+        yi[a] = real ? x.y : 1e30f;
+        zi[a] = real ? x.z : 1e30f;
+    }
 
-    // column window (every column visited once even when the window wraps)
-    int cx0 = (int)floorf((ilo.x - R) / sd.col_w[0]);
-    int cx1 = (int)floorf((ihi.x + R) / sd.col_w[0]);
-    int nx = cx1 - cx0 + 1;
-    // When the window does not cover a whole row of columns, each column in
-    // it is met once at a known unwrapped position, which fixes the x and y
-    // periodic shift of its clusters: only the three z shifts remain to test.
+    // column window (every column visited once even when the window wraps).
+    // When it does not cover a whole row of columns, each column in it is met
+    // once at a known unwrapped position, which fixes the x and y periodic
+    // shift of its clusters: only the three z shifts remain to test.
     // Otherwise every one of the 27 shifts is tested.
+    int cx0 = (int)floorf((ilo.x - R) / sd.col_w[0]);
+    int nx = (int)floorf((ihi.x + R) / sd.col_w[0]) - cx0 + 1;
     bool fixed_xy = true;
     if (nx >= sd.ncol_x) {
         cx0 = 0;
@@ -267,8 +293,7 @@ __global__ void k_pairsearch(DevState st, float rlist) {
         fixed_xy = false;
     }
     int cy0 = (int)floorf((ilo.y - R) / sd.col_w[1]);
-    int cy1 = (int)floorf((ihi.y + R) / sd.col_w[1]);
-    int ny = cy1 - cy0 + 1;
+    int ny = (int)floorf((ihi.y + R) / sd.col_w[1]) - cy0 + 1;
     if (ny >= sd.ncol_y) {
         cy0 = 0;
         ny = sd.ncol_y;
@@ -278,95 +303,165 @@ __global__ void k_pairsearch(DevState st, float rlist) {
     const int cap = st.pl_cap;
     int count = 0;
     const size_t base_out = (size_t)ci * cap;
-    for (int iy = 0; iy < ny; ++iy) {
-        const int cy = wrapi(cy0 + iy, sd.ncol_y);
-        const int sy_col = cy0 + iy < 0 ? -1 : (cy0 + iy >= sd.ncol_y ? 1 : 0);
-        for (int ix = 0; ix < nx; ++ix) {
-            const int cx = wrapi(cx0 + ix, sd.ncol_x);
+
+    // masks of the queued candidates q[head .. head + nb), one per lane
+    auto build_masks = [&](int head, int nb) {
+        unsigned long long mask = 0ull;
+        int ent = 0;
+        if (lane < nb) {
+            ent = q[wib][head + lane];
+            const int jc = ent & ((1 << JCLUSTER_BITS) - 1);
+            const int3 sh = decode_shift((unsigned)ent >> JCLUSTER_BITS);
+            const float shx = sh.x * L[0], shy = sh.y * L[1], shz = sh.z * L[2];
+            const bool share_mol = (isig & st.bb_molsig[jc]) != 0ull;
+#pragma unroll
+            for (int jj = 0; jj < CLUSTER; ++jj) {
+                const int sj = jc * CLUSTER + jj;
+                const int mj = st.slot_mol[sj];
+                const float4 xj = st.xyzq[sj];
+                const float jx = xj.x + shx, jy = xj.y + shy, jz = xj.z + shz;
+                unsigned m8 = 0u;
+#pragma unroll
+                for (int ii = 0; ii < CLUSTER; ++ii) {
+                    const float dx = jx - xi[ii], dy = jy - yi[ii], dz = jz - zi[ii];
+                    if (dx * dx + dy * dy + dz * dz < R2) m8 |= 1u << ii;
+                }
+                if (mj < 0) m8 = 0u;   // padding slot
+                // pairs within one molecule: drop the excluded ones (only when the
+                // clusters' molecule signatures meet; then the exclusion lists decide)
+                if (share_mol && m8 != 0u) {
+#pragma unroll
+                    for (int ii = 0; ii < CLUSTER; ++ii) {
+                        if (((m8 >> ii) & 1u) && mi[ii] == mj) {
+                            const int ai = st.orig[ci * CLUSTER + ii];
+                            if (excluded(st, ai, st.orig[sj], st.excl_off[ai], st.excl_off[ai + 1]))
+                                m8 &= ~(1u << ii);
+                        }
+                    }
+                }
+                mask |= (unsigned long long)m8 << (8 * jj);
+            }
+            // the diagonal cluster counts each pair once: keep jj > ii only
+            if (jc == ci) {
+                unsigned long long upper = 0ull;
+#pragma unroll
+                for (int jj = 0; jj < CLUSTER; ++jj)
+                    for (int ii = 0; ii < jj; ++ii) upper |= 1ull << (8 * jj + ii);
+                mask &= upper;
+            }
+        }
+        const unsigned has = __ballot_sync(0xffffffffu, mask != 0ull);
+        const int pos = count + __popc(has & ((1u << lane) - 1u));
+        if (mask != 0ull && pos < cap) {
+            st.pl_j[base_out + pos] = ent;
+            st.pl_mask[base_out + pos] = mask;
+        }
+        count += __popc(has);
+    };
+
+    // flat walk over (column, batch of 32 clusters) units; after each unit's
+    // candidates are queued, full batches of 32 are turned into masks, and
+    // after the last unit whatever remains
+    int qn = 0;
+    // column counters advance incrementally (no division per unit)
+    int ix = 0, iy = 0, b = 0;
+    int cx = wrapi(cx0, sd.ncol_x), cy = wrapi(cy0, sd.ncol_y);
+    bool done = nx <= 0 || ny <= 0;
+    while (true) {
+        if (!done) {
+            const int sy_col = cy0 + iy < 0 ? -1 : (cy0 + iy >= sd.ncol_y ? 1 : 0);
             const int sx_col = cx0 + ix < 0 ? -1 : (cx0 + ix >= sd.ncol_x ? 1 : 0);
             const int col = sd.col_off + cx + sd.ncol_x * cy;
             const int j0 = st.col_cl_start[col];
             const int nj = st.col_ncl[col];
-            for (int b = 0; b < nj; b += 32) {
-                const int j = j0 + b + lane;
-                unsigned shifts = 0u;  // bit k set: shift code k is in range
-                if (b + lane < nj && j >= ci) {
-                    const float4 jlo = st.bb_lo[j], jhi = st.bb_hi[j];
-                    const float jc[3] = {0.5f * (jlo.x + jhi.x), 0.5f * (jlo.y + jhi.y), 0.5f * (jlo.z + jhi.z)};
-                    const float je[3] = {0.5f * (jhi.x - jlo.x), 0.5f * (jhi.y - jlo.y), 0.5f * (jhi.z - jlo.z)};
-                    if (fixed_xy) {
-                        const float gx = fmaxf(fabsf(jc[0] + sx_col * L[0] - ic[0]) - ie[0] - je[0], 0.f);
-                        const float gy = fmaxf(fabsf(jc[1] + sy_col * L[1] - ic[1]) - ie[1] - je[1], 0.f);
-                        const float gxy = gx * gx + gy * gy;
-                        if (gxy < R2) {
-                            const int base = (sx_col + 1) + 3 * (sy_col + 1);
-                            for (int sz = -1; sz <= 1; ++sz) {
-                                const int code = base + 9 * (sz + 1);
-                                if (j == ci && code != 13) continue;
-                                const float gz = fmaxf(fabsf(jc[2] + sz * L[2] - ic[2]) - ie[2] - je[2], 0.f);
-                                if (gxy + gz * gz < R2) shifts |= 1u << code;
-                            }
+            const int j = j0 + b + lane;
+            unsigned shifts = 0u;  // bit k set: shift code k is in range
+            if (b + lane < nj && j >= ci) {
+                const float4 jlo = st.bb_lo[j], jhi = st.bb_hi[j];
+                const float jc[3] = {0.5f * (jlo.x + jhi.x), 0.5f * (jlo.y + jhi.y), 0.5f * (jlo.z + jhi.z)};
+                const float je[3] = {0.5f * (jhi.x - jlo.x), 0.5f * (jhi.y - jlo.y), 0.5f * (jhi.z - jlo.z)};
+                if (jlo.w == 0.f) {
+                    // empty cluster: nothing to pair with
+                } else if (fixed_xy) {
+                    const float gx = fmaxf(fabsf(jc[0] + sx_col * L[0] - ic[0]) - ie[0] - je[0], 0.f);
+                    const float gy = fmaxf(fabsf(jc[1] + sy_col * L[1] - ic[1]) - ie[1] - je[1], 0.f);
+                    const float gxy = gx * gx + gy * gy;
+                    if (gxy < R2) {
+                        const int base = (sx_col + 1) + 3 * (sy_col + 1);
+                        for (int sz = -1; sz <= 1; ++sz) {
+                            const int code = base + 9 * (sz + 1);
+                            if (j == ci && code != 13) continue;
+                            const float gz = fmaxf(fabsf(jc[2] + sz * L[2] - ic[2]) - ie[2] - je[2], 0.f);
+                            if (gxy + gz * gz < R2) shifts |= 1u << code;
                         }
-                    } else {
-                        float g2[3][3];
-                        for (int d = 0; d < 3; ++d) {
-                            for (int sh = -1; sh <= 1; ++sh) {
-                                const float dd = fabsf(jc[d] + sh * L[d] - ic[d]) - ie[d] - je[d];
-                                const float g = fmaxf(dd, 0.f);
-                                g2[d][sh + 1] = g * g;
-                            }
-                        }
-                        for (int sz = 0; sz < 3; ++sz)
-                            for (int sy = 0; sy < 3; ++sy)
-                                for (int sx = 0; sx < 3; ++sx) {
-                                    const int code = sx + 3 * sy + 9 * sz;
-                                    if (j == ci && code != 13) continue;
-                                    if (g2[0][sx] + g2[1][sy] + g2[2][sz] < R2) shifts |= 1u << code;
-                                }
                     }
-                }
-                unsigned pending = __ballot_sync(0xffffffffu, shifts != 0u);
-                while (pending) {
-                    const int src = __ffs(pending) - 1;
-                    const unsigned sh_src = __shfl_sync(0xffffffffu, shifts, src);
-                    const int jc = __shfl_sync(0xffffffffu, j, src);
-                    const int code = __ffs(sh_src) - 1;
-                    const unsigned rest = sh_src & (sh_src - 1u);
-                    if (lane == src) shifts = rest;
-                    if (rest == 0u) pending &= pending - 1u;
-                    // interaction mask: bit (jj*8 + ii); a pair is kept when both atoms
-                    // are real, it is not excluded, it is counted once on the diagonal
-                    // and its image distance is inside the list radius (Verlet buffer)
-                    const int3 sh = decode_shift(code);
-                    const float shx = sh.x * L[0], shy = sh.y * L[1], shz = sh.z * L[2];
-                    bool ok[2];
-                    for (int h = 0; h < 2; ++h) {
-                        const int jj = jj0 + 4 * h;
-                        const int sj = jc * CLUSTER + jj;
-                        const int mj = st.slot_mol[sj];
-                        bool o = ai >= 0 && mj >= 0;
-                        if (o && jc == ci) o = jj > ii;
-                        if (o) {
-                            const float4 xj = st.xyzq[sj];
-                            const float dx = xj.x + shx - xi.x, dy = xj.y + shy - xi.y, dz = xj.z + shz - xi.z;
-                            o = dx * dx + dy * dy + dz * dz < R2;
+                } else {
+                    float g2[3][3];
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+#pragma unroll
+                        for (int sh = -1; sh <= 1; ++sh) {
+                            const float dd = fabsf(jc[d] + sh * L[d] - ic[d]) - ie[d] - je[d];
+                            const float g = fmaxf(dd, 0.f);
+                            g2[d][sh + 1] = g * g;
                         }
-                        if (o && mi == mj) o = !excluded(st, ai, st.orig[sj], eb, ee);
-                        ok[h] = o;
                     }
-                    const unsigned lo32 = __ballot_sync(0xffffffffu, ok[0]);
-                    const unsigned hi32 = __ballot_sync(0xffffffffu, ok[1]);
-                    const unsigned long long mask = ((unsigned long long)hi32 << 32) | lo32;
-                    if (mask != 0ull) {
-                        if (count < cap && lane == 0) {
-                            st.pl_j[base_out + count] = jc | (code << JCLUSTER_BITS);
-                            st.pl_mask[base_out + count] = mask;
-                        }
-                        ++count;
+#pragma unroll 1
+                    for (int code = 0; code < 27; ++code) {
+                        if (j == ci && code != 13) continue;
+                        const int sx = code % 3, sy = (code / 3) % 3, sz = code / 9;
+                        const float gxs = sx == 0 ? g2[0][0] : (sx == 1 ? g2[0][1] : g2[0][2]);
+                        const float gys = sy == 0 ? g2[1][0] : (sy == 1 ? g2[1][1] : g2[1][2]);
+                        const float gzs = sz == 0 ? g2[2][0] : (sz == 1 ? g2[2][1] : g2[2][2]);
+                        if (gxs + gys + gzs < R2) shifts |= 1u << code;
                     }
                 }
             }
+            // append (cluster, shift) candidates in lane order, then shift order
+            const int c = __popc(shifts);
+            int incl = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
+            }
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            int w = qn + incl - c;
+            while (shifts) {
+                const int code = __ffs(shifts) - 1;
+                shifts &= shifts - 1u;
+                q[wib][w++] = j | (code << JCLUSTER_BITS);
+            }
+            qn += total;
+            b += 32;
+            if (b >= nj) {
+                b = 0;
+                if (++cx == sd.ncol_x) cx = 0;
+                if (++ix == nx) {
+                    ix = 0;
+                    cx = wrapi(cx0, sd.ncol_x);
+                    if (++cy == sd.ncol_y) cy = 0;
+                    done = ++iy == ny;
+                }
+            }
         }
+        __syncwarp();
+        int head = 0;
+        while (qn - head >= 32 || (done && qn > head)) {
+            const int nb = min(32, qn - head);
+            build_masks(head, nb);
+            head += nb;
+        }
+        if (head > 0) {
+            // move the remainder (< 32) to the front of the queue
+            const int rem = qn - head;
+            const int v = lane < rem ? q[wib][head + lane] : 0;
+            __syncwarp();
+            if (lane < rem) q[wib][lane] = v;
+            qn = rem;
+        }
+        __syncwarp();
+        if (done) break;
     }
     if (lane == 0) {
         st.pl_count[ci] = min(count, cap);
@@ -384,7 +479,8 @@ int launch_rebuild(const DevState& st, float rlist, bool from_input, cudaStream_
     k_finish_slots<<<(st.n_slots + TB - 1) / TB, TB, 0, s>>>(st);
     k_bbox<<<(st.n_clusters + TB - 1) / TB, TB, 0, s>>>(st);
     const long long threads = (long long)st.n_clusters * 32;
-    k_pairsearch<<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(st, rlist);
+    const int TP = PS_WARPS * 32;
+    k_pairsearch<<<(unsigned)((threads + TP - 1) / TP), TP, 0, s>>>(st, rlist);
     return 8;
 }
 
