@@ -235,6 +235,26 @@ __global__ void k_spread(DevState st) {
 }
 
 // ------------------------------------------------------------- FFT passes
+// Copies `total` elements with the whole block, four independent loads per
+// thread in flight before their stores (the passes are bound by load latency):
+// load(i) returns element i, store(i, v) places it.
+template <typename T, typename Load, typename Store>
+__device__ __forceinline__ void block_copy4(int total, Load load, Store store) {
+    for (int i0 = threadIdx.x; i0 < total; i0 += 4 * blockDim.x) {
+        T v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int i = i0 + u * blockDim.x;
+            if (i < total) v[u] = load(i);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int i = i0 + u * blockDim.x;
+            if (i < total) store(i, v[u]);
+        }
+    }
+}
+
 // x pass forward: int64 charge grid -> half-complex rows (and zero the int64 grid)
 __global__ void k_fft_x_fwd(DevState st, const PmeSysDev* plans, const int4* items, int maxn) {
     extern __shared__ float2 sm[];
@@ -249,10 +269,13 @@ __global__ void k_fft_x_fwd(DevState st, const PmeSysDev* plans, const int4* ite
     load_twiddles(tw, pl, st.pme_tw);
     const int nl = it.z;
     const long long* g = st.pme_grid_fx + sd.pme_off + (size_t)it.y * K0;
-    for (int i = threadIdx.x; i < nl * K0; i += blockDim.x) {
-        const int l = i / K0, x = i - l * K0;
-        A[l * stride + x] = make_float2((float)((double)g[(size_t)l * K0 + x] * (1.0 / GRID_SCALE)), 0.f);
-    }
+    // the nl lines are contiguous: element i of the tile is g[i]
+    block_copy4<long long>(
+        nl * K0, [&](int i) { return g[i]; },
+        [&](int i, long long v) {
+            const int l = i / K0, x = i - l * K0;
+            A[l * stride + x] = make_float2((float)((double)v * (1.0 / GRID_SCALE)), 0.f);
+        });
     __syncthreads();
     const float2* res = fft_lines(A, B, nl, stride, pl, tw, -1.f);
     float2* out = st.pme_cplx + sd.pme_coff + (size_t)it.y * K0h;
@@ -276,17 +299,23 @@ __global__ void k_fft_x_inv(DevState st, const PmeSysDev* plans, const int4* ite
     load_twiddles(tw, pl, st.pme_tw);
     const int nl = it.z;
     const float2* in = st.pme_cplx + sd.pme_coff + (size_t)it.y * K0h;
-    for (int i = threadIdx.x; i < nl * K0; i += blockDim.x) {
-        const int l = i / K0, k = i - l * K0;
-        float2 v;
-        if (k < K0h) {
-            v = in[(size_t)l * K0h + k];
-        } else {
-            v = in[(size_t)l * K0h + (K0 - k)];
-            v.y = -v.y;  // Hermitian symmetry of a real signal
-        }
-        A[l * stride + k] = v;
-    }
+    block_copy4<float2>(
+        nl * K0,
+        [&](int i) {
+            const int l = i / K0, k = i - l * K0;
+            float2 v;
+            if (k < K0h) {
+                v = in[(size_t)l * K0h + k];
+            } else {
+                v = in[(size_t)l * K0h + (K0 - k)];
+                v.y = -v.y;  // Hermitian symmetry of a real signal
+            }
+            return v;
+        },
+        [&](int i, float2 v) {
+            const int l = i / K0, k = i - l * K0;
+            A[l * stride + k] = v;
+        });
     __syncthreads();
     const float2* res = fft_lines(A, B, nl, stride, pl, tw, 1.f);
     float* out = st.pme_real + sd.pme_off + (size_t)it.y * K0;
@@ -311,10 +340,16 @@ __global__ void k_fft_y(DevState st, const PmeSysDev* plans, const int4* items, 
     const int x0 = it.y, z = it.z;
     const int tx = min(FFT_TX, K0h - x0);
     float2* g = st.pme_cplx + sd.pme_coff + (size_t)z * K1 * K0h + x0;
-    for (int i = threadIdx.x; i < K1 * FFT_TX; i += blockDim.x) {
-        const int y = i / FFT_TX, c = i - y * FFT_TX;
-        A[c * stride + y] = c < tx ? g[(size_t)y * K0h + c] : make_float2(0.f, 0.f);
-    }
+    block_copy4<float2>(
+        K1 * FFT_TX,
+        [&](int i) {
+            const int y = i / FFT_TX, c = i - y * FFT_TX;
+            return c < tx ? g[(size_t)y * K0h + c] : make_float2(0.f, 0.f);
+        },
+        [&](int i, float2 v) {
+            const int y = i / FFT_TX, c = i - y * FFT_TX;
+            A[c * stride + y] = v;
+        });
     __syncthreads();
     const float2* res = fft_lines(A, B, FFT_TX, stride, pl, tw, sigma);
     for (int i = threadIdx.x; i < K1 * FFT_TX; i += blockDim.x) {
@@ -340,17 +375,28 @@ __global__ void k_fft_z_conv(DevState st, const PmeSysDev* plans, const int4* it
     const size_t plane = (size_t)K1 * K0h;
     float2* g = st.pme_cplx + sd.pme_coff + (size_t)y * K0h + x0;
     const float* th = st.pme_theta + sd.pme_coff + (size_t)y * K0h + x0;
-    for (int i = threadIdx.x; i < K2 * FFT_TX; i += blockDim.x) {
-        const int z = i / FFT_TX, c = i - z * FFT_TX;
-        A[c * stride + z] = c < tx ? g[z * plane + c] : make_float2(0.f, 0.f);
-    }
+    block_copy4<float2>(
+        K2 * FFT_TX,
+        [&](int i) {
+            const int z = i / FFT_TX, c = i - z * FFT_TX;
+            return c < tx ? g[z * plane + c] : make_float2(0.f, 0.f);
+        },
+        [&](int i, float2 v) {
+            const int z = i / FFT_TX, c = i - z * FFT_TX;
+            A[c * stride + z] = v;
+        });
     __syncthreads();
     float2* res = fft_lines(A, B, FFT_TX, stride, pl, tw, -1.f);
-    for (int i = threadIdx.x; i < K2 * FFT_TX; i += blockDim.x) {
-        const int z = i / FFT_TX, c = i - z * FFT_TX;
-        const float t = c < tx ? th[z * plane + c] : 0.f;
-        res[c * stride + z] = cscale(res[c * stride + z], t);
-    }
+    block_copy4<float>(
+        K2 * FFT_TX,
+        [&](int i) {
+            const int z = i / FFT_TX, c = i - z * FFT_TX;
+            return c < tx ? th[z * plane + c] : 0.f;
+        },
+        [&](int i, float t) {
+            const int z = i / FFT_TX, c = i - z * FFT_TX;
+            res[c * stride + z] = cscale(res[c * stride + z], t);
+        });
     __syncthreads();
     float2* other = res == A ? B : A;
     const float2* res2 = fft_lines(res, other, FFT_TX, stride, pl, tw, 1.f);
