@@ -292,6 +292,12 @@ LIMA_API int lima_learned_pme_weights(lima_engine* h, int get, float* buf, int64
  * squared error.  For checking the training kernels. */
 LIMA_API int lima_learned_pme_gradients(lima_engine* h, int rows, const float* x, const float* t,
                                         float* grads, double* loss);
+/* Network output for caller rows (features: rows x 68 raw inputs, normalised
+ * with the model's statistics inside; out: rows x 3, in units of the output
+ * scale), rows <= 65536.  impl 0: the tcgen05 tensor-core kernel used in
+ * stepping; 1: the warp-level mma.sync kernel.  LIMA_ERR_TIMEOUT if a bounded
+ * device wait gave up. */
+LIMA_API int lima_learned_pme_predict(lima_engine* h, int rows, const float* features, float* out, int impl);
 
 /* ---------------------------------------------------------- thermostat, log */
 /* Last temperature measurement of the selected system: temperature [K], the

@@ -840,6 +840,7 @@ void lima_engine::learned_setup(int cx, int cy, int cz, int max_frames) {
     m.part = dalloc<float>(chunks * 128 * 128);
     m.bpart = dalloc<float>(chunks * 128);
     m.max_rows = batch_cap;
+    m.tc_err = dalloc<int>(1);
     for (int c = 0; c < MLP_IN; ++c) m.in_mean[c] = 0.f, m.in_std[c] = 1.f;
     mlp = m;
     mlp_sync_bf16(mlp, s_main);
@@ -870,7 +871,10 @@ void lima_engine::learned_features(bool forward, cudaStream_t s) {
     CK(cudaMemsetAsync(lp_fc, 0, sizeof(long long) * 3 * (size_t)st.n_slots, s));
     launches += launch_pme(st_c, pp_c, false, s);
     launches += launch_descriptor(st, lp_fc, lp_feat, s);
-    if (forward && lp_norm) launches += mlp_infer(mlp, st.n_slots, lp_feat, lp_mean, lp_invstd, lp_Y, s);
+    if (forward && lp_norm) {
+        if (mlp.use_tc) launches += mlp_infer_tc(mlp, st.n_slots, lp_feat, lp_mean, lp_invstd, lp_Y, mlp.tc_err, s);
+        else launches += mlp_infer(mlp, st.n_slots, lp_feat, lp_mean, lp_invstd, lp_Y, s);
+    }
 }
 
 // full-grid reciprocal force into lp_ff (energy, when asked, into the engine's
@@ -1826,6 +1830,33 @@ int lima_clear_log(lima_engine* h) {
     h->log_host_pe.shrink_to_fit();
     h->log_host_fs.shrink_to_fit();
     return LIMA_OK;
+}
+
+int lima_learned_pme_predict(lima_engine* h, int rows, const float* features, float* out, int impl) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    if (rows < 1 || !features || !out || impl < 0 || impl > 1)
+        return fail(h, LIMA_ERR_INVALID_ARG, "bad prediction arguments");
+    return guarded(h, [&]() {
+        if (int e = learned_ready(h)) return e;
+        if (rows > h->batch_cap) return fail(h, LIMA_ERR_INVALID_ARG, "more than 65536 rows");
+        cudaStream_t s = h->s_main;
+        CK(cudaMemcpyAsync(h->batch_raw, features, (size_t)rows * MLP_IN * 4, cudaMemcpyHostToDevice, s));
+        CK(cudaMemsetAsync(h->mlp.tc_err, 0, sizeof(int), s));
+        if (impl == 0)
+            h->launches += mlp_infer_tc(h->mlp, rows, h->batch_raw, h->lp_mean, h->lp_invstd, h->acts.y, h->mlp.tc_err, s);
+        else
+            h->launches += mlp_infer(h->mlp, rows, h->batch_raw, h->lp_mean, h->lp_invstd, h->acts.y, s);
+        std::vector<float> y((size_t)rows * 8);
+        int err = 0;
+        CK(cudaMemcpyAsync(y.data(), h->acts.y, y.size() * 4, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(&err, h->mlp.tc_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        CK(cudaGetLastError());
+        if (err) return fail(h, LIMA_ERR_TIMEOUT, "tensor-core inference: a bounded wait gave up");
+        for (int r = 0; r < rows; ++r)
+            for (int c = 0; c < 3; ++c) out[(size_t)r * 3 + c] = y[(size_t)r * 8 + c];
+        return LIMA_OK;
+    });
 }
 
 }  // extern "C"

@@ -360,6 +360,227 @@ __global__ void __launch_bounds__(INF_WARPS * 32, 1)
     }
 }
 
+// ------------------------------------------------ fused inference, tcgen05
+// The same network on the 5th-generation tensor cores: one CTA (a warpgroup
+// of 128 threads) per SM owns 128-row tiles.  All BF16 weights and the tile's
+// activations sit in shared memory in the canonical K-major layout without
+// swizzle (8-row x 16-byte core matrices: the two core matrices of one MMA's
+// K = 16 are LBO = 128 B apart, consecutive 8-row groups SBO = K/8 x 128 B
+// apart).  One thread issues tcgen05.mma (M = 128, N = 128 or 16, K = 16,
+// BF16 x BF16 -> FP32) into 128 TMEM columns and commits to an mbarrier; after
+// the wait, thread t of warp w reads row 32w + t of the accumulator with
+// tcgen05.ld, adds the bias, applies SiLU and writes the next layer's input
+// row back to shared memory.  Every wait on the mbarrier is bounded: on a
+// timeout the kernel records an error, waits (bounded) once more for its MMAs
+// and frees its TMEM before returning.
+namespace tc {
+constexpr int ROWS = 128;
+constexpr int W0_OFF = 0;                              // N 128 x K 80
+constexpr int W1_OFF = W0_OFF + 128 * 80 * 2;          // N 128 x K 128
+constexpr int W2_OFF = W1_OFF + 128 * 128 * 2;
+constexpr int W3_OFF = W2_OFF + 128 * 128 * 2;         // N 16 x K 128 (rows 8..15 zero)
+constexpr int A_OFF = W3_OFF + 16 * 128 * 2;           // 128 rows x K <= 128
+constexpr int BIAS_OFF = A_OFF + ROWS * 128 * 2;       // 3 x 128 + 16 floats
+constexpr int NORM_OFF = BIAS_OFF + (3 * 128 + 16) * 4;
+constexpr int MBAR_OFF = NORM_OFF + 2 * MLP_IN * 4;    // 8-byte aligned
+constexpr int TADDR_OFF = MBAR_OFF + 8;
+constexpr int FLAG_OFF = TADDR_OFF + 4;
+constexpr int SMEM = FLAG_OFF + 4;
+constexpr int TMEM_COLS = 128;
+constexpr unsigned WAIT_LIMIT = 1u << 20;
+static_assert(MBAR_OFF % 8 == 0, "mbarrier alignment");
+static_assert(A_OFF % 16 == 0 && W3_OFF % 16 == 0, "16-byte aligned operands");
+
+// byte offset of 16-byte chunk kc (elements 8kc..8kc+7) of row r, K columns
+__device__ __forceinline__ int boff(int r, int kc, int K) { return ((r >> 3) * (K >> 3) + kc) * 128 + (r & 7) * 16; }
+
+__device__ __forceinline__ uint64_t sdesc(unsigned saddr, int K) {
+    const uint64_t lbo = 128 >> 4, sbo = (uint64_t)((K >> 3) * 128) >> 4;
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | (lbo << 16) | (sbo << 32) | (1ull << 46);
+}
+__host__ __device__ constexpr uint32_t idesc(int N) {
+    // F32 accumulate, BF16 A and B, both K-major, N >> 3, M = 128 >> 4
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+__device__ __forceinline__ void mma(uint32_t tmem, uint64_t a, uint64_t b, uint32_t id, uint32_t accum) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+        "l"(a), "l"(b), "r"(id), "r"(accum), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+__device__ __forceinline__ void commit(unsigned mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar) : "memory");
+}
+__device__ __forceinline__ bool wait_parity(unsigned mbar, unsigned parity) {
+    for (unsigned it = 0; it < WAIT_LIMIT; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P1;\n\t}"
+            : "=r"(done)
+            : "r"(mbar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+__device__ __forceinline__ void ld16(uint32_t taddr, float* v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
+}
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// weights W^T[N][K] (row-major BF16) into the blocked layout; rows >= n_src are zero
+__device__ void load_weights(unsigned char* dst, const __nv_bfloat16* src, int N, int K, int n_src) {
+    const int kch = K >> 3;
+    for (int c = threadIdx.x; c < N * kch; c += blockDim.x) {
+        const int r = c / kch, kc = c - r * kch;
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        if (r < n_src) v = *reinterpret_cast<const uint4*>(src + (size_t)r * K + 8 * kc);
+        *reinterpret_cast<uint4*>(dst + boff(r, kc, K)) = v;
+    }
+}
+}  // namespace tc
+
+__global__ void __launch_bounds__(128, 1)
+    k_mlp_infer_tc(int rows, const float* __restrict__ feat, const float* __restrict__ mean,
+                   const float* __restrict__ inv_std, const __nv_bfloat16* __restrict__ wt0,
+                   const __nv_bfloat16* __restrict__ wt1, const __nv_bfloat16* __restrict__ wt2,
+                   const __nv_bfloat16* __restrict__ wt3, const float* __restrict__ b0, const float* __restrict__ b1,
+                   const float* __restrict__ b2, const float* __restrict__ b3, float* __restrict__ Y,
+                   int* __restrict__ err) {
+    using namespace tc;
+    extern __shared__ __align__(128) unsigned char sm[];
+    const int tid = threadIdx.x, warp = tid >> 5;
+    load_weights(sm + W0_OFF, wt0, 128, 80, 128);
+    load_weights(sm + W1_OFF, wt1, 128, 128, 128);
+    load_weights(sm + W2_OFF, wt2, 128, 128, 128);
+    load_weights(sm + W3_OFF, wt3, 16, 128, 8);
+    float* bias = reinterpret_cast<float*>(sm + BIAS_OFF);
+    float* norm = reinterpret_cast<float*>(sm + NORM_OFF);
+    for (int i = tid; i < 128; i += blockDim.x) {
+        bias[i] = b0[i];
+        bias[128 + i] = b1[i];
+        bias[256 + i] = b2[i];
+    }
+    if (tid < 16) bias[384 + tid] = tid < 8 ? b3[tid] : 0.f;
+    for (int i = tid; i < MLP_IN; i += blockDim.x) {
+        norm[i] = mean[i];
+        norm[MLP_IN + i] = inv_std[i];
+    }
+    const unsigned sbase = (unsigned)__cvta_generic_to_shared(sm);
+    const unsigned mbar = sbase + MBAR_OFF;
+    volatile int* flag = reinterpret_cast<volatile int*>(sm + FLAG_OFF);
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sbase + TADDR_OFF),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(1));
+        *flag = 0;
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(sm + TADDR_OFF);
+    const uint32_t tmem_row = tmem + ((uint32_t)(32 * warp) << 16);   // this warp's 32 lanes
+    unsigned phase = 0;
+    const int n_tiles = (rows + ROWS - 1) / ROWS;
+    unsigned char* A = sm + A_OFF;
+    const unsigned a_addr = sbase + A_OFF;
+    bool ok = true;
+    for (int tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
+        const int row = tile * ROWS + tid;
+        // layer-1 input: this thread's row, normalised, K = 80 (68..79 zero)
+#pragma unroll 1
+        for (int kc = 0; kc < 10; ++kc) {
+            float v[8];
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                const int k = 8 * kc + e;
+                v[e] = (k < MLP_IN && row < rows) ? (feat[(size_t)row * MLP_IN + k] - norm[k]) * norm[MLP_IN + k] : 0.f;
+            }
+            uint4 u;
+            u.x = pack2(__float2bfloat16(v[0]), __float2bfloat16(v[1]));
+            u.y = pack2(__float2bfloat16(v[2]), __float2bfloat16(v[3]));
+            u.z = pack2(__float2bfloat16(v[4]), __float2bfloat16(v[5]));
+            u.w = pack2(__float2bfloat16(v[6]), __float2bfloat16(v[7]));
+            *reinterpret_cast<uint4*>(A + boff(tid, kc, 80)) = u;
+        }
+        fence_async_smem();
+        __syncthreads();
+#pragma unroll 1
+        for (int l = 0; l < 4; ++l) {
+            const int K = l == 0 ? 80 : 128, N = l == 3 ? 16 : 128;
+            if (tid == 0) {
+                const unsigned w_addr = sbase + (l == 0 ? W0_OFF : l == 1 ? W1_OFF : l == 2 ? W2_OFF : W3_OFF);
+                fence_after();
+                for (int ks = 0; ks < K / 16; ++ks)
+                    tc::mma(tmem, sdesc(a_addr + ks * 256, K), sdesc(w_addr + ks * 256, K), idesc(N), ks > 0);
+                commit(mbar);
+            }
+            // on a timeout `phase` stays the pending one, for the last wait below
+            if (wait_parity(mbar, phase)) phase ^= 1u;
+            else *flag = 1;
+            __syncthreads();
+            if (*flag) {
+                ok = false;
+                break;
+            }
+            fence_after();
+            if (l < 3) {
+                const float* bl = bias + 128 * l;
+#pragma unroll 1
+                for (int c = 0; c < 8; ++c) {
+                    float v[16];
+                    ld16(tmem_row + 16 * c, v);
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        uint4 u;
+                        const int b = 16 * c + 8 * h;
+                        u.x = pack2(__float2bfloat16(silu(v[8 * h + 0] + bl[b + 0])), __float2bfloat16(silu(v[8 * h + 1] + bl[b + 1])));
+                        u.y = pack2(__float2bfloat16(silu(v[8 * h + 2] + bl[b + 2])), __float2bfloat16(silu(v[8 * h + 3] + bl[b + 3])));
+                        u.z = pack2(__float2bfloat16(silu(v[8 * h + 4] + bl[b + 4])), __float2bfloat16(silu(v[8 * h + 5] + bl[b + 5])));
+                        u.w = pack2(__float2bfloat16(silu(v[8 * h + 6] + bl[b + 6])), __float2bfloat16(silu(v[8 * h + 7] + bl[b + 7])));
+                        *reinterpret_cast<uint4*>(A + boff(tid, 2 * c + h, 128)) = u;
+                    }
+                }
+            } else {
+                float v[16];
+                ld16(tmem_row, v);
+                if (row < rows) {
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) Y[(size_t)row * 8 + j] = v[j] + bias[384 + j];
+                }
+            }
+            fence_before();
+            fence_async_smem();
+            __syncthreads();
+        }
+    }
+    if (!ok) {
+        if (tid == 0) atomicExch(err, 1);
+        // let any MMA still in flight finish before the accumulator is freed
+        wait_parity(mbar, phase);
+    }
+    fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+    }
+}
+
 // ---------------------------------------------------------- model host side
 namespace {
 inline unsigned blocks(long long n, int tb) { return (unsigned)((n + tb - 1) / tb); }
@@ -388,6 +609,23 @@ int mlp_infer(const MlpModel& m, int rows, const float* feat, const float* mean,
     const int grid = std::max(1, std::min(sms, (tiles + INF_WARPS - 1) / INF_WARPS));
     k_mlp_infer<<<grid, INF_WARPS * 32, INF_SMEM, s>>>(rows, feat, mean, inv_std, m.wtb[0], m.wtb[1], m.wtb[2],
                                                        m.wtb[3], m.b[0], m.b[1], m.b[2], m.b[3], Y);
+    return 1;
+}
+
+int mlp_infer_tc(const MlpModel& m, int rows, const float* feat, const float* mean, const float* inv_std, float* Y,
+                 int* err, cudaStream_t s) {
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_mlp_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM);
+        attr_set = true;
+    }
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int tiles = (rows + tc::ROWS - 1) / tc::ROWS;
+    const int grid = std::max(1, std::min(sms, tiles));
+    k_mlp_infer_tc<<<grid, 128, tc::SMEM, s>>>(rows, feat, mean, inv_std, m.wtb[0], m.wtb[1], m.wtb[2], m.wtb[3],
+                                              m.b[0], m.b[1], m.b[2], m.b[3], Y, err);
     return 1;
 }
 

@@ -36,6 +36,8 @@ struct MlpModel {
     float* part = nullptr;        // weight-gradient partials
     float* bpart = nullptr;       // bias-gradient partials
     int max_rows = 0;             // rows the training buffers hold
+    int* tc_err = nullptr;        // set when a bounded wait of the tcgen05 kernel gave up
+    bool use_tc = true;           // inference on tcgen05 (else warp-level mma.sync)
     int adam_step = 0;
     float in_mean[MLP_IN] = {}, in_std[MLP_IN] = {};   // input normalisation
     float out_scale = 1.f;                             // residual scale [J/mol/nm]
@@ -53,6 +55,10 @@ void mlp_sync_bf16(MlpModel& m, cudaStream_t s);
 // inference of all four layers in one persistent kernel, inputs normalised on the fly
 int mlp_infer(const MlpModel& m, int rows, const float* feat, const float* mean, const float* inv_std, float* Y,
               cudaStream_t s);
+// the same on the tcgen05 tensor cores (TMEM accumulators); *err is set if a
+// bounded wait gave up
+int mlp_infer_tc(const MlpModel& m, int rows, const float* feat, const float* mean, const float* inv_std, float* Y,
+                 int* err, cudaStream_t s);
 int mlp_forward(const MlpModel& m, int rows, const __nv_bfloat16* X, MlpActs* acts, float* Y, cudaStream_t s);
 int mlp_train_step(MlpModel& m, int rows, const __nv_bfloat16* X, const float* T, MlpActs& a, float lr,
                    double* d_loss, cudaStream_t s);

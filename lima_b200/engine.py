@@ -38,7 +38,7 @@ EXPORTED = [
     "lima_get_timings", "lima_reset_timings", "lima_enable_phase_timing", "lima_pme_recip_noalloc",
     "lima_learned_pme_setup", "lima_learned_pme_collect", "lima_learned_pme_train", "lima_learned_pme_enable",
     "lima_learned_pme_eval", "lima_learned_pme_status", "lima_learned_pme_weights",
-    "lima_learned_pme_gradients", "lima_get_thermostat", "lima_get_log", "lima_clear_log",
+    "lima_learned_pme_gradients", "lima_learned_pme_predict", "lima_get_thermostat", "lima_get_log", "lima_clear_log",
 ]
 MLP_NPARAM = 80 * 128 + 128 + 2 * (128 * 128 + 128) + 128 * 8 + 8   # network parameters
 MLP_NSTATE = MLP_NPARAM + 2 * 68 + 1                               # + normalisation and output scale
@@ -127,6 +127,7 @@ def load_library(path: str = LIB_PATH):
                                                   ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                   ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p,
                                                   ctypes.c_void_p]),
+        "lima_learned_pme_predict": (ctypes.c_int, [h, ctypes.c_int, f32p, f32p, ctypes.c_int]),
         "lima_get_thermostat": (ctypes.c_int, [h, f64p, f64p, P(ctypes.c_int64)]),
         "lima_get_log": (ctypes.c_int, [h, ctypes.c_int64, ctypes.c_int64, P(ctypes.c_int64), f32p, f32p,
                                         P(ctypes.c_int64)]),
@@ -415,6 +416,14 @@ class LearnedPME:
     def set_weights(self, state):
         buf, ptr = _f32(np.asarray(state, np.float32).reshape(-1))
         self.engine._check(self.lib.lima_learned_pme_weights(self.engine.h, 0, ptr, buf.size, None))
+
+    def predict(self, features, impl: int = 0) -> np.ndarray:
+        """Network output (rows, 3) for raw feature rows (rows, 68); impl 0 = tcgen05
+        tensor-core kernel, 1 = warp-level mma.sync kernel."""
+        x, xp = _f32(features, 68)
+        y = np.zeros((len(x), 3), np.float32)
+        self.engine._check(self.lib.lima_learned_pme_predict(self.engine.h, len(x), xp, _f32(y)[1], int(impl)))
+        return y
 
     def gradients(self, x, t) -> tuple[float, np.ndarray]:
         """Loss and parameter gradients of one pass over caller rows (no update)."""

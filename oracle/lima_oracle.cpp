@@ -791,6 +791,37 @@ void orc_fft3d(int kx, int ky, int kz, double* data, int sign) {
     fft3d(kx, ky, kz, reinterpret_cast<cd*>(data), sign);
 }
 
+void orc_mlp_forward(int rows, const double* x, const double* params, double* y) {
+    const int K[4] = {80, 128, 128, 128}, N[4] = {128, 128, 128, 8};
+    const double* W[4];
+    const double* b[4];
+    size_t off = 0;
+    for (int l = 0; l < 4; ++l) {
+        W[l] = params + off;
+        off += (size_t)K[l] * N[l];
+        b[l] = params + off;
+        off += N[l];
+    }
+    std::vector<double> a(128), z(128);
+    for (int r = 0; r < rows; ++r) {
+        std::fill(a.begin(), a.end(), 0.0);
+        for (int k = 0; k < 68; ++k) a[k] = x[(size_t)r * 68 + k];
+        for (int l = 0; l < 3; ++l) {
+            for (int n = 0; n < N[l]; ++n) {
+                double s = b[l][n];
+                for (int k = 0; k < K[l]; ++k) s += a[k] * W[l][(size_t)k * N[l] + n];
+                z[n] = s / (1.0 + std::exp(-s));
+            }
+            std::copy(z.begin(), z.end(), a.begin());
+        }
+        for (int n = 0; n < 3; ++n) {
+            double s = b[3][n];
+            for (int k = 0; k < 128; ++k) s += a[k] * W[3][(size_t)k * 8 + n];
+            y[(size_t)r * 3 + n] = s;
+        }
+    }
+}
+
 double orc_mlp_grads(int rows, const double* x, const double* t, const double* params, double* grads) {
     const int K[4] = {80, 128, 128, 128}, N[4] = {128, 128, 128, 8}, nin = 68, nout = 3;
     const double* W[4];

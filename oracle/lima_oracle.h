@@ -147,6 +147,9 @@ void orc_fft3d(int kx, int ky, int kz, double* data, int sign);
  * grads with d loss / d params. */
 double orc_mlp_grads(int rows, const double* x, const double* t, const double* params, double* grads);
 
+/* FP64 forward pass of the same network: y[rows][3] from normalised inputs x[rows][68]. */
+void orc_mlp_forward(int rows, const double* x, const double* params, double* y);
+
 #ifdef __cplusplus
 }
 #endif

@@ -70,6 +70,8 @@ def lib():
         L.orc_exclusion_correction_atoms.restype = None
         L.orc_exclusion_correction_atoms.argtypes = [ctypes.c_int, _d, _d, _d, ctypes.c_int, _i,
                                                      ctypes.c_double, _d, _d, _d]
+        L.orc_mlp_forward.restype = None
+        L.orc_mlp_forward.argtypes = [ctypes.c_int, _d, _d, _d]
         L.orc_mlp_grads.restype = ctypes.c_double
         L.orc_mlp_grads.argtypes = [ctypes.c_int, _d, _d, _d, _d]
         _lib = L
@@ -273,3 +275,12 @@ def atom_energies(s, rc, kappa, grid):
     lib().orc_exclusion_correction_atoms(n, _dp(pos), _dp(q), _dp(box), len(xp), xp.ctypes.data_as(_i), kappa,
                                          _dp(f), ctypes.byref(ee), _dp(ae))
     return ae
+
+
+def mlp_forward(x, params):
+    """FP64 network output (rows, 3) for normalised inputs x (rows, 68)."""
+    x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1, 68)
+    params = np.ascontiguousarray(params, dtype=np.float64).reshape(-1)
+    y = np.zeros((len(x), 3))
+    lib().orc_mlp_forward(len(x), _dp(x), _dp(params), _dp(y))
+    return y

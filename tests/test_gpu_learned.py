@@ -106,3 +106,33 @@ def test_learned_step_check_and_fallback():
     assert e.status() & 0x20
     e.step(5)
     assert np.isfinite(e.energies()["total"])
+
+
+def test_inference_kernels_match_oracle(oracle):
+    """The tcgen05 (TMEM) inference kernel and the warp-level mma.sync one
+    against the FP64 forward pass, on BF16-rounded inputs and weights; 3,000
+    rows leave a partial last 128-row tile."""
+    s, e, lp = small_engine(frames=1)
+    e.step(5)
+    lp.collect()
+    rng = np.random.default_rng(7)
+    state = lp.weights()
+    params = state[: E.MLP_NPARAM].copy()
+    blocks = split_params(params)
+    blocks[6][:, :3] = rng.normal(scale=0.1, size=(128, 3))
+    blocks[7][:3] = rng.normal(scale=0.1, size=3)
+    for b in (1, 3, 5):
+        blocks[b][:] = rng.normal(scale=0.05, size=blocks[b].shape)
+    state[: E.MLP_NPARAM] = params
+    lp.set_weights(state)
+    mean = state[E.MLP_NPARAM:E.MLP_NPARAM + 68].astype(np.float32)
+    std = state[E.MLP_NPARAM + 68:E.MLP_NPARAM + 136].astype(np.float32)
+    feats = (mean + std * rng.normal(size=(3000, 68))).astype(np.float32)
+    xn = (feats - mean) * (np.float32(1.0) / std)
+    ref = oracle.mlp_forward(bf16(xn), bf16(params))
+    y_tc = lp.predict(feats, impl=0).astype(np.float64)
+    y_mma = lp.predict(feats, impl=1).astype(np.float64)
+    scale = np.sqrt((ref ** 2).mean())
+    assert np.sqrt(((y_mma - ref) ** 2).mean()) < 2e-2 * scale
+    assert np.sqrt(((y_tc - ref) ** 2).mean()) < 2e-2 * scale
+    assert np.sqrt(((y_tc - y_mma) ** 2).mean()) < 1e-2 * scale
