@@ -36,6 +36,14 @@ __device__ __forceinline__ uint32_t pack2(__nv_bfloat16 lo, __nv_bfloat16 hi) {
     return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
 }
 __device__ __forceinline__ float silu(float z) { return z / (1.f + __expf(-z)); }
+// inference epilogues: silu(z) = z/2 (1 + tanh(z/2)) with the hardware tanh
+// (PTX tanh.approx.f32, relative error ~2^-11, below the BF16 rounding of the result)
+__device__ __forceinline__ float silu_fast(float z) {
+    const float h = 0.5f * z;
+    float t;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(h));
+    return fmaf(h, t, h);
+}
 __device__ __forceinline__ float dsilu(float z) {
     const float s = 1.f / (1.f + __expf(-z));
     return s * (1.f + z * (1.f - s));
@@ -281,9 +289,9 @@ __device__ __forceinline__ void store_hidden(float (*acc)[4], const float* bias,
         const int c = 8 * n + 2 * t;
         const float b0 = bias[c], b1 = bias[c + 1];
         *reinterpret_cast<uint32_t*>(H + (size_t)g * LDH + c) =
-            pack2(__float2bfloat16(silu(acc[n][0] + b0)), __float2bfloat16(silu(acc[n][1] + b1)));
+            pack2(__float2bfloat16(silu_fast(acc[n][0] + b0)), __float2bfloat16(silu_fast(acc[n][1] + b1)));
         *reinterpret_cast<uint32_t*>(H + (size_t)(g + 8) * LDH + c) =
-            pack2(__float2bfloat16(silu(acc[n][2] + b0)), __float2bfloat16(silu(acc[n][3] + b1)));
+            pack2(__float2bfloat16(silu_fast(acc[n][2] + b0)), __float2bfloat16(silu_fast(acc[n][3] + b1)));
     }
 }
 
@@ -374,19 +382,21 @@ __global__ void __launch_bounds__(INF_WARPS * 32, 1)
 // timeout the kernel records an error, waits (bounded) once more for its MMAs
 // and frees its TMEM before returning.
 namespace tc {
-constexpr int ROWS = 128;
+constexpr int ROWS = 128;                              // rows per tile = TMEM lanes = one warpgroup
+constexpr int GROUPS = 4;                              // warpgroups per CTA, each on its own tiles
 constexpr int W0_OFF = 0;                              // N 128 x K 80
 constexpr int W1_OFF = W0_OFF + 128 * 80 * 2;          // N 128 x K 128
 constexpr int W2_OFF = W1_OFF + 128 * 128 * 2;
 constexpr int W3_OFF = W2_OFF + 128 * 128 * 2;         // N 16 x K 128 (rows 8..15 zero)
-constexpr int A_OFF = W3_OFF + 16 * 128 * 2;           // 128 rows x K <= 128
-constexpr int BIAS_OFF = A_OFF + ROWS * 128 * 2;       // 3 x 128 + 16 floats
+constexpr int A_OFF = W3_OFF + 16 * 128 * 2;           // per group: 128 rows x K <= 128
+constexpr int A_BYTES = ROWS * 128 * 2;
+constexpr int BIAS_OFF = A_OFF + GROUPS * A_BYTES;     // 3 x 128 + 16 floats
 constexpr int NORM_OFF = BIAS_OFF + (3 * 128 + 16) * 4;
-constexpr int MBAR_OFF = NORM_OFF + 2 * MLP_IN * 4;    // 8-byte aligned
-constexpr int TADDR_OFF = MBAR_OFF + 8;
-constexpr int FLAG_OFF = TADDR_OFF + 4;
-constexpr int SMEM = FLAG_OFF + 4;
-constexpr int TMEM_COLS = 128;
+constexpr int MBAR_OFF = NORM_OFF + 2 * MLP_IN * 4;    // one mbarrier per group, 8-byte aligned
+constexpr int TADDR_OFF = MBAR_OFF + 8 * GROUPS;
+constexpr int FLAG_OFF = TADDR_OFF + 4;                // one flag per group
+constexpr int SMEM = FLAG_OFF + 4 * GROUPS;
+constexpr int TMEM_COLS = 128 * GROUPS;
 constexpr unsigned WAIT_LIMIT = 1u << 20;
 static_assert(MBAR_OFF % 8 == 0, "mbarrier alignment");
 static_assert(A_OFF % 16 == 0 && W3_OFF % 16 == 0, "16-byte aligned operands");
@@ -424,20 +434,20 @@ __device__ __forceinline__ bool wait_parity(unsigned mbar, unsigned parity) {
     }
     return false;
 }
-__device__ __forceinline__ void ld16(uint32_t taddr, float* v) {
-    uint32_t r[16];
+// 16 columns of this thread's TMEM lane; the caller waits with ld_wait()
+__device__ __forceinline__ void ld16(uint32_t taddr, uint32_t* r) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
           "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
         : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
 }
+__device__ __forceinline__ void ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// barrier of one warpgroup (named barrier 1 + g, 128 threads)
+__device__ __forceinline__ void group_sync(int g) { asm volatile("bar.sync %0, 128;" ::"r"(1 + g) : "memory"); }
 
 // weights W^T[N][K] (row-major BF16) into the blocked layout; rows >= n_src are zero
 __device__ void load_weights(unsigned char* dst, const __nv_bfloat16* src, int N, int K, int n_src) {
@@ -451,7 +461,7 @@ __device__ void load_weights(unsigned char* dst, const __nv_bfloat16* src, int N
 }
 }  // namespace tc
 
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(128 * tc::GROUPS, 1)
     k_mlp_infer_tc(int rows, const float* __restrict__ feat, const float* __restrict__ mean,
                    const float* __restrict__ inv_std, const __nv_bfloat16* __restrict__ wt0,
                    const __nv_bfloat16* __restrict__ wt1, const __nv_bfloat16* __restrict__ wt2,
@@ -460,7 +470,8 @@ __global__ void __launch_bounds__(128, 1)
                    int* __restrict__ err) {
     using namespace tc;
     extern __shared__ __align__(128) unsigned char sm[];
-    const int tid = threadIdx.x, warp = tid >> 5;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int g = tid / ROWS, gt = tid % ROWS;            // warpgroup, thread (= tile row) in it
     load_weights(sm + W0_OFF, wt0, 128, 80, 128);
     load_weights(sm + W1_OFF, wt1, 128, 128, 128);
     load_weights(sm + W2_OFF, wt2, 128, 128, 128);
@@ -478,51 +489,60 @@ __global__ void __launch_bounds__(128, 1)
         norm[MLP_IN + i] = inv_std[i];
     }
     const unsigned sbase = (unsigned)__cvta_generic_to_shared(sm);
-    const unsigned mbar = sbase + MBAR_OFF;
-    volatile int* flag = reinterpret_cast<volatile int*>(sm + FLAG_OFF);
+    const unsigned mbar = sbase + MBAR_OFF + 8 * g;
+    volatile int* flag = reinterpret_cast<volatile int*>(sm + FLAG_OFF) + g;
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sbase + TADDR_OFF),
                      "r"(TMEM_COLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
     }
-    if (tid == 0) {
+    if (gt == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(1));
         *flag = 0;
     }
     fence_before();
     __syncthreads();
     fence_after();
-    const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(sm + TADDR_OFF);
-    const uint32_t tmem_row = tmem + ((uint32_t)(32 * warp) << 16);   // this warp's 32 lanes
+    const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(sm + TADDR_OFF) + 128u * g;   // this group's columns
+    const uint32_t tmem_row = tmem + ((uint32_t)(32 * (warp & 3)) << 16);   // this warp's 32 lanes
     unsigned phase = 0;
     const int n_tiles = (rows + ROWS - 1) / ROWS;
-    unsigned char* A = sm + A_OFF;
-    const unsigned a_addr = sbase + A_OFF;
+    unsigned char* A = sm + A_OFF + g * A_BYTES;
+    const unsigned a_addr = sbase + A_OFF + g * A_BYTES;
+    const int wr0 = 32 * (warp & 3);                      // this warp's first row in the tile
     bool ok = true;
-    for (int tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
-        const int row = tile * ROWS + tid;
-        // layer-1 input: this thread's row, normalised, K = 80 (68..79 zero)
-#pragma unroll 1
-        for (int kc = 0; kc < 10; ++kc) {
-            float v[8];
-#pragma unroll
-            for (int e = 0; e < 8; ++e) {
-                const int k = 8 * kc + e;
-                v[e] = (k < MLP_IN && row < rows) ? (feat[(size_t)row * MLP_IN + k] - norm[k]) * norm[MLP_IN + k] : 0.f;
+    for (int tile = GROUPS * blockIdx.x + g; tile < n_tiles && ok; tile += GROUPS * gridDim.x) {
+        const int row = tile * ROWS + gt;
+        // layer-1 input: the warp's 32 rows read as one contiguous block (coalesced),
+        // normalised, K = 80 with 68..79 zero
+        const size_t blk = (size_t)(tile * ROWS + wr0) * MLP_IN;
+        const int nrow_w = min(32, rows - (tile * ROWS + wr0));
+        // a row is 17 float4 (272 B, 16-byte aligned); four features -> one 8-byte store
+        constexpr int Q = MLP_IN / 4;
+#pragma unroll 4
+        for (int i = lane; i < 32 * Q; i += 32) {
+            const int r = i / Q, k = 4 * (i - r * Q);
+            float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (r < nrow_w) {
+                f = *reinterpret_cast<const float4*>(feat + blk + (size_t)r * MLP_IN + k);
+                f.x = (f.x - norm[k]) * norm[MLP_IN + k];
+                f.y = (f.y - norm[k + 1]) * norm[MLP_IN + k + 1];
+                f.z = (f.z - norm[k + 2]) * norm[MLP_IN + k + 2];
+                f.w = (f.w - norm[k + 3]) * norm[MLP_IN + k + 3];
             }
-            uint4 u;
-            u.x = pack2(__float2bfloat16(v[0]), __float2bfloat16(v[1]));
-            u.y = pack2(__float2bfloat16(v[2]), __float2bfloat16(v[3]));
-            u.z = pack2(__float2bfloat16(v[4]), __float2bfloat16(v[5]));
-            u.w = pack2(__float2bfloat16(v[6]), __float2bfloat16(v[7]));
-            *reinterpret_cast<uint4*>(A + boff(tid, kc, 80)) = u;
+            *reinterpret_cast<uint2*>(A + boff(wr0 + r, k >> 3, 80) + (k & 7) * 2) =
+                make_uint2(pack2(__float2bfloat16(f.x), __float2bfloat16(f.y)),
+                           pack2(__float2bfloat16(f.z), __float2bfloat16(f.w)));
         }
+        // zero padding k = 68..79 of this thread's row (chunk 8 half, chunk 9)
+        *reinterpret_cast<uint2*>(A + boff(gt, 8, 80) + 8) = make_uint2(0u, 0u);
+        *reinterpret_cast<uint4*>(A + boff(gt, 9, 80)) = make_uint4(0u, 0u, 0u, 0u);
         fence_async_smem();
-        __syncthreads();
+        group_sync(g);
 #pragma unroll 1
         for (int l = 0; l < 4; ++l) {
             const int K = l == 0 ? 80 : 128, N = l == 3 ? 16 : 128;
-            if (tid == 0) {
+            if (gt == 0) {
                 const unsigned w_addr = sbase + (l == 0 ? W0_OFF : l == 1 ? W1_OFF : l == 2 ? W2_OFF : W3_OFF);
                 fence_after();
                 for (int ks = 0; ks < K / 16; ++ks)
@@ -532,7 +552,7 @@ __global__ void __launch_bounds__(128, 1)
             // on a timeout `phase` stays the pending one, for the last wait below
             if (wait_parity(mbar, phase)) phase ^= 1u;
             else *flag = 1;
-            __syncthreads();
+            group_sync(g);
             if (*flag) {
                 ok = false;
                 break;
@@ -541,35 +561,43 @@ __global__ void __launch_bounds__(128, 1)
             if (l < 3) {
                 const float* bl = bias + 128 * l;
 #pragma unroll 1
-                for (int c = 0; c < 8; ++c) {
-                    float v[16];
-                    ld16(tmem_row + 16 * c, v);
+                for (int c4 = 0; c4 < 2; ++c4) {
+                    uint32_t r[4][16];
 #pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        uint4 u;
-                        const int b = 16 * c + 8 * h;
-                        u.x = pack2(__float2bfloat16(silu(v[8 * h + 0] + bl[b + 0])), __float2bfloat16(silu(v[8 * h + 1] + bl[b + 1])));
-                        u.y = pack2(__float2bfloat16(silu(v[8 * h + 2] + bl[b + 2])), __float2bfloat16(silu(v[8 * h + 3] + bl[b + 3])));
-                        u.z = pack2(__float2bfloat16(silu(v[8 * h + 4] + bl[b + 4])), __float2bfloat16(silu(v[8 * h + 5] + bl[b + 5])));
-                        u.w = pack2(__float2bfloat16(silu(v[8 * h + 6] + bl[b + 6])), __float2bfloat16(silu(v[8 * h + 7] + bl[b + 7])));
-                        *reinterpret_cast<uint4*>(A + boff(tid, 2 * c + h, 128)) = u;
-                    }
+                    for (int q = 0; q < 4; ++q) ld16(tmem_row + 64 * c4 + 16 * q, r[q]);
+                    ld_wait();
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            const int b = 64 * c4 + 16 * q + 8 * h;
+                            float v[8];
+#pragma unroll
+                            for (int e = 0; e < 8; ++e) v[e] = silu_fast(__uint_as_float(r[q][8 * h + e]) + bl[b + e]);
+                            uint4 u;
+                            u.x = pack2(__float2bfloat16(v[0]), __float2bfloat16(v[1]));
+                            u.y = pack2(__float2bfloat16(v[2]), __float2bfloat16(v[3]));
+                            u.z = pack2(__float2bfloat16(v[4]), __float2bfloat16(v[5]));
+                            u.w = pack2(__float2bfloat16(v[6]), __float2bfloat16(v[7]));
+                            *reinterpret_cast<uint4*>(A + boff(gt, b >> 3, 128)) = u;
+                        }
                 }
             } else {
-                float v[16];
-                ld16(tmem_row, v);
+                uint32_t r[16];
+                ld16(tmem_row, r);
+                ld_wait();
                 if (row < rows) {
 #pragma unroll
-                    for (int j = 0; j < 8; ++j) Y[(size_t)row * 8 + j] = v[j] + bias[384 + j];
+                    for (int j = 0; j < 8; ++j) Y[(size_t)row * 8 + j] = __uint_as_float(r[j]) + bias[384 + j];
                 }
             }
             fence_before();
             fence_async_smem();
-            __syncthreads();
+            group_sync(g);
         }
     }
     if (!ok) {
-        if (tid == 0) atomicExch(err, 1);
+        if (gt == 0) atomicExch(err, 1);
         // let any MMA still in flight finish before the accumulator is freed
         wait_parity(mbar, phase);
     }
@@ -577,7 +605,8 @@ __global__ void __launch_bounds__(128, 1)
     __syncthreads();
     if (warp == 0) {
         fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
+                     ::"r"(*reinterpret_cast<volatile uint32_t*>(sm + TADDR_OFF)), "r"(TMEM_COLS));
     }
 }
 
@@ -623,8 +652,8 @@ int mlp_infer_tc(const MlpModel& m, int rows, const float* feat, const float* me
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int tiles = (rows + tc::ROWS - 1) / tc::ROWS;
-    const int grid = std::max(1, std::min(sms, tiles));
-    k_mlp_infer_tc<<<grid, 128, tc::SMEM, s>>>(rows, feat, mean, inv_std, m.wtb[0], m.wtb[1], m.wtb[2], m.wtb[3],
+    const int grid = std::max(1, std::min(sms, (tiles + tc::GROUPS - 1) / tc::GROUPS));
+    k_mlp_infer_tc<<<grid, 128 * tc::GROUPS, tc::SMEM, s>>>(rows, feat, mean, inv_std, m.wtb[0], m.wtb[1], m.wtb[2], m.wtb[3],
                                               m.b[0], m.b[1], m.b[2], m.b[3], Y, err);
     return 1;
 }
