@@ -524,9 +524,14 @@ void lima_engine::setup() {
     if (st.pl_cap > pl_cap) pl_cap = st.pl_cap;  // keep a capacity grown earlier
 
     // ---- device allocation
-    CK(cudaStreamCreateWithFlags(&s_main, cudaStreamNonBlocking));
-    CK(cudaStreamCreateWithFlags(&s_bonded, cudaStreamNonBlocking));
-    CK(cudaStreamCreateWithFlags(&s_pme, cudaStreamNonBlocking));
+    // The PME chain and the bonded terms are short, latency-bound kernels; at a
+    // higher priority their blocks take SMs as soon as pair-kernel blocks retire
+    // instead of queueing behind the whole pair kernel.
+    int prio_low = 0, prio_high = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
+    CK(cudaStreamCreateWithPriority(&s_main, cudaStreamNonBlocking, prio_low));
+    CK(cudaStreamCreateWithPriority(&s_bonded, cudaStreamNonBlocking, prio_high));
+    CK(cudaStreamCreateWithPriority(&s_pme, cudaStreamNonBlocking, prio_high));
     CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&ev_bonded, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&ev_pme, cudaEventDisableTiming));
