@@ -683,7 +683,7 @@ PmePlan lima_engine::make_pme(std::vector<SysDesc>& sd, DevState& D) {
     std::vector<float> theta(pme_coff, 0.f);
     std::vector<char> plans(pme_sys_dev_size() * ns, 0);
     std::vector<int4> ix, iy, iz;
-    const int XL = 8, TX = 16;
+    const int XL = PME_FFT_XLINES, TX = PME_FFT_TX;
     for (int s = 0; s < ns; ++s) {
         const SysDesc& Dd = sd[s];
         if (Dd.pme_n[0] == 0) {

@@ -122,6 +122,8 @@ int launch_pairlist_dump(const DevState& st, const NbParams& p, long long cap, i
 // bonded.cu
 int launch_bonded(const DevState& st, const BondedTerms& bt, bool energy, cudaStream_t s);
 // pme.cu
+constexpr int PME_FFT_TX = 16;       // half-complex columns per CTA of the y and z passes
+constexpr int PME_FFT_XLINES = 8;    // lines per CTA of the x passes
 struct PmePlan {
     int n_items_x = 0, n_items_y = 0, n_items_z = 0;   // work items per FFT pass
     int4* items_x = nullptr;     // (system, line0, nlines, 0)

@@ -24,8 +24,9 @@
 namespace lima {
 
 constexpr int FFT_MAXN = 256;
-constexpr int FFT_TX = 16;      // columns per y/z tile
-constexpr int FFT_XLINES = 8;   // lines per x-pass CTA
+constexpr int FFT_TX = PME_FFT_TX;          // columns per y/z tile
+constexpr int FFT_XLINES = PME_FFT_XLINES;  // lines per x-pass CTA
+constexpr int FFT_YZ_THREADS = 256;         // threads per y/z tile
 
 struct FftPlanDev {
     int n;
@@ -514,9 +515,9 @@ int launch_pme(const DevState& st, const PmePlan& plan, bool energy, cudaStream_
     const int g4 = (int)(((long long)st.n_slots * 4 + TB - 1) / TB);
     k_spread<<<g4, TB, 0, s>>>(st);
     k_fft_x_fwd<<<plan.n_items_x, 256, sx, s>>>(st, plans, plan.items_x, mx);
-    k_fft_y<<<plan.n_items_y, 256, sy, s>>>(st, plans, plan.items_y, -1.f, mx);
-    k_fft_z_conv<<<plan.n_items_z, 256, sy, s>>>(st, plans, plan.items_z, mx);
-    k_fft_y<<<plan.n_items_y, 256, sy, s>>>(st, plans, plan.items_y, 1.f, mx);
+    k_fft_y<<<plan.n_items_y, FFT_YZ_THREADS, sy, s>>>(st, plans, plan.items_y, -1.f, mx);
+    k_fft_z_conv<<<plan.n_items_z, FFT_YZ_THREADS, sy, s>>>(st, plans, plan.items_z, mx);
+    k_fft_y<<<plan.n_items_y, FFT_YZ_THREADS, sy, s>>>(st, plans, plan.items_y, 1.f, mx);
     k_fft_x_inv<<<plan.n_items_x, 256, sx, s>>>(st, plans, plan.items_x, mx);
     if (plan.ref_gather) {
         if (energy) k_gather<true, true><<<g4, TB, 0, s>>>(st);
