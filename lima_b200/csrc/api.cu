@@ -767,7 +767,24 @@ PmePlan lima_engine::make_pme(std::vector<SysDesc>& sd, DevState& D) {
     P.n_items_z = (int)iz.size();
     P.ref_gather = p.ref_compat ? 1 : 0;
     P.max_n = max_n;
-    pme_set_smem_limits(max_n);
+    // plane-fused x+y passes when every system's planes fit in shared memory
+    int xy_buf = 0;
+    bool xy_ok = true;
+    std::vector<int4> ixy;
+    for (int s = 0; s < ns; ++s) {
+        const int* g = sd[s].pme_n;
+        if (g[0] == 0) continue;
+        const int b = pme_xy_buffer(g[0], g[1]);
+        if (b == 0) xy_ok = false;
+        xy_buf = std::max(xy_buf, b);
+        for (int z = 0; z < g[2]; ++z) ixy.push_back(make_int4(s, z, 0, 0));
+    }
+    if (xy_ok && !ixy.empty()) {
+        P.items_xy = upload(ixy);
+        P.n_items_xy = (int)ixy.size();
+        P.xy_buf = xy_buf;
+    }
+    pme_set_smem_limits(max_n, P.n_items_xy > 0 ? xy_buf : 0);
     return P;
 }
 

@@ -132,11 +132,19 @@ struct PmePlan {
     const void* sys_plans = nullptr;  // per-system radix plans (device)
     int ref_gather = 0;          // central-difference gather
     int max_n = 0;
+    // plane-fused x+y passes (one CTA per z-plane), used when every plane fits
+    // in shared memory; otherwise the separate x and y passes run
+    int n_items_xy = 0;
+    int4* items_xy = nullptr;    // (system, z, 0, 0)
+    int xy_buf = 0;              // float2 elements per ping-pong buffer
 };
+// shared-memory elements of one buffer of the plane-fused x+y passes for a
+// K0 x K1 plane (0 = does not fit)
+int pme_xy_buffer(int k0, int k1);
 size_t pme_sys_dev_size();
 bool fill_pme_sys_dev(void* dst, int kx, int ky, int kz);
 void set_pme_sys_twiddles(void* dst, int offx, int offy, int offz);
-void pme_set_smem_limits(int maxn);
+void pme_set_smem_limits(int maxn, int xy_buf);
 int launch_pme(const DevState& st, const PmePlan& plan, bool energy, cudaStream_t s);
 // integrate.cu
 struct IntegrateParams {

@@ -16,6 +16,7 @@
 // B-spline weights sit on nodes floor(u)-1..floor(u)+2 exactly as in
 // ChargeblockDistributeToGrid (PME.cuh:249-300) and LAL::CalcBspline
 // (DeviceAlgorithmsPrivate.cuh:7-30).
+#include <algorithm>
 #include <mutex>
 
 #include "engine.h"
@@ -407,6 +408,126 @@ __global__ void k_fft_z_conv(DevState st, const PmeSysDev* plans, const int4* it
     }
 }
 
+// ------------------------------------------------------- plane-fused x+y
+// One CTA per z-plane.  Forward: the plane's K1 real rows are packed two per
+// complex line (row 2p + i row 2p+1), transformed along x, separated with the
+// symmetry of real transforms (X_a[k] = (Z[k] + conj Z[-k]) / 2,
+// X_b[k] = -i (Z[k] - conj Z[-k]) / 2) straight into y-lines, transformed along
+// y and written as the half-complex plane.  Inverse: the reverse, ending with
+// the two real rows of each line in its real and imaginary parts.
+constexpr int FFT_XY_THREADS = 512;
+
+__device__ __forceinline__ int xy_lines(int k1) { return (k1 + 1) / 2; }
+
+__global__ void __launch_bounds__(FFT_XY_THREADS) k_fft_xy_fwd(DevState st, const PmeSysDev* plans, const int4* items,
+                                                               int maxn, int buf) {
+    extern __shared__ float2 sm[];
+    const int4 it = items[blockIdx.x];
+    const SysDesc& sd = st.sys[it.x];
+    const FftPlanDev& plx = plans[it.x].px;
+    const FftPlanDev& ply = plans[it.x].py;
+    const int K0 = plx.n, K1 = ply.n, K0h = K0 / 2 + 1, P = xy_lines(K1), z = it.y;
+    float2* twx = sm;
+    float2* twy = sm + maxn;
+    float2* A = sm + 2 * maxn;
+    float2* B = A + buf;
+    load_twiddles(twx, plx, st.pme_tw);
+    load_twiddles(twy, ply, st.pme_tw);
+    const long long* g = st.pme_grid_fx + sd.pme_off + (size_t)K0 * K1 * z;
+    const int sx = K0 + 1, sy = K1 + 1;
+    block_copy4<float2>(
+        P * K0,
+        [&](int i) {
+            const int pl = i / K0, x = i - pl * K0;
+            const int ya = 2 * pl, yb = ya + 1;
+            const float a = (float)((double)g[(size_t)ya * K0 + x] * (1.0 / GRID_SCALE));
+            const float b = yb < K1 ? (float)((double)g[(size_t)yb * K0 + x] * (1.0 / GRID_SCALE)) : 0.f;
+            return make_float2(a, b);
+        },
+        [&](int i, float2 v) {
+            const int pl = i / K0, x = i - pl * K0;
+            A[pl * sx + x] = v;
+        });
+    __syncthreads();
+    const float2* res = fft_lines(A, B, P, sx, plx, twx, -1.f);
+    float2* yl = res == A ? B : A;
+    for (int i = threadIdx.x; i < P * K0h; i += blockDim.x) {
+        const int pl = i / K0h, k = i - pl * K0h;
+        const float2 Z = res[pl * sx + k];
+        const float2 Zm = res[pl * sx + (k == 0 ? 0 : K0 - k)];
+        yl[k * sy + 2 * pl] = make_float2(0.5f * (Z.x + Zm.x), 0.5f * (Z.y - Zm.y));
+        if (2 * pl + 1 < K1) yl[k * sy + 2 * pl + 1] = make_float2(0.5f * (Z.y + Zm.y), -0.5f * (Z.x - Zm.x));
+    }
+    __syncthreads();
+    const float2* out = fft_lines(yl, const_cast<float2*>(res), K0h, sy, ply, twy, -1.f);
+    float2* gc = st.pme_cplx + sd.pme_coff + (size_t)K0h * K1 * z;
+    for (int i = threadIdx.x; i < K1 * K0h; i += blockDim.x) {
+        const int y = i / K0h, x = i - y * K0h;
+        gc[(size_t)y * K0h + x] = out[x * sy + y];
+    }
+}
+
+__global__ void __launch_bounds__(FFT_XY_THREADS) k_fft_xy_inv(DevState st, const PmeSysDev* plans, const int4* items,
+                                                               int maxn, int buf) {
+    extern __shared__ float2 sm[];
+    const int4 it = items[blockIdx.x];
+    const SysDesc& sd = st.sys[it.x];
+    const FftPlanDev& plx = plans[it.x].px;
+    const FftPlanDev& ply = plans[it.x].py;
+    const int K0 = plx.n, K1 = ply.n, K0h = K0 / 2 + 1, P = xy_lines(K1), z = it.y;
+    float2* twx = sm;
+    float2* twy = sm + maxn;
+    float2* A = sm + 2 * maxn;
+    float2* B = A + buf;
+    load_twiddles(twx, plx, st.pme_tw);
+    load_twiddles(twy, ply, st.pme_tw);
+    const float2* gc = st.pme_cplx + sd.pme_coff + (size_t)K0h * K1 * z;
+    const int sx = K0 + 1, sy = K1 + 1;
+    block_copy4<float2>(
+        K1 * K0h, [&](int i) { return gc[i]; },
+        [&](int i, float2 v) {
+            const int y = i / K0h, x = i - y * K0h;
+            A[x * sy + y] = v;
+        });
+    __syncthreads();
+    const float2* res = fft_lines(A, B, K0h, sy, ply, twy, 1.f);
+    float2* xl = res == A ? B : A;
+    // full spectra of rows 2p and 2p+1 (Hermitian symmetry beyond K0h), packed as a + i b
+    for (int i = threadIdx.x; i < P * K0; i += blockDim.x) {
+        const int pl = i / K0, k = i - pl * K0;
+        const int ya = 2 * pl, yb = ya + 1;
+        float2 a, b = make_float2(0.f, 0.f);
+        if (k < K0h) {
+            a = res[k * sy + ya];
+            if (yb < K1) b = res[k * sy + yb];
+        } else {
+            a = res[(K0 - k) * sy + ya];
+            a.y = -a.y;
+            if (yb < K1) {
+                b = res[(K0 - k) * sy + yb];
+                b.y = -b.y;
+            }
+        }
+        xl[pl * sx + k] = make_float2(a.x - b.y, a.y + b.x);
+    }
+    __syncthreads();
+    const float2* out = fft_lines(xl, const_cast<float2*>(res), P, sx, plx, twx, 1.f);
+    float* gr = st.pme_real + sd.pme_off + (size_t)K0 * K1 * z;
+    for (int i = threadIdx.x; i < K1 * K0; i += blockDim.x) {
+        const int y = i / K0, x = i - y * K0;
+        const float2 v = out[(y >> 1) * sx + x];
+        gr[(size_t)y * K0 + x] = (y & 1) ? v.y : v.x;
+    }
+}
+
+int pme_xy_buffer(int k0, int k1) {
+    const int k0h = k0 / 2 + 1, P = (k1 + 1) / 2;
+    const int buf = std::max(P * (k0 + 1), k0h * (k1 + 1));
+    // two ping-pong buffers and two twiddle tables within ~200 KB
+    if ((size_t)(2 * buf + 2 * FFT_MAXN) * sizeof(float2) > 200 * 1024) return 0;
+    return (buf + 1) & ~1;
+}
+
 // ------------------------------------------------------------------ gather
 // four threads per atom, one z-plane each; partial sums combined with shuffles
 template <bool ENERGY, bool FD>
@@ -514,11 +635,20 @@ int launch_pme(const DevState& st, const PmePlan& plan, bool energy, cudaStream_
     cudaMemsetAsync(st.pme_grid_fx, 0, sizeof(long long) * (size_t)st.pme_total_real, s);
     const int g4 = (int)(((long long)st.n_slots * 4 + TB - 1) / TB);
     k_spread<<<g4, TB, 0, s>>>(st);
-    k_fft_x_fwd<<<plan.n_items_x, 256, sx, s>>>(st, plans, plan.items_x, mx);
-    k_fft_y<<<plan.n_items_y, FFT_YZ_THREADS, sy, s>>>(st, plans, plan.items_y, -1.f, mx);
-    k_fft_z_conv<<<plan.n_items_z, FFT_YZ_THREADS, sy, s>>>(st, plans, plan.items_z, mx);
-    k_fft_y<<<plan.n_items_y, FFT_YZ_THREADS, sy, s>>>(st, plans, plan.items_y, 1.f, mx);
-    k_fft_x_inv<<<plan.n_items_x, 256, sx, s>>>(st, plans, plan.items_x, mx);
+    int n = 7;
+    if (plan.n_items_xy > 0) {
+        const size_t sxy = (size_t)(2 * mx + 2 * plan.xy_buf) * sizeof(float2);
+        k_fft_xy_fwd<<<plan.n_items_xy, FFT_XY_THREADS, sxy, s>>>(st, plans, plan.items_xy, mx, plan.xy_buf);
+        k_fft_z_conv<<<plan.n_items_z, FFT_YZ_THREADS, sy, s>>>(st, plans, plan.items_z, mx);
+        k_fft_xy_inv<<<plan.n_items_xy, FFT_XY_THREADS, sxy, s>>>(st, plans, plan.items_xy, mx, plan.xy_buf);
+        n = 5;
+    } else {
+        k_fft_x_fwd<<<plan.n_items_x, 256, sx, s>>>(st, plans, plan.items_x, mx);
+        k_fft_y<<<plan.n_items_y, FFT_YZ_THREADS, sy, s>>>(st, plans, plan.items_y, -1.f, mx);
+        k_fft_z_conv<<<plan.n_items_z, FFT_YZ_THREADS, sy, s>>>(st, plans, plan.items_z, mx);
+        k_fft_y<<<plan.n_items_y, FFT_YZ_THREADS, sy, s>>>(st, plans, plan.items_y, 1.f, mx);
+        k_fft_x_inv<<<plan.n_items_x, 256, sx, s>>>(st, plans, plan.items_x, mx);
+    }
     if (plan.ref_gather) {
         if (energy) k_gather<true, true><<<g4, TB, 0, s>>>(st);
         else k_gather<false, true><<<g4, TB, 0, s>>>(st);
@@ -526,7 +656,7 @@ int launch_pme(const DevState& st, const PmePlan& plan, bool energy, cudaStream_
         if (energy) k_gather<true, false><<<g4, TB, 0, s>>>(st);
         else k_gather<false, false><<<g4, TB, 0, s>>>(st);
     }
-    return 7;
+    return n;
 }
 
 // Host helper: radix plan for an FFT length (4s first, then 2, 3, 5).
@@ -566,7 +696,14 @@ void set_pme_sys_twiddles(void* dst, int offx, int offy, int offz) {
 
 // The attribute is per kernel and process-wide: it only ever grows, so an
 // engine with small grids cannot shrink the room another engine relies on.
-void pme_set_smem_limits(int maxn) {
+void pme_set_smem_limits(int maxn, int xy_buf) {
+    static int largest_xy = 0;
+    if (xy_buf > largest_xy) {
+        largest_xy = xy_buf;
+        const int b = (int)((size_t)(2 * FFT_MAXN + 2 * xy_buf) * sizeof(float2));
+        cudaFuncSetAttribute(k_fft_xy_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+        cudaFuncSetAttribute(k_fft_xy_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    }
     static int largest = 0;
     if (maxn <= largest) return;
     largest = maxn;
