@@ -398,20 +398,17 @@ def run_lima(args):
 
     # ---- end to end through the C-ABI with host buffers: set_state -> step -> get_state
     n_e2e = min(args.steps, 50)
-    pos_h = torch.from_numpy(s.pos.copy()).pin_memory().numpy()
-    vel_h = torch.from_numpy(s.vel.copy()).pin_memory().numpy()
-    p_cur, v_cur = eng.state()
-    np.copyto(pos_h, p_cur)
-    np.copyto(vel_h, v_cur)
+    # pinned host buffers: the caller's state goes in and comes back through them
+    pos_h = torch.from_numpy(s.pos.astype(np.float64)).pin_memory().numpy()
+    vel_h = torch.from_numpy(s.vel.astype(np.float32)).pin_memory().numpy()
+    eng.state(pos_h, vel_h)
     barrier()
     t0 = time.perf_counter()
     for k in range(n_e2e):
         eng.set_state(pos_h, vel_h)
         eng.step(1)
-        p_cur, v_cur = eng.state()
+        eng.state(pos_h, vel_h)
         en = eng.energies()
-        np.copyto(pos_h, p_cur)
-        np.copyto(vel_h, v_cur)
     barrier()
     e2e_s = (time.perf_counter() - t0) / n_e2e
     if dist is not None:

@@ -107,6 +107,8 @@ struct lima_engine {
     int64_t timed_steps = 0;
 
     // device scratch for readback
+    unsigned* d_disp = nullptr;       // largest squared move since the last list build (float bits)
+    int64_t state_fast_loads = 0;     // lima_set_state calls served without a rebuild
     double* d_out_d = nullptr;
     float* d_out_f = nullptr;
     float* d_maxf = nullptr;
@@ -599,6 +601,7 @@ void lima_engine::setup() {
     D.status = dalloc<unsigned>(1);
     D.energy = dalloc<long long>((size_t)ns * E_COUNT);
     D.epot = dalloc<long long>(S);
+    D.xyz_ref = dalloc<float4>(S);
     D.vscale = upload(std::vector<float>(ns, (float)p.thermostat_scalar));
     d_therm_ke = dalloc<long long>((size_t)ns * E_COUNT);
     therm_T.assign(ns, 0.0);
@@ -649,6 +652,7 @@ void lima_engine::setup() {
     ip.dt = p.dt;
     ip.integrator = p.integrator;
 
+    d_disp = dalloc<unsigned>(1);
     d_out_d = dalloc<double>(3 * (size_t)N);
     d_out_f = dalloc<float>(3 * (size_t)N);
     d_maxf = dalloc<float>(1);
@@ -1270,8 +1274,32 @@ int lima_num_systems(const lima_engine* h, int* n) {
     return LIMA_OK;
 }
 
+// the device state is the current one while the engine is built: copy it back
+// into the host-side systems before a topology change drops the device buffers
+static void pull_device_state(lima_engine* h) {
+    if (!h->built || h->state_pending) return;
+    std::vector<double> pp((size_t)3 * h->st.n_atoms);
+    std::vector<float> vv((size_t)3 * h->st.n_atoms);
+    launch_gather_state(h->st, h->d_out_d, h->d_out_f, h->s_main);
+    CK(cudaMemcpyAsync(pp.data(), h->d_out_d, pp.size() * 8, cudaMemcpyDeviceToHost, h->s_main));
+    CK(cudaMemcpyAsync(vv.data(), h->d_out_f, vv.size() * 4, cudaMemcpyDeviceToHost, h->s_main));
+    CK(cudaStreamSynchronize(h->s_main));
+    for (size_t s = 0; s < h->sys.size(); ++s) {
+        const size_t o = 3 * (size_t)h->n_atoms_off[s];
+        h->sys[s].pos.assign(pp.begin() + o, pp.begin() + o + 3 * h->sys[s].n);
+        h->sys[s].vel.assign(vv.begin() + o, vv.begin() + o + 3 * h->sys[s].n);
+    }
+}
+
 static int topology_changed(lima_engine* h) {
-    if (h->built) h->release();
+    if (h->built) {
+        // keep the current state; the topology call itself reports no CUDA error
+        try {
+            pull_device_state(h);
+        } catch (const CudaError&) {
+        }
+        h->release();
+    }
     h->built = false;
     return LIMA_OK;
 }
@@ -1353,6 +1381,29 @@ int lima_set_state(lima_engine* h, const double* pos, const float* vel) {
     for (int i = 0; i < 3 * S.n; ++i)
         if (!std::isfinite(pos[i])) return fail(h, LIMA_ERR_NOT_FINITE, "non-finite position");
     return guarded(h, [&]() {
+        if (h->built && !h->state_pending) {
+            // Fast path: the atoms keep their slots; the pair list stays valid while no
+            // atom has moved more than half the Verlet buffer since it was built.
+            cudaStream_t s = h->s_main;
+            const size_t o = 3 * (size_t)h->n_atoms_off[h->cur];
+            CK(cudaMemcpyAsync(h->st.in_pos + o, pos, 3 * (size_t)S.n * sizeof(double), cudaMemcpyHostToDevice, s));
+            if (vel)
+                CK(cudaMemcpyAsync(h->st.in_vel + o, vel, 3 * (size_t)S.n * sizeof(float), cudaMemcpyHostToDevice, s));
+            else
+                CK(cudaMemsetAsync(h->st.in_vel + o, 0, 3 * (size_t)S.n * sizeof(float), s));
+            CK(cudaMemsetAsync(h->d_disp, 0, sizeof(unsigned), s));
+            h->launches += launch_load_state(h->st, h->n_atoms_off[h->cur], S.n, h->d_disp, s);
+            unsigned bits = 0;
+            CK(cudaMemcpyAsync(&bits, h->d_disp, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            float d2;
+            std::memcpy(&d2, &bits, sizeof(float));
+            const double half_skin = 0.5 * (h->rlist - h->p.cutoff);
+            if (!((double)d2 < half_skin * half_skin)) h->list_age = h->p.nstlist;   // rebuild before the next forces
+            h->energy_valid = false;
+            ++h->state_fast_loads;
+            return LIMA_OK;
+        }
         // pull the device state of the other systems first so they are kept
         if (h->built && !h->state_pending && h->sys.size() > 1) {
             std::vector<double> pp((size_t)3 * h->st.n_atoms);

@@ -82,6 +82,7 @@ struct DevState {
     unsigned* status = nullptr;
     long long* energy = nullptr;         // [n_sys][E_COUNT]
     long long* epot = nullptr;           // per-slot potential energy (energy steps), fixed point
+    float4* xyz_ref = nullptr;           // per-slot position at the last pair-list build
     float* vscale = nullptr;             // per-system velocity scale of the integrator (thermostat)
 };
 
@@ -159,6 +160,10 @@ int launch_zero_forces(const DevState& st, cudaStream_t s);
 int launch_max_force(const DevState& st, float* out, cudaStream_t s);
 // per-system kinetic energy (E_KINETIC of ke[n_sys][E_COUNT], fixed point)
 int launch_kinetic(const DevState& st, long long* ke, cudaStream_t s);
+// new positions and velocities (original order, in_pos / in_vel) for atoms
+// [a0, a0 + n) written into their current slots; the largest squared move from
+// the last pair-list build goes to *max_disp2 (float bits, atomic max)
+int launch_load_state(const DevState& st, int a0, int n, unsigned* max_disp2, cudaStream_t s);
 // one log frame in original atom order: (x, y, z, potential energy), (F, |v|)
 int launch_log_frame(const DevState& st, float4* pos_epot, float4* force_speed, cudaStream_t s);
 

@@ -146,6 +146,7 @@ __global__ void k_gather_slots(DevState st, int from_input) {
         st.py[s] = y;
         st.pz[s] = z;
         st.xyzq[s] = make_float4((float)x, (float)y, (float)z, st.q[a]);
+        st.xyz_ref[s] = st.xyzq[s];
         st.ljp[s] = st.ljp_atom[a];
         const float im = st.inv_mass[a];
         if (from_input) {

@@ -311,10 +311,14 @@ class Engine:
         self._check(self.lib.lima_get_energies(self.h, ctypes.byref(e)))
         return e.as_dict()
 
-    def state(self):
+    def state(self, pos_out=None, vel_out=None):
+        """Positions (n,3) float64 and velocities (n,3) float32 of the selected
+        system, written into pos_out / vel_out when given (e.g. pinned buffers)."""
         n = self.natoms[self._sel]
-        p = np.zeros((n, 3))
-        v = np.zeros((n, 3), np.float32)
+        p = np.zeros((n, 3)) if pos_out is None else pos_out
+        v = np.zeros((n, 3), np.float32) if vel_out is None else vel_out
+        assert p.dtype == np.float64 and p.flags.c_contiguous and p.size == 3 * n
+        assert v.dtype == np.float32 and v.flags.c_contiguous and v.size == 3 * n
         self._check(self.lib.lima_get_state(self.h, p.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
                                             v.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
         return p, v

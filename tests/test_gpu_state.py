@@ -1,0 +1,64 @@
+"""lima_set_state on a built engine: atoms keep their slots and the pair list is
+kept while no atom moved more than half the Verlet buffer since the list was
+built; larger moves rebuild it.  Results must not depend on which path ran."""
+import numpy as np
+import pytest
+
+from lima_b200 import Engine, systems
+from lima_b200 import engine as E
+from tests._ref import kappa_from_tol, oracle_total, rel_rms
+
+pytestmark = pytest.mark.gpu
+
+
+def make(s, **kw):
+    e = Engine(cutoff=1.0, electrostatics=E.ES_EWALD, ewald_kappa=kappa_from_tol(1.0, 1e-5), **kw)
+    e.load(s, pme_grid=(36, 36, 36))
+    return e
+
+
+def test_state_round_trip_keeps_trajectory_bitwise():
+    s = systems.water_box(1500, 3.6, seed=3, name="w")
+    a, b = make(s), make(s)
+    # one step after the list build at step 10: no atom is near half the buffer
+    a.step(11)
+    b.step(11)
+    p, v = b.state()
+    b.reset_timings()
+    b.set_state(p, v)            # same state back: same slots, the list is kept
+    b.compute_forces()
+    assert b.timings()["rebuilds"] == 0
+    a.compute_forces()
+    a.step(12)
+    b.step(12)
+    pa, va = a.state()
+    pb, vb = b.state()
+    assert np.array_equal(pa, pb) and np.array_equal(va, vb)
+    assert a.energies()["potential"] == b.energies()["potential"]
+
+
+def test_large_moves_and_rewrapped_positions_rebuild(oracle):
+    s = systems.water_box(1500, 3.6, seed=4, name="w")
+    e = make(s)
+    e.step(5)
+    p, v = e.state()
+    q = p + np.array([0.3, -0.2, 0.1])   # a rigid move far beyond half the buffer
+    q[100] += s.box                      # the same point one image away
+    e.reset_timings()
+    e.set_state(q, v)
+    e.compute_forces(energy=True)
+    s2 = systems.System(**{**s.__dict__, "pos": q.astype(np.float64)})
+    fr, _ = oracle_total(oracle, s2, 1.0, 2, kappa_from_tol(1.0, 1e-5), grid=(36, 36, 36))
+    assert rel_rms(e.forces(), fr) < 1e-4
+    assert e.timings()["rebuilds"] == 1
+
+
+def test_topology_change_keeps_current_positions():
+    s = systems.water_box(600, 3.0, seed=5, name="w")
+    e = Engine(cutoff=1.0, electrostatics=E.ES_EWALD, ewald_tol=1e-5)
+    e.load(s, pme_grid=(30, 30, 30))
+    e.step(10)
+    p, v = e.state()
+    e.set_box(s.box)             # forces a new set-up
+    p2, v2 = e.state()
+    assert np.array_equal(p, p2) and np.array_equal(v, v2)
