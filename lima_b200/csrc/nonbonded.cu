@@ -270,9 +270,23 @@ __global__ void __launch_bounds__(256, ENERGY ? 2 : 3) k_nonbonded(DevState st, 
 int launch_nonbonded(const DevState& st, const NbParams& p, bool energy, cudaStream_t s) {
     const long long threads = (long long)st.n_clusters * 32;
     const dim3 grid((unsigned)((threads + 255) / 256));
-#define NB_LAUNCH(ES)                                                       \
-    if (energy) k_nonbonded<ES, true><<<grid, 256, 0, s>>>(st, p);          \
-    else k_nonbonded<ES, false><<<grid, 256, 0, s>>>(st, p);
+    // The force-only launch reserves (unused) shared memory so that at most two of
+    // its blocks share an SM: the registers and slots left free let the PME and
+    // bonded kernels of the same step, on their higher-priority streams, run
+    // beside it instead of waiting for pair-kernel blocks to retire.  The pair
+    // kernel alone is ~9 % slower this way, the whole step ~2 % faster.
+    constexpr int kReserve = 90 * 1024;
+#define NB_LAUNCH(ES)                                                                                        \
+    if (energy) {                                                                                            \
+        k_nonbonded<ES, true><<<grid, 256, 0, s>>>(st, p);                                                   \
+    } else {                                                                                                 \
+        static bool attr_ = false;                                                                           \
+        if (!attr_) {                                                                                        \
+            cudaFuncSetAttribute(k_nonbonded<ES, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kReserve); \
+            attr_ = true;                                                                                    \
+        }                                                                                                    \
+        k_nonbonded<ES, false><<<grid, 256, kReserve, s>>>(st, p);                                           \
+    }
     if (p.es_mode == 0) {
         NB_LAUNCH(0)
     } else if (p.es_mode == 1) {
