@@ -188,6 +188,7 @@ def other_configs(args, local):
     s0 = systems.config0()
     e0 = Engine(cutoff=1.2, electrostatics=E.ES_CUTOFF, nstlist=10, dt=DT_NS, device=local, use_graphs=1)
     e0.load(s0)
+    e0.autotune(2)
     e0.step(20)
     t = _timed_steps(e0, k)[0][0]
     out["c0_water1k_cutoff"] = {"atoms": s0.n, "ns_per_day": ns_per_day(t), "ms_per_step": t * 1e3, "steps": k}
@@ -198,6 +199,7 @@ def other_configs(args, local):
                 use_graphs=1)
     e1.load(s1, pme_grid=(48, 48, 80))
     e1.minimize(force_tol=1e5, max_steps=300)
+    e1.autotune(2)
     e1.step(20)
     t = _timed_steps(e1, k)[0][0]
     out["c1_chains_water_pme48x48x80"] = {"atoms": s1.n, "ns_per_day": ns_per_day(t), "ms_per_step": t * 1e3,
@@ -215,6 +217,7 @@ def other_configs(args, local):
             e4.select(i)
             e4.load(sy)
         e4.minimize(force_tol=1e5, max_steps=100)
+        e4.autotune(2)
         e4.step(20)
         t = _timed_steps(e4, k)[0][0]
         lat = sorted(_timed_steps(e4, min(k, 60), per_step=True))
@@ -330,6 +333,7 @@ def run_lima(args):
         torch.cuda.synchronize()
         print(json.dumps({"profile_steps": args.profile, "timings": eng.timings()}), flush=True)
         return 0
+    shape = eng.autotune(2)
     eng.step(max(args.warmup, 3))
 
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
@@ -422,6 +426,7 @@ def run_lima(args):
     eng_g = Engine(cutoff=CUTOFF, electrostatics=E.ES_EWALD, ewald_tol=1e-5, nstlist=10, dt=DT_NS, device=local,
                    use_graphs=1)
     eng_g.load(s, pme_grid=GRID)
+    eng_g.autotune(2)
     eng_g.step(21)
     graph_step_s = _timed_steps(eng_g, max(args.steps, 21))[0][0]
     eng_g.close()
@@ -451,7 +456,8 @@ def run_lima(args):
                    "dt_fs": 1.0, "integrator": "leapfrog", "parallelism": "replicas" if world > 1 else "single",
                    "l2": "flushed (256 MiB write) before every timed iteration; an iteration is one pair-list "
                          "period: list rebuild + 10 steps, energies evaluated on the last step",
-                   "accumulation": "int64 fixed point forces/energies, FP64 positions"},
+                   "accumulation": "int64 fixed point forces/energies, FP64 positions",
+                   "pair_launch_shape": shape},
         "pairs_per_s": world * pairs / step_s,
         "pairs_per_step": pairs,
         "wall_ms_per_step": t_wall / args.steps * 1e3,

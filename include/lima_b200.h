@@ -141,6 +141,8 @@ typedef struct lima_timings {   /* averages over the steps since the last reset 
     int64_t steps;
     int64_t rebuilds;
     int64_t kernel_launches;  /* kernels of this library launched since the reset     */
+    int32_t pair_shape;       /* launch shape of the force-only pair kernel (lima_autotune) */
+    int32_t reserved;
 } lima_timings;
 
 typedef struct lima_engine lima_engine;
@@ -298,6 +300,15 @@ LIMA_API int lima_learned_pme_gradients(lima_engine* h, int rows, const float* x
  * stepping; 1: the warp-level mma.sync kernel.  LIMA_ERR_TIMEOUT if a bounded
  * device wait gave up. */
 LIMA_API int lima_learned_pme_predict(lima_engine* h, int rows, const float* features, float* out, int impl);
+
+/* Autotuner: after one untimed period per shape, times `periods` pair-list
+ * periods of real MD steps (they advance the simulation), three rounds, with
+ * each launch shape of the force-only pair kernel — 256
+ * or 128 threads per block, with or without leaving SM room to the PME and
+ * bonded kernels of the step — and keeps the fastest for this engine.  All
+ * shapes give identical results.  *shape (may be NULL) receives the choice:
+ * bit 0 room left, bit 1 128-thread blocks. */
+LIMA_API int lima_autotune(lima_engine* h, int periods, int* shape);
 
 /* ---------------------------------------------------------- thermostat, log */
 /* Last temperature measurement of the selected system: temperature [K], the

@@ -106,6 +106,11 @@ struct lima_engine {
     double time_ms = 0.0;
     int64_t timed_steps = 0;
 
+    // launch shape of the force-only pair kernel, picked by autotune()
+    int nb_shape = 0;
+    bool nb_tuned = false;
+    double tune_ms[4] = {0, 0, 0, 0};
+
     // device scratch for readback
     unsigned* d_disp = nullptr;       // largest squared move since the last list build (float bits)
     int64_t state_fast_loads = 0;     // lima_set_state calls served without a rebuild
@@ -237,6 +242,7 @@ struct lima_engine {
     void learned_pme_stage(bool energy, cudaStream_t s);
     void ensure_list();
     void measure_temperature();
+    int autotune(int periods);
     void log_frame();
     void flush_log();
 };
@@ -1011,7 +1017,7 @@ void lima_engine::capture_period() {
         CK(cudaEventRecord(ev_bonded, s_bonded));
         if (pme_on) launches += launch_pme(st, pp, false, s_pme);
         CK(cudaEventRecord(ev_pme, s_pme));
-        launches += launch_nonbonded(st, nb, false, s_main);
+        launches += launch_nonbonded(st, nb, false, s_main, nb_shape);
         CK(cudaStreamWaitEvent(s_main, ev_bonded, 0));
         CK(cudaStreamWaitEvent(s_main, ev_pme, 0));
         launches += launch_integrate(st, ip, false, s_main);
@@ -1053,7 +1059,7 @@ void lima_engine::forces(bool energy) {
     }
     CK(cudaEventRecord(ev_pme, sp));
     mark(1, 0, s_main);
-    launches += launch_nonbonded(st, nb, energy, s_main);
+    launches += launch_nonbonded(st, nb, energy, s_main, nb_shape);
     mark(1, 1, s_main);
     CK(cudaStreamWaitEvent(s_main, ev_bonded, 0));
     CK(cudaStreamWaitEvent(s_main, ev_pme, 0));
@@ -1115,6 +1121,35 @@ void lima_engine::run_steps(int n) {
     time_ms += ms;
     timed_steps += n;
     energy_valid = true;
+}
+
+// Times `periods` pair-list periods of real MD steps with each launch shape of
+// the force-only pair kernel (two rounds, best of each) and keeps the fastest.
+// Every shape gives identical results, so the choice changes only the speed.
+int lima_engine::autotune(int periods) {
+    const int n = std::max(1, periods) * p.nstlist;
+    double best[4] = {1e300, 1e300, 1e300, 1e300};
+    for (int shape = 0; shape < 4; ++shape) {   // first use of each shape, untimed
+        nb_shape = shape;
+        drop_graph();
+        run_steps(p.nstlist);
+    }
+    for (int round = 0; round < 3; ++round)
+        for (int shape = 0; shape < 4; ++shape) {
+            nb_shape = shape;
+            drop_graph();
+            const double t0 = time_ms;
+            run_steps(n);
+            best[shape] = std::min(best[shape], time_ms - t0);
+        }
+    int pick = 0;
+    for (int shape = 1; shape < 4; ++shape)
+        if (best[shape] < best[pick]) pick = shape;
+    for (int shape = 0; shape < 4; ++shape) tune_ms[shape] = best[shape] / n;
+    nb_shape = pick;
+    nb_tuned = true;
+    drop_graph();
+    return pick;
 }
 
 // Temperature of every system from its kinetic energy (3N - 3 degrees of
@@ -1610,6 +1645,7 @@ int lima_get_timings(lima_engine* h, lima_timings* t) {
     t->bonded = 1000.0 * h->phase_ms[2] / ns;
     t->pme = 1000.0 * h->phase_ms[3] / ns;
     t->integrate = 1000.0 * h->phase_ms[4] / ns;
+    t->pair_shape = h->nb_shape;
     return LIMA_OK;
 }
 
@@ -1860,6 +1896,17 @@ int lima_learned_pme_gradients(lima_engine* h, int rows, const float* x, const f
 }
 
 // ------------------------------------------------------------ thermostat, log
+int lima_autotune(lima_engine* h, int periods, int* shape) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    if (periods < 1) return fail(h, LIMA_ERR_INVALID_ARG, "periods must be >= 1");
+    return guarded(h, [&]() {
+        ensure_built(h);
+        const int pick = h->autotune(periods);
+        if (shape) *shape = pick;
+        return LIMA_OK;
+    });
+}
+
 int lima_get_thermostat(lima_engine* h, double* temperature, double* scale, int64_t* step) {
     if (!h) return LIMA_ERR_INVALID_ARG;
     const bool have = h->built && h->cur < (int)h->therm_T.size();

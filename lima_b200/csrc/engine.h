@@ -115,7 +115,8 @@ struct NbParams {
 // nbsearch.cu
 int launch_rebuild(const DevState& st, float rlist, bool from_input, cudaStream_t s);
 // nonbonded.cu
-int launch_nonbonded(const DevState& st, const NbParams& p, bool energy, cudaStream_t s);
+// shape: launch shape of the force-only kernel (bit 0 residency cap, bit 1 128-thread blocks)
+int launch_nonbonded(const DevState& st, const NbParams& p, bool energy, cudaStream_t s, int shape = 0);
 int launch_exclusion_correction(const DevState& st, const BondedTerms& bt, const NbParams& p,
                                  bool energy, cudaStream_t s);
 int launch_pairlist_dump(const DevState& st, const NbParams& p, long long cap, int* out_pairs,

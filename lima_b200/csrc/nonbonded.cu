@@ -267,34 +267,37 @@ __global__ void __launch_bounds__(256, ENERGY ? 2 : 3) k_nonbonded(DevState st, 
     }
 }
 
-int launch_nonbonded(const DevState& st, const NbParams& p, bool energy, cudaStream_t s) {
+// Launch shapes of the force-only pair kernel (results are identical for every
+// shape: the work of a warp does not depend on the block it sits in):
+//   bit 0: reserve unused shared memory so that the kernel holds at most 16
+//          warps of an SM, leaving registers and block slots to the PME and
+//          bonded kernels of the same step on their higher-priority streams
+//          (helps when the PME chain is long next to the pair kernel);
+//   bit 1: 128-thread blocks instead of 256.
+// The engine's autotuner times the shapes on the running system.
+template <int ES>
+static void launch_nb_shape(const DevState& st, const NbParams& p, bool energy, int shape, cudaStream_t s) {
     const long long threads = (long long)st.n_clusters * 32;
-    const dim3 grid((unsigned)((threads + 255) / 256));
-    // The force-only launch reserves (unused) shared memory so that at most two of
-    // its blocks share an SM: the registers and slots left free let the PME and
-    // bonded kernels of the same step, on their higher-priority streams, run
-    // beside it instead of waiting for pair-kernel blocks to retire.  The pair
-    // kernel alone is ~9 % slower this way, the whole step ~2 % faster.
-    constexpr int kReserve = 90 * 1024;
-#define NB_LAUNCH(ES)                                                                                        \
-    if (energy) {                                                                                            \
-        k_nonbonded<ES, true><<<grid, 256, 0, s>>>(st, p);                                                   \
-    } else {                                                                                                 \
-        static bool attr_ = false;                                                                           \
-        if (!attr_) {                                                                                        \
-            cudaFuncSetAttribute(k_nonbonded<ES, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kReserve); \
-            attr_ = true;                                                                                    \
-        }                                                                                                    \
-        k_nonbonded<ES, false><<<grid, 256, kReserve, s>>>(st, p);                                           \
+    const int tb = (shape & 2) ? 128 : 256;
+    const dim3 grid((unsigned)((threads + tb - 1) / tb));
+    if (energy) {
+        k_nonbonded<ES, true><<<grid, tb, 0, s>>>(st, p);
+        return;
     }
-    if (p.es_mode == 0) {
-        NB_LAUNCH(0)
-    } else if (p.es_mode == 1) {
-        NB_LAUNCH(1)
-    } else {
-        NB_LAUNCH(2)
+    // 16 warps per SM: 2 blocks of 256 threads (90 KB each) or 4 of 128 (50 KB each)
+    const int reserve = (shape & 1) ? ((shape & 2) ? 50 * 1024 : 90 * 1024) : 0;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_nonbonded<ES, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 90 * 1024);
+        attr = true;
     }
-#undef NB_LAUNCH
+    k_nonbonded<ES, false><<<grid, tb, reserve, s>>>(st, p);
+}
+
+int launch_nonbonded(const DevState& st, const NbParams& p, bool energy, cudaStream_t s, int shape) {
+    if (p.es_mode == 0) launch_nb_shape<0>(st, p, energy, shape, s);
+    else if (p.es_mode == 1) launch_nb_shape<1>(st, p, energy, shape, s);
+    else launch_nb_shape<2>(st, p, energy, shape, s);
     return 1;
 }
 

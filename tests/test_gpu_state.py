@@ -62,3 +62,20 @@ def test_topology_change_keeps_current_positions():
     e.set_box(s.box)             # forces a new set-up
     p2, v2 = e.state()
     assert np.array_equal(p, p2) and np.array_equal(v, v2)
+
+
+def test_autotune_shapes_give_identical_trajectories():
+    """The autotuner switches the pair kernel's launch shape between periods; every
+    shape must give the same bits, so a tuned run equals an untuned one."""
+    s = systems.water_box(1500, 3.6, seed=6, name="w")
+    a, b = make(s), make(s)
+    shape = a.autotune(1)                      # 16 periods of 10 steps, energies at each period's end
+    assert 0 <= shape <= 3 and a.timings()["pair_shape"] == shape
+    for _ in range(16):
+        b.step(10)
+    a.step(10)
+    b.step(10)
+    pa, va = a.state()
+    pb, vb = b.state()
+    assert np.array_equal(pa, pb) and np.array_equal(va, vb)
+    assert a.energies()["potential"] == b.energies()["potential"]
