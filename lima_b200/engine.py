@@ -283,6 +283,9 @@ class Engine:
         self.set_dihedrals(system.dihedrals, system.dihedral_par)
         self.set_impropers(system.impropers, system.improper_par)
         self.set_pairbonds(system.pairbonds, system.pair_par)
+        extra = getattr(system, "extra_exclusions", None)
+        if extra is not None and len(extra):
+            self.set_exclusions(extra)
         if pme_grid is not None:
             self.set_pme_grid(pme_grid)
         self.set_state(system.pos, system.vel)

@@ -48,6 +48,8 @@ class System:
     pairbonds: np.ndarray = field(default_factory=lambda: np.zeros((0, 2), np.int32))
     pair_par: np.ndarray = field(default_factory=lambda: np.zeros((0, 2), np.float32))
     name: str = ""
+    # pairs excluded beyond those sharing a bonded term (e.g. a topology's [ exclusions ])
+    extra_exclusions: np.ndarray = field(default_factory=lambda: np.zeros((0, 2), np.int32))
 
     @property
     def n(self) -> int:
@@ -56,7 +58,7 @@ class System:
     def exclusions(self) -> np.ndarray:
         """Unique (i<j) atom pairs sharing any bond, angle, dihedral or improper."""
         pairs = []
-        for terms in (self.bonds, self.angles, self.dihedrals, self.impropers):
+        for terms in (self.bonds, self.angles, self.dihedrals, self.impropers, self.extra_exclusions):
             t = np.asarray(terms)
             if len(t) == 0:
                 continue
@@ -219,6 +221,38 @@ def water_box(n_waters: int, box_nm: float, seed: int = 20241203, jitter: float 
                   sigma=s.astype(np.float32), epsilon=e.astype(np.float32),
                   bonds=bonds.astype(np.int32), bond_par=bpar.astype(np.float32),
                   angles=angles.astype(np.int32), angle_par=apar.astype(np.float32), name=name)
+
+
+def water_with_single_sites(n_waters: int, box_nm: float, n_sites: int, seed: int = 20241203,
+                            temperature: float = 300.0) -> System:
+    """Flexible water in which n_sites molecules are replaced by single-site,
+    LJ-only solvent atoms (argon-like: sigma 0.3405 nm, eps 0.996 kJ/mol, no
+    charge) at their oxygen positions.  The reference treats such one-site
+    molecules on a separate solvent-block path; here they are ordinary atoms
+    without bonded terms."""
+    rng = np.random.default_rng(seed + 17)
+    w = water_box(n_waters, box_nm, seed=seed, temperature=temperature)
+    nw = w.n // 3
+    swap = np.sort(rng.choice(nw, n_sites, replace=False))
+    keep_mol = np.ones(nw, bool)
+    keep_mol[swap] = False
+    keep_atoms = np.repeat(keep_mol, 3)
+    new_index = -np.ones(w.n, np.int64)
+    new_index[keep_atoms] = np.arange(int(keep_atoms.sum()))
+    bmask = keep_atoms[w.bonds[:, 0]]
+    amask = keep_atoms[w.angles[:, 0]]
+    site_pos = w.pos[3 * swap]
+    mass = np.float32(39.948e-3)
+    site_vel = maxwell_boltzmann(rng, np.full(n_sites, mass, np.float32), temperature).astype(np.float32)
+    return System(box=w.box, pos=np.concatenate([w.pos[keep_atoms], site_pos]),
+                  vel=np.concatenate([w.vel[keep_atoms], site_vel]),
+                  charge=np.concatenate([w.charge[keep_atoms], np.zeros(n_sites, np.float32)]),
+                  mass=np.concatenate([w.mass[keep_atoms], np.full(n_sites, mass, np.float32)]),
+                  sigma=np.concatenate([w.sigma[keep_atoms], np.full(n_sites, 0.3405, np.float32)]),
+                  epsilon=np.concatenate([w.epsilon[keep_atoms], np.full(n_sites, 0.996 * KJ, np.float32)]),
+                  bonds=new_index[w.bonds[bmask]].astype(np.int32), bond_par=w.bond_par[bmask],
+                  angles=new_index[w.angles[amask]].astype(np.int32), angle_par=w.angle_par[amask],
+                  name="water_single_sites")
 
 
 # ------------------------------------------------------------ lipid-like chains

@@ -280,3 +280,20 @@ def test_batch_with_chains_matches_single():
         pb, vb = batch.state()
         ps, vs = single.state()
         assert np.array_equal(pb, ps) and np.array_equal(vb, vs), k
+
+
+# ------------------------------------------------------- single-site solvent
+def test_single_site_solvent_mixture(oracle):
+    """One-site LJ solvent atoms mixed into water (the reference's separate
+    solvent-block path) go through the general atom path: forces and energies
+    against the oracle with PME, then stable stepping."""
+    s = systems.water_with_single_sites(1500, 3.6, 300, seed=9)
+    kappa = kappa_from_tol(1.0, 1e-5)
+    grid = (36, 36, 36)
+    e = make(s, grid=grid, cutoff=1.0, electrostatics=E.ES_EWALD, ewald_kappa=kappa)
+    e.compute_forces(energy=True)
+    fr, er = oracle_total(oracle, s, 1.0, 2, kappa, grid=grid)
+    assert rel_rms(e.forces(), fr) < FORCE_TOL
+    check_energies(e.energies(), er, keys=["lj", "coulomb_real", "pme_recip", "bond", "angle"])
+    e.step(50)
+    assert np.isfinite(e.energies()["total"])
