@@ -114,7 +114,9 @@ typedef struct lima_params {
     /* per-particle logging (EngineUtils.cuh:143-158, Engine.cu:203-240): every
        log_interval steps (0 = off) the position, potential energy, force and speed of
        every atom go to a device ring of log_ring frames, offloaded to host memory
-       whenever it fills; read with lima_get_log */
+       whenever it fills; read with lima_get_log.  As in the reference
+       (EngineKernels.cuh:399-433) a frame is taken after the step's update: the new
+       position, the energy and force evaluated at the old one, the updated speed */
     int    log_interval;
     int    log_ring;          /* frames held on the device (default 5, as the reference) */
 } lima_params;
@@ -315,8 +317,9 @@ LIMA_API int lima_autotune(lima_engine* h, int periods, int* shape);
  * velocity scale in use, and the step it was taken at (-1 before the first). */
 LIMA_API int lima_get_thermostat(lima_engine* h, double* temperature, double* scale, int64_t* step);
 /* Logged frames of the selected system, oldest first, starting at frame
- * `first`; at most max_frames are written.  Per frame: steps[f]; pos_epot[f][n][4]
- * = x, y, z [nm], potential energy [J/mol] (half of each pair energy, an equal
+ * `first`; at most max_frames are written.  Per frame: steps[f] (the step whose
+ * forces were evaluated); pos_epot[f][n][4] = x, y, z [nm] after that step's update,
+ * potential energy [J/mol] at the step's start (half of each pair energy, an equal
  * share of each bonded term, 1/2 q phi plus the self term); force_speed[f][n][4]
  * = force [J/mol/nm], |v| [nm/ns].  Output arrays may be NULL.  *n_frames
  * receives the number of frames logged so far. */

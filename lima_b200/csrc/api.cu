@@ -1092,10 +1092,12 @@ void lima_engine::run_steps(int n) {
         const bool log_now = p.log_interval > 0 && step % p.log_interval == 0;
         const bool energy = k == n - 1 || log_now;
         forces(energy);
-        if (log_now) log_frame();
         mark(4, 0, s_main);
         launches += launch_integrate(st, ip, energy, s_main);
         mark(4, 1, s_main);
+        // logged after the update, as the reference's integration kernel does:
+        // new position, this step's potential energy and force, updated speed
+        if (log_now) log_frame();
         collect_phases();
         ++list_age;
         ++step;

@@ -190,8 +190,12 @@ int launch_kinetic(const DevState& st, long long* ke, cudaStream_t s) {
 }
 
 // Per-particle log entry (the reference's potE / traj / vel / force buffers,
-// EngineUtils.cuh:143-158): position, potential energy of this step's force
-// evaluation, force and speed of the stored velocity, in original atom order.
+// EngineUtils.cuh:143-158), written after the step's integration as the
+// reference's CompoundIntegrationKernel does (EngineKernels.cuh:399-433): the
+// updated position x(t+dt), the potential energy and force of the step's
+// evaluation at x(t), and the speed of the stored velocity (velocity Verlet:
+// v(t) times the thermostat scale, synchronous with that energy; leapfrog:
+// v(t+dt/2)), in original atom order.
 __global__ void k_log_frame(DevState st, float4* pos_epot, float4* force_speed) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= st.n_slots) return;

@@ -186,6 +186,8 @@ class Engine:
         self._check(self.lib.lima_create_batch(ctypes.byref(self.params), n_systems, ctypes.byref(self.h)))
         self.n_systems = n_systems
         self.natoms = [0] * n_systems
+        self._boxes = [np.zeros(3)] * n_systems
+        self._masses = [np.zeros(0, np.float32)] * n_systems
         self._sel = 0
 
     # ------------------------------------------------------------- plumbing
@@ -220,6 +222,15 @@ class Engine:
     def set_box(self, box):
         b = np.broadcast_to(np.asarray(box, dtype=np.float64), (3,))
         self._check(self.lib.lima_set_box(self.h, float(b[0]), float(b[1]), float(b[2])))
+        self._boxes[self._sel] = np.array(b, np.float64)
+
+    def box(self) -> np.ndarray:
+        """Edge lengths [nm] of the selected system (as last set)."""
+        return self._boxes[self._sel].copy()
+
+    def masses(self) -> np.ndarray:
+        """Atom masses [kg/mol] of the selected system (as last set)."""
+        return self._masses[self._sel].copy()
 
     def set_atoms(self, charge, mass, sigma, epsilon):
         q, qp = _f32(charge)
@@ -228,6 +239,7 @@ class Engine:
         e, ep = _f32(epsilon)
         self._check(self.lib.lima_set_atoms(self.h, len(q), qp, mp, sp, ep))
         self.natoms[self._sel] = len(q)
+        self._masses[self._sel] = m.copy()
 
     def _terms(self, fn, idx, par, k, np_):
         if idx is None or len(idx) == 0:

@@ -4,6 +4,7 @@ import numpy as np
 import pytest
 
 from lima_b200 import Engine, systems
+from lima_b200 import trajectory as T
 from lima_b200 import engine as E
 from tests._ref import kappa_from_tol, oracle_total, rel_rms
 
@@ -25,11 +26,13 @@ def test_logged_energies_and_forces_match_oracle(oracle):
     e.step(1)
     steps, pe, fs = e.log()
     assert list(steps) == [0]
-    # the frame holds the state the step started from and its forces
-    assert np.allclose(pe[0, :, :3], s.pos, atol=1e-5)
+    # the frame holds the updated state and the forces and energies of the
+    # step's evaluation at the starting positions
+    pos, vel = e.state()
+    assert np.array_equal(pe[0, :, :3], pos.astype(np.float32))
     fr, _ = oracle_total(oracle, s, 1.0, 2, kappa, grid=grid)
     assert rel_rms(fs[0, :, :3].astype(np.float64), fr) < 1e-4
-    assert np.allclose(fs[0, :, 3], np.linalg.norm(s.vel, axis=1), rtol=1e-5)
+    assert np.allclose(fs[0, :, 3], np.linalg.norm(vel, axis=1), rtol=1e-5)
     ae = oracle.atom_energies(s, 1.0, kappa, grid)
     got = pe[0, :, 3].astype(np.float64)
     assert rel_rms(got, ae) < 1e-4, rel_rms(got, ae)
@@ -70,3 +73,37 @@ def test_thermostat_measures_and_scales(apply):
     # code/LIMA_ENGINE/src/Thermostat.cuh:55-67: clamp(310/T, 1 -+ 0.001/interval)
     expect = min(max(310.0 / T, 1.0 - 1e-4), 1.0 + 1e-4) if apply else 1.0
     assert abs(th["scale"] - expect) < 1e-7
+
+
+def test_trajectory_file_and_energy_analysis(tmp_path):
+    """Logged frames go to a .trr file and through the reference's post-run
+    energy analysis (variance coefficient, energy gradient)."""
+    s = water(600, 3.0)
+    e = Engine(cutoff=1.0, electrostatics=E.ES_EWALD, ewald_tol=1e-5, log_interval=5,
+               integrator=E.VELOCITY_VERLET)
+    e.load(s, pme_grid=(30, 30, 30))
+    e.step(100)                      # leave the lattice start behind
+    e.clear_log()
+    e.step(200)
+    path = str(tmp_path / "trajectory.trr")
+    assert T.write_log_trr(path, e, with_forces=True) == 40
+    steps, pe, fs = e.log()
+    assert list(steps) == list(range(100, 300, 5))
+    frames = T.read_trr(path)
+    assert [f.step for f in frames] == list(steps)
+    for i in (0, 17, 39):
+        assert np.array_equal(frames[i].x, pe[i, :, :3].astype(np.float64))
+        assert np.allclose(frames[i].f, fs[i, :, :3] / 1000.0, rtol=1e-6)
+        assert np.array_equal(frames[i].box, np.diag(s.box))
+    a = T.analyze_log(e)
+    pot, kin = T.log_energies(pe, fs, s.mass)
+    tot = (pot + kin)[1:-1]
+    assert len(a.total_energy) == 38 and np.allclose(a.total_energy, tot.astype(np.float32))
+    assert abs(a.variance_coefficient - tot.std() / abs(tot.mean())) < 1e-4 * a.variance_coefficient
+    slope = np.polyfit(np.arange(len(tot)), tot, 1)[0] / tot.mean()
+    assert abs(a.energy_gradient - slope) < 1e-3 * abs(slope) + 1e-9
+    # velocity Verlet: the logged speed is synchronous with the logged energy, so
+    # the total only carries the integrator's O(dt^2) wobble (logging the speed a
+    # step behind, as before the update, gave a variance coefficient of 2.6e-2)
+    assert tot.std() < 1e-3 * a.kin_energy.mean(), (tot.std(), a.kin_energy.mean())
+    assert a.variance_coefficient < 5e-3 and abs(a.energy_gradient) < 1e-4
