@@ -522,12 +522,15 @@ void lima_engine::setup() {
                 if (b > a && q[a] != 0.f && q[b] != 0.f) xidx.push_back(make_int2(a, b));
     }
 
-    // ---- pair-list capacity: full neighbour count of clusters (x1.3 margin)
+    // ---- pair-list capacity: full neighbour count of clusters times 4 rows per
+    // cluster pair (about 5.3 of a pair's 8 j-atoms have an i-atom within the list
+    // radius in water, and a cluster's half list is about half its neighbours),
+    // with a 1.3x margin
     const double a_cl = std::cbrt(CLUSTER / max_density);
     const double reach = rlist + 1.5 * a_cl;
     const double est = 4.0 / 3.0 * kPi * reach * reach * reach * max_density / CLUSTER;
     // replayed graphs cannot grow the list between rebuilds: give them more room
-    int pl_cap = (int)std::ceil((p.use_graphs ? 1.8 : 1.3) * est) + 32;
+    int pl_cap = (int)std::ceil((p.use_graphs ? 1.8 : 1.3) * 4.0 * est) + 256;
     pl_cap = (pl_cap + 31) / 32 * 32;
     if (st.pl_cap > pl_cap) pl_cap = st.pl_cap;  // keep a capacity grown earlier
 
@@ -602,8 +605,7 @@ void lima_engine::setup() {
     D.bb_hi = dalloc<float4>(n_clusters);
     D.bb_molsig = dalloc<unsigned long long>(n_clusters);
     D.pl_count = dalloc<int>(n_clusters);
-    D.pl_j = dalloc<int>((size_t)n_clusters * pl_cap);
-    D.pl_mask = dalloc<unsigned long long>((size_t)n_clusters * pl_cap);
+    D.pl_row = dalloc<int2>((size_t)n_clusters * pl_cap);
     D.status = dalloc<unsigned>(1);
     D.energy = dalloc<long long>((size_t)ns * E_COUNT);
     D.epot = dalloc<long long>(S);
@@ -975,13 +977,10 @@ void lima_engine::rebuild(bool from_input) {
         }
         // grow the pair list and redo the build from the (unchanged) source
         const int cap = (st.pl_cap * 3 / 2 + 31) / 32 * 32;
-        cudaFree(st.pl_j);
-        cudaFree(st.pl_mask);
-        allocs.erase(std::remove(allocs.begin(), allocs.end(), (void*)st.pl_j), allocs.end());
-        allocs.erase(std::remove(allocs.begin(), allocs.end(), (void*)st.pl_mask), allocs.end());
+        cudaFree(st.pl_row);
+        allocs.erase(std::remove(allocs.begin(), allocs.end(), (void*)st.pl_row), allocs.end());
         st.pl_cap = cap;
-        st.pl_j = dalloc<int>((size_t)st.n_clusters * cap);
-        st.pl_mask = dalloc<unsigned long long>((size_t)st.n_clusters * cap);
+        st.pl_row = dalloc<int2>((size_t)st.n_clusters * cap);
         drop_graph();
         // the state is already permuted into slot order: rebuild from the slots
         from_input = false;

@@ -15,7 +15,7 @@ struct DevState {
     int n_clusters = 0;       // capacity (sum of per-system max_clusters)
     int n_slots = 0;          // 8 * n_clusters
     int n_cols = 0;           // all columns
-    int pl_cap = 0;           // pair-list entries per i-cluster
+    int pl_cap = 0;           // pair-list rows per i-cluster
     int col_cap = 0;          // atoms a column may hold
 
     SysDesc* sys = nullptr;
@@ -67,8 +67,9 @@ struct DevState {
     float4* bb_hi = nullptr;
     unsigned long long* bb_molsig = nullptr;  // bit (molecule id mod 64) of every atom in the cluster
     int* pl_count = nullptr;
-    int* pl_j = nullptr;
-    unsigned long long* pl_mask = nullptr;
+    // pair-list rows: one per (i-cluster, j-atom) with at least one i-atom in range;
+    // x = j slot, y = 8-bit i-atom mask | periodic shift code << 8
+    int2* pl_row = nullptr;
 
     // PME
     long long* pme_grid_fx = nullptr;    // fixed-point charge grid (all systems)

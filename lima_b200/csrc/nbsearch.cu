@@ -11,7 +11,8 @@
 //   7. k_bbox           per-cluster bounding boxes
 //   8. k_pairsearch     half list of cluster pairs within cutoff+skin, with a
 //                       64-bit interaction mask (padding, exclusions, i<j on
-//                       the diagonal) and a periodic-shift code per entry.
+//                       the diagonal) and a periodic-shift code per pair, stored
+//                       as rows: one per j-atom with a non-empty 8-bit i-mask.
 // The result is bit-identical run to run: every ordering is fixed by keys,
 // never by atomic arrival order.
 #include "engine.h"
@@ -351,13 +352,30 @@ __global__ void __launch_bounds__(PS_WARPS * 32, 1) k_pairsearch(DevState st, fl
                 mask &= upper;
             }
         }
-        const unsigned has = __ballot_sync(0xffffffffu, mask != 0ull);
-        const int pos = count + __popc(has & ((1u << lane) - 1u));
-        if (mask != 0ull && pos < cap) {
-            st.pl_j[base_out + pos] = ent;
-            st.pl_mask[base_out + pos] = mask;
+        // one row per j-atom with a non-empty 8-bit mask, in lane order, then j order
+        int nrow = 0;
+#pragma unroll
+        for (int jj = 0; jj < CLUSTER; ++jj) nrow += ((mask >> (8 * jj)) & 0xffull) != 0ull;
+        int incl = nrow;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
         }
-        count += __popc(has);
+        int pos = count + incl - nrow;
+        if (nrow) {
+            const int jc = ent & ((1 << JCLUSTER_BITS) - 1);
+            const int code = (unsigned)ent >> JCLUSTER_BITS;
+#pragma unroll
+            for (int jj = 0; jj < CLUSTER; ++jj) {
+                const int m8 = (int)((mask >> (8 * jj)) & 0xffull);
+                if (m8) {
+                    if (pos < cap) st.pl_row[base_out + pos] = make_int2(jc * CLUSTER + jj, m8 | (code << 8));
+                    ++pos;
+                }
+            }
+        }
+        count += __shfl_sync(0xffffffffu, incl, 31);
     };
 
     // flat walk over (column, batch of 32 clusters) units; after each unit's

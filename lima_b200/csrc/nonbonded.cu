@@ -12,9 +12,9 @@
 // reference evaluates each directed pair.
 //
 // Work mapping (see k_nonbonded): one warp per i-cluster; each lane owns one
-// j-atom of four list entries at a time and walks the 8 i-atoms.  Forces are
-// added as int64 fixed point, so the result does not depend on the order in
-// which warps finish.
+// row of the list (a j-atom with an 8-bit mask of the i-atoms it meets) and
+// walks the 8 i-atoms.  Forces are added as int64 fixed point, so the result
+// does not depend on the order in which warps finish.
 #include "engine.h"
 
 namespace lima {
@@ -72,12 +72,14 @@ __device__ __forceinline__ float ex2_approx(float x) {
     return y;
 }
 
-// Work mapping: one warp per i-cluster; the warp takes its list four entries at
-// a time and each lane owns one j-atom (entry k0 + lane/8, j-atom lane%8).  A
-// lane walks the 8 i-atoms two at a time, (ip, ip + 4) for ip = 0..3, in packed
-// FP32 (read as float4 pairs from shared memory), keeps its j-atom's force in a
-// packed register and adds it once per entry; the i-forces live in 12 packed
-// registers per lane and are reduced across the warp once, after the list.
+// Work mapping: one warp per i-cluster; the warp takes its list 32 rows at a
+// time and each lane owns one row: a j-atom whose 8-bit mask names the i-atoms
+// it interacts with (rows whose mask would be empty are not in the list, so no
+// lane works on a j-atom out of range of the whole i-cluster).  A lane walks the
+// 8 i-atoms two at a time, (ip, ip + 4) for ip = 0..3, in packed FP32 (read as
+// float4 pairs from shared memory), keeps its j-atom's force in a packed
+// register and adds it once per row; the i-forces live in 12 packed registers
+// per lane and are reduced across the warp once, after the list.
 // Pair arithmetic per lane and the order of every sum are fixed, so results
 // are bit-reproducible.
 template <int ES, bool ENERGY>
@@ -117,21 +119,18 @@ __global__ void __launch_bounds__(256, ENERGY ? 2 : 3) k_nonbonded(DevState st, 
     // energy steps: per-lane packed FP32 sums of LJ, Coulomb and virial
     // (a few tens of pairs each), converted to FP64 once per cluster
     f2p s_elj = zero2, s_ec = zero2, s_vir = zero2;
-    const int jj = lane & 7;
     const size_t base = (size_t)ci * st.pl_cap;
-    for (int k0 = 0; k0 < n; k0 += 4) {
-        const int k = k0 + (lane >> 3);
+    for (int k0 = 0; k0 < n; k0 += 32) {
+        const int k = k0 + lane;
         unsigned bits = 0u;
         int sj = 0;
         float4 xj = make_float4(0.f, 0.f, 0.f, 0.f);
         float2 ljj = make_float2(0.f, 0.f);
         if (k < n) {
-            const int ent = st.pl_j[base + k];
-            const unsigned long long mask = st.pl_mask[base + k];
-            bits = (unsigned)(mask >> (8 * jj)) & 0xffu;   // bit ii: pair (ii, jj)
-            const int cj = ent & ((1 << JCLUSTER_BITS) - 1);
-            const int3 sh = decode_shift((unsigned)ent >> JCLUSTER_BITS);
-            sj = cj * CLUSTER + jj;
+            const int2 row = st.pl_row[base + k];
+            bits = (unsigned)row.y & 0xffu;   // bit ii: pair (ii, this j-atom)
+            const int3 sh = decode_shift((unsigned)row.y >> 8);
+            sj = row.x;
             xj = st.xyzq[sj];
             ljj = st.ljp[sj];
             xj.x += sh.x * Lx;
@@ -364,24 +363,21 @@ __global__ void k_pairlist_dump(DevState st, NbParams p, long long cap, int* out
     const int n = st.pl_count[ci];
     const int sysi = st.cluster_sys[ci];
     const float Lx = st.sys[sysi].boxf[0], Ly = st.sys[sysi].boxf[1], Lz = st.sys[sysi].boxf[2];
-    const int ii = lane & 7, jj0 = lane >> 3;
-    const float4 xi = st.xyzq[ci * CLUSTER + ii];
-    const int ai = st.orig[ci * CLUSTER + ii];
     const size_t base = (size_t)ci * st.pl_cap;
-    for (int k = 0; k < n; ++k) {
-        const int ent = st.pl_j[base + k];
-        const unsigned long long mask = st.pl_mask[base + k];
-        const int cj = ent & ((1 << JCLUSTER_BITS) - 1);
-        const int3 sh = decode_shift((unsigned)ent >> JCLUSTER_BITS);
-        for (int h = 0; h < 2; ++h) {
-            const int jj = jj0 + 4 * h;
-            const float4 xj = st.xyzq[cj * CLUSTER + jj];
+    for (int k = lane; k < n; k += 32) {
+        const int2 row = st.pl_row[base + k];
+        const int sj = row.x;
+        const int3 sh = decode_shift((unsigned)row.y >> 8);
+        const float4 xj = st.xyzq[sj];
+        for (int ii = 0; ii < CLUSTER; ++ii) {
+            const float4 xi = st.xyzq[ci * CLUSTER + ii];
             const float dx = xj.x + sh.x * Lx - xi.x;
             const float dy = xj.y + sh.y * Ly - xi.y;
             const float dz = xj.z + sh.z * Lz - xi.z;
             const float r2 = dx * dx + dy * dy + dz * dz;
-            if (((mask >> (jj * 8 + ii)) & 1ull) && r2 <= p.rc2) {
-                const int aj = st.orig[cj * CLUSTER + jj];
+            if (((row.y >> ii) & 1) && r2 <= p.rc2) {
+                const int ai = st.orig[ci * CLUSTER + ii];
+                const int aj = st.orig[sj];
                 const unsigned long long w = atomicAdd(count, 1ull);
                 if ((long long)w < cap) {
                     out[2 * w] = min(ai, aj);
