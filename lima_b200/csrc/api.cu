@@ -689,7 +689,7 @@ PmePlan lima_engine::make_pme(std::vector<SysDesc>& sd, DevState& D) {
     }
     D.pme_total_real = pme_off;
     D.pme_total_cplx = pme_coff;
-    D.pme_grid_fx = dalloc<long long>(pme_off);
+    D.pme_grid_fx = dalloc<int>(pme_off);
     D.pme_real = dalloc<float>(pme_off);
     D.pme_cplx = dalloc<float2>(pme_coff);
     std::vector<float> theta(pme_coff, 0.f);
@@ -795,6 +795,40 @@ PmePlan lima_engine::make_pme(std::vector<SysDesc>& sd, DevState& D) {
         P.items_xy = upload(ixy);
         P.n_items_xy = (int)ixy.size();
         P.xy_buf = xy_buf;
+    }
+    // spreading by blocks of columns, each block's z range cut into chunks so
+    // that its box fits in shared memory and there are at least two items per SM
+    std::vector<int4> isp, geo(ns, make_int4(0, 0, 0, 0));
+    int box = 0;
+    long long blocks = 0;
+    for (int s = 0; s < ns; ++s)
+        if (sd[s].pme_n[0] > 0)
+            blocks += (long long)((sd[s].ncol_x + PME_SPREAD_COLS - 1) / PME_SPREAD_COLS) *
+                      ((sd[s].ncol_y + PME_SPREAD_COLS - 1) / PME_SPREAD_COLS);
+    int dev = 0, n_sm = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+    const int chunks = blocks > 0 ? (int)std::max(1LL, (2LL * n_sm + blocks - 1) / blocks) : 1;
+    for (int s = 0; s < ns; ++s) {
+        const SysDesc& Dd = sd[s];
+        if (Dd.pme_n[0] == 0) continue;
+        const int NX = pme_spread_box_side(Dd.col_w[0], Dd.pme_inv_h[0]);
+        const int NY = pme_spread_box_side(Dd.col_w[1], Dd.pme_inv_h[1]);
+        const int ZC = std::min({(Dd.pme_n[2] + chunks - 1) / chunks, Dd.pme_n[2], PME_SPREAD_MAX_BOX / (NX * NY)});
+        if (ZC < 4) {  // a box would not fit: keep per-weight atomics for every system
+            isp.clear();
+            break;
+        }
+        geo[s] = make_int4(NX, NY, ZC, 0);
+        box = std::max(box, NX * NY * ZC);
+        for (int z0 = 0; z0 < Dd.pme_n[2]; z0 += ZC)
+            for (int cy = 0; cy < Dd.ncol_y; cy += PME_SPREAD_COLS)
+                for (int cx = 0; cx < Dd.ncol_x; cx += PME_SPREAD_COLS) isp.push_back(make_int4(s, cx, cy, z0));
+    }
+    if (!isp.empty()) {
+        P.items_spread = upload(isp);
+        P.spread_geo = upload(geo);
+        P.n_items_spread = (int)isp.size();
+        P.spread_box = box;
     }
     pme_set_smem_limits(max_n, P.n_items_xy > 0 ? xy_buf : 0);
     return P;

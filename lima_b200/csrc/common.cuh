@@ -18,7 +18,10 @@ namespace lima {
 constexpr int CLUSTER = 8;                       // atoms per cluster
 constexpr double FORCE_SCALE = 4294967296.0;     // 2^32 per J/mol/nm
 constexpr double ENERGY_SCALE = 16777216.0;      // 2^24 per J/mol
-constexpr double GRID_SCALE = 1099511627776.0;   // 2^40 per kC/mol (PME charge grid)
+constexpr double GRID_SCALE = 1099511627776.0;   // 2^40 per kC/mol (int64 PME charge grid)
+// the engine's int32 PME charge grid: 2^20 per kC/mol, so a node holds up to
+// +-2048 kC/mol (about 21 e of B-spline-weighted charge) in steps of 1e-8 e
+constexpr double GRID32_SCALE = 1048576.0;
 constexpr int SHIFT_BITS = 5;                    // periodic-shift code in pair entries
 constexpr int JCLUSTER_BITS = 32 - SHIFT_BITS;
 

@@ -72,7 +72,7 @@ struct DevState {
     int2* pl_row = nullptr;
 
     // PME
-    long long* pme_grid_fx = nullptr;    // fixed-point charge grid (all systems)
+    int* pme_grid_fx = nullptr;          // fixed-point charge grid, GRID32_SCALE (all systems)
     float* pme_real = nullptr;           // real-space potential grid
     float2* pme_cplx = nullptr;          // half-complex grid
     float* pme_theta = nullptr;          // influence function on the half-complex grid
@@ -140,7 +140,21 @@ struct PmePlan {
     int n_items_xy = 0;
     int4* items_xy = nullptr;    // (system, z, 0, 0)
     int xy_buf = 0;              // float2 elements per ping-pong buffer
+    // charge spreading by column blocks (one CTA per item, a shared-memory box
+    // of grid nodes per CTA); none when a box would not fit
+    int n_items_spread = 0;
+    int4* items_spread = nullptr;   // (system, first column x, first column y, first z node)
+    int4* spread_geo = nullptr;     // per system: box nodes in x, y, z (0 = no grid)
+    int spread_box = 0;             // int32 elements of the largest box
 };
+constexpr int PME_SPREAD_COLS = 2;      // columns per block side
+// int32 nodes of a box (40 KB of shared memory): small enough for a 256-thread
+// spreading CTA to fit beside the pair kernel's CTAs on an SM, which the
+// higher-priority PME stream relies on to overlap the two
+constexpr int PME_SPREAD_MAX_BOX = 10240;
+// nodes of a block's box along x or y: the block's width in grid units plus the
+// order-4 stencil and one node of drift on each side
+int pme_spread_box_side(double col_w, double inv_h);
 // shared-memory elements of one buffer of the plane-fused x+y passes for a
 // K0 x K1 plane (0 = does not fit)
 int pme_xy_buffer(int k0, int k1);

@@ -2,9 +2,9 @@
 //
 // Replaces PME::Controller::CalcCharges (code/LIMA_ENGINE/src/PME.cuh:574-608):
 //   DistributeCompoundchargesToBlocksKernel + ChargeblockDistributeToGrid (:172-333)
-//       -> k_spread: every atom adds q*w to its 4^3 grid nodes as int64 fixed
-//          point (the reference uses int32 fixed point in 1 nm^3 shared tiles
-//          for the same reason: an order-free, deterministic sum)
+//       -> k_spread: every atom adds q*w to its 4^3 grid nodes as int32 fixed
+//          point (as the reference does, in 1 nm^3 shared tiles: an order-free,
+//          deterministic sum; here straight into the L2-resident grid)
 //   cufftExecR2C / ApplyGreensFunctionKernel / cufftExecC2R / Normalize (:585-599)
 //       -> five shared-memory passes of a hand-written mixed-radix (2,3,4,5)
 //          Stockham FFT: x (real->half complex), y, z (forward, x theta(k),
@@ -220,7 +220,7 @@ __global__ void k_spread(DevState st) {
     bspline4(f0, wx);
     bspline4(f1, wy);
     bspline4(f2, wz);
-    long long* g = st.pme_grid_fx + sd.pme_off;
+    int* g = st.pme_grid_fx + sd.pme_off;
     int ix[4];
 #pragma unroll
     for (int a = 0; a < 4; ++a) ix[a] = wrapk(b0 - 1 + a, K0);
@@ -230,9 +230,102 @@ __global__ void k_spread(DevState st) {
     for (int b = 0; b < 4; ++b) {
         const int y = wrapk(b1 - 1 + b, K1);
         const float qyz = qz * wy[b];
-        long long* row = g + (size_t)K0 * (y + (size_t)K1 * z);
+        int* row = g + (size_t)K0 * (y + (size_t)K1 * z);
 #pragma unroll
-        for (int a = 0; a < 4; ++a) atomic_add_fixed(row + ix[a], to_fixed(qyz * wx[a], GRID_SCALE));
+        for (int a = 0; a < 4; ++a) atomicAdd(row + ix[a], __float2int_rn(qyz * wx[a] * (float)GRID32_SCALE));
+    }
+}
+
+// Spreading by column blocks.  One CTA per item (system, block of
+// PME_SPREAD_COLS^2 columns of the pair-search grid, chunk of z nodes): every
+// charged atom of the block's columns adds its 4^3 weighted charges, owned by
+// the item's z chunk, into a shared-memory box of nodes, and the box goes to the
+// grid once, x-contiguous, empty nodes skipped — about a third of the global
+// atomics of one per weight, and coalesced.  A weight outside the box (an atom
+// that drifted from its column since the list build, or a grid too fine for the
+// box) is added to the grid directly.  Every weight is the same int32 as in
+// k_spread, so the grid holds the same integers.
+int pme_spread_box_side(double col_w, double inv_h) {
+    return (int)std::ceil(PME_SPREAD_COLS * col_w * inv_h) + 7;
+}
+
+__global__ void __launch_bounds__(256) k_spread_tiles(DevState st, const int4* items, const int4* geo) {
+    extern __shared__ int sbox[];
+    const int4 it = items[blockIdx.x];
+    const SysDesc& sd = st.sys[it.x];
+    const int4 gm = geo[it.x];
+    const int NX = gm.x, NY = gm.y, ZC = gm.z;
+    const int K0 = sd.pme_n[0], K1 = sd.pme_n[1], K2 = sd.pme_n[2];
+    const int z0 = it.w, nz = min(ZC, K2 - z0);
+    const int nbox = NX * NY * ZC;
+    for (int i = threadIdx.x; i < nbox; i += blockDim.x) sbox[i] = 0;
+    // box origin: two nodes below the block's lower edge (stencil start and drift)
+    const int ox = (int)floorf((float)it.y * sd.col_w[0] * sd.pme_inv_h[0]) - 2;
+    const int oy = (int)floorf((float)it.z * sd.col_w[1] * sd.pme_inv_h[1]) - 2;
+    __syncthreads();
+    int* g = st.pme_grid_fx + sd.pme_off;
+    const int cx1 = min(it.y + PME_SPREAD_COLS, sd.ncol_x), cy1 = min(it.z + PME_SPREAD_COLS, sd.ncol_y);
+    for (int cy = it.z; cy < cy1; ++cy) {
+        for (int cx = it.y; cx < cx1; ++cx) {
+            const int col = sd.col_off + cx + sd.ncol_x * cy;
+            const int s0 = st.col_cl_start[col] * CLUSTER;
+            const int ns = st.col_ncl[col] * CLUSTER;
+            // four threads per atom, one per z node of its stencil
+            for (int t = threadIdx.x; t < 4 * ns; t += blockDim.x) {
+                const int s = s0 + (t >> 2), c = t & 3;
+                const float4 p = st.xyzq[s];
+                if (p.w == 0.f || st.orig[s] < 0) continue;
+                int b0, b1, b2;
+                float f0, f1, f2;
+                grid_coord(p.z, sd.pme_inv_h[2], K2, b2, f2);
+                const int z = wrapk(b2 - 1 + c, K2);
+                const int lz = z - z0;
+                if (lz < 0 || lz >= nz) continue;   // another item's chunk
+                grid_coord(p.x, sd.pme_inv_h[0], K0, b0, f0);
+                grid_coord(p.y, sd.pme_inv_h[1], K1, b1, f1);
+                float wx[4], wy[4], wz[4];
+                bspline4(f0, wx);
+                bspline4(f1, wy);
+                bspline4(f2, wz);
+                // box-relative stencil start; b0 is wrapped into [0, K0), so take
+                // the periodic image nearest the box
+                int lx = b0 - 1 - ox, ly = b1 - 1 - oy;
+                if (lx < -K0 / 2) lx += K0;
+                else if (lx > NX + K0 / 2) lx -= K0;
+                if (ly < -K1 / 2) ly += K1;
+                else if (ly > NY + K1 / 2) ly -= K1;
+                const float qz = p.w * wz[c];
+                const bool inside = lx >= 0 && lx + 3 < NX && ly >= 0 && ly + 3 < NY;
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    const float qyz = qz * wy[b];
+#pragma unroll
+                    for (int a = 0; a < 4; ++a) {
+                        const int v = __float2int_rn(qyz * wx[a] * (float)GRID32_SCALE);
+                        if (inside) {
+                            atomicAdd(&sbox[(lx + a) + NX * ((ly + b) + NY * lz)], v);
+                        } else {
+                            const int x = wrapk(b0 - 1 + a, K0), y = wrapk(b1 - 1 + b, K1);
+                            atomicAdd(g + x + (size_t)K0 * (y + (size_t)K1 * z), v);
+                        }
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+    // one thread per (x, y) column of the box, walking its z nodes: consecutive
+    // threads add to consecutive x nodes of the grid
+    const int nxy = NX * NY;
+    const size_t zs = (size_t)K0 * K1;
+    for (int c = threadIdx.x; c < nxy; c += blockDim.x) {
+        const int ix = c % NX, iy = c / NX;
+        const int x = wrapk(ox + ix, K0), y = wrapk(oy + iy, K1);
+        int* gcol = g + x + (size_t)K0 * y + zs * z0;
+        for (int iz = 0; iz < nz; ++iz) {
+            const int v = sbox[c + nxy * iz];
+            if (v != 0) atomicAdd(gcol + zs * iz, v);
+        }
     }
 }
 
@@ -270,13 +363,13 @@ __global__ void k_fft_x_fwd(DevState st, const PmeSysDev* plans, const int4* ite
     float2* B = A + FFT_XLINES * (maxn + 1);
     load_twiddles(tw, pl, st.pme_tw);
     const int nl = it.z;
-    const long long* g = st.pme_grid_fx + sd.pme_off + (size_t)it.y * K0;
+    const int* g = st.pme_grid_fx + sd.pme_off + (size_t)it.y * K0;
     // the nl lines are contiguous: element i of the tile is g[i]
-    block_copy4<long long>(
+    block_copy4<int>(
         nl * K0, [&](int i) { return g[i]; },
-        [&](int i, long long v) {
+        [&](int i, int v) {
             const int l = i / K0, x = i - l * K0;
-            A[l * stride + x] = make_float2((float)((double)v * (1.0 / GRID_SCALE)), 0.f);
+            A[l * stride + x] = make_float2((float)v * (float)(1.0 / GRID32_SCALE), 0.f);
         });
     __syncthreads();
     const float2* res = fft_lines(A, B, nl, stride, pl, tw, -1.f);
@@ -433,15 +526,15 @@ __global__ void __launch_bounds__(FFT_XY_THREADS) k_fft_xy_fwd(DevState st, cons
     float2* B = A + buf;
     load_twiddles(twx, plx, st.pme_tw);
     load_twiddles(twy, ply, st.pme_tw);
-    const long long* g = st.pme_grid_fx + sd.pme_off + (size_t)K0 * K1 * z;
+    const int* g = st.pme_grid_fx + sd.pme_off + (size_t)K0 * K1 * z;
     const int sx = K0 + 1, sy = K1 + 1;
     block_copy4<float2>(
         P * K0,
         [&](int i) {
             const int pl = i / K0, x = i - pl * K0;
             const int ya = 2 * pl, yb = ya + 1;
-            const float a = (float)((double)g[(size_t)ya * K0 + x] * (1.0 / GRID_SCALE));
-            const float b = yb < K1 ? (float)((double)g[(size_t)yb * K0 + x] * (1.0 / GRID_SCALE)) : 0.f;
+            const float a = (float)g[(size_t)ya * K0 + x] * (float)(1.0 / GRID32_SCALE);
+            const float b = yb < K1 ? (float)g[(size_t)yb * K0 + x] * (float)(1.0 / GRID32_SCALE) : 0.f;
             return make_float2(a, b);
         },
         [&](int i, float2 v) {
@@ -632,9 +725,13 @@ int launch_pme(const DevState& st, const PmePlan& plan, bool energy, cudaStream_
     const int TB = 256;
     const int mx = plan.max_n;
     const size_t sx = fft_smem_bytes(FFT_XLINES, mx), sy = fft_smem_bytes(FFT_TX, mx);
-    cudaMemsetAsync(st.pme_grid_fx, 0, sizeof(long long) * (size_t)st.pme_total_real, s);
+    cudaMemsetAsync(st.pme_grid_fx, 0, sizeof(int) * (size_t)st.pme_total_real, s);
     const int g4 = (int)(((long long)st.n_slots * 4 + TB - 1) / TB);
-    k_spread<<<g4, TB, 0, s>>>(st);
+    if (plan.n_items_spread > 0)
+        k_spread_tiles<<<plan.n_items_spread, 256, (size_t)plan.spread_box * sizeof(int), s>>>(
+            st, plan.items_spread, plan.spread_geo);
+    else
+        k_spread<<<g4, TB, 0, s>>>(st);
     int n = 7;
     if (plan.n_items_xy > 0) {
         const size_t sxy = (size_t)(2 * mx + 2 * plan.xy_buf) * sizeof(float2);
@@ -697,6 +794,12 @@ void set_pme_sys_twiddles(void* dst, int offx, int offy, int offz) {
 // The attribute is per kernel and process-wide: it only ever grows, so an
 // engine with small grids cannot shrink the room another engine relies on.
 void pme_set_smem_limits(int maxn, int xy_buf) {
+    static bool spread_attr = false;
+    if (!spread_attr) {
+        cudaFuncSetAttribute(k_spread_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             PME_SPREAD_MAX_BOX * (int)sizeof(int));
+        spread_attr = true;
+    }
     static int largest_xy = 0;
     if (xy_buf > largest_xy) {
         largest_xy = xy_buf;
