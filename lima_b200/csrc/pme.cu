@@ -186,11 +186,21 @@ __device__ __forceinline__ int wrapk(int i, int n) {
     i %= n;
     return i < 0 ? i + n : i;
 }
+// i mod n for i in [-n, 2n): a node index at most one period outside the grid
+__device__ __forceinline__ int wrap1(int i, int n) {
+    return i < 0 ? i + n : (i >= n ? i - n : i);
+}
 
-// grid coordinate in [0,K): integer base and fraction
+// grid coordinate in [0,K): integer base and fraction.  Positions lie within a
+// box length of the box (wrapped at every list build, drifting a little
+// between builds), so one add or subtract of K brings u into range; anything
+// else (far away or non-finite) takes the general reduction.
 __device__ __forceinline__ void grid_coord(float x, float inv_h, int K, int& base, float& frac) {
     float u = x * inv_h;
-    u -= (float)K * floorf(u / (float)K);
+    const float Kf = (float)K;
+    if (u < 0.f) u += Kf;
+    else if (u >= Kf) u -= Kf;
+    if (!(u >= 0.f && u < Kf)) u -= Kf * floorf(u / Kf);
     float fl = floorf(u);
     base = (int)fl;
     frac = u - fl;
@@ -223,12 +233,12 @@ __global__ void k_spread(DevState st) {
     int* g = st.pme_grid_fx + sd.pme_off;
     int ix[4];
 #pragma unroll
-    for (int a = 0; a < 4; ++a) ix[a] = wrapk(b0 - 1 + a, K0);
-    const int z = wrapk(b2 - 1 + c, K2);
+    for (int a = 0; a < 4; ++a) ix[a] = wrap1(b0 - 1 + a, K0);
+    const int z = wrap1(b2 - 1 + c, K2);
     const float qz = p.w * wz[c];
 #pragma unroll
     for (int b = 0; b < 4; ++b) {
-        const int y = wrapk(b1 - 1 + b, K1);
+        const int y = wrap1(b1 - 1 + b, K1);
         const float qyz = qz * wy[b];
         int* row = g + (size_t)K0 * (y + (size_t)K1 * z);
 #pragma unroll
@@ -278,7 +288,7 @@ __global__ void __launch_bounds__(256) k_spread_tiles(DevState st, const int4* i
                 int b0, b1, b2;
                 float f0, f1, f2;
                 grid_coord(p.z, sd.pme_inv_h[2], K2, b2, f2);
-                const int z = wrapk(b2 - 1 + c, K2);
+                const int z = wrap1(b2 - 1 + c, K2);
                 const int lz = z - z0;
                 if (lz < 0 || lz >= nz) continue;   // another item's chunk
                 grid_coord(p.x, sd.pme_inv_h[0], K0, b0, f0);
@@ -305,7 +315,7 @@ __global__ void __launch_bounds__(256) k_spread_tiles(DevState st, const int4* i
                         if (inside) {
                             atomicAdd(&sbox[(lx + a) + NX * ((ly + b) + NY * lz)], v);
                         } else {
-                            const int x = wrapk(b0 - 1 + a, K0), y = wrapk(b1 - 1 + b, K1);
+                            const int x = wrap1(b0 - 1 + a, K0), y = wrap1(b1 - 1 + b, K1);
                             atomicAdd(g + x + (size_t)K0 * (y + (size_t)K1 * z), v);
                         }
                     }
@@ -320,7 +330,9 @@ __global__ void __launch_bounds__(256) k_spread_tiles(DevState st, const int4* i
     const size_t zs = (size_t)K0 * K1;
     for (int c = threadIdx.x; c < nxy; c += blockDim.x) {
         const int ix = c % NX, iy = c / NX;
-        const int x = wrapk(ox + ix, K0), y = wrapk(oy + iy, K1);
+        // ox, oy >= -2 and below K - 2: one period unless the box is wider than the grid
+        const int x = NX <= K0 ? wrap1(ox + ix, K0) : wrapk(ox + ix, K0);
+        const int y = NY <= K1 ? wrap1(oy + iy, K1) : wrapk(oy + iy, K1);
         int* gcol = g + x + (size_t)K0 * y + zs * z0;
         for (int iz = 0; iz < nz; ++iz) {
             const int v = sbox[c + nxy * iz];
@@ -656,15 +668,15 @@ __global__ void k_gather(DevState st) {
             int ix[4], ixp[4], ixm[4];
 #pragma unroll
             for (int a = 0; a < 4; ++a) {
-                ix[a] = wrapk(b0 - 1 + a, K0);
-                ixp[a] = wrapk(b0 + a, K0);
-                ixm[a] = wrapk(b0 - 2 + a, K0);
+                ix[a] = wrap1(b0 - 1 + a, K0);
+                ixp[a] = wrap1(b0 + a, K0);
+                ixm[a] = wrap1(b0 - 2 + a, K0);
             }
-            const int z = wrapk(b2 - 1 + c, K2);
+            const int z = wrap1(b2 - 1 + c, K2);
             const float wzc = wz[c], dzc = dz[c];
 #pragma unroll
             for (int b = 0; b < 4; ++b) {
-                const int y = wrapk(b1 - 1 + b, K1);
+                const int y = wrap1(b1 - 1 + b, K1);
                 const float* row = g + (size_t)K0 * (y + (size_t)K1 * z);
 #pragma unroll
                 for (int a = 0; a < 4; ++a) {
@@ -672,8 +684,8 @@ __global__ void k_gather(DevState st) {
                     const float w = wx[a] * wy[b] * wzc;
                     phi += w * v;
                     if (FD) {
-                        const int yp = wrapk(y + 1, K1), ym = wrapk(y - 1, K1);
-                        const int zp = wrapk(z + 1, K2), zm = wrapk(z - 1, K2);
+                        const int yp = wrap1(y + 1, K1), ym = wrap1(y - 1, K1);
+                        const int zp = wrap1(z + 1, K2), zm = wrap1(z - 1, K2);
                         gx += w * (row[ixp[a]] - row[ixm[a]]);
                         gy += w * (g[(size_t)K0 * (yp + (size_t)K1 * z) + ix[a]] -
                                    g[(size_t)K0 * (ym + (size_t)K1 * z) + ix[a]]);
