@@ -796,24 +796,17 @@ PmePlan lima_engine::make_pme(std::vector<SysDesc>& sd, DevState& D) {
         P.n_items_xy = (int)ixy.size();
         P.xy_buf = xy_buf;
     }
-    // spreading by blocks of columns, each block's z range cut into chunks so
-    // that its box fits in shared memory and there are at least two items per SM
+    // spreading and gathering by blocks of columns: the whole z range per block
+    // when its box fits in shared memory, else chunks of z nodes (each chunk's
+    // CTA walks the block's atoms and keeps the planes it owns)
     std::vector<int4> isp, geo(ns, make_int4(0, 0, 0, 0));
     int box = 0;
-    long long blocks = 0;
-    for (int s = 0; s < ns; ++s)
-        if (sd[s].pme_n[0] > 0)
-            blocks += (long long)((sd[s].ncol_x + PME_SPREAD_COLS - 1) / PME_SPREAD_COLS) *
-                      ((sd[s].ncol_y + PME_SPREAD_COLS - 1) / PME_SPREAD_COLS);
-    int dev = 0, n_sm = 148;
-    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-    const int chunks = blocks > 0 ? (int)std::max(1LL, (2LL * n_sm + blocks - 1) / blocks) : 1;
     for (int s = 0; s < ns; ++s) {
         const SysDesc& Dd = sd[s];
         if (Dd.pme_n[0] == 0) continue;
         const int NX = pme_spread_box_side(Dd.col_w[0], Dd.pme_inv_h[0]);
         const int NY = pme_spread_box_side(Dd.col_w[1], Dd.pme_inv_h[1]);
-        const int ZC = std::min({(Dd.pme_n[2] + chunks - 1) / chunks, Dd.pme_n[2], PME_SPREAD_MAX_BOX / (NX * NY)});
+        const int ZC = std::min(Dd.pme_n[2], PME_SPREAD_MAX_BOX / (NX * NY));
         if (ZC < 4) {  // a box would not fit: keep per-weight atomics for every system
             isp.clear();
             break;

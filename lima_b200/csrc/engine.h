@@ -147,13 +147,13 @@ struct PmePlan {
     int4* spread_geo = nullptr;     // per system: box nodes in x, y, z (0 = no grid)
     int spread_box = 0;             // int32 elements of the largest box
 };
-constexpr int PME_SPREAD_COLS = 2;      // columns per block side
+constexpr int PME_SPREAD_COLS = 1;      // columns per block side
 // int32 nodes of a box (40 KB of shared memory): small enough for a 256-thread
 // spreading CTA to fit beside the pair kernel's CTAs on an SM, which the
 // higher-priority PME stream relies on to overlap the two
 constexpr int PME_SPREAD_MAX_BOX = 10240;
 // nodes of a block's box along x or y: the block's width in grid units plus the
-// order-4 stencil and one node of drift on each side
+// order-4 stencil (atoms that drifted out of their column use the direct route)
 int pme_spread_box_side(double col_w, double inv_h);
 // shared-memory elements of one buffer of the plane-fused x+y passes for a
 // K0 x K1 plane (0 = does not fit)

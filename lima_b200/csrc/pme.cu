@@ -247,16 +247,20 @@ __global__ void k_spread(DevState st) {
 }
 
 // Spreading by column blocks.  One CTA per item (system, block of
-// PME_SPREAD_COLS^2 columns of the pair-search grid, chunk of z nodes): every
-// charged atom of the block's columns adds its 4^3 weighted charges, owned by
-// the item's z chunk, into a shared-memory box of nodes, and the box goes to the
-// grid once, x-contiguous, empty nodes skipped — about a third of the global
-// atomics of one per weight, and coalesced.  A weight outside the box (an atom
-// that drifted from its column since the list build, or a grid too fine for the
-// box) is added to the grid directly.  Every weight is the same int32 as in
-// k_spread, so the grid holds the same integers.
+// PME_SPREAD_COLS^2 columns of the pair-search grid, chunk of z nodes — the whole
+// z range unless the box would not fit): every charged atom of the block's
+// columns adds its 4^3 weighted charges, owned by the item's z chunk, into a
+// shared-memory box of nodes, and the box goes to the grid once, x-contiguous,
+// empty nodes skipped.  On a 0.1 nm grid with 0.43 nm columns a column's 12,000
+// weights land on about 5,000 nodes, so the grid sees 40 % of the atomics of one
+// per weight, coalesced.  A weight outside the box (an atom that drifted from its
+// column since the list build, or a grid too fine for the box) is added to the
+// grid directly.  Every weight is the same int32 as in k_spread, so the grid
+// holds the same integers.
 int pme_spread_box_side(double col_w, double inv_h) {
-    return (int)std::ceil(PME_SPREAD_COLS * col_w * inv_h) + 7;
+    // stencil start floor(u) - 1 with u in [u_lo, u_hi): nodes floor(u_lo) - 1 ..
+    // floor(u_hi) + 2, at most ceil(u_hi - u_lo) + 4 of them; one more for rounding
+    return (int)std::ceil(PME_SPREAD_COLS * col_w * inv_h) + 5;
 }
 
 __global__ void __launch_bounds__(256) k_spread_tiles(DevState st, const int4* items, const int4* geo) {
@@ -269,9 +273,9 @@ __global__ void __launch_bounds__(256) k_spread_tiles(DevState st, const int4* i
     const int z0 = it.w, nz = min(ZC, K2 - z0);
     const int nbox = NX * NY * ZC;
     for (int i = threadIdx.x; i < nbox; i += blockDim.x) sbox[i] = 0;
-    // box origin: two nodes below the block's lower edge (stencil start and drift)
-    const int ox = (int)floorf((float)it.y * sd.col_w[0] * sd.pme_inv_h[0]) - 2;
-    const int oy = (int)floorf((float)it.z * sd.col_w[1] * sd.pme_inv_h[1]) - 2;
+    // box origin: the stencil start of an atom on the block's lower edge
+    const int ox = (int)floorf((float)it.y * sd.col_w[0] * sd.pme_inv_h[0]) - 1;
+    const int oy = (int)floorf((float)it.z * sd.col_w[1] * sd.pme_inv_h[1]) - 1;
     __syncthreads();
     int* g = st.pme_grid_fx + sd.pme_off;
     const int cx1 = min(it.y + PME_SPREAD_COLS, sd.ncol_x), cy1 = min(it.z + PME_SPREAD_COLS, sd.ncol_y);
@@ -324,19 +328,24 @@ __global__ void __launch_bounds__(256) k_spread_tiles(DevState st, const int4* i
         }
     }
     __syncthreads();
-    // one thread per (x, y) column of the box, walking its z nodes: consecutive
-    // threads add to consecutive x nodes of the grid
-    const int nxy = NX * NY;
+    // one thread per (x, y) column of the box and group of eight z nodes:
+    // consecutive threads add to consecutive x nodes of the grid
+    const int nxy = NX * NY, ngz = (nz + 7) >> 3;
     const size_t zs = (size_t)K0 * K1;
-    for (int c = threadIdx.x; c < nxy; c += blockDim.x) {
+    for (int i = threadIdx.x; i < nxy * ngz; i += blockDim.x) {
+        const int c = i % nxy, iz0 = (i / nxy) << 3;
         const int ix = c % NX, iy = c / NX;
-        // ox, oy >= -2 and below K - 2: one period unless the box is wider than the grid
+        // ox, oy >= -1 and below K - 1: one period unless the box is wider than the grid
         const int x = NX <= K0 ? wrap1(ox + ix, K0) : wrapk(ox + ix, K0);
         const int y = NY <= K1 ? wrap1(oy + iy, K1) : wrapk(oy + iy, K1);
-        int* gcol = g + x + (size_t)K0 * y + zs * z0;
-        for (int iz = 0; iz < nz; ++iz) {
-            const int v = sbox[c + nxy * iz];
-            if (v != 0) atomicAdd(gcol + zs * iz, v);
+        int* gcol = g + x + (size_t)K0 * y + zs * (z0 + iz0);
+        const int m = min(8, nz - iz0);
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            if (u < m) {
+                const int v = sbox[c + nxy * (iz0 + u)];
+                if (v != 0) atomicAdd(gcol + zs * u, v);
+            }
         }
     }
 }
