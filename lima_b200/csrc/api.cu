@@ -230,6 +230,9 @@ struct lima_engine {
     }
     PmePlan make_pme(std::vector<SysDesc>& sd, DevState& D);
     void rebuild(bool from_input);
+    void start_rebuild(bool from_input);
+    void finish_rebuild();
+    bool begin_list();
     void rebuild_async();
     void forces(bool energy);
     void run_steps(int n);
@@ -975,24 +978,35 @@ void lima_engine::ensure_list() {
     }
 }
 
-void lima_engine::rebuild(bool from_input) {
-    for (int attempt = 0; attempt < 4; ++attempt) {
-        if (from_input) {
-            std::vector<double> pos((size_t)3 * st.n_atoms);
-            std::vector<float> vel((size_t)3 * st.n_atoms, 0.f);
-            for (size_t s = 0; s < sys.size(); ++s) {
-                std::copy(sys[s].pos.begin(), sys[s].pos.end(), pos.begin() + 3 * (size_t)n_atoms_off[s]);
-                if (sys[s].vel.size() == (size_t)3 * sys[s].n)
-                    std::copy(sys[s].vel.begin(), sys[s].vel.end(), vel.begin() + 3 * (size_t)n_atoms_off[s]);
-            }
-            CK(cudaMemcpyAsync(st.in_pos, pos.data(), pos.size() * sizeof(double), cudaMemcpyHostToDevice, s_main));
-            CK(cudaMemcpyAsync(st.in_vel, vel.data(), vel.size() * sizeof(float), cudaMemcpyHostToDevice, s_main));
+// List rebuild, part one: new slot order and cluster boxes (stages 1-7), no
+// host synchronisation.
+void lima_engine::start_rebuild(bool from_input) {
+    if (from_input) {
+        std::vector<double> pos((size_t)3 * st.n_atoms);
+        std::vector<float> vel((size_t)3 * st.n_atoms, 0.f);
+        for (size_t s = 0; s < sys.size(); ++s) {
+            std::copy(sys[s].pos.begin(), sys[s].pos.end(), pos.begin() + 3 * (size_t)n_atoms_off[s]);
+            if (sys[s].vel.size() == (size_t)3 * sys[s].n)
+                std::copy(sys[s].vel.begin(), sys[s].vel.end(), vel.begin() + 3 * (size_t)n_atoms_off[s]);
         }
-        CK(cudaMemsetAsync(st.status, 0, sizeof(unsigned), s_main));
-        mark(0, 0, s_main);
-        launches += launch_rebuild(st, (float)rlist, from_input, s_main);
-        mark(0, 1, s_main);
-        ++rebuilds;
+        CK(cudaMemcpyAsync(st.in_pos, pos.data(), pos.size() * sizeof(double), cudaMemcpyHostToDevice, s_main));
+        CK(cudaMemcpyAsync(st.in_vel, vel.data(), vel.size() * sizeof(float), cudaMemcpyHostToDevice, s_main));
+    }
+    CK(cudaMemsetAsync(st.status, 0, sizeof(unsigned), s_main));
+    mark(0, 0, s_main);
+    launches += launch_rebuild_slots(st, from_input, s_main);
+}
+
+// Part two: the pair search, then the host checks the status word.  A column
+// overflow rejects the build; a full pair list grows and only the search is
+// redone (the slots are final, and other streams may already be reading them).
+void lima_engine::finish_rebuild() {
+    for (int attempt = 0; attempt < 4; ++attempt) {
+        launches += launch_pairsearch(st, (float)rlist, s_main);
+        if (attempt == 0) {
+            mark(0, 1, s_main);
+            ++rebuilds;
+        }
         CK(cudaGetLastError());
         unsigned status = 0;
         CK(cudaMemcpyAsync(&status, st.status, sizeof(unsigned), cudaMemcpyDeviceToHost, s_main));
@@ -1002,23 +1016,47 @@ void lima_engine::rebuild(bool from_input) {
             list_age = 0;
             return;
         }
-        // grow the pair list and redo the build from the (unchanged) source
         const int cap = (st.pl_cap * 3 / 2 + 31) / 32 * 32;
         cudaFree(st.pl_row);
         allocs.erase(std::remove(allocs.begin(), allocs.end(), (void*)st.pl_row), allocs.end());
         st.pl_cap = cap;
         st.pl_row = dalloc<int2>((size_t)st.n_clusters * cap);
         drop_graph();
-        // the state is already permuted into slot order: rebuild from the slots
-        from_input = false;
+        CK(cudaMemsetAsync(st.status, 0, sizeof(unsigned), s_main));
     }
     throw ApiError{LIMA_ERR_OVERFLOW, "pair list overflow persists"};
+}
+
+void lima_engine::rebuild(bool from_input) {
+    start_rebuild(from_input);
+    finish_rebuild();
+}
+
+// The list step of forces(): when a rebuild is due, only its first part runs
+// here; forces() finishes it after the bonded and PME work has been queued on
+// its own streams, so that those overlap the pair search.  Returns whether a
+// pair search is pending.
+bool lima_engine::begin_list() {
+    if (phase_timing) {
+        ensure_list();
+        return false;
+    }
+    if (state_pending) {
+        start_rebuild(true);
+        state_pending = false;
+        return true;
+    }
+    if (list_age >= p.nstlist) {
+        start_rebuild(false);
+        return true;
+    }
+    return false;
 }
 
 // Pair-list rebuild without the host-side overflow check (inside a CUDA graph);
 // the status word is read after the replay.
 void lima_engine::rebuild_async() {
-    launches += launch_rebuild(st, (float)rlist, false, s_main);
+    launches += launch_rebuild_slots(st, false, s_main);
     ++rebuilds;
 }
 
@@ -1043,6 +1081,8 @@ void lima_engine::capture_period() {
         CK(cudaEventRecord(ev_bonded, s_bonded));
         if (pme_on) launches += launch_pme(st, pp, false, s_pme);
         CK(cudaEventRecord(ev_pme, s_pme));
+        // the period's pair search overlaps its first bonded and PME work
+        if (k == 0) launches += launch_pairsearch(st, (float)rlist, s_main);
         launches += launch_nonbonded(st, nb, false, s_main, nb_shape);
         CK(cudaStreamWaitEvent(s_main, ev_bonded, 0));
         CK(cudaStreamWaitEvent(s_main, ev_pme, 0));
@@ -1059,7 +1099,7 @@ void lima_engine::capture_period() {
 }
 
 void lima_engine::forces(bool energy) {
-    ensure_list();
+    const bool search_pending = begin_list();
     if (energy) {
         CK(cudaMemsetAsync(st.energy, 0, sizeof(long long) * E_COUNT * st.n_sys, s_main));
         CK(cudaMemsetAsync(st.epot, 0, sizeof(long long) * st.n_slots, s_main));
@@ -1084,6 +1124,7 @@ void lima_engine::forces(bool energy) {
         mark(3, 1, sp);
     }
     CK(cudaEventRecord(ev_pme, sp));
+    if (search_pending) finish_rebuild();
     mark(1, 0, s_main);
     launches += launch_nonbonded(st, nb, energy, s_main, nb_shape);
     mark(1, 1, s_main);

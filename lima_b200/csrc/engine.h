@@ -115,6 +115,8 @@ struct NbParams {
 
 // nbsearch.cu
 int launch_rebuild(const DevState& st, float rlist, bool from_input, cudaStream_t s);
+int launch_rebuild_slots(const DevState& st, bool from_input, cudaStream_t s);   // stages 1-7
+int launch_pairsearch(const DevState& st, float rlist, cudaStream_t s);          // stage 8
 // nonbonded.cu
 // shape: launch shape of the force-only kernel (bit 0 residency cap, bit 1 128-thread blocks)
 int launch_nonbonded(const DevState& st, const NbParams& p, bool energy, cudaStream_t s, int shape = 0);

@@ -78,9 +78,12 @@ __global__ void k_scan_columns(DevState st) {
             __syncthreads();
         }
         if (i < ncol) {
+            // clusters past the system's capacity are cut (the overflow flag makes
+            // the host reject the build), so that no reader leaves the system's slots
+            const int c0 = min(carry_c + sc[tid] - ncl, sd.max_clusters);
             st.col_atom_start[sd.col_off + i] = carry_a + sa[tid] - cnt;
-            st.col_cl_start[sd.col_off + i] = sd.cluster_cap_off + carry_c + sc[tid] - ncl;
-            st.col_ncl[sd.col_off + i] = ncl;
+            st.col_cl_start[sd.col_off + i] = sd.cluster_cap_off + c0;
+            st.col_ncl[sd.col_off + i] = min(ncl, sd.max_clusters - c0);
         }
         __syncthreads();
         if (tid == blockDim.x - 1) {
@@ -112,6 +115,7 @@ __global__ void k_sort_columns(DevState st, const int* col_sys) {
     const int n = min(n_all, st.col_cap);
     const int off = st.sys[col_sys[col]].atom_off + st.col_atom_start[col];
     const int slot0 = st.col_cl_start[col] * CLUSTER;
+    const int padded = st.col_ncl[col] * CLUSTER;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         const int a = st.col_list[off + i];
         keys[i] = ((unsigned long long)__float_as_uint(st.z_of_atom[a]) << 32) | (unsigned)a;
@@ -121,9 +125,8 @@ __global__ void k_sort_columns(DevState st, const int* col_sys) {
         const unsigned long long k = keys[i];
         int rank = 0;
         for (int j = 0; j < n; ++j) rank += keys[j] < k;
-        st.new_orig[slot0 + rank] = (int)(k & 0xffffffffu);
+        if (rank < padded) st.new_orig[slot0 + rank] = (int)(k & 0xffffffffu);   // cut on overflow
     }
-    const int padded = st.col_ncl[col] * CLUSTER;
     for (int r = n + threadIdx.x; r < padded; r += blockDim.x) st.new_orig[slot0 + r] = -1;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -393,9 +396,12 @@ __global__ void __launch_bounds__(PS_WARPS * 32, 1) k_pairsearch(DevState st, fl
             const int col = sd.col_off + cx + sd.ncol_x * cy;
             const int j0 = st.col_cl_start[col];
             const int nj = st.col_ncl[col];
+            // clusters are numbered in column order: a column whose clusters all
+            // precede ci holds no pair of ci's half list (warp-uniform skip)
+            const bool live = j0 + nj > ci;
             const int j = j0 + b + lane;
             unsigned shifts = 0u;  // bit k set: shift code k is in range
-            if (b + lane < nj && j >= ci) {
+            if (live && b + lane < nj && j >= ci) {
                 const float4 jlo = st.bb_lo[j], jhi = st.bb_hi[j];
                 const float jc[3] = {0.5f * (jlo.x + jhi.x), 0.5f * (jlo.y + jhi.y), 0.5f * (jlo.z + jhi.z)};
                 const float je[3] = {0.5f * (jhi.x - jlo.x), 0.5f * (jhi.y - jlo.y), 0.5f * (jhi.z - jlo.z)};
@@ -436,23 +442,25 @@ __global__ void __launch_bounds__(PS_WARPS * 32, 1) k_pairsearch(DevState st, fl
                     }
                 }
             }
-            // append (cluster, shift) candidates in lane order, then shift order
-            const int c = __popc(shifts);
-            int incl = c;
+            if (live) {
+                // append (cluster, shift) candidates in lane order, then shift order
+                const int c = __popc(shifts);
+                int incl = c;
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int t = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += t;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += t;
+                }
+                const int total = __shfl_sync(0xffffffffu, incl, 31);
+                int w = qn + incl - c;
+                while (shifts) {
+                    const int code = __ffs(shifts) - 1;
+                    shifts &= shifts - 1u;
+                    q[wib][w++] = j | (code << JCLUSTER_BITS);
+                }
+                qn += total;
             }
-            const int total = __shfl_sync(0xffffffffu, incl, 31);
-            int w = qn + incl - c;
-            while (shifts) {
-                const int code = __ffs(shifts) - 1;
-                shifts &= shifts - 1u;
-                q[wib][w++] = j | (code << JCLUSTER_BITS);
-            }
-            qn += total;
-            b += 32;
+            b = live ? b + 32 : nj;
             if (b >= nj) {
                 b = 0;
                 if (++cx == sd.ncol_x) cx = 0;
@@ -488,7 +496,10 @@ __global__ void __launch_bounds__(PS_WARPS * 32, 1) k_pairsearch(DevState st, fl
     }
 }
 
-int launch_rebuild(const DevState& st, float rlist, bool from_input, cudaStream_t s) {
+// Stages 1-7: the new slot order and the cluster boxes.  Everything but the
+// pair kernel (bonded terms, PME, the learned descriptor) can run once this is
+// done, concurrently with the pair search.
+int launch_rebuild_slots(const DevState& st, bool from_input, cudaStream_t s) {
     const int TB = 256;
     k_bin<<<(st.n_atoms + TB - 1) / TB, TB, 0, s>>>(st, from_input ? 1 : 0);
     k_scan_columns<<<st.n_sys, 1024, 0, s>>>(st);
@@ -497,10 +508,19 @@ int launch_rebuild(const DevState& st, float rlist, bool from_input, cudaStream_
     k_gather_slots<<<(st.n_slots + TB - 1) / TB, TB, 0, s>>>(st, from_input ? 1 : 0);
     k_finish_slots<<<(st.n_slots + TB - 1) / TB, TB, 0, s>>>(st);
     k_bbox<<<(st.n_clusters + TB - 1) / TB, TB, 0, s>>>(st);
+    return 7;
+}
+
+// Stage 8: the pair list of the current slots.
+int launch_pairsearch(const DevState& st, float rlist, cudaStream_t s) {
     const long long threads = (long long)st.n_clusters * 32;
     const int TP = PS_WARPS * 32;
     k_pairsearch<<<(unsigned)((threads + TP - 1) / TP), TP, 0, s>>>(st, rlist);
-    return 8;
+    return 1;
+}
+
+int launch_rebuild(const DevState& st, float rlist, bool from_input, cudaStream_t s) {
+    return launch_rebuild_slots(st, from_input, s) + launch_pairsearch(st, rlist, s);
 }
 
 }  // namespace lima
