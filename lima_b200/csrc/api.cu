@@ -112,7 +112,8 @@ struct lima_engine {
     double tune_ms[4] = {0, 0, 0, 0};
 
     // device scratch for readback
-    unsigned* d_disp = nullptr;       // largest squared move since the last list build (float bits)
+    unsigned* d_disp = nullptr;       // [0] largest squared move since the last list build (float bits),
+                                      // [1] non-finite input flag
     int64_t state_fast_loads = 0;     // lima_set_state calls served without a rebuild
     double* d_out_d = nullptr;
     float* d_out_f = nullptr;
@@ -234,7 +235,7 @@ struct lima_engine {
     void finish_rebuild();
     bool begin_list();
     void rebuild_async();
-    void forces(bool energy);
+    void forces(bool energy, bool atom_energy = false);
     void run_steps(int n);
     void capture_period();
     void read_energies(lima_energies* e);
@@ -663,7 +664,7 @@ void lima_engine::setup() {
     ip.dt = p.dt;
     ip.integrator = p.integrator;
 
-    d_disp = dalloc<unsigned>(1);
+    d_disp = dalloc<unsigned>(2);
     d_out_d = dalloc<double>(3 * (size_t)N);
     d_out_f = dalloc<float>(3 * (size_t)N);
     d_maxf = dalloc<float>(1);
@@ -947,6 +948,7 @@ void lima_engine::learned_full(cudaStream_t s, bool energy) {
     CK(cudaMemsetAsync(lp_ff, 0, sizeof(long long) * 3 * (size_t)st.n_slots, s));
     st_f.pme_grid_fx = st.pme_grid_fx;
     st_f.energy = st.energy;
+    st_f.atom_energy = st.atom_energy;
     launches += launch_pme(st_f, pp, energy, s);
 }
 
@@ -1098,11 +1100,14 @@ void lima_engine::capture_period() {
     phase_timing = pt;
 }
 
-void lima_engine::forces(bool energy) {
+// atom_energy: an energy evaluation that also fills the per-atom shares (epot)
+// of a log frame
+void lima_engine::forces(bool energy, bool atom_energy) {
     const bool search_pending = begin_list();
+    st.atom_energy = energy && atom_energy ? 1 : 0;
     if (energy) {
         CK(cudaMemsetAsync(st.energy, 0, sizeof(long long) * E_COUNT * st.n_sys, s_main));
-        CK(cudaMemsetAsync(st.epot, 0, sizeof(long long) * st.n_slots, s_main));
+        if (st.atom_energy) CK(cudaMemsetAsync(st.epot, 0, sizeof(long long) * st.n_slots, s_main));
     }
     launch_zero_forces(st, s_main);
     // with phase timing on, every phase runs on the main stream so that each
@@ -1158,7 +1163,7 @@ void lima_engine::run_steps(int n) {
     for (; k < n; ++k) {
         const bool log_now = p.log_interval > 0 && step % p.log_interval == 0;
         const bool energy = k == n - 1 || log_now;
-        forces(energy);
+        forces(energy, log_now);
         mark(4, 0, s_main);
         launches += launch_integrate(st, ip, energy, s_main);
         mark(4, 1, s_main);
@@ -1482,12 +1487,12 @@ int lima_set_state(lima_engine* h, const double* pos, const float* vel) {
     SystemHost& S = h->sys[h->cur];
     if (S.n <= 0) return fail(h, LIMA_ERR_STATE, "lima_set_atoms must precede lima_set_state");
     if (!pos) return fail(h, LIMA_ERR_INVALID_ARG, "positions required");
-    for (int i = 0; i < 3 * S.n; ++i)
-        if (!std::isfinite(pos[i])) return fail(h, LIMA_ERR_NOT_FINITE, "non-finite position");
     return guarded(h, [&]() {
         if (h->built && !h->state_pending) {
             // Fast path: the atoms keep their slots; the pair list stays valid while no
-            // atom has moved more than half the Verlet buffer since it was built.
+            // atom has moved more than half the Verlet buffer since it was built.  The
+            // input is staged and checked on the device (finite, largest move) before
+            // it replaces the slot state.
             cudaStream_t s = h->s_main;
             const size_t o = 3 * (size_t)h->n_atoms_off[h->cur];
             CK(cudaMemcpyAsync(h->st.in_pos + o, pos, 3 * (size_t)S.n * sizeof(double), cudaMemcpyHostToDevice, s));
@@ -1495,11 +1500,14 @@ int lima_set_state(lima_engine* h, const double* pos, const float* vel) {
                 CK(cudaMemcpyAsync(h->st.in_vel + o, vel, 3 * (size_t)S.n * sizeof(float), cudaMemcpyHostToDevice, s));
             else
                 CK(cudaMemsetAsync(h->st.in_vel + o, 0, 3 * (size_t)S.n * sizeof(float), s));
-            CK(cudaMemsetAsync(h->d_disp, 0, sizeof(unsigned), s));
-            h->launches += launch_load_state(h->st, h->n_atoms_off[h->cur], S.n, h->d_disp, s);
-            unsigned bits = 0;
-            CK(cudaMemcpyAsync(&bits, h->d_disp, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+            CK(cudaMemsetAsync(h->d_disp, 0, 2 * sizeof(unsigned), s));
+            h->launches += launch_check_state(h->st, h->n_atoms_off[h->cur], S.n, h->d_disp, s);
+            unsigned word[2] = {0u, 0u};
+            CK(cudaMemcpyAsync(word, h->d_disp, sizeof(word), cudaMemcpyDeviceToHost, s));
             CK(cudaStreamSynchronize(s));
+            if (word[1]) return fail(h, LIMA_ERR_NOT_FINITE, "non-finite position");
+            h->launches += launch_load_state(h->st, h->n_atoms_off[h->cur], S.n, s);
+            const unsigned bits = word[0];
             float d2;
             std::memcpy(&d2, &bits, sizeof(float));
             const double half_skin = 0.5 * (h->rlist - h->p.cutoff);
@@ -1508,6 +1516,8 @@ int lima_set_state(lima_engine* h, const double* pos, const float* vel) {
             ++h->state_fast_loads;
             return LIMA_OK;
         }
+        for (int i = 0; i < 3 * S.n; ++i)
+            if (!std::isfinite(pos[i])) return fail(h, LIMA_ERR_NOT_FINITE, "non-finite position");
         // pull the device state of the other systems first so they are kept
         if (h->built && !h->state_pending && h->sys.size() > 1) {
             std::vector<double> pp((size_t)3 * h->st.n_atoms);

@@ -231,7 +231,7 @@ __global__ void k_bonded(DevState st, BondedTerms bt) {
             add_force(st, atoms[k], f[k]);
             if (ENERGY) {
                 vir += -0.5f * dot(r[k], f[k]);
-                add_atom_energy(st.epot, st.slot_of[atoms[k]], (double)en / na);  // equal shares
+                if (st.atom_energy) add_atom_energy(st.epot, st.slot_of[atoms[k]], (double)en / na);  // equal shares
             }
         }
         if (ENERGY) e[kind] = en;

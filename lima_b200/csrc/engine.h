@@ -16,6 +16,7 @@ struct DevState {
     int n_slots = 0;          // 8 * n_clusters
     int n_cols = 0;           // all columns
     int pl_cap = 0;           // pair-list rows per i-cluster
+    int atom_energy = 0;      // energy evaluations also add per-atom shares to epot (log frames)
     int col_cap = 0;          // atoms a column may hold
 
     SysDesc* sys = nullptr;
@@ -181,7 +182,8 @@ int launch_kinetic(const DevState& st, long long* ke, cudaStream_t s);
 // new positions and velocities (original order, in_pos / in_vel) for atoms
 // [a0, a0 + n) written into their current slots; the largest squared move from
 // the last pair-list build goes to *max_disp2 (float bits, atomic max)
-int launch_load_state(const DevState& st, int a0, int n, unsigned* max_disp2, cudaStream_t s);
+int launch_check_state(const DevState& st, int a0, int n, unsigned* word2, cudaStream_t s);
+int launch_load_state(const DevState& st, int a0, int n, cudaStream_t s);
 // one log frame in original atom order: (x, y, z, potential energy), (F, |v|)
 int launch_log_frame(const DevState& st, float4* pos_epot, float4* force_speed, cudaStream_t s);
 

@@ -214,40 +214,64 @@ int launch_log_frame(const DevState& st, float4* pos_epot, float4* force_speed, 
     return 1;
 }
 
-// State handed in by the caller for atoms that keep their slots: positions and
-// velocities replace the slot state (previous-step force and minimiser moments
-// restart at zero, as after a full rebuild from new input), and the largest move
-// since the last pair-list build decides on the host whether the list still holds.
-__global__ void k_load_state(DevState st, int a0, int n, unsigned* max_disp2) {
+// State handed in by the caller for atoms that keep their slots, in two steps.
+// k_check_state reads the staged input only: word[0] receives the largest
+// squared move since the last pair-list build (float bits; it decides on the
+// host whether the list still holds) and word[1] is set when a position is not
+// finite, so that the host can refuse the call with the engine untouched.
+__global__ void k_check_state(DevState st, int a0, int n, unsigned* word) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     float d2 = 0.f;
+    bool bad = false;
     if (i < n) {
         const int a = a0 + i;
         const int s = st.slot_of[a];
         const double x = st.in_pos[3 * a], y = st.in_pos[3 * a + 1], z = st.in_pos[3 * a + 2];
-        st.px[s] = x;
-        st.py[s] = y;
-        st.pz[s] = z;
-        const float4 old = st.xyzq[s];
-        st.xyzq[s] = make_float4((float)x, (float)y, (float)z, old.w);
-        const float4 v = st.vel[s];
-        st.vel[s] = make_float4(st.in_vel[3 * a], st.in_vel[3 * a + 1], st.in_vel[3 * a + 2], v.w);
-        st.fprev[s] = make_float4(0.f, 0.f, 0.f, 0.f);
-        st.adam_m[s] = make_float4(0.f, 0.f, 0.f, 0.f);
-        st.adam_v[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+        bad = !(isfinite(x) && isfinite(y) && isfinite(z));
         const float4 r = st.xyz_ref[s];
         const float dx = (float)x - r.x, dy = (float)y - r.y, dz = (float)z - r.z;
         d2 = dx * dx + dy * dy + dz * dz;
-        if (!(d2 < 3.0e38f)) d2 = 3.0e38f;   // non-finite: force a rebuild
+        if (!(d2 < 3.0e38f)) d2 = 3.0e38f;
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) d2 = fmaxf(d2, __shfl_xor_sync(0xffffffffu, d2, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(max_disp2, __float_as_uint(d2));
+    const bool any_bad = __any_sync(0xffffffffu, bad);
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(word, __float_as_uint(d2));
+        if (any_bad) atomicOr(word + 1, 1u);
+    }
 }
 
-int launch_load_state(const DevState& st, int a0, int n, unsigned* max_disp2, cudaStream_t s) {
+// ... then k_load_state commits it: positions and velocities replace the slot
+// state (previous-step force and minimiser moments restart at zero, as after a
+// full rebuild from new input).
+__global__ void k_load_state(DevState st, int a0, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int a = a0 + i;
+    const int s = st.slot_of[a];
+    const double x = st.in_pos[3 * a], y = st.in_pos[3 * a + 1], z = st.in_pos[3 * a + 2];
+    st.px[s] = x;
+    st.py[s] = y;
+    st.pz[s] = z;
+    const float4 old = st.xyzq[s];
+    st.xyzq[s] = make_float4((float)x, (float)y, (float)z, old.w);
+    const float4 v = st.vel[s];
+    st.vel[s] = make_float4(st.in_vel[3 * a], st.in_vel[3 * a + 1], st.in_vel[3 * a + 2], v.w);
+    st.fprev[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+    st.adam_m[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+    st.adam_v[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+int launch_check_state(const DevState& st, int a0, int n, unsigned* word2, cudaStream_t s) {
     const int TB = 256;
-    k_load_state<<<(n + TB - 1) / TB, TB, 0, s>>>(st, a0, n, max_disp2);
+    k_check_state<<<(n + TB - 1) / TB, TB, 0, s>>>(st, a0, n, word2);
+    return 1;
+}
+
+int launch_load_state(const DevState& st, int a0, int n, cudaStream_t s) {
+    const int TB = 256;
+    k_load_state<<<(n + TB - 1) / TB, TB, 0, s>>>(st, a0, n);
     return 1;
 }
 

@@ -82,8 +82,10 @@ __device__ __forceinline__ float ex2_approx(float x) {
 // per lane and are reduced across the warp once, after the list.
 // Pair arithmetic per lane and the order of every sum are fixed, so results
 // are bit-reproducible.
-template <int ES, bool ENERGY>
-__global__ void __launch_bounds__(256, ENERGY ? 2 : 3) k_nonbonded(DevState st, NbParams p) {
+// EN: 0 forces only, 1 forces and energy totals, 2 also per-atom energy shares
+template <int ES, int EN>
+__global__ void __launch_bounds__(256, EN ? 2 : 3) k_nonbonded(DevState st, NbParams p) {
+    constexpr bool ENERGY = EN > 0, ATOM = EN > 1;
     // per warp, i-atom pairs (ip, ip + 4): (x0, x1, y0, y1), (z0, z1, q0 ke, q1 ke),
     // (sigma0/2, sigma1/2, 24 sqrt(eps0), 24 sqrt(eps1))
     __shared__ float4 s_xy[8][4], s_zq[8][4], s_lj[8][4];
@@ -207,9 +209,11 @@ __global__ void __launch_bounds__(256, ENERGY ? 2 : 3) k_nonbonded(DevState st, 
                 s_elj = add2(s_elj, elj);
                 s_ec = add2(s_ec, ecm);
                 s_vir = fma2(fs, r2, s_vir);   // fs is already dropped; -1/2 r_ij . f_ij = fs r^2 / 2
-                const f2p eh = mul2(splat2(0.5f), add2(elj, ecm));
-                ei[ip] = add2(ei[ip], eh);
-                ej = add2(ej, eh);
+                if (ATOM) {
+                    const f2p eh = mul2(splat2(0.5f), add2(elj, ecm));
+                    ei[ip] = add2(ei[ip], eh);
+                    ej = add2(ej, eh);
+                }
             }
         }
         if (bits) {
@@ -217,7 +221,7 @@ __global__ void __launch_bounds__(256, ENERGY ? 2 : 3) k_nonbonded(DevState st, 
             atomic_add_fixed(st.fx + sj, to_fixed(x.x + x.y, FORCE_SCALE));
             atomic_add_fixed(st.fy + sj, to_fixed(y.x + y.y, FORCE_SCALE));
             atomic_add_fixed(st.fz + sj, to_fixed(z.x + z.y, FORCE_SCALE));
-            if (ENERGY) {
+            if (ATOM) {
                 const float2 e = up2(ej);
                 add_atom_energy(st.epot, sj, (double)(e.x + e.y));
             }
@@ -240,7 +244,7 @@ __global__ void __launch_bounds__(256, ENERGY ? 2 : 3) k_nonbonded(DevState st, 
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
             fi[a][c] = v;
         }
-        if (ENERGY) {
+        if (ATOM) {
             float v = eiv[a];
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -256,7 +260,7 @@ __global__ void __launch_bounds__(256, ENERGY ? 2 : 3) k_nonbonded(DevState st, 
         atomic_add_fixed(st.fx + si, to_fixed(vx, FORCE_SCALE));
         atomic_add_fixed(st.fy + si, to_fixed(vy, FORCE_SCALE));
         atomic_add_fixed(st.fz + si, to_fixed(vz, FORCE_SCALE));
-        if (ENERGY) add_atom_energy(st.epot, si, (double)ve);
+        if (ATOM) add_atom_energy(st.epot, si, (double)ve);
     }
     if (ENERGY) {
         const float2 el = up2(s_elj), ecs = up2(s_ec), vr = up2(s_vir);
@@ -280,17 +284,18 @@ static void launch_nb_shape(const DevState& st, const NbParams& p, bool energy, 
     const int tb = (shape & 2) ? 128 : 256;
     const dim3 grid((unsigned)((threads + tb - 1) / tb));
     if (energy) {
-        k_nonbonded<ES, true><<<grid, tb, 0, s>>>(st, p);
+        if (st.atom_energy) k_nonbonded<ES, 2><<<grid, tb, 0, s>>>(st, p);
+        else k_nonbonded<ES, 1><<<grid, tb, 0, s>>>(st, p);
         return;
     }
     // 16 warps per SM: 2 blocks of 256 threads (90 KB each) or 4 of 128 (50 KB each)
     const int reserve = (shape & 1) ? ((shape & 2) ? 50 * 1024 : 90 * 1024) : 0;
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_nonbonded<ES, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 90 * 1024);
+        cudaFuncSetAttribute(k_nonbonded<ES, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 90 * 1024);
         attr = true;
     }
-    k_nonbonded<ES, false><<<grid, tb, reserve, s>>>(st, p);
+    k_nonbonded<ES, 0><<<grid, tb, reserve, s>>>(st, p);
 }
 
 int launch_nonbonded(const DevState& st, const NbParams& p, bool energy, cudaStream_t s, int shape) {
@@ -334,8 +339,10 @@ __global__ void k_exclusion_correction(DevState st, BondedTerms bt, NbParams p) 
         atomic_add_fixed(st.fz + sj, to_fixed(-fz, FORCE_SCALE));
         if (ENERGY) {
             e = -(double)qq * (double)erf_kr * (double)rinv;
-            add_atom_energy(st.epot, si, 0.5 * e);
-            add_atom_energy(st.epot, sj, 0.5 * e);
+            if (st.atom_energy) {
+                add_atom_energy(st.epot, si, 0.5 * e);
+                add_atom_energy(st.epot, sj, 0.5 * e);
+            }
         }
     }
     if (ENERGY) add_energy_fixed(st.energy, sysi, e, E_EXCL);

@@ -727,9 +727,11 @@ __global__ void k_gather(DevState st) {
         if (ENERGY) {
             e = 0.5 * (double)q * (double)phi;
             // the atom's reciprocal energy and its share of the Ewald self term
-            const SysDesc& sd = st.sys[sysi];
-            const double self = sd.self_per_charge ? (double)sd.self_coef : (double)sd.self_coef * q * q;
-            add_atom_energy(st.epot, s, e + self);
+            if (st.atom_energy) {
+                const SysDesc& sd = st.sys[sysi];
+                const double self = sd.self_per_charge ? (double)sd.self_coef : (double)sd.self_coef * q * q;
+                add_atom_energy(st.epot, s, e + self);
+            }
         }
     }
     if (ENERGY) add_energy_fixed(st.energy, c == 0 ? sysi : -1, e, E_RECIP);

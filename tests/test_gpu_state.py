@@ -4,7 +4,7 @@ built; larger moves rebuild it.  Results must not depend on which path ran."""
 import numpy as np
 import pytest
 
-from lima_b200 import Engine, systems
+from lima_b200 import Engine, LimaError, systems
 from lima_b200 import engine as E
 from tests._ref import kappa_from_tol, oracle_total, rel_rms
 
@@ -79,3 +79,24 @@ def test_autotune_shapes_give_identical_trajectories():
     pb, vb = b.state()
     assert np.array_equal(pa, pb) and np.array_equal(va, vb)
     assert a.energies()["potential"] == b.energies()["potential"]
+
+
+def test_nonfinite_state_refused_on_built_engine():
+    """On a built engine the handed-in state is checked on the device before it
+    replaces the slot state: a non-finite position is refused with
+    LIMA_ERR_NOT_FINITE and leaves the engine exactly as it was."""
+    s = systems.water_box(600, 3.0, seed=4)
+    e = Engine(cutoff=1.0, electrostatics=E.ES_EWALD, ewald_tol=1e-5)
+    e.load(s, pme_grid=(30, 30, 30))
+    e.step(3)
+    p0, v0 = e.state()
+    bad = p0.copy()
+    bad[17, 2] = np.inf
+    with pytest.raises(LimaError) as ex:
+        e.set_state(bad, v0)
+    assert ex.value.code == 7
+    p1, v1 = e.state()
+    assert np.array_equal(p0, p1) and np.array_equal(v0, v1)
+    e.set_state(p0, v0)
+    e.step(2)
+    assert np.isfinite(e.energies()["total"])
