@@ -249,7 +249,7 @@ __device__ __forceinline__ int wrapi(int i, int n) {
 constexpr int PS_WARPS = 4;
 constexpr int PS_QCAP = 32 + 32 * 27;   // a full batch left over + one column batch with every shift
 
-__global__ void __launch_bounds__(PS_WARPS * 32, 6) k_pairsearch(DevState st, float rlist) {
+__global__ void __launch_bounds__(PS_WARPS * 32, 1) k_pairsearch(DevState st, float rlist) {
     __shared__ int q[PS_WARPS][PS_QCAP];
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
