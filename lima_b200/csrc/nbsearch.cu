@@ -251,6 +251,7 @@ constexpr int PS_QCAP = 32 + 32 * 27;   // a full batch left over + one column b
 
 __global__ void __launch_bounds__(PS_WARPS * 32, 1) k_pairsearch(DevState st, float rlist) {
     __shared__ int q[PS_WARPS][PS_QCAP];
+    __shared__ int s_mi[PS_WARPS][CLUSTER], s_ai[PS_WARPS][CLUSTER];
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     if (warp >= st.n_clusters) return;
@@ -272,17 +273,21 @@ __global__ void __launch_bounds__(PS_WARPS * 32, 1) k_pairsearch(DevState st, fl
     // the eight i-atoms in every lane's registers; a padding i-atom is moved far
     // away so that no distance test passes for it
     float xi[CLUSTER], yi[CLUSTER], zi[CLUSTER];
-    int mi[CLUSTER];
 #pragma unroll
     for (int a = 0; a < CLUSTER; ++a) {
         const int s = ci * CLUSTER + a;
         const float4 x = st.xyzq[s];
-        mi[a] = st.slot_mol[s];
         const bool real = st.orig[s] >= 0;
         xi[a] = real ? x.x : 1e30f;
         yi[a] = real ? x.y : 1e30f;
         zi[a] = real ? x.z : 1e30f;
     }
+    // molecule ids and atom indices of the i-atoms, for the rare exclusion test
+    if (lane < CLUSTER) {
+        s_mi[wib][lane] = st.slot_mol[ci * CLUSTER + lane];
+        s_ai[wib][lane] = st.orig[ci * CLUSTER + lane];
+    }
+    __syncwarp();
 
     // column window (every column visited once even when the window wraps).
     // When it does not cover a whole row of columns, each column in it is met
@@ -309,23 +314,25 @@ __global__ void __launch_bounds__(PS_WARPS * 32, 1) k_pairsearch(DevState st, fl
     int count = 0;
     const size_t base_out = (size_t)ci * cap;
 
-    // masks of the queued candidates q[head .. head + nb), one per lane
+    // rows of the queued candidates q[head .. head + nb): four candidates per
+    // pass, one lane per (candidate, j-atom), each lane testing its j-atom against
+    // the 8 i-atoms; rows leave in candidate order, then j-atom order
     auto build_masks = [&](int head, int nb) {
-        unsigned long long mask = 0ull;
-        int ent = 0;
-        if (lane < nb) {
-            ent = q[wib][head + lane];
-            const int jc = ent & ((1 << JCLUSTER_BITS) - 1);
-            const int3 sh = decode_shift((unsigned)ent >> JCLUSTER_BITS);
-            const float shx = sh.x * L[0], shy = sh.y * L[1], shz = sh.z * L[2];
-            const bool share_mol = (isig & st.bb_molsig[jc]) != 0ull;
-#pragma unroll
-            for (int jj = 0; jj < CLUSTER; ++jj) {
-                const int sj = jc * CLUSTER + jj;
+        const int jj = lane & 7;
+#pragma unroll 1
+        for (int c0 = 0; c0 < nb; c0 += 4) {
+            const int c = c0 + (lane >> 3);
+            unsigned m8 = 0u;
+            int sj = 0, code = 0;
+            if (c < nb) {
+                const int ent = q[wib][head + c];
+                const int jc = ent & ((1 << JCLUSTER_BITS) - 1);
+                code = (int)((unsigned)ent >> JCLUSTER_BITS);
+                const int3 sh = decode_shift(code);
+                sj = jc * CLUSTER + jj;
                 const int mj = st.slot_mol[sj];
                 const float4 xj = st.xyzq[sj];
-                const float jx = xj.x + shx, jy = xj.y + shy, jz = xj.z + shz;
-                unsigned m8 = 0u;
+                const float jx = xj.x + sh.x * L[0], jy = xj.y + sh.y * L[1], jz = xj.z + sh.z * L[2];
 #pragma unroll
                 for (int ii = 0; ii < CLUSTER; ++ii) {
                     const float dx = jx - xi[ii], dy = jy - yi[ii], dz = jz - zi[ii];
@@ -334,51 +341,24 @@ __global__ void __launch_bounds__(PS_WARPS * 32, 1) k_pairsearch(DevState st, fl
                 if (mj < 0) m8 = 0u;   // padding slot
                 // pairs within one molecule: drop the excluded ones (only when the
                 // clusters' molecule signatures meet; then the exclusion lists decide)
-                if (share_mol && m8 != 0u) {
-#pragma unroll
+                if (m8 != 0u && (isig & st.bb_molsig[jc]) != 0ull) {
+                    const int aj = st.orig[sj];
+#pragma unroll 1
                     for (int ii = 0; ii < CLUSTER; ++ii) {
-                        if (((m8 >> ii) & 1u) && mi[ii] == mj) {
-                            const int ai = st.orig[ci * CLUSTER + ii];
-                            if (excluded(st, ai, st.orig[sj], st.excl_off[ai], st.excl_off[ai + 1]))
-                                m8 &= ~(1u << ii);
+                        if (((m8 >> ii) & 1u) && s_mi[wib][ii] == mj) {
+                            const int ai = s_ai[wib][ii];
+                            if (excluded(st, ai, aj, st.excl_off[ai], st.excl_off[ai + 1])) m8 &= ~(1u << ii);
                         }
                     }
                 }
-                mask |= (unsigned long long)m8 << (8 * jj);
+                // the diagonal cluster counts each pair once: keep ii < jj only
+                if (jc == ci) m8 &= (1u << jj) - 1u;
             }
-            // the diagonal cluster counts each pair once: keep jj > ii only
-            if (jc == ci) {
-                unsigned long long upper = 0ull;
-#pragma unroll
-                for (int jj = 0; jj < CLUSTER; ++jj)
-                    for (int ii = 0; ii < jj; ++ii) upper |= 1ull << (8 * jj + ii);
-                mask &= upper;
-            }
+            const unsigned has = __ballot_sync(0xffffffffu, m8 != 0u);
+            const int pos = count + __popc(has & ((1u << lane) - 1u));
+            if (m8 != 0u && pos < cap) st.pl_row[base_out + pos] = make_int2(sj, (int)m8 | (code << 8));
+            count += __popc(has);
         }
-        // one row per j-atom with a non-empty 8-bit mask, in lane order, then j order
-        int nrow = 0;
-#pragma unroll
-        for (int jj = 0; jj < CLUSTER; ++jj) nrow += ((mask >> (8 * jj)) & 0xffull) != 0ull;
-        int incl = nrow;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int t = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += t;
-        }
-        int pos = count + incl - nrow;
-        if (nrow) {
-            const int jc = ent & ((1 << JCLUSTER_BITS) - 1);
-            const int code = (unsigned)ent >> JCLUSTER_BITS;
-#pragma unroll
-            for (int jj = 0; jj < CLUSTER; ++jj) {
-                const int m8 = (int)((mask >> (8 * jj)) & 0xffull);
-                if (m8) {
-                    if (pos < cap) st.pl_row[base_out + pos] = make_int2(jc * CLUSTER + jj, m8 | (code << 8));
-                    ++pos;
-                }
-            }
-        }
-        count += __shfl_sync(0xffffffffu, incl, 31);
     };
 
     // flat walk over (column, batch of 32 clusters) units; after each unit's
