@@ -228,11 +228,6 @@ __device__ __forceinline__ bool excluded(const DevState& st, int ai, int aj, int
     return false;
 }
 
-__device__ __forceinline__ int wrapi(int i, int n) {
-    i %= n;
-    return i < 0 ? i + n : i;
-}
-
 // One warp per i-cluster, in two phases that alternate through the column
 // window:
 //   1. candidate search: the clusters of a column are tested 32 at a time
@@ -252,6 +247,7 @@ constexpr int PS_QCAP = 32 + 32 * 27;   // a full batch left over + one column b
 __global__ void __launch_bounds__(PS_WARPS * 32, 1) k_pairsearch(DevState st, float rlist) {
     __shared__ int q[PS_WARPS][PS_QCAP];
     __shared__ int s_mi[PS_WARPS][CLUSTER], s_ai[PS_WARPS][CLUSTER];
+    __shared__ int s_end[PS_WARPS][32], s_js[PS_WARPS][32], s_sh[PS_WARPS][32];
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     if (warp >= st.n_clusters) return;
@@ -361,27 +357,58 @@ __global__ void __launch_bounds__(PS_WARPS * 32, 1) k_pairsearch(DevState st, fl
         }
     };
 
-    // flat walk over (column, batch of 32 clusters) units; after each unit's
-    // candidates are queued, full batches of 32 are turned into masks, and
-    // after the last unit whatever remains
+    // Walk of the window's columns, flattened.  The window is taken 32 columns
+    // at a time: one pass gives each lane a column (its periodic shift and the
+    // clusters it holds for ci's half list, those >= ci) and a scan of their
+    // counts; the warp then takes the concatenated clusters 32 at a time, each lane
+    // finding its column by binary search over the scan.  Candidates are queued in
+    // column, cluster, lane and shift order; full batches of 32 are turned into
+    // rows, and after the walk whatever remains.
     int qn = 0;
-    // column counters advance incrementally (no division per unit)
-    int ix = 0, iy = 0, b = 0;
-    int cx = wrapi(cx0, sd.ncol_x), cy = wrapi(cy0, sd.ncol_y);
-    bool done = nx <= 0 || ny <= 0;
-    while (true) {
-        if (!done) {
-            const int sy_col = cy0 + iy < 0 ? -1 : (cy0 + iy >= sd.ncol_y ? 1 : 0);
-            const int sx_col = cx0 + ix < 0 ? -1 : (cx0 + ix >= sd.ncol_x ? 1 : 0);
-            const int col = sd.col_off + cx + sd.ncol_x * cy;
-            const int j0 = st.col_cl_start[col];
-            const int nj = st.col_ncl[col];
-            // clusters are numbered in column order: a column whose clusters all
-            // precede ci holds no pair of ci's half list (warp-uniform skip)
-            const bool live = j0 + nj > ci;
-            const int j = j0 + b + lane;
+    const int nwin = (nx > 0 && ny > 0) ? nx * ny : 0;
+    for (int w0 = 0; w0 < nwin; w0 += 32) {
+        const int w = w0 + lane;
+        int cnt = 0, jstart = 0, shc = 5;   // shc: (sx + 1) | (sy + 1) << 2
+        const int wy = w / nx, wx = w - wy * nx;
+        const int ux = cx0 + wx, uy = cy0 + wy;   // unwrapped column
+        // a window narrower than the grid sits within one period of it; a column
+        // further out (not met in practice) is left out rather than misaddressed
+        if (w < nwin && ux >= -sd.ncol_x && ux < 2 * sd.ncol_x && uy >= -sd.ncol_y && uy < 2 * sd.ncol_y) {
+            const int sxc = ux < 0 ? -1 : (ux >= sd.ncol_x ? 1 : 0);
+            const int syc = uy < 0 ? -1 : (uy >= sd.ncol_y ? 1 : 0);
+            const int col = sd.col_off + (ux - sxc * sd.ncol_x) + sd.ncol_x * (uy - syc * sd.ncol_y);
+            const int j0 = st.col_cl_start[col], nj = st.col_ncl[col];
+            // clusters are numbered in column order: those before ci are in
+            // their own half lists
+            jstart = max(j0, ci);
+            cnt = max(0, j0 + nj - jstart);
+            shc = (sxc + 1) | ((syc + 1) << 2);
+        }
+        int incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        s_end[wib][lane] = incl;
+        s_js[wib][lane] = jstart;
+        s_sh[wib][lane] = shc;
+        const int tot = __shfl_sync(0xffffffffu, incl, 31);
+        __syncwarp();
+        for (int t0 = 0; t0 < tot; t0 += 32) {
+            const int t = t0 + lane;
             unsigned shifts = 0u;  // bit k set: shift code k is in range
-            if (live && b + lane < nj && j >= ci) {
+            int j = 0;
+            if (t < tot) {
+                // the lane's column: the first whose running count exceeds t
+                int lo = 0, hi = 31;
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (s_end[wib][mid] > t) hi = mid;
+                    else lo = mid + 1;
+                }
+                j = s_js[wib][lo] + t - (lo ? s_end[wib][lo - 1] : 0);
+                const int sx_col = (s_sh[wib][lo] & 3) - 1, sy_col = (s_sh[wib][lo] >> 2) - 1;
                 const float4 jlo = st.bb_lo[j], jhi = st.bb_hi[j];
                 const float jc[3] = {0.5f * (jlo.x + jhi.x), 0.5f * (jlo.y + jhi.y), 0.5f * (jlo.z + jhi.z)};
                 const float je[3] = {0.5f * (jhi.x - jlo.x), 0.5f * (jhi.y - jlo.y), 0.5f * (jhi.z - jlo.z)};
@@ -422,54 +449,41 @@ __global__ void __launch_bounds__(PS_WARPS * 32, 1) k_pairsearch(DevState st, fl
                     }
                 }
             }
-            if (live) {
-                // append (cluster, shift) candidates in lane order, then shift order
-                const int c = __popc(shifts);
-                int incl = c;
+            // append (cluster, shift) candidates in lane order, then shift order
+            const int c = __popc(shifts);
+            int inc2 = c;
 #pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const int t = __shfl_up_sync(0xffffffffu, incl, o);
-                    if (lane >= o) incl += t;
-                }
-                const int total = __shfl_sync(0xffffffffu, incl, 31);
-                int w = qn + incl - c;
-                while (shifts) {
-                    const int code = __ffs(shifts) - 1;
-                    shifts &= shifts - 1u;
-                    q[wib][w++] = j | (code << JCLUSTER_BITS);
-                }
-                qn += total;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, inc2, o);
+                if (lane >= o) inc2 += v;
             }
-            b = live ? b + 32 : nj;
-            if (b >= nj) {
-                b = 0;
-                if (++cx == sd.ncol_x) cx = 0;
-                if (++ix == nx) {
-                    ix = 0;
-                    cx = wrapi(cx0, sd.ncol_x);
-                    if (++cy == sd.ncol_y) cy = 0;
-                    done = ++iy == ny;
-                }
+            const int added = __shfl_sync(0xffffffffu, inc2, 31);
+            int wq = qn + inc2 - c;
+            while (shifts) {
+                const int code = __ffs(shifts) - 1;
+                shifts &= shifts - 1u;
+                q[wib][wq++] = j | (code << JCLUSTER_BITS);
             }
-        }
-        __syncwarp();
-        int head = 0;
-        while (qn - head >= 32 || (done && qn > head)) {
-            const int nb = min(32, qn - head);
-            build_masks(head, nb);
-            head += nb;
-        }
-        if (head > 0) {
-            // move the remainder (< 32) to the front of the queue
-            const int rem = qn - head;
-            const int v = lane < rem ? q[wib][head + lane] : 0;
+            qn += added;
             __syncwarp();
-            if (lane < rem) q[wib][lane] = v;
-            qn = rem;
+            int head = 0;
+            while (qn - head >= 32) {
+                build_masks(head, 32);
+                head += 32;
+            }
+            if (head > 0) {
+                // move the remainder (< 32) to the front of the queue
+                const int rem = qn - head;
+                const int v = lane < rem ? q[wib][head + lane] : 0;
+                __syncwarp();
+                if (lane < rem) q[wib][lane] = v;
+                qn = rem;
+            }
+            __syncwarp();
         }
-        __syncwarp();
-        if (done) break;
+        __syncwarp();   // s_end etc. are rewritten by the next 32 columns
     }
+    if (qn > 0) build_masks(0, qn);
     if (lane == 0) {
         st.pl_count[ci] = min(count, cap);
         if (count > cap) atomicOr(st.status, ST_PAIRLIST_OVERFLOW);
