@@ -660,6 +660,7 @@ void lima_engine::setup() {
     nb.kappa = (float)kappa;
     nb.ke = (float)kCoulomb;
     nb.two_kappa_sqrtpi = (float)(2.0 * kappa / std::sqrt(p.ref_compat ? kPiRef : kPi));
+    nb.mk2_log2e = (float)(-kappa * kappa / std::log(2.0));
     nb.em = 0;
     ip.dt = p.dt;
     ip.integrator = p.integrator;

@@ -352,7 +352,10 @@ __global__ void __launch_bounds__(PS_WARPS * 32, 1) k_pairsearch(DevState st, fl
             }
             const unsigned has = __ballot_sync(0xffffffffu, m8 != 0u);
             const int pos = count + __popc(has & ((1u << lane) - 1u));
-            if (m8 != 0u && pos < cap) st.pl_row[base_out + pos] = make_int2(sj, (int)m8 | (code << 8));
+            if (m8 != 0u && pos < cap) {
+                const int img = code % 3 | ((code / 3) % 3) << 2 | (code / 9) << 4;
+                st.pl_row[base_out + pos] = make_int2(sj, (int)m8 | (img << ROW_SHIFT_BIT));
+            }
             count += __popc(has);
         }
     };

@@ -86,7 +86,7 @@ __device__ __forceinline__ float ex2_approx(float x) {
 template <int ES, int EN>
 __global__ void __launch_bounds__(256, EN ? 2 : 3) k_nonbonded(DevState st, NbParams p) {
     constexpr bool ENERGY = EN > 0, ATOM = EN > 1;
-    // per warp, i-atom pairs (ip, ip + 4): (x0, x1, y0, y1), (z0, z1, q0 ke, q1 ke),
+    // per warp, i-atom pairs (ip, ip + 4): (x0, x1, y0, y1), (z0, z1, -q0 ke, -q1 ke),
     // (sigma0/2, sigma1/2, 24 sqrt(eps0), 24 sqrt(eps1))
     __shared__ float4 s_xy[8][4], s_zq[8][4], s_lj[8][4];
     const int wib = threadIdx.x >> 5;
@@ -108,7 +108,7 @@ __global__ void __launch_bounds__(256, EN ? 2 : 3) k_nonbonded(DevState st, NbPa
         xy[h] = x.x;
         xy[2 + h] = x.y;
         zq[h] = x.z;
-        zq[2 + h] = x.w * p.ke;   // i-charges carry the Coulomb constant
+        zq[2 + h] = -x.w * p.ke;  // i-charges carry minus the Coulomb constant
         lv[h] = lj.x;
         lv[2 + h] = 24.f * lj.y;  // the LJ force prefactor folded into the i side
     }
@@ -131,13 +131,14 @@ __global__ void __launch_bounds__(256, EN ? 2 : 3) k_nonbonded(DevState st, NbPa
         if (k < n) {
             const int2 row = st.pl_row[base + k];
             bits = (unsigned)row.y & 0xffu;   // bit ii: pair (ii, this j-atom)
-            const int3 sh = decode_shift((unsigned)row.y >> 8);
+            const unsigned img = (unsigned)row.y >> ROW_SHIFT_BIT;
             sj = row.x;
             xj = st.xyzq[sj];
             ljj = st.ljp[sj];
-            xj.x += sh.x * Lx;
-            xj.y += sh.y * Ly;
-            xj.z += sh.z * Lz;
+            // image shift s L with s + 1 in two bits per axis
+            xj.x += fmaf((float)(img & 3u), Lx, -Lx);
+            xj.y += fmaf((float)((img >> 2) & 3u), Ly, -Ly);
+            xj.z += fmaf((float)(img >> 4), Lz, -Lz);
         }
         f2p fjx = zero2, fjy = zero2, fjz = zero2, ej = zero2;
         const f2p jx = splat2(xj.x), jy = splat2(xj.y), jz = splat2(xj.z);
@@ -167,24 +168,24 @@ __global__ void __launch_bounds__(256, EN ? 2 : 3) k_nonbonded(DevState st, NbPa
             f2p fs = mul2(mul2(eps24, s6), mul2(rinv2, fma2(s6, mtwo2, one2)));
             f2p ec = zero2;
             if (ES != 0) {
-                const f2p qq = mul2(pk2(vzq.z, vzq.w), jq);
+                // qn = -k_e q_i q_j (the sign rides on the i-charge)
+                const f2p qn = mul2(pk2(vzq.z, vzq.w), jq);
                 if (ES == 2) {
-                    const f2p r = mul2(r2, rinv);
-                    const f2p x = mul2(splat2(p.kappa), r);
+                    const f2p x = mul2(mul2(r2, rinv), splat2(p.kappa));   // kappa r
                     const float2 den = up2(fma2(splat2(AS_P), x, one2));
                     const f2p t = pk2(__fdividef(1.f, den.x), __fdividef(1.f, den.y));
+                    // erfc(kappa r) = poly e^{-kappa^2 r^2}
                     const f2p poly = mul2(t, fma2(t, fma2(t, fma2(t, fma2(t, splat2(AS_A5), splat2(AS_A4)),
                                                                 splat2(AS_A3)), splat2(AS_A2)), splat2(AS_A1)));
-                    // exp(-x^2) = 2^(-x^2 log2 e)
-                    const float2 xs = up2(mul2(mul2(x, x), splat2(-1.4426950408889634f)));
+                    const float2 xs = up2(mul2(r2, splat2(p.mk2_log2e)));
                     const f2p ex = pk2(ex2_approx(xs.x), ex2_approx(xs.y));
-                    const f2p erfc_x = mul2(poly, ex);
-                    const f2p qr3 = mul2(qq, mul2(rinv2, rinv));
-                    fs = sub2(fs, mul2(qr3, fma2(mul2(splat2(p.two_kappa_sqrtpi), r), ex, erfc_x)));
-                    if (ENERGY) ec = mul2(qq, mul2(rinv, erfc_x));
+                    // k_e q_i q_j [erfc(kappa r)/r + 2 kappa/sqrt(pi) e^{-kappa^2 r^2}] / r^2
+                    //   = -qn e^{-kappa^2 r^2} (poly/r + 2 kappa/sqrt(pi)) / r^2, away from j
+                    fs = fma2(mul2(qn, rinv2), mul2(ex, fma2(poly, rinv, splat2(p.two_kappa_sqrtpi))), fs);
+                    if (ENERGY) ec = sub2(zero2, mul2(mul2(qn, rinv), mul2(poly, ex)));
                 } else {
-                    fs = sub2(fs, mul2(qq, mul2(rinv2, rinv)));
-                    if (ENERGY) ec = mul2(qq, rinv);
+                    fs = fma2(mul2(qn, rinv2), rinv, fs);
+                    if (ENERGY) ec = sub2(zero2, mul2(qn, rinv));
                 }
             }
             float2 fsv = up2(fs);
@@ -374,7 +375,8 @@ __global__ void k_pairlist_dump(DevState st, NbParams p, long long cap, int* out
     for (int k = lane; k < n; k += 32) {
         const int2 row = st.pl_row[base + k];
         const int sj = row.x;
-        const int3 sh = decode_shift((unsigned)row.y >> 8);
+        const unsigned img = (unsigned)row.y >> ROW_SHIFT_BIT;
+        const int3 sh = make_int3((int)(img & 3u) - 1, (int)((img >> 2) & 3u) - 1, (int)(img >> 4) - 1);
         const float4 xj = st.xyzq[sj];
         for (int ii = 0; ii < CLUSTER; ++ii) {
             const float4 xi = st.xyzq[ci * CLUSTER + ii];
