@@ -307,9 +307,10 @@ LIMA_API int lima_learned_pme_predict(lima_engine* h, int rows, const float* fea
  * periods of real MD steps (they advance the simulation), three rounds, with
  * each launch shape of the force-only pair kernel — 256
  * or 128 threads per block, with or without leaving SM room to the PME and
- * bonded kernels of the step — and keeps the fastest for this engine.  All
- * shapes give identical results.  *shape (may be NULL) receives the choice:
- * bit 0 room left, bit 1 128-thread blocks. */
+ * bonded kernels of the step, one or two pair-list rows' loads in flight per
+ * lane — and keeps the fastest for this engine.  All shapes give identical
+ * results.  *shape (may be NULL) receives the choice: bit 0 room left, bit 1
+ * 128-thread blocks, bit 2 two rows in flight. */
 LIMA_API int lima_autotune(lima_engine* h, int periods, int* shape);
 
 /* ---------------------------------------------------------- thermostat, log */

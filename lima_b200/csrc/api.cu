@@ -109,7 +109,7 @@ struct lima_engine {
     // launch shape of the force-only pair kernel, picked by autotune()
     int nb_shape = 0;
     bool nb_tuned = false;
-    double tune_ms[4] = {0, 0, 0, 0};
+    double tune_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // per launch shape of the pair kernel
 
     // device scratch for readback
     unsigned* d_disp = nullptr;       // [0] largest squared move since the last list build (float bits),
@@ -1203,14 +1203,16 @@ void lima_engine::run_steps(int n) {
 // Every shape gives identical results, so the choice changes only the speed.
 int lima_engine::autotune(int periods) {
     const int n = std::max(1, periods) * p.nstlist;
-    double best[4] = {1e300, 1e300, 1e300, 1e300};
-    for (int shape = 0; shape < 4; ++shape) {   // first use of each shape, untimed
+    constexpr int NS = 8;
+    double best[NS];
+    for (int shape = 0; shape < NS; ++shape) {   // first use of each shape, untimed
+        best[shape] = 1e300;
         nb_shape = shape;
         drop_graph();
         run_steps(p.nstlist);
     }
     for (int round = 0; round < 3; ++round)
-        for (int shape = 0; shape < 4; ++shape) {
+        for (int shape = 0; shape < NS; ++shape) {
             nb_shape = shape;
             drop_graph();
             const double t0 = time_ms;
@@ -1218,9 +1220,9 @@ int lima_engine::autotune(int periods) {
             best[shape] = std::min(best[shape], time_ms - t0);
         }
     int pick = 0;
-    for (int shape = 1; shape < 4; ++shape)
+    for (int shape = 1; shape < NS; ++shape)
         if (best[shape] < best[pick]) pick = shape;
-    for (int shape = 0; shape < 4; ++shape) tune_ms[shape] = best[shape] / n;
+    for (int shape = 0; shape < NS; ++shape) tune_ms[shape] = best[shape] / n;
     nb_shape = pick;
     nb_tuned = true;
     drop_graph();

@@ -82,9 +82,12 @@ __device__ __forceinline__ float ex2_approx(float x) {
 // per lane and are reduced across the warp once, after the list.
 // Pair arithmetic per lane and the order of every sum are fixed, so results
 // are bit-reproducible.
-// EN: 0 forces only, 1 forces and energy totals, 2 also per-atom energy shares
-template <int ES, int EN>
-__global__ void __launch_bounds__(256, EN ? 2 : 3) k_nonbonded(DevState st, NbParams p) {
+// EN: 0 forces only, 1 forces and energy totals, 2 also per-atom energy shares.
+// PF: each lane loads two rows (k and k + 32) before working on either, so that
+// the second row's loads overlap the first row's arithmetic; the rows are
+// worked in the same order, so the results are the same bits either way.
+template <int ES, int EN, bool PF>
+__global__ void __launch_bounds__(256, (EN || PF) ? 2 : 3) k_nonbonded(DevState st, NbParams p) {
     constexpr bool ENERGY = EN > 0, ATOM = EN > 1;
     // per warp, i-atom pairs (ip, ip + 4): (x0, x1, y0, y1), (z0, z1, -q0 ke, -q1 ke),
     // (sigma0/2, sigma1/2, 24 sqrt(eps0), 24 sqrt(eps1))
@@ -122,12 +125,12 @@ __global__ void __launch_bounds__(256, EN ? 2 : 3) k_nonbonded(DevState st, NbPa
     // (a few tens of pairs each), converted to FP64 once per cluster
     f2p s_elj = zero2, s_ec = zero2, s_vir = zero2;
     const size_t base = (size_t)ci * st.pl_cap;
-    for (int k0 = 0; k0 < n; k0 += 32) {
-        const int k = k0 + lane;
-        unsigned bits = 0u;
-        int sj = 0;
-        float4 xj = make_float4(0.f, 0.f, 0.f, 0.f);
-        float2 ljj = make_float2(0.f, 0.f);
+    // one row: its mask, j slot, j position with the row's image applied, j LJ
+    auto load_row = [&](int k, unsigned& bits, int& sj, float4& xj, float2& ljj) {
+        bits = 0u;
+        sj = 0;
+        xj = make_float4(0.f, 0.f, 0.f, 0.f);
+        ljj = make_float2(0.f, 0.f);
         if (k < n) {
             const int2 row = st.pl_row[base + k];
             bits = (unsigned)row.y & 0xffu;   // bit ii: pair (ii, this j-atom)
@@ -140,6 +143,8 @@ __global__ void __launch_bounds__(256, EN ? 2 : 3) k_nonbonded(DevState st, NbPa
             xj.y += fmaf((float)((img >> 2) & 3u), Ly, -Ly);
             xj.z += fmaf((float)(img >> 4), Lz, -Lz);
         }
+    };
+    auto do_row = [&](unsigned bits, int sj, float4 xj, float2 ljj) {
         f2p fjx = zero2, fjy = zero2, fjz = zero2, ej = zero2;
         const f2p jx = splat2(xj.x), jy = splat2(xj.y), jz = splat2(xj.z);
         const f2p jsig = splat2(ljj.x), jeps = splat2(ljj.y), jq = splat2(xj.w);
@@ -227,6 +232,27 @@ __global__ void __launch_bounds__(256, EN ? 2 : 3) k_nonbonded(DevState st, NbPa
                 add_atom_energy(st.epot, sj, (double)(e.x + e.y));
             }
         }
+    };
+    if (PF) {
+        for (int k0 = 0; k0 < n; k0 += 64) {
+            unsigned ba, bb;
+            int sa, sb;
+            float4 xa, xb;
+            float2 la, lb;
+            load_row(k0 + lane, ba, sa, xa, la);
+            load_row(k0 + 32 + lane, bb, sb, xb, lb);
+            do_row(ba, sa, xa, la);
+            do_row(bb, sb, xb, lb);
+        }
+    } else {
+        for (int k0 = 0; k0 < n; k0 += 32) {
+            unsigned ba;
+            int sa;
+            float4 xa;
+            float2 la;
+            load_row(k0 + lane, ba, sa, xa, la);
+            do_row(ba, sa, xa, la);
+        }
     }
     // i-forces: sum each of the 24 values over the warp; lane a (< 8) adds atom a's
     float fi[CLUSTER][3], eiv[CLUSTER];
@@ -277,7 +303,8 @@ __global__ void __launch_bounds__(256, EN ? 2 : 3) k_nonbonded(DevState st, NbPa
 //          warps of an SM, leaving registers and block slots to the PME and
 //          bonded kernels of the same step on their higher-priority streams
 //          (helps when the PME chain is long next to the pair kernel);
-//   bit 1: 128-thread blocks instead of 256.
+//   bit 1: 128-thread blocks instead of 256;
+//   bit 2: two rows' loads in flight per lane (PF).
 // The engine's autotuner times the shapes on the running system.
 template <int ES>
 static void launch_nb_shape(const DevState& st, const NbParams& p, bool energy, int shape, cudaStream_t s) {
@@ -285,18 +312,20 @@ static void launch_nb_shape(const DevState& st, const NbParams& p, bool energy, 
     const int tb = (shape & 2) ? 128 : 256;
     const dim3 grid((unsigned)((threads + tb - 1) / tb));
     if (energy) {
-        if (st.atom_energy) k_nonbonded<ES, 2><<<grid, tb, 0, s>>>(st, p);
-        else k_nonbonded<ES, 1><<<grid, tb, 0, s>>>(st, p);
+        if (st.atom_energy) k_nonbonded<ES, 2, false><<<grid, tb, 0, s>>>(st, p);
+        else k_nonbonded<ES, 1, false><<<grid, tb, 0, s>>>(st, p);
         return;
     }
     // 16 warps per SM: 2 blocks of 256 threads (90 KB each) or 4 of 128 (50 KB each)
     const int reserve = (shape & 1) ? ((shape & 2) ? 50 * 1024 : 90 * 1024) : 0;
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_nonbonded<ES, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 90 * 1024);
+        cudaFuncSetAttribute(k_nonbonded<ES, 0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 90 * 1024);
+        cudaFuncSetAttribute(k_nonbonded<ES, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 90 * 1024);
         attr = true;
     }
-    k_nonbonded<ES, 0><<<grid, tb, reserve, s>>>(st, p);
+    if (shape & 4) k_nonbonded<ES, 0, true><<<grid, tb, reserve, s>>>(st, p);
+    else k_nonbonded<ES, 0, false><<<grid, tb, reserve, s>>>(st, p);
 }
 
 int launch_nonbonded(const DevState& st, const NbParams& p, bool energy, cudaStream_t s, int shape) {

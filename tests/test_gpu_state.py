@@ -69,9 +69,9 @@ def test_autotune_shapes_give_identical_trajectories():
     shape must give the same bits, so a tuned run equals an untuned one."""
     s = systems.water_box(1500, 3.6, seed=6, name="w")
     a, b = make(s), make(s)
-    shape = a.autotune(1)                      # 16 periods of 10 steps, energies at each period's end
-    assert 0 <= shape <= 3 and a.timings()["pair_shape"] == shape
-    for _ in range(16):
+    shape = a.autotune(1)                      # 8 + 3 x 8 periods of 10 steps, energies at each period's end
+    assert 0 <= shape <= 7 and a.timings()["pair_shape"] == shape
+    for _ in range(32):
         b.step(10)
     a.step(10)
     b.step(10)
