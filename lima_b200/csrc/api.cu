@@ -829,6 +829,8 @@ PmePlan lima_engine::make_pme(std::vector<SysDesc>& sd, DevState& D) {
         P.spread_box = box;
     }
     pme_set_smem_limits(max_n, P.n_items_xy > 0 ? xy_buf : 0);
+    P.n_sys = ns;
+    if (ns > 0) P.sys0 = sd[0];
     return P;
 }
 

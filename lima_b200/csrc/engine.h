@@ -153,6 +153,8 @@ struct PmePlan {
     int4* items_spread = nullptr;   // (system, first column x, first column y, first z node)
     int4* spread_geo = nullptr;     // per system: box nodes in x, y, z (0 = no grid)
     int spread_box = 0;             // int32 elements of the largest box
+    int n_sys = 0;                  // systems of the plan; with one, its descriptor
+    SysDesc sys0{};                 //   travels as a kernel argument
 };
 constexpr int PME_SPREAD_COLS = 1;      // columns per block side
 // int32 nodes of a box (40 KB of shared memory): small enough for a 256-thread

@@ -643,9 +643,11 @@ int pme_xy_buffer(int k0, int k1) {
 }
 
 // ------------------------------------------------------------------ gather
-// four threads per atom, one z-plane each; partial sums combined with shuffles
-template <bool ENERGY, bool FD>
-__global__ void k_gather(DevState st) {
+// four threads per atom, one z-plane each; partial sums combined with shuffles.
+// ONE: a single system, whose descriptor sd1 comes as a kernel argument instead
+// of a dependent load through the cluster's system index.
+template <bool ENERGY, bool FD, bool ONE>
+__global__ void k_gather(DevState st, const SysDesc sd1) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int s = t >> 2, c = t & 3;
     double e = 0.0;
@@ -655,8 +657,8 @@ __global__ void k_gather(DevState st) {
     float sc0 = 0.f, sc1 = 0.f, sc2 = 0.f;
     if (s < st.n_slots) {
         const float4 p = st.xyzq[s];
-        const int sy = st.cluster_sys[s / CLUSTER];
-        const SysDesc& sd = st.sys[sy];
+        const int sy = ONE ? 0 : st.cluster_sys[s / CLUSTER];
+        const SysDesc& sd = ONE ? sd1 : st.sys[sy];
         if (p.w != 0.f && st.orig[s] >= 0 && sd.pme_n[0] != 0) {
             sysi = sy;
             q = p.w;
@@ -728,7 +730,7 @@ __global__ void k_gather(DevState st) {
             e = 0.5 * (double)q * (double)phi;
             // the atom's reciprocal energy and its share of the Ewald self term
             if (st.atom_energy) {
-                const SysDesc& sd = st.sys[sysi];
+                const SysDesc& sd = ONE ? sd1 : st.sys[sysi];
                 const double self = sd.self_per_charge ? (double)sd.self_coef : (double)sd.self_coef * q * q;
                 add_atom_energy(st.epot, s, e + self);
             }
@@ -769,12 +771,21 @@ int launch_pme(const DevState& st, const PmePlan& plan, bool energy, cudaStream_
         k_fft_y<<<plan.n_items_y, FFT_YZ_THREADS, sy, s>>>(st, plans, plan.items_y, 1.f, mx);
         k_fft_x_inv<<<plan.n_items_x, 256, sx, s>>>(st, plans, plan.items_x, mx);
     }
-    if (plan.ref_gather) {
-        if (energy) k_gather<true, true><<<g4, TB, 0, s>>>(st);
-        else k_gather<false, true><<<g4, TB, 0, s>>>(st);
+    const SysDesc& sd1 = plan.sys0;
+    if (plan.n_sys == 1) {
+        if (plan.ref_gather) {
+            if (energy) k_gather<true, true, true><<<g4, TB, 0, s>>>(st, sd1);
+            else k_gather<false, true, true><<<g4, TB, 0, s>>>(st, sd1);
+        } else {
+            if (energy) k_gather<true, false, true><<<g4, TB, 0, s>>>(st, sd1);
+            else k_gather<false, false, true><<<g4, TB, 0, s>>>(st, sd1);
+        }
+    } else if (plan.ref_gather) {
+        if (energy) k_gather<true, true, false><<<g4, TB, 0, s>>>(st, sd1);
+        else k_gather<false, true, false><<<g4, TB, 0, s>>>(st, sd1);
     } else {
-        if (energy) k_gather<true, false><<<g4, TB, 0, s>>>(st);
-        else k_gather<false, false><<<g4, TB, 0, s>>>(st);
+        if (energy) k_gather<true, false, false><<<g4, TB, 0, s>>>(st, sd1);
+        else k_gather<false, false, false><<<g4, TB, 0, s>>>(st, sd1);
     }
     return n;
 }
