@@ -86,6 +86,24 @@ __device__ __forceinline__ void small_dft(float2* v, float sigma) {
         v[4] = csub(m1, n1);
         v[2] = cadd(m2, n2);
         v[3] = csub(m2, n2);
+    } else if (R == 8) {
+        // two 4-point transforms (even and odd samples) joined by the eighth roots
+        // of unity w^k = e^{sigma 2 pi i k / 8}: 1, (1 + sigma i)/sqrt 2, sigma i, (-1 + sigma i)/sqrt 2
+        float2 e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};
+        small_dft<4>(e, sigma);
+        small_dft<4>(o, sigma);
+        const float r = 0.70710678118654752f;
+        const float2 o1 = make_float2(r * (o[1].x - sigma * o[1].y), r * (o[1].y + sigma * o[1].x));
+        const float2 o2 = mul_si(o[2], sigma);
+        const float2 o3 = make_float2(r * (-o[3].x - sigma * o[3].y), r * (-o[3].y + sigma * o[3].x));
+        v[0] = cadd(e[0], o[0]);
+        v[4] = csub(e[0], o[0]);
+        v[1] = cadd(e[1], o1);
+        v[5] = csub(e[1], o1);
+        v[2] = cadd(e[2], o2);
+        v[6] = csub(e[2], o2);
+        v[3] = cadd(e[3], o3);
+        v[7] = csub(e[3], o3);
     }
 }
 
@@ -138,6 +156,7 @@ __device__ float2* fft_lines(float2* a, float2* b, int nlines, int stride, const
             case 2: stockham_stage<2>(src, dst, nlines, stride, pl.n, Ns, tw, sigma); break;
             case 3: stockham_stage<3>(src, dst, nlines, stride, pl.n, Ns, tw, sigma); break;
             case 4: stockham_stage<4>(src, dst, nlines, stride, pl.n, Ns, tw, sigma); break;
+            case 8: stockham_stage<8>(src, dst, nlines, stride, pl.n, Ns, tw, sigma); break;
             default: stockham_stage<5>(src, dst, nlines, stride, pl.n, Ns, tw, sigma); break;
         }
         __syncthreads();
@@ -790,13 +809,18 @@ int launch_pme(const DevState& st, const PmePlan& plan, bool energy, cudaStream_
     return n;
 }
 
-// Host helper: radix plan for an FFT length (4s first, then 2, 3, 5).
+// Host helper: radix plan for an FFT length (8s first, then 4s, 2, 3, 5: fewer
+// stages mean fewer shared-memory passes and barriers).
 bool make_fft_plan(int n, FftPlanDev* out) {
     if (n < 2 || n > FFT_MAXN) return false;
     out->n = n;
     out->nrad = 0;
     out->tw_off = -1;
     int m = n;
+    while (m % 8 == 0) {
+        out->rad[out->nrad++] = 8;
+        m /= 8;
+    }
     while (m % 4 == 0) {
         out->rad[out->nrad++] = 4;
         m /= 4;
