@@ -19,37 +19,60 @@
 
 namespace lima {
 
+// Adds one to counter[key] for every lane with key >= 0, one atomic per group of
+// lanes sharing a key; returns the lane's place within its group's block.
+__device__ __forceinline__ int warp_add_counts(int* counter, int key) {
+    const int lane = threadIdx.x & 31;
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    const int leader = __ffs(peers) - 1;
+    int base = 0;
+    if (lane == leader && key >= 0) base = atomicAdd(counter + key, __popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    return base + __popc(peers & ((1u << lane) - 1u));
+}
+
+// One thread per atom (a build from new input) or per slot (a rebuild from the
+// engine's own slots: the atoms of a warp then mostly share a column, and the
+// column counts take one atomic per column and warp).
 __global__ void k_bin(DevState st, int from_input) {
-    const int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= st.n_atoms) return;
-    const SysDesc& sd = st.sys[st.atom_sys[a]];
-    double p[3];
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    int a = -1, s = -1;
     if (from_input) {
-        p[0] = st.in_pos[3 * a];
-        p[1] = st.in_pos[3 * a + 1];
-        p[2] = st.in_pos[3 * a + 2];
-    } else {
-        const int s = st.slot_of[a];
-        p[0] = st.px[s];
-        p[1] = st.py[s];
-        p[2] = st.pz[s];
+        if (t < st.n_atoms) a = t;
+    } else if (t < st.n_slots) {
+        s = t;
+        a = st.orig[t];
     }
-    for (int d = 0; d < 3; ++d) {
-        const double L = sd.box[d];
-        double x = p[d] - L * floor(p[d] / L);
-        if (x >= L) x -= L;
-        if (x < 0.0) x = 0.0;
-        p[d] = x;
-        st.in_pos[3 * a + d] = x;
+    int col = -1;
+    if (a >= 0) {
+        const SysDesc& sd = st.sys[st.atom_sys[a]];
+        double p[3];
+        if (from_input) {
+            p[0] = st.in_pos[3 * a];
+            p[1] = st.in_pos[3 * a + 1];
+            p[2] = st.in_pos[3 * a + 2];
+        } else {
+            p[0] = st.px[s];
+            p[1] = st.py[s];
+            p[2] = st.pz[s];
+        }
+        for (int d = 0; d < 3; ++d) {
+            const double L = sd.box[d];
+            double x = p[d] - L * floor(p[d] / L);
+            if (x >= L) x -= L;
+            if (x < 0.0) x = 0.0;
+            p[d] = x;
+            st.in_pos[3 * a + d] = x;
+        }
+        int cx = (int)(p[0] * sd.ncol_x / sd.box[0]);
+        int cy = (int)(p[1] * sd.ncol_y / sd.box[1]);
+        cx = min(max(cx, 0), sd.ncol_x - 1);
+        cy = min(max(cy, 0), sd.ncol_y - 1);
+        col = sd.col_off + cx + sd.ncol_x * cy;
+        st.col_of_atom[a] = col;
+        st.z_of_atom[a] = (float)p[2];
     }
-    int cx = (int)(p[0] * sd.ncol_x / sd.box[0]);
-    int cy = (int)(p[1] * sd.ncol_y / sd.box[1]);
-    cx = min(max(cx, 0), sd.ncol_x - 1);
-    cy = min(max(cy, 0), sd.ncol_y - 1);
-    const int col = sd.col_off + cx + sd.ncol_x * cy;
-    st.col_of_atom[a] = col;
-    st.z_of_atom[a] = (float)p[2];
-    atomicAdd(&st.col_count[col], 1);
+    warp_add_counts(st.col_count, col);
 }
 
 // one CTA per system; Hillis-Steele block scan over chunks of columns
@@ -98,13 +121,22 @@ __global__ void k_scan_columns(DevState st) {
     }
 }
 
-__global__ void k_scatter(DevState st) {
-    const int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= st.n_atoms) return;
-    const int col = st.col_of_atom[a];
-    const int k = atomicAdd(&st.col_fill[col], 1);
-    const int off = st.sys[st.atom_sys[a]].atom_off;
-    st.col_list[off + st.col_atom_start[col] + k] = a;
+// atoms -> column lists, in the same thread order as k_bin (the order within a
+// column is fixed afterwards by the sort)
+__global__ void k_scatter(DevState st, int from_input) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    int a = -1;
+    if (from_input) {
+        if (t < st.n_atoms) a = t;
+    } else if (t < st.n_slots) {
+        a = st.orig[t];
+    }
+    const int col = a >= 0 ? st.col_of_atom[a] : -1;
+    const int k = warp_add_counts(st.col_fill, col);
+    if (a >= 0) {
+        const int off = st.sys[st.atom_sys[a]].atom_off;
+        st.col_list[off + st.col_atom_start[col] + k] = a;
+    }
 }
 
 // one CTA per column: rank each atom by the unique key (z bits, atom index)
@@ -498,9 +530,10 @@ __global__ void __launch_bounds__(PS_WARPS * 32, 1) k_pairsearch(DevState st, fl
 // done, concurrently with the pair search.
 int launch_rebuild_slots(const DevState& st, bool from_input, cudaStream_t s) {
     const int TB = 256;
-    k_bin<<<(st.n_atoms + TB - 1) / TB, TB, 0, s>>>(st, from_input ? 1 : 0);
+    const int nt = from_input ? st.n_atoms : st.n_slots;   // threads of the bin and scatter passes
+    k_bin<<<(nt + TB - 1) / TB, TB, 0, s>>>(st, from_input ? 1 : 0);
     k_scan_columns<<<st.n_sys, 1024, 0, s>>>(st);
-    k_scatter<<<(st.n_atoms + TB - 1) / TB, TB, 0, s>>>(st);
+    k_scatter<<<(nt + TB - 1) / TB, TB, 0, s>>>(st, from_input ? 1 : 0);
     k_sort_columns<<<st.n_cols, 128, (size_t)st.col_cap * sizeof(unsigned long long), s>>>(st, st.col_sys);
     k_gather_slots<<<(st.n_slots + TB - 1) / TB, TB, 0, s>>>(st, from_input ? 1 : 0);
     k_finish_slots<<<(st.n_slots + TB - 1) / TB, TB, 0, s>>>(st);
