@@ -1510,13 +1510,17 @@ int lima_set_state(lima_engine* h, const double* pos, const float* vel) {
             unsigned word[2] = {0u, 0u};
             CK(cudaMemcpyAsync(word, h->d_disp, sizeof(word), cudaMemcpyDeviceToHost, s));
             CK(cudaStreamSynchronize(s));
-            if (word[1]) return fail(h, LIMA_ERR_NOT_FINITE, "non-finite position");
+            if (word[1] & 1u) return fail(h, LIMA_ERR_NOT_FINITE, "non-finite position");
             h->launches += launch_load_state(h->st, h->n_atoms_off[h->cur], S.n, s);
             const unsigned bits = word[0];
             float d2;
             std::memcpy(&d2, &bits, sizeof(float));
+            // a moved state must keep every atom within half the Verlet buffer of its
+            // build position; one handed back unchanged is the engine's own state and
+            // keeps the usual nstlist cadence, as stepping without the hand-in would
             const double half_skin = 0.5 * (h->rlist - h->p.cutoff);
-            if (!((double)d2 < half_skin * half_skin)) h->list_age = h->p.nstlist;   // rebuild before the next forces
+            if ((word[1] & 2u) && !((double)d2 < half_skin * half_skin))
+                h->list_age = h->p.nstlist;   // rebuild before the next forces
             h->energy_valid = false;
             ++h->state_fast_loads;
             return LIMA_OK;

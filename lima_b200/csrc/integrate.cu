@@ -217,17 +217,20 @@ int launch_log_frame(const DevState& st, float4* pos_epot, float4* force_speed, 
 // State handed in by the caller for atoms that keep their slots, in two steps.
 // k_check_state reads the staged input only: word[0] receives the largest
 // squared move since the last pair-list build (float bits; it decides on the
-// host whether the list still holds) and word[1] is set when a position is not
-// finite, so that the host can refuse the call with the engine untouched.
+// host whether the list still holds), word[1] bit 0 is set when a position is
+// not finite, so that the host can refuse the call with the engine untouched,
+// and bit 1 when any position differs from the engine's own (a state handed
+// back unchanged keeps the list on its usual rebuild cadence).
 __global__ void k_check_state(DevState st, int a0, int n, unsigned* word) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     float d2 = 0.f;
-    bool bad = false;
+    bool bad = false, moved = false;
     if (i < n) {
         const int a = a0 + i;
         const int s = st.slot_of[a];
         const double x = st.in_pos[3 * a], y = st.in_pos[3 * a + 1], z = st.in_pos[3 * a + 2];
         bad = !(isfinite(x) && isfinite(y) && isfinite(z));
+        moved = x != st.px[s] || y != st.py[s] || z != st.pz[s];
         const float4 r = st.xyz_ref[s];
         const float dx = (float)x - r.x, dy = (float)y - r.y, dz = (float)z - r.z;
         d2 = dx * dx + dy * dy + dz * dz;
@@ -235,10 +238,10 @@ __global__ void k_check_state(DevState st, int a0, int n, unsigned* word) {
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) d2 = fmaxf(d2, __shfl_xor_sync(0xffffffffu, d2, o));
-    const bool any_bad = __any_sync(0xffffffffu, bad);
+    const bool any_bad = __any_sync(0xffffffffu, bad), any_moved = __any_sync(0xffffffffu, moved);
     if ((threadIdx.x & 31) == 0) {
         atomicMax(word, __float_as_uint(d2));
-        if (any_bad) atomicOr(word + 1, 1u);
+        if (any_bad || any_moved) atomicOr(word + 1, (any_bad ? 1u : 0u) | (any_moved ? 2u : 0u));
     }
 }
 

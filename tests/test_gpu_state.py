@@ -37,6 +37,27 @@ def test_state_round_trip_keeps_trajectory_bitwise():
     assert a.energies()["potential"] == b.energies()["potential"]
 
 
+def test_unchanged_hand_back_every_step_keeps_cadence():
+    """Handing the engine's own state back before every step (the end-to-end
+    pattern) keeps the pair list on its nstlist cadence: the same rebuilds and the
+    same trajectory bits as stepping alone."""
+    s = systems.water_box(1500, 3.6, seed=8, name="w")
+    a, b = make(s), make(s)
+    a.step(1)
+    b.step(1)
+    a.reset_timings()
+    b.reset_timings()
+    a.step(30)
+    for _ in range(30):
+        p, v = b.state()
+        b.set_state(p, v)
+        b.step(1)
+    assert b.timings()["rebuilds"] == a.timings()["rebuilds"] == 3
+    pa, va = a.state()
+    pb, vb = b.state()
+    assert np.array_equal(pa, pb) and np.array_equal(va, vb)
+
+
 def test_large_moves_and_rewrapped_positions_rebuild(oracle):
     s = systems.water_box(1500, 3.6, seed=4, name="w")
     e = make(s)
