@@ -299,10 +299,10 @@ __global__ void __launch_bounds__(256, (EN || PF) ? 2 : 3) k_nonbonded(DevState 
 
 // Launch shapes of the force-only pair kernel (results are identical for every
 // shape: the work of a warp does not depend on the block it sits in):
-//   bit 0: reserve unused shared memory so that the kernel holds at most 16
-//          warps of an SM, leaving registers and block slots to the PME and
-//          bonded kernels of the same step on their higher-priority streams
-//          (helps when the PME chain is long next to the pair kernel);
+//   bit 0: reserve unused shared memory so that the kernel holds at most 24-28
+//          warps of an SM, leaving registers, shared memory and block slots to
+//          the PME and bonded kernels of the same step on their higher-priority
+//          streams (helps when the PME chain is long next to the pair kernel);
 //   bit 1: 128-thread blocks instead of 256;
 //   bit 2: two rows' loads in flight per lane (PF).
 // The engine's autotuner times the shapes on the running system.
@@ -316,8 +316,9 @@ static void launch_nb_shape(const DevState& st, const NbParams& p, bool energy, 
         else k_nonbonded<ES, 1, false><<<grid, tb, 0, s>>>(st, p);
         return;
     }
-    // 16 warps per SM: 2 blocks of 256 threads (90 KB each) or 4 of 128 (50 KB each)
-    const int reserve = (shape & 1) ? ((shape & 2) ? 50 * 1024 : 90 * 1024) : 0;
+    // 24 to 28 warps per SM: 3 blocks of 256 threads (60 KB each) or 7 of 128 (28 KB
+    // each), leaving room for a charge-spreading CTA beside them
+    const int reserve = (shape & 1) ? ((shape & 2) ? 28 * 1024 : 60 * 1024) : 0;
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(k_nonbonded<ES, 0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 90 * 1024);
