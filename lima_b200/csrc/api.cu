@@ -577,9 +577,10 @@ void lima_engine::setup() {
     D.fprev = dalloc<float4>(S);
     D.adam_m = dalloc<float4>(S);
     D.adam_v = dalloc<float4>(S);
-    D.fx = dalloc<long long>(S);
-    D.fy = dalloc<long long>(S);
-    D.fz = dalloc<long long>(S);
+    // the three force accumulators in one block, cleared by one memset per step
+    D.fx = dalloc<long long>(3 * S);
+    D.fy = D.fx + S;
+    D.fz = D.fx + 2 * S;
     D.orig = dalloc<int>(S);
     D.slot_mol = dalloc<int>(S);
     D.tvel = dalloc<float4>(S);

@@ -300,12 +300,10 @@ int launch_gather_forces(const DevState& st, double* f_out, cudaStream_t s) {
     return 1;
 }
 
+// fx, fy and fz are one block (fy = fx + n_slots, fz = fy + n_slots)
 int launch_zero_forces(const DevState& st, cudaStream_t s) {
-    const size_t bytes = (size_t)st.n_slots * sizeof(long long);
-    cudaMemsetAsync(st.fx, 0, bytes, s);
-    cudaMemsetAsync(st.fy, 0, bytes, s);
-    cudaMemsetAsync(st.fz, 0, bytes, s);
-    return 0;  // memsets, not kernels of this library
+    cudaMemsetAsync(st.fx, 0, 3 * (size_t)st.n_slots * sizeof(long long), s);
+    return 0;  // a memset, not a kernel of this library
 }
 
 }  // namespace lima
