@@ -283,7 +283,7 @@ int pme_spread_box_side(double col_w, double inv_h) {
 }
 
 __global__ void __launch_bounds__(256) k_spread_tiles(DevState st, const int4* items, const int4* geo) {
-    extern __shared__ int sbox[];
+    extern __shared__ __align__(16) int sbox[];
     const int4 it = items[blockIdx.x];
     const SysDesc& sd = st.sys[it.x];
     const int4 gm = geo[it.x];
@@ -291,7 +291,9 @@ __global__ void __launch_bounds__(256) k_spread_tiles(DevState st, const int4* i
     const int K0 = sd.pme_n[0], K1 = sd.pme_n[1], K2 = sd.pme_n[2];
     const int z0 = it.w, nz = min(ZC, K2 - z0);
     const int nbox = NX * NY * ZC;
-    for (int i = threadIdx.x; i < nbox; i += blockDim.x) sbox[i] = 0;
+    // clear the box, 16 bytes per store (dynamic shared memory starts 16-byte aligned)
+    for (int i = threadIdx.x; i < nbox / 4; i += blockDim.x) reinterpret_cast<int4*>(sbox)[i] = make_int4(0, 0, 0, 0);
+    for (int i = (nbox & ~3) + threadIdx.x; i < nbox; i += blockDim.x) sbox[i] = 0;
     // box origin: the stencil start of an atom on the block's lower edge
     const int ox = (int)floorf((float)it.y * sd.col_w[0] * sd.pme_inv_h[0]) - 1;
     const int oy = (int)floorf((float)it.z * sd.col_w[1] * sd.pme_inv_h[1]) - 1;
@@ -351,6 +353,28 @@ __global__ void __launch_bounds__(256) k_spread_tiles(DevState st, const int4* i
     // consecutive threads add to consecutive x nodes of the grid
     const int nxy = NX * NY, ngz = (nz + 7) >> 3;
     const size_t zs = (size_t)K0 * K1;
+    if (nxy <= (int)blockDim.x) {
+        // each thread keeps one column and strides over its z groups (no division per group)
+        const int tpc = blockDim.x / nxy;
+        const int c = threadIdx.x % nxy, g0 = threadIdx.x / nxy;
+        if (g0 < tpc) {
+            const int ix = c % NX, iy = c / NX;
+            const int x = NX <= K0 ? wrap1(ox + ix, K0) : wrapk(ox + ix, K0);
+            const int y = NY <= K1 ? wrap1(oy + iy, K1) : wrapk(oy + iy, K1);
+            int* gcol = g + x + (size_t)K0 * y + zs * z0;
+            for (int gz = g0; gz < ngz; gz += tpc) {
+                const int iz0 = gz << 3, m = min(8, nz - iz0);
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    if (u < m) {
+                        const int v = sbox[c + nxy * (iz0 + u)];
+                        if (v != 0) atomicAdd(gcol + zs * (iz0 + u), v);
+                    }
+                }
+            }
+        }
+        return;
+    }
     for (int i = threadIdx.x; i < nxy * ngz; i += blockDim.x) {
         const int c = i % nxy, iz0 = (i / nxy) << 3;
         const int ix = c % NX, iy = c / NX;
