@@ -686,18 +686,18 @@ int pme_xy_buffer(int k0, int k1) {
 }
 
 // ------------------------------------------------------------------ gather
-// four threads per atom, one z-plane each; partial sums combined with shuffles.
+// Two threads per atom (adjacent lanes), each taking two z-planes of the stencil:
+// the lane of planes 0 and 1 sums p0 + p1, its partner p2 + p3, and one shuffle
+// gives (p0 + p1) + (p2 + p3).
 // ONE: a single system, whose descriptor sd1 comes as a kernel argument instead
 // of a dependent load through the cluster's system index.
 template <bool ENERGY, bool FD, bool ONE>
 __global__ void k_gather(DevState st, const SysDesc sd1) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int s = t >> 2, c = t & 3;
+    const int s = t >> 1, half = t & 1;
     double e = 0.0;
     int sysi = -1;
-    float phi = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
-    float q = 0.f;
-    float sc0 = 0.f, sc1 = 0.f, sc2 = 0.f;
+    float q = 0.f, phi = 0.f, gx = 0.f, gy = 0.f, gz = 0.f, sc0 = 0.f, sc1 = 0.f, sc2 = 0.f;
     if (s < st.n_slots) {
         const float4 p = st.xyzq[s];
         const int sy = ONE ? 0 : st.cluster_sys[s / CLUSTER];
@@ -719,53 +719,68 @@ __global__ void k_gather(DevState st, const SysDesc sd1) {
             bspline4_d(f1, dy);
             bspline4_d(f2, dz);
             const float* g = st.pme_real + sd.pme_off;
-            int ix[4], ixp[4], ixm[4];
+            int ix[4], ixp[4], ixm[4], iy[4];
 #pragma unroll
             for (int a = 0; a < 4; ++a) {
                 ix[a] = wrap1(b0 - 1 + a, K0);
                 ixp[a] = wrap1(b0 + a, K0);
                 ixm[a] = wrap1(b0 - 2 + a, K0);
+                iy[a] = wrap1(b1 - 1 + a, K1);
             }
-            const int z = wrap1(b2 - 1 + c, K2);
-            const float wzc = wz[c], dzc = dz[c];
+            // this lane's two planes (selected, so that the weights stay in registers)
+            const float wzh[2] = {half ? wz[2] : wz[0], half ? wz[3] : wz[1]};
+            const float dzh[2] = {half ? dz[2] : dz[0], half ? dz[3] : dz[1]};
+            float ph[2], pgx[2], pgy[2], pgz[2];
 #pragma unroll
-            for (int b = 0; b < 4; ++b) {
-                const int y = wrap1(b1 - 1 + b, K1);
-                const float* row = g + (size_t)K0 * (y + (size_t)K1 * z);
+            for (int cc = 0; cc < 2; ++cc) {
+                const int c = 2 * half + cc;
+                float phi = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
+                const int z = wrap1(b2 - 1 + c, K2);
+                const float wzc = wzh[cc], dzc = dzh[cc];
 #pragma unroll
-                for (int a = 0; a < 4; ++a) {
-                    const float v = row[ix[a]];
-                    const float w = wx[a] * wy[b] * wzc;
-                    phi += w * v;
-                    if (FD) {
-                        const int yp = wrap1(y + 1, K1), ym = wrap1(y - 1, K1);
-                        const int zp = wrap1(z + 1, K2), zm = wrap1(z - 1, K2);
-                        gx += w * (row[ixp[a]] - row[ixm[a]]);
-                        gy += w * (g[(size_t)K0 * (yp + (size_t)K1 * z) + ix[a]] -
-                                   g[(size_t)K0 * (ym + (size_t)K1 * z) + ix[a]]);
-                        gz += w * (g[(size_t)K0 * (y + (size_t)K1 * zp) + ix[a]] -
-                                   g[(size_t)K0 * (y + (size_t)K1 * zm) + ix[a]]);
-                    } else {
-                        gx += dx[a] * wy[b] * wzc * v;
-                        gy += wx[a] * dy[b] * wzc * v;
-                        gz += wx[a] * wy[b] * dzc * v;
+                for (int b = 0; b < 4; ++b) {
+                    const int y = iy[b];
+                    const float* row = g + (size_t)K0 * (y + (size_t)K1 * z);
+#pragma unroll
+                    for (int a = 0; a < 4; ++a) {
+                        const float v = row[ix[a]];
+                        const float w = wx[a] * wy[b] * wzc;
+                        phi += w * v;
+                        if (FD) {
+                            const int yp = wrap1(y + 1, K1), ym = wrap1(y - 1, K1);
+                            const int zp = wrap1(z + 1, K2), zm = wrap1(z - 1, K2);
+                            gx += w * (row[ixp[a]] - row[ixm[a]]);
+                            gy += w * (g[(size_t)K0 * (yp + (size_t)K1 * z) + ix[a]] -
+                                       g[(size_t)K0 * (ym + (size_t)K1 * z) + ix[a]]);
+                            gz += w * (g[(size_t)K0 * (y + (size_t)K1 * zp) + ix[a]] -
+                                       g[(size_t)K0 * (y + (size_t)K1 * zm) + ix[a]]);
+                        } else {
+                            gx += dx[a] * wy[b] * wzc * v;
+                            gy += wx[a] * dy[b] * wzc * v;
+                            gz += wx[a] * wy[b] * dzc * v;
+                        }
                     }
                 }
+                ph[cc] = phi;
+                pgx[cc] = gx;
+                pgy[cc] = gy;
+                pgz[cc] = gz;
             }
+            phi = ph[0] + ph[1];
+            gx = pgx[0] + pgx[1];
+            gy = pgy[0] + pgy[1];
+            gz = pgz[0] + pgz[1];
             sc0 = FD ? 0.5f * sd.pme_inv_h[0] : sd.pme_inv_h[0];
             sc1 = FD ? 0.5f * sd.pme_inv_h[1] : sd.pme_inv_h[1];
             sc2 = FD ? 0.5f * sd.pme_inv_h[2] : sd.pme_inv_h[2];
         }
     }
-    // the four planes of one atom sit in adjacent lanes: fixed-order reduction
-#pragma unroll
-    for (int o = 1; o < 4; o <<= 1) {
-        phi += __shfl_xor_sync(0xffffffffu, phi, o);
-        gx += __shfl_xor_sync(0xffffffffu, gx, o);
-        gy += __shfl_xor_sync(0xffffffffu, gy, o);
-        gz += __shfl_xor_sync(0xffffffffu, gz, o);
-    }
-    if (sysi >= 0 && c == 0) {
+    // (p0 + p1) + (p2 + p3): the partner lane holds the second pair
+    phi += __shfl_xor_sync(0xffffffffu, phi, 1);
+    gx += __shfl_xor_sync(0xffffffffu, gx, 1);
+    gy += __shfl_xor_sync(0xffffffffu, gy, 1);
+    gz += __shfl_xor_sync(0xffffffffu, gz, 1);
+    if (sysi >= 0 && half == 0) {
         atomic_add_fixed(st.fx + s, to_fixed(-q * gx * sc0, FORCE_SCALE));
         atomic_add_fixed(st.fy + s, to_fixed(-q * gy * sc1, FORCE_SCALE));
         atomic_add_fixed(st.fz + s, to_fixed(-q * gz * sc2, FORCE_SCALE));
@@ -779,7 +794,7 @@ __global__ void k_gather(DevState st, const SysDesc sd1) {
             }
         }
     }
-    if (ENERGY) add_energy_fixed(st.energy, c == 0 ? sysi : -1, e, E_RECIP);
+    if (ENERGY) add_energy_fixed(st.energy, half == 0 ? sysi : -1, e, E_RECIP);
 }
 
 // ------------------------------------------------------------------ driver
@@ -815,20 +830,21 @@ int launch_pme(const DevState& st, const PmePlan& plan, bool energy, cudaStream_
         k_fft_x_inv<<<plan.n_items_x, 256, sx, s>>>(st, plans, plan.items_x, mx);
     }
     const SysDesc& sd1 = plan.sys0;
+    const int g1 = (int)(((long long)st.n_slots * 2 + TB - 1) / TB);   // gather: two threads per slot
     if (plan.n_sys == 1) {
         if (plan.ref_gather) {
-            if (energy) k_gather<true, true, true><<<g4, TB, 0, s>>>(st, sd1);
-            else k_gather<false, true, true><<<g4, TB, 0, s>>>(st, sd1);
+            if (energy) k_gather<true, true, true><<<g1, TB, 0, s>>>(st, sd1);
+            else k_gather<false, true, true><<<g1, TB, 0, s>>>(st, sd1);
         } else {
-            if (energy) k_gather<true, false, true><<<g4, TB, 0, s>>>(st, sd1);
-            else k_gather<false, false, true><<<g4, TB, 0, s>>>(st, sd1);
+            if (energy) k_gather<true, false, true><<<g1, TB, 0, s>>>(st, sd1);
+            else k_gather<false, false, true><<<g1, TB, 0, s>>>(st, sd1);
         }
     } else if (plan.ref_gather) {
-        if (energy) k_gather<true, true, false><<<g4, TB, 0, s>>>(st, sd1);
-        else k_gather<false, true, false><<<g4, TB, 0, s>>>(st, sd1);
+        if (energy) k_gather<true, true, false><<<g1, TB, 0, s>>>(st, sd1);
+        else k_gather<false, true, false><<<g1, TB, 0, s>>>(st, sd1);
     } else {
-        if (energy) k_gather<true, false, false><<<g4, TB, 0, s>>>(st, sd1);
-        else k_gather<false, false, false><<<g4, TB, 0, s>>>(st, sd1);
+        if (energy) k_gather<true, false, false><<<g1, TB, 0, s>>>(st, sd1);
+        else k_gather<false, false, false><<<g1, TB, 0, s>>>(st, sd1);
     }
     return n;
 }
