@@ -421,6 +421,7 @@ __global__ void k_fft_x_fwd(DevState st, const PmeSysDev* plans, const int4* ite
     const SysDesc& sd = st.sys[it.x];
     const FftPlanDev& pl = plans[it.x].px;
     const int K0 = pl.n, K0h = K0 / 2 + 1;
+    const float iK0 = 1.f / (float)K0, iK0h = 1.f / (float)(K0 / 2 + 1);   // exact small quotients (div_small)
     const int stride = K0 | 1;
     float2* tw = sm;
     float2* A = sm + maxn;
@@ -432,14 +433,14 @@ __global__ void k_fft_x_fwd(DevState st, const PmeSysDev* plans, const int4* ite
     block_copy4<int>(
         nl * K0, [&](int i) { return g[i]; },
         [&](int i, int v) {
-            const int l = i / K0, x = i - l * K0;
+            const int l = div_small(i, iK0), x = i - l * K0;
             A[l * stride + x] = make_float2((float)v * (float)(1.0 / GRID32_SCALE), 0.f);
         });
     __syncthreads();
     const float2* res = fft_lines(A, B, nl, stride, pl, tw, -1.f);
     float2* out = st.pme_cplx + sd.pme_coff + (size_t)it.y * K0h;
     for (int i = threadIdx.x; i < nl * K0h; i += blockDim.x) {
-        const int l = i / K0h, k = i - l * K0h;
+        const int l = div_small(i, iK0h), k = i - l * K0h;
         out[(size_t)l * K0h + k] = res[l * stride + k];
     }
 }
@@ -451,6 +452,7 @@ __global__ void k_fft_x_inv(DevState st, const PmeSysDev* plans, const int4* ite
     const SysDesc& sd = st.sys[it.x];
     const FftPlanDev& pl = plans[it.x].px;
     const int K0 = pl.n, K0h = K0 / 2 + 1;
+    const float iK0 = 1.f / (float)K0, iK0h = 1.f / (float)(K0 / 2 + 1);   // exact small quotients (div_small)
     const int stride = K0 | 1;
     float2* tw = sm;
     float2* A = sm + maxn;
@@ -461,7 +463,7 @@ __global__ void k_fft_x_inv(DevState st, const PmeSysDev* plans, const int4* ite
     block_copy4<float2>(
         nl * K0,
         [&](int i) {
-            const int l = i / K0, k = i - l * K0;
+            const int l = div_small(i, iK0), k = i - l * K0;
             float2 v;
             if (k < K0h) {
                 v = in[(size_t)l * K0h + k];
@@ -472,14 +474,14 @@ __global__ void k_fft_x_inv(DevState st, const PmeSysDev* plans, const int4* ite
             return v;
         },
         [&](int i, float2 v) {
-            const int l = i / K0, k = i - l * K0;
+            const int l = div_small(i, iK0), k = i - l * K0;
             A[l * stride + k] = v;
         });
     __syncthreads();
     const float2* res = fft_lines(A, B, nl, stride, pl, tw, 1.f);
     float* out = st.pme_real + sd.pme_off + (size_t)it.y * K0;
     for (int i = threadIdx.x; i < nl * K0; i += blockDim.x) {
-        const int l = i / K0, x = i - l * K0;
+        const int l = div_small(i, iK0), x = i - l * K0;
         out[(size_t)l * K0 + x] = res[l * stride + x].x;
     }
 }
@@ -584,6 +586,7 @@ __global__ void __launch_bounds__(FFT_XY_THREADS) k_fft_xy_fwd(DevState st, cons
     const FftPlanDev& plx = plans[it.x].px;
     const FftPlanDev& ply = plans[it.x].py;
     const int K0 = plx.n, K1 = ply.n, K0h = K0 / 2 + 1, P = xy_lines(K1), z = it.y;
+    const float iK0 = 1.f / (float)K0, iK0h = 1.f / (float)(K0 / 2 + 1);   // exact small quotients (div_small)
     float2* twx = sm;
     float2* twy = sm + maxn;
     float2* A = sm + 2 * maxn;
@@ -595,21 +598,21 @@ __global__ void __launch_bounds__(FFT_XY_THREADS) k_fft_xy_fwd(DevState st, cons
     block_copy4<float2>(
         P * K0,
         [&](int i) {
-            const int pl = i / K0, x = i - pl * K0;
+            const int pl = div_small(i, iK0), x = i - pl * K0;
             const int ya = 2 * pl, yb = ya + 1;
             const float a = (float)g[(size_t)ya * K0 + x] * (float)(1.0 / GRID32_SCALE);
             const float b = yb < K1 ? (float)g[(size_t)yb * K0 + x] * (float)(1.0 / GRID32_SCALE) : 0.f;
             return make_float2(a, b);
         },
         [&](int i, float2 v) {
-            const int pl = i / K0, x = i - pl * K0;
+            const int pl = div_small(i, iK0), x = i - pl * K0;
             A[pl * sx + x] = v;
         });
     __syncthreads();
     const float2* res = fft_lines(A, B, P, sx, plx, twx, -1.f);
     float2* yl = res == A ? B : A;
     for (int i = threadIdx.x; i < P * K0h; i += blockDim.x) {
-        const int pl = i / K0h, k = i - pl * K0h;
+        const int pl = div_small(i, iK0h), k = i - pl * K0h;
         const float2 Z = res[pl * sx + k];
         const float2 Zm = res[pl * sx + (k == 0 ? 0 : K0 - k)];
         yl[k * sy + 2 * pl] = make_float2(0.5f * (Z.x + Zm.x), 0.5f * (Z.y - Zm.y));
@@ -619,7 +622,7 @@ __global__ void __launch_bounds__(FFT_XY_THREADS) k_fft_xy_fwd(DevState st, cons
     const float2* out = fft_lines(yl, const_cast<float2*>(res), K0h, sy, ply, twy, -1.f);
     float2* gc = st.pme_cplx + sd.pme_coff + (size_t)K0h * K1 * z;
     for (int i = threadIdx.x; i < K1 * K0h; i += blockDim.x) {
-        const int y = i / K0h, x = i - y * K0h;
+        const int y = div_small(i, iK0h), x = i - y * K0h;
         gc[(size_t)y * K0h + x] = out[x * sy + y];
     }
 }
@@ -632,6 +635,7 @@ __global__ void __launch_bounds__(FFT_XY_THREADS) k_fft_xy_inv(DevState st, cons
     const FftPlanDev& plx = plans[it.x].px;
     const FftPlanDev& ply = plans[it.x].py;
     const int K0 = plx.n, K1 = ply.n, K0h = K0 / 2 + 1, P = xy_lines(K1), z = it.y;
+    const float iK0 = 1.f / (float)K0, iK0h = 1.f / (float)(K0 / 2 + 1);   // exact small quotients (div_small)
     float2* twx = sm;
     float2* twy = sm + maxn;
     float2* A = sm + 2 * maxn;
@@ -643,7 +647,7 @@ __global__ void __launch_bounds__(FFT_XY_THREADS) k_fft_xy_inv(DevState st, cons
     block_copy4<float2>(
         K1 * K0h, [&](int i) { return gc[i]; },
         [&](int i, float2 v) {
-            const int y = i / K0h, x = i - y * K0h;
+            const int y = div_small(i, iK0h), x = i - y * K0h;
             A[x * sy + y] = v;
         });
     __syncthreads();
@@ -651,7 +655,7 @@ __global__ void __launch_bounds__(FFT_XY_THREADS) k_fft_xy_inv(DevState st, cons
     float2* xl = res == A ? B : A;
     // full spectra of rows 2p and 2p+1 (Hermitian symmetry beyond K0h), packed as a + i b
     for (int i = threadIdx.x; i < P * K0; i += blockDim.x) {
-        const int pl = i / K0, k = i - pl * K0;
+        const int pl = div_small(i, iK0), k = i - pl * K0;
         const int ya = 2 * pl, yb = ya + 1;
         float2 a, b = make_float2(0.f, 0.f);
         if (k < K0h) {
@@ -671,7 +675,7 @@ __global__ void __launch_bounds__(FFT_XY_THREADS) k_fft_xy_inv(DevState st, cons
     const float2* out = fft_lines(xl, const_cast<float2*>(res), P, sx, plx, twx, 1.f);
     float* gr = st.pme_real + sd.pme_off + (size_t)K0 * K1 * z;
     for (int i = threadIdx.x; i < K1 * K0; i += blockDim.x) {
-        const int y = i / K0, x = i - y * K0;
+        const int y = div_small(i, iK0), x = i - y * K0;
         const float2 v = out[(y >> 1) * sx + x];
         gr[(size_t)y * K0 + x] = (y & 1) ? v.y : v.x;
     }
