@@ -22,7 +22,7 @@ constexpr double GRID_SCALE = 1099511627776.0;   // 2^40 per kC/mol (int64 PME c
 // the engine's int32 PME charge grid: 2^20 per kC/mol, so a node holds up to
 // +-2048 kC/mol (about 21 e of B-spline-weighted charge) in steps of 1e-8 e
 constexpr double GRID32_SCALE = 1048576.0;
-constexpr int SHIFT_BITS = 5;                    // periodic-shift code in pair entries
+constexpr int SHIFT_BITS = 5;                    // periodic-shift code in the pair search's candidates
 constexpr int JCLUSTER_BITS = 32 - SHIFT_BITS;
 
 enum EnergyTerm {

@@ -9,10 +9,10 @@
 //   5. k_gather_slots   state permuted into the new slot order
 //   6. k_finish_slots   slot_of map, permuted velocity state
 //   7. k_bbox           per-cluster bounding boxes
-//   8. k_pairsearch     half list of cluster pairs within cutoff+skin, with a
-//                       64-bit interaction mask (padding, exclusions, i<j on
-//                       the diagonal) and a periodic-shift code per pair, stored
-//                       as rows: one per j-atom with a non-empty 8-bit i-mask.
+//   8. k_pairsearch     half list of cluster pairs within cutoff+skin, stored
+//                       as rows: one per j-atom with a non-empty 8-bit mask of
+//                       the i-atoms it meets (padding, exclusions and i<j on the
+//                       diagonal taken out) and the pair's periodic image.
 // The result is bit-identical run to run: every ordering is fixed by keys,
 // never by atomic arrival order.
 #include "engine.h"
@@ -262,17 +262,18 @@ __device__ __forceinline__ bool excluded(const DevState& st, int ai, int aj, int
 
 // One warp per i-cluster, in two phases that alternate through the column
 // window:
-//   1. candidate search: the clusters of a column are tested 32 at a time
-//      (one per lane) against the i-cluster's extent, for each periodic shift
-//      in range; every (cluster, shift) in range is appended, in lane order, to
-//      a per-warp queue in shared memory;
-//   2. masks: whenever 32 candidates are queued, each lane builds the full
-//      64-bit interaction mask of one of them on its own (the eight i-atoms sit
-//      in registers), and the non-empty ones are appended to the pair list in
+//   1. candidate search: the window's columns are scanned 32 at a time (one per
+//      lane: periodic shift, clusters of the half list) and their clusters taken
+//      32 at a time (one per lane) and tested against the i-cluster's extent for
+//      each periodic image in range; every (cluster, image) in range is
+//      appended, in lane order, to a per-warp queue in shared memory;
+//   2. rows: whenever 32 candidates are queued, four at a time are turned into
+//      rows, one lane per (candidate, j-atom) testing its j-atom against the
+//      eight i-atoms (held in registers); the non-empty rows are appended in
 //      lane order.
-// Instruction count, not memory, bounds this kernel; giving every lane a whole
-// candidate keeps all 32 lanes on distinct work.  The list order is fixed by
-// the column, lane and shift order, so the list is identical run to run.
+// Instruction count, not memory, bounds this kernel.  The list order is fixed
+// by the column, cluster, lane and image order, so the list is identical run to
+// run.
 constexpr int PS_WARPS = 4;
 constexpr int PS_QCAP = 32 + 32 * 27;   // a full batch left over + one column batch with every shift
 

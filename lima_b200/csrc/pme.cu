@@ -414,7 +414,7 @@ __device__ __forceinline__ void block_copy4(int total, Load load, Store store) {
     }
 }
 
-// x pass forward: int64 charge grid -> half-complex rows (and zero the int64 grid)
+// x pass forward: int32 charge grid -> half-complex rows
 __global__ void k_fft_x_fwd(DevState st, const PmeSysDev* plans, const int4* items, int maxn) {
     extern __shared__ float2 sm[];
     const int4 it = items[blockIdx.x];
