@@ -190,7 +190,14 @@ LIMA_API int lima_set_exclusions(lima_engine* h, int n, const int32_t* atoms2);
 LIMA_API int lima_set_pme_grid(lima_engine* h, int nx, int ny, int nz);
 
 /* -------------------------------------------------------------------- state
- * pos [nm] x 3N (double), vel [nm/ns] x 3N (NULL = zero). */
+ * pos [nm] x 3N (double), vel [nm/ns] x 3N (NULL = zero), for the selected system.
+ * A non-finite position is refused with LIMA_ERR_NOT_FINITE and leaves the engine
+ * as it was.  On a built engine the atoms keep their slots and the pair list: a
+ * state handed back unchanged keeps the list's nstlist cadence; a moved one keeps
+ * the list only while every atom stays within half the Verlet buffer of its
+ * position at the last list build, else the list is rebuilt before the next
+ * forces.  The previous-step force (velocity Verlet) and the minimiser's moments
+ * restart at zero, as for a new input. */
 LIMA_API int lima_set_state(lima_engine* h, const double* pos, const float* vel);
 LIMA_API int lima_get_state(lima_engine* h, double* pos, float* vel);
 
