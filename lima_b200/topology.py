@@ -255,7 +255,9 @@ def build_system(top: Topology, gro: GroFile, name: str = "") -> System:
         types = [a[0] for a in mt.atoms]
         for _ in range(count):
             for (t, charge, mass, _nm) in mt.atoms:
-                at = top.atomtypes.get(t, (mass or 0.0, 0.0, 0.0))
+                if t not in top.atomtypes:
+                    raise KeyError(f"atom type {t!r} of molecule {molname!r} is not in [ atomtypes ]")
+                at = top.atomtypes[t]
                 q.append(charge * E_KCMOL)
                 m.append((mass if mass is not None else at[0]) * 1e-3)
                 sig.append(at[1])
@@ -285,6 +287,8 @@ def build_system(top: Topology, gro: GroFile, name: str = "") -> System:
                         ipar.append((pp[0] * DEG, pp[1] * KJ))
                 else:
                     plist = [par] if par else _match_dihedral(top, quad, (1, 4, 9))
+                    if any(len(pp) < 3 for pp in plist):
+                        raise ValueError(f"dihedral {quad} (func {func}) needs phi0, k and multiplicity")
                     for pp in plist:
                         # the reference halves the force constant on load (Bodies.cpp:36-38)
                         dihs.append((off + i, off + j, off + k, off + l))

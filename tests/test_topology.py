@@ -124,6 +124,14 @@ def test_type_tables_and_units(tmp_path):
     assert np.allclose(s.epsilon[0], 0.12 * kj) and np.allclose(s.sigma[1], 0.34)
 
 
+def test_unknown_atom_type_is_an_error(tmp_path):
+    (tmp_path / "ff.itp").write_text(FF)
+    (tmp_path / "m.top").write_text(MOL.replace("5 OX 1 MOL O1 1  0.00", "5 QQ 1 MOL O1 1  0.00"))
+    g = topology.GroFile("t", [1] * 10, ["MOL"] * 10, ["X"] * 10, np.zeros((10, 3)), None, np.array([3.0, 3.0, 3.0]))
+    with pytest.raises(KeyError, match="QQ"):
+        topology.build_system(topology.read_top(str(tmp_path / "m.top")), g)
+
+
 @pytest.mark.skipif(not os.path.isdir(REF), reason="reference tree not present")
 def test_reference_example_inputs():
     top_path = os.path.join(REF, "tests/userinterfacetests/test.top")
