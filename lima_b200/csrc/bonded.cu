@@ -159,12 +159,13 @@ __global__ void k_bonded(DevState st, BondedTerms bt) {
     const int total = bt.nb + bt.na + bt.nd + bt.ni + bt.np;
     float e[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
     float vir = 0.f;
-    int sysi = -1;
+    int sysi = -1, kind = -1;
     if (t < total) {
         f3 f[4];
         f3 r[4];
         int atoms[4];
-        int na = 0, kind = 0;
+        int na = 0;
+        kind = 0;
         if (t < bt.nb) {
             const int2 ix = bt.bidx[t];
             atoms[0] = ix.x;
@@ -238,7 +239,14 @@ __global__ void k_bonded(DevState st, BondedTerms bt) {
     }
     if (ENERGY) {
         const int terms[5] = {E_BOND, E_ANGLE, E_DIHEDRAL, E_IMPROPER, E_PAIRBOND};
-        for (int k = 0; k < 5; ++k) add_energy_fixed(st.energy, sysi, (double)e[k], terms[k]);
+        // terms are stored kind by kind, so a warp almost always holds one kind:
+        // then only that kind's total (and the virial) needs a warp sum
+        const int k0 = __reduce_max_sync(0xffffffffu, kind);
+        if (__all_sync(0xffffffffu, kind < 0 || kind == k0)) {
+            if (k0 >= 0) add_energy_fixed(st.energy, sysi, kind >= 0 ? (double)e[kind] : 0.0, terms[k0]);
+        } else {
+            for (int k = 0; k < 5; ++k) add_energy_fixed(st.energy, sysi, (double)e[k], terms[k]);
+        }
         add_energy_fixed(st.energy, sysi, (double)vir, E_VIRIAL);
     }
 }
