@@ -312,6 +312,23 @@ def run_lima(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
+    if args.profile_large:
+        # profiling mode for the memory-bound kernels (binning and sort, bonded,
+        # exclusion correction, integrator) on a box whose per-atom state is
+        # larger than the 126 MB L2: 2.0 M atoms of water with 64 chains (bonds,
+        # angles, dihedrals), PME spacing 0.12 nm; set-up plus `profile_large`
+        # plain steps
+        sl = systems.water_with_chains(2_000_000, 64, seed=7, name="water2M")
+        el = Engine(cutoff=CUTOFF, electrostatics=E.ES_EWALD, ewald_tol=1e-5, pme_spacing=0.12, nstlist=10,
+                    dt=DT_NS, device=local)
+        el.load(sl)
+        el.step(args.profile_large)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_large_steps": args.profile_large, "atoms": sl.n,
+                          "bonds": len(sl.bonds), "angles": len(sl.angles), "dihedrals": len(sl.dihedrals),
+                          "timings": el.timings()}), flush=True)
+        el.close()
+        return 0
     s = systems.config2()
     eng = Engine(cutoff=CUTOFF, electrostatics=E.ES_EWALD, ewald_tol=1e-5, nstlist=10, dt=DT_NS, device=local)
     eng.load(s, pme_grid=GRID)
@@ -492,6 +509,8 @@ def main():
     ap.add_argument("--profile", type=int, default=0, help="only set up and run this many steps (ncu)")
     ap.add_argument("--profile-learned", type=int, default=0,
                     help="only set up the learned correction and run this many steps with it (ncu)")
+    ap.add_argument("--profile-large", type=int, default=0,
+                    help="only set up a 2 M-atom water box with chains and run this many steps (ncu)")
     ap.add_argument("--no-other-configs", action="store_true")
     ap.add_argument("--skip-batch", action="store_true")
     ap.add_argument("--other-steps", type=int, default=100)

@@ -139,7 +139,10 @@ __global__ void k_scatter(DevState st, int from_input) {
     }
 }
 
-// one CTA per column: rank each atom by the unique key (z bits, atom index)
+// One CTA per column: the column's atoms sorted by the unique key (z bits, atom
+// index) with a bitonic network in shared memory over the next power of two of
+// the column's count; padding keys are all ones and sort last.  The keys are
+// unique, so the order is the one a rank count gives, whatever the network.
 __global__ void k_sort_columns(DevState st, const int* col_sys) {
     extern __shared__ unsigned long long keys[];
     const int col = blockIdx.x;
@@ -148,18 +151,33 @@ __global__ void k_sort_columns(DevState st, const int* col_sys) {
     const int off = st.sys[col_sys[col]].atom_off + st.col_atom_start[col];
     const int slot0 = st.col_cl_start[col] * CLUSTER;
     const int padded = st.col_ncl[col] * CLUSTER;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const int a = st.col_list[off + i];
-        keys[i] = ((unsigned long long)__float_as_uint(st.z_of_atom[a]) << 32) | (unsigned)a;
+    int m = 1;
+    while (m < n) m <<= 1;
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        unsigned long long k = ~0ull;
+        if (i < n) {
+            const int a = st.col_list[off + i];
+            k = ((unsigned long long)__float_as_uint(st.z_of_atom[a]) << 32) | (unsigned)a;
+        }
+        keys[i] = k;
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const unsigned long long k = keys[i];
-        int rank = 0;
-        for (int j = 0; j < n; ++j) rank += keys[j] < k;
-        if (rank < padded) st.new_orig[slot0 + rank] = (int)(k & 0xffffffffu);   // cut on overflow
-    }
-    for (int r = n + threadIdx.x; r < padded; r += blockDim.x) st.new_orig[slot0 + r] = -1;
+    for (int k = 2; k <= m; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            // pair t compares elements i and i + j, i with bit j clear
+            for (int t = threadIdx.x; t < (m >> 1); t += blockDim.x) {
+                const int i = ((t & ~(j - 1)) << 1) | (t & (j - 1));
+                const unsigned long long a = keys[i], b = keys[i + j];
+                if ((a > b) == ((i & k) == 0)) {
+                    keys[i] = b;
+                    keys[i + j] = a;
+                }
+            }
+            __syncthreads();
+        }
+    // ranks past the column's cluster range are cut (overflow, flagged below)
+    for (int r = threadIdx.x; r < padded; r += blockDim.x)
+        st.new_orig[slot0 + r] = r < n ? (int)(keys[r] & 0xffffffffu) : -1;
     __syncthreads();
     if (threadIdx.x == 0) {
         if (n_all > st.col_cap) atomicOr(st.status, ST_COLUMN_OVERFLOW);
@@ -535,7 +553,16 @@ int launch_rebuild_slots(const DevState& st, bool from_input, cudaStream_t s) {
     k_bin<<<(nt + TB - 1) / TB, TB, 0, s>>>(st, from_input ? 1 : 0);
     k_scan_columns<<<st.n_sys, 1024, 0, s>>>(st);
     k_scatter<<<(nt + TB - 1) / TB, TB, 0, s>>>(st, from_input ? 1 : 0);
-    k_sort_columns<<<st.n_cols, 128, (size_t)st.col_cap * sizeof(unsigned long long), s>>>(st, st.col_sys);
+    // keys for the next power of two of the column capacity (at most 8192: 64 KB)
+    int m = 1;
+    while (m < st.col_cap) m <<= 1;
+    static bool sort_attr = false;
+    if (!sort_attr) {
+        cudaFuncSetAttribute(k_sort_columns, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             8192 * (int)sizeof(unsigned long long));
+        sort_attr = true;
+    }
+    k_sort_columns<<<st.n_cols, 128, (size_t)m * sizeof(unsigned long long), s>>>(st, st.col_sys);
     k_gather_slots<<<(st.n_slots + TB - 1) / TB, TB, 0, s>>>(st, from_input ? 1 : 0);
     k_finish_slots<<<(st.n_slots + TB - 1) / TB, TB, 0, s>>>(st);
     k_bbox<<<(st.n_clusters + TB - 1) / TB, TB, 0, s>>>(st);
