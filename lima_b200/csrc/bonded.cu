@@ -49,7 +49,7 @@ __device__ __forceinline__ void add_force(const DevState& st, int a, f3 f) {
 }
 
 // harmonic bond: E = kb/2 (|d|-b0)^2, force on a along -d
-__device__ float bond_term(f3 d /* a - b */, float b0, float kb, f3* f) {
+__device__ __forceinline__ float bond_term(f3 d /* a - b */, float b0, float kb, f3* f) {
     const float r = len(d);
     const float err = r - b0;
     const f3 u = unit(d);
@@ -59,7 +59,7 @@ __device__ float bond_term(f3 d /* a - b */, float b0, float kb, f3* f) {
 }
 
 // harmonic angle on in-plane normals + Urey-Bradley spring (positions relative to the middle atom)
-__device__ float angle_term(f3 a1 /* l - m */, f3 a2 /* r - m */, float4 par, f3* f) {
+__device__ __forceinline__ float angle_term(f3 a1 /* l - m */, f3 a2 /* r - m */, float4 par, f3* f) {
     const f3 v1 = unit(a1), v2 = unit(a2);
     const f3 nrm = unit(cross(v1, v2));
     const f3 dl = unit(cross(nrm, v1));
@@ -81,7 +81,7 @@ __device__ float angle_term(f3 a1 /* l - m */, f3 a2 /* r - m */, float4 par, f3
 }
 
 // periodic dihedral k(1+cos(n tau - phi0)), tau = -atan2(sin phi, cos phi)
-__device__ float dihedral_term(f3 b1, f3 b2, f3 b3, float4 par, f3* f) {
+__device__ __forceinline__ float dihedral_term(f3 b1, f3 b2, f3 b3, float4 par, f3* f) {
     const float phi0 = par.x, k = par.y, mult = par.z;
     const f3 A = cross(b1, b2), B = cross(b2, b3), C = cross(b2, A);
     const float iA = 1.f / len(A), iB = 1.f / len(B), iC = 1.f / len(C);
@@ -122,7 +122,7 @@ __device__ __forceinline__ float dist_to_line(f3 p, f3 a, f3 b) {
 }
 
 // improper: signed angle between the (i,j,k) and (l,j,k) planes
-__device__ float improper_term(f3 pi, f3 pj, f3 pk, f3 pl, float2 par, f3* f) {
+__device__ __forceinline__ float improper_term(f3 pi, f3 pj, f3 pk, f3 pl, float2 par, f3* f) {
     const f3 ij = unit(pj - pi), ik = unit(pk - pi), il = unit(pl - pi);
     const f3 lj = unit(pj - pl), lk = unit(pk - pl);
     const f3 n1 = unit(cross(ij, ik));
@@ -142,7 +142,7 @@ __device__ float improper_term(f3 pi, f3 pj, f3 pk, f3 pl, float2 par, f3* f) {
 }
 
 // LJ pair bond, no cutoff; d = b - a
-__device__ float pairbond_term(f3 d, float sig, float eps, f3* f) {
+__device__ __forceinline__ float pairbond_term(f3 d, float sig, float eps, f3* f) {
     const float r2 = dot(d, d);
     float s = sig * sig / r2;
     s = s * s * s;
@@ -157,8 +157,7 @@ template <bool ENERGY>
 __global__ void k_bonded(DevState st, BondedTerms bt) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int total = bt.nb + bt.na + bt.nd + bt.ni + bt.np;
-    float e[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
-    float vir = 0.f;
+    float en = 0.f, vir = 0.f;   // this thread's term energy (of kind `kind`) and virial
     int sysi = -1, kind = -1;
     if (t < total) {
         f3 f[4];
@@ -206,9 +205,12 @@ __global__ void k_bonded(DevState st, BondedTerms bt) {
         sysi = st.atom_sys[atoms[0]];
         const SysDesc& sd = st.sys[sysi];
         const int s0 = st.slot_of[atoms[0]];
+        // loops over the term's atoms run to 4 with a guard, so that every index is
+        // a constant and atoms, r and f stay in registers
         r[0] = f3{0.f, 0.f, 0.f};
-        for (int k = 1; k < na; ++k) r[k] = rel(st, sd, s0, atoms[k]);
-        float en = 0.f;
+#pragma unroll
+        for (int k = 1; k < 4; ++k)
+            if (k < na) r[k] = rel(st, sd, s0, atoms[k]);
         switch (kind) {
             case 0: {
                 const float2 p = bt.bpar[t];
@@ -228,14 +230,16 @@ __global__ void k_bonded(DevState st, BondedTerms bt) {
                 en = pairbond_term(r[1] - r[0], p.x, p.y, f);
             } break;
         }
-        for (int k = 0; k < na; ++k) {
-            add_force(st, atoms[k], f[k]);
-            if (ENERGY) {
-                vir += -0.5f * dot(r[k], f[k]);
-                if (st.atom_energy) add_atom_energy(st.epot, st.slot_of[atoms[k]], (double)en / na);  // equal shares
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (k < na) {
+                add_force(st, atoms[k], f[k]);
+                if (ENERGY) {
+                    vir += -0.5f * dot(r[k], f[k]);
+                    if (st.atom_energy) add_atom_energy(st.epot, st.slot_of[atoms[k]], (double)en / na);  // equal shares
+                }
             }
         }
-        if (ENERGY) e[kind] = en;
     }
     if (ENERGY) {
         const int terms[5] = {E_BOND, E_ANGLE, E_DIHEDRAL, E_IMPROPER, E_PAIRBOND};
@@ -243,9 +247,10 @@ __global__ void k_bonded(DevState st, BondedTerms bt) {
         // then only that kind's total (and the virial) needs a warp sum
         const int k0 = __reduce_max_sync(0xffffffffu, kind);
         if (__all_sync(0xffffffffu, kind < 0 || kind == k0)) {
-            if (k0 >= 0) add_energy_fixed(st.energy, sysi, kind >= 0 ? (double)e[kind] : 0.0, terms[k0]);
+            if (k0 >= 0) add_energy_fixed(st.energy, sysi, kind >= 0 ? (double)en : 0.0, terms[k0]);
         } else {
-            for (int k = 0; k < 5; ++k) add_energy_fixed(st.energy, sysi, (double)e[k], terms[k]);
+#pragma unroll
+            for (int k = 0; k < 5; ++k) add_energy_fixed(st.energy, sysi, kind == k ? (double)en : 0.0, terms[k]);
         }
         add_energy_fixed(st.energy, sysi, (double)vir, E_VIRIAL);
     }

@@ -205,6 +205,10 @@ __device__ __forceinline__ int wrapk(int i, int n) {
     i %= n;
     return i < 0 ? i + n : i;
 }
+// element c of a 4-array for a c known only at run time, without local memory
+__device__ __forceinline__ float pick4(const float (&w)[4], int c) {
+    return c == 0 ? w[0] : (c == 1 ? w[1] : (c == 2 ? w[2] : w[3]));
+}
 // i mod n for i in [-n, 2n): a node index at most one period outside the grid
 __device__ __forceinline__ int wrap1(int i, int n) {
     return i < 0 ? i + n : (i >= n ? i - n : i);
@@ -254,7 +258,7 @@ __global__ void k_spread(DevState st) {
 #pragma unroll
     for (int a = 0; a < 4; ++a) ix[a] = wrap1(b0 - 1 + a, K0);
     const int z = wrap1(b2 - 1 + c, K2);
-    const float qz = p.w * wz[c];
+    const float qz = p.w * pick4(wz, c);
 #pragma unroll
     for (int b = 0; b < 4; ++b) {
         const int y = wrap1(b1 - 1 + b, K1);
@@ -329,20 +333,25 @@ __global__ void __launch_bounds__(256) k_spread_tiles(DevState st, const int4* i
                 else if (lx > NX + K0 / 2) lx -= K0;
                 if (ly < -K1 / 2) ly += K1;
                 else if (ly > NY + K1 / 2) ly -= K1;
-                const float qz = p.w * wz[c];
-                const bool inside = lx >= 0 && lx + 3 < NX && ly >= 0 && ly + 3 < NY;
+                // the fixed-point scale is a power of two, so taking it into the
+                // charge first gives every product that can round to a non-zero
+                // integer exactly as q w_z w_y w_x scaled last (k_spread's order)
+                const float qz = p.w * pick4(wz, c) * (float)GRID32_SCALE;
+                if (lx >= 0 && lx + 3 < NX && ly >= 0 && ly + 3 < NY) {
+                    int* node = sbox + lx + NX * (ly + NY * lz);
 #pragma unroll
-                for (int b = 0; b < 4; ++b) {
-                    const float qyz = qz * wy[b];
+                    for (int b = 0; b < 4; ++b) {
+                        const float qyz = qz * wy[b];
 #pragma unroll
-                    for (int a = 0; a < 4; ++a) {
-                        const int v = __float2int_rn(qyz * wx[a] * (float)GRID32_SCALE);
-                        if (inside) {
-                            atomicAdd(&sbox[(lx + a) + NX * ((ly + b) + NY * lz)], v);
-                        } else {
-                            const int x = wrap1(b0 - 1 + a, K0), y = wrap1(b1 - 1 + b, K1);
-                            atomicAdd(g + x + (size_t)K0 * (y + (size_t)K1 * z), v);
-                        }
+                        for (int a = 0; a < 4; ++a) atomicAdd(node + a + NX * b, __float2int_rn(qyz * wx[a]));
+                    }
+                } else {
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) {
+                        const float qyz = qz * wy[b];
+                        int* row = g + (size_t)K0 * (wrap1(b1 - 1 + b, K1) + (size_t)K1 * z);
+#pragma unroll
+                        for (int a = 0; a < 4; ++a) atomicAdd(row + wrap1(b0 - 1 + a, K0), __float2int_rn(qyz * wx[a]));
                     }
                 }
             }
