@@ -11,8 +11,10 @@
 //   7. k_bbox           per-cluster bounding boxes
 //   8. k_pairsearch     half list of cluster pairs within cutoff+skin, stored
 //                       as rows: one per j-atom with a non-empty 8-bit mask of
-//                       the i-atoms it meets (padding, exclusions and i<j on the
-//                       diagonal taken out) and the pair's periodic image.
+//                       the i-atoms it meets (padding and exclusions taken out;
+//                       a cluster with itself keeps i<j unshifted and one image
+//                       of each +/- pair of its own periodic images) and the
+//                       pair's periodic image.
 // The result is bit-identical run to run: every ordering is fixed by keys,
 // never by atomic arrival order.
 #include "engine.h"
@@ -398,8 +400,12 @@ __global__ void __launch_bounds__(PS_WARPS * 32, 1) k_pairsearch(DevState st, fl
                         }
                     }
                 }
-                // the diagonal cluster counts each pair once: keep ii < jj only
-                if (jc == ci) m8 &= (1u << jj) - 1u;
+                // the i-cluster with itself counts each pair once: unshifted, ii < jj;
+                // against its own periodic image (code > 13 only: the image -s of a
+                // pair under shift s is the same pair), every ii other than jj.  An
+                // own image is in range only when the cluster spans most of the box
+                // (a sparse system), never for an atom with itself (box > 2 r_list)
+                if (jc == ci) m8 &= code == 13 ? (1u << jj) - 1u : ~(1u << jj);
             }
             const unsigned has = __ballot_sync(0xffffffffu, m8 != 0u);
             const int pos = count + __popc(has & ((1u << lane) - 1u));
@@ -476,7 +482,7 @@ __global__ void __launch_bounds__(PS_WARPS * 32, 1) k_pairsearch(DevState st, fl
                         const int base = (sx_col + 1) + 3 * (sy_col + 1);
                         for (int sz = -1; sz <= 1; ++sz) {
                             const int code = base + 9 * (sz + 1);
-                            if (j == ci && code != 13) continue;
+                            if (j == ci && code < 13) continue;   // own images: one of each +/- pair
                             const float gz = fmaxf(fabsf(jc[2] + sz * L[2] - ic[2]) - ie[2] - je[2], 0.f);
                             if (gxy + gz * gz < R2) shifts |= 1u << code;
                         }
@@ -494,7 +500,7 @@ __global__ void __launch_bounds__(PS_WARPS * 32, 1) k_pairsearch(DevState st, fl
                     }
 #pragma unroll 1
                     for (int code = 0; code < 27; ++code) {
-                        if (j == ci && code != 13) continue;
+                        if (j == ci && code < 13) continue;   // own images: one of each +/- pair
                         const int sx = code % 3, sy = (code / 3) % 3, sz = code / 9;
                         const float gxs = sx == 0 ? g2[0][0] : (sx == 1 ? g2[0][1] : g2[0][2]);
                         const float gys = sy == 0 ? g2[1][0] : (sy == 1 ? g2[1][1] : g2[1][2]);
