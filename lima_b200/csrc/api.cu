@@ -12,6 +12,7 @@
 //   bonded :        bonded terms + Ewald exclusion correction --^
 //   pme    :        spread -> 5 FFT passes -> gather -----------^
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -382,6 +383,27 @@ void lima_engine::setup() {
         const int ncols = D.ncol_x * D.ncol_y;
         const double per_col = (double)S.n / ncols;
         col_cap = std::max(col_cap, (int)std::ceil(3.0 * per_col + 64.0));
+        // an inhomogeneous system (a droplet, a slab with vacuum) fills some
+        // columns far above the average: size the capacity from the columns the
+        // current positions fill (the device binning maps the same way)
+        {
+            std::vector<int> cc(ncols, 0);
+            for (int a = 0; a < S.n; ++a) {
+                int c[2];
+                const int nc[2] = {D.ncol_x, D.ncol_y};
+                for (int d = 0; d < 2; ++d) {
+                    const double L = S.box[d];
+                    double x = S.pos[3 * (size_t)a + d];
+                    x -= L * std::floor(x / L);
+                    if (!(x < L)) x -= L;
+                    if (!(x >= 0.0)) x = 0.0;
+                    c[d] = std::min(std::max((int)(x * nc[d] / L), 0), nc[d] - 1);
+                }
+                ++cc[c[0] + D.ncol_x * c[1]];
+            }
+            const int fullest = *std::max_element(cc.begin(), cc.end());
+            col_cap = std::max(col_cap, (int)std::ceil(1.5 * fullest + 64.0));
+        }
         D.atom_off = n_atoms_off[s];
         D.n_atoms = S.n;
         D.max_clusters = (S.n + CLUSTER - 1) / CLUSTER + ncols;
@@ -611,7 +633,7 @@ void lima_engine::setup() {
     D.bb_molsig = dalloc<unsigned long long>(n_clusters);
     D.pl_count = dalloc<int>(n_clusters);
     D.pl_row = dalloc<int2>((size_t)n_clusters * pl_cap);
-    D.status = dalloc<unsigned>(1);
+    D.status = dalloc<unsigned>(2);   // [0] ST_* flags, [1] largest pair-list row count a search needed
     D.energy = dalloc<long long>((size_t)ns * E_COUNT);
     D.epot = dalloc<long long>(S);
     D.xyz_ref = dalloc<float4>(S);
@@ -998,37 +1020,43 @@ void lima_engine::start_rebuild(bool from_input) {
         CK(cudaMemcpyAsync(st.in_pos, pos.data(), pos.size() * sizeof(double), cudaMemcpyHostToDevice, s_main));
         CK(cudaMemcpyAsync(st.in_vel, vel.data(), vel.size() * sizeof(float), cudaMemcpyHostToDevice, s_main));
     }
-    CK(cudaMemsetAsync(st.status, 0, sizeof(unsigned), s_main));
+    CK(cudaMemsetAsync(st.status, 0, 2 * sizeof(unsigned), s_main));
     mark(0, 0, s_main);
     launches += launch_rebuild_slots(st, from_input, s_main);
 }
 
 // Part two: the pair search, then the host checks the status word.  A column
-// overflow rejects the build; a full pair list grows and only the search is
-// redone (the slots are final, and other streams may already be reading them).
+// overflow rejects the build; a full pair list grows to the largest row count
+// the search needed (it counts past the capacity) and only the search is redone
+// (the slots are final, and other streams may already be reading them).
 void lima_engine::finish_rebuild() {
-    for (int attempt = 0; attempt < 4; ++attempt) {
+    for (int attempt = 0; attempt < 3; ++attempt) {
         launches += launch_pairsearch(st, (float)rlist, s_main);
         if (attempt == 0) {
             mark(0, 1, s_main);
             ++rebuilds;
         }
         CK(cudaGetLastError());
-        unsigned status = 0;
-        CK(cudaMemcpyAsync(&status, st.status, sizeof(unsigned), cudaMemcpyDeviceToHost, s_main));
+        unsigned status[2] = {0u, 0u};
+        CK(cudaMemcpyAsync(status, st.status, sizeof(status), cudaMemcpyDeviceToHost, s_main));
         CK(cudaStreamSynchronize(s_main));
-        if (status & ST_COLUMN_OVERFLOW) throw ApiError{LIMA_ERR_OVERFLOW, "column capacity exceeded (atoms too dense)"};
-        if (!(status & ST_PAIRLIST_OVERFLOW)) {
+        if (status[0] & ST_COLUMN_OVERFLOW) throw ApiError{LIMA_ERR_OVERFLOW, "column capacity exceeded (atoms too dense)"};
+        if (!(status[0] & ST_PAIRLIST_OVERFLOW)) {
             list_age = 0;
             return;
         }
-        const int cap = (st.pl_cap * 3 / 2 + 31) / 32 * 32;
+        // room for the largest row count of this build plus an eighth for the
+        // motion until the next one
+        const long long need = (long long)status[1] + status[1] / 8 + 32;
+        const long long grown = std::max<long long>((long long)st.pl_cap * 3 / 2, need);
+        if (grown > INT_MAX / 2) throw ApiError{LIMA_ERR_OVERFLOW, "pair list too long for one cluster"};
+        const int cap = (int)((grown + 31) / 32 * 32);
         cudaFree(st.pl_row);
         allocs.erase(std::remove(allocs.begin(), allocs.end(), (void*)st.pl_row), allocs.end());
         st.pl_cap = cap;
         st.pl_row = dalloc<int2>((size_t)st.n_clusters * cap);
         drop_graph();
-        CK(cudaMemsetAsync(st.status, 0, sizeof(unsigned), s_main));
+        CK(cudaMemsetAsync(st.status, 0, 2 * sizeof(unsigned), s_main));
     }
     throw ApiError{LIMA_ERR_OVERFLOW, "pair list overflow persists"};
 }

@@ -546,7 +546,10 @@ __global__ void __launch_bounds__(PS_WARPS * 32, 1) k_pairsearch(DevState st, fl
     if (qn > 0) build_masks(0, qn);
     if (lane == 0) {
         st.pl_count[ci] = min(count, cap);
-        if (count > cap) atomicOr(st.status, ST_PAIRLIST_OVERFLOW);
+        if (count > cap) {
+            atomicOr(st.status, ST_PAIRLIST_OVERFLOW);
+            atomicMax(st.status + 1, (unsigned)count);   // the capacity this build needed
+        }
     }
 }
 

@@ -1,4 +1,4 @@
-"""Sparse and tiny systems through the C-ABI against the FP64 CPU oracle.
+"""Sparse, tiny and inhomogeneous systems through the C-ABI against the FP64 CPU oracle.
 
 A few ions in a 3 nm box (the reference's electrostatics tests use such
 systems, ElectrostaticsTests.h:300-396): the column grid has one column and all
@@ -77,3 +77,52 @@ def test_sparse_system_matches_oracle(oracle, case):
     en = e.energies()
     for k, b in er.items():
         assert abs(en[k] - b) <= 1e-5 * max(abs(b), 1e-3 * abs(en["potential"]), 1e-6), (k, en[k], b)
+
+
+def droplet(radius=1.4, box=6.0):
+    """Waters of a 3 nm box within `radius` of its centre, whole molecules, in the
+    middle of an empty `box` nm cube: the central columns of the pair-search grid
+    hold several times the average column count."""
+    w = systems.water_box(900, 3.0, seed=11)
+    c = w.box / 2
+    d = w.pos[0::3] - c
+    d -= w.box * np.round(d / w.box)
+    keep = np.nonzero(np.linalg.norm(d, axis=1) < radius)[0]
+    atoms = (3 * keep[:, None] + np.arange(3)).ravel()
+    p = (w.pos[atoms] - c).reshape(-1, 3, 3)
+    p[:, 0] -= w.box * np.round(p[:, 0] / w.box)
+    h = p[:, 1:] - p[:, :1]
+    p[:, 1:] = p[:, :1] + (h - w.box * np.round(h / w.box))
+    p = p.reshape(-1, 3) + box / 2
+    remap = -np.ones(w.n, np.int64)
+    remap[atoms] = np.arange(len(atoms))
+    kb = np.all(np.isin(w.bonds, atoms), axis=1)
+    ka = np.all(np.isin(w.angles, atoms), axis=1)
+    return systems.System(box=np.array([box] * 3), pos=p, vel=w.vel[atoms], charge=w.charge[atoms],
+                          mass=w.mass[atoms], sigma=w.sigma[atoms], epsilon=w.epsilon[atoms],
+                          bonds=remap[w.bonds[kb]].astype(np.int32), bond_par=w.bond_par[kb],
+                          angles=remap[w.angles[ka]].astype(np.int32), angle_par=w.angle_par[ka],
+                          name="droplet")
+
+
+def test_droplet_in_vacuum(oracle):
+    """An inhomogeneous system: column and pair-list capacities follow the
+    densest columns, not the average density; forces and energies match the
+    oracle before and after 20 steps (two list rebuilds)."""
+    s = droplet()
+    kappa = kappa_from_tol(RC, 1e-5)
+    grid = (60, 60, 60)
+    e = Engine(cutoff=RC, electrostatics=E.ES_EWALD, ewald_kappa=kappa, nstlist=10, dt=1e-6)
+    e.load(s, pme_grid=grid)
+    for n_steps in (0, 20):
+        if n_steps:
+            e.step(n_steps)
+        e.compute_forces(energy=True)
+        pos, _ = e.state()
+        s2 = systems.System(**{**s.__dict__, "pos": pos})
+        fr, er = oracle_total(oracle, s2, RC, 2, kappa, grid)
+        f = e.forces()
+        assert rel_rms(f, fr) < 1e-4, (n_steps, rel_rms(f, fr))
+        en = e.energies()
+        for k, b in er.items():
+            assert abs(en[k] - b) <= 1e-5 * max(abs(b), 1e-3 * abs(en["potential"]), 1e-6), (n_steps, k, en[k], b)
