@@ -126,3 +126,47 @@ def test_droplet_in_vacuum(oracle):
         en = e.energies()
         for k, b in er.items():
             assert abs(en[k] - b) <= 1e-5 * max(abs(b), 1e-3 * abs(en["potential"]), 1e-6), (n_steps, k, en[k], b)
+
+
+def dilute_slab(n=240, lxy=14.0, lz=2.4, seed=3, min_dist=0.35):
+    """A dilute gas of +/-0.5 e ions in a thin slab box: columns of the pair
+    search hold about 10 atoms spread over the whole 2.4 nm height, so a cluster
+    meets its own periodic image along z while the column window stays narrower
+    than the grid in x and y (the search's fixed x-y shift branch)."""
+    rng = np.random.default_rng(seed)
+    box = np.array([lxy, lxy, lz])
+    pts = []
+    while len(pts) < n:
+        p = rng.random(3) * box
+        if pts:
+            d = np.asarray(pts) - p
+            d -= box * np.round(d / box)
+            if (np.linalg.norm(d, axis=1) < min_dist).any():
+                continue
+        pts.append(p)
+    q = np.where(np.arange(n) % 2 == 0, 0.5, -0.5)
+    s = ions(pts, q)
+    s.box = box
+    return s
+
+
+def test_dilute_slab_own_z_images(oracle):
+    s = dilute_slab()
+    kappa = kappa_from_tol(RC, 1e-5)
+    grid = (144, 144, 24)
+    e = Engine(cutoff=RC, electrostatics=E.ES_EWALD, ewald_kappa=kappa)
+    e.load(s, pme_grid=grid)
+    e.compute_forces(energy=True)
+    got = e.pairlist()
+    ref, flags, nband = oracle.pairset(s.pos, s.box, s.exclusions(), RC, band=1e-5)
+    assert len(got) == len(set(map(tuple, got.tolist())))
+    assert set(map(tuple, got.tolist())) == set(map(tuple, ref.tolist()))
+    # pairs that meet only across the z boundary (direct distance beyond the cutoff)
+    across = [(i, j) for i, j in ref.tolist() if np.linalg.norm(s.pos[i] - s.pos[j]) > RC]
+    assert len(across) > 5
+    f = e.forces()
+    fr, er = oracle_total(oracle, s, RC, 2, kappa, grid)
+    assert rel_rms(f, fr) < 1e-4, rel_rms(f, fr)
+    en = e.energies()
+    for k, b in er.items():
+        assert abs(en[k] - b) <= 1e-5 * max(abs(b), 1e-3 * abs(en["potential"]), 1e-6), (k, en[k], b)
