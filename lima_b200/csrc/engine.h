@@ -112,7 +112,7 @@ struct NbParams {
     float ke;             // Coulomb constant
     float two_kappa_sqrtpi;
     float mk2_log2e;      // -kappa^2 log2(e): exp(-kappa^2 r^2) = 2^(mk2_log2e r^2)
-    int em;               // energy-minimisation force clamp
+    int em;               // energy minimisation: force-only launches take the pair kernel's EM variant
 };
 // periodic image of a pair-list row: (sx + 1) | (sy + 1) << 2 | (sz + 1) << 4 in bits
 // 8-13 of the row's second word, above the 8-bit i-mask

@@ -65,6 +65,17 @@ __device__ __forceinline__ f2p fma2(f2p a, f2p b, f2p c) {
     asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d.v) : "l"(a.v), "l"(b.v), "l"(c.v));
     return d;
 }
+// Energy minimisation: every LJ pair force passes through the reference's tanh
+// activation, |F| -> A tanh(|F| / A) with A = 1e8 in its 1/24 J/mol/nm force unit
+// (LennardJonesInteractions.cuh:85-101 with EngineUtils.cuh:112-140), after its
+// +-1e20 guard on the scalar.  fsl multiplies the pair vector, r is the distance.
+__device__ __forceinline__ float em_lj_clamp(float fsl, float r) {
+    constexpr float A = 24.f * 1e8f;   // [J/mol/nm]
+    fsl = fmaxf(fminf(fsl, 24.f * 1e20f), -24.f * 1e20f);
+    const float f = fabsf(fsl) * r;
+    return fsl * (A * tanhf(f / A) / (f + 24.f * 1e-8f));
+}
+
 // 2^x, the hardware approximation (PTX ex2.approx.ftz.f32)
 __device__ __forceinline__ float ex2_approx(float x) {
     float y;
@@ -86,8 +97,9 @@ __device__ __forceinline__ float ex2_approx(float x) {
 // PF: each lane loads two rows (k and k + 32) before working on either, so that
 // the second row's loads overlap the first row's arithmetic; the rows are
 // worked in the same order, so the results are the same bits either way.
-template <int ES, int EN, bool PF>
-__global__ void __launch_bounds__(256, (EN || PF) ? 2 : 3) k_nonbonded(DevState st, NbParams p) {
+// EM: the energy-minimisation variant (force only, the per-pair LJ clamp above).
+template <int ES, int EN, bool PF, bool EM = false>
+__global__ void __launch_bounds__(256, (EN || PF || EM) ? 2 : 3) k_nonbonded(DevState st, NbParams p) {
     constexpr bool ENERGY = EN > 0, ATOM = EN > 1;
     // per warp, i-atom pairs (ip, ip + 4): (x0, x1, y0, y1), (z0, z1, -q0 ke, -q1 ke),
     // (sigma0/2, sigma1/2, 24 sqrt(eps0), 24 sqrt(eps1))
@@ -171,6 +183,10 @@ __global__ void __launch_bounds__(256, (EN || PF) ? 2 : 3) k_nonbonded(DevState 
             const f2p s6 = mul2(mul2(s2, s2), s2);
             // LJ: 24 eps s6 (1 - 2 s6) / r^2
             f2p fs = mul2(mul2(eps24, s6), mul2(rinv2, fma2(s6, mtwo2, one2)));
+            if (EM) {
+                const float2 v = up2(fs), rr = up2(mul2(r2, rinv));
+                fs = pk2(em_lj_clamp(v.x, rr.x), em_lj_clamp(v.y, rr.y));
+            }
             f2p ec = zero2;
             if (ES != 0) {
                 // qn = -k_e q_i q_j (the sign rides on the i-charge)
@@ -194,7 +210,7 @@ __global__ void __launch_bounds__(256, (EN || PF) ? 2 : 3) k_nonbonded(DevState 
                 }
             }
             float2 fsv = up2(fs);
-            if (p.em) {
+            if (EM) {   // a non-finite Coulomb term (coincident atoms) kept finite
                 fsv.x = fmaxf(fminf(fsv.x, 1e20f), -1e20f);
                 fsv.y = fmaxf(fminf(fsv.y, 1e20f), -1e20f);
             }
@@ -309,6 +325,10 @@ __global__ void __launch_bounds__(256, (EN || PF) ? 2 : 3) k_nonbonded(DevState 
 template <int ES>
 static void launch_nb_shape(const DevState& st, const NbParams& p, bool energy, int shape, cudaStream_t s) {
     const long long threads = (long long)st.n_clusters * 32;
+    if (p.em && !energy) {   // energy minimisation: forces with the per-pair LJ clamp
+        k_nonbonded<ES, 0, false, true><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(st, p);
+        return;
+    }
     const int tb = (shape & 2) ? 128 : 256;
     const dim3 grid((unsigned)((threads + tb - 1) / tb));
     if (energy) {

@@ -137,12 +137,23 @@ struct PairOut {
 
 template <typename T>
 inline PairOut<T> pair_interaction(V3<T> diff /* r_j - r_i */, T r2, T sig, T eps, T qq, int es_mode,
-                                   T kappa, T ke, T pi_c) {
+                                   T kappa, T ke, T pi_c, bool em = false) {
     PairOut<T> o;
     const T inv_r2 = T(1) / r2;
     T s = sig * sig * inv_r2;
     s = s * s * s;
-    const T lj_scalar = T(24) * eps * s * inv_r2 * (T(1) - T(2) * s);  // attractive when positive
+    T lj_scalar = T(24) * eps * s * inv_r2 * (T(1) - T(2) * s);  // attractive when positive
+    if (em) {
+        // energy-minimisation variant (LennardJonesInteractions.cuh:85-101): the
+        // scalar is bounded by +-1e20 in the reference's 1/24 J/mol/nm unit, then
+        // the pair force passes through ForceActivationFunction(force, 100)
+        // (EngineUtils.cuh:112-140): |F| -> A tanh(|F|/A), A = 1e3 * 1e3 * 100 in
+        // that unit; the 1e-8 guard of its division is in the same unit
+        const T A = T(24) * T(1e8);
+        lj_scalar = std::fmax(std::fmin(lj_scalar, T(24) * T(1e20)), -T(24) * T(1e20));
+        const T f = std::fabs(lj_scalar) * std::sqrt(r2);
+        lj_scalar *= A * std::tanh(f / A) / (f + T(24) * T(1e-8));
+    }
     o.e_lj = T(4) * eps * s * (s - T(1));
     T coul_scalar = T(0);  // multiplies (r_i - r_j)
     o.e_coul = T(0);
@@ -169,7 +180,7 @@ template <typename T>
 int64_t nonbonded_impl(int n, const double* pos, const double* box, const double* q,
                        const double* sigma, const double* eps, const int* eo, const int* ei,
                        double rc, int es_mode, double kappa, int nthreads, double* forces,
-                       double* energies, double* atom_energy = nullptr) {
+                       double* energies, double* atom_energy = nullptr, bool em = false) {
     CellGrid grid;
     grid.build(n, pos, box, rc);
     const T rcT = (T)rc;
@@ -205,7 +216,7 @@ int64_t nonbonded_impl(int n, const double* pos, const double* box, const double
             }
             const T sig = (si + (T)sigma[j]) * T(0.5);
             const T ep = std::sqrt(epi * (T)eps[j]);
-            PairOut<T> o = pair_interaction<T>(diff, r2, sig, ep, qi * (T)q[j], es_mode, (T)kappa, ke, pi_c);
+            PairOut<T> o = pair_interaction<T>(diff, r2, sig, ep, qi * (T)q[j], es_mode, (T)kappa, ke, pi_c, em);
             fi = fi + o.f_on_i;
             el += 0.5 * (double)o.e_lj;
             ec += 0.5 * (double)o.e_coul;
@@ -474,6 +485,14 @@ int64_t orc_nonbonded_atoms(int n, const double* pos, const double* box, const d
                             double* forces, double* energies, double* atom_energy) {
     return nonbonded_impl<double>(n, pos, box, q, sigma, eps, excl_off, excl_idx, rc, es_mode,
                                   kappa, nthreads, forces, energies, atom_energy);
+}
+
+int64_t orc_nonbonded_em(int n, const double* pos, const double* box, const double* q,
+                         const double* sigma, const double* eps, const int* excl_off,
+                         const int* excl_idx, double rc, int es_mode, double kappa, int nthreads,
+                         double* forces, double* energies) {
+    return nonbonded_impl<double>(n, pos, box, q, sigma, eps, excl_off, excl_idx, rc, es_mode,
+                                  kappa, nthreads, forces, energies, nullptr, true);
 }
 
 int64_t orc_pairset(int n, const double* pos, const double* box, const int* excl_off,

@@ -45,6 +45,16 @@ int64_t orc_nonbonded(int n, const double* pos, const double* box,
                       double rc, int es_mode, double kappa, int precision, int nthreads,
                       double* forces, double* energies);
 
+/* orc_nonbonded in FP64 with the energy-minimisation variant of the LJ pair
+ * force: bounded by +-1e20 and passed through the tanh activation with scale
+ * 100 (LennardJonesInteractions.cuh:85-101, EngineUtils.cuh:112-140); Coulomb
+ * and the energies are unchanged. */
+int64_t orc_nonbonded_em(int n, const double* pos, const double* box,
+                         const double* q, const double* sigma, const double* eps,
+                         const int* excl_off, const int* excl_idx,
+                         double rc, int es_mode, double kappa, int nthreads,
+                         double* forces, double* energies);
+
 /* orc_nonbonded in FP64 that also adds, per atom, half of the energy of each of
  * its pairs (LJ + Coulomb) to atom_energy[n]: the per-particle potential
  * energy the reference logs (LennardJonesInteractions.cuh:101, factor 0.5). */

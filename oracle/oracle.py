@@ -25,9 +25,9 @@ _i64 = ctypes.POINTER(ctypes.c_int64)
 
 
 def build(force: bool = False) -> str:
-    """Compile the oracle with its Makefile (g++ -O3 -fopenmp)."""
-    if force or not os.path.exists(_LIB_PATH):
-        subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    """Compile the oracle with its Makefile (g++ -O3 -fopenmp); make rebuilds it
+    when its sources are newer than the library."""
+    subprocess.run(["make", "-s", "-C", _HERE] + (["-B"] if force else []), check=True)
     return _LIB_PATH
 
 
@@ -42,6 +42,9 @@ def lib():
         L.orc_nonbonded.restype = ctypes.c_int64
         L.orc_nonbonded.argtypes = [ctypes.c_int, _d, _d, _d, _d, _d, _i, _i, ctypes.c_double,
                                     ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, _d, _d]
+        L.orc_nonbonded_em.restype = ctypes.c_int64
+        L.orc_nonbonded_em.argtypes = [ctypes.c_int, _d, _d, _d, _d, _d, _i, _i, ctypes.c_double,
+                                       ctypes.c_int, ctypes.c_double, ctypes.c_int, _d, _d]
         L.orc_pairset.restype = ctypes.c_int64
         L.orc_pairset.argtypes = [ctypes.c_int, _d, _d, _i, _i, ctypes.c_double, ctypes.c_double,
                                   ctypes.c_int64, _i32, _u8, _i64]
@@ -114,14 +117,20 @@ def exclusion_csr(n: int, pairs) -> tuple[np.ndarray, np.ndarray]:
 
 
 def nonbonded(pos, box, q, sigma, eps, excl_pairs, rc, es_mode, kappa=0.0, precision=64,
-              nthreads=0):
-    """Returns (forces (n,3), {'lj','coulomb','virial'}, n_pairs)."""
+              nthreads=0, em=False):
+    """Returns (forces (n,3), {'lj','coulomb','virial'}, n_pairs).  em: the
+    energy-minimisation variant of the LJ pair force (FP64 only)."""
     pos = _f64(pos).reshape(-1, 3)
     n = len(pos)
     off, idx = exclusion_csr(n, excl_pairs)
     f = np.zeros((n, 3))
     e = np.zeros(3)
     box = _f64(box)
+    if em:
+        npairs = lib().orc_nonbonded_em(n, _dp(pos), _dp(box), _dp(_f64(q)), _dp(_f64(sigma)),
+                                        _dp(_f64(eps)), _ip(off), _ip(idx), rc, es_mode, kappa, nthreads,
+                                        _dp(f), _dp(e))
+        return f, {"lj": e[0], "coulomb": e[1], "virial": e[2]}, int(npairs)
     npairs = lib().orc_nonbonded(n, _dp(pos), _dp(box), _dp(_f64(q)), _dp(_f64(sigma)), _dp(_f64(eps)),
                                  _ip(off), _ip(idx), rc, es_mode, kappa, precision, nthreads, _dp(f), _dp(e))
     return f, {"lj": e[0], "coulomb": e[1], "virial": e[2]}, int(npairs)
