@@ -188,6 +188,14 @@ LIMA_API int lima_set_pairbonds(lima_engine* h, int n, const int32_t* atoms2, co
 LIMA_API int lima_set_exclusions(lima_engine* h, int n, const int32_t* atoms2);
 /* Per-system PME grid; overrides lima_params.pme_grid / pme_spacing. */
 LIMA_API int lima_set_pme_grid(lima_engine* h, int nx, int ny, int nz);
+/* Uniform external electric field [V/nm] on the selected system (default 0):
+ * every atom feels q E (q [kC/mol] x E x 1000 = J/mol/nm), included in the forces
+ * that lima_get_forces and the log return, with no potential energy term.
+ * Replaces Box::uniformElectricField with SimParams::snf_select =
+ * HorizontalChargeField (code/LIMA_BASE/include/Bodies.cuh:363-385,
+ * code/LIMA_ENGINE/src/EngineKernels.cuh:321-343); the reference's other
+ * snf_select kernels (SupernaturalForces.cuh) have empty bodies. */
+LIMA_API int lima_set_electric_field(lima_engine* h, double ex, double ey, double ez);
 
 /* -------------------------------------------------------------------- state
  * pos [nm] x 3N (double), vel [nm/ns] x 3N (NULL = zero), for the selected system.

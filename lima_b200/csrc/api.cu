@@ -43,6 +43,7 @@ struct SystemHost {
     bool pme_set = false;
     std::vector<double> pos;
     std::vector<float> vel;
+    double efield[3] = {0.0, 0.0, 0.0};   // external field [V/nm]
 };
 
 struct CudaError {
@@ -361,6 +362,7 @@ void lima_engine::setup() {
     int col_cap = 64;
     double max_density = 0.0;
     pme_on = false;
+    bool has_field = false;
     self_energy.assign(ns, 0.0);
     for (int s = 0; s < ns; ++s) {
         const SystemHost& S = sys[s];
@@ -375,6 +377,8 @@ void lima_engine::setup() {
             D.boxf[d] = (float)S.box[d];
             D.inv_boxf[d] = (float)(1.0 / S.box[d]);
         }
+        for (int d = 0; d < 3; ++d) D.efield[d] = (float)(S.efield[d] * 1000.0);
+        if (S.efield[0] != 0.0 || S.efield[1] != 0.0 || S.efield[2] != 0.0) has_field = true;
         D.ncol_x = std::max(1, (int)std::floor(S.box[0] / a));
         D.ncol_y = std::max(1, (int)std::floor(S.box[1] / a));
         D.col_w[0] = (float)(S.box[0] / D.ncol_x);
@@ -579,6 +583,7 @@ void lima_engine::setup() {
 
     DevState D{};
     D.n_sys = ns;
+    D.has_field = has_field ? 1 : 0;
     D.n_atoms = N;
     D.n_clusters = n_clusters;
     D.n_slots = n_clusters * CLUSTER;
@@ -1106,7 +1111,7 @@ void lima_engine::capture_period() {
     CK(cudaStreamBeginCapture(s_main, cudaStreamCaptureModeThreadLocal));
     rebuild_async();
     for (int k = 0; k < p.nstlist; ++k) {
-        launch_zero_forces(st, s_main);
+        launches += launch_zero_forces(st, s_main);
         CK(cudaEventRecord(ev_fork, s_main));
         CK(cudaStreamWaitEvent(s_bonded, ev_fork, 0));
         CK(cudaStreamWaitEvent(s_pme, ev_fork, 0));
@@ -1141,7 +1146,7 @@ void lima_engine::forces(bool energy, bool atom_energy) {
         CK(cudaMemsetAsync(st.energy, 0, sizeof(long long) * E_COUNT * st.n_sys, s_main));
         if (st.atom_energy) CK(cudaMemsetAsync(st.epot, 0, sizeof(long long) * st.n_slots, s_main));
     }
-    launch_zero_forces(st, s_main);
+    launches += launch_zero_forces(st, s_main);
     // with phase timing on, every phase runs on the main stream so that each
     // phase's events bracket that phase alone
     cudaStream_t sb = phase_timing ? s_main : s_bonded;
@@ -1503,6 +1508,17 @@ int lima_set_exclusions(lima_engine* h, int n, const int32_t* a) {
     if (!h) return LIMA_ERR_INVALID_ARG;
     std::vector<float> unused;
     return set_terms(h, n, a, 2, nullptr, 0, h->sys[h->cur].excl, unused);
+}
+
+int lima_set_electric_field(lima_engine* h, double ex, double ey, double ez) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    if (!(std::isfinite(ex) && std::isfinite(ey) && std::isfinite(ez)))
+        return fail(h, LIMA_ERR_INVALID_ARG, "electric field must be finite");
+    SystemHost& S = h->sys[h->cur];
+    S.efield[0] = ex;
+    S.efield[1] = ey;
+    S.efield[2] = ez;
+    return topology_changed(h);
 }
 
 int lima_set_pme_grid(lima_engine* h, int nx, int ny, int nz) {

@@ -301,7 +301,30 @@ int launch_gather_forces(const DevState& st, double* f_out, cudaStream_t s) {
 }
 
 // fx, fy and fz are one block (fy = fx + n_slots, fz = fy + n_slots)
+// Force accumulators at the start of a force evaluation: the external field's
+// q E on every atom (EngineKernels.cuh:321-343: the field force joins the
+// step's force sum, without potential energy), zero on padding slots.
+__global__ void k_field_forces(DevState st) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= st.n_slots) return;
+    long long fx = 0, fy = 0, fz = 0;
+    if (st.orig[s] >= 0) {
+        const SysDesc& sd = st.sys[st.cluster_sys[s / CLUSTER]];
+        const float q = st.xyzq[s].w;
+        fx = to_fixed(q * sd.efield[0], FORCE_SCALE);
+        fy = to_fixed(q * sd.efield[1], FORCE_SCALE);
+        fz = to_fixed(q * sd.efield[2], FORCE_SCALE);
+    }
+    st.fx[s] = fx;
+    st.fy[s] = fy;
+    st.fz[s] = fz;
+}
+
 int launch_zero_forces(const DevState& st, cudaStream_t s) {
+    if (st.has_field) {
+        k_field_forces<<<(st.n_slots + 255) / 256, 256, 0, s>>>(st);
+        return 1;
+    }
     cudaMemsetAsync(st.fx, 0, 3 * (size_t)st.n_slots * sizeof(long long), s);
     return 0;  // a memset, not a kernel of this library
 }

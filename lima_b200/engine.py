@@ -32,7 +32,8 @@ EXPORTED = [
     "lima_default_params", "lima_error_string", "lima_last_error", "lima_version", "lima_create",
     "lima_create_batch", "lima_destroy", "lima_select_system", "lima_num_systems", "lima_set_box",
     "lima_set_atoms", "lima_set_bonds", "lima_set_angles", "lima_set_dihedrals", "lima_set_impropers",
-    "lima_set_pairbonds", "lima_set_exclusions", "lima_set_pme_grid", "lima_set_state",
+    "lima_set_pairbonds", "lima_set_exclusions", "lima_set_pme_grid", "lima_set_electric_field",
+    "lima_set_state",
     "lima_get_state", "lima_compute_forces", "lima_step", "lima_minimize", "lima_get_forces",
     "lima_get_energies", "lima_get_pairlist", "lima_get_status", "lima_clear_status",
     "lima_get_timings", "lima_reset_timings", "lima_enable_phase_timing", "lima_pme_recip_noalloc",
@@ -111,6 +112,7 @@ def load_library(path: str = LIB_PATH):
         "lima_set_pairbonds": (ctypes.c_int, [h, ctypes.c_int, i32p, f32p]),
         "lima_set_exclusions": (ctypes.c_int, [h, ctypes.c_int, i32p]),
         "lima_set_pme_grid": (ctypes.c_int, [h, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+        "lima_set_electric_field": (ctypes.c_int, [h, ctypes.c_double, ctypes.c_double, ctypes.c_double]),
         "lima_set_state": (ctypes.c_int, [h, f64p, f32p]),
         "lima_get_state": (ctypes.c_int, [h, f64p, f32p]),
         "lima_compute_forces": (ctypes.c_int, [h, ctypes.c_int]),
@@ -276,6 +278,10 @@ class Engine:
 
     def set_pme_grid(self, grid):
         self._check(self.lib.lima_set_pme_grid(self.h, int(grid[0]), int(grid[1]), int(grid[2])))
+
+    def set_electric_field(self, field):
+        """Uniform external electric field [V/nm] on the selected system."""
+        self._check(self.lib.lima_set_electric_field(self.h, float(field[0]), float(field[1]), float(field[2])))
 
     def set_state(self, pos, vel=None):
         p = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
