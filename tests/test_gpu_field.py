@@ -1,4 +1,5 @@
-"""Uniform external electric field through the C-ABI.
+"""The reference's dynamics known-answer tests through the C-ABI: a uniform
+external electric field, and a single bond's oscillation frequency.
 
 The reference's known-answer test (ForceCorrectness.h:621-669,
 VerletintegrationTesting::TestIntegration): one charged particle in a field of
@@ -64,3 +65,32 @@ def test_field_adds_qE_and_no_energy():
     e.set_electric_field((0.0, 0.0, 0.0))
     e.compute_forces(energy=True)
     assert np.array_equal(e.forces(), f0)
+
+
+@pytest.mark.parametrize("integrator", [E.LEAPFROG, E.VELOCITY_VERLET])
+def test_bond_oscillation_frequency(integrator):
+    """The reference's known-answer test ForceCorrectness.h:169-230 through the
+    engine: a stretched bond between masses 12 and 16 g/mol oscillates at
+    sqrt(k / mu) within 1 %."""
+    import math
+    m = np.array([12e-3, 16e-3], np.float32)
+    kb, b0 = 2.5e8, 0.12
+    mu = float(m[0]) * float(m[1]) / float(m.sum())
+    period = 2 * math.pi * math.sqrt(mu / kb)      # [ns]
+    dt = period / 400
+    s = systems.System(box=np.array([3.0] * 3), pos=np.array([[1.0, 1.0, 1.0], [1.0 + b0 + 0.004, 1.0, 1.0]]),
+                       vel=np.zeros((2, 3), np.float32), charge=np.zeros(2, np.float32), mass=m,
+                       sigma=np.zeros(2, np.float32), epsilon=np.zeros(2, np.float32),
+                       bonds=np.array([[0, 1]], np.int32), bond_par=np.array([[b0, kb]], np.float32), name="bond")
+    e = Engine(cutoff=1.0, electrostatics=E.ES_NONE, dt=dt, integrator=integrator)
+    e.load(s)
+    xs = []
+    for _ in range(3000):
+        e.step(1)
+        p, _ = e.state()
+        xs.append(np.linalg.norm(p[1] - p[0]) - b0)
+    xs = np.array(xs)
+    crossings = np.where((xs[:-1] > 0) & (xs[1:] <= 0))[0]
+    measured = np.mean(np.diff(crossings)) * dt
+    assert len(crossings) >= 5
+    assert abs(measured - period) / period < 0.01, (measured, period)
