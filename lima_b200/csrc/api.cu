@@ -70,6 +70,7 @@ struct lima_engine {
     int cur = 0;
     std::string err;
     bool built = false;
+    bool device_ok = false;   // set-up selected p.device successfully: calls select it again
     bool state_pending = false;
     int list_age = 1 << 30;
     int64_t step = 0;
@@ -263,6 +264,9 @@ int fail(lima_engine* h, int code, const std::string& msg) {
 template <typename F>
 int guarded(lima_engine* h, F&& fn) {
     if (!h) return LIMA_ERR_INVALID_ARG;
+    // the current device is per host thread: a process may drive engines on
+    // several devices, so every call works on its own engine's device
+    if (h->device_ok) cudaSetDevice(h->p.device);
     try {
         return fn();
     } catch (const CudaError& e) {
@@ -319,6 +323,7 @@ void lima_engine::setup() {
     if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0)
         throw ApiError{LIMA_ERR_NO_DEVICE, "no CUDA device available"};
     CK(cudaSetDevice(p.device));
+    device_ok = true;
     cudaDeviceProp prop;
     CK(cudaGetDeviceProperties(&prop, p.device));
     if (prop.major < 10) throw ApiError{LIMA_ERR_NO_DEVICE, "this build targets sm_100a (B200)"};
@@ -1405,6 +1410,7 @@ int lima_create(const lima_params* p, lima_engine** out) { return lima_create_ba
 
 int lima_destroy(lima_engine* h) {
     if (!h) return LIMA_ERR_INVALID_ARG;
+    if (h->device_ok) cudaSetDevice(h->p.device);
     delete h;
     return LIMA_OK;
 }
@@ -1440,6 +1446,7 @@ static void pull_device_state(lima_engine* h) {
 }
 
 static int topology_changed(lima_engine* h) {
+    if (h->device_ok) cudaSetDevice(h->p.device);
     if (h->built) {
         // keep the current state; the topology call itself reports no CUDA error
         try {

@@ -4,9 +4,21 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
 #include "common.cuh"
 
 namespace lima {
+
+// Kernel attributes (the dynamic shared-memory limit) belong to one device's
+// context.  True the first time it is called for the current device with this
+// flag set (bit d for device d), so that each device sets them once.
+inline bool first_on_device(std::atomic<unsigned long long>& done) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const unsigned long long bit = 1ull << (dev & 63);
+    return (done.fetch_or(bit) & bit) == 0ull;
+}
 
 // Every device pointer the per-step kernels touch; passed to kernels by value.
 struct DevState {

@@ -902,25 +902,30 @@ void set_pme_sys_twiddles(void* dst, int offx, int offy, int offz) {
     d->pz.tw_off = offz;
 }
 
-// The attribute is per kernel and process-wide: it only ever grows, so an
-// engine with small grids cannot shrink the room another engine relies on.
+// The attribute belongs to the kernel on one device and is shared by every
+// engine on that device: it only ever grows there, so an engine with small grids
+// cannot shrink the room another engine relies on.
 void pme_set_smem_limits(int maxn, int xy_buf) {
-    static bool spread_attr = false;
-    if (!spread_attr) {
+    static std::mutex mu;
+    static int largest_xy[64] = {}, largest[64] = {};
+    static bool spread_attr[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    dev &= 63;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!spread_attr[dev]) {
         cudaFuncSetAttribute(k_spread_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              PME_SPREAD_MAX_BOX * (int)sizeof(int));
-        spread_attr = true;
+        spread_attr[dev] = true;
     }
-    static int largest_xy = 0;
-    if (xy_buf > largest_xy) {
-        largest_xy = xy_buf;
+    if (xy_buf > largest_xy[dev]) {
+        largest_xy[dev] = xy_buf;
         const int b = (int)((size_t)(2 * FFT_MAXN + 2 * xy_buf) * sizeof(float2));
         cudaFuncSetAttribute(k_fft_xy_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
         cudaFuncSetAttribute(k_fft_xy_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
     }
-    static int largest = 0;
-    if (maxn <= largest) return;
-    largest = maxn;
+    if (maxn <= largest[dev]) return;
+    largest[dev] = maxn;
     const int by = (int)fft_smem_bytes(FFT_TX, maxn), bx = (int)fft_smem_bytes(FFT_XLINES, maxn);
     cudaFuncSetAttribute(k_fft_y, cudaFuncAttributeMaxDynamicSharedMemorySize, by);
     cudaFuncSetAttribute(k_fft_z_conv, cudaFuncAttributeMaxDynamicSharedMemorySize, by);
