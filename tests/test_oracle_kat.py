@@ -292,3 +292,28 @@ def test_em_step_reduces_energy(oracle):
         oracle.em_step(pos, f, adam, k)
     e1 = oracle.bonded(pos, None, bonds=[[0, 1]], bond_par=[[0.1, 3e8]])[1]["bond"]
     assert e1 < 0.05 * e0, (e0, e1)
+
+
+def test_em_lj_pair_bound_kat(oracle):
+    """LennardJonesInteractions.cuh:85-101 with EngineUtils.cuh:112-140: in the
+    energy-minimisation variant an LJ pair force F becomes F tanh(|F|/A) A/|F|,
+    A = 1e3 * 1e3 * 100 in the reference's 1/24 J/mol/nm unit (2.4e9 J/mol/nm);
+    Coulomb is not bounded."""
+    sig, eps = 0.3, 500.0
+    for r in (0.145, 0.2, 0.35):
+        pos = np.array([[1.0, 1.0, 1.0], [1.0 + r, 1.0, 1.0]])
+        q = np.array([0.0, 0.0])
+        args = (pos, np.array([3.0] * 3), q, [sig] * 2, [eps] * 2, np.zeros((0, 2), np.int32), 1.0, 1)
+        f_em = oracle.nonbonded(*args, em=True)[0]
+        f = oracle.nonbonded(*args)[0]
+        s6 = (sig / r) ** 6
+        mag = abs(24 * eps * s6 * (2 * s6 - 1) / r)          # |F| [J/mol/nm]
+        assert abs(np.linalg.norm(f[0]) - mag) / mag < 1e-12
+        A = 24 * 1e3 * 1e3 * 100
+        want = A * math.tanh(mag / A) / (mag + 24e-8) * mag
+        assert abs(np.linalg.norm(f_em[0]) - want) / want < 1e-12, (r, np.linalg.norm(f_em[0]), want)
+        assert np.allclose(f_em[0], -f_em[1], rtol=1e-14, atol=0)
+    # charges: the Coulomb part is the same with and without the bound
+    pos = np.array([[1.0, 1.0, 1.0], [1.4, 1.0, 1.0]])
+    args = (pos, np.array([3.0] * 3), np.array([E, -E]), [0.0, 0.0], [0.0, 0.0], np.zeros((0, 2), np.int32), 1.0, 1)
+    assert np.array_equal(oracle.nonbonded(*args, em=True)[0], oracle.nonbonded(*args)[0])
