@@ -48,6 +48,8 @@ def test_default_params_and_errors_without_device():
     assert lib.lima_set_box(h, -1.0, 1.0, 1.0) == 1
     assert lib.lima_select_system(h, 3) == 1
     assert lib.lima_step(h, -1) == 1
+    assert lib.lima_set_electric_field(h, float("nan"), 0.0, 0.0) == 1
+    assert lib.lima_set_electric_field(h, 0.5, 0.0, 0.0) == 0
     bad = E.default_params(dt=0.0)
     h2 = ctypes.c_void_p()
     assert lib.lima_create(ctypes.byref(bad), ctypes.byref(h2)) == 1
