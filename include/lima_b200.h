@@ -119,6 +119,11 @@ typedef struct lima_params {
        position, the energy and force evaluated at the old one, the updated speed */
     int    log_interval;
     int    log_ring;          /* frames held on the device (default 5, as the reference) */
+    /* boundary condition (BoundaryConditionSelect, code/LIMA_BASE/include/Simulation.cuh:13;
+       BoundaryCondition.cuh): 1 = periodic (PBC, default); 0 = none (NoBC): no images,
+       no wrapping of positions, plain differences in every term; the box only sets the
+       column grid (atoms outside it are binned at its edge); needs cutoff Coulomb or none */
+    int    periodic;
 } lima_params;
 
 typedef struct lima_energies {

@@ -403,10 +403,12 @@ void lima_engine::setup() {
                 for (int d = 0; d < 2; ++d) {
                     const double L = S.box[d];
                     double x = S.pos[3 * (size_t)a + d];
-                    x -= L * std::floor(x / L);
-                    if (!(x < L)) x -= L;
-                    if (!(x >= 0.0)) x = 0.0;
-                    c[d] = std::min(std::max((int)(x * nc[d] / L), 0), nc[d] - 1);
+                    if (p.periodic) {
+                        x -= L * std::floor(x / L);
+                        if (!(x < L)) x -= L;
+                        if (!(x >= 0.0)) x = 0.0;
+                    }
+                    c[d] = (int)std::fmin(std::fmax(x * nc[d] / L, 0.0), (double)(nc[d] - 1));
                 }
                 ++cc[c[0] + D.ncol_x * c[1]];
             }
@@ -589,6 +591,7 @@ void lima_engine::setup() {
     DevState D{};
     D.n_sys = ns;
     D.has_field = has_field ? 1 : 0;
+    D.periodic = p.periodic ? 1 : 0;
     D.n_atoms = N;
     D.n_clusters = n_clusters;
     D.n_slots = n_clusters * CLUSTER;
@@ -1372,6 +1375,7 @@ void lima_default_params(lima_params* p) {
     p->target_temperature = 310.0;  // Thermostat.cuh:56
     p->log_interval = 0;
     p->log_ring = 5;                // DatabuffersDeviceController::nStepsInBuffer
+    p->periodic = 1;                // BoundaryConditionSelect::PBC
 }
 
 const char* lima_error_string(int code) {
@@ -1398,6 +1402,8 @@ int lima_create_batch(const lima_params* p, int n_systems, lima_engine** out) {
     if (!(p->dt > 0.0) || !(p->cutoff > 0.0) || p->nstlist < 1) return LIMA_ERR_INVALID_ARG;
     if (p->electrostatics < LIMA_ES_NONE || p->electrostatics > LIMA_ES_EWALD) return LIMA_ERR_INVALID_ARG;
     if (p->integrator != LIMA_INTEGRATOR_LEAPFROG && p->integrator != LIMA_INTEGRATOR_VV) return LIMA_ERR_INVALID_ARG;
+    if (p->periodic != 0 && p->periodic != 1) return LIMA_ERR_INVALID_ARG;
+    if (!p->periodic && p->electrostatics == LIMA_ES_EWALD) return LIMA_ERR_INVALID_ARG;   // Ewald needs images
     lima_engine* h = new (std::nothrow) lima_engine();
     if (!h) return LIMA_ERR_INVALID_ARG;
     h->p = *p;

@@ -32,12 +32,14 @@ __device__ __forceinline__ f3 unit(f3 a) {
     return l > 0.f ? a * (1.f / l) : f3{0.f, 0.f, 0.f};
 }
 
-// position of atom a relative to atom a0 (minimum image, FP64 difference)
+// position of atom a relative to atom a0 (FP64 difference; minimum image in a periodic box)
 __device__ __forceinline__ f3 rel(const DevState& st, const SysDesc& sd, int s0, int a) {
     const int s = st.slot_of[a];
     double d[3] = {st.px[s] - st.px[s0], st.py[s] - st.py[s0], st.pz[s] - st.pz[s0]};
+    if (st.periodic) {
 #pragma unroll
-    for (int k = 0; k < 3; ++k) d[k] -= sd.box[k] * rint(d[k] / sd.box[k]);
+        for (int k = 0; k < 3; ++k) d[k] -= sd.box[k] * rint(d[k] / sd.box[k]);
+    }
     return {(float)d[0], (float)d[1], (float)d[2]};
 }
 

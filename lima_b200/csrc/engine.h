@@ -30,6 +30,7 @@ struct DevState {
     int pl_cap = 0;           // pair-list rows per i-cluster
     int atom_energy = 0;      // energy evaluations also add per-atom shares to epot (log frames)
     int has_field = 0;        // some system has an external field: forces start from q E, not zero
+    int periodic = 1;         // 0: no boundary condition (no images, no wrapping, plain differences)
     int col_cap = 0;          // atoms a column may hold
 
     SysDesc* sys = nullptr;

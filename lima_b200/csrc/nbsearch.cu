@@ -59,17 +59,20 @@ __global__ void k_bin(DevState st, int from_input) {
             p[2] = st.pz[s];
         }
         for (int d = 0; d < 3; ++d) {
-            const double L = sd.box[d];
-            double x = p[d] - L * floor(p[d] / L);
-            if (x >= L) x -= L;
-            if (x < 0.0) x = 0.0;
+            double x = p[d];
+            if (st.periodic) {   // wrapped into the box; without a boundary condition kept as is
+                const double L = sd.box[d];
+                x -= L * floor(x / L);
+                if (x >= L) x -= L;
+                if (x < 0.0) x = 0.0;
+            }
             p[d] = x;
             st.in_pos[3 * a + d] = x;
         }
-        int cx = (int)(p[0] * sd.ncol_x / sd.box[0]);
-        int cy = (int)(p[1] * sd.ncol_y / sd.box[1]);
-        cx = min(max(cx, 0), sd.ncol_x - 1);
-        cy = min(max(cy, 0), sd.ncol_y - 1);
+        // column of the position; one outside the box (no boundary condition) is
+        // binned at the box's edge
+        const int cx = (int)fmin(fmax(p[0] * sd.ncol_x / sd.box[0], 0.0), (double)(sd.ncol_x - 1));
+        const int cy = (int)fmin(fmax(p[1] * sd.ncol_y / sd.box[1], 0.0), (double)(sd.ncol_y - 1));
         col = sd.col_off + cx + sd.ncol_x * cy;
         st.col_of_atom[a] = col;
         st.z_of_atom[a] = (float)p[2];
@@ -159,7 +162,10 @@ __global__ void k_sort_columns(DevState st, const int* col_sys) {
         unsigned long long k = ~0ull;
         if (i < n) {
             const int a = st.col_list[off + i];
-            k = ((unsigned long long)__float_as_uint(st.z_of_atom[a]) << 32) | (unsigned)a;
+            // z bits made order-preserving for negative z too (no boundary condition)
+            unsigned z = __float_as_uint(st.z_of_atom[a]);
+            z ^= (z >> 31) ? 0xffffffffu : 0x80000000u;
+            k = ((unsigned long long)z << 32) | (unsigned)a;
         }
         keys[i] = k;
     }
@@ -358,6 +364,16 @@ __global__ void __launch_bounds__(PS_WARPS * 32, 1) k_pairsearch(DevState st, fl
         ny = sd.ncol_y;
         fixed_xy = false;
     }
+    if (!st.periodic) {
+        // no images: the columns the extent reaches, clamped to the grid (atoms
+        // outside the box are binned in its edge columns), each met once unshifted
+        auto col_of = [](float v, int n) { return (int)fminf(fmaxf(v, 0.f), (float)(n - 1)); };
+        cx0 = col_of(floorf((ilo.x - R) / sd.col_w[0]), sd.ncol_x);
+        nx = col_of(floorf((ihi.x + R) / sd.col_w[0]), sd.ncol_x) - cx0 + 1;
+        cy0 = col_of(floorf((ilo.y - R) / sd.col_w[1]), sd.ncol_y);
+        ny = col_of(floorf((ihi.y + R) / sd.col_w[1]), sd.ncol_y) - cy0 + 1;
+        fixed_xy = true;
+    }
 
     const int cap = st.pl_cap;
     int count = 0;
@@ -509,6 +525,7 @@ __global__ void __launch_bounds__(PS_WARPS * 32, 1) k_pairsearch(DevState st, fl
                     }
                 }
             }
+            if (!st.periodic) shifts &= 1u << 13;   // the unshifted image only
             // append (cluster, shift) candidates in lane order, then shift order
             const int c = __popc(shifts);
             int inc2 = c;
