@@ -68,3 +68,27 @@ def test_no_silent_fallback_without_gpu():
     with pytest.raises(LimaError) as ex:
         e.compute_forces()
     assert ex.value.code == 6
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """The ctypes mirrors of lima_params, lima_energies and lima_timings have the
+    header's sizes and field offsets (a C program compiled against the header
+    prints them)."""
+    from lima_b200 import engine as E
+    structs = {"lima_params": E.Params, "lima_energies": E.Energies, "lima_timings": E.Timings}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "lima_b200.h"', 'int main(void) {']
+    for cname, py in structs.items():
+        lines.append(f'    printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'    printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ['    return 0;', '}']
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l}
+    for cname, py in structs.items():
+        assert got[(cname, "size")] == ctypes.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
