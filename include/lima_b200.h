@@ -244,10 +244,11 @@ LIMA_API int lima_enable_phase_timing(lima_engine* h, int enable);
 
 /* ------------------------------------------------ allocation-free PME stage
  * No counterpart in the reference: this entry point exists for callers that
- * may not allocate device memory (work recorded while a stream is captured
- * into a CUDA graph, a plug-in inside an application that owns every device
- * allocation through its own pool, a real-time loop that must not allocate
- * after start-up).  It computes the smooth-PME reciprocal forces and energy of
+ * may not allocate device memory: a plug-in inside an application that owns
+ * every device allocation through its own pool (a cudaMalloc of its own would
+ * bypass the host's accounting and can fail or fragment the pool), or a
+ * real-time loop that must not allocate after start-up (cudaMalloc may
+ * synchronise the device and take unbounded time).  It computes the smooth-PME reciprocal forces and energy of
  * one set of charges with the engine's own PME kernels (accurate conventions:
  * B-spline moduli, analytic gather), using a static scratch array instead of
  * allocated grids; it calls no allocator.
@@ -260,8 +261,9 @@ LIMA_API int lima_enable_phase_timing(lima_engine* h, int enable);
  * grids return LIMA_ERR_OVERFLOW; dimensions must factor into 2, 3 and 5
  * (LIMA_ERR_UNSUPPORTED otherwise).  Every GPU that loads the library holds
  * about 5 MB of static device memory for it until the process exits.  The first
- * call on a device looks up the scratch array's device address; make that
- * first call before any stream capture.  All calls share the array and it
+ * call on a device looks up the scratch array's device address (and looks it up
+ * again whenever the device's context has changed, e.g. after cudaDeviceReset);
+ * make that first call before any stream capture.  All calls share the array and it
  * keeps the last call's contents (each call clears what must start at zero):
  * calls that overlap on the GPU race. */
 LIMA_API int lima_pme_recip_noalloc(const float* d_xyzq, int n_atoms, double lx, double ly, double lz,

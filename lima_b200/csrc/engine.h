@@ -5,19 +5,28 @@
 #include <stdint.h>
 
 #include <atomic>
+#include <mutex>
 
 #include "common.cuh"
 
 namespace lima {
 
 // Kernel attributes (the dynamic shared-memory limit) belong to one device's
-// context.  True the first time it is called for the current device with this
-// flag set (bit d for device d), so that each device sets them once.
-inline bool first_on_device(std::atomic<unsigned long long>& done) {
+// context.  Runs set_attributes once per device (bit d of `done` for device d):
+// under a lock, and the bit is published only after set_attributes returns, so
+// a second host thread driving another engine on the same device never
+// launches before the attributes are in place.
+template <class F>
+inline void once_per_device(std::atomic<unsigned long long>& done, F&& set_attributes) {
     int dev = 0;
     cudaGetDevice(&dev);
     const unsigned long long bit = 1ull << (dev & 63);
-    return (done.fetch_or(bit) & bit) == 0ull;
+    if (done.load(std::memory_order_acquire) & bit) return;
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    if (done.load(std::memory_order_relaxed) & bit) return;
+    set_attributes();
+    done.fetch_or(bit, std::memory_order_release);
 }
 
 // Every device pointer the per-step kernels touch; passed to kernels by value.

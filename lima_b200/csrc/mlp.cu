@@ -627,7 +627,9 @@ void mlp_sync_bf16(MlpModel& m, cudaStream_t s) {
 int mlp_infer(const MlpModel& m, int rows, const float* feat, const float* mean, const float* inv_std, float* Y,
               cudaStream_t s) {
     static std::atomic<unsigned long long> attr_set{0ull};
-    if (first_on_device(attr_set)) cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)INF_SMEM);
+    once_per_device(attr_set, [] {
+        cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)INF_SMEM);
+    });
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -641,7 +643,9 @@ int mlp_infer(const MlpModel& m, int rows, const float* feat, const float* mean,
 int mlp_infer_tc(const MlpModel& m, int rows, const float* feat, const float* mean, const float* inv_std, float* Y,
                  int* err, cudaStream_t s) {
     static std::atomic<unsigned long long> attr_set{0ull};
-    if (first_on_device(attr_set)) cudaFuncSetAttribute(k_mlp_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM);
+    once_per_device(attr_set, [] {
+        cudaFuncSetAttribute(k_mlp_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM);
+    });
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

@@ -583,9 +583,10 @@ int launch_rebuild_slots(const DevState& st, bool from_input, cudaStream_t s) {
     int m = 1;
     while (m < st.col_cap) m <<= 1;
     static std::atomic<unsigned long long> sort_attr{0ull};
-    if (first_on_device(sort_attr))
+    once_per_device(sort_attr, [] {
         cudaFuncSetAttribute(k_sort_columns, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              8192 * (int)sizeof(unsigned long long));
+    });
     k_sort_columns<<<st.n_cols, 128, (size_t)m * sizeof(unsigned long long), s>>>(st, st.col_sys);
     k_gather_slots<<<(st.n_slots + TB - 1) / TB, TB, 0, s>>>(st, from_input ? 1 : 0);
     k_finish_slots<<<(st.n_slots + TB - 1) / TB, TB, 0, s>>>(st);

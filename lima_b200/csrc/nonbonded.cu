@@ -340,10 +340,10 @@ static void launch_nb_shape(const DevState& st, const NbParams& p, bool energy, 
     // each), leaving room for a charge-spreading CTA beside them
     const int reserve = (shape & 1) ? ((shape & 2) ? 28 * 1024 : 60 * 1024) : 0;
     static std::atomic<unsigned long long> attr{0ull};
-    if (first_on_device(attr)) {
+    once_per_device(attr, [] {
         cudaFuncSetAttribute(k_nonbonded<ES, 0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 90 * 1024);
         cudaFuncSetAttribute(k_nonbonded<ES, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 90 * 1024);
-    }
+    });
     if (shape & 4) k_nonbonded<ES, 0, true><<<grid, tb, reserve, s>>>(st, p);
     else k_nonbonded<ES, 0, false><<<grid, tb, reserve, s>>>(st, p);
 }

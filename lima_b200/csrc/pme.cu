@@ -940,10 +940,10 @@ namespace lima {
 // ===================================================================== no-alloc
 // Reciprocal-space PME for callers that cannot allocate device memory.
 //
-// Some callers of this library may not call cudaMalloc: code running while a
-// stream is being captured into a CUDA graph, a plug-in inside an application
-// that owns every device allocation through its own pool, or a real-time loop
-// that must not allocate after start-up.  For them lima_pme_recip_noalloc
+// Some callers of this library may not call cudaMalloc: a plug-in inside an
+// application that owns every device allocation through its own pool (its own
+// cudaMalloc would bypass the host's accounting), or a real-time loop that must
+// not allocate after start-up (cudaMalloc may synchronise the device).  For them lima_pme_recip_noalloc
 // computes the same reciprocal-space forces and energy as the engine's PME
 // stage, using the static scratch array below instead of allocated grids.
 //
@@ -1228,6 +1228,37 @@ __global__ void k_na_finish(unsigned char* scratch, double* energy) {
 namespace {
 std::mutex g_noalloc_mutex;
 void* g_noalloc_ptr[64] = {};
+unsigned long long g_noalloc_ctx[64] = {};   // context id the cached address belongs to
+
+// Unique id of the calling thread's current context (0 if the driver cannot
+// tell).  The static array's address belongs to one context: after a
+// cudaDeviceReset the runtime loads the module into a new context, so the
+// cached address is refreshed whenever this id changes.  The driver entry
+// points are fetched through the runtime, so the library needs no link
+// against libcuda.
+unsigned long long current_context_id() {
+    using GetCurrent = int (*)(void**);
+    using GetId = int (*)(void*, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static bool looked_up = false;
+    if (!looked_up) {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<GetCurrent>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<GetId>(f);
+        looked_up = true;
+    }
+    void* ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_current && get_id && get_current(&ctx) == 0 && ctx && get_id(ctx, &id) == 0) return id;
+    return 0;
+}
 }  // namespace
 
 }  // namespace lima
@@ -1258,12 +1289,17 @@ extern "C" int lima_pme_recip_noalloc(const float* d_xyzq, int n_atoms, double l
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return LIMA_ERR_NO_DEVICE;
     void* scratch = nullptr;
     {
-        // set-up once per device: the device address of the static array
+        // set-up once per device (and again if the device's context changed):
+        // the device address of the static array
         std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-        if (!g_noalloc_ptr[dev]) {
+        // (no context yet reads as id 0; the lookup below creates the primary
+        // context, and the next call refreshes the cache once under its id)
+        const unsigned long long ctx = current_context_id();
+        if (!g_noalloc_ptr[dev] || ctx != g_noalloc_ctx[dev]) {
             void* ptr = nullptr;
             if (cudaGetSymbolAddress(&ptr, g_pme_noalloc_scratch) != cudaSuccess || !ptr) return LIMA_ERR_CUDA;
             g_noalloc_ptr[dev] = ptr;
+            g_noalloc_ctx[dev] = ctx;
         }
         scratch = g_noalloc_ptr[dev];
     }
