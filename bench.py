@@ -18,6 +18,7 @@ PME a distributed FFT), value = the sum of all ranks' ns/day over the max time.
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import math
 import os
@@ -105,13 +106,111 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_step_time(system, n_steps: int, threads: int):
+class NvmlSampler:
+    """SM clock and throttle reasons polled through NVML every ~1 ms on a
+    thread, so that even a timed region of a few milliseconds holds samples.
+    Falls back to the nvidia-smi sampler when NVML is not available."""
+
+    # clocks-event reason bits (nvml.h: nvmlClocksEventReason*)
+    REASONS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+               "hw_thermal_slowdown": 0x40}
+
+    def __init__(self, device: int, period_s: float = 0.001):
+        self.device = device
+        self.period = period_s
+        self.samples = []
+        self.fallback = None
+        self.nv = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(device)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
+        except Exception:
+            self.nv = None
+            self.fallback = ClockSampler(device)
+
+    def _run(self):
+        nv = self.nv
+        while not self.stop_flag.is_set():
+            try:
+                mhz = float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                try:
+                    rs = int(nv.nvmlDeviceGetCurrentClocksEventReasons(self.h))
+                except Exception:
+                    rs = int(nv.nvmlDeviceGetCurrentClocksThrottleReasons(self.h))
+                self.samples.append((mhz, rs))
+            except Exception:
+                pass
+            time.sleep(self.period)
+
+    def start(self):
+        if self.fallback is not None:
+            return self.fallback.start()
+        self.stop_flag = threading.Event()
+        self.t = threading.Thread(target=self._run, daemon=True)
+        self.t.start()
+
+    def stop(self):
+        if self.fallback is not None:
+            return self.fallback.stop()
+        self.stop_flag.set()
+        self.t.join(timeout=5)
+        sm = [m for m, _ in self.samples]
+        reasons = sorted(k for k, b in self.REASONS.items() if any(r & b for _, r in self.samples))
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz,
+                "reasons": reasons, "samples": len(sm), "source": "NVML, ~1 ms polling"}
+
+
+def headline_config(n_atoms: int, world: int) -> dict:
+    """The workload's description, identical in both arms' JSON lines."""
+    return {"workload": WORKLOAD, "atoms": n_atoms, "pme_grid": list(GRID), "cutoff_nm": CUTOFF, "nstlist": PERIOD,
+            "dt_fs": 1.0, "integrator": "leapfrog", "parallelism": "replicas" if world > 1 else "single",
+            "l2": "flushed (256 MiB write) before every timed iteration; an iteration is one pair-list "
+                  "period: list rebuild + 10 steps, energies evaluated on the last step",
+            "accumulation": "int64 fixed point forces/energies, FP64 positions"}
+
+
+def stage_rooflines(ph: dict, s, n_rows: int, hbm_gbs: float) -> dict:
+    """Algorithmic bytes per stage (per-unit figures in DESIGN.md section 3) over
+    the stage's event-timed average duration, against the measured HBM copy
+    bandwidth.  ph: per-phase microseconds (phases serialised)."""
+    n = s.n
+    pts = GRID[0] * GRID[1] * GRID[2]
+    half = (GRID[0] // 2 + 1) * GRID[1] * GRID[2]
+    ex = s.exclusions()
+    nx = int(((s.charge[ex[:, 0]] != 0) & (s.charge[ex[:, 1]] != 0)).sum())
+    work = {
+        "integrate": (108 * n, "108 B/atom"),
+        "bonded": (96 * len(s.bonds) + 144 * len(s.angles) + 192 * len(s.dihedrals) + 112 * nx,
+                   "96 B/bond + 144 B/angle + 192 B/dihedral + 112 B/excluded charged pair (Ewald correction)"),
+        "pme": (16 * n + 4 * pts + 2 * 16 * pts + 20 * half + 40 * n,
+                "spread 16 B/atom + 4 B/grid point, two 3-D FFTs 16 B/point each, convolution 20 B/half-complex "
+                "point, gather 40 B/atom"),
+        "nblist": (40 * n + 8 * n_rows, "40 B/atom + 8 B per pair-list row written (per rebuild)"),
+    }
+    out = {}
+    for k, (b, rule) in work.items():
+        us = ph.get(k)
+        if not us:
+            continue
+        gbs = b / (us * 1e-6) / 1e9
+        out[k] = {"us": us, "bytes": b, "achieved_gbs": gbs, "peak_gbs": hbm_gbs, "frac": gbs / hbm_gbs,
+                  "rule": rule}
+    if ph.get("pme"):
+        out["pme"]["grid_points_per_s"] = pts / (ph["pme"] * 1e-6)
+    return out
+
+
+def cpu_step_time(system, n_steps: int, threads: int, cutoff: float = CUTOFF, grid=GRID, es_mode: int = 2):
     """The CPU oracle port of the same step (FP32 reference-faithful pair loop with
-    all host threads, FP64 SPME and bonded terms, leapfrog), seconds per step."""
+    all host threads, FP64 SPME and bonded terms, leapfrog), seconds per step.
+    es_mode 1 (cutoff Coulomb) runs without PME."""
     from oracle import oracle as O
     from lima_b200.systems import ewald_kappa
     O.build()
-    kappa = ewald_kappa(CUTOFF, 1e-5)
+    kappa = ewald_kappa(cutoff, 1e-5) if es_mode == 2 else 0.0
     s = system
     ex = s.exclusions()
     xp = ex[(s.charge[ex[:, 0]] != 0) & (s.charge[ex[:, 1]] != 0)]
@@ -122,12 +221,15 @@ def cpu_step_time(system, n_steps: int, threads: int):
     times = []
     for k in range(n_steps + 1):
         t0 = time.perf_counter()
-        f, _, _ = O.nonbonded(pos, s.box, s.charge, s.sigma, s.epsilon, ex, CUTOFF, 2, kappa, precision=32,
+        f, _, _ = O.nonbonded(pos, s.box, s.charge, s.sigma, s.epsilon, ex, cutoff, es_mode, kappa, precision=32,
                               nthreads=threads)
-        fl, _, _ = O.pme(pos, s.charge, s.box, GRID, kappa)
-        fx, _ = O.exclusion_correction(pos, s.charge, s.box, xp, kappa)
-        fb, _ = O.bonded(pos, s.box, s.bonds, s.bond_par, s.angles, s.angle_par)
-        O.integrate(pos, vel, fprev, f + fl + fx + fb, m, DT_NS, 0)
+        if es_mode == 2:
+            fl, _, _ = O.pme(pos, s.charge, s.box, grid, kappa)
+            fx, _ = O.exclusion_correction(pos, s.charge, s.box, xp, kappa)
+            f = f + fl + fx
+        fb, _ = O.bonded(pos, s.box, s.bonds, s.bond_par, s.angles, s.angle_par, s.dihedrals, s.dihedral_par,
+                         s.impropers, s.improper_par, s.pairbonds, s.pair_par)
+        O.integrate(pos, vel, fprev, f + fb, m, DT_NS, 0)
         if k > 0:                      # first step is warm-up
             times.append(time.perf_counter() - t0)
     return statistics.median(times)
@@ -147,8 +249,7 @@ def run_reference(args):
         "impl": "reference", "metric": "ns_per_day", "value": v, "unit": "ns/day", "n_gpus": args.gpus,
         "steps": n, "warmup": 1, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "atoms": s.n, "pme_grid": list(GRID), "cutoff_nm": CUTOFF,
-                   "nstlist": 10, "dt_fs": 1.0, "parallelism": "replicas"},
+        "config": headline_config(s.n, int(os.environ.get("WORLD_SIZE", "1"))),
         "cpu_baseline": {"value": v, "unit": "ns/day", "cores": threads, "kind": "port",
                          "sample": f"{n} full MD steps of the {s.n}-atom box on the host (oracle port: FP32 "
                                    f"pair loop, FP64 SPME 96^3 and bonded terms), median"},
@@ -193,6 +294,13 @@ def other_configs(args, local):
     t = _timed_steps(e0, k)[0][0]
     out["c0_water1k_cutoff"] = {"atoms": s0.n, "ns_per_day": ns_per_day(t), "ms_per_step": t * 1e3, "steps": k}
     e0.close()
+    if args.cpu_other:
+        threads = os.cpu_count() or 1
+        tc = cpu_step_time(s0, 5, threads, cutoff=1.2, es_mode=1)
+        out["c0_water1k_cutoff"]["cpu_baseline"] = {
+            "ns_per_day": ns_per_day(tc), "ms_per_step": tc * 1e3, "cores": threads, "kind": "port",
+            "sample": "5 full MD steps of the same box on the host (oracle port: FP32 pair loop, cutoff Coulomb, "
+                      "FP64 bonded terms), median"}
     # C1
     s1 = systems.config1()
     e1 = Engine(cutoff=1.2, electrostatics=E.ES_EWALD, ewald_tol=1e-5, nstlist=10, dt=DT_NS, device=local,
@@ -204,6 +312,15 @@ def other_configs(args, local):
     t = _timed_steps(e1, k)[0][0]
     out["c1_chains_water_pme48x48x80"] = {"atoms": s1.n, "ns_per_day": ns_per_day(t), "ms_per_step": t * 1e3,
                                           "steps": k, "prep": "300 energy-minimisation steps"}
+    if args.cpu_other:
+        threads = os.cpu_count() or 1
+        p1, v1 = e1.state()
+        s1c = dataclasses.replace(s1, pos=p1, vel=v1)
+        tc = cpu_step_time(s1c, 3, threads, cutoff=1.2, grid=(48, 48, 80), es_mode=2)
+        out["c1_chains_water_pme48x48x80"]["cpu_baseline"] = {
+            "ns_per_day": ns_per_day(tc), "ms_per_step": tc * 1e3, "cores": threads, "kind": "port",
+            "sample": "3 full MD steps of the minimised box on the host (oracle port: FP32 pair loop, FP64 SPME "
+                      "48x48x80, exclusion correction and bonded terms incl. dihedrals), median"}
     e1.close()
     # C4
     if not args.skip_batch:
@@ -354,7 +471,7 @@ def run_lima(args):
     eng.step(max(args.warmup, 3))
 
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
-    sampler = ClockSampler(local)
+    sampler = NvmlSampler(local)
 
     def barrier():
         if dist is not None:
@@ -409,6 +526,10 @@ def run_lima(args):
     sm_max = float(peaks.get("sm_max_mhz", 1965.0))
     fp32_peak = 148 * 128 * 2 * sm_max * 1e6 / 1e12      # TFLOP/s, FMA = 2
     achieved = pairs * FLOPS_PER_PAIR / nb_s / 1e12 if nb_s > 0 else None
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    plstats = eng.pairlist_stats()
+    stages = stage_rooflines({k: ph[k] for k in ("integrate", "bonded", "pme", "nblist")}, s,
+                             plstats["rows_built"], hbm)
     traffic = None
     prof = os.path.join(ROOT, "profiles", "nonbonded_water100k.json")
     if os.path.exists(prof):
@@ -469,16 +590,15 @@ def run_lima(args):
         "metric": "ns_per_day", "value": value, "unit": "ns/day", "n_gpus": world, "steps": n_timed,
         "warmup": max(args.warmup, 3), "ms_per_step": step_s * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "atoms": s.n, "pme_grid": list(GRID), "cutoff_nm": CUTOFF, "nstlist": 10,
-                   "dt_fs": 1.0, "integrator": "leapfrog", "parallelism": "replicas" if world > 1 else "single",
-                   "l2": "flushed (256 MiB write) before every timed iteration; an iteration is one pair-list "
-                         "period: list rebuild + 10 steps, energies evaluated on the last step",
-                   "accumulation": "int64 fixed point forces/energies, FP64 positions",
-                   "pair_launch_shape": shape},
+        "config": headline_config(s.n, world),
+        "pair_launch_shape": shape,
         "pairs_per_s": world * pairs / step_s,
         "pairs_per_step": pairs,
+        "pairlist": plstats,
         "wall_ms_per_step": t_wall / args.steps * 1e3,
         "phase_us": {k: ph[k] for k in ("nonbonded", "bonded", "pme", "integrate", "nblist")},
+        "pme_grid_points_per_s": stages.get("pme", {}).get("grid_points_per_s"),
+        "stages": stages,
         "roofline": {"kernel": "k_nonbonded (pair kernel)", "bound": "fp32", "achieved": achieved,
                      "peak": fp32_peak, "unit": "TFLOP/s",
                      "frac": achieved / fp32_peak if achieved else None, "traffic": traffic,
@@ -517,6 +637,8 @@ def main():
     ap.add_argument("--skip-learned", action="store_true")
     ap.add_argument("--c3-frames", type=int, default=64)
     ap.add_argument("--c3-epochs", type=int, default=20)
+    ap.add_argument("--no-cpu-other", dest="cpu_other", action="store_false",
+                    help="skip the CPU baselines of the secondary workloads")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

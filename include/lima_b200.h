@@ -233,6 +233,21 @@ LIMA_API int lima_get_energies(lima_engine* h, lima_energies* e);
  * pair kernel evaluates at the current positions.  Writes up to cap pairs
  * into pairs[2*cap] and the total count into *n. */
 LIMA_API int lima_get_pairlist(lima_engine* h, int64_t cap, int32_t* pairs, int64_t* n);
+/* Size of the cluster pair list over all systems of the handle (no
+ * counterpart in the reference, whose compound lists are fixed-size arrays):
+ * the rows built at the last rebuild (an i-cluster of 8 atoms and one j-atom
+ * in range of at least one of them), the rows the pair kernel walks each step
+ * (fewer than the built rows when the list is pruned between rebuilds), the
+ * atom pairs it evaluates (8 per walked row) and the pairs among them within
+ * the cutoff at the current positions. */
+typedef struct lima_pairlist_stats {
+    int64_t rows_built;
+    int64_t rows_walked;
+    int64_t pairs_evaluated;
+    int64_t pairs_in_cutoff;
+    int64_t reserved[4];
+} lima_pairlist_stats;
+LIMA_API int lima_get_pairlist_stats(lima_engine* h, lima_pairlist_stats* out);
 LIMA_API int lima_get_status(lima_engine* h, uint32_t* status);
 LIMA_API int lima_clear_status(lima_engine* h);
 LIMA_API int lima_get_timings(lima_engine* h, lima_timings* t);

@@ -1757,6 +1757,35 @@ int lima_get_pairlist(lima_engine* h, int64_t cap, int32_t* pairs, int64_t* n) {
     });
 }
 
+int lima_get_pairlist_stats(lima_engine* h, lima_pairlist_stats* out) {
+    if (!h || !out) return LIMA_ERR_INVALID_ARG;
+    return guarded(h, [&]() {
+        ensure_built(h);
+        if (h->state_pending) {
+            h->rebuild(true);
+            h->state_pending = false;
+        }
+        *out = lima_pairlist_stats{};
+        std::vector<int> cnt(h->st.n_clusters);
+        CK(cudaMemcpyAsync(cnt.data(), h->st.pl_count, cnt.size() * sizeof(int), cudaMemcpyDeviceToHost,
+                           h->s_main));
+        unsigned long long* dcount = h->dalloc<unsigned long long>(1);
+        launch_pairlist_dump(h->st, h->nb, 0, nullptr, dcount, h->s_main);
+        unsigned long long in_cut = 0;
+        CK(cudaMemcpyAsync(&in_cut, dcount, 8, cudaMemcpyDeviceToHost, h->s_main));
+        CK(cudaStreamSynchronize(h->s_main));
+        cudaFree(dcount);
+        h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), (void*)dcount), h->allocs.end());
+        long long rows = 0;
+        for (int c : cnt) rows += std::min(c, h->st.pl_cap);
+        out->rows_built = rows;
+        out->rows_walked = rows;
+        out->pairs_evaluated = rows * CLUSTER;
+        out->pairs_in_cutoff = (int64_t)in_cut;
+        return LIMA_OK;
+    });
+}
+
 int lima_get_status(lima_engine* h, uint32_t* status) {
     if (!h || !status) return LIMA_ERR_INVALID_ARG;
     *status = 0;

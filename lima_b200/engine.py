@@ -35,7 +35,7 @@ EXPORTED = [
     "lima_set_pairbonds", "lima_set_exclusions", "lima_set_pme_grid", "lima_set_electric_field",
     "lima_set_state",
     "lima_get_state", "lima_compute_forces", "lima_step", "lima_minimize", "lima_get_forces",
-    "lima_get_energies", "lima_get_pairlist", "lima_get_status", "lima_clear_status",
+    "lima_get_energies", "lima_get_pairlist", "lima_get_pairlist_stats", "lima_get_status", "lima_clear_status",
     "lima_get_timings", "lima_reset_timings", "lima_enable_phase_timing", "lima_pme_recip_noalloc",
     "lima_learned_pme_setup", "lima_learned_pme_collect", "lima_learned_pme_train", "lima_learned_pme_enable",
     "lima_learned_pme_eval", "lima_learned_pme_status", "lima_learned_pme_weights",
@@ -71,6 +71,11 @@ class Energies(ctypes.Structure):
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class PairlistStats(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int64) for k in ("rows_built", "rows_walked", "pairs_evaluated", "pairs_in_cutoff")] + \
+               [("reserved", ctypes.c_int64 * 4)]
 
 
 class Timings(ctypes.Structure):
@@ -121,6 +126,7 @@ def load_library(path: str = LIB_PATH):
         "lima_get_forces": (ctypes.c_int, [h, f64p]),
         "lima_get_energies": (ctypes.c_int, [h, P(Energies)]),
         "lima_get_pairlist": (ctypes.c_int, [h, ctypes.c_int64, i32p, P(ctypes.c_int64)]),
+        "lima_get_pairlist_stats": (ctypes.c_int, [h, P(PairlistStats)]),
         "lima_get_status": (ctypes.c_int, [h, P(ctypes.c_uint32)]),
         "lima_clear_status": (ctypes.c_int, [h]),
         "lima_get_timings": (ctypes.c_int, [h, P(Timings)]),
@@ -353,6 +359,12 @@ class Engine:
         self._check(self.lib.lima_get_pairlist(self.h, n.value, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
                                                ctypes.byref(n)))
         return out[: n.value]
+
+    def pairlist_stats(self) -> dict:
+        """Rows built / walked, pairs evaluated and pairs within the cutoff (all systems)."""
+        st = PairlistStats()
+        self._check(self.lib.lima_get_pairlist_stats(self.h, ctypes.byref(st)))
+        return {k: getattr(st, k) for k in ("rows_built", "rows_walked", "pairs_evaluated", "pairs_in_cutoff")}
 
     def status(self) -> int:
         s = ctypes.c_uint32(0)

@@ -75,7 +75,8 @@ def test_struct_layouts_match_the_header(tmp_path):
     header's sizes and field offsets (a C program compiled against the header
     prints them)."""
     from lima_b200 import engine as E
-    structs = {"lima_params": E.Params, "lima_energies": E.Energies, "lima_timings": E.Timings}
+    structs = {"lima_params": E.Params, "lima_energies": E.Energies, "lima_timings": E.Timings,
+               "lima_pairlist_stats": E.PairlistStats}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "lima_b200.h"', 'int main(void) {']
     for cname, py in structs.items():
         lines.append(f'    printf("{cname} size %zu\\n", sizeof({cname}));')
