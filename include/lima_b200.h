@@ -191,6 +191,19 @@ LIMA_API int lima_set_impropers(lima_engine* h, int n, const int32_t* atoms4, co
 LIMA_API int lima_set_pairbonds(lima_engine* h, int n, const int32_t* atoms2, const float* params2);
 /* Extra excluded pairs on top of the bonded-term rule. */
 LIMA_API int lima_set_exclusions(lima_engine* h, int n, const int32_t* atoms2);
+/* Compound membership, the unit the reference's builder groups atoms into
+ * (CompoundBuilder.cpp:425-565; at most 32 atoms per compound, Constants.h:91)
+ * and the bonded compound pairs (CreateCompounds, CompoundBuilder.cpp:546-560;
+ * at most 6 per compound, Bodies.cuh:205).  compound[n_atoms]: the compound of
+ * each atom of the selected system, or -1 for none; bonded[2 n_bonded]:
+ * compound ids.  Used with ref_compat = 1: as in the reference's
+ * immediate-neighbour kernel (EngineKernels.cuh:150-317 with
+ * LennardJonesInteractions.cuh:121-161), every atom pair inside one compound or
+ * across two bonded compounds, minus the excluded pairs, is evaluated with no
+ * cutoff (LJ and real-space Coulomb), and only all other pairs go through the
+ * cutoff pair list.  Without ref_compat the membership is kept but unused. */
+LIMA_API int lima_set_compounds(lima_engine* h, int n_atoms, const int32_t* compound, int n_bonded,
+                                const int32_t* bonded);
 /* Per-system PME grid; overrides lima_params.pme_grid / pme_spacing. */
 LIMA_API int lima_set_pme_grid(lima_engine* h, int nx, int ny, int nz);
 /* Uniform external electric field [V/nm] on the selected system (default 0):

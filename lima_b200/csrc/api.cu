@@ -13,6 +13,8 @@
 //   pme    :        spread -> 5 FFT passes -> gather -----------^
 #include <algorithm>
 #include <climits>
+#include <map>
+#include <set>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -44,6 +46,8 @@ struct SystemHost {
     std::vector<double> pos;
     std::vector<float> vel;
     double efield[3] = {0.0, 0.0, 0.0};   // external field [V/nm]
+    std::vector<int32_t> compound;        // compound of each atom (-1: none); empty = not set
+    std::vector<int32_t> bonded_compounds;  // pairs of bonded compound ids
 };
 
 struct CudaError {
@@ -546,6 +550,44 @@ void lima_engine::setup() {
             exclude_all(a, 2, off);
         }
     }
+    // ---- the reference's immediate-neighbour pairs (ref_compat with compounds):
+    // every pair inside a compound or across bonded compounds that is not
+    // excluded is evaluated with no cutoff by its own kernel, and joins the
+    // exclusion lists so that the cutoff pair list skips it
+    std::vector<int2> midx;
+    if (p.ref_compat) {
+        for (int s = 0; s < ns; ++s) {
+            const SystemHost& S = sys[s];
+            if (S.compound.empty()) continue;
+            const int off = n_atoms_off[s];
+            std::map<int, std::vector<int>> members;
+            for (int i = 0; i < S.n; ++i)
+                if (S.compound[i] >= 0) members[S.compound[i]].push_back(i + off);
+            auto add_pair = [&](int a, int b) {
+                if (a == b) return;
+                if (std::find(ex[a].begin(), ex[a].end(), b) != ex[a].end()) return;
+                midx.push_back(make_int2(std::min(a, b), std::max(a, b)));
+            };
+            for (auto& kv : members) {
+                const auto& m = kv.second;
+                for (size_t x = 0; x < m.size(); ++x)
+                    for (size_t y = x + 1; y < m.size(); ++y) add_pair(m[x], m[y]);
+            }
+            std::set<std::pair<int, int>> seen;
+            for (size_t t = 0; t < S.bonded_compounds.size() / 2; ++t) {
+                const int c0 = std::min(S.bonded_compounds[2 * t], S.bonded_compounds[2 * t + 1]);
+                const int c1 = std::max(S.bonded_compounds[2 * t], S.bonded_compounds[2 * t + 1]);
+                if (!seen.insert({c0, c1}).second) continue;
+                for (int a : members[c0])
+                    for (int b : members[c1]) add_pair(a, b);
+            }
+        }
+        std::sort(midx.begin(), midx.end(), [](int2 u, int2 v) { return u.x != v.x ? u.x < v.x : u.y < v.y; });
+        for (const int2 pr : midx) {
+            ex[pr.x].push_back(pr.y);
+            ex[pr.y].push_back(pr.x);
+        }
+    }
     std::vector<int> excl_off(N + 1, 0), excl_idx, mol(N);
     for (int a = 0; a < N; ++a) {
         auto& v = ex[a];
@@ -676,6 +718,8 @@ void lima_engine::setup() {
     B.ni = (int)iidx.size();
     B.np = (int)pidx.size();
     B.nx = (int)xidx.size();
+    B.nm = (int)midx.size();
+    B.midx = upload(midx);
     B.bidx = upload(bidx);
     B.bpar = upload(bpar);
     B.aidx = upload(aidx);
@@ -1125,6 +1169,7 @@ void lima_engine::capture_period() {
         CK(cudaStreamWaitEvent(s_pme, ev_fork, 0));
         launches += launch_bonded(st, bt, false, s_bonded);
         if (pme_on) launches += launch_exclusion_correction(st, bt, nb, false, s_bonded);
+        launches += launch_immediate_pairs(st, bt, nb, false, s_bonded);
         CK(cudaEventRecord(ev_bonded, s_bonded));
         if (pme_on) launches += launch_pme(st, pp, false, s_pme);
         CK(cudaEventRecord(ev_pme, s_pme));
@@ -1165,6 +1210,7 @@ void lima_engine::forces(bool energy, bool atom_energy) {
     mark(2, 0, sb);
     launches += launch_bonded(st, bt, energy, sb);
     if (pme_on) launches += launch_exclusion_correction(st, bt, nb, energy, sb);
+    launches += launch_immediate_pairs(st, bt, nb, energy, sb);
     mark(2, 1, sb);
     CK(cudaEventRecord(ev_bonded, sb));
     if (pme_on) {
@@ -1521,6 +1567,31 @@ int lima_set_exclusions(lima_engine* h, int n, const int32_t* a) {
     if (!h) return LIMA_ERR_INVALID_ARG;
     std::vector<float> unused;
     return set_terms(h, n, a, 2, nullptr, 0, h->sys[h->cur].excl, unused);
+}
+
+int lima_set_compounds(lima_engine* h, int n_atoms, const int32_t* compound, int n_bonded, const int32_t* bonded) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    SystemHost& S = h->sys[h->cur];
+    if (n_atoms != S.n || (n_atoms > 0 && !compound) || n_bonded < 0 || (n_bonded > 0 && !bonded))
+        return fail(h, LIMA_ERR_INVALID_ARG, "compound arrays must cover every atom of the system");
+    std::vector<int> count(std::max(n_atoms, 1), 0);
+    for (int i = 0; i < n_atoms; ++i) {
+        const int c = compound[i];
+        if (c < -1 || c >= n_atoms) return fail(h, LIMA_ERR_INVALID_ARG, "compound id out of range");
+        if (c >= 0 && ++count[c] > 32)
+            return fail(h, LIMA_ERR_INVALID_ARG, "a compound holds at most 32 atoms (MAX_COMPOUND_PARTICLES)");
+    }
+    std::vector<int> nb(std::max(n_atoms, 1), 0);
+    for (int t = 0; t < n_bonded; ++t) {
+        const int a = bonded[2 * t], b = bonded[2 * t + 1];
+        if (a < 0 || b < 0 || a >= n_atoms || b >= n_atoms || a == b || !count[a] || !count[b])
+            return fail(h, LIMA_ERR_INVALID_ARG, "bonded compound pair names a missing compound");
+        if (++nb[a] > 6 || ++nb[b] > 6)
+            return fail(h, LIMA_ERR_INVALID_ARG, "a compound is bonded to at most 6 others (max_bonded_compounds)");
+    }
+    S.compound.assign(compound, compound + n_atoms);
+    S.bonded_compounds.assign(bonded, bonded + 2 * (size_t)n_bonded);
+    return topology_changed(h);
 }
 
 int lima_set_electric_field(lima_engine* h, double ex, double ey, double ez) {

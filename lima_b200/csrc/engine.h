@@ -125,6 +125,8 @@ struct BondedTerms {
     float2* ppar = nullptr;
     int nx = 0;                 // excluded charged pairs for the Ewald correction
     int2* xidx = nullptr;
+    int nm = 0;                 // immediate-neighbour pairs (ref_compat compounds): no cutoff
+    int2* midx = nullptr;
 };
 
 struct NbParams {
@@ -152,6 +154,8 @@ int launch_exclusion_correction(const DevState& st, const BondedTerms& bt, const
                                  bool energy, cudaStream_t s);
 int launch_pairlist_dump(const DevState& st, const NbParams& p, long long cap, int* out_pairs,
                           unsigned long long* out_count, cudaStream_t s);
+int launch_immediate_pairs(const DevState& st, const BondedTerms& bt, const NbParams& p, bool energy,
+                           cudaStream_t s);
 // bonded.cu
 int launch_bonded(const DevState& st, const BondedTerms& bt, bool energy, cudaStream_t s);
 // pme.cu

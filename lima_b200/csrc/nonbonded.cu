@@ -409,6 +409,89 @@ int launch_exclusion_correction(const DevState& st, const BondedTerms& bt, const
     return 1;
 }
 
+// The reference's immediate-neighbour pairs (reference convention with
+// compounds): every pair inside one compound or across two bonded compounds,
+// minus the excluded pairs, evaluated with NO cutoff
+// (compoundImmediateneighborAndSelfShortrangeInteractionsKernel,
+// EngineKernels.cuh:150-317, through the LUT overload of
+// computeCompoundCompoundLJForces, LennardJonesInteractions.cuh:121-161).  The
+// same LJ and real-space Coulomb arithmetic as the pair kernel (sigma/2 and
+// sqrt(eps) per atom, erfc(kappa r) in Ewald mode); the EM variant clamps the LJ
+// force as the reference's energy minimiser does.  One thread per pair; the
+// difference vector comes from the FP64 positions with the minimum image.
+template <bool ENERGY>
+__global__ void k_immediate_pairs(DevState st, BondedTerms bt, NbParams p) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    double elj = 0.0, ecl = 0.0, vir = 0.0;
+    int sysi = -1;
+    if (t < bt.nm) {
+        const int2 pr = bt.midx[t];
+        const int si = st.slot_of[pr.x], sj = st.slot_of[pr.y];
+        sysi = st.atom_sys[pr.x];
+        const SysDesc& sd = st.sys[sysi];
+        double d[3] = {st.px[sj] - st.px[si], st.py[sj] - st.py[si], st.pz[sj] - st.pz[si]};   // r_j - r_i
+        if (st.periodic)
+            for (int k = 0; k < 3; ++k) d[k] -= sd.box[k] * rint(d[k] / sd.box[k]);
+        const float dx = (float)d[0], dy = (float)d[1], dz = (float)d[2];
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        const float rinv = rsqrtf(r2);
+        const float rinv2 = rinv * rinv;
+        const float2 li = st.ljp[si], lj = st.ljp[sj];
+        const float sig = li.x + lj.x, eps = li.y * lj.y;
+        float s6 = sig * sig * rinv2;
+        s6 = s6 * s6 * s6;
+        // attraction along r_j - r_i when positive
+        float fs = 24.f * eps * s6 * rinv2 * (1.f - 2.f * s6);
+        if (p.em) fs = em_lj_clamp(fs, r2 * rinv);
+        const float qq = p.ke * st.xyzq[si].w * st.xyzq[sj].w;
+        float ec = 0.f;
+        if (p.es_mode != 0 && qq != 0.f) {
+            float fc = qq * rinv * rinv2;   // repulsion along r_i - r_j
+            ec = qq * rinv;
+            if (p.es_mode == 2) {
+                const float r = r2 * rinv, kr = p.kappa * r;
+                const float erfc_kr = erfcf(kr);
+                fc *= erfc_kr + p.two_kappa_sqrtpi * r * __expf(-kr * kr);
+                ec *= erfc_kr;
+            }
+            fs -= fc;
+        }
+        if (p.em) fs = fmaxf(fminf(fs, 1e20f), -1e20f);
+        const float fx = fs * dx, fy = fs * dy, fz = fs * dz;   // force on i
+        atomic_add_fixed(st.fx + si, to_fixed(fx, FORCE_SCALE));
+        atomic_add_fixed(st.fy + si, to_fixed(fy, FORCE_SCALE));
+        atomic_add_fixed(st.fz + si, to_fixed(fz, FORCE_SCALE));
+        atomic_add_fixed(st.fx + sj, to_fixed(-fx, FORCE_SCALE));
+        atomic_add_fixed(st.fy + sj, to_fixed(-fy, FORCE_SCALE));
+        atomic_add_fixed(st.fz + sj, to_fixed(-fz, FORCE_SCALE));
+        if (ENERGY) {
+            elj = 4.0 * (double)eps * (double)s6 * ((double)s6 - 1.0);
+            ecl = (double)ec;
+            vir = 0.5 * (double)fs * (double)r2;   // -1/2 r_ij . f_ij
+            if (st.atom_energy) {
+                add_atom_energy(st.epot, si, 0.5 * (elj + ecl));
+                add_atom_energy(st.epot, sj, 0.5 * (elj + ecl));
+            }
+        }
+    }
+    if (ENERGY) {
+        add_energy_fixed(st.energy, sysi, elj, E_LJ);
+        add_energy_fixed(st.energy, sysi, ecl, E_COUL);
+        add_energy_fixed(st.energy, sysi, vir, E_VIRIAL);
+    }
+}
+
+int launch_immediate_pairs(const DevState& st, const BondedTerms& bt, const NbParams& p, bool energy,
+                           cudaStream_t s) {
+    if (bt.nm == 0) return 0;
+    const int TB = 256;
+    if (energy)
+        k_immediate_pairs<true><<<(bt.nm + TB - 1) / TB, TB, 0, s>>>(st, bt, p);
+    else
+        k_immediate_pairs<false><<<(bt.nm + TB - 1) / TB, TB, 0, s>>>(st, bt, p);
+    return 1;
+}
+
 // Writes every (orig_i, orig_j) pair the pair kernel evaluates (mask bit set and
 // r^2 <= rc^2) with i < j; order is not defined (the host sorts).
 __global__ void k_pairlist_dump(DevState st, NbParams p, long long cap, int* out,

@@ -32,7 +32,7 @@ EXPORTED = [
     "lima_default_params", "lima_error_string", "lima_last_error", "lima_version", "lima_create",
     "lima_create_batch", "lima_destroy", "lima_select_system", "lima_num_systems", "lima_set_box",
     "lima_set_atoms", "lima_set_bonds", "lima_set_angles", "lima_set_dihedrals", "lima_set_impropers",
-    "lima_set_pairbonds", "lima_set_exclusions", "lima_set_pme_grid", "lima_set_electric_field",
+    "lima_set_pairbonds", "lima_set_exclusions", "lima_set_compounds", "lima_set_pme_grid", "lima_set_electric_field",
     "lima_set_state",
     "lima_get_state", "lima_compute_forces", "lima_step", "lima_minimize", "lima_get_forces",
     "lima_get_energies", "lima_get_pairlist", "lima_get_pairlist_stats", "lima_get_status", "lima_clear_status",
@@ -116,6 +116,7 @@ def load_library(path: str = LIB_PATH):
         "lima_set_impropers": (ctypes.c_int, [h, ctypes.c_int, i32p, f32p]),
         "lima_set_pairbonds": (ctypes.c_int, [h, ctypes.c_int, i32p, f32p]),
         "lima_set_exclusions": (ctypes.c_int, [h, ctypes.c_int, i32p]),
+        "lima_set_compounds": (ctypes.c_int, [h, ctypes.c_int, i32p, ctypes.c_int, i32p]),
         "lima_set_pme_grid": (ctypes.c_int, [h, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
         "lima_set_electric_field": (ctypes.c_int, [h, ctypes.c_double, ctypes.c_double, ctypes.c_double]),
         "lima_set_state": (ctypes.c_int, [h, f64p, f32p]),
@@ -282,6 +283,16 @@ class Engine:
         ia, ip = _i32(idx, 2)
         self._check(self.lib.lima_set_exclusions(self.h, len(ia), ip))
 
+    def set_compounds(self, compound, bonded=None):
+        """Compound of each atom (-1: none) and bonded compound pairs; with
+        ref_compat the engine evaluates pairs inside a compound and across bonded
+        compounds without a cutoff, as the reference does."""
+        c = np.ascontiguousarray(compound, dtype=np.int32).ravel()
+        b = np.ascontiguousarray(np.zeros((0, 2)) if bonded is None else bonded, dtype=np.int32).reshape(-1, 2)
+        i32 = ctypes.POINTER(ctypes.c_int32)
+        self._check(self.lib.lima_set_compounds(self.h, len(c), c.ctypes.data_as(i32), len(b),
+                                                b.ctypes.data_as(i32) if len(b) else None))
+
     def set_pme_grid(self, grid):
         self._check(self.lib.lima_set_pme_grid(self.h, int(grid[0]), int(grid[1]), int(grid[2])))
 
@@ -310,6 +321,9 @@ class Engine:
         extra = getattr(system, "extra_exclusions", None)
         if extra is not None and len(extra):
             self.set_exclusions(extra)
+        comp = getattr(system, "compound", None)
+        if comp is not None and len(comp):
+            self.set_compounds(comp, getattr(system, "bonded_compounds", None))
         if pme_grid is not None:
             self.set_pme_grid(pme_grid)
         self.set_state(system.pos, system.vel)

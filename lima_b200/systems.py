@@ -50,6 +50,18 @@ class System:
     name: str = ""
     # pairs excluded beyond those sharing a bonded term (e.g. a topology's [ exclusions ])
     extra_exclusions: np.ndarray = field(default_factory=lambda: np.zeros((0, 2), np.int32))
+    # compound of each atom (-1: none) and bonded compound pairs (lima_b200.compounds);
+    # None: not set
+    compound: np.ndarray | None = None
+    bonded_compounds: np.ndarray | None = None
+
+    def with_compounds(self, tinymol_max_atoms: int = 0) -> "System":
+        """This system with the reference builder's compound grouping attached."""
+        from dataclasses import replace
+
+        from .compounds import build_compounds
+        c, b = build_compounds(self, tinymol_max_atoms)
+        return replace(self, compound=c, bonded_compounds=b)
 
     @property
     def n(self) -> int:

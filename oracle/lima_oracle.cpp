@@ -460,6 +460,77 @@ inline int wrapi(int i, int n) {
     return i < 0 ? i + n : i;
 }
 
+// The reference convention's influence function at wave index m
+// (PME.cuh:434-495): 4 pi/k^2 e^{-k^2/4 kappa^2} k_e times the squared product
+// of sinc^4(k_d h_d / 2), with the truncated pi of Constants.h:51; zero at k = 0.
+// Without the N/V factor of the oracle's own normalisation.
+inline double influence_ref(const int* m, const double* box, const int* K, double kappa) {
+    if (m[0] == 0 && m[1] == 0 && m[2] == 0) return 0.0;
+    double kv[3], k2 = 0.0;
+    for (int d = 0; d < 3; ++d) {
+        kv[d] = 2.0 * kPiRef * m[d] / box[d];
+        k2 += kv[d] * kv[d];
+    }
+    const double g = 4.0 * kPiRef / k2 * std::exp(-k2 / (4.0 * kappa * kappa)) * kCoulomb;
+    double s = 1.0;
+    for (int d = 0; d < 3; ++d) {
+        const double kh = kv[d] * (box[d] / K[d]) * 0.5;
+        const double sc = std::fabs(kh) < 1e-14 ? 1.0 : std::sin(kh) / kh;
+        s *= sc * sc * sc * sc;
+    }
+    return g * s * s;
+}
+
+// EngineUtils.cuh:112-140 — the energy minimiser's force activation: the force
+// is rescaled to length A tanh(|F|/A), A = 1e6 * scalar [J/mol/nm], with the
+// reference's 1e-8 guard on the division.
+inline void force_activation(const double* f, double scalar, double* out) {
+    const double A = 1000.0 * 1000.0 * scalar;
+    const double fl = std::sqrt(f[0] * f[0] + f[1] * f[1] + f[2] * f[2]);
+    const double k = A * std::tanh(fl / A) / (fl + 1e-8);
+    for (int d = 0; d < 3; ++d) out[d] = f[d] * k;
+}
+
+// EngineUtils.cuh:44-72 — one ADAM move: the force is scaled by 1e-8, the
+// moments updated with beta 0.9 / 0.999, bias-corrected at `step`, and the
+// position moves by alpha 1e-8 m/(sqrt(v) + 1e-8), alpha = 8000.
+inline void adam_move(const double* f, double* m1, double* m2, int step, double* pos) {
+    const double alpha = 8000.0, b1 = 0.9, b2 = 0.999, epsn = 1e-8;
+    for (int d = 0; d < 3; ++d) {
+        const double g = f[d] * 1e-8;
+        m1[d] = m1[d] * b1 + g * (1 - b1);
+        m2[d] = m2[d] * b2 + g * g * (1 - b2);
+        const double mh = m1[d] / (1 - std::pow(b1, step));
+        const double vh = m2[d] / (1 - std::pow(b2, step));
+        pos[d] += mh / (std::sqrt(vh) + epsn) * alpha * 1e-8;
+    }
+}
+
+// Neighborlists.cuh:64-79 with LimaPositionSystem.cuh:194-198 and
+// BoundaryCondition.cuh:56-65 — two compounds are neighbours when any pair of
+// their two key particles is closer than cutoff + radius_left + radius_right.
+// The distance is taken in FP32 with the reference's hyper-position rule: the
+// right particle moves by one box length along each axis where it lies more
+// than half a box away (a strict comparison against L/2), then |left - right|.
+inline bool compounds_interact(const double* kl, const double* kr, const double* rl, const double* rr, float L,
+                               float cutoff) {
+    const float half = L / 2.f;
+    for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b) {
+            float d2 = 0.f;
+            for (int c = 0; c < 3; ++c) {
+                const float s = (float)kl[3 * a + c];
+                float m = (float)kr[3 * b + c];
+                m += L * (float)((s - m) > half);
+                m -= L * (float)((s - m) < -half);
+                const float dd = s - m;
+                d2 += dd * dd;
+            }
+            if (std::sqrt(d2) < cutoff + (float)rl[a] + (float)rr[b]) return true;
+        }
+    return false;
+}
+
 }  // namespace
 
 // ====================================================================== API
@@ -649,14 +720,7 @@ void orc_pme(int n, const double* pos, const double* q, const double* box, int k
                 if (m[0] != 0 || m[1] != 0 || m[2] != 0) {
                     const double g = 4.0 * pi_c / k2 * std::exp(-k2 / (4.0 * kappa * kappa)) * kCoulomb;
                     if (influence == 1) {
-                        double s = 1.0;
-                        for (int d = 0; d < 3; ++d) {
-                            const double h = box[d] / K[d];
-                            const double kh = kv[d] * h * 0.5;
-                            const double sc = std::fabs(kh) < 1e-14 ? 1.0 : std::sin(kh) / kh;
-                            s *= sc * sc * sc * sc;
-                        }
-                        th = g * s * s * (double)N / V;
+                        th = influence_ref(m, box, K, kappa) * (double)N / V;
                     } else {
                         double B = 1.0;
                         for (int d = 0; d < 3; ++d) {
@@ -786,24 +850,99 @@ void orc_integrate(int n, double* pos, double* vel, double* fprev, const double*
 }
 
 void orc_em_step(int n, double* pos, const double* forces, double* adam, int step) {
-    const double alpha = 8000.0, b1 = 0.9, b2 = 0.999, epsn = 1e-8;
-    const double fmax = 1000.0 * 1000.0;  // tanh clamp scale [J/mol/nm]
     for (int i = 0; i < n; ++i) {
-        D3 f = load(forces, i);
-        const double fl = len(f);
-        const double sm = fmax * std::tanh(fl / fmax);
-        f = f * (sm / (fl + 1e-8));
-        double* m1 = adam + 6 * i;
-        double* m2 = adam + 6 * i + 3;
-        const double g[3] = {f.x * 1e-8, f.y * 1e-8, f.z * 1e-8};
-        for (int d = 0; d < 3; ++d) {
-            m1[d] = m1[d] * b1 + g[d] * (1 - b1);
-            m2[d] = m2[d] * b2 + g[d] * g[d] * (1 - b2);
-            const double mh = m1[d] / (1 - std::pow(b1, step));
-            const double vh = m2[d] / (1 - std::pow(b2, step));
-            pos[3 * i + d] += mh / (std::sqrt(vh) + epsn) * alpha * 1e-8;
+        double f[3];
+        force_activation(&forces[3 * i], 1.0, f);
+        adam_move(f, adam + 6 * i, adam + 6 * i + 3, step, &pos[3 * i]);
+    }
+}
+
+// ------------------------------------------------ per-term entry points
+// Each evaluates, sample by sample, the same internal function the system
+// loops above use, so that the golden vectors of the reference's own device
+// functions pin exactly the code the system-level checks run.
+
+void orc_pair_terms(int n, const double* diff, const double* sig, const double* eps, const double* qq,
+                    int es_mode, double kappa, int precision, int em, double* f_out, double* e_out) {
+    for (int t = 0; t < n; ++t) {
+        if (precision == 32) {
+            const V3<float> d{(float)diff[3 * t], (float)diff[3 * t + 1], (float)diff[3 * t + 2]};
+            const PairOut<float> o = pair_interaction<float>(d, dot(d, d), (float)sig[t], (float)eps[t], (float)qq[t],
+                                                             es_mode, (float)kappa, (float)kCoulomb, (float)kPiRef,
+                                                             em != 0);
+            f_out[3 * t] = o.f_on_i.x, f_out[3 * t + 1] = o.f_on_i.y, f_out[3 * t + 2] = o.f_on_i.z;
+            e_out[2 * t] = o.e_lj, e_out[2 * t + 1] = o.e_coul;
+        } else {
+            const D3 d = load(diff, t);
+            const PairOut<double> o = pair_interaction<double>(d, dot(d, d), sig[t], eps[t], qq[t], es_mode, kappa,
+                                                               kCoulomb, kPi, em != 0);
+            f_out[3 * t] = o.f_on_i.x, f_out[3 * t + 1] = o.f_on_i.y, f_out[3 * t + 2] = o.f_on_i.z;
+            e_out[2 * t] = o.e_lj, e_out[2 * t + 1] = o.e_coul;
         }
     }
+}
+
+void orc_bonded_terms(int kind, int n, const double* pos, const double* par, double* f_out, double* e_out) {
+    static const int natoms[5] = {2, 3, 4, 4, 2}, npar[5] = {2, 4, 3, 2, 2};
+    if (kind < 0 || kind > 4) return;
+    const int na = natoms[kind], np = npar[kind];
+    for (int t = 0; t < n; ++t) {
+        const double* x = pos + (size_t)3 * na * t;
+        const double* p = par + (size_t)np * t;
+        D3 f[4];
+        double e = 0.0;
+        if (kind == 0) bond_term(load(x, 0), load(x, 1), p[0], p[1], f, &e);
+        else if (kind == 1) angle_term(load(x, 0), load(x, 1), load(x, 2), p, f, &e);
+        else if (kind == 2) dihedral_term(load(x, 0), load(x, 1), load(x, 2), load(x, 3), p, f, &e);
+        else if (kind == 3) improper_term(load(x, 0), load(x, 1), load(x, 2), load(x, 3), p, f, &e);
+        else pairbond_term(load(x, 0), load(x, 1), p[0], p[1], f, &e);
+        for (int a = 0; a < na; ++a) {
+            double* o = f_out + (size_t)3 * (na * t + a);
+            o[0] = f[a].x, o[1] = f[a].y, o[2] = f[a].z;
+        }
+        e_out[t] = e;
+    }
+}
+
+void orc_bspline4(int n, const double* f, double* w) {
+    for (int t = 0; t < n; ++t) bspline4(f[t], w + 4 * t, nullptr);
+}
+
+void orc_ref_green(int K, double L, double kappa, double* out) {
+    // the reference's layout: x (the half dimension, K/2 + 1) fastest, then y, z
+    const int H = K / 2 + 1;
+    const double box[3] = {L, L, L};
+    const int Ks[3] = {K, K, K};
+    for (int z = 0; z < K; ++z)
+        for (int y = 0; y < K; ++y)
+            for (int x = 0; x < H; ++x) {
+                const int m[3] = {x, y <= K / 2 ? y : y - K, z <= K / 2 ? z : z - K};
+                out[(size_t)x + (size_t)H * ((size_t)y + (size_t)K * z)] = influence_ref(m, box, Ks, kappa);
+            }
+}
+
+void orc_force_activation(int n, const double* f, double scalar, double* out) {
+    for (int t = 0; t < n; ++t) force_activation(f + 3 * t, scalar, out + 3 * t);
+}
+
+void orc_adam(int n, const double* f, double* m1, double* m2, const int* step, double* dpos) {
+    for (int t = 0; t < n; ++t) {
+        dpos[3 * t] = dpos[3 * t + 1] = dpos[3 * t + 2] = 0.0;
+        adam_move(f + 3 * t, m1 + 3 * t, m2 + 3 * t, step[t], dpos + 3 * t);
+    }
+}
+
+int orc_compounds_interact(int n, const double* keys_left, const double* keys_right, const double* radii_left,
+                           const double* radii_right, double box_nm, double cutoff, uint8_t* out) {
+    int hits = 0;
+    for (int t = 0; t < n; ++t) {
+        out[t] = compounds_interact(keys_left + 6 * t, keys_right + 6 * t, radii_left + 2 * t,
+                                    radii_right + 2 * t, (float)box_nm, (float)cutoff)
+                     ? 1
+                     : 0;
+        hits += out[t];
+    }
+    return hits;
 }
 
 void orc_fft3d(int kx, int ky, int kz, double* data, int sign) {

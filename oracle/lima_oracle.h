@@ -143,6 +143,38 @@ void orc_integrate(int n, double* pos, double* vel, double* fprev, const double*
  * adam[6n] = first and second moments; step counts from 1. */
 void orc_em_step(int n, double* pos, const double* forces, double* adam, int step);
 
+/* ---- per-term entry points: each runs, sample by sample, the same internal
+ * function the system-level calls above use (checked against golden vectors of
+ * the reference's own device functions, tests/golden/). */
+
+/* Pair term (LennardJonesInteractions.cuh:74-108, DeviceAlgorithmsPrivate.cuh:38-95):
+ * diff[3n] = r_j - r_i, combined sigma/epsilon, qq = q_i q_j [kC/mol]^2; force on i
+ * [J/mol/nm] -> f_out[3n]; full pair energies (LJ, Coulomb) -> e_out[2n].
+ * precision 32 = the FP32 reference-faithful arithmetic; em = EM clamp variant. */
+void orc_pair_terms(int n, const double* diff, const double* sig, const double* eps, const double* qq,
+                    int es_mode, double kappa, int precision, int em, double* f_out, double* e_out);
+/* Bonded term of one kind per call: 0 bond (2 atoms; b0, kb), 1 angle + UB (3; theta0,
+ * k_theta, ub0, k_ub), 2 dihedral (4; phi0, k_phi, n), 3 improper (4; psi0, k_psi),
+ * 4 pair bond (2; sigma, epsilon).  pos[3 natoms n], par[npar n]; forces per atom
+ * -> f_out[3 natoms n], energy -> e_out[n]. */
+void orc_bonded_terms(int kind, int n, const double* pos, const double* par, double* f_out, double* e_out);
+/* Order-4 cardinal B-spline weights at fractions f (DeviceAlgorithmsPrivate.cuh:7-30). */
+void orc_bspline4(int n, const double* f, double* w);
+/* The reference convention's influence function on a K^3 grid of a cubic box L
+ * (PME.cuh:434-495), in its half-complex layout (x in 0..K/2 fastest, then y, z). */
+void orc_ref_green(int K, double L, double kappa, double* out);
+/* Energy-minimisation force activation (EngineUtils.cuh:112-140), scale A = 1e6 scalar. */
+void orc_force_activation(int n, const double* f, double scalar, double* out);
+/* One ADAM move per sample (EngineUtils.cuh:44-72): updates m1[3n], m2[3n] in place and
+ * writes the position change [nm] to dpos[3n]; step[n] counts from 1. */
+void orc_adam(int n, const double* f, double* m1, double* m2, const int* step, double* dpos);
+/* The reference's compound-neighbour test (Neighborlists.cuh:64-79): two compounds with
+ * two key particles each (keys[6n], positions in nm) and their radii[2n] interact when
+ * a key pair is closer than cutoff + r_left + r_right, distances in FP32 under the
+ * reference's hyper-position rule in a cubic box of box_nm.  out[n] = 0/1; returns the count. */
+int orc_compounds_interact(int n, const double* keys_left, const double* keys_right, const double* radii_left,
+                           const double* radii_right, double box_nm, double cutoff, uint8_t* out);
+
 /* 3-D complex DFT in FP64 (x fastest), sign -1 forward, +1 inverse (no
  * normalisation).  data is interleaved re,im. */
 void orc_fft3d(int kx, int ky, int kz, double* data, int sign);

@@ -31,6 +31,18 @@ def build(force: bool = False) -> str:
     return _LIB_PATH
 
 
+def build_reference_harness(ref_dir: str | None = None) -> str | None:
+    """Compile oracle/_ref/ref_terms (the reference's own per-term device
+    functions, built from the reference tree; see ref_harness.cu) when that tree
+    is at hand: LIMA_REFERENCE_DIR, or the given directory.  Returns the binary's
+    path, or None when there is no reference tree."""
+    ref_dir = ref_dir or os.environ.get("LIMA_REFERENCE_DIR", "")
+    if not ref_dir or not os.path.isdir(os.path.join(ref_dir, "code", "LIMA_ENGINE")):
+        return None
+    subprocess.run(["make", "-s", "-C", _HERE, "ref", f"REF_DIR={ref_dir}"], check=True)
+    return os.path.join(_HERE, "_ref", "ref_terms")
+
+
 def lib():
     global _lib
     if _lib is None:
@@ -77,6 +89,21 @@ def lib():
         L.orc_mlp_forward.argtypes = [ctypes.c_int, _d, _d, _d]
         L.orc_mlp_grads.restype = ctypes.c_double
         L.orc_mlp_grads.argtypes = [ctypes.c_int, _d, _d, _d, _d]
+        L.orc_pair_terms.restype = None
+        L.orc_pair_terms.argtypes = [ctypes.c_int, _d, _d, _d, _d, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                     ctypes.c_int, _d, _d]
+        L.orc_bonded_terms.restype = None
+        L.orc_bonded_terms.argtypes = [ctypes.c_int, ctypes.c_int, _d, _d, _d, _d]
+        L.orc_bspline4.restype = None
+        L.orc_bspline4.argtypes = [ctypes.c_int, _d, _d]
+        L.orc_ref_green.restype = None
+        L.orc_ref_green.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, _d]
+        L.orc_force_activation.restype = None
+        L.orc_force_activation.argtypes = [ctypes.c_int, _d, ctypes.c_double, _d]
+        L.orc_adam.restype = None
+        L.orc_adam.argtypes = [ctypes.c_int, _d, _d, _d, _i, _d]
+        L.orc_compounds_interact.restype = ctypes.c_int
+        L.orc_compounds_interact.argtypes = [ctypes.c_int, _d, _d, _d, _d, ctypes.c_double, ctypes.c_double, _u8]
         _lib = L
     return _lib
 
@@ -293,3 +320,119 @@ def mlp_forward(x, params):
     y = np.zeros((len(x), 3))
     lib().orc_mlp_forward(len(x), _dp(x), _dp(params), _dp(y))
     return y
+
+
+# ------------------------------------------------ per-term entry points
+def pair_terms(diff, sig, eps, qq, es_mode, kappa=0.0, precision=64, em=False):
+    """Per-sample pair term: (force on i (n,3), LJ energy (n,), Coulomb energy (n,))."""
+    diff = _f64(diff).reshape(-1, 3)
+    n = len(diff)
+    f = np.zeros((n, 3))
+    e = np.zeros((n, 2))
+    lib().orc_pair_terms(n, _dp(diff), _dp(_f64(sig)), _dp(_f64(eps)), _dp(_f64(qq)), int(es_mode), float(kappa),
+                         int(precision), 1 if em else 0, _dp(f), _dp(e))
+    return f, e[:, 0], e[:, 1]
+
+
+BONDED_KINDS = {"bond": (0, 2, 2), "angle": (1, 3, 4), "dihedral": (2, 4, 3), "improper": (3, 4, 2),
+                "pairbond": (4, 2, 2)}
+
+
+def bonded_terms(kind, pos, par):
+    """Per-sample bonded term: (forces (n, natoms, 3), energy (n,))."""
+    k, na, npar = BONDED_KINDS[kind]
+    pos = _f64(pos).reshape(-1, na, 3)
+    par = _f64(par).reshape(-1, npar)
+    n = len(pos)
+    f = np.zeros((n, na, 3))
+    e = np.zeros(n)
+    lib().orc_bonded_terms(k, n, _dp(pos), _dp(par), _dp(f), _dp(e))
+    return f, e
+
+
+def bspline4(f):
+    f = _f64(f).ravel()
+    w = np.zeros((len(f), 4))
+    lib().orc_bspline4(len(f), _dp(f), _dp(w))
+    return w
+
+
+def ref_green(K, L, kappa):
+    out = np.zeros((K // 2 + 1) * K * K)
+    lib().orc_ref_green(int(K), float(L), float(kappa), _dp(out))
+    return out
+
+
+def force_activation(f, scalar):
+    f = _f64(f).reshape(-1, 3)
+    out = np.zeros_like(f)
+    lib().orc_force_activation(len(f), _dp(f), float(scalar), _dp(out))
+    return out
+
+
+def adam(f, m1, m2, step):
+    f = _f64(f).reshape(-1, 3)
+    m1 = _f64(m1).reshape(-1, 3).copy()
+    m2 = _f64(m2).reshape(-1, 3).copy()
+    st = np.ascontiguousarray(step, dtype=np.int32).ravel()
+    d = np.zeros_like(f)
+    lib().orc_adam(len(f), _dp(f), _dp(m1), _dp(m2), _ip(st), _dp(d))
+    return d, m1, m2
+
+
+def compounds_interact(keys_left, keys_right, radii_left, radii_right, box_nm, cutoff):
+    kl = _f64(keys_left).reshape(-1, 6)
+    n = len(kl)
+    out = np.zeros(n, np.uint8)
+    lib().orc_compounds_interact(n, _dp(kl), _dp(_f64(keys_right).reshape(-1, 6)), _dp(_f64(radii_left)),
+                                 _dp(_f64(radii_right)), float(box_nm), float(cutoff),
+                                 out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)))
+    return out.astype(bool)
+
+
+def immediate_pairs(compound, bonded, excl_pairs):
+    """The reference's immediate-neighbour pair set (EngineKernels.cuh:150-317):
+    every (i<j) pair inside one compound or across two bonded compounds that is
+    not excluded (the BondedParticlesLUT, CompoundBuilder.cpp:40-60)."""
+    compound = np.asarray(compound)
+    members = {}
+    for i, c in enumerate(compound):
+        if c >= 0:
+            members.setdefault(int(c), []).append(i)
+    ex = {(int(min(a, b)), int(max(a, b))) for a, b in np.asarray(excl_pairs).reshape(-1, 2)}
+    out = set()
+    def add(a, b):
+        p = (min(a, b), max(a, b))
+        if a != b and p not in ex:
+            out.add(p)
+    for m in members.values():
+        for x in range(len(m)):
+            for y in range(x + 1, len(m)):
+                add(m[x], m[y])
+    for c0, c1 in np.asarray(bonded if bonded is not None else np.zeros((0, 2)), dtype=np.int64).reshape(-1, 2):
+        for a in members.get(int(c0), ()):
+            for b in members.get(int(c1), ()):
+                add(a, b)
+    return np.array(sorted(out), np.int32).reshape(-1, 2)
+
+
+def immediate_forces(pos, box, q, sigma, eps, pairs, es_mode, kappa, precision=64):
+    """Forces and (LJ, Coulomb) energies of the immediate pairs, no cutoff,
+    minimum image; the same pair function as the cutoff loop."""
+    pos = _f64(pos).reshape(-1, 3)
+    f = np.zeros_like(pos)
+    pairs = np.asarray(pairs, np.int64).reshape(-1, 2)
+    if len(pairs) == 0:
+        return f, 0.0, 0.0
+    i, j = pairs[:, 0], pairs[:, 1]
+    d = pos[j] - pos[i]
+    if box is not None:
+        b = _f64(box)
+        d -= b * np.rint(d / b)
+    sig = 0.5 * (_f64(sigma)[i] + _f64(sigma)[j])
+    ep = np.sqrt(_f64(eps)[i] * _f64(eps)[j])
+    qq = _f64(q)[i] * _f64(q)[j]
+    fi, elj, ec = pair_terms(d, sig, ep, qq, es_mode, kappa, precision=precision)
+    np.add.at(f, i, fi)
+    np.add.at(f, j, -fi)
+    return f, float(elj.sum()), float(ec.sum())

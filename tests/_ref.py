@@ -14,16 +14,28 @@ def kappa_from_tol(rc, tol):
 
 def oracle_total(O, s, rc, es_mode, kappa=0.0, grid=None, ref_compat=False, nb=True, bonded=True,
                  precision=64):
-    """Forces (n,3) and the energy terms the engine reports, from the CPU oracle."""
+    """Forces (n,3) and the energy terms the engine reports, from the CPU oracle.
+    With ref_compat and compounds on the system, pairs inside a compound and
+    across bonded compounds are evaluated without a cutoff and left out of the
+    cutoff loop, as in the reference."""
     ex = s.exclusions()
     f = np.zeros((s.n, 3))
     e = {}
+    imm = None
+    if ref_compat and getattr(s, "compound", None) is not None:
+        imm = O.immediate_pairs(s.compound, s.bonded_compounds, ex)
     if nb:
-        fn, en, npairs = O.nonbonded(s.pos, s.box, s.charge, s.sigma, s.epsilon, ex, rc, es_mode, kappa,
+        ex_nb = np.concatenate([ex, imm]) if imm is not None and len(imm) else ex
+        fn, en, npairs = O.nonbonded(s.pos, s.box, s.charge, s.sigma, s.epsilon, ex_nb, rc, es_mode, kappa,
                                      precision=precision)
         f += fn
         e["lj"] = en["lj"]
         e["coulomb_real"] = en["coulomb"]
+        if imm is not None:
+            fi, elj, ec = O.immediate_forces(s.pos, s.box, s.charge, s.sigma, s.epsilon, imm, es_mode, kappa)
+            f += fi
+            e["lj"] += elj
+            e["coulomb_real"] += ec
     if grid is not None:
         if ref_compat:
             fl, er, es = O.pme(s.pos, s.charge, s.box, grid, kappa, influence=1, gather=1)

@@ -98,6 +98,34 @@ def test_ewald_pme_reference_conventions(oracle):
     check_energies(en, er)
 
 
+def test_reference_immediate_pairs_without_cutoff(oracle):
+    """ref_compat with the reference builder's compounds (config 1's chains split
+    into 32 + 20 atom compounds, one water per compound): pairs inside a
+    compound and across bonded compounds are evaluated with no cutoff
+    (EngineKernels.cuh:150-317), all others through the cutoff list; against
+    the oracle's restatement of the same rule."""
+    s = systems.config1().with_compounds()
+    rc = 1.2
+    grid = (50, 50, 80)                 # the reference's 10 points per nm
+    ex = s.exclusions()
+    imm = oracle.immediate_pairs(s.compound, s.bonded_compounds, ex)
+    d = s.pos[imm[:, 1]] - s.pos[imm[:, 0]]
+    d -= s.box * np.round(d / s.box)
+    beyond = int((np.linalg.norm(d, axis=1) > rc).sum())
+    assert len(imm) > 70000 and beyond > 1000     # pairs the cutoff alone would drop
+    e = make(s, grid=grid, cutoff=rc, electrostatics=E.ES_EWALD, ref_compat=1)
+    e.compute_forces(energy=True)
+    f = e.forces()
+    fr, er = oracle_total(oracle, s, rc, 2, 3.0 / rc, grid, ref_compat=True)
+    assert rel_rms(f, fr) < FORCE_TOL, rel_rms(f, fr)
+    check_energies(e.energies(), er)
+    # without compounds the same system gives visibly different forces: the
+    # rule is active, not absorbed by the tolerance
+    e2 = make(systems.config1(), grid=grid, cutoff=rc, electrostatics=E.ES_EWALD, ref_compat=1)
+    e2.compute_forces(energy=True)
+    assert rel_rms(e2.forces(), f) > 100 * FORCE_TOL
+
+
 def test_full_config1(oracle):
     """Config 1: chains + water, LJ per atom, Ewald + PME 48x48x80, bonds/angles/dihedrals."""
     s = systems.config1()
