@@ -66,7 +66,11 @@ extern "C" {
 #define LIMA_STATUS_PAIRLIST_OVERFLOW  0x1u
 #define LIMA_STATUS_COLUMN_OVERFLOW    0x2u
 #define LIMA_STATUS_NONFINITE          0x4u
+/* a force accumulator reached half the int64 fixed-point range (2^30 J/mol/nm):
+   overlapping atoms; the forces of that step are not trustworthy */
 #define LIMA_STATUS_FORCE_SATURATED    0x8u
+/* an atom moved more than half the Verlet buffer (skin) since the pair list was
+   built: pairs that came within the cutoff may be missing until the next build */
 #define LIMA_STATUS_MOVED_TOO_FAR      0x10u
 #define LIMA_STATUS_MLP_FALLBACK       0x20u
 
@@ -353,15 +357,19 @@ LIMA_API int lima_learned_pme_gradients(lima_engine* h, int rows, const float* x
  * device wait gave up. */
 LIMA_API int lima_learned_pme_predict(lima_engine* h, int rows, const float* features, float* out, int impl);
 
-/* Autotuner: after one untimed period per shape, times `periods` pair-list
- * periods of real MD steps (they advance the simulation), three rounds, with
- * each launch shape of the force-only pair kernel — 256
- * or 128 threads per block, with or without leaving SM room to the PME and
- * bonded kernels of the step, one or two pair-list rows' loads in flight per
- * lane — and keeps the fastest for this engine.  All shapes give identical
- * results.  *shape (may be NULL) receives the choice: bit 0 room left, bit 1
- * 128-thread blocks, bit 2 two rows in flight. */
+/* Autotuner (no counterpart in the reference, whose launch shapes are fixed):
+ * after one untimed period per shape, times `periods` pair-list periods of real
+ * MD steps (they advance the simulation), three rounds, with each of the 12
+ * launch shapes of the pair kernel — 256 or 128 threads per block, with or
+ * without leaving SM room to the PME and bonded kernels of the step, one or two
+ * pair-list rows' loads in flight per lane, or the persistent kernel whose rows
+ * and j-atoms are staged through shared memory — and keeps the fastest for
+ * this engine.  All shapes give identical results.  *shape (may be NULL)
+ * receives the choice: bit 0 room left, bit 1 128-thread blocks, bit 2 two
+ * rows in flight (bit 3 clear), bit 3 the staged persistent kernel. */
 LIMA_API int lima_autotune(lima_engine* h, int periods, int* shape);
+/* Sets the pair kernel's launch shape (0-11, as lima_autotune reports it). */
+LIMA_API int lima_set_pair_shape(lima_engine* h, int shape);
 
 /* ---------------------------------------------------------- thermostat, log */
 /* Last temperature measurement of the selected system: temperature [K], the

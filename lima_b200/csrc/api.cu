@@ -116,7 +116,7 @@ struct lima_engine {
     // launch shape of the force-only pair kernel, picked by autotune()
     int nb_shape = 0;
     bool nb_tuned = false;
-    double tune_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // per launch shape of the pair kernel
+    double tune_ms[12] = {};   // per launch shape of the pair kernel
 
     // device scratch for readback
     unsigned* d_disp = nullptr;       // [0] largest squared move since the last list build (float bits),
@@ -688,6 +688,7 @@ void lima_engine::setup() {
     D.bb_molsig = dalloc<unsigned long long>(n_clusters);
     D.pl_count = dalloc<int>(n_clusters);
     D.pl_row = dalloc<int2>((size_t)n_clusters * pl_cap);
+    D.nb_counter = dalloc<int>(1);
     D.status = dalloc<unsigned>(2);   // [0] ST_* flags, [1] largest pair-list row count a search needed
     D.energy = dalloc<long long>((size_t)ns * E_COUNT);
     D.epot = dalloc<long long>(S);
@@ -744,6 +745,7 @@ void lima_engine::setup() {
     nb.em = 0;
     ip.dt = p.dt;
     ip.integrator = p.integrator;
+    ip.half_skin2 = (float)(0.25 * (rlist - rc) * (rlist - rc));
 
     d_disp = dalloc<unsigned>(2);
     d_out_d = dalloc<double>(3 * (size_t)N);
@@ -1293,7 +1295,8 @@ void lima_engine::run_steps(int n) {
 // Every shape gives identical results, so the choice changes only the speed.
 int lima_engine::autotune(int periods) {
     const int n = std::max(1, periods) * p.nstlist;
-    constexpr int NS = 8;
+    // eight launch shapes of k_nonbonded (0-7), four of the staged kernel (8-11)
+    constexpr int NS = 12;
     double best[NS];
     for (int shape = 0; shape < NS; ++shape) {   // first use of each shape, untimed
         best[shape] = 1e300;
@@ -2151,6 +2154,15 @@ int lima_autotune(lima_engine* h, int periods, int* shape) {
         if (shape) *shape = pick;
         return LIMA_OK;
     });
+}
+
+int lima_set_pair_shape(lima_engine* h, int shape) {
+    if (!h) return LIMA_ERR_INVALID_ARG;
+    if (shape < 0 || shape > 11 || ((shape & 8) && (shape & 4)))
+        return fail(h, LIMA_ERR_INVALID_ARG, "pair kernel shape must be 0-11 (bit 2 only without bit 3)");
+    h->nb_shape = shape;
+    h->drop_graph();
+    return LIMA_OK;
 }
 
 int lima_get_thermostat(lima_engine* h, double* temperature, double* scale, int64_t* step) {

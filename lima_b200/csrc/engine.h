@@ -94,6 +94,7 @@ struct DevState {
     // pair-list rows: one per (i-cluster, j-atom) with at least one i-atom in range;
     // x = j slot, y = 8-bit i-atom mask | periodic shift code << 8
     int2* pl_row = nullptr;
+    int* nb_counter = nullptr;      // next i-cluster of the persistent (staged) pair kernel
 
     // PME
     int* pme_grid_fx = nullptr;          // fixed-point charge grid, GRID32_SCALE (all systems)
@@ -203,6 +204,7 @@ int launch_pme(const DevState& st, const PmePlan& plan, bool energy, cudaStream_
 struct IntegrateParams {
     double dt;
     int integrator;         // 0 leapfrog, 1 velocity Verlet (velocity scale: DevState::vscale)
+    float half_skin2;       // (Verlet buffer / 2)^2: a larger move since the list build is flagged
 };
 int launch_integrate(const DevState& st, const IntegrateParams& p, bool energy, cudaStream_t s);
 int launch_em_step(const DevState& st, int step, float* max_force_out_dev, cudaStream_t s);

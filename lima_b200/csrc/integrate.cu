@@ -22,6 +22,16 @@ __device__ __forceinline__ float3 load_force(const DevState& st, int s) {
                        (float)((double)st.fz[s] * inv));
 }
 
+// Flags a force accumulator at or beyond half the int64 range (2^30 J/mol/nm):
+// a single contribution there has saturated its conversion and a sum may wrap,
+// so the step's forces cannot be trusted (LIMA_STATUS_FORCE_SATURATED).
+__device__ __forceinline__ void check_saturation(const DevState& st, int s) {
+    constexpr long long LIM = 1ll << 62;
+    const long long x = st.fx[s], y = st.fy[s], z = st.fz[s];
+    if (x >= LIM || x <= -LIM || y >= LIM || y <= -LIM || z >= LIM || z <= -LIM)
+        atomicOr(st.status, ST_FORCE_SATURATED);
+}
+
 template <int INTEGRATOR, bool ENERGY>
 __global__ void k_integrate(DevState st, IntegrateParams p) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -35,6 +45,7 @@ __global__ void k_integrate(DevState st, IntegrateParams p) {
         const float im = v.w;
         const float dt = (float)p.dt;
         if (!(isfinite(F.x) && isfinite(F.y) && isfinite(F.z))) atomicOr(st.status, ST_NONFINITE);
+        check_saturation(st, s);
         double dx, dy, dz;
         if (INTEGRATOR == 0) {
             const float m = im > 0.f ? 1.f / im : 0.f;
@@ -78,6 +89,11 @@ __global__ void k_integrate(DevState st, IntegrateParams p) {
         st.pz[s] = z;
         const float q = st.xyzq[s].w;
         st.xyzq[s] = make_float4((float)x, (float)y, (float)z, q);
+        // an atom beyond half the Verlet buffer from its position at the list
+        // build may meet a partner the list does not hold
+        const float4 r = st.xyz_ref[s];
+        const float ex = (float)x - r.x, ey = (float)y - r.y, ez = (float)z - r.z;
+        if (ex * ex + ey * ey + ez * ez > p.half_skin2) atomicOr(st.status, ST_MOVED_TOO_FAR);
     }
     if (ENERGY) add_energy_fixed(st.energy, sysi, ke, E_KINETIC);
 }
@@ -99,6 +115,7 @@ int launch_integrate(const DevState& st, const IntegrateParams& p, bool energy, 
 __global__ void k_em_step(DevState st, int step) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= st.n_slots || st.orig[s] < 0) return;
+    check_saturation(st, s);
     float3 F = load_force(st, s);
     const float fmax = 1.0e6f;  // 1000 kJ/mol/nm
     const float fl = sqrtf(F.x * F.x + F.y * F.y + F.z * F.z);

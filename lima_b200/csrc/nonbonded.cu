@@ -133,9 +133,8 @@ __global__ void __launch_bounds__(256, (EN || PF || EM) ? 2 : 3) k_nonbonded(Dev
 #pragma unroll
     for (int ip = 0; ip < 4; ++ip) fix[ip] = fiy[ip] = fiz[ip] = ei[ip] = zero2;
     const f2p one2 = splat2(1.f), mtwo2 = splat2(-2.f);
-    // energy steps: per-lane packed FP32 sums of LJ, Coulomb and virial
-    // (a few tens of pairs each), converted to FP64 once per cluster
-    f2p s_elj = zero2, s_ec = zero2, s_vir = zero2;
+    // energy steps: per-lane FP64 sums of the pair energies and virial terms
+    double s_elj = 0.0, s_ec = 0.0, s_vir = 0.0;
     const size_t base = (size_t)ci * st.pl_cap;
     // one row: its mask, j slot, j position with the row's image applied, j LJ
     auto load_row = [&](int k, unsigned& bits, int& sj, float4& xj, float2& ljj) {
@@ -203,7 +202,12 @@ __global__ void __launch_bounds__(256, (EN || PF || EM) ? 2 : 3) k_nonbonded(Dev
                     // k_e q_i q_j [erfc(kappa r)/r + 2 kappa/sqrt(pi) e^{-kappa^2 r^2}] / r^2
                     //   = -qn e^{-kappa^2 r^2} (poly/r + 2 kappa/sqrt(pi)) / r^2, away from j
                     fs = fma2(mul2(qn, rinv2), mul2(ex, fma2(poly, rinv, splat2(p.two_kappa_sqrtpi))), fs);
-                    if (ENERGY) ec = sub2(zero2, mul2(mul2(qn, rinv), mul2(poly, ex)));
+                    if (ENERGY) {
+                        // energy steps take erfc from the library function (a few ulp)
+                        // rather than the 1.5e-7 absolute bound of the force's A&S form
+                        const float2 rr = up2(mul2(r2, rinv)), qr = up2(mul2(qn, rinv));
+                        ec = pk2(-qr.x * erfcf(p.kappa * rr.x), -qr.y * erfcf(p.kappa * rr.y));
+                    }
                 } else {
                     fs = fma2(mul2(qn, rinv2), rinv, fs);
                     if (ENERGY) ec = sub2(zero2, mul2(qn, rinv));
@@ -215,22 +219,26 @@ __global__ void __launch_bounds__(256, (EN || PF || EM) ? 2 : 3) k_nonbonded(Dev
                 fsv.y = fmaxf(fminf(fsv.y, 1e20f), -1e20f);
             }
             fs = pk2(oka ? fsv.x : 0.f, okb ? fsv.y : 0.f);
-            const f2p fx = mul2(fs, dx), fy = mul2(fs, dy), fz = mul2(fs, dz);
-            fix[ip] = add2(fix[ip], fx);
-            fiy[ip] = add2(fiy[ip], fy);
-            fiz[ip] = add2(fiz[ip], fz);
-            fjx = sub2(fjx, fx);
-            fjy = sub2(fjy, fy);
-            fjz = sub2(fjz, fz);
+            // force on i: fs d; on j: -fs d (both summed as +fs d, j negated at the end)
+            fix[ip] = fma2(fs, dx, fix[ip]);
+            fiy[ip] = fma2(fs, dy, fiy[ip]);
+            fiz[ip] = fma2(fs, dz, fiz[ip]);
+            fjx = fma2(fs, dx, fjx);
+            fjy = fma2(fs, dy, fjy);
+            fjz = fma2(fs, dz, fjz);
             if (ENERGY) {
                 // 4 eps s6 (s6 - 1) = (24 eps / 6) s6 (s6 - 1); dropped like the force
                 const float2 eljv = up2(mul2(mul2(eps24, splat2(1.f / 6.f)), mul2(s6, sub2(s6, one2))));
                 const float2 ecv = up2(ec);
                 const f2p elj = pk2(oka ? eljv.x : 0.f, okb ? eljv.y : 0.f);
                 const f2p ecm = pk2(oka ? ecv.x : 0.f, okb ? ecv.y : 0.f);
-                s_elj = add2(s_elj, elj);
-                s_ec = add2(s_ec, ecm);
-                s_vir = fma2(fs, r2, s_vir);   // fs is already dropped; -1/2 r_ij . f_ij = fs r^2 / 2
+                const float2 ev = up2(elj), cv = up2(ecm), vv = up2(mul2(fs, r2));
+                s_elj += (double)ev.x;
+                s_elj += (double)ev.y;
+                s_ec += (double)cv.x;
+                s_ec += (double)cv.y;
+                s_vir += (double)vv.x;
+                s_vir += (double)vv.y;   // fs is already dropped; -1/2 r_ij . f_ij = fs r^2 / 2
                 if (ATOM) {
                     const f2p eh = mul2(splat2(0.5f), add2(elj, ecm));
                     ei[ip] = add2(ei[ip], eh);
@@ -240,9 +248,9 @@ __global__ void __launch_bounds__(256, (EN || PF || EM) ? 2 : 3) k_nonbonded(Dev
         }
         if (bits) {
             const float2 x = up2(fjx), y = up2(fjy), z = up2(fjz);
-            atomic_add_fixed(st.fx + sj, to_fixed(x.x + x.y, FORCE_SCALE));
-            atomic_add_fixed(st.fy + sj, to_fixed(y.x + y.y, FORCE_SCALE));
-            atomic_add_fixed(st.fz + sj, to_fixed(z.x + z.y, FORCE_SCALE));
+            atomic_add_fixed(st.fx + sj, to_fixed(-(x.x + x.y), FORCE_SCALE));
+            atomic_add_fixed(st.fy + sj, to_fixed(-(y.x + y.y), FORCE_SCALE));
+            atomic_add_fixed(st.fz + sj, to_fixed(-(z.x + z.y), FORCE_SCALE));
             if (ATOM) {
                 const float2 e = up2(ej);
                 add_atom_energy(st.epot, sj, (double)(e.x + e.y));
@@ -306,11 +314,289 @@ __global__ void __launch_bounds__(256, (EN || PF || EM) ? 2 : 3) k_nonbonded(Dev
         if (ATOM) add_atom_energy(st.epot, si, (double)ve);
     }
     if (ENERGY) {
-        const float2 el = up2(s_elj), ecs = up2(s_ec), vr = up2(s_vir);
-        add_energy_fixed(st.energy, sysi, (double)el.x + (double)el.y, E_LJ);
-        add_energy_fixed(st.energy, sysi, (double)ecs.x + (double)ecs.y, E_COUL);
-        add_energy_fixed(st.energy, sysi, 0.5 * ((double)vr.x + (double)vr.y), E_VIRIAL);
+        add_energy_fixed(st.energy, sysi, s_elj, E_LJ);
+        add_energy_fixed(st.energy, sysi, s_ec, E_COUL);
+        add_energy_fixed(st.energy, sysi, 0.5 * s_vir, E_VIRIAL);
     }
+}
+
+// ------------------------------------------------------- staged pair kernel
+// cp.async (sm_80+ LDGSTS): copies from global to shared memory that complete
+// asynchronously; wait_all makes the calling thread's copies visible to it.
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Per warp: three stages of 32 pair-list rows and of their j-atoms' (x, y, z, q)
+// and LJ parameters, plus the i-cluster's packed atom pairs.
+constexpr int NB_STAGES = 3;
+struct alignas(16) NbWarpStage {
+    float4 xj[NB_STAGES][32];
+    float2 lj[NB_STAGES][32];
+    int2 row[NB_STAGES][32];
+    float4 xy[4], zq[4], ljp[4];
+};
+
+// The pair kernel with its list rows and j-atoms staged through shared memory.
+// The same pair arithmetic and per-lane work as k_nonbonded (one lane per list
+// row, the 8 i-atoms in packed pairs (ip, ip + 4)); what changes is how the
+// operands arrive and how clusters reach warps:
+//  * staging: while a warp works on chunk c of its cluster's list (32 rows),
+//    the j-atoms of chunk c + 1 and the rows of chunk c + 2 are already in
+//    flight as cp.async copies into the warp's shared-memory stages, so the
+//    dependent row -> j-atom loads never stall the arithmetic (each lane
+//    copies its own row and that row's j-atom, three stages deep);
+//  * persistence: a grid of a few CTAs per SM whose warps take i-clusters from
+//    a counter (atomicAdd) until the list is done, so no partial last wave;
+//  * both the i-force and the j-force sums take fs * d with one FMA each.
+// Every sum is still rounded to int64 fixed point before it is added, so the
+// results do not depend on which warp takes which cluster.
+template <int ES, int EN, bool EM>
+__global__ void __launch_bounds__(256, (EN || EM) ? 2 : 3) k_nonbonded_staged(DevState st, NbParams p, int* counter) {
+    constexpr bool ENERGY = EN > 0, ATOM = EN > 1;
+    extern __shared__ __align__(16) unsigned char nb_smem[];
+    NbWarpStage& S = reinterpret_cast<NbWarpStage*>(nb_smem)[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const f2p zero2 = splat2(0.f), one2 = splat2(1.f), mtwo2 = splat2(-2.f);
+    for (;;) {
+        int ci = 0;
+        if (lane == 0) ci = atomicAdd(counter, 1);
+        ci = __shfl_sync(0xffffffffu, ci, 0);
+        if (ci >= st.n_clusters) break;
+        const int n = min(st.pl_count[ci], st.pl_cap);
+        if (n == 0) continue;
+        const int sysi = st.cluster_sys[ci];
+        const float Lx = st.sys[sysi].boxf[0], Ly = st.sys[sysi].boxf[1], Lz = st.sys[sysi].boxf[2];
+        const size_t base = (size_t)ci * st.pl_cap;
+        const int nchunk = (n + 31) >> 5;
+        // rows of chunk 0 first: the j-atom copies need them
+        if (lane < n) cp_async8(&S.row[0][lane], &st.pl_row[base + lane]);
+        cp_async_commit();
+        if (lane < CLUSTER) {
+            const float4 x = st.xyzq[ci * CLUSTER + lane];
+            const float2 lj = st.ljp[ci * CLUSTER + lane];
+            const int ip = lane & 3, h = lane >> 2;
+            float* xy = reinterpret_cast<float*>(&S.xy[ip]);
+            float* zq = reinterpret_cast<float*>(&S.zq[ip]);
+            float* lv = reinterpret_cast<float*>(&S.ljp[ip]);
+            xy[h] = x.x;
+            xy[2 + h] = x.y;
+            zq[h] = x.z;
+            zq[2 + h] = -x.w * p.ke;  // i-charges carry minus the Coulomb constant
+            lv[h] = lj.x;
+            lv[2 + h] = 24.f * lj.y;  // the LJ force prefactor folded into the i side
+        }
+        cp_async_wait_all();
+        // j-atoms of chunk 0 and rows of chunk 1
+        if (lane < n) {
+            const int sj = S.row[0][lane].x;
+            cp_async16(&S.xj[0][lane], &st.xyzq[sj]);
+            cp_async8(&S.lj[0][lane], &st.ljp[sj]);
+        }
+        if (32 + lane < n) cp_async8(&S.row[1][lane], &st.pl_row[base + 32 + lane]);
+        cp_async_commit();
+        __syncwarp();   // the i-atoms written by lanes 0-7 are visible to the warp
+
+        f2p fix[4], fiy[4], fiz[4], ei[4];
+#pragma unroll
+        for (int ip = 0; ip < 4; ++ip) fix[ip] = fiy[ip] = fiz[ip] = ei[ip] = zero2;
+        double s_elj = 0.0, s_ec = 0.0, s_vir = 0.0;   // energy steps: per-lane FP64 sums
+        for (int c = 0; c < nchunk; ++c) {
+            const int b0 = c % NB_STAGES, b1 = (c + 1) % NB_STAGES, b2 = (c + 2) % NB_STAGES;
+            cp_async_wait_all();        // rows of c + 1 and j-atoms of c have landed
+            const int k = (c << 5) + lane;
+            const int2 row = k < n ? S.row[b0][lane] : make_int2(0, 0);
+            // next: j-atoms of chunk c + 1, rows of chunk c + 2
+            if (k + 32 < n) {
+                const int sj1 = S.row[b1][lane].x;
+                cp_async16(&S.xj[b1][lane], &st.xyzq[sj1]);
+                cp_async8(&S.lj[b1][lane], &st.ljp[sj1]);
+            }
+            if (k + 64 < n) cp_async8(&S.row[b2][lane], &st.pl_row[base + k + 64]);
+            cp_async_commit();
+
+            const unsigned bits = (unsigned)row.y & 0xffu;   // bit ii: pair (ii, this j-atom); 0 past the list
+            const unsigned img = (unsigned)row.y >> ROW_SHIFT_BIT;
+            const int sj = row.x;
+            // lanes past the list take zeros, never a stage slot's stale contents
+            // (a non-finite stale value times fs = 0 would reach the sums)
+            float4 xj = k < n ? S.xj[b0][lane] : make_float4(0.f, 0.f, 0.f, 0.f);
+            const float2 ljj = k < n ? S.lj[b0][lane] : make_float2(0.f, 0.f);
+            xj.x += fmaf((float)(img & 3u), Lx, -Lx);
+            xj.y += fmaf((float)((img >> 2) & 3u), Ly, -Ly);
+            xj.z += fmaf((float)(img >> 4), Lz, -Lz);
+            f2p fjx = zero2, fjy = zero2, fjz = zero2, ej = zero2;
+            const f2p jx = splat2(xj.x), jy = splat2(xj.y), jz = splat2(xj.z);
+            const f2p jsig = splat2(ljj.x), jeps = splat2(ljj.y), jq = splat2(xj.w);
+#pragma unroll
+            for (int ip = 0; ip < 4; ++ip) {
+                // mask bit folded into the cutoff; elements outside the mask or the
+                // cutoff (possibly non-finite: padding, stale stage slots past the
+                // list) are dropped by the select
+                const float tha = (bits >> ip) & 1u ? p.rc2 : -1.f;
+                const float thb = (bits >> (ip + 4)) & 1u ? p.rc2 : -1.f;
+                const float4 vxy = S.xy[ip], vzq = S.zq[ip], vlj = S.ljp[ip];
+                const f2p dx = sub2(jx, pk2(vxy.x, vxy.y));
+                const f2p dy = sub2(jy, pk2(vxy.z, vxy.w));
+                const f2p dz = sub2(jz, pk2(vzq.x, vzq.y));
+                const f2p r2 = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
+                const float2 r2v = up2(r2);
+                const bool oka = r2v.x <= tha, okb = r2v.y <= thb;
+                const f2p rinv = pk2(rsqrtf(r2v.x), rsqrtf(r2v.y));
+                const f2p rinv2 = mul2(rinv, rinv);
+                const f2p sig = add2(pk2(vlj.x, vlj.y), jsig);
+                const f2p eps24 = mul2(pk2(vlj.z, vlj.w), jeps);
+                const f2p s2 = mul2(mul2(sig, sig), rinv2);
+                const f2p s6 = mul2(mul2(s2, s2), s2);
+                f2p fs = mul2(mul2(eps24, s6), mul2(rinv2, fma2(s6, mtwo2, one2)));
+                if (EM) {
+                    const float2 v = up2(fs), rr = up2(mul2(r2, rinv));
+                    fs = pk2(em_lj_clamp(v.x, rr.x), em_lj_clamp(v.y, rr.y));
+                }
+                f2p ec = zero2;
+                if (ES != 0) {
+                    const f2p qn = mul2(pk2(vzq.z, vzq.w), jq);
+                    if (ES == 2) {
+                        const f2p x = mul2(mul2(r2, rinv), splat2(p.kappa));
+                        const float2 den = up2(fma2(splat2(AS_P), x, one2));
+                        const f2p t = pk2(__fdividef(1.f, den.x), __fdividef(1.f, den.y));
+                        const f2p poly = mul2(t, fma2(t, fma2(t, fma2(t, fma2(t, splat2(AS_A5), splat2(AS_A4)),
+                                                                    splat2(AS_A3)), splat2(AS_A2)), splat2(AS_A1)));
+                        const float2 xs = up2(mul2(r2, splat2(p.mk2_log2e)));
+                        const f2p ex = pk2(ex2_approx(xs.x), ex2_approx(xs.y));
+                        fs = fma2(mul2(qn, rinv2), mul2(ex, fma2(poly, rinv, splat2(p.two_kappa_sqrtpi))), fs);
+                        if (ENERGY) {
+                        // energy steps take erfc from the library function (a few ulp)
+                        // rather than the 1.5e-7 absolute bound of the force's A&S form
+                        const float2 rr = up2(mul2(r2, rinv)), qr = up2(mul2(qn, rinv));
+                        ec = pk2(-qr.x * erfcf(p.kappa * rr.x), -qr.y * erfcf(p.kappa * rr.y));
+                    }
+                    } else {
+                        fs = fma2(mul2(qn, rinv2), rinv, fs);
+                        if (ENERGY) ec = sub2(zero2, mul2(qn, rinv));
+                    }
+                }
+                float2 fsv = up2(fs);
+                if (EM) {
+                    fsv.x = fmaxf(fminf(fsv.x, 1e20f), -1e20f);
+                    fsv.y = fmaxf(fminf(fsv.y, 1e20f), -1e20f);
+                }
+                fs = pk2(oka ? fsv.x : 0.f, okb ? fsv.y : 0.f);
+                // force on i: fs d; on j: -fs d (both summed as +fs d, j negated at the end)
+                fix[ip] = fma2(fs, dx, fix[ip]);
+                fiy[ip] = fma2(fs, dy, fiy[ip]);
+                fiz[ip] = fma2(fs, dz, fiz[ip]);
+                fjx = fma2(fs, dx, fjx);
+                fjy = fma2(fs, dy, fjy);
+                fjz = fma2(fs, dz, fjz);
+                if (ENERGY) {
+                    const float2 eljv = up2(mul2(mul2(eps24, splat2(1.f / 6.f)), mul2(s6, sub2(s6, one2))));
+                    const float2 ecv = up2(ec);
+                    const f2p elj = pk2(oka ? eljv.x : 0.f, okb ? eljv.y : 0.f);
+                    const f2p ecm = pk2(oka ? ecv.x : 0.f, okb ? ecv.y : 0.f);
+                    const float2 ev = up2(elj), cv = up2(ecm), vv = up2(mul2(fs, r2));
+                    s_elj += (double)ev.x;
+                    s_elj += (double)ev.y;
+                    s_ec += (double)cv.x;
+                    s_ec += (double)cv.y;
+                    s_vir += (double)vv.x;
+                    s_vir += (double)vv.y;
+                    if (ATOM) {
+                        const f2p eh = mul2(splat2(0.5f), add2(elj, ecm));
+                        ei[ip] = add2(ei[ip], eh);
+                        ej = add2(ej, eh);
+                    }
+                }
+            }
+            if (bits) {
+                const float2 x = up2(fjx), y = up2(fjy), z = up2(fjz);
+                atomic_add_fixed(st.fx + sj, to_fixed(-(x.x + x.y), FORCE_SCALE));
+                atomic_add_fixed(st.fy + sj, to_fixed(-(y.x + y.y), FORCE_SCALE));
+                atomic_add_fixed(st.fz + sj, to_fixed(-(z.x + z.y), FORCE_SCALE));
+                if (ATOM) {
+                    const float2 e = up2(ej);
+                    add_atom_energy(st.epot, sj, (double)(e.x + e.y));
+                }
+            }
+        }
+        // i-forces: sum each of the 24 values over the warp; lane a (< 8) adds atom a's
+        float fi[CLUSTER][3], eiv[CLUSTER];
+#pragma unroll
+        for (int ip = 0; ip < 4; ++ip) {
+            const float2 x = up2(fix[ip]), y = up2(fiy[ip]), z = up2(fiz[ip]), e = up2(ei[ip]);
+            fi[ip][0] = x.x, fi[ip][1] = y.x, fi[ip][2] = z.x, eiv[ip] = e.x;
+            fi[ip + 4][0] = x.y, fi[ip + 4][1] = y.y, fi[ip + 4][2] = z.y, eiv[ip + 4] = e.y;
+        }
+#pragma unroll
+        for (int a = 0; a < CLUSTER; ++a) {
+#pragma unroll
+            for (int cc = 0; cc < 3; ++cc) {
+                float v = fi[a][cc];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                fi[a][cc] = v;
+            }
+            if (ATOM) {
+                float v = eiv[a];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                eiv[a] = v;
+            }
+        }
+        if (lane < CLUSTER) {
+            float vx = 0.f, vy = 0.f, vz = 0.f, ve = 0.f;
+#pragma unroll
+            for (int a = 0; a < CLUSTER; ++a)
+                if (a == lane) vx = fi[a][0], vy = fi[a][1], vz = fi[a][2], ve = eiv[a];
+            const int si = ci * CLUSTER + lane;
+            atomic_add_fixed(st.fx + si, to_fixed(vx, FORCE_SCALE));
+            atomic_add_fixed(st.fy + si, to_fixed(vy, FORCE_SCALE));
+            atomic_add_fixed(st.fz + si, to_fixed(vz, FORCE_SCALE));
+            if (ATOM) add_atom_energy(st.epot, si, (double)ve);
+        }
+        if (ENERGY) {
+            add_energy_fixed(st.energy, sysi, s_elj, E_LJ);
+            add_energy_fixed(st.energy, sysi, s_ec, E_COUL);
+            add_energy_fixed(st.energy, sysi, 0.5 * s_vir, E_VIRIAL);
+        }
+        cp_async_wait_all();   // nothing of this cluster still in flight into the stages
+        __syncwarp();          // every lane done with the i-atoms before the next cluster's
+    }
+}
+
+// Staged launch shapes (shape bit 3): bit 1 selects 128-thread blocks, bit 0
+// fewer resident blocks per SM (room for the PME and bonded kernels beside
+// them).  The grid is persistent: blocks per SM x SM count.
+template <int ES>
+static void launch_nb_staged(const DevState& st, const NbParams& p, bool energy, int shape, cudaStream_t s) {
+    const int tb = (shape & 2) ? 128 : 256;
+    const size_t smem = (size_t)(tb / 32) * sizeof(NbWarpStage);
+    static std::atomic<unsigned long long> attr{0ull};
+    once_per_device(attr, [] {
+        const int mx = 8 * (int)sizeof(NbWarpStage);
+        cudaFuncSetAttribute(k_nonbonded_staged<ES, 0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+        cudaFuncSetAttribute(k_nonbonded_staged<ES, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+        cudaFuncSetAttribute(k_nonbonded_staged<ES, 2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+        cudaFuncSetAttribute(k_nonbonded_staged<ES, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+    });
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int warps_per_sm = (shape & 1) ? 16 : 24;
+    const long long need = ((long long)st.n_clusters * 32 + tb - 1) / tb;
+    const unsigned grid = (unsigned)std::max(1ll, std::min<long long>(need, (long long)sms * (warps_per_sm * 32 / tb)));
+    cudaMemsetAsync(st.nb_counter, 0, sizeof(int), s);
+    if (p.em && !energy) k_nonbonded_staged<ES, 0, true><<<grid, tb, smem, s>>>(st, p, st.nb_counter);
+    else if (!energy) k_nonbonded_staged<ES, 0, false><<<grid, tb, smem, s>>>(st, p, st.nb_counter);
+    else if (st.atom_energy) k_nonbonded_staged<ES, 2, false><<<grid, tb, smem, s>>>(st, p, st.nb_counter);
+    else k_nonbonded_staged<ES, 1, false><<<grid, tb, smem, s>>>(st, p, st.nb_counter);
 }
 
 // Launch shapes of the force-only pair kernel (results are identical for every
@@ -349,6 +635,12 @@ static void launch_nb_shape(const DevState& st, const NbParams& p, bool energy, 
 }
 
 int launch_nonbonded(const DevState& st, const NbParams& p, bool energy, cudaStream_t s, int shape) {
+    if (shape & 8) {
+        if (p.es_mode == 0) launch_nb_staged<0>(st, p, energy, shape, s);
+        else if (p.es_mode == 1) launch_nb_staged<1>(st, p, energy, shape, s);
+        else launch_nb_staged<2>(st, p, energy, shape, s);
+        return 1;
+    }
     if (p.es_mode == 0) launch_nb_shape<0>(st, p, energy, shape, s);
     else if (p.es_mode == 1) launch_nb_shape<1>(st, p, energy, shape, s);
     else launch_nb_shape<2>(st, p, energy, shape, s);

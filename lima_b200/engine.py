@@ -39,7 +39,8 @@ EXPORTED = [
     "lima_get_timings", "lima_reset_timings", "lima_enable_phase_timing", "lima_pme_recip_noalloc",
     "lima_learned_pme_setup", "lima_learned_pme_collect", "lima_learned_pme_train", "lima_learned_pme_enable",
     "lima_learned_pme_eval", "lima_learned_pme_status", "lima_learned_pme_weights",
-    "lima_learned_pme_gradients", "lima_learned_pme_predict", "lima_autotune", "lima_get_thermostat", "lima_get_log", "lima_clear_log",
+    "lima_learned_pme_gradients", "lima_learned_pme_predict", "lima_autotune", "lima_set_pair_shape",
+    "lima_get_thermostat", "lima_get_log", "lima_clear_log",
 ]
 MLP_NPARAM = 80 * 128 + 128 + 2 * (128 * 128 + 128) + 128 * 8 + 8   # network parameters
 MLP_NSTATE = MLP_NPARAM + 2 * 68 + 1                               # + normalisation and output scale
@@ -139,6 +140,7 @@ def load_library(path: str = LIB_PATH):
                                                   ctypes.c_void_p]),
         "lima_learned_pme_predict": (ctypes.c_int, [h, ctypes.c_int, f32p, f32p, ctypes.c_int]),
         "lima_autotune": (ctypes.c_int, [h, ctypes.c_int, P(ctypes.c_int)]),
+        "lima_set_pair_shape": (ctypes.c_int, [h, ctypes.c_int]),
         "lima_get_thermostat": (ctypes.c_int, [h, f64p, f64p, P(ctypes.c_int64)]),
         "lima_get_log": (ctypes.c_int, [h, ctypes.c_int64, ctypes.c_int64, P(ctypes.c_int64), f32p, f32p,
                                         P(ctypes.c_int64)]),
@@ -396,9 +398,13 @@ class Engine:
     def phase_timing(self, enable: bool):
         self._check(self.lib.lima_enable_phase_timing(self.h, 1 if enable else 0))
 
+    def set_pair_shape(self, shape: int):
+        """Launch shape of the pair kernel (0-11, see lima_autotune)."""
+        self._check(self.lib.lima_set_pair_shape(self.h, int(shape)))
+
     def autotune(self, periods: int = 1) -> int:
         """Picks the fastest launch shape of the pair kernel on this system (advances
-        the simulation by 4 + 12 x periods pair-list periods); returns the shape."""
+        the simulation by 12 + 36 x periods pair-list periods); returns the shape."""
         shape = ctypes.c_int(0)
         self._check(self.lib.lima_autotune(self.h, int(periods), ctypes.byref(shape)))
         return shape.value

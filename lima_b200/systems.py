@@ -277,11 +277,11 @@ CHAIN = dict(b0=0.153, kb=2.2e5 * KJ, theta0=111.0 * DEG, kth=460.0 * KJ, kphi=0
 
 def chain_topology():
     """Bond graph of one 52-atom chain: an 8-atom linear head (0..7), tail A
-    (8..29) attached to head atom 5 and tail B (30..51) to head atom 7; every
+    (8..29) attached to head atom 6 and tail B (30..51) to head atom 7; every
     angle and proper dihedral along the bond paths."""
     bonds = [(i, i + 1) for i in range(CHAIN_HEAD - 1)]
     a0, b0 = CHAIN_HEAD, CHAIN_HEAD + CHAIN_TAIL
-    bonds.append((5, a0))
+    bonds.append((6, a0))
     bonds += [(a0 + i, a0 + i + 1) for i in range(CHAIN_TAIL - 1)]
     bonds.append((7, b0))
     bonds += [(b0 + i, b0 + i + 1) for i in range(CHAIN_TAIL - 1)]
@@ -306,29 +306,85 @@ def chain_topology():
     return (np.array(bonds, np.int32), np.array(angles, np.int32), np.array(dihedrals, np.int32))
 
 
+def _zigzag(p0, axis, zig, n):
+    """n atoms of an all-trans strand after p0: bonds of b0, bond angles theta0,
+    advancing along `axis` and zig-zagging along `zig` (both unit, orthogonal)."""
+    b = CHAIN["b0"]
+    hang = CHAIN["theta0"] / 2
+    dz, zz = b * math.sin(hang), 0.5 * b * math.cos(hang)
+    return np.array([p0 + m * dz * axis + ((-1) ** m - 1) * zz * zig for m in range(1, n + 1)])
+
+
 def _chain_geometry(up: bool, half: float) -> np.ndarray:
-    """One chain around the origin.  Each tail is a hairpin of two all-trans
-    strands; the four strands of a chain sit at (+-half, +-half) in x-y.  The
-    8 head atoms lie just beyond the strand tops, above (upper leaflet) or
-    below them."""
+    """One chain around the origin with every bond at b0.  Each tail is a
+    hairpin: an all-trans strand of 10 atoms, a 2-atom turn, a second strand
+    of 10; tail A's strands sit at x = +half, y = +-half, tail B's at
+    x = -half.  Head atoms 6 and 7 sit a bond from the first atoms of tails A
+    and B, at the bond angle to the tails' first bonds, and a bond apart;
+    atoms 5..0 continue from atom 6 outwards, every bond angle at theta0."""
     b = CHAIN["b0"]
     hang = CHAIN["theta0"] / 2
     dz = b * math.sin(hang)           # axial advance per bond of an all-trans strand
     zz = 0.5 * b * math.cos(hang)     # lateral zig-zag amplitude
     sgn = -1.0 if up else 1.0         # tails grow away from the head
-    strand = CHAIN_TAIL // 2
+    strand = (CHAIN_TAIL - 2) // 2    # 10 atoms per strand, 2 in the turn
     pos = np.zeros((CHAIN_ATOMS, 3))
-    # head: a 2 x 4 snake just beyond the tail tops; atom 5 sits over tail A's
-    # first strand (+half, +half) and atom 7 over tail B's (-half, +half)
-    snake = [(-0.1, -0.3), (0.1, -0.3), (0.1, -0.1), (-0.1, -0.1), (-0.1, 0.1), (0.1, 0.1), (0.1, 0.3), (-0.1, 0.3)]
-    for i, (hx, hy) in enumerate(snake):
-        pos[i] = [hx, hy, -sgn * 0.2]
-    for start, x0 in ((CHAIN_HEAD, half), (CHAIN_HEAD + CHAIN_TAIL, -half)):
+    # turn atoms at y = +-b/2 on the strands' x line, offset along the tail so
+    # that their bonds to the strand ends are b: zz^2 + (half - b/2)^2 + e^2 = b^2
+    e_turn = math.sqrt(max(b * b - zz * zz - (half - 0.5 * b) ** 2, 1e-4))
+    z_end = sgn * dz * (strand - 1)
+    for start, x0, side in ((CHAIN_HEAD, half, 1.0), (CHAIN_HEAD + CHAIN_TAIL, -half, -1.0)):
         for k in range(CHAIN_TAIL):
-            leg = k // strand
-            kk = k if leg == 0 else (CHAIN_TAIL - 1 - k)
-            y0 = half if leg == 0 else -half
-            pos[start + k] = [x0 + (zz if kk % 2 else -zz), y0, sgn * dz * kk]
+            if k < strand or k >= CHAIN_TAIL - strand:
+                kk = k if k < strand else (CHAIN_TAIL - 1 - k)
+                y0 = half if k < strand else -half
+                # the zig-zag starts towards the chain's centre line on both tails
+                pos[start + k] = [x0 + side * (zz if kk % 2 else -zz), y0, sgn * dz * kk]
+            else:
+                yt = 0.5 * b if k == strand else -0.5 * b
+                pos[start + k] = [x0, yt, z_end + sgn * e_turn]
+    # head atoms 6 and 7, a bond apart, each a bond from its tail's first atom
+    # at the bond angle theta0 to the tail's first bond: on the cone of such
+    # points, the one at x = +-b/2 on the outer (+y) side
+    def attach(first, second, x_target):
+        w = (second - first) / b
+        e1 = np.cross(w, [0.0, 1.0, 0.0])
+        e1 /= np.linalg.norm(e1)
+        e2 = np.cross(w, e1)
+        phis = np.linspace(-math.pi, math.pi, 20001)
+        c, s_ = math.cos(CHAIN["theta0"]), math.sin(CHAIN["theta0"])
+        pts = first + b * (c * w[None, :] + s_ * (np.cos(phis)[:, None] * e1 + np.sin(phis)[:, None] * e2))
+        ok = pts[:, 1] > first[1]
+        k = np.argmin(np.where(ok, np.abs(pts[:, 0] - x_target), np.inf))
+        return pts[k]
+    ta, tb = pos[CHAIN_HEAD], pos[CHAIN_HEAD + CHAIN_TAIL]
+    p6 = attach(ta, pos[CHAIN_HEAD + 1], 0.5 * b)
+    p7 = attach(tb, pos[CHAIN_HEAD + CHAIN_TAIL + 1], -0.5 * b)
+    pos[6], pos[7] = p6, p7
+    u = (p6 - p7) / np.linalg.norm(p6 - p7)
+    # atoms 5..0: each a bond from the previous at the bond angle theta0 to the
+    # previous bond, at the azimuth (of 72 tried) that advances furthest along
+    # the leaflet's outward normal among those at least 0.3 nm from every atom
+    # placed so far (a deterministic walk away from the tails)
+    out = np.array([0.0, 0.0, -sgn])
+    placed = [i for i in range(6, CHAIN_ATOMS)]
+    prev, cur = ta, p6
+    c, s_ = math.cos(CHAIN["theta0"]), math.sin(CHAIN["theta0"])
+    for m in range(5, -1, -1):
+        w = (prev - cur) / np.linalg.norm(prev - cur)
+        e1 = np.cross(w, out if abs(np.dot(w, out)) < 0.9 else [1.0, 0.0, 0.0])
+        e1 /= np.linalg.norm(e1)
+        e2 = np.cross(w, e1)
+        best, best_score = None, -1e9
+        for phi in np.linspace(0.0, 2 * math.pi, 72, endpoint=False):
+            cand = cur + b * (c * w + s_ * (math.cos(phi) * e1 + math.sin(phi) * e2))
+            dmin = np.linalg.norm(pos[placed] - cand, axis=1).min()
+            score = np.dot(cand - cur, out) - (10.0 if dmin < 0.3 else 0.0)
+            if score > best_score:
+                best, best_score = cand, score
+        pos[m] = best
+        placed.append(m)
+        prev, cur = cur, best
     return pos
 
 
@@ -348,7 +404,10 @@ def lipid_slab(n_chains: int = 64, n_waters: int = 4500, box=(5.0, 5.0, 8.0),
     d = box[0] / nx                   # chain spacing
     half = d / 4                      # strands on a uniform d/2 lattice
     sites = [(ix, iy) for ix in range(nx) for iy in range(nx)][:per_leaflet]
-    strand_len = (CHAIN_TAIL // 2 - 1) * CHAIN["b0"] * math.sin(CHAIN["theta0"] / 2)
+    # depth of a tail below its chain's top (strand plus turn), and 0.35 nm of
+    # clearance between one leaflet's tail turns and the other's head atoms
+    g0 = _chain_geometry(True, half)
+    strand_len = float(-g0[CHAIN_HEAD:, 2].min()) + 0.35
     zc = box[2] / 2
     z_top = zc + 0.5 * strand_len     # upper tails hang down from here
     z_bot = zc - 0.5 * strand_len     # lower tails rise from here
@@ -458,13 +517,23 @@ def _merge(a: System, b: System) -> System:
 def _chains(rng, n_chains: int, box: np.ndarray, temperature: float) -> System:
     """n_chains lipid-like chains (config-1 topology and parameters) at random
     positions and orientations."""
+    from scipy.spatial import cKDTree
+
     cb, ca, cd = chain_topology()
     geo = _chain_geometry(True, 0.21)
     geo -= geo.mean(0)
-    rot = _random_rotations(rng, n_chains)
     pos, q, s, e, bonds, angles, dihedrals = [], [], [], [], [], [], []
     for c in range(n_chains):
-        pos.append(geo @ rot[c].T + rng.uniform(0, 1, 3) * box)
+        # a random placement clear of the chains placed before (no atom pair
+        # closer than 0.4 nm across chains); the last try is kept if none is
+        for _ in range(200):
+            cand = np.mod(geo @ _random_rotations(rng, 1)[0].T + rng.uniform(0, 1, 3) * box, box)
+            if not pos:
+                break
+            d, _ = cKDTree(np.concatenate(pos), boxsize=box).query(cand, k=1)
+            if d.min() >= 0.4:
+                break
+        pos.append(cand)
         hq = rng.normal(0.0, 0.4, CHAIN_HEAD)
         hq -= hq.mean()
         qq = np.zeros(CHAIN_ATOMS)

@@ -119,11 +119,18 @@ def test_reference_immediate_pairs_without_cutoff(oracle):
     fr, er = oracle_total(oracle, s, rc, 2, 3.0 / rc, grid, ref_compat=True)
     assert rel_rms(f, fr) < FORCE_TOL, rel_rms(f, fr)
     check_energies(e.energies(), er)
-    # without compounds the same system gives visibly different forces: the
-    # rule is active, not absorbed by the tolerance
+    # Without compounds the same engine drops exactly the immediate pairs beyond
+    # the cutoff.  On this unrelaxed box their share is small next to the
+    # total (about 6 kJ/mol of LJ; ~10 J/mol/nm per chain atom, below the
+    # rounding of the 1e7 J/mol/nm near-neighbour forces the two runs evaluate
+    # in different kernels), so the LJ energy difference is checked against the
+    # oracle's value for those pairs.
     e2 = make(systems.config1(), grid=grid, cutoff=rc, electrostatics=E.ES_EWALD, ref_compat=1)
     e2.compute_forces(energy=True)
-    assert rel_rms(e2.forces(), f) > 100 * FORCE_TOL
+    far = imm[np.linalg.norm(d, axis=1) > rc]
+    _, elj_far, _ = oracle.immediate_forces(s.pos, s.box, s.charge, s.sigma, s.epsilon, far, 2, 3.0 / rc)
+    d_lj = e.energies()["lj"] - e2.energies()["lj"]
+    assert abs(d_lj - elj_far) <= 0.02 * abs(elj_far) + 2e-6 * abs(er["lj"]), (d_lj, elj_far)
 
 
 def test_full_config1(oracle):

@@ -90,9 +90,9 @@ def test_autotune_shapes_give_identical_trajectories():
     shape must give the same bits, so a tuned run equals an untuned one."""
     s = systems.water_box(1500, 3.6, seed=6, name="w")
     a, b = make(s), make(s)
-    shape = a.autotune(1)                      # 8 + 3 x 8 periods of 10 steps, energies at each period's end
-    assert 0 <= shape <= 7 and a.timings()["pair_shape"] == shape
-    for _ in range(32):
+    shape = a.autotune(1)                      # 12 + 3 x 12 periods of 10 steps, energies at each period's end
+    assert 0 <= shape <= 11 and a.timings()["pair_shape"] == shape
+    for _ in range(48):
         b.step(10)
     a.step(10)
     b.step(10)
@@ -100,6 +100,32 @@ def test_autotune_shapes_give_identical_trajectories():
     pb, vb = b.state()
     assert np.array_equal(pa, pb) and np.array_equal(va, vb)
     assert a.energies()["potential"] == b.energies()["potential"]
+
+
+@pytest.mark.parametrize("es", [E.ES_CUTOFF, E.ES_EWALD])
+def test_every_pair_kernel_shape_gives_the_same_bits(es):
+    """The eight shapes of the plain pair kernel and the four of the staged,
+    persistent one: forces (a step with a rebuild and the next one) and the
+    energies of an energy step are bitwise identical."""
+    s = systems.water_box(1500, 3.6, seed=8, name="w")
+    ref = None
+    for shape in [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11]:
+        e = Engine(cutoff=1.0, electrostatics=es, ewald_tol=1e-5, nstlist=10)
+        e.load(s, pme_grid=(30, 30, 30) if es == E.ES_EWALD else None)
+        e.set_pair_shape(shape)
+        e.compute_forces(energy=False)
+        f0 = e.forces()
+        e.step(3)
+        e.compute_forces(energy=True)
+        got = (f0, e.forces(), e.energies()["lj"], e.energies()["coulomb_real"], e.energies()["virial"])
+        e.close()
+        if ref is None:
+            ref = got
+            continue
+        for a, b in zip(got, ref):
+            assert np.array_equal(a, b), shape
+    with pytest.raises(LimaError):
+        Engine(cutoff=1.0).set_pair_shape(12)
 
 
 def test_nonfinite_state_refused_on_built_engine():
