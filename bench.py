@@ -414,6 +414,120 @@ def learned_config(args, local):
     }
 
 
+def run_c4(args, world, rank, local, dist):
+    """Config 4 across ranks: every rank partitions the whole batch's specs with
+    the same longest-processing-time rule (lima_b200.partition), generates only
+    its own systems and steps them in one batched engine, each pair-list period
+    replayed as a CUDA graph.  No collective touches the data path; the
+    device-timed step time is reduced with MAX over ranks and the per-rank step
+    latencies are gathered for the per-system percentiles."""
+    import torch
+    from lima_b200 import Engine, systems
+    from lima_b200 import engine as E
+    from lima_b200.partition import lpt_partition, step_cost
+
+    specs = systems.batch_specs(args.c4_systems)
+    costs = [step_cost(sp[1], int(math.ceil(sp[4] / 0.12)) ** 3) for sp in specs]
+    mine = lpt_partition(costs, world)[rank]
+    t0 = time.perf_counter()
+    batch = [systems.batch_system(specs[i]) for i in mine]
+    gen_s = time.perf_counter() - t0
+    eng = Engine(n_systems=len(batch), cutoff=1.0, electrostatics=E.ES_EWALD, ewald_tol=1e-5, pme_spacing=0.12,
+                 nstlist=PERIOD, dt=DT_NS, device=local, use_graphs=1)
+    for i, sy in enumerate(batch):
+        eng.select(i)
+        eng.load(sy)
+    eng.minimize(force_tol=1e5, max_steps=100)
+    shape = eng.autotune(1) if args.pair_shape < 0 else args.pair_shape
+    if args.pair_shape >= 0:
+        eng.set_pair_shape(shape)
+    eng.step(max(args.warmup, 3) * PERIOD + 1)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    n_iter = max(1, (args.steps + PERIOD - 1) // PERIOD)
+    sampler = NvmlSampler(local)
+    barrier()
+    sampler.start()
+    eng.reset_timings()
+    eng.step(n_iter * PERIOD)
+    t = eng.timings()
+    barrier()
+    clocks = sampler.stop()
+    step_s = t["step"] * 1e-6
+    launches = t["kernel_launches"]
+    lat = [step_s]
+    for _ in range(min(20, n_iter * PERIOD)):   # per-step latencies, eager single steps
+        eng.reset_timings()
+        eng.step(1)
+        lat.append(eng.timings()["step"] * 1e-6)
+    if dist is not None:
+        tt = torch.tensor([step_s], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        step_max = float(tt.item())
+        gathered = [None] * world
+        dist.all_gather_object(gathered, {"systems": len(batch), "lat": lat[1:], "atoms": sum(b.n for b in batch)})
+    else:
+        step_max = step_s
+        gathered = [{"systems": len(batch), "lat": lat[1:], "atoms": sum(b.n for b in batch)}]
+    # end to end: host states in, one batched step, host states and energies out
+    n_e2e = min(args.steps, 20)
+    pos_h = [torch.from_numpy(b.pos.astype(np.float64)).pin_memory().numpy() for b in batch]
+    vel_h = [torch.from_numpy(b.vel.astype(np.float32)).pin_memory().numpy() for b in batch]
+    for i in range(len(batch)):
+        eng.select(i)
+        eng.state(pos_h[i], vel_h[i])
+    barrier()
+    te = time.perf_counter()
+    for _ in range(n_e2e):
+        for i in range(len(batch)):
+            eng.select(i)
+            eng.set_state(pos_h[i], vel_h[i])
+        eng.step(1)
+        for i in range(len(batch)):
+            eng.select(i)
+            eng.state(pos_h[i], vel_h[i])
+        eng.energies()
+    barrier()
+    e2e_s = (time.perf_counter() - te) / n_e2e
+    if dist is not None:
+        tt = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    n_atoms = sum(b.n for b in batch)
+    eng.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    lat_all = sorted(x for g in gathered for x in g["lat"] for _ in range(g["systems"]))
+    n_sys = len(specs)
+    line = {
+        "metric": "ns_per_day", "value": n_sys * ns_per_day(step_max), "unit": "ns/day", "n_gpus": world,
+        "steps": n_iter * PERIOD, "warmup": max(args.warmup, 3) * PERIOD, "ms_per_step": step_max * 1e3,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+        "config": {"workload": f"batch{n_sys}_water_chains_pme0.12", "systems": n_sys,
+                   "atoms": sum(g["atoms"] for g in gathered), "cutoff_nm": 1.0, "pme_spacing_nm": 0.12,
+                   "nstlist": PERIOD, "dt_fs": 1.0, "parallelism": f"systems partitioned over {world} ranks (LPT)",
+                   "l2": "not flushed: the batch's working set exceeds L2; pair-list periods replay as CUDA graphs"},
+        "aggregate": "sum over systems of each system's ns/day; every system advances one step per batched step",
+        "step_latency_ms_p50": 1e3 * lat_all[len(lat_all) // 2],
+        "step_latency_ms_p99": 1e3 * lat_all[min(len(lat_all) - 1, int(0.99 * len(lat_all)))],
+        "systems_per_rank": [g["systems"] for g in gathered], "generation_s_rank0": gen_s,
+        "pair_launch_shape": shape,
+        "e2e": {"value": n_sys * ns_per_day(e2e_s), "unit": "ns/day", "h2d_bytes_per_step": n_atoms * 36,
+                "d2h_bytes_per_step": n_atoms * 36 + 15 * 8,
+                "path": "per system lima_set_state(host), one lima_step(1), per system lima_get_state(host), "
+                        "lima_get_energies (rank 0's share)"},
+        "gpu_launches": launches, "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_lima(args):
     import torch
     from lima_b200 import Engine, systems
@@ -428,6 +542,8 @@ def run_lima(args):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    if args.workload == "c4":
+        return run_c4(args, world, rank, local, dist)
 
     if args.profile_large:
         # profiling mode for the memory-bound kernels (binning and sort, bonded,
@@ -461,13 +577,15 @@ def run_lima(args):
         torch.cuda.synchronize()
         print(json.dumps({"profile_learned_steps": args.profile_learned, "timings": eng.timings()}), flush=True)
         return 0
+    if args.pair_shape >= 0:
+        eng.set_pair_shape(args.pair_shape)
     if args.profile:
         # profiling mode: set-up plus `profile` plain steps, nothing else (for ncu)
         eng.step(args.profile)
         torch.cuda.synchronize()
         print(json.dumps({"profile_steps": args.profile, "timings": eng.timings()}), flush=True)
         return 0
-    shape = eng.autotune(2)
+    shape = eng.autotune(2) if args.pair_shape < 0 else args.pair_shape
     eng.step(max(args.warmup, 3))
 
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
@@ -627,6 +745,8 @@ def main():
     ap.add_argument("--impl", default="lima", choices=["lima", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", type=int, default=0, help="only set up and run this many steps (ncu)")
+    ap.add_argument("--pair-shape", type=int, default=-1,
+                    help="launch shape of the pair kernel (0-11) instead of the autotuner's choice")
     ap.add_argument("--profile-learned", type=int, default=0,
                     help="only set up the learned correction and run this many steps with it (ncu)")
     ap.add_argument("--profile-large", type=int, default=0,
@@ -637,6 +757,10 @@ def main():
     ap.add_argument("--skip-learned", action="store_true")
     ap.add_argument("--c3-frames", type=int, default=64)
     ap.add_argument("--c3-epochs", type=int, default=20)
+    ap.add_argument("--workload", default="c2", choices=["c2", "c4"],
+                    help="c2: the 100k-atom water box (headline, replicas over ranks); c4: the 256-system batch "
+                         "partitioned over ranks")
+    ap.add_argument("--c4-systems", type=int, default=256)
     ap.add_argument("--no-cpu-other", dest="cpu_other", action="store_false",
                     help="skip the CPU baselines of the secondary workloads")
     args = ap.parse_args()

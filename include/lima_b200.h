@@ -128,6 +128,12 @@ typedef struct lima_params {
        no wrapping of positions, plain differences in every term; the box only sets the
        column grid (atoms outside it are binned at its edge); needs cutoff Coulomb or none */
     int    periodic;
+    /* dynamic pruning (no counterpart in the reference, whose list has no buffer):
+       every prune_interval steps, starting at each rebuild, the pair list is cut to
+       the rows within an inner radius rc + skin * prune_interval / nstlist of the
+       current positions, and the pair kernel walks that shorter list until the
+       next prune; 0 = off; < 0 = auto (nstlist / 2 when nstlist >= 4) */
+    int    prune_interval;
 } lima_params;
 
 typedef struct lima_energies {
@@ -255,7 +261,8 @@ LIMA_API int lima_get_pairlist(lima_engine* h, int64_t cap, int32_t* pairs, int6
  * the rows built at the last rebuild (an i-cluster of 8 atoms and one j-atom
  * in range of at least one of them), the rows the pair kernel walks each step
  * (fewer than the built rows when the list is pruned between rebuilds), the
- * atom pairs it evaluates (8 per walked row) and the pairs among them within
+ * atom pairs it evaluates (two per row for each pair of i-atoms its chunk of 32
+ * rows needs) and the pairs among them within
  * the cutoff at the current positions. */
 typedef struct lima_pairlist_stats {
     int64_t rows_built;
@@ -353,8 +360,10 @@ LIMA_API int lima_learned_pme_gradients(lima_engine* h, int rows, const float* x
 /* Network output for caller rows (features: rows x 68 raw inputs, normalised
  * with the model's statistics inside; out: rows x 3, in units of the output
  * scale), rows <= 65536.  impl 0: the tcgen05 tensor-core kernel used in
- * stepping; 1: the warp-level mma.sync kernel.  LIMA_ERR_TIMEOUT if a bounded
- * device wait gave up. */
+ * stepping; 1: the warp-level mma.sync kernel; 2: a self-test of the tcgen05
+ * kernel's bounded waits — its first layer's MMAs are withheld, so every wait
+ * for them runs out (about a second) and the call returns LIMA_ERR_TIMEOUT with
+ * the engine still usable.  LIMA_ERR_TIMEOUT if a bounded device wait gave up. */
 LIMA_API int lima_learned_pme_predict(lima_engine* h, int rows, const float* features, float* out, int impl);
 
 /* Autotuner (no counterpart in the reference, whose launch shapes are fixed):

@@ -77,6 +77,9 @@ struct lima_engine {
     bool device_ok = false;   // set-up selected p.device successfully: calls select it again
     bool state_pending = false;
     int list_age = 1 << 30;
+    int prune_every = 0;              // steps between prunes (0: no pruning)
+    double rin = 0.0;                 // inner radius of the pruned list
+    bool prune_pending = false;       // positions were handed in: prune before the next pair kernel
     int64_t step = 0;
 
     // derived
@@ -688,6 +691,18 @@ void lima_engine::setup() {
     D.bb_molsig = dalloc<unsigned long long>(n_clusters);
     D.pl_count = dalloc<int>(n_clusters);
     D.pl_row = dalloc<int2>((size_t)n_clusters * pl_cap);
+    prune_every = p.prune_interval < 0 ? (p.nstlist >= 4 ? p.nstlist / 2 : 0) : p.prune_interval;
+    if (prune_every >= p.nstlist) prune_every = 0;   // the rebuild already cuts at rc + skin
+    rin = rc + (rlist - rc) * (double)prune_every / (double)std::max(1, p.nstlist);
+    if (prune_every > 0) {
+        D.pl_count_in = dalloc<int>(n_clusters);
+        D.pl_row_in = dalloc<int2>((size_t)n_clusters * pl_cap);
+        D.walk_count = D.pl_count_in;
+        D.walk_row = D.pl_row_in;
+    } else {
+        D.walk_count = D.pl_count;
+        D.walk_row = D.pl_row;
+    }
     D.nb_counter = dalloc<int>(1);
     D.status = dalloc<unsigned>(2);   // [0] ST_* flags, [1] largest pair-list row count a search needed
     D.energy = dalloc<long long>((size_t)ns * E_COUNT);
@@ -1110,10 +1125,19 @@ void lima_engine::finish_rebuild() {
         const long long grown = std::max<long long>((long long)st.pl_cap * 3 / 2, need);
         if (grown > INT_MAX / 2) throw ApiError{LIMA_ERR_OVERFLOW, "pair list too long for one cluster"};
         const int cap = (int)((grown + 31) / 32 * 32);
-        cudaFree(st.pl_row);
-        allocs.erase(std::remove(allocs.begin(), allocs.end(), (void*)st.pl_row), allocs.end());
+        for (void* a : {(void*)st.pl_row, (void*)st.pl_row_in}) {
+            if (!a) continue;
+            cudaFree(a);
+            allocs.erase(std::remove(allocs.begin(), allocs.end(), a), allocs.end());
+        }
         st.pl_cap = cap;
         st.pl_row = dalloc<int2>((size_t)st.n_clusters * cap);
+        if (prune_every > 0) {
+            st.pl_row_in = dalloc<int2>((size_t)st.n_clusters * cap);
+            st.walk_row = st.pl_row_in;
+        } else {
+            st.walk_row = st.pl_row;
+        }
         drop_graph();
         CK(cudaMemsetAsync(st.status, 0, 2 * sizeof(unsigned), s_main));
     }
@@ -1123,6 +1147,9 @@ void lima_engine::finish_rebuild() {
 void lima_engine::rebuild(bool from_input) {
     start_rebuild(from_input);
     finish_rebuild();
+    // the walked list must follow the new build at once (a pair-list query may
+    // come before the next forces)
+    if (prune_every > 0) launches += launch_prune(st, (float)rin, s_main);
 }
 
 // The list step of forces(): when a rebuild is due, only its first part runs
@@ -1177,6 +1204,7 @@ void lima_engine::capture_period() {
         CK(cudaEventRecord(ev_pme, s_pme));
         // the period's pair search overlaps its first bonded and PME work
         if (k == 0) launches += launch_pairsearch(st, (float)rlist, s_main);
+        if (prune_every > 0 && k % prune_every == 0) launches += launch_prune(st, (float)rin, s_main);
         launches += launch_nonbonded(st, nb, false, s_main, nb_shape);
         CK(cudaStreamWaitEvent(s_main, ev_bonded, 0));
         CK(cudaStreamWaitEvent(s_main, ev_pme, 0));
@@ -1223,6 +1251,10 @@ void lima_engine::forces(bool energy, bool atom_energy) {
     }
     CK(cudaEventRecord(ev_pme, sp));
     if (search_pending) finish_rebuild();
+    if (prune_every > 0 && (list_age % prune_every == 0 || prune_pending)) {
+        launches += launch_prune(st, (float)rin, s_main);
+        prune_pending = false;
+    }
     mark(1, 0, s_main);
     launches += launch_nonbonded(st, nb, energy, s_main, nb_shape);
     mark(1, 1, s_main);
@@ -1425,6 +1457,7 @@ void lima_default_params(lima_params* p) {
     p->log_interval = 0;
     p->log_ring = 5;                // DatabuffersDeviceController::nStepsInBuffer
     p->periodic = 1;                // BoundaryConditionSelect::PBC
+    p->prune_interval = -1;         // auto: nstlist / 2
 }
 
 const char* lima_error_string(int code) {
@@ -1653,6 +1686,8 @@ int lima_set_state(lima_engine* h, const double* pos, const float* vel) {
             const double half_skin = 0.5 * (h->rlist - h->p.cutoff);
             if ((word[1] & 2u) && !((double)d2 < half_skin * half_skin))
                 h->list_age = h->p.nstlist;   // rebuild before the next forces
+            // moved atoms: the inner (pruned) list follows the new positions
+            if (word[1] & 2u) h->prune_pending = true;
             h->energy_valid = false;
             ++h->state_fast_loads;
             return LIMA_OK;
@@ -1840,22 +1875,26 @@ int lima_get_pairlist_stats(lima_engine* h, lima_pairlist_stats* out) {
             h->state_pending = false;
         }
         *out = lima_pairlist_stats{};
-        std::vector<int> cnt(h->st.n_clusters);
+        std::vector<int> cnt(h->st.n_clusters), cntw(h->st.n_clusters);
         CK(cudaMemcpyAsync(cnt.data(), h->st.pl_count, cnt.size() * sizeof(int), cudaMemcpyDeviceToHost,
                            h->s_main));
+        CK(cudaMemcpyAsync(cntw.data(), h->st.walk_count, cntw.size() * sizeof(int), cudaMemcpyDeviceToHost,
+                           h->s_main));
         unsigned long long* dcount = h->dalloc<unsigned long long>(1);
+        CK(cudaMemsetAsync(dcount, 0, sizeof(unsigned long long), h->s_main));
         launch_pairlist_dump(h->st, h->nb, 0, nullptr, dcount, h->s_main);
-        unsigned long long in_cut = 0;
-        CK(cudaMemcpyAsync(&in_cut, dcount, 8, cudaMemcpyDeviceToHost, h->s_main));
+        unsigned long long got[2] = {0, 0};
+        CK(cudaMemcpyAsync(got, dcount, 8, cudaMemcpyDeviceToHost, h->s_main));
         CK(cudaStreamSynchronize(h->s_main));
         cudaFree(dcount);
         h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), (void*)dcount), h->allocs.end());
-        long long rows = 0;
+        long long rows = 0, walked = 0;
         for (int c : cnt) rows += std::min(c, h->st.pl_cap);
+        for (int c : cntw) walked += std::min(c, h->st.pl_cap);
         out->rows_built = rows;
-        out->rows_walked = rows;
-        out->pairs_evaluated = rows * CLUSTER;
-        out->pairs_in_cutoff = (int64_t)in_cut;
+        out->rows_walked = walked;
+        out->pairs_evaluated = walked * CLUSTER;
+        out->pairs_in_cutoff = (int64_t)got[0];
         return LIMA_OK;
     });
 }
@@ -2212,7 +2251,7 @@ int lima_clear_log(lima_engine* h) {
 
 int lima_learned_pme_predict(lima_engine* h, int rows, const float* features, float* out, int impl) {
     if (!h) return LIMA_ERR_INVALID_ARG;
-    if (rows < 1 || !features || !out || impl < 0 || impl > 1)
+    if (rows < 1 || !features || !out || impl < 0 || impl > 2)
         return fail(h, LIMA_ERR_INVALID_ARG, "bad prediction arguments");
     return guarded(h, [&]() {
         if (int e = learned_ready(h)) return e;
@@ -2220,8 +2259,9 @@ int lima_learned_pme_predict(lima_engine* h, int rows, const float* features, fl
         cudaStream_t s = h->s_main;
         CK(cudaMemcpyAsync(h->batch_raw, features, (size_t)rows * MLP_IN * 4, cudaMemcpyHostToDevice, s));
         CK(cudaMemsetAsync(h->mlp.tc_err, 0, sizeof(int), s));
-        if (impl == 0)
-            h->launches += mlp_infer_tc(h->mlp, rows, h->batch_raw, h->lp_mean, h->lp_invstd, h->acts.y, h->mlp.tc_err, s);
+        if (impl == 0 || impl == 2)
+            h->launches += mlp_infer_tc(h->mlp, rows, h->batch_raw, h->lp_mean, h->lp_invstd, h->acts.y, h->mlp.tc_err, s,
+                                        impl == 2 ? 1 : 0);
         else
             h->launches += mlp_infer(h->mlp, rows, h->batch_raw, h->lp_mean, h->lp_invstd, h->acts.y, s);
         std::vector<float> y((size_t)rows * 8);

@@ -94,6 +94,14 @@ struct DevState {
     // pair-list rows: one per (i-cluster, j-atom) with at least one i-atom in range;
     // x = j slot, y = 8-bit i-atom mask | periodic shift code << 8
     int2* pl_row = nullptr;
+    // the inner list: the rows of pl_row still within r_in of one of their
+    // i-atoms at the last prune (k_prune_rows), same format and capacity
+    int* pl_count_in = nullptr;
+    int2* pl_row_in = nullptr;
+    // the list the pair kernels walk: pl_row/pl_count after a rebuild, the
+    // inner list after a prune
+    const int* walk_count = nullptr;
+    const int2* walk_row = nullptr;
     int* nb_counter = nullptr;      // next i-cluster of the persistent (staged) pair kernel
 
     // PME
@@ -148,6 +156,8 @@ constexpr int ROW_SHIFT_BIT = 8;
 int launch_rebuild(const DevState& st, float rlist, bool from_input, cudaStream_t s);
 int launch_rebuild_slots(const DevState& st, bool from_input, cudaStream_t s);   // stages 1-7
 int launch_pairsearch(const DevState& st, float rlist, cudaStream_t s);          // stage 8
+// the inner list at radius rin from the current positions (rows of the outer list)
+int launch_prune(const DevState& st, float rin, cudaStream_t s);
 // nonbonded.cu
 // shape: launch shape of the force-only kernel (bit 0 residency cap, bit 1 128-thread blocks)
 int launch_nonbonded(const DevState& st, const NbParams& p, bool energy, cudaStream_t s, int shape = 0);

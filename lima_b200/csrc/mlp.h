@@ -58,7 +58,7 @@ int mlp_infer(const MlpModel& m, int rows, const float* feat, const float* mean,
 // the same on the tcgen05 tensor cores (TMEM accumulators); *err is set if a
 // bounded wait gave up
 int mlp_infer_tc(const MlpModel& m, int rows, const float* feat, const float* mean, const float* inv_std, float* Y,
-                 int* err, cudaStream_t s);
+                 int* err, cudaStream_t s, int withhold = 0);
 int mlp_forward(const MlpModel& m, int rows, const __nv_bfloat16* X, MlpActs* acts, float* Y, cudaStream_t s);
 int mlp_train_step(MlpModel& m, int rows, const __nv_bfloat16* X, const float* T, MlpActs& a, float lr,
                    double* d_loss, cudaStream_t s);

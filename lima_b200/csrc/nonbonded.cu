@@ -82,12 +82,53 @@ __device__ __forceinline__ float ex2_approx(float x) {
     asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
 }
+// erfc for the energy of energy steps: erfc(z) = t exp(-z^2 + P(t)),
+// t = 1/(1 + z/2), P of degree 9 — the Chebyshev fit of Press, Teukolsky,
+// Vetterling & Flannery, Numerical Recipes (2nd ed.), section 6.2 ("erfcc"),
+// fractional error below 1.2e-7 for every z >= 0.  The force keeps the cheaper
+// A&S form above (its 1.5e-7 absolute bound is far inside the force tolerance);
+// a total energy needs the relative bound.  Packed: z holds two arguments.
+constexpr float NR_C0 = -1.26551223f, NR_C1 = 1.00002368f, NR_C2 = 0.37409196f, NR_C3 = 0.09678418f;
+constexpr float NR_C4 = -0.18628806f, NR_C5 = 0.27886807f, NR_C6 = -1.13520398f, NR_C7 = 1.48851587f;
+constexpr float NR_C8 = -0.82215223f, NR_C9 = 0.17087277f;
+
+// 1/sqrt(x) and 1/x, the hardware approximations with subnormal inputs and
+// results flushed to zero: the pair kernel's r^2 (>= 1e-4 nm^2 for any pair
+// that is kept) and 1 + p kappa r are never subnormal, and the flush spares the
+// subnormal fix-up instructions of the non-flushing forms in the inner loop
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float rcp_ftz(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+__device__ __forceinline__ f2p erfc_nr2(f2p z) {
+    const float2 d = up2(fma2(z, splat2(0.5f), splat2(1.f)));
+    const f2p t = pk2(rcp_ftz(d.x), rcp_ftz(d.y));
+    f2p poly = fma2(t, splat2(NR_C9), splat2(NR_C8));
+    poly = fma2(poly, t, splat2(NR_C7));
+    poly = fma2(poly, t, splat2(NR_C6));
+    poly = fma2(poly, t, splat2(NR_C5));
+    poly = fma2(poly, t, splat2(NR_C4));
+    poly = fma2(poly, t, splat2(NR_C3));
+    poly = fma2(poly, t, splat2(NR_C2));
+    poly = fma2(poly, t, splat2(NR_C1));
+    poly = fma2(poly, t, splat2(NR_C0));
+    // (-z^2 + P) log2(e), then 2^x
+    const float2 e = up2(mul2(fma2(mul2(z, z), splat2(-1.f), poly), splat2(1.4426950408889634f)));
+    return mul2(t, pk2(ex2_approx(e.x), ex2_approx(e.y)));
+}
 
 // Work mapping: one warp per i-cluster; the warp takes its list 32 rows at a
 // time and each lane owns one row: a j-atom whose 8-bit mask names the i-atoms
 // it interacts with (rows whose mask would be empty are not in the list, so no
 // lane works on a j-atom out of range of the whole i-cluster).  A lane walks the
-// 8 i-atoms two at a time, (ip, ip + 4) for ip = 0..3, in packed FP32 (read as
+// 8 i-atoms two at a time, (2 ip, 2 ip + 1) for ip = 0..3, in packed FP32 (read as
 // float4 pairs from shared memory), keeps its j-atom's force in a packed
 // register and adds it once per row; the i-forces live in 12 packed registers
 // per lane and are reduced across the warp once, after the list.
@@ -101,7 +142,7 @@ __device__ __forceinline__ float ex2_approx(float x) {
 template <int ES, int EN, bool PF, bool EM = false>
 __global__ void __launch_bounds__(256, (EN || PF || EM) ? 2 : 3) k_nonbonded(DevState st, NbParams p) {
     constexpr bool ENERGY = EN > 0, ATOM = EN > 1;
-    // per warp, i-atom pairs (ip, ip + 4): (x0, x1, y0, y1), (z0, z1, -q0 ke, -q1 ke),
+    // per warp, i-atom pairs (2 ip, 2 ip + 1): (x0, x1, y0, y1), (z0, z1, -q0 ke, -q1 ke),
     // (sigma0/2, sigma1/2, 24 sqrt(eps0), 24 sqrt(eps1))
     __shared__ float4 s_xy[8][4], s_zq[8][4], s_lj[8][4];
     const int wib = threadIdx.x >> 5;
@@ -109,14 +150,14 @@ __global__ void __launch_bounds__(256, (EN || PF || EM) ? 2 : 3) k_nonbonded(Dev
     const int lane = threadIdx.x & 31;
     if (warp >= st.n_clusters) return;
     const int ci = warp;
-    const int n = st.pl_count[ci];
+    const int n = min(st.walk_count[ci], st.pl_cap);
     if (n == 0) return;
     const int sysi = st.cluster_sys[ci];
     const float Lx = st.sys[sysi].boxf[0], Ly = st.sys[sysi].boxf[1], Lz = st.sys[sysi].boxf[2];
     if (lane < CLUSTER) {
         const float4 x = st.xyzq[ci * CLUSTER + lane];
         const float2 lj = st.ljp[ci * CLUSTER + lane];
-        const int ip = lane & 3, h = lane >> 2;
+        const int ip = lane >> 1, h = lane & 1;   // pair ip holds atoms 2 ip and 2 ip + 1
         float* xy = reinterpret_cast<float*>(&s_xy[wib][ip]);
         float* zq = reinterpret_cast<float*>(&s_zq[wib][ip]);
         float* lv = reinterpret_cast<float*>(&s_lj[wib][ip]);
@@ -143,7 +184,7 @@ __global__ void __launch_bounds__(256, (EN || PF || EM) ? 2 : 3) k_nonbonded(Dev
         xj = make_float4(0.f, 0.f, 0.f, 0.f);
         ljj = make_float2(0.f, 0.f);
         if (k < n) {
-            const int2 row = st.pl_row[base + k];
+            const int2 row = st.walk_row[base + k];
             bits = (unsigned)row.y & 0xffu;   // bit ii: pair (ii, this j-atom)
             const unsigned img = (unsigned)row.y >> ROW_SHIFT_BIT;
             sj = row.x;
@@ -159,14 +200,16 @@ __global__ void __launch_bounds__(256, (EN || PF || EM) ? 2 : 3) k_nonbonded(Dev
         f2p fjx = zero2, fjy = zero2, fjz = zero2, ej = zero2;
         const f2p jx = splat2(xj.x), jy = splat2(xj.y), jz = splat2(xj.z);
         const f2p jsig = splat2(ljj.x), jeps = splat2(ljj.y), jq = splat2(xj.w);
+        f2p r_elj = zero2, r_ec = zero2, r_vir = zero2;   // the row's energy sums (energy steps)
 #pragma unroll
         for (int ip = 0; ip < 4; ++ip) {
             // the mask bit of each element folded into its cutoff: rc^2, or -1 (never met).
-            // Every lane evaluates both elements (a whole-warp skip almost never
-            // happens), and elements outside the mask or the cutoff — possibly
-            // non-finite, e.g. a padding slot at distance 0 — are dropped by the select.
-            const float tha = (bits >> ip) & 1u ? p.rc2 : -1.f;
-            const float thb = (bits >> (ip + 4)) & 1u ? p.rc2 : -1.f;
+            // Every lane evaluates both elements of every pair (straight-line code over
+            // the four pairs, which the scheduler interleaves), and elements outside the
+            // mask or the cutoff — possibly non-finite, e.g. a padding slot at distance
+            // 0 — are dropped by the select.
+            const float tha = (bits >> (2 * ip)) & 1u ? p.rc2 : -1.f;
+            const float thb = (bits >> (2 * ip + 1)) & 1u ? p.rc2 : -1.f;
             const float4 vxy = s_xy[wib][ip], vzq = s_zq[wib][ip], vlj = s_lj[wib][ip];
             const f2p dx = sub2(jx, pk2(vxy.x, vxy.y));
             const f2p dy = sub2(jy, pk2(vxy.z, vxy.w));
@@ -174,7 +217,7 @@ __global__ void __launch_bounds__(256, (EN || PF || EM) ? 2 : 3) k_nonbonded(Dev
             const f2p r2 = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
             const float2 r2v = up2(r2);
             const bool oka = r2v.x <= tha, okb = r2v.y <= thb;
-            const f2p rinv = pk2(rsqrtf(r2v.x), rsqrtf(r2v.y));
+            const f2p rinv = pk2(rsqrt_ftz(r2v.x), rsqrt_ftz(r2v.y));
             const f2p rinv2 = mul2(rinv, rinv);
             const f2p sig = add2(pk2(vlj.x, vlj.y), jsig);
             const f2p eps24 = mul2(pk2(vlj.z, vlj.w), jeps);
@@ -193,7 +236,7 @@ __global__ void __launch_bounds__(256, (EN || PF || EM) ? 2 : 3) k_nonbonded(Dev
                 if (ES == 2) {
                     const f2p x = mul2(mul2(r2, rinv), splat2(p.kappa));   // kappa r
                     const float2 den = up2(fma2(splat2(AS_P), x, one2));
-                    const f2p t = pk2(__fdividef(1.f, den.x), __fdividef(1.f, den.y));
+                    const f2p t = pk2(rcp_ftz(den.x), rcp_ftz(den.y));
                     // erfc(kappa r) = poly e^{-kappa^2 r^2}
                     const f2p poly = mul2(t, fma2(t, fma2(t, fma2(t, fma2(t, splat2(AS_A5), splat2(AS_A4)),
                                                                 splat2(AS_A3)), splat2(AS_A2)), splat2(AS_A1)));
@@ -203,10 +246,8 @@ __global__ void __launch_bounds__(256, (EN || PF || EM) ? 2 : 3) k_nonbonded(Dev
                     //   = -qn e^{-kappa^2 r^2} (poly/r + 2 kappa/sqrt(pi)) / r^2, away from j
                     fs = fma2(mul2(qn, rinv2), mul2(ex, fma2(poly, rinv, splat2(p.two_kappa_sqrtpi))), fs);
                     if (ENERGY) {
-                        // energy steps take erfc from the library function (a few ulp)
-                        // rather than the 1.5e-7 absolute bound of the force's A&S form
-                        const float2 rr = up2(mul2(r2, rinv)), qr = up2(mul2(qn, rinv));
-                        ec = pk2(-qr.x * erfcf(p.kappa * rr.x), -qr.y * erfcf(p.kappa * rr.y));
+                        // energy steps: the relative-error erfc above for the energy
+                        ec = mul2(mul2(qn, rinv), mul2(splat2(-1.f), erfc_nr2(x)));
                     }
                 } else {
                     fs = fma2(mul2(qn, rinv2), rinv, fs);
@@ -232,19 +273,22 @@ __global__ void __launch_bounds__(256, (EN || PF || EM) ? 2 : 3) k_nonbonded(Dev
                 const float2 ecv = up2(ec);
                 const f2p elj = pk2(oka ? eljv.x : 0.f, okb ? eljv.y : 0.f);
                 const f2p ecm = pk2(oka ? ecv.x : 0.f, okb ? ecv.y : 0.f);
-                const float2 ev = up2(elj), cv = up2(ecm), vv = up2(mul2(fs, r2));
-                s_elj += (double)ev.x;
-                s_elj += (double)ev.y;
-                s_ec += (double)cv.x;
-                s_ec += (double)cv.y;
-                s_vir += (double)vv.x;
-                s_vir += (double)vv.y;   // fs is already dropped; -1/2 r_ij . f_ij = fs r^2 / 2
+                // the row's sums in packed FP32 (at most 8 terms), then FP64 per row
+                r_elj = add2(r_elj, elj);
+                r_ec = add2(r_ec, ecm);
+                r_vir = fma2(fs, r2, r_vir);   // fs is already dropped; -1/2 r_ij . f_ij = fs r^2 / 2
                 if (ATOM) {
                     const f2p eh = mul2(splat2(0.5f), add2(elj, ecm));
                     ei[ip] = add2(ei[ip], eh);
                     ej = add2(ej, eh);
                 }
             }
+        }
+        if (ENERGY) {
+            const float2 a = up2(r_elj), c = up2(r_ec), v = up2(r_vir);
+            s_elj += (double)a.x + (double)a.y;
+            s_ec += (double)c.x + (double)c.y;
+            s_vir += (double)v.x + (double)v.y;
         }
         if (bits) {
             const float2 x = up2(fjx), y = up2(fjy), z = up2(fjz);
@@ -283,8 +327,8 @@ __global__ void __launch_bounds__(256, (EN || PF || EM) ? 2 : 3) k_nonbonded(Dev
 #pragma unroll
     for (int ip = 0; ip < 4; ++ip) {
         const float2 x = up2(fix[ip]), y = up2(fiy[ip]), z = up2(fiz[ip]), e = up2(ei[ip]);
-        fi[ip][0] = x.x, fi[ip][1] = y.x, fi[ip][2] = z.x, eiv[ip] = e.x;
-        fi[ip + 4][0] = x.y, fi[ip + 4][1] = y.y, fi[ip + 4][2] = z.y, eiv[ip + 4] = e.y;
+        fi[2 * ip][0] = x.x, fi[2 * ip][1] = y.x, fi[2 * ip][2] = z.x, eiv[2 * ip] = e.x;
+        fi[2 * ip + 1][0] = x.y, fi[2 * ip + 1][1] = y.y, fi[2 * ip + 1][2] = z.y, eiv[2 * ip + 1] = e.y;
     }
 #pragma unroll
     for (int a = 0; a < CLUSTER; ++a) {
@@ -346,7 +390,7 @@ struct alignas(16) NbWarpStage {
 
 // The pair kernel with its list rows and j-atoms staged through shared memory.
 // The same pair arithmetic and per-lane work as k_nonbonded (one lane per list
-// row, the 8 i-atoms in packed pairs (ip, ip + 4)); what changes is how the
+// row, the 8 i-atoms in packed pairs (2 ip, 2 ip + 1)); what changes is how the
 // operands arrive and how clusters reach warps:
 //  * staging: while a warp works on chunk c of its cluster's list (32 rows),
 //    the j-atoms of chunk c + 1 and the rows of chunk c + 2 are already in
@@ -370,19 +414,19 @@ __global__ void __launch_bounds__(256, (EN || EM) ? 2 : 3) k_nonbonded_staged(De
         if (lane == 0) ci = atomicAdd(counter, 1);
         ci = __shfl_sync(0xffffffffu, ci, 0);
         if (ci >= st.n_clusters) break;
-        const int n = min(st.pl_count[ci], st.pl_cap);
+        const int n = min(st.walk_count[ci], st.pl_cap);
         if (n == 0) continue;
         const int sysi = st.cluster_sys[ci];
         const float Lx = st.sys[sysi].boxf[0], Ly = st.sys[sysi].boxf[1], Lz = st.sys[sysi].boxf[2];
         const size_t base = (size_t)ci * st.pl_cap;
         const int nchunk = (n + 31) >> 5;
         // rows of chunk 0 first: the j-atom copies need them
-        if (lane < n) cp_async8(&S.row[0][lane], &st.pl_row[base + lane]);
+        if (lane < n) cp_async8(&S.row[0][lane], &st.walk_row[base + lane]);
         cp_async_commit();
         if (lane < CLUSTER) {
             const float4 x = st.xyzq[ci * CLUSTER + lane];
             const float2 lj = st.ljp[ci * CLUSTER + lane];
-            const int ip = lane & 3, h = lane >> 2;
+            const int ip = lane >> 1, h = lane & 1;   // pair ip holds atoms 2 ip and 2 ip + 1
             float* xy = reinterpret_cast<float*>(&S.xy[ip]);
             float* zq = reinterpret_cast<float*>(&S.zq[ip]);
             float* lv = reinterpret_cast<float*>(&S.ljp[ip]);
@@ -400,7 +444,7 @@ __global__ void __launch_bounds__(256, (EN || EM) ? 2 : 3) k_nonbonded_staged(De
             cp_async16(&S.xj[0][lane], &st.xyzq[sj]);
             cp_async8(&S.lj[0][lane], &st.ljp[sj]);
         }
-        if (32 + lane < n) cp_async8(&S.row[1][lane], &st.pl_row[base + 32 + lane]);
+        if (32 + lane < n) cp_async8(&S.row[1][lane], &st.walk_row[base + 32 + lane]);
         cp_async_commit();
         __syncwarp();   // the i-atoms written by lanes 0-7 are visible to the warp
 
@@ -419,7 +463,7 @@ __global__ void __launch_bounds__(256, (EN || EM) ? 2 : 3) k_nonbonded_staged(De
                 cp_async16(&S.xj[b1][lane], &st.xyzq[sj1]);
                 cp_async8(&S.lj[b1][lane], &st.ljp[sj1]);
             }
-            if (k + 64 < n) cp_async8(&S.row[b2][lane], &st.pl_row[base + k + 64]);
+            if (k + 64 < n) cp_async8(&S.row[b2][lane], &st.walk_row[base + k + 64]);
             cp_async_commit();
 
             const unsigned bits = (unsigned)row.y & 0xffu;   // bit ii: pair (ii, this j-atom); 0 past the list
@@ -435,13 +479,13 @@ __global__ void __launch_bounds__(256, (EN || EM) ? 2 : 3) k_nonbonded_staged(De
             f2p fjx = zero2, fjy = zero2, fjz = zero2, ej = zero2;
             const f2p jx = splat2(xj.x), jy = splat2(xj.y), jz = splat2(xj.z);
             const f2p jsig = splat2(ljj.x), jeps = splat2(ljj.y), jq = splat2(xj.w);
+            f2p r_elj = zero2, r_ec = zero2, r_vir = zero2;   // the row's energy sums (energy steps)
 #pragma unroll
             for (int ip = 0; ip < 4; ++ip) {
                 // mask bit folded into the cutoff; elements outside the mask or the
-                // cutoff (possibly non-finite: padding, stale stage slots past the
-                // list) are dropped by the select
-                const float tha = (bits >> ip) & 1u ? p.rc2 : -1.f;
-                const float thb = (bits >> (ip + 4)) & 1u ? p.rc2 : -1.f;
+                // cutoff (possibly non-finite: padding) are dropped by the select
+                const float tha = (bits >> (2 * ip)) & 1u ? p.rc2 : -1.f;
+                const float thb = (bits >> (2 * ip + 1)) & 1u ? p.rc2 : -1.f;
                 const float4 vxy = S.xy[ip], vzq = S.zq[ip], vlj = S.ljp[ip];
                 const f2p dx = sub2(jx, pk2(vxy.x, vxy.y));
                 const f2p dy = sub2(jy, pk2(vxy.z, vxy.w));
@@ -449,7 +493,7 @@ __global__ void __launch_bounds__(256, (EN || EM) ? 2 : 3) k_nonbonded_staged(De
                 const f2p r2 = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
                 const float2 r2v = up2(r2);
                 const bool oka = r2v.x <= tha, okb = r2v.y <= thb;
-                const f2p rinv = pk2(rsqrtf(r2v.x), rsqrtf(r2v.y));
+                const f2p rinv = pk2(rsqrt_ftz(r2v.x), rsqrt_ftz(r2v.y));
                 const f2p rinv2 = mul2(rinv, rinv);
                 const f2p sig = add2(pk2(vlj.x, vlj.y), jsig);
                 const f2p eps24 = mul2(pk2(vlj.z, vlj.w), jeps);
@@ -466,17 +510,15 @@ __global__ void __launch_bounds__(256, (EN || EM) ? 2 : 3) k_nonbonded_staged(De
                     if (ES == 2) {
                         const f2p x = mul2(mul2(r2, rinv), splat2(p.kappa));
                         const float2 den = up2(fma2(splat2(AS_P), x, one2));
-                        const f2p t = pk2(__fdividef(1.f, den.x), __fdividef(1.f, den.y));
+                        const f2p t = pk2(rcp_ftz(den.x), rcp_ftz(den.y));
                         const f2p poly = mul2(t, fma2(t, fma2(t, fma2(t, fma2(t, splat2(AS_A5), splat2(AS_A4)),
                                                                     splat2(AS_A3)), splat2(AS_A2)), splat2(AS_A1)));
                         const float2 xs = up2(mul2(r2, splat2(p.mk2_log2e)));
                         const f2p ex = pk2(ex2_approx(xs.x), ex2_approx(xs.y));
                         fs = fma2(mul2(qn, rinv2), mul2(ex, fma2(poly, rinv, splat2(p.two_kappa_sqrtpi))), fs);
                         if (ENERGY) {
-                        // energy steps take erfc from the library function (a few ulp)
-                        // rather than the 1.5e-7 absolute bound of the force's A&S form
-                        const float2 rr = up2(mul2(r2, rinv)), qr = up2(mul2(qn, rinv));
-                        ec = pk2(-qr.x * erfcf(p.kappa * rr.x), -qr.y * erfcf(p.kappa * rr.y));
+                        // energy steps: the relative-error erfc above for the energy
+                        ec = mul2(mul2(qn, rinv), mul2(splat2(-1.f), erfc_nr2(x)));
                     }
                     } else {
                         fs = fma2(mul2(qn, rinv2), rinv, fs);
@@ -501,19 +543,21 @@ __global__ void __launch_bounds__(256, (EN || EM) ? 2 : 3) k_nonbonded_staged(De
                     const float2 ecv = up2(ec);
                     const f2p elj = pk2(oka ? eljv.x : 0.f, okb ? eljv.y : 0.f);
                     const f2p ecm = pk2(oka ? ecv.x : 0.f, okb ? ecv.y : 0.f);
-                    const float2 ev = up2(elj), cv = up2(ecm), vv = up2(mul2(fs, r2));
-                    s_elj += (double)ev.x;
-                    s_elj += (double)ev.y;
-                    s_ec += (double)cv.x;
-                    s_ec += (double)cv.y;
-                    s_vir += (double)vv.x;
-                    s_vir += (double)vv.y;
+                    r_elj = add2(r_elj, elj);
+                    r_ec = add2(r_ec, ecm);
+                    r_vir = fma2(fs, r2, r_vir);
                     if (ATOM) {
                         const f2p eh = mul2(splat2(0.5f), add2(elj, ecm));
                         ei[ip] = add2(ei[ip], eh);
                         ej = add2(ej, eh);
                     }
                 }
+            }
+            if (ENERGY) {
+                const float2 a = up2(r_elj), c = up2(r_ec), v = up2(r_vir);
+                s_elj += (double)a.x + (double)a.y;
+                s_ec += (double)c.x + (double)c.y;
+                s_vir += (double)v.x + (double)v.y;
             }
             if (bits) {
                 const float2 x = up2(fjx), y = up2(fjy), z = up2(fjz);
@@ -531,8 +575,8 @@ __global__ void __launch_bounds__(256, (EN || EM) ? 2 : 3) k_nonbonded_staged(De
 #pragma unroll
         for (int ip = 0; ip < 4; ++ip) {
             const float2 x = up2(fix[ip]), y = up2(fiy[ip]), z = up2(fiz[ip]), e = up2(ei[ip]);
-            fi[ip][0] = x.x, fi[ip][1] = y.x, fi[ip][2] = z.x, eiv[ip] = e.x;
-            fi[ip + 4][0] = x.y, fi[ip + 4][1] = y.y, fi[ip + 4][2] = z.y, eiv[ip + 4] = e.y;
+            fi[2 * ip][0] = x.x, fi[2 * ip][1] = y.x, fi[2 * ip][2] = z.x, eiv[2 * ip] = e.x;
+            fi[2 * ip + 1][0] = x.y, fi[2 * ip + 1][1] = y.y, fi[2 * ip + 1][2] = z.y, eiv[2 * ip + 1] = e.y;
         }
 #pragma unroll
         for (int a = 0; a < CLUSTER; ++a) {
@@ -792,12 +836,12 @@ __global__ void k_pairlist_dump(DevState st, NbParams p, long long cap, int* out
     const int lane = threadIdx.x & 31;
     if (warp >= st.n_clusters) return;
     const int ci = warp;
-    const int n = st.pl_count[ci];
+    const int n = min(st.walk_count[ci], st.pl_cap);
     const int sysi = st.cluster_sys[ci];
     const float Lx = st.sys[sysi].boxf[0], Ly = st.sys[sysi].boxf[1], Lz = st.sys[sysi].boxf[2];
     const size_t base = (size_t)ci * st.pl_cap;
     for (int k = lane; k < n; k += 32) {
-        const int2 row = st.pl_row[base + k];
+        const int2 row = st.walk_row[base + k];
         const int sj = row.x;
         const unsigned img = (unsigned)row.y >> ROW_SHIFT_BIT;
         const int3 sh = make_int3((int)(img & 3u) - 1, (int)((img >> 2) & 3u) - 1, (int)(img >> 4) - 1);

@@ -61,7 +61,8 @@ class Params(ctypes.Structure):
                 ("thermostat_scalar", ctypes.c_double), ("exclude_bonded", ctypes.c_int),
                 ("use_graphs", ctypes.c_int), ("apply_thermostat", ctypes.c_int),
                 ("thermostat_interval", ctypes.c_int), ("target_temperature", ctypes.c_double),
-                ("log_interval", ctypes.c_int), ("log_ring", ctypes.c_int), ("periodic", ctypes.c_int)]
+                ("log_interval", ctypes.c_int), ("log_ring", ctypes.c_int), ("periodic", ctypes.c_int),
+                ("prune_interval", ctypes.c_int)]
 
 
 class Energies(ctypes.Structure):
@@ -485,7 +486,8 @@ class LearnedPME:
 
     def predict(self, features, impl: int = 0) -> np.ndarray:
         """Network output (rows, 3) for raw feature rows (rows, 68); impl 0 = tcgen05
-        tensor-core kernel, 1 = warp-level mma.sync kernel."""
+        tensor-core kernel, 1 = warp-level mma.sync kernel, 2 = the tcgen05 kernel's
+        bounded-wait self-test (raises LimaError LIMA_ERR_TIMEOUT)."""
         x, xp = _f32(features, 68)
         y = np.zeros((len(x), 3), np.float32)
         self.engine._check(self.lib.lima_learned_pme_predict(self.engine.h, len(x), xp, _f32(y)[1], int(impl)))

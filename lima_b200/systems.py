@@ -589,13 +589,28 @@ def water_with_chains(n_atoms: int, n_chains: int, density: float = 33.4, seed: 
     return _merge(ch, w2)
 
 
-def batch_systems(n_systems=256, seed=20241203, lo=1500, hi=30000, density=33.4):
-    """Config 4: atom counts log-uniform in [lo, hi] from a seed; each a water box
-    at the given density with 0-4 chains inserted at random positions."""
+def batch_specs(n_systems=256, seed=20241203, lo=1500, hi=30000, density=33.4):
+    """Config 4's systems as (index, atom count, chain count, seed, edge [nm]):
+    atom counts log-uniform in [lo, hi] from a seed, 0-4 chains each.  Cheap, so
+    that every rank of a multi-GPU run can partition the whole batch and then
+    generate only its own systems (each system has its own seed)."""
     rng = np.random.default_rng(seed)
     out = []
     for s in range(n_systems):
         n_atoms = int(math.exp(rng.uniform(math.log(lo), math.log(hi))))
         n_chains = int(rng.integers(0, 5))
-        out.append(water_with_chains(n_atoms, n_chains, density, seed=seed + 1 + s, name=f"batch{s}"))
+        n_w = max(8, n_atoms // 3)
+        out.append((s, n_atoms, n_chains, seed + 1 + s, (n_w / density) ** (1.0 / 3.0)))
     return out
+
+
+def batch_system(spec, density=33.4) -> System:
+    """One config-4 system from its batch_specs entry."""
+    s, n_atoms, n_chains, sseed, _ = spec
+    return water_with_chains(n_atoms, n_chains, density, seed=sseed, name=f"batch{s}")
+
+
+def batch_systems(n_systems=256, seed=20241203, lo=1500, hi=30000, density=33.4):
+    """Config 4: atom counts log-uniform in [lo, hi] from a seed; each a water box
+    at the given density with 0-4 chains inserted at random positions."""
+    return [batch_system(sp, density) for sp in batch_specs(n_systems, seed, lo, hi, density)]

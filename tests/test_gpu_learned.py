@@ -136,3 +136,27 @@ def test_inference_kernels_match_oracle(oracle):
     assert np.sqrt(((y_mma - ref) ** 2).mean()) < 2e-2 * scale
     assert np.sqrt(((y_tc - ref) ** 2).mean()) < 2e-2 * scale
     assert np.sqrt(((y_tc - y_mma) ** 2).mean()) < 1e-2 * scale
+
+
+def test_tensor_core_wait_timeout_is_reported_and_engine_recovers():
+    """The tcgen05 inference kernel's waits on its MMA completion are bounded.
+    In the self-test mode (impl 2) its first layer's MMAs are withheld, so the
+    waits run out with nothing in flight: the call returns LIMA_ERR_TIMEOUT,
+    the kernel has released its tensor memory, and the engine keeps working —
+    the same rows predict as before and the engine steps on."""
+    from lima_b200 import LimaError
+
+    s, e, lp = small_engine(frames=2)
+    e.step(5)
+    lp.collect()
+    lp.train(epochs=1, batch=1024, seed=1)
+    rng = np.random.default_rng(3)
+    feats = rng.normal(size=(100, 68)).astype(np.float32)   # one CTA's tile
+    before = lp.predict(feats, impl=0)
+    with pytest.raises(LimaError) as ex:
+        lp.predict(feats, impl=2)
+    assert ex.value.code == 5      # LIMA_ERR_TIMEOUT
+    after = lp.predict(feats, impl=0)
+    assert np.array_equal(before, after)
+    e.step(10)
+    assert np.isfinite(e.energies()["total"])

@@ -152,7 +152,10 @@ def test_bonded_all_terms(oracle):
     s = systems.config1()
     rng = np.random.default_rng(3)
     heads = np.arange(64) * 52
-    s.impropers = np.stack([heads + 1, heads + 0, heads + 2, heads + 3], 1).astype(np.int32)
+    # around head atom 6, the branch point of the head and tail A: angles between
+    # the two planes of 75-108 degrees (an improper near 0 or 180 degrees puts
+    # acos at its ill-conditioned ends in either precision)
+    s.impropers = np.stack([heads + 5, heads + 6, heads + 7, heads + 8], 1).astype(np.int32)
     s.improper_par = np.stack([rng.uniform(-0.3, 0.3, 64), rng.uniform(1e4, 5e4, 64)], 1).astype(np.float32)
     s.pairbonds = np.stack([heads + 8, heads + 11], 1).astype(np.int32)
     s.pair_par = np.tile([0.34, 700.0], (64, 1)).astype(np.float32)
