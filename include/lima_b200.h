@@ -132,7 +132,7 @@ typedef struct lima_params {
        every prune_interval steps, starting at each rebuild, the pair list is cut to
        the rows within an inner radius rc + skin * prune_interval / nstlist of the
        current positions, and the pair kernel walks that shorter list until the
-       next prune; 0 = off; < 0 = auto (nstlist / 2 when nstlist >= 4) */
+       next prune; 0 = off; < 0 = auto (every 2 steps when nstlist >= 4) */
     int    prune_interval;
 } lima_params;
 

@@ -691,7 +691,7 @@ void lima_engine::setup() {
     D.bb_molsig = dalloc<unsigned long long>(n_clusters);
     D.pl_count = dalloc<int>(n_clusters);
     D.pl_row = dalloc<int2>((size_t)n_clusters * pl_cap);
-    prune_every = p.prune_interval < 0 ? (p.nstlist >= 4 ? p.nstlist / 2 : 0) : p.prune_interval;
+    prune_every = p.prune_interval < 0 ? (p.nstlist >= 4 ? 2 : 0) : p.prune_interval;
     if (prune_every >= p.nstlist) prune_every = 0;   // the rebuild already cuts at rc + skin
     rin = rc + (rlist - rc) * (double)prune_every / (double)std::max(1, p.nstlist);
     if (prune_every > 0) {
@@ -1457,7 +1457,7 @@ void lima_default_params(lima_params* p) {
     p->log_interval = 0;
     p->log_ring = 5;                // DatabuffersDeviceController::nStepsInBuffer
     p->periodic = 1;                // BoundaryConditionSelect::PBC
-    p->prune_interval = -1;         // auto: nstlist / 2
+    p->prune_interval = -1;         // auto: every 2 steps when nstlist >= 4
 }
 
 const char* lima_error_string(int code) {

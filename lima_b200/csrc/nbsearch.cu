@@ -18,6 +18,7 @@
 // The result is bit-identical run to run: every ordering is fixed by keys,
 // never by atomic arrival order.
 #include "engine.h"
+#include "packed.cuh"
 
 namespace lima {
 
@@ -580,7 +581,8 @@ __global__ void __launch_bounds__(PS_WARPS * 32, 1) k_pairsearch(DevState st, fl
 // each chunk of 32 are compacted with a ballot, so the order is fixed.
 // Four rows per lane are in flight at once (their row and j-atom loads issue
 // together); the kept rows are written in list order, so the inner list is the
-// same whatever the launch shape.
+// same whatever the launch shape.  The distance tests are branch-free and take
+// the i-atoms two at a time in packed FP32, (2 ip, 2 ip + 1) as the mask bits.
 constexpr int PRUNE_ROWS_PER_LANE = 4;
 
 __global__ void __launch_bounds__(256) k_prune_rows(DevState st, float rin2) {
@@ -592,11 +594,11 @@ __global__ void __launch_bounds__(256) k_prune_rows(DevState st, float rin2) {
     const size_t base = (size_t)ci * st.pl_cap;
     const int sysi = st.cluster_sys[ci];
     const float Lx = st.sys[sysi].boxf[0], Ly = st.sys[sysi].boxf[1], Lz = st.sys[sysi].boxf[2];
-    float xi[CLUSTER], yi[CLUSTER], zi[CLUSTER];
+    f2p xi[CLUSTER / 2], yi[CLUSTER / 2], zi[CLUSTER / 2];
 #pragma unroll
-    for (int a = 0; a < CLUSTER; ++a) {
-        const float4 v = st.xyzq[ci * CLUSTER + a];
-        xi[a] = v.x, yi[a] = v.y, zi[a] = v.z;
+    for (int ip = 0; ip < CLUSTER / 2; ++ip) {
+        const float4 a = st.xyzq[ci * CLUSTER + 2 * ip], b = st.xyzq[ci * CLUSTER + 2 * ip + 1];
+        xi[ip] = pk2(a.x, b.x), yi[ip] = pk2(a.y, b.y), zi[ip] = pk2(a.z, b.z);
     }
     const unsigned below = (1u << lane) - 1u;
     int out = 0;
@@ -607,22 +609,25 @@ __global__ void __launch_bounds__(256) k_prune_rows(DevState st, float rin2) {
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const int k = k0 + u * 32 + lane;
-            row[u] = k < n ? st.pl_row[base + k] : make_int2(-1, 0);
+            row[u] = k < n ? st.pl_row[base + k] : make_int2(0, 0);   // mask 0: never kept
         }
 #pragma unroll
-        for (int u = 0; u < U; ++u) xj[u] = row[u].x >= 0 ? st.xyzq[row[u].x] : make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int u = 0; u < U; ++u) xj[u] = st.xyzq[row[u].x];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const unsigned img = (unsigned)row[u].y >> ROW_SHIFT_BIT;
-            const float jx = xj[u].x + fmaf((float)(img & 3u), Lx, -Lx);
-            const float jy = xj[u].y + fmaf((float)((img >> 2) & 3u), Ly, -Ly);
-            const float jz = xj[u].z + fmaf((float)(img >> 4), Lz, -Lz);
+            const f2p jx = splat2(xj[u].x + fmaf((float)(img & 3u), Lx, -Lx));
+            const f2p jy = splat2(xj[u].y + fmaf((float)((img >> 2) & 3u), Ly, -Ly));
+            const f2p jz = splat2(xj[u].z + fmaf((float)(img >> 4), Lz, -Lz));
             unsigned bits = 0u;
 #pragma unroll
-            for (int a = 0; a < CLUSTER; ++a) {
-                const float dx = jx - xi[a], dy = jy - yi[a], dz = jz - zi[a];
-                if (((row[u].y >> a) & 1) && dx * dx + dy * dy + dz * dz <= rin2) bits |= 1u << a;
+            for (int ip = 0; ip < CLUSTER / 2; ++ip) {
+                const f2p dx = sub2(jx, xi[ip]), dy = sub2(jy, yi[ip]), dz = sub2(jz, zi[ip]);
+                const float2 r2 = up2(fma2(dx, dx, fma2(dy, dy, mul2(dz, dz))));
+                bits |= (r2.x <= rin2 ? 1u : 0u) << (2 * ip);
+                bits |= (r2.y <= rin2 ? 1u : 0u) << (2 * ip + 1);
             }
+            bits &= (unsigned)row[u].y & 0xffu;
             const unsigned keep = __ballot_sync(0xffffffffu, bits != 0u);
             if (bits) st.pl_row_in[base + out + __popc(keep & below)] = make_int2(row[u].x, (row[u].y & ~0xff) | (int)bits);
             out += __popc(keep);

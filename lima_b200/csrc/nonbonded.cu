@@ -16,6 +16,7 @@
 // walks the 8 i-atoms.  Forces are added as int64 fixed point, so the result
 // does not depend on the order in which warps finish.
 #include "engine.h"
+#include "packed.cuh"
 
 namespace lima {
 
@@ -27,44 +28,6 @@ constexpr float AS_P = 0.3275911f;
 constexpr float AS_A1 = 0.254829592f, AS_A2 = -0.284496736f, AS_A3 = 1.421413741f;
 constexpr float AS_A4 = -1.453152027f, AS_A5 = 1.061405429f;
 
-// ---------------------------------------------------------------- packed FP32
-// Blackwell's packed FP32 instructions ({add,sub,mul,fma}.rn.f32x2, sm_100):
-// one instruction computes two lanes of a float pair held in a 64-bit register,
-// each rounded exactly like its scalar counterpart.
-struct f2p {
-    unsigned long long v;
-};
-__device__ __forceinline__ f2p pk2(float a, float b) {
-    f2p r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(a), "f"(b));
-    return r;
-}
-__device__ __forceinline__ float2 up2(f2p a) {
-    float2 r;
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(a.v));
-    return r;
-}
-__device__ __forceinline__ f2p splat2(float a) { return pk2(a, a); }
-__device__ __forceinline__ f2p add2(f2p a, f2p b) {
-    f2p d;
-    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d.v) : "l"(a.v), "l"(b.v));
-    return d;
-}
-__device__ __forceinline__ f2p sub2(f2p a, f2p b) {
-    f2p d;
-    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d.v) : "l"(a.v), "l"(b.v));
-    return d;
-}
-__device__ __forceinline__ f2p mul2(f2p a, f2p b) {
-    f2p d;
-    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d.v) : "l"(a.v), "l"(b.v));
-    return d;
-}
-__device__ __forceinline__ f2p fma2(f2p a, f2p b, f2p c) {
-    f2p d;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d.v) : "l"(a.v), "l"(b.v), "l"(c.v));
-    return d;
-}
 // Energy minimisation: every LJ pair force passes through the reference's tanh
 // activation, |F| -> A tanh(|F| / A) with A = 1e8 in its 1/24 J/mol/nm force unit
 // (LennardJonesInteractions.cuh:85-101 with EngineUtils.cuh:112-140), after its
@@ -135,12 +98,13 @@ __device__ __forceinline__ f2p erfc_nr2(f2p z) {
 // Pair arithmetic per lane and the order of every sum are fixed, so results
 // are bit-reproducible.
 // EN: 0 forces only, 1 forces and energy totals, 2 also per-atom energy shares.
-// PF: each lane loads two rows (k and k + 32) before working on either, so that
-// the second row's loads overlap the first row's arithmetic; the rows are
-// worked in the same order, so the results are the same bits either way.
+// PF: software-pipelined loads — the row two chunks ahead and the j-atom one
+// chunk ahead are loaded before the current row's arithmetic, so their latency
+// overlaps it; the rows are worked in the same order, so the results are the
+// same bits either way.
 // EM: the energy-minimisation variant (force only, the per-pair LJ clamp above).
 template <int ES, int EN, bool PF, bool EM = false>
-__global__ void __launch_bounds__(256, (EN || PF || EM) ? 2 : 3) k_nonbonded(DevState st, NbParams p) {
+__global__ void __launch_bounds__(256, (EN || EM) ? 2 : 3) k_nonbonded(DevState st, NbParams p) {
     constexpr bool ENERGY = EN > 0, ATOM = EN > 1;
     // per warp, i-atom pairs (2 ip, 2 ip + 1): (x0, x1, y0, y1), (z0, z1, -q0 ke, -q1 ke),
     // (sigma0/2, sigma1/2, 24 sqrt(eps0), 24 sqrt(eps1))
@@ -178,13 +142,12 @@ __global__ void __launch_bounds__(256, (EN || PF || EM) ? 2 : 3) k_nonbonded(Dev
     double s_elj = 0.0, s_ec = 0.0, s_vir = 0.0;
     const size_t base = (size_t)ci * st.pl_cap;
     // one row: its mask, j slot, j position with the row's image applied, j LJ
-    auto load_row = [&](int k, unsigned& bits, int& sj, float4& xj, float2& ljj) {
+    auto load_j = [&](int k, int2 row, unsigned& bits, int& sj, float4& xj, float2& ljj) {
         bits = 0u;
         sj = 0;
         xj = make_float4(0.f, 0.f, 0.f, 0.f);
         ljj = make_float2(0.f, 0.f);
         if (k < n) {
-            const int2 row = st.walk_row[base + k];
             bits = (unsigned)row.y & 0xffu;   // bit ii: pair (ii, this j-atom)
             const unsigned img = (unsigned)row.y >> ROW_SHIFT_BIT;
             sj = row.x;
@@ -195,6 +158,10 @@ __global__ void __launch_bounds__(256, (EN || PF || EM) ? 2 : 3) k_nonbonded(Dev
             xj.y += fmaf((float)((img >> 2) & 3u), Ly, -Ly);
             xj.z += fmaf((float)(img >> 4), Lz, -Lz);
         }
+    };
+    auto load_rowid = [&](int k) { return k < n ? st.walk_row[base + k] : make_int2(0, 0); };
+    auto load_row = [&](int k, unsigned& bits, int& sj, float4& xj, float2& ljj) {
+        load_j(k, load_rowid(k), bits, sj, xj, ljj);
     };
     auto do_row = [&](unsigned bits, int sj, float4 xj, float2 ljj) {
         f2p fjx = zero2, fjy = zero2, fjz = zero2, ej = zero2;
@@ -302,15 +269,23 @@ __global__ void __launch_bounds__(256, (EN || PF || EM) ? 2 : 3) k_nonbonded(Dev
         }
     };
     if (PF) {
-        for (int k0 = 0; k0 < n; k0 += 64) {
-            unsigned ba, bb;
-            int sa, sb;
-            float4 xa, xb;
-            float2 la, lb;
-            load_row(k0 + lane, ba, sa, xa, la);
-            load_row(k0 + 32 + lane, bb, sb, xb, lb);
+        // software pipeline: while a lane works on row k, the j-atom loads of row
+        // k + 32 and the row load of row k + 64 are in flight
+        unsigned ba;
+        int sa;
+        float4 xa;
+        float2 la;
+        int2 rb = load_rowid(32 + lane);
+        load_row(lane, ba, sa, xa, la);
+        for (int k0 = 0; k0 < n; k0 += 32) {
+            const int2 rc = load_rowid(k0 + 64 + lane);
+            unsigned bb;
+            int sb;
+            float4 xb;
+            float2 lb;
+            load_j(k0 + 32 + lane, rb, bb, sb, xb, lb);
             do_row(ba, sa, xa, la);
-            do_row(bb, sb, xb, lb);
+            ba = bb, sa = sb, xa = xb, la = lb, rb = rc;
         }
     } else {
         for (int k0 = 0; k0 < n; k0 += 32) {

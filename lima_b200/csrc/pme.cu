@@ -423,6 +423,24 @@ __device__ __forceinline__ void block_copy4(int total, Load load, Store store) {
     }
 }
 
+// The same with load(i, v) filling v in place (for element types that are arrays).
+template <typename T, typename Load, typename Store>
+__device__ __forceinline__ void block_copy4_into(int total, Load load, Store store) {
+    for (int i0 = threadIdx.x; i0 < total; i0 += 4 * blockDim.x) {
+        T v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int i = i0 + u * blockDim.x;
+            if (i < total) load(i, v[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int i = i0 + u * blockDim.x;
+            if (i < total) store(i, v[u]);
+        }
+    }
+}
+
 // x pass forward: int32 charge grid -> half-complex rows
 __global__ void k_fft_x_fwd(DevState st, const PmeSysDev* plans, const int4* items, int maxn) {
     extern __shared__ float2 sm[];
@@ -528,7 +546,9 @@ __global__ void k_fft_y(DevState st, const PmeSysDev* plans, const int4* items, 
     }
 }
 
-// z pass: forward FFT along z, multiply by theta(k), inverse FFT along z
+// z pass: forward FFT along z, multiply by theta(k), inverse FFT along z.  The
+// tile's theta values are loaded together with its grid values (one round of
+// global-load latency for both) and wait in shared memory for the product.
 __global__ void k_fft_z_conv(DevState st, const PmeSysDev* plans, const int4* items, int maxn) {
     extern __shared__ float2 sm[];
     const int4 it = items[blockIdx.x];
@@ -539,38 +559,45 @@ __global__ void k_fft_z_conv(DevState st, const PmeSysDev* plans, const int4* it
     float2* tw = sm;
     float2* A = sm + maxn;
     float2* B = A + FFT_TX * (maxn + 1);
+    float* T = reinterpret_cast<float*>(B + FFT_TX * (maxn + 1));   // theta, [z][c]
     load_twiddles(tw, pl, st.pme_tw);
     const int x0 = it.y, y = it.z;
     const int tx = min(FFT_TX, K0h - x0);
     const size_t plane = (size_t)K1 * K0h;
     float2* g = st.pme_cplx + sd.pme_coff + (size_t)y * K0h + x0;
     const float* th = st.pme_theta + sd.pme_coff + (size_t)y * K0h + x0;
-    block_copy4<float2>(
-        K2 * FFT_TX,
-        [&](int i) {
+    const int total = K2 * FFT_TX;
+    for (int i0 = threadIdx.x; i0 < total; i0 += 4 * blockDim.x) {
+        float2 v[4];
+        float t[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int i = i0 + u * blockDim.x;
             const int z = i / FFT_TX, c = i - z * FFT_TX;
-            return c < tx ? g[z * plane + c] : make_float2(0.f, 0.f);
-        },
-        [&](int i, float2 v) {
-            const int z = i / FFT_TX, c = i - z * FFT_TX;
-            A[c * stride + z] = v;
-        });
+            const bool ok = i < total && c < tx;
+            v[u] = ok ? g[z * plane + c] : make_float2(0.f, 0.f);
+            t[u] = ok ? th[z * plane + c] : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int i = i0 + u * blockDim.x;
+            if (i < total) {
+                const int z = i / FFT_TX, c = i - z * FFT_TX;
+                A[c * stride + z] = v[u];
+                T[i] = t[u];
+            }
+        }
+    }
     __syncthreads();
     float2* res = fft_lines(A, B, FFT_TX, stride, pl, tw, -1.f);
-    block_copy4<float>(
-        K2 * FFT_TX,
-        [&](int i) {
-            const int z = i / FFT_TX, c = i - z * FFT_TX;
-            return c < tx ? th[z * plane + c] : 0.f;
-        },
-        [&](int i, float t) {
-            const int z = i / FFT_TX, c = i - z * FFT_TX;
-            res[c * stride + z] = cscale(res[c * stride + z], t);
-        });
+    for (int i = threadIdx.x; i < total; i += blockDim.x) {
+        const int z = i / FFT_TX, c = i - z * FFT_TX;
+        res[c * stride + z] = cscale(res[c * stride + z], T[i]);
+    }
     __syncthreads();
     float2* other = res == A ? B : A;
     const float2* res2 = fft_lines(res, other, FFT_TX, stride, pl, tw, 1.f);
-    for (int i = threadIdx.x; i < K2 * FFT_TX; i += blockDim.x) {
+    for (int i = threadIdx.x; i < total; i += blockDim.x) {
         const int z = i / FFT_TX, c = i - z * FFT_TX;
         if (c < tx) g[z * plane + c] = res2[c * stride + z];
     }
@@ -604,19 +631,43 @@ __global__ void __launch_bounds__(FFT_XY_THREADS) k_fft_xy_fwd(DevState st, cons
     load_twiddles(twy, ply, st.pme_tw);
     const int* g = st.pme_grid_fx + sd.pme_off + (size_t)K0 * K1 * z;
     const int sx = K0 + 1, sy = K1 + 1;
-    block_copy4<float2>(
-        P * K0,
-        [&](int i) {
-            const int pl = div_small(i, iK0), x = i - pl * K0;
-            const int ya = 2 * pl, yb = ya + 1;
-            const float a = (float)g[(size_t)ya * K0 + x] * (float)(1.0 / GRID32_SCALE);
-            const float b = yb < K1 ? (float)g[(size_t)yb * K0 + x] * (float)(1.0 / GRID32_SCALE) : 0.f;
-            return make_float2(a, b);
-        },
-        [&](int i, float2 v) {
-            const int pl = div_small(i, iK0), x = i - pl * K0;
-            A[pl * sx + x] = v;
-        });
+    constexpr float isc = (float)(1.0 / GRID32_SCALE);
+    if ((K0 & 3) == 0 && (sd.pme_off & 3) == 0) {
+        // rows of a multiple of four nodes from a 16-byte aligned plane: four x
+        // nodes of both rows of a line per element
+        const int K0q = K0 >> 2;
+        const float iK0q = 1.f / (float)K0q;
+        block_copy4_into<int4[2]>(
+            P * K0q,
+            [&](int i, int4 (&v)[2]) {
+                const int pl = div_small(i, iK0q), x = 4 * (i - pl * K0q);
+                const int ya = 2 * pl, yb = ya + 1;
+                v[0] = *reinterpret_cast<const int4*>(g + (size_t)ya * K0 + x);
+                v[1] = yb < K1 ? *reinterpret_cast<const int4*>(g + (size_t)yb * K0 + x) : make_int4(0, 0, 0, 0);
+            },
+            [&](int i, const int4 (&v)[2]) {
+                const int pl = div_small(i, iK0q), x = 4 * (i - pl * K0q);
+                float2* a = A + pl * sx + x;
+                a[0] = make_float2((float)v[0].x * isc, (float)v[1].x * isc);
+                a[1] = make_float2((float)v[0].y * isc, (float)v[1].y * isc);
+                a[2] = make_float2((float)v[0].z * isc, (float)v[1].z * isc);
+                a[3] = make_float2((float)v[0].w * isc, (float)v[1].w * isc);
+            });
+    } else {
+        block_copy4<float2>(
+            P * K0,
+            [&](int i) {
+                const int pl = div_small(i, iK0), x = i - pl * K0;
+                const int ya = 2 * pl, yb = ya + 1;
+                const float a = (float)g[(size_t)ya * K0 + x] * isc;
+                const float b = yb < K1 ? (float)g[(size_t)yb * K0 + x] * isc : 0.f;
+                return make_float2(a, b);
+            },
+            [&](int i, float2 v) {
+                const int pl = div_small(i, iK0), x = i - pl * K0;
+                A[pl * sx + x] = v;
+            });
+    }
     __syncthreads();
     const float2* res = fft_lines(A, B, P, sx, plx, twx, -1.f);
     float2* yl = res == A ? B : A;
@@ -683,10 +734,23 @@ __global__ void __launch_bounds__(FFT_XY_THREADS) k_fft_xy_inv(DevState st, cons
     __syncthreads();
     const float2* out = fft_lines(xl, const_cast<float2*>(res), P, sx, plx, twx, 1.f);
     float* gr = st.pme_real + sd.pme_off + (size_t)K0 * K1 * z;
-    for (int i = threadIdx.x; i < K1 * K0; i += blockDim.x) {
-        const int y = div_small(i, iK0), x = i - y * K0;
-        const float2 v = out[(y >> 1) * sx + x];
-        gr[(size_t)y * K0 + x] = (y & 1) ? v.y : v.x;
+    if ((K0 & 3) == 0 && (sd.pme_off & 3) == 0) {
+        // four x nodes per store (16-byte aligned rows)
+        const int K0q = K0 >> 2;
+        const float iK0q = 1.f / (float)K0q;
+        for (int i = threadIdx.x; i < K1 * K0q; i += blockDim.x) {
+            const int y = div_small(i, iK0q), x = 4 * (i - y * K0q);
+            const float2* o = out + (y >> 1) * sx + x;
+            const float2 v0 = o[0], v1 = o[1], v2 = o[2], v3 = o[3];
+            *reinterpret_cast<float4*>(gr + (size_t)y * K0 + x) =
+                (y & 1) ? make_float4(v0.y, v1.y, v2.y, v3.y) : make_float4(v0.x, v1.x, v2.x, v3.x);
+        }
+    } else {
+        for (int i = threadIdx.x; i < K1 * K0; i += blockDim.x) {
+            const int y = div_small(i, iK0), x = i - y * K0;
+            const float2 v = out[(y >> 1) * sx + x];
+            gr[(size_t)y * K0 + x] = (y & 1) ? v.y : v.x;
+        }
     }
 }
 
@@ -814,6 +878,10 @@ __global__ void k_gather(DevState st, const SysDesc sd1) {
 static size_t fft_smem_bytes(int lines, int maxn) {
     return (size_t)(maxn + 2 * lines * (maxn + 1)) * sizeof(float2);
 }
+// the z pass also holds its tile's theta values
+static size_t zconv_smem_bytes(int maxn) {
+    return fft_smem_bytes(FFT_TX, maxn) + (size_t)FFT_TX * maxn * sizeof(float);
+}
 
 int launch_pme(const DevState& st, const PmePlan& plan, bool energy, cudaStream_t s) {
     if (plan.n_items_x == 0) return 0;
@@ -832,13 +900,13 @@ int launch_pme(const DevState& st, const PmePlan& plan, bool energy, cudaStream_
     if (plan.n_items_xy > 0) {
         const size_t sxy = (size_t)(2 * mx + 2 * plan.xy_buf) * sizeof(float2);
         k_fft_xy_fwd<<<plan.n_items_xy, FFT_XY_THREADS, sxy, s>>>(st, plans, plan.items_xy, mx, plan.xy_buf);
-        k_fft_z_conv<<<plan.n_items_z, FFT_YZ_THREADS, sy, s>>>(st, plans, plan.items_z, mx);
+        k_fft_z_conv<<<plan.n_items_z, FFT_YZ_THREADS, zconv_smem_bytes(mx), s>>>(st, plans, plan.items_z, mx);
         k_fft_xy_inv<<<plan.n_items_xy, FFT_XY_THREADS, sxy, s>>>(st, plans, plan.items_xy, mx, plan.xy_buf);
         n = 5;
     } else {
         k_fft_x_fwd<<<plan.n_items_x, 256, sx, s>>>(st, plans, plan.items_x, mx);
         k_fft_y<<<plan.n_items_y, FFT_YZ_THREADS, sy, s>>>(st, plans, plan.items_y, -1.f, mx);
-        k_fft_z_conv<<<plan.n_items_z, FFT_YZ_THREADS, sy, s>>>(st, plans, plan.items_z, mx);
+        k_fft_z_conv<<<plan.n_items_z, FFT_YZ_THREADS, zconv_smem_bytes(mx), s>>>(st, plans, plan.items_z, mx);
         k_fft_y<<<plan.n_items_y, FFT_YZ_THREADS, sy, s>>>(st, plans, plan.items_y, 1.f, mx);
         k_fft_x_inv<<<plan.n_items_x, 256, sx, s>>>(st, plans, plan.items_x, mx);
     }
@@ -928,7 +996,7 @@ void pme_set_smem_limits(int maxn, int xy_buf) {
     largest[dev] = maxn;
     const int by = (int)fft_smem_bytes(FFT_TX, maxn), bx = (int)fft_smem_bytes(FFT_XLINES, maxn);
     cudaFuncSetAttribute(k_fft_y, cudaFuncAttributeMaxDynamicSharedMemorySize, by);
-    cudaFuncSetAttribute(k_fft_z_conv, cudaFuncAttributeMaxDynamicSharedMemorySize, by);
+    cudaFuncSetAttribute(k_fft_z_conv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zconv_smem_bytes(maxn));
     cudaFuncSetAttribute(k_fft_x_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, bx);
     cudaFuncSetAttribute(k_fft_x_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, bx);
 }

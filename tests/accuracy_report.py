@@ -67,10 +67,16 @@ def frame_errors(eng, s, rc, es_mode, kappa, grid):
     if es_mode == 1:
         # plain cutoff Coulomb: a pair within 1e-5 nm of the cutoff is in or out
         # by the rounding of r^2 (FP32 here, FP64 in the oracle) and moves its
-        # atoms' forces by a whole k q q / rc^2; the error over the other atoms
-        band_pairs, flags, _ = O.pairset(sf.pos, sf.box, sf.exclusions(), rc, band=1e-5)
+        # atoms' forces by a whole k q q / rc^2; the error over the other atoms.
+        # Band pairs lie on both sides of the cutoff, so they are taken from the
+        # oracle's pair set within rc + band.
+        band = 1e-5
+        near, _, _ = O.pairset(sf.pos, sf.box, sf.exclusions(), rc + band)
+        d = sf.pos[near[:, 0]] - sf.pos[near[:, 1]]
+        d -= sf.box * np.round(d / sf.box)
+        in_band = np.abs(np.linalg.norm(d, axis=1) - rc) < band
         touched = np.zeros(sf.n, bool)
-        touched[band_pairs[flags == 1].ravel()] = True
+        touched[near[in_band].ravel()] = True
         keep = ~touched
         out["band_atoms"] = int(touched.sum())
         out["rel_rms_outside_band"] = float(np.sqrt((df[keep] ** 2).mean()) /

@@ -59,6 +59,55 @@ def test_pairset_bit_exact(oracle, rc):
     assert len(rs) > 100000 if rc == 1.2 else True
 
 
+def _pair_keys(pairs, n):
+    p = np.asarray(pairs, np.int64)
+    return np.unique(p[:, 0] * n + p[:, 1])
+
+
+@pytest.mark.parametrize("cfg", ["config1", "config2"])
+def test_pairset_bit_exact_large(oracle, cfg):
+    """The pair sets of the chain slab (C1, rc 1.2 nm) and the 100k-atom water box
+    (C2, rc 1.0 nm) against the oracle: identical outside the 1e-5 nm band and
+    no pair listed twice."""
+    s = getattr(systems, cfg)()
+    rc = 1.2 if cfg == "config1" else 1.0
+    e = make(s, cutoff=rc, electrostatics=E.ES_CUTOFF)
+    e.compute_forces()
+    got = e.pairlist()
+    gk = _pair_keys(got, s.n)
+    assert len(gk) == len(got)                       # no duplicates
+    band = 1e-5
+    near, _, _ = oracle.pairset(s.pos, s.box, s.exclusions(), rc + band)
+    d = s.pos[near[:, 0]] - s.pos[near[:, 1]]
+    d -= s.box * np.round(d / s.box)
+    r = np.linalg.norm(d, axis=1)
+    ref_in = _pair_keys(near[r <= rc], s.n)
+    in_band = _pair_keys(near[np.abs(r - rc) < band], s.n)
+    only_ref = np.setdiff1d(np.setdiff1d(ref_in, gk), in_band)
+    only_gpu = np.setdiff1d(np.setdiff1d(gk, ref_in), in_band)
+    assert len(only_ref) == 0 and len(only_gpu) == 0, (len(only_ref), len(only_gpu))
+    assert len(ref_in) > (3_000_000 if cfg == "config1" else 20_000_000)
+
+
+# Energy bars per term against the FP64 oracle.  The engine's positions are FP32
+# absolute coordinates (a 10 nm box resolves 1e-6 nm), which bounds the LJ term,
+# whose r^-12 wall amplifies the coordinate rounding, near 1e-6; the
+# reciprocal-space term sums an FP32 grid through two FP32 FFTs.
+TERM_BARS = {"lj": 3e-6, "pme_recip": 2e-6}
+TERM_BAR = 1e-6
+
+
+def check_energy_bars(eng, ref):
+    # a term below 1e-4 of the summed magnitudes (bonds at their rest length in a
+    # freshly built system: ~1 J/mol beside 1e9) is measured against that floor
+    floor = 1e-4 * sum(abs(v) for v in ref.values())
+    for k, b in ref.items():
+        a = eng[k]
+        assert abs(a - b) <= TERM_BARS.get(k, TERM_BAR) * max(abs(b), floor), (k, a, b, abs(a - b) / max(abs(b), floor))
+    pot = sum(ref.values())
+    assert abs(sum(eng[k] for k in ref) - pot) <= TERM_BAR * abs(pot)
+
+
 # ------------------------------------------------- (b)+(c) forces and energies
 def test_cutoff_coulomb_config0(oracle):
     """Config 0: LJ + plain cutoff Coulomb at 1.2 nm, flexible water bonds/angles."""
@@ -182,6 +231,29 @@ def test_config2_full_size(oracle):
     fr, er = oracle_total(oracle, s, 1.0, 2, kappa, grid)
     assert rel_rms(f, fr) < FORCE_TOL, rel_rms(f, fr)
     check_energies(e.energies(), er)
+
+
+@pytest.mark.parametrize("cfg", ["config1", "config2"])
+def test_energy_bars_prepared(oracle, cfg):
+    """The 1e-6 energy bars on a prepared state (energy minimisation, then
+    thermostatted MD at 300 K: no lattice clashes left), the state the
+    configurations are run from; forces at 1e-4 relative RMS as everywhere."""
+    from tests.accuracy_report import equilibrate
+    s = getattr(systems, cfg)()
+    rc = 1.2 if cfg == "config1" else 1.0
+    grid = (48, 48, 80) if cfg == "config1" else (96, 96, 96)
+    kappa = kappa_from_tol(rc, 1e-5)
+
+    def make_engine(**extra):
+        return Engine(cutoff=rc, electrostatics=E.ES_EWALD, ewald_kappa=kappa, nstlist=10, dt=1e-6, **extra)
+
+    s, _ = equilibrate(make_engine, s, grid, 300, 500)
+    e = make_engine()
+    e.load(s, pme_grid=grid)
+    e.compute_forces(energy=True)
+    fr, er = oracle_total(oracle, s, rc, 2, kappa, grid)
+    assert rel_rms(e.forces(), fr) < FORCE_TOL
+    check_energy_bars(e.energies(), er)
 
 
 # ------------------------------------------------------------- reproducibility
