@@ -172,6 +172,37 @@ def headline_config(n_atoms: int, world: int) -> dict:
             "accumulation": "int64 fixed point forces/energies, FP64 positions"}
 
 
+def accuracy_summary():
+    """Per-configuration accuracy against the FP64 oracle, from the committed
+    report of tests/accuracy_report.py (profiles/accuracy_configs.json): force
+    errors over the frames, the worst energy term, and the constant-energy
+    drift and variance coefficient at dt = 1 fs."""
+    path = os.path.join(ROOT, "profiles", "accuracy_configs.json")
+    if not os.path.exists(path):
+        return None
+    try:
+        rep = json.load(open(path))
+    except Exception:
+        return None
+    out = {"source": "profiles/accuracy_configs.json (tests/accuracy_report.py, one B200)", "configs": {}}
+    for r in rep:
+        sm = r["summary"]
+        terms = {k: v["max"] for k, v in sm["energy_rel"].items()}
+        worst = max(((k, v) for k, v in terms.items() if k != "potential"), key=lambda x: x[1])
+        c = {"atoms": r["atoms"], "frames": sm["frames"], "max_force_err_j_mol_nm": sm["max_abs_err"]["max"],
+             "rms_force_err_j_mol_nm": sm["rms_err"]["max"], "rel_rms_force_err": sm["rel_rms"]["max"],
+             "worst_energy_term": worst[0], "worst_energy_rel": worst[1], "potential_rel": terms.get("potential")}
+        if "rel_rms_outside_band" in sm:
+            c["rel_rms_force_err_outside_cutoff_band"] = sm["rel_rms_outside_band"]["max"]
+        for d in r.get("drift") or []:
+            if abs(d["dt_fs"] - 1.0) < 1e-9:
+                c["drift_kj_mol_ns_atom"] = d["drift_kj_mol_per_ns_per_atom"]
+                c["drift_per_ns_over_kinetic"] = d["drift_per_ns_over_kinetic"]
+                c["variance_coefficient"] = d["variance_coefficient"]
+        out["configs"][r["config"]] = c
+    return out
+
+
 def stage_rooflines(ph: dict, s, n_rows: int, hbm_gbs: float) -> dict:
     """Algorithmic bytes per stage (per-unit figures in DESIGN.md section 3) over
     the stage's event-timed average duration, against the measured HBM copy
@@ -732,6 +763,7 @@ def run_lima(args):
         "graph_mode": {"ns_per_day": world * ns_per_day(graph_step_s), "ms_per_step": graph_step_s * 1e3,
                        "l2": "not flushed: each pair-list period (rebuild + 10 steps) replays as one CUDA graph"},
         "other_configs": others,
+        "accuracy": accuracy_summary(),
     }
     print(json.dumps(line), flush=True)
     return 0

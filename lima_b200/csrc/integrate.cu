@@ -32,68 +32,76 @@ __device__ __forceinline__ void check_saturation(const DevState& st, int s) {
         atomicOr(st.status, ST_FORCE_SATURATED);
 }
 
+// Every load of a slot is issued before the padding test (padding slots hold
+// valid memory), so the per-slot loads form one round of memory latency
+// instead of a chain behind the slot's `orig` entry.
 template <int INTEGRATOR, bool ENERGY>
 __global__ void k_integrate(DevState st, IntegrateParams p) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     double ke = 0.0;
     int sysi = -1;
-    if (s < st.n_slots && st.orig[s] >= 0) {
-        sysi = st.cluster_sys[s / CLUSTER];
-        const float scale = st.vscale[sysi];
+    if (s < st.n_slots) {
+        const int o = st.orig[s];
+        const int sy = st.cluster_sys[s / CLUSTER];
         const float3 F = load_force(st, s);
         float4 v = st.vel[s];
-        const float im = v.w;
-        const float dt = (float)p.dt;
-        if (!(isfinite(F.x) && isfinite(F.y) && isfinite(F.z))) atomicOr(st.status, ST_NONFINITE);
-        check_saturation(st, s);
-        double dx, dy, dz;
-        if (INTEGRATOR == 0) {
-            const float m = im > 0.f ? 1.f / im : 0.f;
-            const float vx = (v.x + F.x * im * dt) * scale;
-            const float vy = (v.y + F.y * im * dt) * scale;
-            const float vz = (v.z + F.z * im * dt) * scale;
-            if (ENERGY) {
-                // average of the two half-step kinetic energies
-                ke = 0.25 * (double)m * ((double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z +
-                                         (double)vx * vx + (double)vy * vy + (double)vz * vz);
-            }
-            v.x = vx;
-            v.y = vy;
-            v.z = vz;
-            dx = (double)vx * p.dt;
-            dy = (double)vy * p.dt;
-            dz = (double)vz * p.dt;
-        } else {
-            const float4 fp = st.fprev[s];
-            const float h = 0.5f * dt * im;
-            const float vx = v.x + (F.x + fp.x) * h;
-            const float vy = v.y + (F.y + fp.y) * h;
-            const float vz = v.z + (F.z + fp.z) * h;
-            if (ENERGY) {
-                const float m = im > 0.f ? 1.f / im : 0.f;
-                ke = 0.5 * (double)m * ((double)vx * vx + (double)vy * vy + (double)vz * vz);
-            }
-            const float a = 0.5f * im * dt * dt;
-            dx = (double)vx * p.dt + (double)(F.x * a);
-            dy = (double)vy * p.dt + (double)(F.y * a);
-            dz = (double)vz * p.dt + (double)(F.z * a);
-            st.fprev[s] = make_float4(F.x, F.y, F.z, 0.f);
-            v.x = vx * scale;
-            v.y = vy * scale;
-            v.z = vz * scale;
-        }
-        st.vel[s] = v;
-        const double x = st.px[s] + dx, y = st.py[s] + dy, z = st.pz[s] + dz;
-        st.px[s] = x;
-        st.py[s] = y;
-        st.pz[s] = z;
+        const double px = st.px[s], py = st.py[s], pz = st.pz[s];
         const float q = st.xyzq[s].w;
-        st.xyzq[s] = make_float4((float)x, (float)y, (float)z, q);
-        // an atom beyond half the Verlet buffer from its position at the list
-        // build may meet a partner the list does not hold
         const float4 r = st.xyz_ref[s];
-        const float ex = (float)x - r.x, ey = (float)y - r.y, ez = (float)z - r.z;
-        if (ex * ex + ey * ey + ez * ez > p.half_skin2) atomicOr(st.status, ST_MOVED_TOO_FAR);
+        const float4 fp = INTEGRATOR == 0 ? make_float4(0.f, 0.f, 0.f, 0.f) : st.fprev[s];
+        const float scale = st.vscale[sy];
+        if (o >= 0) {
+            sysi = sy;
+            const float im = v.w;
+            const float dt = (float)p.dt;
+            if (!(isfinite(F.x) && isfinite(F.y) && isfinite(F.z))) atomicOr(st.status, ST_NONFINITE);
+            check_saturation(st, s);
+            double dx, dy, dz;
+            if (INTEGRATOR == 0) {
+                const float m = im > 0.f ? 1.f / im : 0.f;
+                const float vx = (v.x + F.x * im * dt) * scale;
+                const float vy = (v.y + F.y * im * dt) * scale;
+                const float vz = (v.z + F.z * im * dt) * scale;
+                if (ENERGY) {
+                    // average of the two half-step kinetic energies
+                    ke = 0.25 * (double)m * ((double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z +
+                                             (double)vx * vx + (double)vy * vy + (double)vz * vz);
+                }
+                v.x = vx;
+                v.y = vy;
+                v.z = vz;
+                dx = (double)vx * p.dt;
+                dy = (double)vy * p.dt;
+                dz = (double)vz * p.dt;
+            } else {
+                const float h = 0.5f * dt * im;
+                const float vx = v.x + (F.x + fp.x) * h;
+                const float vy = v.y + (F.y + fp.y) * h;
+                const float vz = v.z + (F.z + fp.z) * h;
+                if (ENERGY) {
+                    const float m = im > 0.f ? 1.f / im : 0.f;
+                    ke = 0.5 * (double)m * ((double)vx * vx + (double)vy * vy + (double)vz * vz);
+                }
+                const float a = 0.5f * im * dt * dt;
+                dx = (double)vx * p.dt + (double)(F.x * a);
+                dy = (double)vy * p.dt + (double)(F.y * a);
+                dz = (double)vz * p.dt + (double)(F.z * a);
+                st.fprev[s] = make_float4(F.x, F.y, F.z, 0.f);
+                v.x = vx * scale;
+                v.y = vy * scale;
+                v.z = vz * scale;
+            }
+            st.vel[s] = v;
+            const double x = px + dx, y = py + dy, z = pz + dz;
+            st.px[s] = x;
+            st.py[s] = y;
+            st.pz[s] = z;
+            st.xyzq[s] = make_float4((float)x, (float)y, (float)z, q);
+            // an atom beyond half the Verlet buffer from its position at the list
+            // build may meet a partner the list does not hold
+            const float ex = (float)x - r.x, ey = (float)y - r.y, ez = (float)z - r.z;
+            if (ex * ex + ey * ey + ez * ez > p.half_skin2) atomicOr(st.status, ST_MOVED_TOO_FAR);
+        }
     }
     if (ENERGY) add_energy_fixed(st.energy, sysi, ke, E_KINETIC);
 }

@@ -262,10 +262,10 @@ def main():
     kap2 = kappa_from_tol(1.0, 1e-5)
     add("C0 water1k cutoff 1.2", systems.config0(), 1.2, E.ES_CUTOFF, 0.0, None,
         3 if q else 10, 100, 500 if q else 4000, prep_min=300)
-    # plain truncated Coulomb: a pair the list misses (an atom that moved more
-    # than half the buffer since the build) costs the whole force jump
-    # q_i q_j k_e / rc^2 at the cutoff, so C0 is also run with a buffer that no
-    # atom outruns in ten steps
+    # plain truncated Coulomb: a pair the list missed (an atom that moved more
+    # than half the buffer since the build) would cost the whole force jump
+    # q_i q_j k_e / rc^2 at the cutoff, so C0 also runs with a buffer that no
+    # atom outruns in ten steps; its errors match the 0.1 nm run's
     add("C0 water1k cutoff 1.2, skin 0.25", systems.config0(), 1.2, E.ES_CUTOFF, 0.0, None,
         3 if q else 10, 100, 500 if q else 4000, prep_min=300, kw={"skin": 0.25})
     add("C1 chains+water PME 48x48x80", systems.config1(), 1.2, E.ES_EWALD, kap1, (48, 48, 80),
