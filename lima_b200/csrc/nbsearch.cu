@@ -441,16 +441,39 @@ __global__ void __launch_bounds__(PS_WARPS * 32, 1) k_pairsearch(DevState st, fl
     // finding its column by binary search over the scan.  Candidates are queued in
     // column, cluster, lane and shift order; full batches of 32 are turned into
     // rows, and after the walk whatever remains.
+    // With the x and y shifts fixed, the window is also cut in z: a column's
+    // atoms are sorted by z, so its clusters' lower and upper z bounds both rise
+    // with the cluster index, and the clusters whose z extent (under a z shift)
+    // reaches the i-cluster's z range widened by r_list form one index range,
+    // found by two binary searches.  The window is then walked as virtual
+    // columns (column, z shift): only the unshifted image, plus the shift down
+    // or up when the range crosses the bottom or top of the box.  The range is
+    // widened by 1e-4 nm so that it holds every cluster the extent test below
+    // could pass; that test still decides.
+    const bool zcut = fixed_xy;
+    int zs1 = 0, zs2 = 0, nsz = 1;   // z shifts of the second and third virtual column
+    float zr_lo = 0.f, zr_hi = 0.f;
+    if (zcut) {
+        zr_lo = ilo.z - R - 1e-4f;
+        zr_hi = ihi.z + R + 1e-4f;
+        if (st.periodic) {
+            const bool down = zr_lo < 0.f, up = zr_hi >= L[2];
+            nsz = 1 + (down ? 1 : 0) + (up ? 1 : 0);
+            zs1 = down ? -1 : 1;
+            zs2 = 1;
+        }
+    }
     int qn = 0;
-    const int nwin = (nx > 0 && ny > 0) ? nx * ny : 0;
+    const int nwin = (nx > 0 && ny > 0) ? nx * ny * nsz : 0;
     for (int w0 = 0; w0 < nwin; w0 += 32) {
-        const int w = w0 + lane;
-        int cnt = 0, jstart = 0, shc = 5;   // shc: (sx + 1) | (sy + 1) << 2
+        const int v = w0 + lane;
+        const int w = v / nsz, vz = v - w * nsz;
+        int cnt = 0, jstart = 0, shc = 5 | (1 << 4);   // shc: (sx + 1) | (sy + 1) << 2 | (sz + 1) << 4
         const int wy = w / nx, wx = w - wy * nx;
         const int ux = cx0 + wx, uy = cy0 + wy;   // unwrapped column
         // a window narrower than the grid sits within one period of it; a column
         // further out (not met in practice) is left out rather than misaddressed
-        if (w < nwin && ux >= -sd.ncol_x && ux < 2 * sd.ncol_x && uy >= -sd.ncol_y && uy < 2 * sd.ncol_y) {
+        if (v < nwin && ux >= -sd.ncol_x && ux < 2 * sd.ncol_x && uy >= -sd.ncol_y && uy < 2 * sd.ncol_y) {
             const int sxc = ux < 0 ? -1 : (ux >= sd.ncol_x ? 1 : 0);
             const int syc = uy < 0 ? -1 : (uy >= sd.ncol_y ? 1 : 0);
             const int col = sd.col_off + (ux - sxc * sd.ncol_x) + sd.ncol_x * (uy - syc * sd.ncol_y);
@@ -458,8 +481,30 @@ __global__ void __launch_bounds__(PS_WARPS * 32, 1) k_pairsearch(DevState st, fl
             // clusters are numbered in column order: those before ci are in
             // their own half lists
             jstart = max(j0, ci);
-            cnt = max(0, j0 + nj - jstart);
-            shc = (sxc + 1) | ((syc + 1) << 2);
+            int jend = j0 + nj;
+            const int szc = vz == 0 ? 0 : (vz == 1 ? zs1 : zs2);
+            if (zcut && jstart < jend) {
+                // first cluster whose top reaches the range, first whose bottom is past it
+                const float zl = zr_lo - szc * L[2], zh = zr_hi - szc * L[2];
+                int a0 = jstart, a1 = jend, b0 = jstart, b1 = jend;
+                while (a0 < a1 || b0 < b1) {
+                    const int am = (a0 + a1) >> 1, bm = (b0 + b1) >> 1;
+                    const float hz = a0 < a1 ? st.bb_hi[am].z : 0.f;
+                    const float lz = b0 < b1 ? st.bb_lo[bm].z : 0.f;
+                    if (a0 < a1) {
+                        if (hz < zl) a0 = am + 1;
+                        else a1 = am;
+                    }
+                    if (b0 < b1) {
+                        if (lz <= zh) b0 = bm + 1;
+                        else b1 = bm;
+                    }
+                }
+                jstart = a0;
+                jend = max(a0, b0);
+            }
+            cnt = max(0, jend - jstart);
+            shc = (sxc + 1) | ((syc + 1) << 2) | ((szc + 1) << 4);
         }
         int incl = cnt;
 #pragma unroll
@@ -485,7 +530,8 @@ __global__ void __launch_bounds__(PS_WARPS * 32, 1) k_pairsearch(DevState st, fl
                     else lo = mid + 1;
                 }
                 j = s_js[wib][lo] + t - (lo ? s_end[wib][lo - 1] : 0);
-                const int sx_col = (s_sh[wib][lo] & 3) - 1, sy_col = (s_sh[wib][lo] >> 2) - 1;
+                const int sx_col = (s_sh[wib][lo] & 3) - 1, sy_col = ((s_sh[wib][lo] >> 2) & 3) - 1;
+                const int sz_col = (s_sh[wib][lo] >> 4) - 1;
                 const float4 jlo = st.bb_lo[j], jhi = st.bb_hi[j];
                 const float jc[3] = {0.5f * (jlo.x + jhi.x), 0.5f * (jlo.y + jhi.y), 0.5f * (jlo.z + jhi.z)};
                 const float je[3] = {0.5f * (jhi.x - jlo.x), 0.5f * (jhi.y - jlo.y), 0.5f * (jhi.z - jlo.z)};
@@ -496,13 +542,11 @@ __global__ void __launch_bounds__(PS_WARPS * 32, 1) k_pairsearch(DevState st, fl
                     const float gy = fmaxf(fabsf(jc[1] + sy_col * L[1] - ic[1]) - ie[1] - je[1], 0.f);
                     const float gxy = gx * gx + gy * gy;
                     if (gxy < R2) {
-                        const int base = (sx_col + 1) + 3 * (sy_col + 1);
-                        for (int sz = -1; sz <= 1; ++sz) {
-                            const int code = base + 9 * (sz + 1);
-                            if (j == ci && code < 13) continue;   // own images: one of each +/- pair
-                            const float gz = fmaxf(fabsf(jc[2] + sz * L[2] - ic[2]) - ie[2] - je[2], 0.f);
-                            if (gxy + gz * gz < R2) shifts |= 1u << code;
-                        }
+                        // the virtual column's z shift
+                        const int code = (sx_col + 1) + 3 * (sy_col + 1) + 9 * (sz_col + 1);
+                        const float gz = fmaxf(fabsf(jc[2] + sz_col * L[2] - ic[2]) - ie[2] - je[2], 0.f);
+                        // own images: one of each +/- pair
+                        if (!(j == ci && code < 13) && gxy + gz * gz < R2) shifts |= 1u << code;
                     }
                 } else {
                     float g2[3][3];
