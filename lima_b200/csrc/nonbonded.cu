@@ -45,15 +45,30 @@ __device__ __forceinline__ float ex2_approx(float x) {
     asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
 }
-// erfc for the energy of energy steps: erfc(z) = t exp(-z^2 + P(t)),
-// t = 1/(1 + z/2), P of degree 9 — the Chebyshev fit of Press, Teukolsky,
-// Vetterling & Flannery, Numerical Recipes (2nd ed.), section 6.2 ("erfcc"),
-// fractional error below 1.2e-7 for every z >= 0.  The force keeps the cheaper
-// A&S form above (its 1.5e-7 absolute bound is far inside the force tolerance);
-// a total energy needs the relative bound.  Packed: z holds two arguments.
-constexpr float NR_C0 = -1.26551223f, NR_C1 = 1.00002368f, NR_C2 = 0.37409196f, NR_C3 = 0.09678418f;
-constexpr float NR_C4 = -0.18628806f, NR_C5 = 0.27886807f, NR_C6 = -1.13520398f, NR_C7 = 1.48851587f;
-constexpr float NR_C8 = -0.82215223f, NR_C9 = 0.17087277f;
+// erfc for the energy of energy steps: erfc(x) = t (c0 + c1 t + ... + c9 t^9) e^{-x^2}
+// with the force's t = 1/(1 + p x) and e^{-x^2}, so an energy step adds only this
+// polynomial to the force's arithmetic.  The coefficients are this build's own
+// weighted least-squares fit of erfc(x) e^{x^2} over x in [0, 7]
+// (lima_b200/csrc/erfcx_fit.py): relative error below 7e-10 in exact arithmetic,
+// 2e-7 evaluated in FP32 — the relative bound a total energy needs, where the
+// force's A&S form only bounds the absolute error (1.5e-7).
+constexpr float EC0 = 0.184739336f, EC1 = 0.186472416f, EC2 = 0.16061303f, EC3 = 0.227135599f;
+constexpr float EC4 = -0.106458984f, EC5 = 0.59804976f, EC6 = -0.668688476f, EC7 = 0.704147577f;
+constexpr float EC8 = -0.348146588f, EC9 = 0.0621363297f;
+
+// erfc(x) from the force's t and e^{-x^2} (packed pairs)
+__device__ __forceinline__ f2p erfc_from_t(f2p t, f2p ex) {
+    f2p q = fma2(t, splat2(EC9), splat2(EC8));
+    q = fma2(q, t, splat2(EC7));
+    q = fma2(q, t, splat2(EC6));
+    q = fma2(q, t, splat2(EC5));
+    q = fma2(q, t, splat2(EC4));
+    q = fma2(q, t, splat2(EC3));
+    q = fma2(q, t, splat2(EC2));
+    q = fma2(q, t, splat2(EC1));
+    q = fma2(q, t, splat2(EC0));
+    return mul2(mul2(q, t), ex);
+}
 
 // 1/sqrt(x) and 1/x, the hardware approximations with subnormal inputs and
 // results flushed to zero: the pair kernel's r^2 (>= 1e-4 nm^2 for any pair
@@ -68,23 +83,6 @@ __device__ __forceinline__ float rcp_ftz(float x) {
     float y;
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
-}
-
-__device__ __forceinline__ f2p erfc_nr2(f2p z) {
-    const float2 d = up2(fma2(z, splat2(0.5f), splat2(1.f)));
-    const f2p t = pk2(rcp_ftz(d.x), rcp_ftz(d.y));
-    f2p poly = fma2(t, splat2(NR_C9), splat2(NR_C8));
-    poly = fma2(poly, t, splat2(NR_C7));
-    poly = fma2(poly, t, splat2(NR_C6));
-    poly = fma2(poly, t, splat2(NR_C5));
-    poly = fma2(poly, t, splat2(NR_C4));
-    poly = fma2(poly, t, splat2(NR_C3));
-    poly = fma2(poly, t, splat2(NR_C2));
-    poly = fma2(poly, t, splat2(NR_C1));
-    poly = fma2(poly, t, splat2(NR_C0));
-    // (-z^2 + P) log2(e), then 2^x
-    const float2 e = up2(mul2(fma2(mul2(z, z), splat2(-1.f), poly), splat2(1.4426950408889634f)));
-    return mul2(t, pk2(ex2_approx(e.x), ex2_approx(e.y)));
 }
 
 // Work mapping: one warp per i-cluster; the warp takes its list 32 rows at a
@@ -213,8 +211,8 @@ __global__ void __launch_bounds__(256, (EN || EM) ? 2 : 3) k_nonbonded(DevState 
                     //   = -qn e^{-kappa^2 r^2} (poly/r + 2 kappa/sqrt(pi)) / r^2, away from j
                     fs = fma2(mul2(qn, rinv2), mul2(ex, fma2(poly, rinv, splat2(p.two_kappa_sqrtpi))), fs);
                     if (ENERGY) {
-                        // energy steps: the relative-error erfc above for the energy
-                        ec = mul2(mul2(qn, rinv), mul2(splat2(-1.f), erfc_nr2(x)));
+                        // energy steps: the relative-error erfc for the energy
+                        ec = mul2(mul2(qn, rinv), mul2(splat2(-1.f), erfc_from_t(t, ex)));
                     }
                 } else {
                     fs = fma2(mul2(qn, rinv2), rinv, fs);
@@ -492,9 +490,9 @@ __global__ void __launch_bounds__(256, (EN || EM) ? 2 : 3) k_nonbonded_staged(De
                         const f2p ex = pk2(ex2_approx(xs.x), ex2_approx(xs.y));
                         fs = fma2(mul2(qn, rinv2), mul2(ex, fma2(poly, rinv, splat2(p.two_kappa_sqrtpi))), fs);
                         if (ENERGY) {
-                        // energy steps: the relative-error erfc above for the energy
-                        ec = mul2(mul2(qn, rinv), mul2(splat2(-1.f), erfc_nr2(x)));
-                    }
+                            // energy steps: the relative-error erfc for the energy
+                            ec = mul2(mul2(qn, rinv), mul2(splat2(-1.f), erfc_from_t(t, ex)));
+                        }
                     } else {
                         fs = fma2(mul2(qn, rinv2), rinv, fs);
                         if (ENERGY) ec = sub2(zero2, mul2(qn, rinv));

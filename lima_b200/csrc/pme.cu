@@ -763,15 +763,15 @@ int pme_xy_buffer(int k0, int k1) {
 }
 
 // ------------------------------------------------------------------ gather
-// Two threads per atom (adjacent lanes), each taking two z-planes of the stencil:
-// the lane of planes 0 and 1 sums p0 + p1, its partner p2 + p3, and one shuffle
-// gives (p0 + p1) + (p2 + p3).
+// Four threads per atom (adjacent lanes), one z-plane of the stencil each: the
+// first shuffle pairs planes 0 and 1, and 2 and 3, the second gives
+// (p0 + p1) + (p2 + p3).
 // ONE: a single system, whose descriptor sd1 comes as a kernel argument instead
 // of a dependent load through the cluster's system index.
 template <bool ENERGY, bool FD, bool ONE>
 __global__ void k_gather(DevState st, const SysDesc sd1) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int s = t >> 1, half = t & 1;
+    const int s = t >> 2, quarter = t & 3;
     double e = 0.0;
     int sysi = -1;
     float q = 0.f, phi = 0.f, gx = 0.f, gy = 0.f, gz = 0.f, sc0 = 0.f, sc1 = 0.f, sc2 = 0.f;
@@ -804,16 +804,11 @@ __global__ void k_gather(DevState st, const SysDesc sd1) {
                 ixm[a] = wrap1(b0 - 2 + a, K0);
                 iy[a] = wrap1(b1 - 1 + a, K1);
             }
-            // this lane's two planes (selected, so that the weights stay in registers)
-            const float wzh[2] = {half ? wz[2] : wz[0], half ? wz[3] : wz[1]};
-            const float dzh[2] = {half ? dz[2] : dz[0], half ? dz[3] : dz[1]};
-            float ph[2], pgx[2], pgy[2], pgz[2];
-#pragma unroll
-            for (int cc = 0; cc < 2; ++cc) {
-                const int c = 2 * half + cc;
-                float phi = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
+            // this lane's plane of the stencil
+            {
+                const int c = quarter;
                 const int z = wrap1(b2 - 1 + c, K2);
-                const float wzc = wzh[cc], dzc = dzh[cc];
+                const float wzc = pick4(wz, c), dzc = pick4(dz, c);
 #pragma unroll
                 for (int b = 0; b < 4; ++b) {
                     const int y = iy[b];
@@ -838,26 +833,22 @@ __global__ void k_gather(DevState st, const SysDesc sd1) {
                         }
                     }
                 }
-                ph[cc] = phi;
-                pgx[cc] = gx;
-                pgy[cc] = gy;
-                pgz[cc] = gz;
             }
-            phi = ph[0] + ph[1];
-            gx = pgx[0] + pgx[1];
-            gy = pgy[0] + pgy[1];
-            gz = pgz[0] + pgz[1];
             sc0 = FD ? 0.5f * sd.pme_inv_h[0] : sd.pme_inv_h[0];
             sc1 = FD ? 0.5f * sd.pme_inv_h[1] : sd.pme_inv_h[1];
             sc2 = FD ? 0.5f * sd.pme_inv_h[2] : sd.pme_inv_h[2];
         }
     }
-    // (p0 + p1) + (p2 + p3): the partner lane holds the second pair
+    // (p0 + p1) + (p2 + p3)
     phi += __shfl_xor_sync(0xffffffffu, phi, 1);
     gx += __shfl_xor_sync(0xffffffffu, gx, 1);
     gy += __shfl_xor_sync(0xffffffffu, gy, 1);
     gz += __shfl_xor_sync(0xffffffffu, gz, 1);
-    if (sysi >= 0 && half == 0) {
+    phi += __shfl_xor_sync(0xffffffffu, phi, 2);
+    gx += __shfl_xor_sync(0xffffffffu, gx, 2);
+    gy += __shfl_xor_sync(0xffffffffu, gy, 2);
+    gz += __shfl_xor_sync(0xffffffffu, gz, 2);
+    if (sysi >= 0 && quarter == 0) {
         atomic_add_fixed(st.fx + s, to_fixed(-q * gx * sc0, FORCE_SCALE));
         atomic_add_fixed(st.fy + s, to_fixed(-q * gy * sc1, FORCE_SCALE));
         atomic_add_fixed(st.fz + s, to_fixed(-q * gz * sc2, FORCE_SCALE));
@@ -871,7 +862,7 @@ __global__ void k_gather(DevState st, const SysDesc sd1) {
             }
         }
     }
-    if (ENERGY) add_energy_fixed(st.energy, half == 0 ? sysi : -1, e, E_RECIP);
+    if (ENERGY) add_energy_fixed(st.energy, quarter == 0 ? sysi : -1, e, E_RECIP);
 }
 
 // ------------------------------------------------------------------ driver
@@ -911,7 +902,7 @@ int launch_pme(const DevState& st, const PmePlan& plan, bool energy, cudaStream_
         k_fft_x_inv<<<plan.n_items_x, 256, sx, s>>>(st, plans, plan.items_x, mx);
     }
     const SysDesc& sd1 = plan.sys0;
-    const int g1 = (int)(((long long)st.n_slots * 2 + TB - 1) / TB);   // gather: two threads per slot
+    const int g1 = (int)(((long long)st.n_slots * 4 + TB - 1) / TB);   // gather: four threads per slot
     if (plan.n_sys == 1) {
         if (plan.ref_gather) {
             if (energy) k_gather<true, true, true><<<g1, TB, 0, s>>>(st, sd1);
