@@ -45,3 +45,24 @@ def test_droplet_without_boundary(oracle):
 def test_no_boundary_refuses_ewald():
     with pytest.raises(LimaError):
         Engine(cutoff=RC, electrostatics=E.ES_EWALD, periodic=0)
+
+
+def test_system_entirely_outside_box(oracle):
+    """Without a boundary the box only lays out the column grid: a droplet lying
+    wholly at x < 0 is binned in the grid's first column row (each of those
+    columns then holds atoms spread over 2.8 nm in x) and must still give the
+    oracle's forces, before and after 20 steps."""
+    s = droplet()
+    s.pos = s.pos - np.array([6.0, 0.0, 0.0])
+    assert (s.pos[:, 0] < 0).all()
+    e = Engine(cutoff=RC, electrostatics=E.ES_CUTOFF, periodic=0, nstlist=10, dt=1e-6)
+    e.load(s)
+    for n_steps in (0, 20):
+        if n_steps:
+            e.step(n_steps)
+        e.compute_forces(energy=True)
+        pos, _ = e.state()
+        assert (pos[:, 0] < 0).all()
+        fr, _ = oracle_open(oracle, s, pos)
+        assert rel_rms(e.forces(), fr) < 1e-4, (n_steps, rel_rms(e.forces(), fr))
+    assert e.status() & 0x3 == 0      # no pair-list or column overflow
