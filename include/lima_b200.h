@@ -132,7 +132,8 @@ typedef struct lima_params {
        every prune_interval steps, starting at each rebuild, the pair list is cut to
        the rows within an inner radius rc + skin * prune_interval / nstlist of the
        current positions, and the pair kernel walks that shorter list until the
-       next prune; 0 = off; < 0 = auto (every 2 steps when nstlist >= 4) */
+       next prune; 0 = off; < 0 = auto (every 2 steps for an engine of one system with
+       at least 1,024 8-atom clusters and nstlist >= 4, else off) */
     int    prune_interval;
 } lima_params;
 
