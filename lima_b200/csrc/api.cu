@@ -112,6 +112,13 @@ struct lima_engine {
 
     // host mirrors
     std::vector<long long> energy_host;
+    // pinned host words for the small read-backs that end a call (a copy to
+    // pageable memory is staged and takes longer): [0, 2) status word and the
+    // overflow count, [2, 4) the state hand-in's check words, then the energies
+    unsigned* h_pin = nullptr;
+    size_t h_pin_bytes = 0;
+    unsigned last_status = 0;         // status word read at the end of the last run_steps
+    long long* pin_energy() { return reinterpret_cast<long long*>(h_pin + 4); }
     bool energy_valid = false;
     double time_ms = 0.0;
     int64_t timed_steps = 0;
@@ -203,6 +210,9 @@ struct lima_engine {
         drop_graph();
         for (void* a : allocs) cudaFree(a);
         allocs.clear();
+        if (h_pin) cudaFreeHost(h_pin);
+        h_pin = nullptr;
+        h_pin_bytes = 0;
         for (cudaStream_t* s : {&s_main, &s_bonded, &s_pme})
             if (*s) cudaStreamDestroy(*s), *s = nullptr;
         for (cudaEvent_t* e : {&ev_fork, &ev_bonded, &ev_pme, &ev_t0, &ev_t1})
@@ -773,6 +783,9 @@ void lima_engine::setup() {
     d_out_f = dalloc<float>(3 * (size_t)N);
     d_maxf = dalloc<float>(1);
     energy_host.assign((size_t)ns * E_COUNT, 0);
+    h_pin_bytes = 4 * sizeof(unsigned) + energy_host.size() * sizeof(long long);
+    CK(cudaMallocHost((void**)&h_pin, h_pin_bytes));
+    std::memset(h_pin, 0, h_pin_bytes);
 
     built = true;
     state_pending = true;
@@ -1317,10 +1330,14 @@ void lima_engine::run_steps(int n) {
         }
     }
     CK(cudaEventRecord(ev_t1, s_main));
-    CK(cudaMemcpyAsync(energy_host.data(), st.energy, sizeof(long long) * energy_host.size(),
-                       cudaMemcpyDeviceToHost, s_main));
+    // energies and the status word in one read-back, into pinned memory
+    CK(cudaMemcpyAsync(pin_energy(), st.energy, sizeof(long long) * energy_host.size(), cudaMemcpyDeviceToHost,
+                       s_main));
+    CK(cudaMemcpyAsync(h_pin, st.status, sizeof(unsigned), cudaMemcpyDeviceToHost, s_main));
     CK(cudaStreamSynchronize(s_main));
     CK(cudaGetLastError());
+    std::memcpy(energy_host.data(), pin_energy(), sizeof(long long) * energy_host.size());
+    last_status = h_pin[0];
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, ev_t0, ev_t1));
     time_ms += ms;
@@ -1669,20 +1686,32 @@ int lima_set_state(lima_engine* h, const double* pos, const float* vel) {
             // atom has moved more than half the Verlet buffer since it was built.  The
             // input is staged and checked on the device (finite, largest move) before
             // it replaces the slot state.
-            cudaStream_t s = h->s_main;
+            // positions on the main stream, checked as soon as they arrive;
+            // velocities (needed only by the commit) on a second stream, so that
+            // their copy overlaps the check and its read-back
+            cudaStream_t s = h->s_main, sv = h->s_bonded;
             const size_t o = 3 * (size_t)h->n_atoms_off[h->cur];
             CK(cudaMemcpyAsync(h->st.in_pos + o, pos, 3 * (size_t)S.n * sizeof(double), cudaMemcpyHostToDevice, s));
+            CK(cudaEventRecord(h->ev_fork, s));
+            CK(cudaStreamWaitEvent(sv, h->ev_fork, 0));
             if (vel)
-                CK(cudaMemcpyAsync(h->st.in_vel + o, vel, 3 * (size_t)S.n * sizeof(float), cudaMemcpyHostToDevice, s));
+                CK(cudaMemcpyAsync(h->st.in_vel + o, vel, 3 * (size_t)S.n * sizeof(float), cudaMemcpyHostToDevice, sv));
             else
-                CK(cudaMemsetAsync(h->st.in_vel + o, 0, 3 * (size_t)S.n * sizeof(float), s));
+                CK(cudaMemsetAsync(h->st.in_vel + o, 0, 3 * (size_t)S.n * sizeof(float), sv));
+            CK(cudaEventRecord(h->ev_bonded, sv));
             CK(cudaMemsetAsync(h->d_disp, 0, 2 * sizeof(unsigned), s));
             h->launches += launch_check_state(h->st, h->n_atoms_off[h->cur], S.n, h->d_disp, s);
-            unsigned word[2] = {0u, 0u};
-            CK(cudaMemcpyAsync(word, h->d_disp, sizeof(word), cudaMemcpyDeviceToHost, s));
+            CK(cudaMemcpyAsync(h->h_pin + 2, h->d_disp, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
             CK(cudaStreamSynchronize(s));
-            if (word[1] & 1u) return fail(h, LIMA_ERR_NOT_FINITE, "non-finite position");
+            const unsigned word[2] = {h->h_pin[2], h->h_pin[3]};
+            if (word[1] & 1u) {
+                CK(cudaStreamSynchronize(sv));   // the caller may reuse its buffers on return
+                return fail(h, LIMA_ERR_NOT_FINITE, "non-finite position");
+            }
+            CK(cudaStreamWaitEvent(s, h->ev_bonded, 0));
             h->launches += launch_load_state(h->st, h->n_atoms_off[h->cur], S.n, s);
+            // the caller's velocity buffer is read by the copy: done before return
+            CK(cudaStreamSynchronize(sv));
             const unsigned bits = word[0];
             float d2;
             std::memcpy(&d2, &bits, sizeof(float));
@@ -1756,12 +1785,15 @@ int lima_compute_forces(lima_engine* h, int flags) {
         const bool energy = (flags & LIMA_CALC_ENERGY) != 0;
         h->forces(energy);
         if (energy) {
-            CK(cudaMemcpyAsync(h->energy_host.data(), h->st.energy, sizeof(long long) * h->energy_host.size(),
+            CK(cudaMemcpyAsync(h->pin_energy(), h->st.energy, sizeof(long long) * h->energy_host.size(),
                                cudaMemcpyDeviceToHost, h->s_main));
         }
         CK(cudaStreamSynchronize(h->s_main));
         CK(cudaGetLastError());
-        if (energy) h->energy_valid = true;
+        if (energy) {
+            std::memcpy(h->energy_host.data(), h->pin_energy(), sizeof(long long) * h->energy_host.size());
+            h->energy_valid = true;
+        }
         return LIMA_OK;
     });
 }
@@ -1773,8 +1805,7 @@ int lima_step(lima_engine* h, int n_steps) {
         ensure_built(h);
         if (n_steps == 0) return LIMA_OK;
         h->run_steps(n_steps);
-        unsigned status = 0;
-        CK(cudaMemcpy(&status, h->st.status, sizeof(unsigned), cudaMemcpyDeviceToHost));
+        const unsigned status = h->last_status;   // read back with the energies
         if (status & ST_NONFINITE) return fail(h, LIMA_ERR_NOT_FINITE, "non-finite force during stepping");
         if (status & (ST_PAIRLIST_OVERFLOW | ST_COLUMN_OVERFLOW))
             return fail(h, LIMA_ERR_OVERFLOW, "pair list or column capacity exceeded inside a graph replay");
