@@ -436,6 +436,23 @@ void lima_engine::setup() {
         D.n_atoms = S.n;
         D.max_clusters = (S.n + CLUSTER - 1) / CLUSTER + ncols;
         D.cluster_cap_off = cl_off;
+        // pair-kernel warps per i-cluster: one warp per cluster leaves a small
+        // system's SMs short of warps (3,000 atoms: 375 warps on 148 SMs), so an
+        // engine of one system splits its rows over up to 8 warps, aiming at
+        // ~4,096 warps; a batch has warps enough and does not split unless asked
+        // (a fixed pair_split applies to every system alike, so a system then
+        // gives the same bits alone and in a batch)
+        if (p.pair_split > 0) {
+            int k = 1;
+            while (k * 2 <= std::min(8, p.pair_split)) k *= 2;
+            D.nb_parts = k;
+        } else if (p.pair_split < 0 && ns == 1) {
+            const double ncl = std::max(1.0, std::ceil(S.n / (double)CLUSTER));
+            const int e2 = (int)std::floor(std::log2(4096.0 / ncl));
+            D.nb_parts = 1 << std::min(3, std::max(0, e2));
+        } else {
+            D.nb_parts = 1;
+        }
         for (int c = 0; c < D.max_clusters; ++c) cluster_sys.push_back(s);
         for (int c = 0; c < ncols; ++c) col_sys.push_back(s);
         col_off += ncols;
@@ -643,8 +660,18 @@ void lima_engine::setup() {
     for (auto& pr : ev_ph)
         for (cudaEvent_t& e : pr) CK(cudaEventCreate(&e));
 
+    std::vector<int> nb_warp_off(ns + 1, 0);
+    int nb_split = 0;
+    for (int s = 0; s < ns; ++s) {
+        nb_warp_off[s + 1] = nb_warp_off[s] + sd[s].max_clusters * sd[s].nb_parts;
+        if (sd[s].nb_parts > 1) nb_split = 1;
+    }
+
     DevState D{};
     D.n_sys = ns;
+    D.nb_warps = nb_warp_off[ns];
+    D.nb_split = nb_split;
+    D.nb_warp_off = upload(nb_warp_off);
     D.has_field = has_field ? 1 : 0;
     D.periodic = p.periodic ? 1 : 0;
     D.n_atoms = N;
@@ -1481,6 +1508,7 @@ void lima_default_params(lima_params* p) {
     p->log_ring = 5;                // DatabuffersDeviceController::nStepsInBuffer
     p->periodic = 1;                // BoundaryConditionSelect::PBC
     p->prune_interval = -1;         // auto: every 2 steps for one system of >= 1,024 clusters
+    p->pair_split = -1;             // auto: split a small single system's pair-kernel rows
 }
 
 const char* lima_error_string(int code) {

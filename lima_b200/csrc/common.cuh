@@ -56,7 +56,8 @@ struct SysDesc {
     float self_coef;                // per-atom self energy: self_coef * q^2, or self_coef per
     int self_per_charge;            //   charged atom when self_per_charge (reference convention)
     float efield[3];                // uniform external field x 1000: force = q [kC/mol] x efield [J/mol/nm]
-    int pad_[2];
+    int nb_parts;                   // pair-kernel warps per i-cluster (its rows split in 32-row multiples)
+    int pad_;
 };
 
 // scale is a power of two, so v * (float)scale is exact and one float->int64

@@ -41,6 +41,11 @@ struct DevState {
     int has_field = 0;        // some system has an external field: forces start from q E, not zero
     int periodic = 1;         // 0: no boundary condition (no images, no wrapping, plain differences)
     int col_cap = 0;          // atoms a column may hold
+    // pair-kernel warps: system s owns warps [nb_warp_off[s], nb_warp_off[s + 1]),
+    // max_clusters x nb_parts of them; nb_split: some system has nb_parts > 1
+    int nb_warps = 0;
+    int nb_split = 0;
+    const int* nb_warp_off = nullptr;
 
     SysDesc* sys = nullptr;
     int* sys_nclusters = nullptr;   // actual clusters per system (device-written)

@@ -101,7 +101,9 @@ __device__ __forceinline__ float rcp_ftz(float x) {
 // overlaps it; the rows are worked in the same order, so the results are the
 // same bits either way.
 // EM: the energy-minimisation variant (force only, the per-pair LJ clamp above).
-template <int ES, int EN, bool PF, bool EM = false>
+// SPLIT: the rows of a cluster may be split over several warps (a small
+// system's engine, see below); without it a warp is a whole cluster.
+template <int ES, int EN, bool PF, bool EM = false, bool SPLIT = false>
 __global__ void __launch_bounds__(256, (EN || EM) ? 2 : 3) k_nonbonded(DevState st, NbParams p) {
     constexpr bool ENERGY = EN > 0, ATOM = EN > 1;
     // per warp, i-atom pairs (2 ip, 2 ip + 1): (x0, x1, y0, y1), (z0, z1, -q0 ke, -q1 ke),
@@ -110,11 +112,31 @@ __global__ void __launch_bounds__(256, (EN || EM) ? 2 : 3) k_nonbonded(DevState 
     const int wib = threadIdx.x >> 5;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
-    if (warp >= st.n_clusters) return;
-    const int ci = warp;
-    const int n = min(st.walk_count[ci], st.pl_cap);
-    if (n == 0) return;
-    const int sysi = st.cluster_sys[ci];
+    // warp -> (system, i-cluster, part): a small system's rows are split over
+    // nb_parts warps (parts of 32-row multiples, so a row meets the same lane
+    // either way); the system is found by binary search over the warp offsets
+    if (warp >= st.nb_warps) return;
+    int sysi, ci, parts = 1, part = 0;
+    if (!SPLIT) {   // one warp per cluster: no lookups before the row loads
+        ci = warp;
+        sysi = st.cluster_sys[ci];
+    } else {
+        sysi = 0;
+        for (int hi = st.n_sys - 1; sysi < hi;) {
+            const int mid = (sysi + hi + 1) >> 1;
+            if (st.nb_warp_off[mid] <= warp) sysi = mid;
+            else hi = mid - 1;
+        }
+        parts = max(1, st.sys[sysi].nb_parts);
+        const int local = warp - st.nb_warp_off[sysi], lp = __ffs(parts) - 1;
+        ci = st.sys[sysi].cluster_cap_off + (local >> lp);
+        part = local & (parts - 1);
+    }
+    const int n_rows = min(st.walk_count[ci], st.pl_cap);
+    const int chunk = SPLIT ? ((n_rows + parts - 1) / parts + 31) & ~31 : n_rows;
+    const int k_begin = SPLIT ? part * chunk : 0;
+    const int n = SPLIT ? min(n_rows, k_begin + chunk) : n_rows;   // end of this warp's rows
+    if (k_begin >= n) return;
     const float Lx = st.sys[sysi].boxf[0], Ly = st.sys[sysi].boxf[1], Lz = st.sys[sysi].boxf[2];
     if (lane < CLUSTER) {
         const float4 x = st.xyzq[ci * CLUSTER + lane];
@@ -273,9 +295,9 @@ __global__ void __launch_bounds__(256, (EN || EM) ? 2 : 3) k_nonbonded(DevState 
         int sa;
         float4 xa;
         float2 la;
-        int2 rb = load_rowid(32 + lane);
-        load_row(lane, ba, sa, xa, la);
-        for (int k0 = 0; k0 < n; k0 += 32) {
+        int2 rb = load_rowid(k_begin + 32 + lane);
+        load_row(k_begin + lane, ba, sa, xa, la);
+        for (int k0 = k_begin; k0 < n; k0 += 32) {
             const int2 rc = load_rowid(k0 + 64 + lane);
             unsigned bb;
             int sb;
@@ -286,7 +308,7 @@ __global__ void __launch_bounds__(256, (EN || EM) ? 2 : 3) k_nonbonded(DevState 
             ba = bb, sa = sb, xa = xb, la = lb, rb = rc;
         }
     } else {
-        for (int k0 = 0; k0 < n; k0 += 32) {
+        for (int k0 = k_begin; k0 < n; k0 += 32) {
             unsigned ba;
             int sa;
             float4 xa;
@@ -625,18 +647,18 @@ static void launch_nb_staged(const DevState& st, const NbParams& p, bool energy,
 //   bit 1: 128-thread blocks instead of 256;
 //   bit 2: two rows' loads in flight per lane (PF).
 // The engine's autotuner times the shapes on the running system.
-template <int ES>
+template <int ES, bool SP>
 static void launch_nb_shape(const DevState& st, const NbParams& p, bool energy, int shape, cudaStream_t s) {
-    const long long threads = (long long)st.n_clusters * 32;
+    const long long threads = (long long)st.nb_warps * 32;
     if (p.em && !energy) {   // energy minimisation: forces with the per-pair LJ clamp
-        k_nonbonded<ES, 0, false, true><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(st, p);
+        k_nonbonded<ES, 0, false, true, SP><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(st, p);
         return;
     }
     const int tb = (shape & 2) ? 128 : 256;
     const dim3 grid((unsigned)((threads + tb - 1) / tb));
     if (energy) {
-        if (st.atom_energy) k_nonbonded<ES, 2, false><<<grid, tb, 0, s>>>(st, p);
-        else k_nonbonded<ES, 1, false><<<grid, tb, 0, s>>>(st, p);
+        if (st.atom_energy) k_nonbonded<ES, 2, false, false, SP><<<grid, tb, 0, s>>>(st, p);
+        else k_nonbonded<ES, 1, false, false, SP><<<grid, tb, 0, s>>>(st, p);
         return;
     }
     // 24 to 28 warps per SM: 3 blocks of 256 threads (60 KB each) or 7 of 128 (28 KB
@@ -644,23 +666,34 @@ static void launch_nb_shape(const DevState& st, const NbParams& p, bool energy, 
     const int reserve = (shape & 1) ? ((shape & 2) ? 28 * 1024 : 60 * 1024) : 0;
     static std::atomic<unsigned long long> attr{0ull};
     once_per_device(attr, [] {
-        cudaFuncSetAttribute(k_nonbonded<ES, 0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 90 * 1024);
-        cudaFuncSetAttribute(k_nonbonded<ES, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 90 * 1024);
+        cudaFuncSetAttribute(k_nonbonded<ES, 0, false, false, SP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             90 * 1024);
+        cudaFuncSetAttribute(k_nonbonded<ES, 0, true, false, SP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             90 * 1024);
     });
-    if (shape & 4) k_nonbonded<ES, 0, true><<<grid, tb, reserve, s>>>(st, p);
-    else k_nonbonded<ES, 0, false><<<grid, tb, reserve, s>>>(st, p);
+    if (shape & 4) k_nonbonded<ES, 0, true, false, SP><<<grid, tb, reserve, s>>>(st, p);
+    else k_nonbonded<ES, 0, false, false, SP><<<grid, tb, reserve, s>>>(st, p);
+}
+
+template <int ES>
+static void launch_nb_plain(const DevState& st, const NbParams& p, bool energy, int shape, cudaStream_t s) {
+    if (st.nb_split) launch_nb_shape<ES, true>(st, p, energy, shape, s);
+    else launch_nb_shape<ES, false>(st, p, energy, shape, s);
 }
 
 int launch_nonbonded(const DevState& st, const NbParams& p, bool energy, cudaStream_t s, int shape) {
+    // the staged kernel takes whole clusters: with rows split over warps, its
+    // shapes run the plain kernel's matching shape (the same bits either way)
+    if ((shape & 8) && st.nb_split) shape &= 7;
     if (shape & 8) {
         if (p.es_mode == 0) launch_nb_staged<0>(st, p, energy, shape, s);
         else if (p.es_mode == 1) launch_nb_staged<1>(st, p, energy, shape, s);
         else launch_nb_staged<2>(st, p, energy, shape, s);
         return 1;
     }
-    if (p.es_mode == 0) launch_nb_shape<0>(st, p, energy, shape, s);
-    else if (p.es_mode == 1) launch_nb_shape<1>(st, p, energy, shape, s);
-    else launch_nb_shape<2>(st, p, energy, shape, s);
+    if (p.es_mode == 0) launch_nb_plain<0>(st, p, energy, shape, s);
+    else if (p.es_mode == 1) launch_nb_plain<1>(st, p, energy, shape, s);
+    else launch_nb_plain<2>(st, p, energy, shape, s);
     return 1;
 }
 

@@ -62,7 +62,7 @@ class Params(ctypes.Structure):
                 ("use_graphs", ctypes.c_int), ("apply_thermostat", ctypes.c_int),
                 ("thermostat_interval", ctypes.c_int), ("target_temperature", ctypes.c_double),
                 ("log_interval", ctypes.c_int), ("log_ring", ctypes.c_int), ("periodic", ctypes.c_int),
-                ("prune_interval", ctypes.c_int)]
+                ("prune_interval", ctypes.c_int), ("pair_split", ctypes.c_int)]
 
 
 class Energies(ctypes.Structure):

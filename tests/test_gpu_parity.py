@@ -256,6 +256,24 @@ def test_energy_bars_prepared(oracle, cfg):
     check_energy_bars(e.energies(), er)
 
 
+@pytest.mark.parametrize("split", [1, 2, 8])
+def test_pair_split_matches_oracle(oracle, split):
+    """The pair kernel's rows split over 1, 2 or 8 warps per i-cluster: forces
+    and energies against the oracle, and the split results agree with the
+    unsplit ones to FP32 summation order."""
+    s = small_water()
+    kappa = kappa_from_tol(1.0, 1e-5)
+    grid = (48, 48, 48)
+    e = make(s, grid=grid, cutoff=1.0, electrostatics=E.ES_EWALD, ewald_kappa=kappa, pair_split=split)
+    e.compute_forces(energy=True)
+    fr, er = oracle_total(oracle, s, 1.0, 2, kappa, grid)
+    assert rel_rms(e.forces(), fr) < FORCE_TOL
+    check_energies(e.energies(), er)
+    u = make(s, grid=grid, cutoff=1.0, electrostatics=E.ES_EWALD, ewald_kappa=kappa, pair_split=1)
+    u.compute_forces(energy=True)
+    assert rel_rms(e.forces(), u.forces()) < 1e-6
+
+
 # ------------------------------------------------------------- reproducibility
 def test_bit_reproducible():
     s = small_water()
@@ -330,16 +348,20 @@ def test_minimize_reduces_max_force():
 
 
 # --------------------------------------------------------------------- batching
-def test_batch_matches_single():
+@pytest.mark.parametrize("split", [1, 8])
+def test_batch_matches_single(split):
+    """Each system of a batch gives the same bits as the system alone, with the
+    pair kernel's rows unsplit (a batch's default) or split over 8 warps per
+    i-cluster (batch warps mapped to systems by their warp offsets)."""
     sys_list = [systems.water_box(n, L, seed=11 + n, name="b") for n, L in ((600, 2.8), (1500, 3.6), (900, 3.1))]
     grids = [(32, 32, 32), (40, 40, 40), (36, 36, 36)]
-    batch = Engine(n_systems=3, cutoff=1.0)
+    batch = Engine(n_systems=3, cutoff=1.0, pair_split=split)
     for k, (s, g) in enumerate(zip(sys_list, grids)):
         batch.select(k)
         batch.load(s, pme_grid=g)
     batch.compute_forces(energy=True)
     for k, (s, g) in enumerate(zip(sys_list, grids)):
-        single = make(s, grid=g, cutoff=1.0)
+        single = make(s, grid=g, cutoff=1.0, pair_split=split)
         single.compute_forces(energy=True)
         batch.select(k)
         assert np.array_equal(batch.forces(), single.forces())
@@ -383,7 +405,7 @@ def test_batch_with_chains_matches_single():
         batch.load(s)
     batch.step(12)
     for k, s in enumerate(sys_list):
-        single = Engine(cutoff=1.0, pme_spacing=0.12)
+        single = Engine(cutoff=1.0, pme_spacing=0.12, pair_split=1)   # a batch does not split
         single.load(s)
         single.step(12)
         batch.select(k)
