@@ -396,6 +396,7 @@ void lima_engine::setup() {
         const double a = std::cbrt(CLUSTER / rho);
         for (int d = 0; d < 3; ++d) {
             D.box[d] = S.box[d];
+            D.inv_box[d] = 1.0 / S.box[d];
             D.boxf[d] = (float)S.box[d];
             D.inv_boxf[d] = (float)(1.0 / S.box[d]);
         }
@@ -728,6 +729,10 @@ void lima_engine::setup() {
     D.bb_molsig = dalloc<unsigned long long>(n_clusters);
     D.pl_count = dalloc<int>(n_clusters);
     D.pl_row = dalloc<int2>((size_t)n_clusters * pl_cap);
+    if (D.nb_split) {   // the split pair search's per-warp rows (small systems only)
+        D.ps_stage = dalloc<int2>((size_t)D.nb_warps * pl_cap);
+        D.ps_stage_count = dalloc<int>(D.nb_warps);
+    }
     // auto: prune every 2 steps for one system of at least 1,024 clusters.  A
     // smaller system's pair kernel has too few warps to hide the pass's latency
     // (3,000 atoms: 42 -> 47 us per step with pruning), and a batch of small
@@ -1171,13 +1176,14 @@ void lima_engine::finish_rebuild() {
         const long long grown = std::max<long long>((long long)st.pl_cap * 3 / 2, need);
         if (grown > INT_MAX / 2) throw ApiError{LIMA_ERR_OVERFLOW, "pair list too long for one cluster"};
         const int cap = (int)((grown + 31) / 32 * 32);
-        for (void* a : {(void*)st.pl_row, (void*)st.pl_row_in}) {
+        for (void* a : {(void*)st.pl_row, (void*)st.pl_row_in, (void*)st.ps_stage}) {
             if (!a) continue;
             cudaFree(a);
             allocs.erase(std::remove(allocs.begin(), allocs.end(), a), allocs.end());
         }
         st.pl_cap = cap;
         st.pl_row = dalloc<int2>((size_t)st.n_clusters * cap);
+        if (st.nb_split) st.ps_stage = dalloc<int2>((size_t)st.nb_warps * cap);
         if (prune_every > 0) {
             st.pl_row_in = dalloc<int2>((size_t)st.n_clusters * cap);
             st.walk_row = st.pl_row_in;

@@ -38,7 +38,7 @@ __device__ __forceinline__ f3 rel(const DevState& st, const SysDesc& sd, int s0,
     double d[3] = {st.px[s] - st.px[s0], st.py[s] - st.py[s0], st.pz[s] - st.pz[s0]};
     if (st.periodic) {
 #pragma unroll
-        for (int k = 0; k < 3; ++k) d[k] -= sd.box[k] * rint(d[k] / sd.box[k]);
+        for (int k = 0; k < 3; ++k) d[k] -= sd.box[k] * rint(d[k] * sd.inv_box[k]);
     }
     return {(float)d[0], (float)d[1], (float)d[2]};
 }

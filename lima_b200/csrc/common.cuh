@@ -40,6 +40,7 @@ constexpr unsigned ST_MOVED_TOO_FAR = 0x10u;
 // Per-system descriptor (one per system of a batch), resident in global memory.
 struct SysDesc {
     double box[3];        // [nm]
+    double inv_box[3];    // 1 / box
     float boxf[3];
     float inv_boxf[3];
     int atom_off, n_atoms;          // original-order atom range

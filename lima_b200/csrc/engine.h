@@ -108,6 +108,11 @@ struct DevState {
     const int* walk_count = nullptr;
     const int2* walk_row = nullptr;
     int* nb_counter = nullptr;      // next i-cluster of the persistent (staged) pair kernel
+    // split pair search (nb_split): warp w of the search writes its rows to
+    // ps_stage[w * pl_cap ...] and their count to ps_stage_count[w]; a second
+    // kernel concatenates each cluster's parts in order into pl_row
+    int2* ps_stage = nullptr;
+    int* ps_stage_count = nullptr;
 
     // PME
     int* pme_grid_fx = nullptr;          // fixed-point charge grid, GRID32_SCALE (all systems)

@@ -304,19 +304,40 @@ __device__ __forceinline__ bool excluded(const DevState& st, int ai, int aj, int
 constexpr int PS_WARPS = 4;
 constexpr int PS_QCAP = 32 + 32 * 27;   // a full batch left over + one column batch with every shift
 
+// SPLIT (a small system's engine, as in the pair kernel): the warps of an
+// i-cluster share its window, each taking a contiguous slice of the virtual
+// columns; their rows, concatenated in slice order, are the rows one warp would
+// have produced (k_pairsearch_concat).
+template <bool SPLIT>
 __global__ void __launch_bounds__(PS_WARPS * 32, 1) k_pairsearch(DevState st, float rlist) {
     __shared__ int q[PS_WARPS][PS_QCAP];
     __shared__ int s_mi[PS_WARPS][CLUSTER], s_ai[PS_WARPS][CLUSTER];
     __shared__ int s_end[PS_WARPS][32], s_js[PS_WARPS][32], s_sh[PS_WARPS][32];
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    if (warp >= st.n_clusters) return;
-    const int ci = warp;
-    const int sysi = st.cluster_sys[ci];
+    if (warp >= (SPLIT ? st.nb_warps : st.n_clusters)) return;
+    int ci = warp, sysi, parts = 1, part = 0;
+    if (!SPLIT) {
+        sysi = st.cluster_sys[ci];
+    } else {
+        sysi = 0;
+        for (int hi = st.n_sys - 1; sysi < hi;) {
+            const int mid = (sysi + hi + 1) >> 1;
+            if (st.nb_warp_off[mid] <= warp) sysi = mid;
+            else hi = mid - 1;
+        }
+        parts = max(1, st.sys[sysi].nb_parts);
+        const int lw = warp - st.nb_warp_off[sysi], lp = __ffs(parts) - 1;
+        ci = st.sys[sysi].cluster_cap_off + (lw >> lp);
+        part = lw & (parts - 1);
+    }
     const SysDesc& sd = st.sys[sysi];
     const int local = ci - sd.cluster_cap_off;
     if (local >= st.sys_nclusters[sysi]) {
-        if (lane == 0) st.pl_count[ci] = 0;
+        if (lane == 0) {
+            if (SPLIT) st.ps_stage_count[warp] = 0;
+            else st.pl_count[ci] = 0;
+        }
         return;
     }
     const float4 ilo = st.bb_lo[ci], ihi = st.bb_hi[ci];
@@ -378,7 +399,8 @@ __global__ void __launch_bounds__(PS_WARPS * 32, 1) k_pairsearch(DevState st, fl
 
     const int cap = st.pl_cap;
     int count = 0;
-    const size_t base_out = (size_t)ci * cap;
+    int2* const rows_out = SPLIT ? st.ps_stage : st.pl_row;
+    const size_t base_out = (size_t)(SPLIT ? warp : ci) * cap;
 
     // rows of the queued candidates q[head .. head + nb): four candidates per
     // pass, one lane per (candidate, j-atom), each lane testing its j-atom against
@@ -428,7 +450,7 @@ __global__ void __launch_bounds__(PS_WARPS * 32, 1) k_pairsearch(DevState st, fl
             const int pos = count + __popc(has & ((1u << lane) - 1u));
             if (m8 != 0u && pos < cap) {
                 const int img = code % 3 | ((code / 3) % 3) << 2 | (code / 9) << 4;
-                st.pl_row[base_out + pos] = make_int2(sj, (int)m8 | (img << ROW_SHIFT_BIT));
+                rows_out[base_out + pos] = make_int2(sj, (int)m8 | (img << ROW_SHIFT_BIT));
             }
             count += __popc(has);
         }
@@ -465,7 +487,10 @@ __global__ void __launch_bounds__(PS_WARPS * 32, 1) k_pairsearch(DevState st, fl
     }
     int qn = 0;
     const int nwin = (nx > 0 && ny > 0) ? nx * ny * nsz : 0;
-    for (int w0 = 0; w0 < nwin; w0 += 32) {
+    // this warp's slice of the virtual columns
+    const int v_begin = SPLIT ? (int)((long long)nwin * part / parts) : 0;
+    const int v_end = SPLIT ? (int)((long long)nwin * (part + 1) / parts) : nwin;
+    for (int w0 = v_begin; w0 < v_end; w0 += 32) {
         const int v = w0 + lane;
         const int w = v / nsz, vz = v - w * nsz;
         int cnt = 0, jstart = 0, shc = 5 | (1 << 4);   // shc: (sx + 1) | (sy + 1) << 2 | (sz + 1) << 4
@@ -473,7 +498,7 @@ __global__ void __launch_bounds__(PS_WARPS * 32, 1) k_pairsearch(DevState st, fl
         const int ux = cx0 + wx, uy = cy0 + wy;   // unwrapped column
         // a window narrower than the grid sits within one period of it; a column
         // further out (not met in practice) is left out rather than misaddressed
-        if (v < nwin && ux >= -sd.ncol_x && ux < 2 * sd.ncol_x && uy >= -sd.ncol_y && uy < 2 * sd.ncol_y) {
+        if (v < v_end && ux >= -sd.ncol_x && ux < 2 * sd.ncol_x && uy >= -sd.ncol_y && uy < 2 * sd.ncol_y) {
             const int sxc = ux < 0 ? -1 : (ux >= sd.ncol_x ? 1 : 0);
             const int syc = uy < 0 ? -1 : (uy >= sd.ncol_y ? 1 : 0);
             const int col = sd.col_off + (ux - sxc * sd.ncol_x) + sd.ncol_x * (uy - syc * sd.ncol_y);
@@ -607,10 +632,44 @@ __global__ void __launch_bounds__(PS_WARPS * 32, 1) k_pairsearch(DevState st, fl
     }
     if (qn > 0) build_masks(0, qn);
     if (lane == 0) {
-        st.pl_count[ci] = min(count, cap);
-        if (count > cap) {
+        if (SPLIT) {
+            st.ps_stage_count[warp] = count;   // may pass cap: the concatenation flags it
+        } else {
+            st.pl_count[ci] = min(count, cap);
+            if (count > cap) {
+                atomicOr(st.status, ST_PAIRLIST_OVERFLOW);
+                atomicMax(st.status + 1, (unsigned)count);   // the capacity this build needed
+            }
+        }
+    }
+}
+
+// The split search's rows of each i-cluster, part after part, into pl_row: one
+// warp per cluster.  A list longer than the capacity is cut there and flagged
+// with the length it needs, as the unsplit search does.
+__global__ void k_pairsearch_concat(DevState st) {
+    const int ci = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (ci >= st.n_clusters) return;
+    const int sysi = st.cluster_sys[ci];
+    const SysDesc& sd = st.sys[sysi];
+    const int parts = max(1, sd.nb_parts);
+    const int w0 = st.nb_warp_off[sysi] + (ci - sd.cluster_cap_off) * parts;
+    const int cap = st.pl_cap;
+    int2* out = st.pl_row + (size_t)ci * cap;
+    int total = 0;
+    for (int pp = 0; pp < parts; ++pp) {
+        const int c = st.ps_stage_count[w0 + pp];
+        const int2* in = st.ps_stage + (size_t)(w0 + pp) * cap;
+        const int nc = min(c, cap);
+        for (int k = lane; k < nc && total + k < cap; k += 32) out[total + k] = in[k];
+        total += c;
+    }
+    if (lane == 0) {
+        st.pl_count[ci] = min(total, cap);
+        if (total > cap) {
             atomicOr(st.status, ST_PAIRLIST_OVERFLOW);
-            atomicMax(st.status + 1, (unsigned)count);   // the capacity this build needed
+            atomicMax(st.status + 1, (unsigned)total);
         }
     }
 }
@@ -706,9 +765,16 @@ int launch_rebuild_slots(const DevState& st, bool from_input, cudaStream_t s) {
 
 // Stage 8: the pair list of the current slots.
 int launch_pairsearch(const DevState& st, float rlist, cudaStream_t s) {
-    const long long threads = (long long)st.n_clusters * 32;
     const int TP = PS_WARPS * 32;
-    k_pairsearch<<<(unsigned)((threads + TP - 1) / TP), TP, 0, s>>>(st, rlist);
+    if (st.nb_split) {
+        const long long threads = (long long)st.nb_warps * 32;
+        k_pairsearch<true><<<(unsigned)((threads + TP - 1) / TP), TP, 0, s>>>(st, rlist);
+        const long long tc = (long long)st.n_clusters * 32;
+        k_pairsearch_concat<<<(unsigned)((tc + 255) / 256), 256, 0, s>>>(st);
+        return 2;
+    }
+    const long long threads = (long long)st.n_clusters * 32;
+    k_pairsearch<false><<<(unsigned)((threads + TP - 1) / TP), TP, 0, s>>>(st, rlist);
     return 1;
 }
 

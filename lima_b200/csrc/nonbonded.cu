@@ -711,7 +711,7 @@ __global__ void k_exclusion_correction(DevState st, BondedTerms bt, NbParams p) 
         sysi = st.atom_sys[pr.x];
         const SysDesc& sd = st.sys[sysi];
         double d[3] = {st.px[si] - st.px[sj], st.py[si] - st.py[sj], st.pz[si] - st.pz[sj]};
-        for (int k = 0; k < 3; ++k) d[k] -= sd.box[k] * rint(d[k] / sd.box[k]);
+        for (int k = 0; k < 3; ++k) d[k] -= sd.box[k] * rint(d[k] * sd.inv_box[k]);
         const float dx = (float)d[0], dy = (float)d[1], dz = (float)d[2];
         const float r2 = dx * dx + dy * dy + dz * dz;
         const float rinv = rsqrtf(r2);
@@ -773,7 +773,7 @@ __global__ void k_immediate_pairs(DevState st, BondedTerms bt, NbParams p) {
         const SysDesc& sd = st.sys[sysi];
         double d[3] = {st.px[sj] - st.px[si], st.py[sj] - st.py[si], st.pz[sj] - st.pz[si]};   // r_j - r_i
         if (st.periodic)
-            for (int k = 0; k < 3; ++k) d[k] -= sd.box[k] * rint(d[k] / sd.box[k]);
+            for (int k = 0; k < 3; ++k) d[k] -= sd.box[k] * rint(d[k] * sd.inv_box[k]);
         const float dx = (float)d[0], dy = (float)d[1], dz = (float)d[2];
         const float r2 = dx * dx + dy * dy + dz * dz;
         const float rinv = rsqrtf(r2);
