@@ -135,9 +135,9 @@ typedef struct lima_params {
        next prune; 0 = off; < 0 = auto (every 2 steps for an engine of one system with
        at least 1,024 8-atom clusters and nstlist >= 4, else off) */
     int    prune_interval;
-    /* warps per i-cluster in the pair kernel (no counterpart in the reference):
-       1, 2, 4 or 8 (a value in between is rounded down) splits every system's
-       rows over that many warps; < 0 = auto (an engine of one system splits so
+    /* warps per i-cluster in the pair kernel and the pair-list search (no
+       counterpart in the reference): 1, 2, 4 or 8 (a value in between is rounded
+       down) splits every system's rows, and its search window, over that many warps; < 0 = auto (an engine of one system splits so
        that it has up to ~4,096 pair-kernel warps: 8 for 3,000 atoms, 1 from ~16,400;
        a batch does not split); 0 = 1.  Results depend on the split (FP32 sums
        per part), so a system gives the same bits alone and inside a batch when
