@@ -107,7 +107,8 @@ typedef struct lima_params {
     int    exclude_bonded;    /* 1 = every atom pair sharing a bond, angle, dihedral
                                  or improper is excluded from LJ and Coulomb
                                  (code/LIMA_TOOLS/src/CompoundBuilder.cpp:40-60)      */
-    int    use_graphs;        /* 1 = replay each nstlist block of steps as a CUDA graph */
+    int    use_graphs;        /* G > 0: replay each block of G pair-list periods (a rebuild and
+                                 nstlist steps each) as one CUDA graph; 0 = launch eagerly */
     /* thermostat (code/LIMA_ENGINE/src/Thermostat.cuh:55-103, Engine.cu:167-174): every
        thermostat_interval steps the temperature of each system is measured from its
        kinetic energy (3N - 3 degrees of freedom); with apply_thermostat the integrator's

@@ -1232,9 +1232,9 @@ void lima_engine::rebuild_async() {
     ++rebuilds;
 }
 
-// Records one pair-list period — rebuild, then nstlist steps of forces and
-// integration without energies — as a CUDA graph on the main stream (the bonded
-// and PME streams join through the fork/join events).
+// Records use_graphs pair-list periods — each a rebuild, then nstlist steps of
+// forces and integration without energies — as one CUDA graph on the main
+// stream (the bonded and PME streams join through the fork/join events).
 void lima_engine::capture_period() {
     drop_graph();
     const int64_t l0 = launches, r0 = rebuilds;
@@ -1242,25 +1242,27 @@ void lima_engine::capture_period() {
     phase_timing = false;
     cudaGraph_t graph = nullptr;
     CK(cudaStreamBeginCapture(s_main, cudaStreamCaptureModeThreadLocal));
-    rebuild_async();
-    for (int k = 0; k < p.nstlist; ++k) {
-        launches += launch_zero_forces(st, s_main);
-        CK(cudaEventRecord(ev_fork, s_main));
-        CK(cudaStreamWaitEvent(s_bonded, ev_fork, 0));
-        CK(cudaStreamWaitEvent(s_pme, ev_fork, 0));
-        launches += launch_bonded(st, bt, false, s_bonded);
-        if (pme_on) launches += launch_exclusion_correction(st, bt, nb, false, s_bonded);
-        launches += launch_immediate_pairs(st, bt, nb, false, s_bonded);
-        CK(cudaEventRecord(ev_bonded, s_bonded));
-        if (pme_on) launches += launch_pme(st, pp, false, s_pme);
-        CK(cudaEventRecord(ev_pme, s_pme));
-        // the period's pair search overlaps its first bonded and PME work
-        if (k == 0) launches += launch_pairsearch(st, (float)rlist, s_main);
-        if (prune_every > 0 && k % prune_every == 0) launches += launch_prune(st, (float)rin, s_main);
-        launches += launch_nonbonded(st, nb, false, s_main, nb_shape);
-        CK(cudaStreamWaitEvent(s_main, ev_bonded, 0));
-        CK(cudaStreamWaitEvent(s_main, ev_pme, 0));
-        launches += launch_integrate(st, ip, false, s_main);
+    for (int period = 0; period < std::max(1, p.use_graphs); ++period) {
+        rebuild_async();
+        for (int k = 0; k < p.nstlist; ++k) {
+            launches += launch_zero_forces(st, s_main);
+            CK(cudaEventRecord(ev_fork, s_main));
+            CK(cudaStreamWaitEvent(s_bonded, ev_fork, 0));
+            CK(cudaStreamWaitEvent(s_pme, ev_fork, 0));
+            launches += launch_bonded(st, bt, false, s_bonded);
+            if (pme_on) launches += launch_exclusion_correction(st, bt, nb, false, s_bonded);
+            launches += launch_immediate_pairs(st, bt, nb, false, s_bonded);
+            CK(cudaEventRecord(ev_bonded, s_bonded));
+            if (pme_on) launches += launch_pme(st, pp, false, s_pme);
+            CK(cudaEventRecord(ev_pme, s_pme));
+            // the period's pair search overlaps its first bonded and PME work
+            if (k == 0) launches += launch_pairsearch(st, (float)rlist, s_main);
+            if (prune_every > 0 && k % prune_every == 0) launches += launch_prune(st, (float)rin, s_main);
+            launches += launch_nonbonded(st, nb, false, s_main, nb_shape);
+            CK(cudaStreamWaitEvent(s_main, ev_bonded, 0));
+            CK(cudaStreamWaitEvent(s_main, ev_pme, 0));
+            launches += launch_integrate(st, ip, false, s_main);
+        }
     }
     CK(cudaStreamEndCapture(s_main, &graph));
     const cudaError_t e = cudaGraphInstantiate(&graph_exec, graph, 0);
@@ -1319,19 +1321,20 @@ void lima_engine::run_steps(int n) {
     CK(cudaEventRecord(ev_t0, s_main));
     int k = 0;
     if (p.use_graphs && !phase_timing && !state_pending && !learned_active() && p.log_interval <= 0) {
-        // whole pair-list periods replay as one graph; the last step stays eager
-        // so that it can evaluate energies
-        while (n - k > p.nstlist && list_age >= p.nstlist) {
+        // blocks of use_graphs whole pair-list periods replay as one graph; the
+        // last step stays eager so that it can evaluate energies
+        const int periods = std::max(1, p.use_graphs), block = periods * p.nstlist;
+        while (n - k > block && list_age >= p.nstlist) {
             if (!graph_exec) capture_period();
             CK(cudaMemsetAsync(st.status, 0, sizeof(unsigned), s_main));
             CK(cudaGraphLaunch(graph_exec, s_main));
             launches += graph_launches_per_replay;
-            ++rebuilds;
+            rebuilds += periods;
             ++graph_replays;
             list_age = p.nstlist;
-            k += p.nstlist;
+            k += block;
             const int64_t before = step;
-            step += p.nstlist;
+            step += block;
             // a thermostat measurement due inside the replayed period is taken after it
             if (p.thermostat_interval > 0 && step / p.thermostat_interval != before / p.thermostat_interval)
                 measure_temperature();

@@ -382,17 +382,20 @@ def test_nonfinite_positions_rejected():
 
 
 def test_graph_replay_equals_eager():
-    """Pair-list periods replayed as CUDA graphs give the same trajectory bits."""
+    """Pair-list periods replayed as CUDA graphs, one or two periods per graph,
+    give the same trajectory bits as eager launches."""
     s = small_water(n_waters=1500, box=3.6)
     out = []
-    for graphs in (0, 1):
+    for graphs in (0, 1, 2):
         e = make(s, grid=(40, 40, 40), cutoff=1.0, nstlist=10, use_graphs=graphs)
         e.step(1)
         e.step(45)
         p, v = e.state()
         out.append((p, v, e.energies()["total"], e.timings()))
-    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
-    assert out[0][2] == out[1][2]
+    for o in out[1:]:
+        assert np.array_equal(out[0][0], o[0]) and np.array_equal(out[0][1], o[1])
+        assert out[0][2] == o[2]
+    assert out[2][3]["rebuilds"] == out[1][3]["rebuilds"] == out[0][3]["rebuilds"]
 
 
 def test_batch_with_chains_matches_single():
