@@ -41,6 +41,8 @@ def test_default_params_and_errors_without_device():
     lib = E.load_library()
     p = E.default_params()
     assert p.nstlist == 10 and abs(p.dt - 1e-6) < 1e-18 and p.electrostatics == E.ES_EWALD
+    # automatic pruning and pair-kernel row split, eager launches by default
+    assert p.prune_interval < 0 and p.pair_split < 0 and p.use_graphs == 0
     assert lib.lima_error_string(E.LIMA_OK) == b"ok"
     h = ctypes.c_void_p()
     assert lib.lima_create(ctypes.byref(p), ctypes.byref(h)) == 0
