@@ -805,6 +805,7 @@ void lima_engine::setup() {
     nb.ke = (float)kCoulomb;
     nb.two_kappa_sqrtpi = (float)(2.0 * kappa / std::sqrt(p.ref_compat ? kPiRef : kPi));
     nb.mk2_log2e = (float)(-kappa * kappa / std::log(2.0));
+    nb.p_kappa = AS_P * (float)kappa;
     nb.em = 0;
     ip.dt = p.dt;
     ip.integrator = p.integrator;

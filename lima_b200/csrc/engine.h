@@ -148,6 +148,8 @@ struct BondedTerms {
     int2* midx = nullptr;
 };
 
+// p of the Abramowitz & Stegun 7.1.26 erfc form the pair kernel uses
+constexpr float AS_P = 0.3275911f;
 struct NbParams {
     float rc2;
     float rlist;          // cutoff + skin
@@ -156,6 +158,7 @@ struct NbParams {
     float ke;             // Coulomb constant
     float two_kappa_sqrtpi;
     float mk2_log2e;      // -kappa^2 log2(e): exp(-kappa^2 r^2) = 2^(mk2_log2e r^2)
+    float p_kappa;        // AS_P kappa: the pair kernel's erfc takes t = 1/(1 + p kappa r)
     int em;               // energy minimisation: force-only launches take the pair kernel's EM variant
 };
 // periodic image of a pair-list row: (sx + 1) | (sy + 1) << 2 | (sz + 1) << 4 in bits

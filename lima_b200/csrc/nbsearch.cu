@@ -5,7 +5,8 @@
 //   1. k_bin            atom -> column of an x-y grid (wrapped positions)
 //   2. k_scan_columns   per-system exclusive scans: atom and cluster offsets
 //   3. k_scatter        atoms -> column lists (unordered)
-//   4. k_sort_columns   deterministic order inside a column: (z, atom index)
+//   4. k_sort_columns   deterministic order inside a column: (z, atom index),
+//                       then in each cluster of 8 the atoms with LJ first
 //   5. k_gather_slots   state permuted into the new slot order
 //   6. k_finish_slots   slot_of map, permuted velocity state
 //   7. k_bbox           per-cluster bounding boxes
@@ -184,9 +185,28 @@ __global__ void k_sort_columns(DevState st, const int* col_sys) {
             }
             __syncthreads();
         }
-    // ranks past the column's cluster range are cut (overflow, flagged below)
-    for (int r = threadIdx.x; r < padded; r += blockDim.x)
-        st.new_orig[slot0 + r] = r < n ? (int)(keys[r] & 0xffffffffu) : -1;
+    // Clusters are runs of 8 ranks; inside each, the atoms with LJ (eps != 0) take
+    // the first slots, each part in z order (so the pair kernel can leave the LJ
+    // arithmetic out for the cluster's trailing LJ-free atom pairs: in water the
+    // hydrogens).  The cluster's atom set, and so its box, is that of the z order.
+    // Ranks past the column's cluster range are cut (overflow, flagged below).
+    for (int g = threadIdx.x; g * CLUSTER < padded; g += blockDim.x) {
+        int a[CLUSTER];
+        unsigned lj = 0u;
+#pragma unroll
+        for (int r = 0; r < CLUSTER; ++r) {
+            const int rr = g * CLUSTER + r;
+            a[r] = rr < n ? (int)(keys[rr] & 0xffffffffu) : -1;
+            if (a[r] >= 0 && st.ljp_atom[a[r]].y != 0.f) lj |= 1u << r;
+        }
+        int out = 0;
+#pragma unroll
+        for (int r = 0; r < CLUSTER; ++r)
+            if ((lj >> r) & 1u) st.new_orig[slot0 + g * CLUSTER + out++] = a[r];
+#pragma unroll
+        for (int r = 0; r < CLUSTER; ++r)   // then the other atoms, padding (-1) last
+            if (!((lj >> r) & 1u)) st.new_orig[slot0 + g * CLUSTER + out++] = a[r];
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
         if (n_all > st.col_cap) atomicOr(st.status, ST_COLUMN_OVERFLOW);

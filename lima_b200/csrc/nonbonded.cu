@@ -15,6 +15,8 @@
 // row of the list (a j-atom with an 8-bit mask of the i-atoms it meets) and
 // walks the 8 i-atoms.  Forces are added as int64 fixed point, so the result
 // does not depend on the order in which warps finish.
+#include <type_traits>
+
 #include "engine.h"
 #include "packed.cuh"
 
@@ -24,7 +26,7 @@ namespace lima {
 // Abramowitz & Stegun, Handbook of Mathematical Functions, 7.1.26 (|error| <=
 // 1.5e-7).  Its exp(-x^2) factor is the one the Ewald force's Gaussian term
 // needs, so the pair costs one exponential and one reciprocal.
-constexpr float AS_P = 0.3275911f;
+// (AS_P, the p of the form, is in engine.h: the host folds it into NbParams::p_kappa)
 constexpr float AS_A1 = 0.254829592f, AS_A2 = -0.284496736f, AS_A3 = 1.421413741f;
 constexpr float AS_A4 = -1.453152027f, AS_A5 = 1.061405429f;
 
@@ -85,6 +87,140 @@ __device__ __forceinline__ float rcp_ftz(float x) {
     return y;
 }
 
+// One pair-list row: the lane's j-atom against the 8 i-atoms of its warp's
+// cluster, two at a time, (2 ip, 2 ip + 1) for ip = 0..3, in packed FP32.
+// sxy, szq, slj: the cluster's i-atom pairs in shared memory, (x0, x1, y0, y1),
+// (z0, z1, -q0 ke, -q1 ke), (sigma0/2, sigma1/2, 24 sqrt(eps0), 24 sqrt(eps1)).
+// NLJ: the i-pairs ip < NLJ carry LJ; the pairs above hold only atoms with
+// eps = 0, whose LJ force and energy are exactly zero against any j-atom, so
+// their LJ arithmetic is left out (a cluster's atoms with LJ come first in its
+// slots; in water 60 % of the i-pairs are LJ-free).  Leaving it out changes no
+// bit: the LJ term would add +-0 to the same Coulomb product.
+// The pair force is rinv^2 (LJ + Coulomb) with both terms taken times r^2:
+//   LJ r^2 = 24 eps s6 (1 - 2 s6),  Coulomb r^2 = -qn e^{-k^2 r^2} (poly/r + 2k/sqrt(pi))
+// (Ewald), -qn/r (plain cutoff).  Every lane evaluates both elements of every
+// pair (straight-line code over the four pairs, which the scheduler
+// interleaves); the mask bit of each element is folded into its cutoff (rc^2,
+// or -1: never met) and elements outside the mask or the cutoff — possibly
+// non-finite, e.g. a padding slot at distance 0 — are dropped by the select.
+template <int ES, int EN, bool EM, int NLJ>
+__device__ __forceinline__ void pair_row(const float4* sxy, const float4* szq, const float4* slj,
+                                         const NbParams& p, unsigned bits, float4 xj, float2 ljj,
+                                         f2p (&fix)[4], f2p (&fiy)[4], f2p (&fiz)[4], f2p (&ei)[4],
+                                         f2p& fjx, f2p& fjy, f2p& fjz, f2p& ej,
+                                         f2p& r_elj, f2p& r_ec, f2p& r_vir) {
+    constexpr bool ENERGY = EN > 0, ATOM = EN > 1;
+    const f2p zero2 = splat2(0.f), one2 = splat2(1.f), mtwo2 = splat2(-2.f);
+    const f2p jx = splat2(xj.x), jy = splat2(xj.y), jz = splat2(xj.z);
+    const f2p jsig = splat2(ljj.x), jeps = splat2(ljj.y), jq = splat2(xj.w);
+#pragma unroll
+    for (int ip = 0; ip < 4; ++ip) {
+        const bool lj = ip < NLJ;
+        const float tha = (bits >> (2 * ip)) & 1u ? p.rc2 : -1.f;
+        const float thb = (bits >> (2 * ip + 1)) & 1u ? p.rc2 : -1.f;
+        const float4 vxy = sxy[ip], vzq = szq[ip];
+        const f2p dx = sub2(jx, pk2(vxy.x, vxy.y));
+        const f2p dy = sub2(jy, pk2(vxy.z, vxy.w));
+        const f2p dz = sub2(jz, pk2(vzq.x, vzq.y));
+        const f2p r2 = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
+        const float2 r2v = up2(r2);
+        const bool oka = r2v.x <= tha, okb = r2v.y <= thb;
+        const f2p rinv = pk2(rsqrt_ftz(r2v.x), rsqrt_ftz(r2v.y));
+        const f2p rinv2 = mul2(rinv, rinv);
+        f2p eps24 = zero2, s6 = zero2, lj_r2 = zero2, flj = zero2;
+        if (lj) {
+            const float4 vlj = slj[ip];
+            const f2p sig = add2(pk2(vlj.x, vlj.y), jsig);
+            eps24 = mul2(pk2(vlj.z, vlj.w), jeps);
+            const f2p s2 = mul2(mul2(sig, sig), rinv2);
+            s6 = mul2(mul2(s2, s2), s2);
+            lj_r2 = mul2(mul2(eps24, s6), fma2(s6, mtwo2, one2));   // 24 eps s6 (1 - 2 s6)
+            if (EM) {
+                // energy minimisation: the LJ force alone passes the reference's clamp
+                const float2 v = up2(mul2(lj_r2, rinv2)), rr = up2(mul2(r2, rinv));
+                flj = pk2(em_lj_clamp(v.x, rr.x), em_lj_clamp(v.y, rr.y));
+            }
+        }
+        f2p fs = zero2, ec = zero2;
+        if (ES != 0) {
+            // qn = -k_e q_i q_j (the sign rides on the i-charge)
+            const f2p qn = mul2(pk2(vzq.z, vzq.w), jq);
+            if (ES == 2) {
+                const f2p r = mul2(r2, rinv);
+                const float2 den = up2(fma2(splat2(p.p_kappa), r, one2));   // 1 + p kappa r
+                const f2p t = pk2(rcp_ftz(den.x), rcp_ftz(den.y));
+                // erfc(kappa r) = poly e^{-kappa^2 r^2}
+                const f2p poly = mul2(t, fma2(t, fma2(t, fma2(t, fma2(t, splat2(AS_A5), splat2(AS_A4)),
+                                                            splat2(AS_A3)), splat2(AS_A2)), splat2(AS_A1)));
+                const float2 xs = up2(mul2(r2, splat2(p.mk2_log2e)));
+                const f2p ex = pk2(ex2_approx(xs.x), ex2_approx(xs.y));
+                const f2p g = fma2(poly, rinv, splat2(p.two_kappa_sqrtpi));
+                const f2p qe = mul2(qn, ex);
+                if (EM) fs = lj ? fma2(mul2(qe, rinv2), g, flj) : mul2(mul2(qe, rinv2), g);
+                else fs = mul2(lj ? fma2(qe, g, lj_r2) : mul2(qe, g), rinv2);
+                if (ENERGY) ec = mul2(mul2(qn, rinv), mul2(splat2(-1.f), erfc_from_t(t, ex)));
+            } else {
+                if (EM) fs = lj ? fma2(mul2(qn, rinv2), rinv, flj) : mul2(mul2(qn, rinv2), rinv);
+                else fs = mul2(lj ? fma2(qn, rinv, lj_r2) : mul2(qn, rinv), rinv2);
+                if (ENERGY) ec = sub2(zero2, mul2(qn, rinv));
+            }
+        } else if (lj) {
+            fs = EM ? flj : mul2(lj_r2, rinv2);
+        }
+        float2 fsv = up2(fs);
+        if (EM) {   // a non-finite Coulomb term (coincident atoms) kept finite
+            fsv.x = fmaxf(fminf(fsv.x, 1e20f), -1e20f);
+            fsv.y = fmaxf(fminf(fsv.y, 1e20f), -1e20f);
+        }
+        fs = pk2(oka ? fsv.x : 0.f, okb ? fsv.y : 0.f);
+        // force on i: fs d; on j: -fs d (both summed as +fs d, j negated at the end)
+        fix[ip] = fma2(fs, dx, fix[ip]);
+        fiy[ip] = fma2(fs, dy, fiy[ip]);
+        fiz[ip] = fma2(fs, dz, fiz[ip]);
+        fjx = fma2(fs, dx, fjx);
+        fjy = fma2(fs, dy, fjy);
+        fjz = fma2(fs, dz, fjz);
+        if (ENERGY) {
+            const float2 ecv = up2(ec);
+            const f2p ecm = pk2(oka ? ecv.x : 0.f, okb ? ecv.y : 0.f);
+            f2p elj = zero2;
+            if (lj) {
+                // 4 eps s6 (s6 - 1) = (24 eps / 6) s6 (s6 - 1); dropped like the force
+                const float2 eljv = up2(mul2(mul2(eps24, splat2(1.f / 6.f)), mul2(s6, sub2(s6, one2))));
+                elj = pk2(oka ? eljv.x : 0.f, okb ? eljv.y : 0.f);
+                r_elj = add2(r_elj, elj);
+            }
+            // the row's sums in packed FP32 (at most 8 terms), then FP64 per row
+            r_ec = add2(r_ec, ecm);
+            r_vir = fma2(fs, r2, r_vir);   // fs is already dropped; -1/2 r_ij . f_ij = fs r^2 / 2
+            if (ATOM) {
+                const f2p eh = mul2(splat2(0.5f), lj ? add2(elj, ecm) : ecm);
+                ei[ip] = add2(ei[ip], eh);
+                ej = add2(ej, eh);
+            }
+        }
+    }
+}
+
+// The number of leading i-pairs (2 ip, 2 ip + 1) of a cluster that hold an atom
+// with LJ (eps != 0), from the ballot of those atoms over the cluster's 8 slots.
+__device__ __forceinline__ int lj_pairs_of(unsigned lj_atoms) {
+    return lj_atoms ? ((31 - __clz(lj_atoms)) >> 1) + 1 : 0;
+}
+
+// Calls f(std::integral_constant<int, NLJ>) for the runtime count nlj (0..4), so
+// that a warp's whole walk over its rows is one specialisation.
+template <typename F>
+__device__ __forceinline__ void with_lj_pairs(int nlj, F&& f) {
+    switch (nlj) {
+        case 0: f(std::integral_constant<int, 0>{}); break;
+        case 1: f(std::integral_constant<int, 1>{}); break;
+        case 2: f(std::integral_constant<int, 2>{}); break;
+        case 3: f(std::integral_constant<int, 3>{}); break;
+        default: f(std::integral_constant<int, 4>{}); break;
+    }
+}
+
 // Work mapping: one warp per i-cluster; the warp takes its list 32 rows at a
 // time and each lane owns one row: a j-atom whose 8-bit mask names the i-atoms
 // it interacts with (rows whose mask would be empty are not in the list, so no
@@ -138,9 +274,10 @@ __global__ void __launch_bounds__(256, (EN || EM) ? 2 : 3) k_nonbonded(DevState 
     const int n = SPLIT ? min(n_rows, k_begin + chunk) : n_rows;   // end of this warp's rows
     if (k_begin >= n) return;
     const float Lx = st.sys[sysi].boxf[0], Ly = st.sys[sysi].boxf[1], Lz = st.sys[sysi].boxf[2];
+    float2 lj_i = make_float2(0.f, 0.f);
     if (lane < CLUSTER) {
         const float4 x = st.xyzq[ci * CLUSTER + lane];
-        const float2 lj = st.ljp[ci * CLUSTER + lane];
+        lj_i = st.ljp[ci * CLUSTER + lane];
         const int ip = lane >> 1, h = lane & 1;   // pair ip holds atoms 2 ip and 2 ip + 1
         float* xy = reinterpret_cast<float*>(&s_xy[wib][ip]);
         float* zq = reinterpret_cast<float*>(&s_zq[wib][ip]);
@@ -149,15 +286,16 @@ __global__ void __launch_bounds__(256, (EN || EM) ? 2 : 3) k_nonbonded(DevState 
         xy[2 + h] = x.y;
         zq[h] = x.z;
         zq[2 + h] = -x.w * p.ke;  // i-charges carry minus the Coulomb constant
-        lv[h] = lj.x;
-        lv[2 + h] = 24.f * lj.y;  // the LJ force prefactor folded into the i side
+        lv[h] = lj_i.x;
+        lv[2 + h] = 24.f * lj_i.y;  // the LJ force prefactor folded into the i side
     }
+    // i-pairs with LJ: the cluster's atoms with eps != 0 lead its slots
+    const int nlj = lj_pairs_of(__ballot_sync(0xffffffffu, lj_i.y != 0.f));
     __syncwarp();
     f2p fix[4], fiy[4], fiz[4], ei[4];
     const f2p zero2 = splat2(0.f);
 #pragma unroll
     for (int ip = 0; ip < 4; ++ip) fix[ip] = fiy[ip] = fiz[ip] = ei[ip] = zero2;
-    const f2p one2 = splat2(1.f), mtwo2 = splat2(-2.f);
     // energy steps: per-lane FP64 sums of the pair energies and virial terms
     double s_elj = 0.0, s_ec = 0.0, s_vir = 0.0;
     const size_t base = (size_t)ci * st.pl_cap;
@@ -183,140 +321,62 @@ __global__ void __launch_bounds__(256, (EN || EM) ? 2 : 3) k_nonbonded(DevState 
     auto load_row = [&](int k, unsigned& bits, int& sj, float4& xj, float2& ljj) {
         load_j(k, load_rowid(k), bits, sj, xj, ljj);
     };
-    auto do_row = [&](unsigned bits, int sj, float4 xj, float2 ljj) {
-        f2p fjx = zero2, fjy = zero2, fjz = zero2, ej = zero2;
-        const f2p jx = splat2(xj.x), jy = splat2(xj.y), jz = splat2(xj.z);
-        const f2p jsig = splat2(ljj.x), jeps = splat2(ljj.y), jq = splat2(xj.w);
-        f2p r_elj = zero2, r_ec = zero2, r_vir = zero2;   // the row's energy sums (energy steps)
-#pragma unroll
-        for (int ip = 0; ip < 4; ++ip) {
-            // the mask bit of each element folded into its cutoff: rc^2, or -1 (never met).
-            // Every lane evaluates both elements of every pair (straight-line code over
-            // the four pairs, which the scheduler interleaves), and elements outside the
-            // mask or the cutoff — possibly non-finite, e.g. a padding slot at distance
-            // 0 — are dropped by the select.
-            const float tha = (bits >> (2 * ip)) & 1u ? p.rc2 : -1.f;
-            const float thb = (bits >> (2 * ip + 1)) & 1u ? p.rc2 : -1.f;
-            const float4 vxy = s_xy[wib][ip], vzq = s_zq[wib][ip], vlj = s_lj[wib][ip];
-            const f2p dx = sub2(jx, pk2(vxy.x, vxy.y));
-            const f2p dy = sub2(jy, pk2(vxy.z, vxy.w));
-            const f2p dz = sub2(jz, pk2(vzq.x, vzq.y));
-            const f2p r2 = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
-            const float2 r2v = up2(r2);
-            const bool oka = r2v.x <= tha, okb = r2v.y <= thb;
-            const f2p rinv = pk2(rsqrt_ftz(r2v.x), rsqrt_ftz(r2v.y));
-            const f2p rinv2 = mul2(rinv, rinv);
-            const f2p sig = add2(pk2(vlj.x, vlj.y), jsig);
-            const f2p eps24 = mul2(pk2(vlj.z, vlj.w), jeps);
-            const f2p s2 = mul2(mul2(sig, sig), rinv2);
-            const f2p s6 = mul2(mul2(s2, s2), s2);
-            // LJ: 24 eps s6 (1 - 2 s6) / r^2
-            f2p fs = mul2(mul2(eps24, s6), mul2(rinv2, fma2(s6, mtwo2, one2)));
-            if (EM) {
-                const float2 v = up2(fs), rr = up2(mul2(r2, rinv));
-                fs = pk2(em_lj_clamp(v.x, rr.x), em_lj_clamp(v.y, rr.y));
-            }
-            f2p ec = zero2;
-            if (ES != 0) {
-                // qn = -k_e q_i q_j (the sign rides on the i-charge)
-                const f2p qn = mul2(pk2(vzq.z, vzq.w), jq);
-                if (ES == 2) {
-                    const f2p x = mul2(mul2(r2, rinv), splat2(p.kappa));   // kappa r
-                    const float2 den = up2(fma2(splat2(AS_P), x, one2));
-                    const f2p t = pk2(rcp_ftz(den.x), rcp_ftz(den.y));
-                    // erfc(kappa r) = poly e^{-kappa^2 r^2}
-                    const f2p poly = mul2(t, fma2(t, fma2(t, fma2(t, fma2(t, splat2(AS_A5), splat2(AS_A4)),
-                                                                splat2(AS_A3)), splat2(AS_A2)), splat2(AS_A1)));
-                    const float2 xs = up2(mul2(r2, splat2(p.mk2_log2e)));
-                    const f2p ex = pk2(ex2_approx(xs.x), ex2_approx(xs.y));
-                    // k_e q_i q_j [erfc(kappa r)/r + 2 kappa/sqrt(pi) e^{-kappa^2 r^2}] / r^2
-                    //   = -qn e^{-kappa^2 r^2} (poly/r + 2 kappa/sqrt(pi)) / r^2, away from j
-                    fs = fma2(mul2(qn, rinv2), mul2(ex, fma2(poly, rinv, splat2(p.two_kappa_sqrtpi))), fs);
-                    if (ENERGY) {
-                        // energy steps: the relative-error erfc for the energy
-                        ec = mul2(mul2(qn, rinv), mul2(splat2(-1.f), erfc_from_t(t, ex)));
-                    }
-                } else {
-                    fs = fma2(mul2(qn, rinv2), rinv, fs);
-                    if (ENERGY) ec = sub2(zero2, mul2(qn, rinv));
-                }
-            }
-            float2 fsv = up2(fs);
-            if (EM) {   // a non-finite Coulomb term (coincident atoms) kept finite
-                fsv.x = fmaxf(fminf(fsv.x, 1e20f), -1e20f);
-                fsv.y = fmaxf(fminf(fsv.y, 1e20f), -1e20f);
-            }
-            fs = pk2(oka ? fsv.x : 0.f, okb ? fsv.y : 0.f);
-            // force on i: fs d; on j: -fs d (both summed as +fs d, j negated at the end)
-            fix[ip] = fma2(fs, dx, fix[ip]);
-            fiy[ip] = fma2(fs, dy, fiy[ip]);
-            fiz[ip] = fma2(fs, dz, fiz[ip]);
-            fjx = fma2(fs, dx, fjx);
-            fjy = fma2(fs, dy, fjy);
-            fjz = fma2(fs, dz, fjz);
+    // the warp's rows, one specialisation per number of LJ i-pairs
+    auto walk = [&](auto nlj_c) {
+        constexpr int NLJ = decltype(nlj_c)::value;
+        auto do_row = [&](unsigned bits, int sj, float4 xj, float2 ljj) {
+            f2p fjx = zero2, fjy = zero2, fjz = zero2, ej = zero2;
+            f2p r_elj = zero2, r_ec = zero2, r_vir = zero2;   // the row's energy sums (energy steps)
+            pair_row<ES, EN, EM, NLJ>(s_xy[wib], s_zq[wib], s_lj[wib], p, bits, xj, ljj, fix, fiy, fiz, ei,
+                                      fjx, fjy, fjz, ej, r_elj, r_ec, r_vir);
             if (ENERGY) {
-                // 4 eps s6 (s6 - 1) = (24 eps / 6) s6 (s6 - 1); dropped like the force
-                const float2 eljv = up2(mul2(mul2(eps24, splat2(1.f / 6.f)), mul2(s6, sub2(s6, one2))));
-                const float2 ecv = up2(ec);
-                const f2p elj = pk2(oka ? eljv.x : 0.f, okb ? eljv.y : 0.f);
-                const f2p ecm = pk2(oka ? ecv.x : 0.f, okb ? ecv.y : 0.f);
-                // the row's sums in packed FP32 (at most 8 terms), then FP64 per row
-                r_elj = add2(r_elj, elj);
-                r_ec = add2(r_ec, ecm);
-                r_vir = fma2(fs, r2, r_vir);   // fs is already dropped; -1/2 r_ij . f_ij = fs r^2 / 2
+                const float2 a = up2(r_elj), c = up2(r_ec), v = up2(r_vir);
+                s_elj += (double)a.x + (double)a.y;
+                s_ec += (double)c.x + (double)c.y;
+                s_vir += (double)v.x + (double)v.y;
+            }
+            if (bits) {
+                const float2 x = up2(fjx), y = up2(fjy), z = up2(fjz);
+                atomic_add_fixed(st.fx + sj, to_fixed(-(x.x + x.y), FORCE_SCALE));
+                atomic_add_fixed(st.fy + sj, to_fixed(-(y.x + y.y), FORCE_SCALE));
+                atomic_add_fixed(st.fz + sj, to_fixed(-(z.x + z.y), FORCE_SCALE));
                 if (ATOM) {
-                    const f2p eh = mul2(splat2(0.5f), add2(elj, ecm));
-                    ei[ip] = add2(ei[ip], eh);
-                    ej = add2(ej, eh);
+                    const float2 e = up2(ej);
+                    add_atom_energy(st.epot, sj, (double)(e.x + e.y));
                 }
             }
-        }
-        if (ENERGY) {
-            const float2 a = up2(r_elj), c = up2(r_ec), v = up2(r_vir);
-            s_elj += (double)a.x + (double)a.y;
-            s_ec += (double)c.x + (double)c.y;
-            s_vir += (double)v.x + (double)v.y;
-        }
-        if (bits) {
-            const float2 x = up2(fjx), y = up2(fjy), z = up2(fjz);
-            atomic_add_fixed(st.fx + sj, to_fixed(-(x.x + x.y), FORCE_SCALE));
-            atomic_add_fixed(st.fy + sj, to_fixed(-(y.x + y.y), FORCE_SCALE));
-            atomic_add_fixed(st.fz + sj, to_fixed(-(z.x + z.y), FORCE_SCALE));
-            if (ATOM) {
-                const float2 e = up2(ej);
-                add_atom_energy(st.epot, sj, (double)(e.x + e.y));
-            }
-        }
-    };
-    if (PF) {
-        // software pipeline: while a lane works on row k, the j-atom loads of row
-        // k + 32 and the row load of row k + 64 are in flight
-        unsigned ba;
-        int sa;
-        float4 xa;
-        float2 la;
-        int2 rb = load_rowid(k_begin + 32 + lane);
-        load_row(k_begin + lane, ba, sa, xa, la);
-        for (int k0 = k_begin; k0 < n; k0 += 32) {
-            const int2 rc = load_rowid(k0 + 64 + lane);
-            unsigned bb;
-            int sb;
-            float4 xb;
-            float2 lb;
-            load_j(k0 + 32 + lane, rb, bb, sb, xb, lb);
-            do_row(ba, sa, xa, la);
-            ba = bb, sa = sb, xa = xb, la = lb, rb = rc;
-        }
-    } else {
-        for (int k0 = k_begin; k0 < n; k0 += 32) {
+        };
+        if (PF) {
+            // software pipeline: while a lane works on row k, the j-atom loads of row
+            // k + 32 and the row load of row k + 64 are in flight
             unsigned ba;
             int sa;
             float4 xa;
             float2 la;
-            load_row(k0 + lane, ba, sa, xa, la);
-            do_row(ba, sa, xa, la);
+            int2 rb = load_rowid(k_begin + 32 + lane);
+            load_row(k_begin + lane, ba, sa, xa, la);
+            for (int k0 = k_begin; k0 < n; k0 += 32) {
+                const int2 rc = load_rowid(k0 + 64 + lane);
+                unsigned bb;
+                int sb;
+                float4 xb;
+                float2 lb;
+                load_j(k0 + 32 + lane, rb, bb, sb, xb, lb);
+                do_row(ba, sa, xa, la);
+                ba = bb, sa = sb, xa = xb, la = lb, rb = rc;
+            }
+        } else {
+            for (int k0 = k_begin; k0 < n; k0 += 32) {
+                unsigned ba;
+                int sa;
+                float4 xa;
+                float2 la;
+                load_row(k0 + lane, ba, sa, xa, la);
+                do_row(ba, sa, xa, la);
+            }
         }
-    }
+    };
+    with_lj_pairs(nlj, walk);
     // i-forces: sum each of the 24 values over the warp; lane a (< 8) adds atom a's
     float fi[CLUSTER][3], eiv[CLUSTER];
 #pragma unroll
@@ -403,7 +463,7 @@ __global__ void __launch_bounds__(256, (EN || EM) ? 2 : 3) k_nonbonded_staged(De
     extern __shared__ __align__(16) unsigned char nb_smem[];
     NbWarpStage& S = reinterpret_cast<NbWarpStage*>(nb_smem)[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
-    const f2p zero2 = splat2(0.f), one2 = splat2(1.f), mtwo2 = splat2(-2.f);
+    const f2p zero2 = splat2(0.f);
     for (;;) {
         int ci = 0;
         if (lane == 0) ci = atomicAdd(counter, 1);
@@ -472,82 +532,11 @@ __global__ void __launch_bounds__(256, (EN || EM) ? 2 : 3) k_nonbonded_staged(De
             xj.y += fmaf((float)((img >> 2) & 3u), Ly, -Ly);
             xj.z += fmaf((float)(img >> 4), Lz, -Lz);
             f2p fjx = zero2, fjy = zero2, fjz = zero2, ej = zero2;
-            const f2p jx = splat2(xj.x), jy = splat2(xj.y), jz = splat2(xj.z);
-            const f2p jsig = splat2(ljj.x), jeps = splat2(ljj.y), jq = splat2(xj.w);
             f2p r_elj = zero2, r_ec = zero2, r_vir = zero2;   // the row's energy sums (energy steps)
-#pragma unroll
-            for (int ip = 0; ip < 4; ++ip) {
-                // mask bit folded into the cutoff; elements outside the mask or the
-                // cutoff (possibly non-finite: padding) are dropped by the select
-                const float tha = (bits >> (2 * ip)) & 1u ? p.rc2 : -1.f;
-                const float thb = (bits >> (2 * ip + 1)) & 1u ? p.rc2 : -1.f;
-                const float4 vxy = S.xy[ip], vzq = S.zq[ip], vlj = S.ljp[ip];
-                const f2p dx = sub2(jx, pk2(vxy.x, vxy.y));
-                const f2p dy = sub2(jy, pk2(vxy.z, vxy.w));
-                const f2p dz = sub2(jz, pk2(vzq.x, vzq.y));
-                const f2p r2 = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
-                const float2 r2v = up2(r2);
-                const bool oka = r2v.x <= tha, okb = r2v.y <= thb;
-                const f2p rinv = pk2(rsqrt_ftz(r2v.x), rsqrt_ftz(r2v.y));
-                const f2p rinv2 = mul2(rinv, rinv);
-                const f2p sig = add2(pk2(vlj.x, vlj.y), jsig);
-                const f2p eps24 = mul2(pk2(vlj.z, vlj.w), jeps);
-                const f2p s2 = mul2(mul2(sig, sig), rinv2);
-                const f2p s6 = mul2(mul2(s2, s2), s2);
-                f2p fs = mul2(mul2(eps24, s6), mul2(rinv2, fma2(s6, mtwo2, one2)));
-                if (EM) {
-                    const float2 v = up2(fs), rr = up2(mul2(r2, rinv));
-                    fs = pk2(em_lj_clamp(v.x, rr.x), em_lj_clamp(v.y, rr.y));
-                }
-                f2p ec = zero2;
-                if (ES != 0) {
-                    const f2p qn = mul2(pk2(vzq.z, vzq.w), jq);
-                    if (ES == 2) {
-                        const f2p x = mul2(mul2(r2, rinv), splat2(p.kappa));
-                        const float2 den = up2(fma2(splat2(AS_P), x, one2));
-                        const f2p t = pk2(rcp_ftz(den.x), rcp_ftz(den.y));
-                        const f2p poly = mul2(t, fma2(t, fma2(t, fma2(t, fma2(t, splat2(AS_A5), splat2(AS_A4)),
-                                                                    splat2(AS_A3)), splat2(AS_A2)), splat2(AS_A1)));
-                        const float2 xs = up2(mul2(r2, splat2(p.mk2_log2e)));
-                        const f2p ex = pk2(ex2_approx(xs.x), ex2_approx(xs.y));
-                        fs = fma2(mul2(qn, rinv2), mul2(ex, fma2(poly, rinv, splat2(p.two_kappa_sqrtpi))), fs);
-                        if (ENERGY) {
-                            // energy steps: the relative-error erfc for the energy
-                            ec = mul2(mul2(qn, rinv), mul2(splat2(-1.f), erfc_from_t(t, ex)));
-                        }
-                    } else {
-                        fs = fma2(mul2(qn, rinv2), rinv, fs);
-                        if (ENERGY) ec = sub2(zero2, mul2(qn, rinv));
-                    }
-                }
-                float2 fsv = up2(fs);
-                if (EM) {
-                    fsv.x = fmaxf(fminf(fsv.x, 1e20f), -1e20f);
-                    fsv.y = fmaxf(fminf(fsv.y, 1e20f), -1e20f);
-                }
-                fs = pk2(oka ? fsv.x : 0.f, okb ? fsv.y : 0.f);
-                // force on i: fs d; on j: -fs d (both summed as +fs d, j negated at the end)
-                fix[ip] = fma2(fs, dx, fix[ip]);
-                fiy[ip] = fma2(fs, dy, fiy[ip]);
-                fiz[ip] = fma2(fs, dz, fiz[ip]);
-                fjx = fma2(fs, dx, fjx);
-                fjy = fma2(fs, dy, fjy);
-                fjz = fma2(fs, dz, fjz);
-                if (ENERGY) {
-                    const float2 eljv = up2(mul2(mul2(eps24, splat2(1.f / 6.f)), mul2(s6, sub2(s6, one2))));
-                    const float2 ecv = up2(ec);
-                    const f2p elj = pk2(oka ? eljv.x : 0.f, okb ? eljv.y : 0.f);
-                    const f2p ecm = pk2(oka ? ecv.x : 0.f, okb ? ecv.y : 0.f);
-                    r_elj = add2(r_elj, elj);
-                    r_ec = add2(r_ec, ecm);
-                    r_vir = fma2(fs, r2, r_vir);
-                    if (ATOM) {
-                        const f2p eh = mul2(splat2(0.5f), add2(elj, ecm));
-                        ei[ip] = add2(ei[ip], eh);
-                        ej = add2(ej, eh);
-                    }
-                }
-            }
+            // every i-pair takes the LJ arithmetic here (the same bits as leaving it
+            // out for the LJ-free pairs, as the plain kernel does)
+            pair_row<ES, EN, EM, 4>(S.xy, S.zq, S.ljp, p, bits, xj, ljj, fix, fiy, fiz, ei, fjx, fjy, fjz, ej,
+                                    r_elj, r_ec, r_vir);
             if (ENERGY) {
                 const float2 a = up2(r_elj), c = up2(r_ec), v = up2(r_vir);
                 s_elj += (double)a.x + (double)a.y;

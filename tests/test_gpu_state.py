@@ -102,18 +102,23 @@ def test_autotune_shapes_give_identical_trajectories():
     assert a.energies()["potential"] == b.energies()["potential"]
 
 
+@pytest.mark.parametrize("prune", [-1, 2])
 @pytest.mark.parametrize("split", [1, -1])
 @pytest.mark.parametrize("es", [E.ES_CUTOFF, E.ES_EWALD])
-def test_every_pair_kernel_shape_gives_the_same_bits(es, split):
+def test_every_pair_kernel_shape_gives_the_same_bits(es, split, prune):
     """The eight shapes of the plain pair kernel and the four of the staged,
     persistent one: forces (a step with a rebuild and the next one) and the
     energies of an energy step are bitwise identical — with whole clusters per
     warp, and with this small box's automatic row split (where the staged
-    shapes run the plain kernel)."""
+    shapes run the plain kernel), on the built list and on a pruned one.  The
+    plain kernel leaves the LJ arithmetic out for the LJ-free (hydrogen)
+    i-pairs; the staged one evaluates LJ for every pair, so equal bits show
+    that leaving it out changes nothing."""
     s = systems.water_box(1500, 3.6, seed=8, name="w")
     ref = None
     for shape in [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11]:
-        e = Engine(cutoff=1.0, electrostatics=es, ewald_tol=1e-5, nstlist=10, pair_split=split)
+        e = Engine(cutoff=1.0, electrostatics=es, ewald_tol=1e-5, nstlist=10, pair_split=split,
+                   prune_interval=prune)
         e.load(s, pme_grid=(30, 30, 30) if es == E.ES_EWALD else None)
         e.set_pair_shape(shape)
         e.compute_forces(energy=False)
