@@ -737,7 +737,10 @@ void lima_engine::setup() {
     // smaller system's pair kernel has too few warps to hide the pass's latency
     // (3,000 atoms: 42 -> 47 us per step with pruning), and a batch of small
     // systems gains nothing (32 systems, 280k atoms: 571 -> 578 us); from
-    // 2,000 clusters on it pays (16,828 atoms: 80 -> 76 us; 100,200: 1.5 %)
+    // 2,000 clusters on it pays (16,828 atoms: 80 -> 76 us; 100,200: 1.5 %).
+    // Longer intervals are about even on the 100,200-atom box: 182.7, 183.3,
+    // 181.7 and 181.1 us per step pruning every 2, 3, 4 and 5 steps (4.55, 4.67,
+    // 4.78 and 4.89 M rows walked of 5.52 M built, 31 us per pass)
     const bool prune_auto = p.nstlist >= 4 && D.n_sys == 1 && n_clusters >= 1024;
     prune_every = p.prune_interval < 0 ? (prune_auto ? 2 : 0) : p.prune_interval;
     if (prune_every >= p.nstlist) prune_every = 0;   // the rebuild already cuts at rc + skin
