@@ -1,11 +1,14 @@
 """Coefficients of the pair kernel's energy-step erfc (nonbonded.cu, EC_*).
 
-erfc(x) e^{x^2} is fitted as t (c0 + c1 t + ... + c9 t^9) with
+erfc(x) e^{x^2} is fitted as t (c0 + c1 t + ... + c7 t^7) with
 t = 1 / (1 + p x), p = 0.3275911 (the same t as the force's Abramowitz & Stegun
 7.1.26 form, so an energy step reuses the force's reciprocal and e^{-x^2}):
 weighted least squares for the relative error on 6,000 Chebyshev nodes of t
-over x in [0, 7].  Maximum relative error 7e-10 in exact arithmetic, 2e-7
-with the polynomial evaluated by Horner's rule in FP32.
+over x in [0, 5.5].  Maximum relative error 6e-8 in exact arithmetic, 4.4e-7
+with t, the polynomial (Horner's rule) and the product in FP32 — the same as a
+degree-9 fit over [0, 7], whose extra accuracy the FP32 evaluation loses.
+Past x = 5.5 (erfc < 1e-14, nothing a sum of pair energies can see) the
+polynomial is extrapolated, within 2e-4 relative up to x = 30.
 
     python lima_b200/csrc/erfcx_fit.py
 """
@@ -13,8 +16,8 @@ import numpy as np
 from scipy.special import erfcx
 
 P = 0.3275911
-X_MAX = 7.0
-DEG = 9
+X_MAX = 5.5
+DEG = 7
 
 
 def fit():

@@ -47,22 +47,20 @@ __device__ __forceinline__ float ex2_approx(float x) {
     asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
 }
-// erfc for the energy of energy steps: erfc(x) = t (c0 + c1 t + ... + c9 t^9) e^{-x^2}
+// erfc for the energy of energy steps: erfc(x) = t (c0 + c1 t + ... + c7 t^7) e^{-x^2}
 // with the force's t = 1/(1 + p x) and e^{-x^2}, so an energy step adds only this
 // polynomial to the force's arithmetic.  The coefficients are this build's own
-// weighted least-squares fit of erfc(x) e^{x^2} over x in [0, 7]
-// (lima_b200/csrc/erfcx_fit.py): relative error below 7e-10 in exact arithmetic,
-// 2e-7 evaluated in FP32 — the relative bound a total energy needs, where the
-// force's A&S form only bounds the absolute error (1.5e-7).
-constexpr float EC0 = 0.184739336f, EC1 = 0.186472416f, EC2 = 0.16061303f, EC3 = 0.227135599f;
-constexpr float EC4 = -0.106458984f, EC5 = 0.59804976f, EC6 = -0.668688476f, EC7 = 0.704147577f;
-constexpr float EC8 = -0.348146588f, EC9 = 0.0621363297f;
+// weighted least-squares fit of erfc(x) e^{x^2} over x in [0, 5.5]
+// (lima_b200/csrc/erfcx_fit.py): relative error below 6e-8 in exact arithmetic,
+// 4.4e-7 evaluated in FP32 — the relative bound a total energy needs, where the
+// force's A&S form only bounds the absolute error (1.5e-7).  Past x = 5.5, where
+// erfc < 1e-14, the polynomial is extrapolated (2e-4 relative up to x = 30).
+constexpr float EC0 = 0.185084581f, EC1 = 0.180205658f, EC2 = 0.209264949f, EC3 = 0.014182996f;
+constexpr float EC4 = 0.474507362f, EC5 = -0.428924263f, EC6 = 0.509979844f, EC7 = -0.144301191f;
 
 // erfc(x) from the force's t and e^{-x^2} (packed pairs)
 __device__ __forceinline__ f2p erfc_from_t(f2p t, f2p ex) {
-    f2p q = fma2(t, splat2(EC9), splat2(EC8));
-    q = fma2(q, t, splat2(EC7));
-    q = fma2(q, t, splat2(EC6));
+    f2p q = fma2(t, splat2(EC7), splat2(EC6));
     q = fma2(q, t, splat2(EC5));
     q = fma2(q, t, splat2(EC4));
     q = fma2(q, t, splat2(EC3));
