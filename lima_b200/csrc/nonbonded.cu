@@ -156,11 +156,11 @@ __device__ __forceinline__ void pair_row(const float4* sxy, const float4* szq, c
                 const f2p qe = mul2(qn, ex);
                 if (EM) fs = lj ? fma2(mul2(qe, rinv2), g, flj) : mul2(mul2(qe, rinv2), g);
                 else fs = mul2(lj ? fma2(qe, g, lj_r2) : mul2(qe, g), rinv2);
-                if (ENERGY) ec = mul2(mul2(qn, rinv), mul2(splat2(-1.f), erfc_from_t(t, ex)));
+                if (ENERGY) ec = mul2(mul2(qn, rinv), erfc_from_t(t, ex));   // minus the pair energy
             } else {
                 if (EM) fs = lj ? fma2(mul2(qn, rinv2), rinv, flj) : mul2(mul2(qn, rinv2), rinv);
                 else fs = mul2(lj ? fma2(qn, rinv, lj_r2) : mul2(qn, rinv), rinv2);
-                if (ENERGY) ec = sub2(zero2, mul2(qn, rinv));
+                if (ENERGY) ec = mul2(qn, rinv);   // minus the pair energy
             }
         } else if (lj) {
             fs = EM ? flj : mul2(lj_r2, rinv2);
@@ -179,20 +179,23 @@ __device__ __forceinline__ void pair_row(const float4* sxy, const float4* szq, c
         fjy = fma2(fs, dy, fjy);
         fjz = fma2(fs, dz, fjz);
         if (ENERGY) {
+            // the row sums carry minus the Coulomb energy and six times the LJ energy
+            // (24 eps s6 (s6 - 1) = 6 x 4 eps s6 (s6 - 1)); the kernel's FP64 totals
+            // take the sign and the sixth once per warp.  Dropped like the force.
             const float2 ecv = up2(ec);
             const f2p ecm = pk2(oka ? ecv.x : 0.f, okb ? ecv.y : 0.f);
-            f2p elj = zero2;
+            f2p elj6 = zero2;
             if (lj) {
-                // 4 eps s6 (s6 - 1) = (24 eps / 6) s6 (s6 - 1); dropped like the force
-                const float2 eljv = up2(mul2(mul2(eps24, splat2(1.f / 6.f)), mul2(s6, sub2(s6, one2))));
-                elj = pk2(oka ? eljv.x : 0.f, okb ? eljv.y : 0.f);
-                r_elj = add2(r_elj, elj);
+                const float2 eljv = up2(mul2(eps24, mul2(s6, sub2(s6, one2))));
+                elj6 = pk2(oka ? eljv.x : 0.f, okb ? eljv.y : 0.f);
+                r_elj = add2(r_elj, elj6);
             }
             // the row's sums in packed FP32 (at most 8 terms), then FP64 per row
             r_ec = add2(r_ec, ecm);
             r_vir = fma2(fs, r2, r_vir);   // fs is already dropped; -1/2 r_ij . f_ij = fs r^2 / 2
-            if (ATOM) {
-                const f2p eh = mul2(splat2(0.5f), lj ? add2(elj, ecm) : ecm);
+            if (ATOM) {   // half of each pair's energy to each atom
+                const f2p eh = lj ? fma2(elj6, splat2(1.f / 12.f), mul2(ecm, splat2(-0.5f)))
+                                  : mul2(ecm, splat2(-0.5f));
                 ei[ip] = add2(ei[ip], eh);
                 ej = add2(ej, eh);
             }
@@ -330,7 +333,7 @@ __global__ void __launch_bounds__(256, (EN || EM) ? 2 : 3) k_nonbonded(DevState 
             if (ENERGY) {
                 const float2 a = up2(r_elj), c = up2(r_ec), v = up2(r_vir);
                 s_elj += (double)a.x + (double)a.y;
-                s_ec += (double)c.x + (double)c.y;
+                s_ec -= (double)c.x + (double)c.y;
                 s_vir += (double)v.x + (double)v.y;
             }
             if (bits) {
@@ -411,7 +414,7 @@ __global__ void __launch_bounds__(256, (EN || EM) ? 2 : 3) k_nonbonded(DevState 
         if (ATOM) add_atom_energy(st.epot, si, (double)ve);
     }
     if (ENERGY) {
-        add_energy_fixed(st.energy, sysi, s_elj, E_LJ);
+        add_energy_fixed(st.energy, sysi, s_elj * (1.0 / 6.0), E_LJ);
         add_energy_fixed(st.energy, sysi, s_ec, E_COUL);
         add_energy_fixed(st.energy, sysi, 0.5 * s_vir, E_VIRIAL);
     }
@@ -538,7 +541,7 @@ __global__ void __launch_bounds__(256, (EN || EM) ? 2 : 3) k_nonbonded_staged(De
             if (ENERGY) {
                 const float2 a = up2(r_elj), c = up2(r_ec), v = up2(r_vir);
                 s_elj += (double)a.x + (double)a.y;
-                s_ec += (double)c.x + (double)c.y;
+                s_ec -= (double)c.x + (double)c.y;
                 s_vir += (double)v.x + (double)v.y;
             }
             if (bits) {
@@ -588,7 +591,7 @@ __global__ void __launch_bounds__(256, (EN || EM) ? 2 : 3) k_nonbonded_staged(De
             if (ATOM) add_atom_energy(st.epot, si, (double)ve);
         }
         if (ENERGY) {
-            add_energy_fixed(st.energy, sysi, s_elj, E_LJ);
+            add_energy_fixed(st.energy, sysi, s_elj * (1.0 / 6.0), E_LJ);
             add_energy_fixed(st.energy, sysi, s_ec, E_COUL);
             add_energy_fixed(st.energy, sysi, 0.5 * s_vir, E_VIRIAL);
         }
