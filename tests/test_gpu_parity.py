@@ -132,6 +132,51 @@ def test_ewald_pme_accurate(oracle):
     check_energies(e.energies(), er)
 
 
+def lj_pattern(s, pattern, seed=3):
+    """The water box with other atoms LJ-free (epsilon = 0): all of them, only
+    the oxygens (the hydrogens given a small LJ site), or a random half of the
+    atoms (hydrogens with LJ too), so clusters carry every count of LJ atoms."""
+    sig, eps = s.sigma.copy(), s.epsilon.copy()
+    hyd = eps == 0.0
+    if pattern == "none":
+        eps[:] = 0.0
+    else:
+        sig[hyd], eps[hyd] = 0.1, 100.0
+        if pattern == "oxygens_free":
+            eps[~hyd] = 0.0
+        else:
+            eps[np.random.default_rng(seed).random(s.n) < 0.5] = 0.0
+    return systems.System(**{**s.__dict__, "sigma": sig.astype(np.float32), "epsilon": eps.astype(np.float32)})
+
+
+@pytest.mark.parametrize("pattern", ["none", "oxygens_free", "random_half"])
+def test_lj_free_atoms(oracle, pattern):
+    """The pair kernel leaves the LJ arithmetic out for a cluster's trailing
+    i-atom pairs without LJ (each cluster's LJ atoms take its first slots).
+    Whatever atoms are LJ-free, forces of force-only and energy steps and the
+    energy terms match the oracle, and the staged kernel, which evaluates LJ for
+    every pair, gives the same bits as the plain one."""
+    s = lj_pattern(small_water(), pattern)
+    kappa = kappa_from_tol(1.0, 1e-5)
+    grid = (48, 48, 48)
+    fr, er = oracle_total(oracle, s, 1.0, 2, kappa, grid)
+    got = []
+    for shape in (0, 8):
+        e = make(s, grid=grid, cutoff=1.0, electrostatics=E.ES_EWALD, ewald_kappa=kappa, pair_split=1)
+        e.set_pair_shape(shape)
+        e.compute_forces(energy=False)
+        f0 = e.forces()
+        e.compute_forces(energy=True)
+        got.append((f0, e.forces(), e.energies()))
+        e.close()
+    for f0, f1, en in got:
+        assert rel_rms(f0, fr) < FORCE_TOL, rel_rms(f0, fr)
+        assert rel_rms(f1, fr) < FORCE_TOL, rel_rms(f1, fr)
+        check_energies(en, er)
+    assert np.array_equal(got[0][0], got[1][0]) and np.array_equal(got[0][1], got[1][1])
+    assert all(got[0][2][k] == got[1][2][k] for k in ("lj", "coulomb_real", "virial"))
+
+
 def test_ewald_pme_reference_conventions(oracle):
     """ref_compat: kappa = 3/rc, sinc^8 influence, central-difference gather, no
     exclusion correction, the reference's per-atom self-energy bookkeeping."""
