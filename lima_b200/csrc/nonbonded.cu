@@ -229,7 +229,9 @@ __device__ __forceinline__ void with_lj_pairs(int nlj, F&& f) {
 // 8 i-atoms two at a time, (2 ip, 2 ip + 1) for ip = 0..3, in packed FP32 (read as
 // float4 pairs from shared memory), keeps its j-atom's force in a packed
 // register and adds it once per row; the i-forces live in 12 packed registers
-// per lane and are reduced across the warp once, after the list.
+// per lane and are reduced across the warp once, after the list.  The walk is
+// compiled once per count of the cluster's i-pairs with LJ (pair_row's NLJ),
+// chosen per warp from a ballot of its atoms' epsilon.
 // Pair arithmetic per lane and the order of every sum are fixed, so results
 // are bit-reproducible.
 // EN: 0 forces only, 1 forces and energy totals, 2 also per-atom energy shares.
